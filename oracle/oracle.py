@@ -1,0 +1,325 @@
+"""ctypes access to the oracle (CPU restatement) and to the reference harness.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()`` as the checker and
+by bench.py's CPU-baseline and reference legs. Never imported by the product package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_I = np.int32
+_D = np.float64
+
+
+def _p(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _load(path):
+    lib = C.CDLL(path)
+    return lib
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        from . import build as _b  # type: ignore
+        _lib = _load(_b.build_oracle())
+        _lib.or_dot.restype = C.c_double
+        for name in ("or_ilu_create", "or_amg_setup"):
+            getattr(_lib, name).restype = C.c_void_p
+        for name in ("or_ilu_colours", "or_ilu_factor", "or_ilu_apply", "or_ilu_free", "or_ilu_export",
+                     "or_amg_num_levels", "or_amg_level_info", "or_amg_level_agg", "or_amg_level_csr",
+                     "or_amg_level_dinv", "or_amg_coarse_n", "or_amg_coarse", "or_amg_apply", "or_amg_free"):
+            getattr(_lib, name).argtypes = None
+    return _lib
+
+
+def ref():
+    """The reference's own code (host parts run anywhere; GPU parts need a GPU)."""
+    global _ref
+    if _ref is None:
+        from . import build as _b  # type: ignore
+        path = _b.build_ref()
+        if path is None:
+            raise RuntimeError("reference harness library not built")
+        _ref = _load(path)
+        _ref.ref_spectral_radius.restype = C.c_double
+        _ref.ref_amg_host_setup.restype = C.c_void_p
+        _ref.ref_amg_host_omega.restype = C.c_double
+        _ref.ref_step_create.restype = C.c_void_p
+        _ref.ref_step_amg_setup.restype = C.c_double
+        _ref.ref_step_run.restype = C.c_double
+        for name in ("ref_amg_host_levels", "ref_amg_host_level", "ref_amg_host_omega",
+                     "ref_amg_host_coarse_inv", "ref_amg_host_free", "ref_step_amg_setup", "ref_step_run",
+                     "ref_step_systems", "ref_step_free"):
+            getattr(_ref, name).argtypes = None
+    return _ref
+
+
+def i32(a):
+    return np.ascontiguousarray(a, dtype=_I)
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=_D)
+
+
+# ---------------------------------------------------------------------------------------------
+# CSR
+# ---------------------------------------------------------------------------------------------
+def csr_build(n, elem_v):
+    ev = i32(elem_v)
+    ne = ev.size // 3
+    rp = np.zeros(n + 1, _I)
+    nnz = lib().or_csr_count(n, ne, _p(ev), _p(rp))
+    ci = np.zeros(nnz, _I)
+    lib().or_csr_fill(n, ne, _p(ev), _p(rp), _p(ci))
+    return rp, ci
+
+
+def spmv(rp, ci, val, x):
+    n = rp.size - 1
+    y = np.zeros(n, _D)
+    lib().or_spmv(n, _p(i32(rp)), _p(i32(ci)), _p(f64(val)), _p(f64(x)), _p(y))
+    return y
+
+
+def csr_multiply(A, B):
+    """A, B: (rows, cols, rp, ci, v) tuples. Reference host SpGEMM order."""
+    ar, ac, arp, aci, av = A
+    br, bc, brp, bci, bv = B
+    crp = np.zeros(ar + 1, _I)
+    nnz = lib().or_csr_multiply(ar, ac, _p(arp), _p(aci), _p(av), bc, _p(brp), _p(bci), _p(bv), _p(crp), None, None)
+    cci = np.zeros(nnz, _I)
+    cv = np.zeros(nnz, _D)
+    lib().or_csr_multiply(ar, ac, _p(arp), _p(aci), _p(av), bc, _p(brp), _p(bci), _p(bv), _p(crp), _p(cci), _p(cv))
+    return (ar, bc, crp, cci, cv)
+
+
+def csr_transpose(A):
+    rows, cols, rp, ci, v = A
+    trp = np.zeros(cols + 1, _I)
+    tci = np.zeros(ci.size, _I)
+    tv = np.zeros(ci.size, _D)
+    lib().or_csr_transpose(rows, cols, _p(rp), _p(ci), _p(v), _p(trp), _p(tci), _p(tv))
+    return (cols, rows, trp, tci, tv)
+
+
+# ---------------------------------------------------------------------------------------------
+# assembly
+# ---------------------------------------------------------------------------------------------
+class MomParams(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("dt", "nu", "rho", "a0", "a1", "a2", "c1", "c2", "tau_time", "skew_coef")]
+
+
+def bdf2_params(dt=1e-3, nu=1e-3, rho=1.0, tau_time=1e-3, skew=0.5, bdf2=True):
+    if bdf2:
+        return MomParams(dt, nu, rho, 1.5 / dt, 2.0 / dt, -0.5 / dt, 2.0, -1.0, tau_time, skew)
+    return MomParams(dt, nu, rho, 1.0 / dt, 1.0 / dt, 0.0, 1.0, 0.0, tau_time, skew)
+
+
+def assemble_momentum(mesh, rp, ci, u_old, v_old, u_prev, v_prev, p_old, prm):
+    n, ne = mesh.n, mesh.ne
+    A = np.zeros(rp[-1], _D)
+    ru, rv, m = np.zeros(n, _D), np.zeros(n, _D), np.zeros(n, _D)
+    lib().or_assemble_momentum(n, ne, _p(mesh.elem_v), _p(f64(mesh.x)), _p(f64(mesh.y)), _p(f64(u_old)),
+                               _p(f64(v_old)), _p(f64(u_prev)), _p(f64(v_prev)), _p(f64(p_old)), C.byref(prm),
+                               _p(rp), _p(ci), _p(A), _p(ru), _p(rv), _p(m))
+    return A, ru, rv, m
+
+
+def apply_bc_momentum(mesh, rp, ci, A, ru, rv, u, v, u_max=1.5, H=1.0, outlet_dirichlet=0, outlet_scale=1.0):
+    lib().or_apply_bc_momentum(mesh.n, _p(i32(mesh.tag)), _p(f64(mesh.y)), C.c_double(u_max), C.c_double(H),
+                               outlet_dirichlet, C.c_double(outlet_scale), _p(rp), _p(ci), _p(A), _p(ru), _p(rv),
+                               _p(u), _p(v))
+
+
+def oss_weights(mesh, u, v, dt, rho, nu, stab):
+    s = np.zeros(mesh.ne, _D)
+    lib().or_oss_weights(mesh.ne, _p(mesh.elem_v), _p(f64(mesh.x)), _p(f64(mesh.y)), _p(f64(u)), _p(f64(v)),
+                         C.c_double(dt), C.c_double(rho), C.c_double(nu), C.c_double(stab), _p(s))
+    return s
+
+
+def scalar_gradient(mesh, f, elem_s):
+    gx, gy = np.zeros(mesh.n, _D), np.zeros(mesh.n, _D)
+    lib().or_scalar_gradient(mesh.ne, _p(mesh.elem_v), _p(f64(mesh.x)), _p(f64(mesh.y)), _p(f64(f)),
+                             _p(f64(elem_s)) if elem_s is not None else None, _p(gx), _p(gy))
+    return gx, gy
+
+
+def lumped_mass(mesh):
+    m = np.zeros(mesh.n, _D)
+    lib().or_lumped_mass(mesh.n, mesh.ne, _p(mesh.elem_v), _p(f64(mesh.x)), _p(f64(mesh.y)), _p(m))
+    return m
+
+
+def assemble_ppe(mesh, rp, ci, u, v, p, gpx, gpy, mass, elem_s, dt, rho, stab):
+    Kp = np.zeros(rp[-1], _D)
+    rhs, div = np.zeros(mesh.n, _D), np.zeros(mesh.n, _D)
+    lib().or_assemble_ppe(mesh.n, mesh.ne, _p(mesh.elem_v), _p(f64(mesh.x)), _p(f64(mesh.y)), _p(f64(u)), _p(f64(v)),
+                          _p(f64(p)), _p(f64(gpx)), _p(f64(gpy)), _p(f64(mass)), _p(f64(elem_s)), C.c_double(dt),
+                          C.c_double(rho), C.c_double(stab), _p(rp), _p(ci), _p(Kp), _p(rhs), _p(div))
+    return Kp, rhs, div
+
+
+def apply_bc_pressure(mesh, rp, ci, Kp, rhs, dp, mass, outlet_dirichlet=0, pin=-1):
+    lib().or_apply_bc_pressure(mesh.n, _p(i32(mesh.tag)), outlet_dirichlet, pin, _p(rp), _p(ci), _p(Kp), _p(rhs),
+                               _p(dp), _p(f64(mass)))
+
+
+def assemble_oss(mesh, rp, ci, elem_s, mass):
+    oss = np.zeros(4 * rp[-1], _D)
+    inv_m = np.zeros(mesh.n, _D)
+    lib().or_assemble_oss(mesh.n, mesh.ne, _p(mesh.elem_v), _p(f64(mesh.x)), _p(f64(mesh.y)), _p(f64(elem_s)),
+                          _p(rp), _p(ci), _p(f64(mass)), _p(oss), _p(inv_m))
+    return oss, inv_m
+
+
+def oss_apply(mesh, rp, ci, oss, inv_m, x, out, outlet_dirichlet=0, pin=-1):
+    lib().or_oss_apply(mesh.n, _p(rp), _p(ci), _p(oss), _p(inv_m), _p(i32(mesh.tag)), outlet_dirichlet, pin,
+                       _p(f64(x)), _p(out))
+
+
+def oss_matrix_free(mesh, elem_s, mass, x, out, outlet_dirichlet=0, pin=-1):
+    lib().or_oss_matrix_free(mesh.n, mesh.ne, _p(mesh.elem_v), _p(f64(mesh.x)), _p(f64(mesh.y)), _p(i32(mesh.tag)),
+                             outlet_dirichlet, pin, _p(f64(elem_s)), _p(f64(mass)), _p(f64(x)), _p(out))
+
+
+# ---------------------------------------------------------------------------------------------
+# ILU, AMG, Krylov
+# ---------------------------------------------------------------------------------------------
+class Report(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("rel_residual", C.c_double)]
+
+
+class Ilu:
+    def __init__(self, rp, ci):
+        self.rp, self.ci = i32(rp), i32(ci)
+        self.n = self.rp.size - 1
+        self.h = lib().or_ilu_create(self.n, _p(self.rp), _p(self.ci))
+        if not self.h:
+            raise ValueError("row longer than 32 entries")
+        self.h = C.c_void_p(self.h)
+        self.nc = lib().or_ilu_colours(self.h)
+        n = self.n
+        nlnu = np.zeros(2, _I)
+        lib().or_ilu_export(self.h, None, None, None, None, None, None, None, None, None, None, _p(nlnu))
+        self.nl, self.nu = int(nlnu[0]), int(nlnu[1])
+        self.colour = np.zeros(n, _I)
+        self.colour_start = np.zeros(self.nc + 1, _I)
+        self.rows = np.zeros(n, _I)
+        self.lp, self.up = np.zeros(n + 1, _I), np.zeros(n + 1, _I)
+        self.lc, self.uc = np.zeros(self.nl, _I), np.zeros(self.nu, _I)
+        self.l_src, self.u_src = np.zeros(self.nl, _I), np.zeros(self.nu, _I)
+        self.d_src = np.zeros(n, _I)
+        lib().or_ilu_export(self.h, _p(self.colour), _p(self.colour_start), _p(self.rows), _p(self.lp), _p(self.up),
+                            _p(self.lc), _p(self.uc), _p(self.l_src), _p(self.u_src), _p(self.d_src), None)
+
+    def factor(self, val):
+        lu = np.zeros(self.rp[-1], _D)
+        lv, uv, dinv = np.zeros(self.nl, _D), np.zeros(self.nu, _D), np.zeros(self.n, _D)
+        lib().or_ilu_factor(self.h, _p(f64(val)), _p(lu), _p(lv), _p(uv), _p(dinv))
+        return lu, lv, uv, dinv
+
+    def apply(self, r, nrhs=1):
+        z = np.zeros(self.n * nrhs, _D)
+        lib().or_ilu_apply(self.h, _p(f64(r)), _p(z), nrhs)
+        return z
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_ilu_free(self.h)
+            self.h = None
+
+
+class Amg:
+    def __init__(self, rp, ci, val, theta=0.08, smooth_steps=2, coarse_target=300, max_levels=15):
+        self.rp, self.ci, self.val = i32(rp), i32(ci), f64(val)
+        n = self.rp.size - 1
+        h = lib().or_amg_setup(n, _p(self.rp), _p(self.ci), _p(self.val), C.c_double(theta), smooth_steps,
+                               coarse_target, max_levels)
+        if not h:
+            raise ValueError("coarse operator not SPD")
+        self.h = C.c_void_p(h)
+        self.n = n
+        self.nlev = lib().or_amg_num_levels(self.h)
+        self.coarse_n = lib().or_amg_coarse_n(self.h)
+
+    def level(self, l):
+        info = np.zeros(4, _I)
+        om = C.c_double()
+        lib().or_amg_level_info(self.h, l, _p(info), C.byref(om))
+        rows, annz, pcols, pnnz = (int(v) for v in info)
+        out = {"rows": rows, "omega": om.value, "pcols": pcols}
+        for which, name, r, c, z in ((0, "A", rows, rows, annz), (1, "P", rows, pcols, pnnz), (2, "R", pcols, rows, pnnz)):
+            rp = np.zeros(r + 1, _I)
+            ci = np.zeros(z, _I)
+            v = np.zeros(z, _D)
+            lib().or_amg_level_csr(self.h, l, which, _p(rp), _p(ci), _p(v))
+            out[name] = (r, c, rp, ci, v)
+        agg = np.zeros(rows, _I)
+        lib().or_amg_level_agg(self.h, l, _p(agg))
+        dinv = np.zeros(rows, _D)
+        lib().or_amg_level_dinv(self.h, l, _p(dinv))
+        out["agg"] = agg
+        out["dinv"] = dinv
+        return out
+
+    def coarse(self):
+        cn = self.coarse_n
+        A = np.zeros(cn * cn, _D)
+        inv = np.zeros(cn * cn, _D)
+        lib().or_amg_coarse(self.h, _p(A), _p(inv))
+        return A.reshape(cn, cn), inv.reshape(cn, cn)
+
+    def apply(self, r):
+        z = np.zeros(self.n, _D)
+        lib().or_amg_apply(self.h, _p(f64(r)), _p(z))
+        return z
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_amg_free(self.h)
+            self.h = None
+
+
+def pcg(rp, ci, val, b, x0, max_iter=4000, tol=1e-7, oss=None, inv_m=None, tag=None, amg=None,
+        outlet_dirichlet=0, pin=-1):
+    n = rp.size - 1
+    x = f64(x0).copy()
+    rep = Report()
+    lib().or_pcg(n, _p(i32(rp)), _p(i32(ci)), _p(f64(val)), _p(f64(b)), _p(x), max_iter, C.c_double(tol),
+                 _p(oss) if oss is not None else None, _p(inv_m) if inv_m is not None else None,
+                 _p(i32(tag)) if tag is not None else None, outlet_dirichlet, pin,
+                 amg.h if amg is not None else None, C.byref(rep))
+    return x, rep
+
+
+def bicgstab(rp, ci, val, b, x0, max_iter=200, tol=1e-7):
+    n = rp.size - 1
+    x = f64(x0).copy()
+    rep = Report()
+    lib().or_bicgstab(n, _p(i32(rp)), _p(i32(ci)), _p(f64(val)), _p(f64(b)), _p(x), max_iter, C.c_double(tol),
+                      C.byref(rep))
+    return x, rep
+
+
+def bicgstab2(rp, ci, val, bu, bv, xu0, xv0, ilu, max_iter=150, tol=1e-7):
+    n = rp.size - 1
+    xu, xv = f64(xu0).copy(), f64(xv0).copy()
+    reps = (Report * 2)()
+    lib().or_bicgstab2(n, _p(i32(rp)), _p(i32(ci)), _p(f64(val)), _p(f64(bu)), _p(f64(bv)), _p(xu), _p(xv),
+                       max_iter, C.c_double(tol), ilu.h, reps)
+    return xu, xv, (reps[0], reps[1])
