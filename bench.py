@@ -1,0 +1,358 @@
+"""Benchmark of the per-timestep solve path: pressure + momentum solve ms/step, mixed precision
+(FP32 SA-AMG / ILU inside FP64 Krylov) and plain FP64, at 1e-10 relative residual.
+
+Workload (default): the adaptive ~400k-vertex mesh (seeded Delaunay + NVB, refined near the disc
+and in the wake band), BDF2 step with dt = 1e-3, nu = 1e-3, SUPG T = 1 ms, OSS stab 0.3, inflow
+U = 1.5; u^n = u^{n-1} and p^n are seeded Fourier fields (synthetic data). One step = momentum
+assembly + BCs, ILU(0) factor, BiCGSTAB2 (u, v) to 1e-10, OSS weights, G(p^n), pressure system
+assembly (PPE + BCs + OSS operator), PCG (K + OSS, SA-AMG) to 1e-10. The AMG setup is timed
+separately and amortised over 50 steps, the reference driver's rebuild interval.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c1]
+
+With N > 1 (torchrun) each rank solves its own replica (the single-system path does not shard):
+`value` is then the job's aggregate time per step (max over ranks / (N K)).
+`--impl reference` runs the reference's own CUDA build (oracle/_ref, compiled from the
+reference sources) on the same workload on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "cylinder-fem-amr_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+AMG_REBUILD = 50          # src/cfa/options.cuh:26
+STAB, DT, NU, U_MAX, TOL = 0.3, 1e-3, 1e-3, 1.5, 1e-10
+METRIC = "pressure+momentum solve ms/step & HBM GB/s, mixed vs FP64 at 1e-10 rel res"
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"cfa_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload_inputs(name):
+    import fixtures as F
+    m = F.make_mesh(name)
+    u = F.fourier_field(m.x, m.y, 1)
+    v = F.fourier_field(m.x, m.y, 2)
+    p = 0.3 * F.fourier_field(m.x, m.y, 3)
+    return m, u, v, p
+
+
+def l2_flush(buf):
+    buf.add_(1.0)
+
+
+# ------------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------------
+def operator_bytes(n, nnz):
+    """Algorithmic bytes of one pressure-operator application (K + OSS, two row passes):
+    pass 1 reads col_ind + Bx + By (20 B/nnz), row_ptr, z and p (pn = z + beta p), writes pn
+    and g (x, y); pass 2 reads col_ind + K + BTx + BTy (28 B/nnz), row_ptr, pn, g, tags, writes q."""
+    p1 = nnz * 20 + 4 * (n + 1) + n * (8 + 8 + 8 + 16 + 8)
+    p2 = nnz * 28 + 4 * (n + 1) + n * (8 + 16 + 4 + 8)
+    return p1, p2
+
+
+def time_operator(cfa, st, reps, flush):
+    """Live CUDA-event timing of the dominant kernel pair: the pressure operator passes."""
+    import torch
+    x = st.dp.clone().normal_()
+    y = torch.empty_like(x)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(3):
+        cfa.pressure_operator(st.ctx, st.dm.rp, st.dm.ci, st.Kp, x, y, st.oss)
+    total = 0.0
+    for _ in range(reps):
+        l2_flush(flush)
+        ev[0].record()
+        cfa.pressure_operator(st.ctx, st.dm.rp, st.dm.ci, st.Kp, x, y, st.oss)
+        ev[1].record()
+        ev[1].synchronize()
+        total += ev[0].elapsed_time(ev[1])
+    return total / reps
+
+
+def run_ours(args, rank, world):
+    import torch
+    import cfa_b200 as cfa
+    import step as S
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    m, u, v, p = workload_inputs(args.workload)
+    ctx = cfa.Context()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
+    res = {}
+    for prec_name, prec in (("fp64", cfa.FP64), ("mixed", cfa.MIXED)):
+        st = S.SolveStep(m, u, v, p, precision=prec, ctx=ctx, dt=DT, nu=NU, stab=STAB, u_max=U_MAX, tol=TOL)
+        setup_ms = st.amg_setup()
+        for _ in range(args.warmup):
+            st.run()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        total = 0.0
+        l0 = ctx.launches
+        reports = []
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+            for _ in range(args.steps):
+                l2_flush(flush)
+                ev[0].record()
+                st.run()
+                ev[1].record()
+                ev[1].synchronize()
+                total += ev[0].elapsed_time(ev[1])
+                reports.append(st.report())
+        launches = ctx.launches - l0
+        torch.cuda.synchronize()
+        step_ms = total / args.steps
+        # end-to-end through the API with host buffers: H2D of the step inputs, D2H of the results
+        hu = torch.from_numpy(u).pin_memory()
+        hv = torch.from_numpy(v).pin_memory()
+        hp = torch.from_numpy(p).pin_memory()
+        outs = [torch.empty(m.n, dtype=torch.float64).pin_memory() for _ in range(3)]
+        e2e_total = 0.0
+        for _ in range(args.steps):
+            l2_flush(flush)
+            ev[0].record()
+            st.u_n.copy_(hu, non_blocking=True)
+            st.v_n.copy_(hv, non_blocking=True)
+            st.p_n.copy_(hp, non_blocking=True)
+            st.u_prev.copy_(st.u_n)
+            st.v_prev.copy_(st.v_n)
+            st.run()
+            outs[0].copy_(st.u, non_blocking=True)
+            outs[1].copy_(st.v, non_blocking=True)
+            outs[2].copy_(st.dp, non_blocking=True)
+            ev[1].record()
+            ev[1].synchronize()
+            e2e_total += ev[0].elapsed_time(ev[1])
+        e2e_ms = e2e_total / args.steps
+        op_ms = time_operator(cfa, st, 20, flush) if prec == cfa.FP64 else None
+        res[prec_name] = dict(step_ms=step_ms, setup_ms=setup_ms, e2e_ms=e2e_ms, launches=launches,
+                              clocks=clk.summary(), report=reports[-1], op_ms=op_ms, levels=st.amg.num_levels(),
+                              colours=st.ilu.n_colours, nnz=st.nnz, n=st.n)
+        del st
+    return m, res
+
+
+def cpu_baseline(m, u, v, p):
+    """The oracle (C restatement, OpenMP) on one full step of the same workload, host cores."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    t_pattern = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    A, ru, rv, mass = O.assemble_momentum(m, rp, ci, u, v, u, v, p, O.bdf2_params())
+    uu, vv = u.copy(), v.copy()
+    O.apply_bc_momentum(m, rp, ci, A, ru, rv, uu, vv)
+    ilu = O.Ilu(rp, ci)
+    ilu.factor(A)
+    xu, xv, _ = O.bicgstab2(rp, ci, A, ru, rv, uu, vv, ilu, 1000, TOL)
+    dt_proj = 2 * DT / 3
+    s = O.oss_weights(m, xu, xv, dt_proj, 1.0, NU, STAB)
+    gx, gy = O.scalar_gradient(m, p, s)
+    Kp, rhs, div = O.assemble_ppe(m, rp, ci, xu, xv, p, gx, gy, mass, s, dt_proj, 1.0, STAB)
+    dp = np.zeros(m.n)
+    O.apply_bc_pressure(m, rp, ci, Kp, rhs, dp, mass)
+    oss, inv_m = O.assemble_oss(m, rp, ci, s, mass)
+    t_solve_start = time.perf_counter()
+    amg = O.Amg(rp, ci, Kp)
+    t_setup = time.perf_counter() - t_solve_start
+    O.pcg(rp, ci, Kp, rhs, dp, 4000, TOL, oss, inv_m, m.tag, amg)
+    t_step = time.perf_counter() - t0 - t_setup
+    ms = 1e3 * t_step + 1e3 * t_setup / AMG_REBUILD
+    return dict(value=ms, unit="ms/step", cores=O.lib().or_num_threads(), kind="port",
+                sample=f"1 full FP64 step of the same workload (n={m.n}) by the oracle port, OpenMP; "
+                       f"AMG setup {1e3 * t_setup:.0f} ms amortised over {AMG_REBUILD} steps")
+
+
+# ------------------------------------------------------------------------------------------------
+# reference arm: the reference's own CUDA build (oracle/_ref)
+# ------------------------------------------------------------------------------------------------
+def run_reference(args):
+    import ctypes as C
+    import torch
+    from oracle import oracle as O
+    m, u, v, p = workload_inputs(args.workload)
+    R = O.ref()
+    if not R.ref_gpu_available():
+        return {"impl": "reference", "unavailable": "no GPU visible to the reference build"}
+    ev = np.ascontiguousarray(m.elem_v, np.int32)
+    tag = np.ascontiguousarray(m.tag, np.int32)
+    h = C.c_void_p(R.ref_step_create(m.n, m.ne, O._p(ev), O._p(m.x), O._p(m.y), O._p(tag), O._p(u), O._p(v),
+                                     O._p(p), C.c_double(DT), C.c_double(NU), C.c_double(1.0), C.c_double(U_MAX),
+                                     C.c_double(1.0), C.c_double(1e-3), C.c_double(STAB), C.c_double(TOL), 1000, 4000))
+    setup_ms = R.ref_step_amg_setup(h)
+    its, conv, rel = np.zeros(3, np.int32), np.zeros(3, np.int32), np.zeros(3)
+    for _ in range(args.warmup):
+        R.ref_step_run(h, O._p(its), O._p(conv), O._p(rel), None, None, None)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    total = 0.0
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        for _ in range(args.steps):
+            flush.add_(1.0)
+            torch.cuda.synchronize()
+            total += R.ref_step_run(h, O._p(its), O._p(conv), O._p(rel), None, None, None)
+    R.ref_step_free(h)
+    step_ms = total / args.steps
+    value = step_ms + setup_ms / AMG_REBUILD
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {
+        "metric": METRIC, "value": round(value, 4), "unit": "ms/step", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 4),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: adaptive NVB mesh n={m.n}, BDF2 step, OSS 0.3, tol 1e-10",
+                   "precision": "fp64 (the reference has no mixed mode)", "l2": "flushed between steps",
+                   "amg_setup_ms": round(setup_ms, 3), "amg_rebuild": AMG_REBUILD,
+                   "iterations": {"u": int(its[0]), "v": int(its[1]), "p": int(its[2])},
+                   "converged": [bool(c) for c in conv]},
+        "cpu_baseline": {"value": round(value, 4), "unit": "ms/step", "cores": threads, "kind": "reference",
+                         "sample": "the reference's own CUDA build (nvcc sm_100a, host-timed steps with its "
+                                   "device syncs) on the same workload; OpenMP host setup threads"},
+        "e2e": {"value": round(value, 4), "unit": "ms/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk.summary(),
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    import torch
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        print(json.dumps(run_reference(args)))
+        return
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    m, res = run_ours(args, rank, world)
+    mixed, fp64 = res["mixed"], res["fp64"]
+    value = mixed["step_ms"] + mixed["setup_ms"] / AMG_REBUILD
+    value64 = fp64["step_ms"] + fp64["setup_ms"] / AMG_REBUILD
+    e2e = mixed["e2e_ms"] + mixed["setup_ms"] / AMG_REBUILD
+    if world > 1:
+        t = torch.tensor([value, e2e, value64], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        value, e2e, value64 = (float(x) / world for x in t.tolist())
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    n, nnz = mixed["n"], mixed["nnz"]
+    hbm, peak_kind = peaks()
+    p1, p2 = operator_bytes(n, nnz)
+    op_ms = fp64["op_ms"]
+    achieved = (p1 + p2) / (op_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(f"pressure_operator_{args.workload}")
+    cpu = None if args.no_cpu else cpu_baseline(m, *workload_inputs(args.workload)[1:])
+    clocks = mixed["clocks"]
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "ms/step", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(value, 4), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 outer / f32 preconditioners", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: adaptive NVB mesh n={n}, nnz={nnz}, BDF2 step, OSS 0.3, tol 1e-10",
+                   "parallelism": "replicas" if world > 1 else "single GPU", "l2": "flushed between steps (256 MB write)",
+                   "fp64_ms_per_step": round(value64, 4), "mixed_speedup_vs_fp64": round(value64 / value, 3),
+                   "amg_setup_ms": {"mixed": round(mixed["setup_ms"], 3), "fp64": round(fp64["setup_ms"], 3)},
+                   "amg_rebuild": AMG_REBUILD, "step_ms_without_setup": round(mixed["step_ms"], 4),
+                   "iterations_mixed": {"u": mixed["report"]["it_u"], "v": mixed["report"]["it_v"], "p": mixed["report"]["it_p"]},
+                   "iterations_fp64": {"u": fp64["report"]["it_u"], "v": fp64["report"]["it_v"], "p": fp64["report"]["it_p"]},
+                   "converged": mixed["report"]["conv"] + fp64["report"]["conv"],
+                   "amg_levels": mixed["levels"], "ilu_colours": mixed["colours"]},
+        "e2e": {"value": round(e2e, 4), "unit": "ms/step", "h2d_bytes_per_step": 3 * 8 * n, "d2h_bytes_per_step": 3 * 8 * n},
+        "gpu_launches": int(mixed["launches"]),
+        "roofline": {"bound": "hbm", "kernel": "pressure operator K + OSS (k_op_b + k_op_k), FP64",
+                     "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": peak_kind,
+                     "bytes_per_launch": p1 + p2, "launch_us": round(op_ms * 1e3, 2)},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,830 @@
+// SA-AMG on the GPU.
+//
+// Setup (AmgPreconditioner::setup, src/cfa/linalg.cuh:995-1060): every FP64 operation of the
+// reference's host setup is reproduced in the same order with explicitly rounded multiplies and
+// adds (no fused multiply-add), so the hierarchy -- aggregates, P, R, Galerkin operators, omega,
+// coarse inverse -- is bit-identical to the reference's:
+//   * D^-1, strength of connection, P smoothing, transposes: one thread per row on the GPU;
+//   * the power iteration for rho(D^-1 A) with the reference's fixed 4096-row chunk sums;
+//   * the Galerkin products with an exact-order row SpGEMM (csr_multiply, :797-845): per row,
+//     products are accumulated in A's row order then B's row order into a sorted list;
+//   * the coarsest dense Cholesky inverse in one CTA / one thread per column (:1394-1431);
+//   * the greedy aggregation (:1321-1348), whose phases 1 and 3 are sequential in node order,
+//     runs on the host over the strength flags computed on the GPU.
+// V-cycle (vcycle, :1184-1206): symmetric V(s,s) with damped Jacobi, thread groups of TPR lanes
+// per row; the first pre-smoothing step is fused with the x = omega D^-1 b initialisation; FP64
+// or FP32 hierarchy (mixed precision: FP32 values and vectors, FP64 coarsest solve).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <type_traits>
+
+#include "amg.cuh"
+
+namespace cfa {
+
+// =============================================================================================
+// setup kernels (FP64, reference operation order)
+// =============================================================================================
+__global__ void k_amg_dinv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
+                           double* __restrict__ dinv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = 0.0;
+    for (int a = rp[i]; a < rp[i + 1]; ++a) if (ci[a] == i) d = v[a];
+    dinv[i] = (fabs(d) > 1.0e-300) ? __ddiv_rn(1.0, d) : 1.0;
+}
+
+// power iteration pieces (spectral_radius_DinvA, :1276-1304)
+__global__ void k_pow_y(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
+                        const double* __restrict__ dinv, const double* __restrict__ x, double* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int a = rp[i]; a < rp[i + 1]; ++a) s = __dadd_rn(s, __dmul_rn(v[a], x[ci[a]]));
+    y[i] = __dmul_rn(dinv[i], s);
+}
+
+__global__ void k_pow_chunks(int n, int nch, const double* __restrict__ x, const double* __restrict__ y,
+                             double* __restrict__ py, double* __restrict__ px) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nch) return;
+    double sy = 0.0, sx = 0.0;
+    const int e = min(n, (c + 1) * 4096);
+    for (int i = c * 4096; i < e; ++i) {
+        const double yi = y[i], xi = x[i];
+        sy = __dadd_rn(sy, __dmul_rn(yi, yi));
+        sx = __dadd_rn(sx, __dmul_rn(xi, xi));
+    }
+    py[c] = sy;
+    px[c] = sx;
+}
+
+__global__ void k_pow_finish(int nch, const double* __restrict__ py, const double* __restrict__ px, double* __restrict__ st) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double nrm = 0.0, xn = 0.0;
+    for (int c = 0; c < nch; ++c) { nrm = __dadd_rn(nrm, py[c]); xn = __dadd_rn(xn, px[c]); }
+    nrm = __dsqrt_rn(nrm);
+    st[0] = nrm;
+    st[1] = __ddiv_rn(nrm, __dsqrt_rn(xn));
+}
+
+__global__ void k_pow_scale(int n, const double* __restrict__ y, const double* __restrict__ st, double* __restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = __ddiv_rn(y[i], st[0]);
+}
+
+// strong connections (smoothed_prolongator, :1310-1319)
+__global__ void k_strength(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
+                           const double* __restrict__ dinv, double theta, unsigned char* __restrict__ strong) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double di = __ddiv_rn(1.0, dinv[i]);
+    for (int a = rp[i]; a < rp[i + 1]; ++a) {
+        const int j = ci[a];
+        const double dj = __ddiv_rn(1.0, dinv[j]);
+        strong[a] = (j != i) && fabs(v[a]) >= __dmul_rn(theta, __dsqrt_rn(fabs(__dmul_rn(di, dj))));
+    }
+}
+
+// exact-order SpGEMM (csr_multiply): upper bounds, sorted accumulation, copy
+__global__ void k_sg_ub(int rows, const int* __restrict__ arp, const int* __restrict__ aci, const int* __restrict__ brp,
+                        int* __restrict__ ub) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    int s = 0;
+    for (int a = arp[i]; a < arp[i + 1]; ++a) s += brp[aci[a] + 1] - brp[aci[a]];
+    ub[i] = s;
+}
+
+__global__ void k_sg_accum(int rows, const int* __restrict__ arp, const int* __restrict__ aci, const double* __restrict__ av,
+                           const int* __restrict__ brp, const int* __restrict__ bci, const double* __restrict__ bv,
+                           const long long* __restrict__ off, int* __restrict__ scol, double* __restrict__ sval,
+                           int* __restrict__ cnt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    int* cols = scol + off[i];
+    double* vals = sval + off[i];
+    int m = 0;
+    for (int a = arp[i]; a < arp[i + 1]; ++a) {
+        const int k = aci[a];
+        const double x = av[a];
+        for (int b = brp[k]; b < brp[k + 1]; ++b) {
+            const int j = bci[b];
+            const double prod = __dmul_rn(x, bv[b]);
+            int lo = 0, hi = m;
+            while (lo < hi) { const int mid = (lo + hi) >> 1; if (cols[mid] < j) lo = mid + 1; else hi = mid; }
+            if (lo < m && cols[lo] == j) {
+                vals[lo] = __dadd_rn(vals[lo], prod);
+            } else {
+                for (int q = m; q > lo; --q) { cols[q] = cols[q - 1]; vals[q] = vals[q - 1]; }
+                cols[lo] = j;
+                vals[lo] = __dadd_rn(0.0, prod);   // acc[j] = 0.0; acc[j] += ...
+                ++m;
+            }
+        }
+    }
+    cnt[i] = m;
+}
+
+__global__ void k_sg_copy(int rows, const long long* __restrict__ off, const int* __restrict__ scol,
+                          const double* __restrict__ sval, const int* __restrict__ crp, int* __restrict__ cci,
+                          double* __restrict__ cv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    const long long o = off[i];
+    const int c0 = crp[i], m = crp[i + 1] - c0;
+    for (int q = 0; q < m; ++q) { cci[c0 + q] = scol[o + q]; cv[c0 + q] = sval[o + q]; }
+}
+
+// P = P0 - omega D^-1 A P0 from the rows of AP0 (build_row, :1367-1383)
+__global__ void k_p_rows(int n, const int* __restrict__ aprp, const int* __restrict__ apci, const double* __restrict__ apv,
+                         const int* __restrict__ agg, const double* __restrict__ p0v, const double* __restrict__ dinv,
+                         double omega, const int* __restrict__ prp, int* __restrict__ pci, double* __restrict__ pv,
+                         int* __restrict__ cnt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool fill = pci != nullptr;
+    int out = 0;
+    const int base = fill ? prp[i] : 0;
+    bool own = false;
+    const int own_col = agg[i];
+    const double coef = __dmul_rn(-omega, dinv[i]);
+    for (int a = aprp[i]; a < aprp[i + 1]; ++a) {
+        const int j = apci[a];
+        if (!own && j > own_col) {
+            if (fill) { pci[base + out] = own_col; pv[base + out] = p0v[i]; }
+            ++out;
+            own = true;
+        }
+        double val = __dmul_rn(coef, apv[a]);
+        if (j == own_col) { val = __dadd_rn(val, p0v[i]); own = true; }
+        if (val != 0.0) { if (fill) { pci[base + out] = j; pv[base + out] = val; } ++out; }
+    }
+    if (!own) { if (fill) { pci[base + out] = own_col; pv[base + out] = p0v[i]; } ++out; }
+    if (!fill) cnt[i] = out;
+}
+
+__global__ void k_entry_rows(int rows, const int* __restrict__ rp, int* __restrict__ row_of) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    for (int a = rp[i]; a < rp[i + 1]; ++a) row_of[a] = i;
+}
+
+__global__ void k_iota(int n, int* __restrict__ v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
+}
+
+__global__ void k_ptr_from_sorted(int rows, int m, const int* __restrict__ keys, int* __restrict__ ptr) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > m) return;
+    const int cur = t < m ? keys[t] : rows;
+    const int prev = t > 0 ? keys[t - 1] : -1;
+    for (int i = prev + 1; i <= cur && i <= rows; ++i) ptr[i] = t;
+}
+
+__global__ void k_transpose_fill(int m, const int* __restrict__ perm, const int* __restrict__ row_of,
+                                 const double* __restrict__ v, int* __restrict__ tci, double* __restrict__ tv) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    const int e = perm[t];
+    tci[t] = row_of[e];
+    tv[t] = v[e];
+}
+
+__global__ void k_dense_build(int cn, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
+                              double* __restrict__ D) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cn) return;
+    for (int q = 0; q < cn; ++q) D[(size_t)i * cn + q] = 0.0;
+    for (int a = rp[i]; a < rp[i + 1]; ++a) D[(size_t)i * cn + ci[a]] = v[a];
+}
+
+// Cholesky M = L L^T in place, one CTA (dense_spd_inverse, :1396-1410); err = 1 if not SPD
+__global__ void k_cholesky(int cn, double* __restrict__ M, int* __restrict__ err) {
+    __shared__ double ljj_s;
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    for (int j = 0; j < cn; ++j) {
+        if (threadIdx.x == 0) {
+            double d = M[(size_t)j * cn + j];
+            for (int k = 0; k < j; ++k) d = __dsub_rn(d, __dmul_rn(M[(size_t)j * cn + k], M[(size_t)j * cn + k]));
+            if (!(d > 0.0)) { bad = 1; d = 1.0; }
+            const double l = __dsqrt_rn(d);
+            M[(size_t)j * cn + j] = l;
+            ljj_s = l;
+        }
+        __syncthreads();
+        if (bad) break;
+        const double ljj = ljj_s;
+        for (int i = j + 1 + threadIdx.x; i < cn; i += blockDim.x) {
+            double s = M[(size_t)i * cn + j];
+            for (int k = 0; k < j; ++k) s = __dsub_rn(s, __dmul_rn(M[(size_t)i * cn + k], M[(size_t)j * cn + k]));
+            M[(size_t)i * cn + j] = __ddiv_rn(s, ljj);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *err = bad;
+}
+
+// Column c of the inverse from L (:1411-1429)
+__global__ void k_chol_inverse(int cn, const double* __restrict__ M, double* __restrict__ inv, double* __restrict__ colbuf) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cn) return;
+    double* col = colbuf + (size_t)c * cn;
+    for (int i = 0; i < cn; ++i) {
+        double s = (i == c) ? 1.0 : 0.0;
+        for (int k = 0; k < i; ++k) s = __dsub_rn(s, __dmul_rn(M[(size_t)i * cn + k], col[k]));
+        col[i] = __ddiv_rn(s, M[(size_t)i * cn + i]);
+    }
+    for (int i = cn - 1; i >= 0; --i) {
+        double s = col[i];
+        for (int k = i + 1; k < cn; ++k) s = __dsub_rn(s, __dmul_rn(M[(size_t)k * cn + i], col[k]));
+        col[i] = __ddiv_rn(s, M[(size_t)i * cn + i]);
+    }
+    for (int i = 0; i < cn; ++i) inv[(size_t)i * cn + c] = col[i];
+}
+
+__global__ void k_to_float(long long n, const double* __restrict__ a, float* __restrict__ b) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+// =============================================================================================
+// V-cycle kernels. Thread groups of TPR lanes per row, warp-uniform loops, the lane-strided
+// sum and shuffle tree of the reference's k_csr_op (:885-901).
+// =============================================================================================
+template <int TPR, class T, class X>
+__device__ __forceinline__ T group_row_sum(const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
+                                           const X* __restrict__ x, int row, bool valid, int lane) {
+    T s = (T)0;
+    if (valid)
+        for (int k = rp[row] + lane; k < rp[row + 1]; k += TPR) s += val[k] * (T)x[ci[k]];
+#pragma unroll
+    for (int o = TPR / 2; o > 0; o /= 2) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
+    return s;
+}
+
+#define ROW_LOOP_BEGIN(TPR, n)                                                                    \
+    const int lane_ = threadIdx.x % (TPR);                                                        \
+    const int gw_ = (blockIdx.x * blockDim.x + threadIdx.x) / 32;                                 \
+    const int nw_ = gridDim.x * blockDim.x / 32;                                                  \
+    constexpr int rpw_ = 32 / (TPR);                                                              \
+    for (int base_ = gw_ * rpw_; base_ < (n); base_ += nw_ * rpw_) {                              \
+        const int row = base_ + (threadIdx.x & 31) / (TPR);                                       \
+        const bool valid = row < (n);                                                             \
+        const int lane = lane_;
+
+#define ROW_LOOP_END }
+
+// x = omega D^-1 b, then (fused) one Jacobi step x <- x + omega D^-1 (b - A x) when `jac`
+template <int TPR, class T, class B>
+__global__ void k_vc_pre(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
+                         const T* __restrict__ dinv, T omega, const B* __restrict__ b, int jac, T* __restrict__ xo,
+                         const int* __restrict__ done) {
+    if (done && *done) return;
+    ROW_LOOP_BEGIN(TPR, n)
+    if (!jac) {
+        if (valid && lane == 0) xo[row] = omega * dinv[row] * (T)b[row];
+        continue;
+    }
+    T s = (T)0;
+    if (valid)
+        for (int k = rp[row] + lane; k < rp[row + 1]; k += TPR) {
+            const int j = ci[k];
+            s += val[k] * (omega * dinv[j] * (T)b[j]);
+        }
+#pragma unroll
+    for (int o = TPR / 2; o > 0; o /= 2) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
+    if (valid && lane == 0) {
+        const T x0 = omega * dinv[row] * (T)b[row];
+        xo[row] = x0 + omega * dinv[row] * ((T)b[row] - s);
+    }
+    ROW_LOOP_END
+}
+
+// y = x + omega D^-1 (b - A x); O = output type (FP64 z at the end of level 0)
+template <int TPR, class T, class B, class O>
+__global__ void k_vc_jacobi(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
+                            const T* __restrict__ dinv, T omega, const B* __restrict__ b, const T* __restrict__ x,
+                            O* __restrict__ y, const int* __restrict__ done) {
+    if (done && *done) return;
+    ROW_LOOP_BEGIN(TPR, n)
+    const T s = group_row_sum<TPR, T, T>(rp, ci, val, x, row, valid, lane);
+    if (valid && lane == 0) y[row] = (O)(x[row] + omega * dinv[row] * ((T)b[row] - s));
+    ROW_LOOP_END
+}
+
+// r = b - A x
+template <int TPR, class T, class B>
+__global__ void k_vc_resid(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
+                           const B* __restrict__ b, const T* __restrict__ x, T* __restrict__ r, const int* __restrict__ done) {
+    if (done && *done) return;
+    ROW_LOOP_BEGIN(TPR, n)
+    const T s = group_row_sum<TPR, T, T>(rp, ci, val, x, row, valid, lane);
+    if (valid && lane == 0) r[row] = (T)b[row] - s;
+    ROW_LOOP_END
+}
+
+// y = M x (add = 0) or y += M x (add = 1); Y output type
+template <int TPR, class T, class Y>
+__global__ void k_vc_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
+                          const T* __restrict__ x, int add, Y* __restrict__ y, const int* __restrict__ done) {
+    if (done && *done) return;
+    ROW_LOOP_BEGIN(TPR, n)
+    const T s = group_row_sum<TPR, T, T>(rp, ci, val, x, row, valid, lane);
+    if (valid && lane == 0) y[row] = add ? (Y)((T)y[row] + s) : (Y)s;
+    ROW_LOOP_END
+}
+
+// x = A_c^-1 b with the stored FP64 inverse, one warp per row (k_dense_matvec, :929-937)
+template <class B, class X>
+__global__ void k_vc_dense(int cn, const double* __restrict__ inv, const B* __restrict__ b, X* __restrict__ x,
+                           const int* __restrict__ done) {
+    if (done && *done) return;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x & 31;
+    if (i >= cn) return;
+    double s = 0.0;
+    for (int j = lane; j < cn; j += 32) s += inv[(size_t)i * cn + j] * (double)b[j];
+    s = warp_sum(s);
+    if (lane == 0) x[i] = (X)s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// launch helpers with the TPR dispatch
+// ---------------------------------------------------------------------------------------------
+#define CFA_TPR_SWITCH(tpr, ...)                                                               \
+    do {                                                                                       \
+        switch (tpr) {                                                                         \
+            case 1: { constexpr int TPR = 1; __VA_ARGS__; } break;                              \
+            case 2: { constexpr int TPR = 2; __VA_ARGS__; } break;                              \
+            case 4: { constexpr int TPR = 4; __VA_ARGS__; } break;                              \
+            case 8: { constexpr int TPR = 8; __VA_ARGS__; } break;                              \
+            case 16: { constexpr int TPR = 16; __VA_ARGS__; } break;                            \
+            default: { constexpr int TPR = 32; __VA_ARGS__; } break;                            \
+        }                                                                                      \
+    } while (0)
+
+template <class T>
+struct LevelView {
+    const int *Arp, *Aci, *Prp, *Pci, *Rrp, *Rci;
+    const T *Av, *Pv, *Rv, *dinv;
+    T *x, *t, *b, *r;
+    T omega;
+};
+
+template <class T>
+static LevelView<T> view(AmgLevel& L);
+template <>
+LevelView<double> view<double>(AmgLevel& L) {
+    return {L.A.rp.p, L.A.ci.p, L.P.rp.p, L.P.ci.p, L.R.rp.p, L.R.ci.p, L.A.v.p, L.P.v.p, L.R.v.p, L.dinv.p,
+            L.x64.p, L.t64.p, L.b64.p, L.r64.p, L.omega};
+}
+template <>
+LevelView<float> view<float>(AmgLevel& L) {
+    return {L.A.rp.p, L.A.ci.p, L.P.rp.p, L.P.ci.p, L.R.rp.p, L.R.ci.p, L.A.v32.p, L.P.v32.p, L.R.v32.p, L.dinv32.p,
+            L.x32.p, L.t32.p, L.b32.p, L.r32.p, (float)L.omega};
+}
+
+// V-cycle on level l; b is the level's right-hand side (level 0: caller's FP64 r), the result
+// ends in the level's x (level 0: in z).
+template <class T, class B>
+static void vcycle_level(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* z, const int* done) {
+    AmgLevel& L = amg->levels[l];
+    LevelView<T> V = view<T>(L);
+    const int n = L.A.rows, s = amg->opts.smooth_steps;
+    const int tA = L.A.tpr, tP = L.P.tpr, tR = L.R.tpr;
+    const int gA = row_grid(ctx, n, tA);
+    // pre-smoothing from x = 0
+    CFA_TPR_SWITCH(tA, CFA_LAUNCH(ctx, (k_vc_pre<TPR, T, B>), gA, kThreads, 0, n, V.Arp, V.Aci, V.Av, V.dinv, V.omega,
+                                  b, s >= 2 ? 1 : 0, V.x, done));
+    T* x = V.x;
+    T* t = V.t;
+    for (int k = 2; k < s; ++k) {
+        CFA_TPR_SWITCH(tA, CFA_LAUNCH(ctx, (k_vc_jacobi<TPR, T, B, T>), gA, kThreads, 0, n, V.Arp, V.Aci, V.Av, V.dinv,
+                                      V.omega, b, x, t, done));
+        std::swap(x, t);
+    }
+    // restricted residual
+    CFA_TPR_SWITCH(tA, CFA_LAUNCH(ctx, (k_vc_resid<TPR, T, B>), gA, kThreads, 0, n, V.Arp, V.Aci, V.Av, b, x, V.r, done));
+    const bool last = l + 1 == (int)amg->levels.size();
+    const int nc = L.P.cols;
+    T* cb = last ? (std::is_same<T, double>::value ? (T*)amg->cb64.p : (T*)amg->cb32.p)
+                 : view<T>(amg->levels[l + 1]).b;
+    CFA_TPR_SWITCH(tR, CFA_LAUNCH(ctx, (k_vc_spmv<TPR, T, T>), row_grid(ctx, nc, tR), kThreads, 0, nc, V.Rrp, V.Rci,
+                                  V.Rv, V.r, 0, cb, done));
+    const T* cx;
+    if (!last) {
+        vcycle_level<T, T>(ctx, amg, l + 1, cb, nullptr, done);
+        cx = view<T>(amg->levels[l + 1]).x;
+    } else {
+        T* dst = std::is_same<T, double>::value ? (T*)amg->cx64.p : (T*)amg->cx32.p;
+        CFA_LAUNCH(ctx, (k_vc_dense<T, T>), ceil_div((long long)amg->coarse_n * 32, kThreads), kThreads, 0,
+                   amg->coarse_n, amg->coarse_inv.p, (const T*)cb, dst, done);
+        cx = dst;
+    }
+    // coarse correction x += P x_c
+    CFA_TPR_SWITCH(tP, CFA_LAUNCH(ctx, (k_vc_spmv<TPR, T, T>), row_grid(ctx, n, tP), kThreads, 0, n, V.Prp, V.Pci, V.Pv,
+                                  cx, 1, x, done));
+    // post-smoothing; the last step of level 0 writes z
+    for (int k = 0; k < s; ++k) {
+        if (l == 0 && k == s - 1) {
+            CFA_TPR_SWITCH(tA, CFA_LAUNCH(ctx, (k_vc_jacobi<TPR, T, B, double>), gA, kThreads, 0, n, V.Arp, V.Aci, V.Av,
+                                          V.dinv, V.omega, b, x, z, done));
+        } else {
+            CFA_TPR_SWITCH(tA, CFA_LAUNCH(ctx, (k_vc_jacobi<TPR, T, B, T>), gA, kThreads, 0, n, V.Arp, V.Aci, V.Av,
+                                          V.dinv, V.omega, b, x, t, done));
+            std::swap(x, t);
+        }
+    }
+    // the level's result must be in L.x for the caller's prolongation
+    if (l > 0 && x != V.x) {
+        // odd number of swaps: copy back (only for odd smoothing counts)
+        cudaMemcpyAsync(V.x, x, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream);
+    }
+}
+
+cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done) {
+    if (amg->levels.empty()) {
+        CFA_LAUNCH(ctx, (k_vc_dense<double, double>), ceil_div((long long)amg->coarse_n * 32, kThreads), kThreads, 0,
+                   amg->coarse_n, amg->coarse_inv.p, r, z, done);
+    } else if (amg->opts.precision == CFA_MIXED) {
+        vcycle_level<float, double>(ctx, amg, 0, r, z, done);
+    } else {
+        vcycle_level<double, double>(ctx, amg, 0, r, z, done);
+    }
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+// =============================================================================================
+// setup driver
+// =============================================================================================
+// Exact-order SpGEMM C = A B into C (device CSR).
+static cfa_status spgemm(cfa_ctx* ctx, int ar, int bc, const int* arp, const int* aci, const double* av, const int* brp,
+                         const int* bci, const double* bv, DCsr& C) {
+    DevBuf<int> ub, cnt;
+    DevBuf<long long> off;
+    CFA_CUDA(ub.ensure(ar + 1));
+    CFA_CUDA(off.ensure(ar + 1));
+    CFA_CUDA(cnt.ensure(ar + 1));
+    CFA_CUDA(cudaMemsetAsync(ub.p + ar, 0, sizeof(int), ctx->stream));
+    CFA_LAUNCH(ctx, k_sg_ub, ceil_div(ar, kThreads), kThreads, 0, ar, arp, aci, brp, ub.p);
+    // 64-bit offsets of the per-row scratch regions (host scan)
+    std::vector<int> h_ub(ar + 1);
+    CFA_CUDA(cudaMemcpyAsync(h_ub.data(), ub.p, (ar + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::vector<long long> h_off(ar + 1, 0);
+    for (int i = 0; i < ar; ++i) h_off[i + 1] = h_off[i] + h_ub[i];
+    const long long total = h_off[ar];
+    CFA_CUDA(cudaMemcpyAsync(off.p, h_off.data(), (ar + 1) * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
+    DevBuf<int> scol;
+    DevBuf<double> sval;
+    CFA_CUDA(scol.ensure(std::max<long long>(total, 1)));
+    CFA_CUDA(sval.ensure(std::max<long long>(total, 1)));
+    CFA_LAUNCH(ctx, k_sg_accum, ceil_div(ar, 128), 128, 0, ar, arp, aci, av, brp, bci, bv, off.p, scol.p, sval.p, cnt.p);
+    std::vector<int> h_cnt(ar);
+    CFA_CUDA(cudaMemcpyAsync(h_cnt.data(), cnt.p, ar * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::vector<int> h_rp(ar + 1, 0);
+    for (int i = 0; i < ar; ++i) h_rp[i + 1] = h_rp[i] + h_cnt[i];
+    C.rows = ar;
+    C.cols = bc;
+    C.nnz = h_rp[ar];
+    CFA_CUDA(C.rp.ensure(ar + 1));
+    CFA_CUDA(C.ci.ensure(std::max(C.nnz, 1)));
+    CFA_CUDA(C.v.ensure(std::max(C.nnz, 1)));
+    CFA_CUDA(cudaMemcpyAsync(C.rp.p, h_rp.data(), (ar + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CFA_LAUNCH(ctx, k_sg_copy, ceil_div(ar, kThreads), kThreads, 0, ar, off.p, scol.p, sval.p, C.rp.p, C.ci.p, C.v.p);
+    CFA_CHECK_LAUNCH();
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    return CFA_OK;
+}
+
+// T = A^T (csr_transpose, :847-862): entries of each column in ascending row order
+static cfa_status transpose(cfa_ctx* ctx, const DCsr& A, DCsr& T) {
+    const int m = A.nnz;
+    DevBuf<int> keys_out, idx, perm, row_of;
+    CFA_CUDA(keys_out.ensure(std::max(m, 1)));
+    CFA_CUDA(idx.ensure(std::max(m, 1)));
+    CFA_CUDA(perm.ensure(std::max(m, 1)));
+    CFA_CUDA(row_of.ensure(std::max(m, 1)));
+    T.rows = A.cols;
+    T.cols = A.rows;
+    T.nnz = m;
+    CFA_CUDA(T.rp.ensure(A.cols + 1));
+    CFA_CUDA(T.ci.ensure(std::max(m, 1)));
+    CFA_CUDA(T.v.ensure(std::max(m, 1)));
+    if (m > 0) {
+        CFA_LAUNCH(ctx, k_iota, ceil_div(m, kThreads), kThreads, 0, m, idx.p);
+        CFA_LAUNCH(ctx, k_entry_rows, ceil_div(A.rows, kThreads), kThreads, 0, A.rows, A.rp.p, row_of.p);
+        int bits = 1;
+        while ((1LL << bits) <= A.cols) ++bits;
+        size_t tmp_bytes = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, A.ci.p, keys_out.p, idx.p, perm.p, m, 0, bits, ctx->stream);
+        DevBuf<char> tmp;
+        CFA_CUDA(tmp.ensure(tmp_bytes + 16));
+        CFA_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, A.ci.p, keys_out.p, idx.p, perm.p, m, 0, bits,
+                                                 ctx->stream));
+        ctx->launches += 4;
+        CFA_LAUNCH(ctx, k_transpose_fill, ceil_div(m, kThreads), kThreads, 0, m, perm.p, row_of.p, A.v.p, T.ci.p, T.v.p);
+    }
+    CFA_LAUNCH(ctx, k_ptr_from_sorted, ceil_div(m + 1, kThreads), kThreads, 0, A.cols, m, keys_out.p, T.rp.p);
+    CFA_CHECK_LAUNCH();
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    return CFA_OK;
+}
+
+// Greedy 3-phase aggregation of smoothed_prolongator (:1321-1348) on the host strength flags.
+static int aggregate_host(int n, const std::vector<int>& rp, const std::vector<int>& ci,
+                          const std::vector<unsigned char>& strong, std::vector<int>& agg) {
+    agg.assign(n, -1);
+    int na = 0;
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] >= 0) continue;
+        bool free_nbhd = true;
+        for (int a = rp[i]; a < rp[i + 1] && free_nbhd; ++a)
+            if (strong[a] && agg[ci[a]] >= 0) free_nbhd = false;
+        if (!free_nbhd) continue;
+        agg[i] = na;
+        for (int a = rp[i]; a < rp[i + 1]; ++a) if (strong[a]) agg[ci[a]] = na;
+        ++na;
+    }
+    std::vector<int> agg2(agg);
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] >= 0) continue;
+        for (int a = rp[i]; a < rp[i + 1]; ++a)
+            if (strong[a] && agg[ci[a]] >= 0) { agg2[i] = agg[ci[a]]; break; }
+    }
+    agg.swap(agg2);
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] >= 0) continue;
+        agg[i] = na;
+        for (int a = rp[i]; a < rp[i + 1]; ++a)
+            if (strong[a] && agg[ci[a]] < 0) agg[ci[a]] = na;
+        ++na;
+    }
+    return na;
+}
+
+static cfa_status copy_csr(cfa_ctx* ctx, int rows, int nnz, const int* rp, const int* ci, const double* v, DCsr& D) {
+    D.rows = rows;
+    D.cols = rows;
+    D.nnz = nnz;
+    CFA_CUDA(D.rp.ensure(rows + 1));
+    CFA_CUDA(D.ci.ensure(std::max(nnz, 1)));
+    CFA_CUDA(D.v.ensure(std::max(nnz, 1)));
+    CFA_CUDA(cudaMemcpyAsync(D.rp.p, rp, (rows + 1) * sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(D.ci.p, ci, (size_t)nnz * sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(D.v.p, v, (size_t)nnz * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    return CFA_OK;
+}
+
+static cfa_status to_float(cfa_ctx* ctx, DCsr& M) {
+    CFA_CUDA(M.v32.ensure(std::max(M.nnz, 1)));
+    if (M.nnz) CFA_LAUNCH(ctx, k_to_float, std::min(ceil_div(M.nnz, kThreads), 8 * ctx->num_sms), kThreads, 0,
+                          (long long)M.nnz, M.v.p, M.v32.p);
+    return CFA_OK;
+}
+
+// rho(D^-1 A) by 20 power iterations (spectral_radius_DinvA, :1276-1304), on the device.
+static cfa_status spectral_radius(cfa_ctx* ctx, cfa_amg* amg, const DCsr& A, const double* dinv, double* rho) {
+    const int n = A.rows, nch = (n + 4095) / 4096;
+    if ((int)amg->host_x0.size() < n) {
+        const size_t old = amg->host_x0.size();
+        amg->host_x0.resize(n);
+        for (size_t i = old; i < (size_t)n; ++i) amg->host_x0[i] = 1.0 + 0.1 * std::sin(1.0 + (double)i);
+        CFA_CUDA(amg->x0.ensure(n));
+        CFA_CUDA(cudaMemcpyAsync(amg->x0.p, amg->host_x0.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    DevBuf<double> x, y, py, px, st;
+    CFA_CUDA(x.ensure(n));
+    CFA_CUDA(y.ensure(n));
+    CFA_CUDA(py.ensure(nch));
+    CFA_CUDA(px.ensure(nch));
+    CFA_CUDA(st.ensure(2));
+    CFA_CUDA(cudaMemcpyAsync(x.p, amg->x0.p, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    for (int it = 0; it < 20; ++it) {
+        CFA_LAUNCH(ctx, k_pow_y, ceil_div(n, kThreads), kThreads, 0, n, A.rp.p, A.ci.p, A.v.p, dinv, x.p, y.p);
+        CFA_LAUNCH(ctx, k_pow_chunks, ceil_div(nch, 64), 64, 0, n, nch, x.p, y.p, py.p, px.p);
+        CFA_LAUNCH(ctx, k_pow_finish, 1, 32, 0, nch, py.p, px.p, st.p);
+        CFA_LAUNCH(ctx, k_pow_scale, ceil_div(n, kThreads), kThreads, 0, n, y.p, st.p, x.p);
+    }
+    double h[2];
+    CFA_CUDA(cudaMemcpyAsync(h, st.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    *rho = std::max(h[1], 1.0e-12) * 1.05;
+    return CFA_OK;
+}
+
+static cfa_status level_vectors(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int n) {
+    if (amg->opts.precision == CFA_MIXED) {
+        CFA_CUDA(L.x32.ensure(n)); CFA_CUDA(L.t32.ensure(n)); CFA_CUDA(L.b32.ensure(n)); CFA_CUDA(L.r32.ensure(n));
+    } else {
+        CFA_CUDA(L.x64.ensure(n)); CFA_CUDA(L.t64.ensure(n)); CFA_CUDA(L.b64.ensure(n)); CFA_CUDA(L.r64.ensure(n));
+    }
+    return CFA_OK;
+}
+
+static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* d_rp, const int* d_ci,
+                            const double* d_v) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const cfa_amg_opts& o = amg->opts;
+    amg->levels.clear();
+    amg->version++;
+    DCsr A;
+    CFA_PROPAGATE(copy_csr(ctx, n, nnz, d_rp, d_ci, d_v, A));
+    while (A.rows > o.coarse_target && (int)amg->levels.size() < o.max_levels - 1) {
+        const int m = A.rows;
+        AmgLevel L;
+        CFA_CUDA(L.dinv.ensure(m));
+        CFA_LAUNCH(ctx, k_amg_dinv, ceil_div(m, kThreads), kThreads, 0, m, A.rp.p, A.ci.p, A.v.p, L.dinv.p);
+        double rho = 1.0;
+        CFA_PROPAGATE(spectral_radius(ctx, amg, A, L.dinv.p, &rho));
+        const double omega = 4.0 / (3.0 * rho);
+        // strength on the device, aggregation on the host
+        DevBuf<unsigned char> strong;
+        CFA_CUDA(strong.ensure(std::max(A.nnz, 1)));
+        CFA_LAUNCH(ctx, k_strength, ceil_div(m, kThreads), kThreads, 0, m, A.rp.p, A.ci.p, A.v.p, L.dinv.p, o.theta,
+                   strong.p);
+        std::vector<int> h_rp(m + 1), h_ci(A.nnz);
+        std::vector<unsigned char> h_strong(A.nnz);
+        CFA_CUDA(cudaMemcpyAsync(h_rp.data(), A.rp.p, (m + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CFA_CUDA(cudaMemcpyAsync(h_ci.data(), A.ci.p, (size_t)A.nnz * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CFA_CUDA(cudaMemcpyAsync(h_strong.data(), strong.p, (size_t)A.nnz, cudaMemcpyDeviceToHost, ctx->stream));
+        CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+        std::vector<int> agg;
+        const int na = aggregate_host(m, h_rp, h_ci, h_strong, agg);
+        if (na >= (int)(0.85 * m) || na == 0) break;   // coarsening stalled (:1019)
+        std::vector<int> size(na, 0);
+        for (int i = 0; i < m; ++i) size[agg[i]]++;
+        std::vector<double> p0v(m);
+        std::vector<int> p0rp(m + 1);
+        for (int i = 0; i < m; ++i) { p0v[i] = 1.0 / std::sqrt((double)size[agg[i]]); p0rp[i] = i; }
+        p0rp[m] = m;
+        DevBuf<double> d_p0v;
+        DevBuf<int> d_p0rp;
+        CFA_CUDA(L.agg.ensure(m));
+        CFA_CUDA(d_p0v.ensure(m));
+        CFA_CUDA(d_p0rp.ensure(m + 1));
+        CFA_CUDA(cudaMemcpyAsync(L.agg.p, agg.data(), m * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        CFA_CUDA(cudaMemcpyAsync(d_p0v.p, p0v.data(), m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        CFA_CUDA(cudaMemcpyAsync(d_p0rp.p, p0rp.data(), (m + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        // AP0 = A P0, then P = P0 - omega D^-1 A P0
+        DCsr AP0;
+        CFA_PROPAGATE(spgemm(ctx, m, na, A.rp.p, A.ci.p, A.v.p, d_p0rp.p, L.agg.p, d_p0v.p, AP0));
+        DevBuf<int> cnt;
+        CFA_CUDA(cnt.ensure(m));
+        CFA_LAUNCH(ctx, k_p_rows, ceil_div(m, kThreads), kThreads, 0, m, AP0.rp.p, AP0.ci.p, AP0.v.p, L.agg.p, d_p0v.p,
+                   L.dinv.p, omega, (const int*)nullptr, (int*)nullptr, (double*)nullptr, cnt.p);
+        std::vector<int> h_cnt(m), h_prp(m + 1, 0);
+        CFA_CUDA(cudaMemcpyAsync(h_cnt.data(), cnt.p, m * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (int i = 0; i < m; ++i) h_prp[i + 1] = h_prp[i] + h_cnt[i];
+        L.P.rows = m;
+        L.P.cols = na;
+        L.P.nnz = h_prp[m];
+        CFA_CUDA(L.P.rp.ensure(m + 1));
+        CFA_CUDA(L.P.ci.ensure(std::max(L.P.nnz, 1)));
+        CFA_CUDA(L.P.v.ensure(std::max(L.P.nnz, 1)));
+        CFA_CUDA(cudaMemcpyAsync(L.P.rp.p, h_prp.data(), (m + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        CFA_LAUNCH(ctx, k_p_rows, ceil_div(m, kThreads), kThreads, 0, m, AP0.rp.p, AP0.ci.p, AP0.v.p, L.agg.p, d_p0v.p,
+                   L.dinv.p, omega, L.P.rp.p, L.P.ci.p, L.P.v.p, cnt.p);
+        CFA_CHECK_LAUNCH();
+        // R = P^T, A_c = R (A P)
+        CFA_PROPAGATE(transpose(ctx, L.P, L.R));
+        DCsr AP, Ac;
+        CFA_PROPAGATE(spgemm(ctx, m, na, A.rp.p, A.ci.p, A.v.p, L.P.rp.p, L.P.ci.p, L.P.v.p, AP));
+        CFA_PROPAGATE(spgemm(ctx, na, na, L.R.rp.p, L.R.ci.p, L.R.v.p, AP.rp.p, AP.ci.p, AP.v.p, Ac));
+        L.omega = omega;
+        L.A = std::move(A);
+        CFA_PROPAGATE(level_vectors(ctx, amg, L, m));
+        amg->levels.push_back(std::move(L));
+        A = std::move(Ac);
+    }
+    // coarsest level: dense Cholesky inverse on the device
+    const int cn = A.rows;
+    amg->coarse_n = cn;
+    DevBuf<double> M, colbuf;
+    DevBuf<int> err;
+    CFA_CUDA(M.ensure((size_t)cn * cn + 1));
+    CFA_CUDA(colbuf.ensure((size_t)cn * cn + 1));
+    CFA_CUDA(amg->coarse_inv.ensure((size_t)cn * cn + 1));
+    CFA_CUDA(err.ensure(1));
+    CFA_LAUNCH(ctx, k_dense_build, ceil_div(cn, 64), 64, 0, cn, A.rp.p, A.ci.p, A.v.p, M.p);
+    CFA_LAUNCH(ctx, k_cholesky, 1, 256, 0, cn, M.p, err.p);
+    CFA_LAUNCH(ctx, k_chol_inverse, ceil_div(cn, 32), 32, 0, cn, M.p, amg->coarse_inv.p, colbuf.p);
+    CFA_CHECK_LAUNCH();
+    int h_err = 0;
+    CFA_CUDA(cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(amg->cb64.ensure(cn + 1));
+    CFA_CUDA(amg->cx64.ensure(cn + 1));
+    if (o.precision == CFA_MIXED) {
+        CFA_CUDA(amg->cb32.ensure(cn + 1));
+        CFA_CUDA(amg->cx32.ensure(cn + 1));
+    }
+    // precision and kernel shapes of the V-cycle
+    for (AmgLevel& L : amg->levels) {
+        L.A.tpr = threads_per_row(L.A.rows, L.A.nnz);
+        L.P.tpr = threads_per_row(L.P.rows, L.P.nnz);
+        L.R.tpr = threads_per_row(L.R.rows, L.R.nnz);
+        if (o.precision == CFA_MIXED) {
+            CFA_PROPAGATE(to_float(ctx, L.A));
+            CFA_PROPAGATE(to_float(ctx, L.P));
+            CFA_PROPAGATE(to_float(ctx, L.R));
+            CFA_CUDA(L.dinv32.ensure(L.A.rows));
+            CFA_LAUNCH(ctx, k_to_float, std::min(ceil_div(L.A.rows, kThreads), 8 * ctx->num_sms), kThreads, 0,
+                       (long long)L.A.rows, L.dinv.p, L.dinv32.p);
+        }
+    }
+    CFA_CHECK_LAUNCH();
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    amg->setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (h_err) return set_error(ctx, CFA_COARSE_NOT_SPD, "coarsest AMG operator not SPD", __FILE__, __LINE__);
+    return CFA_OK;
+}
+
+}  // namespace cfa
+
+using namespace cfa;
+
+extern "C" {
+
+void cfa_amg_default_opts(cfa_amg_opts* o) {
+    if (!o) return;
+    o->theta = 0.08;
+    o->smooth_steps = 2;
+    o->coarse_target = 300;
+    o->max_levels = 15;
+    o->precision = CFA_FP64;
+}
+
+cfa_status cfa_amg_create(cfa_ctx* ctx, const cfa_amg_opts* opts, cfa_amg** out) {
+    if (!ctx || !out) return CFA_BAD_ARG;
+    auto* a = new cfa_amg();
+    if (opts) a->opts = *opts; else cfa_amg_default_opts(&a->opts);
+    if (a->opts.smooth_steps < 1 || a->opts.max_levels < 1 ||
+        (a->opts.precision != CFA_FP64 && a->opts.precision != CFA_MIXED)) {
+        delete a;
+        return set_error(ctx, CFA_BAD_ARG, "bad AMG options", __FILE__, __LINE__);
+    }
+    *out = a;
+    return CFA_OK;
+}
+
+cfa_status cfa_amg_destroy(cfa_amg* amg) {
+    delete amg;
+    return CFA_OK;
+}
+
+cfa_status cfa_amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* rp, const int* ci, const double* v) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(amg && n > 0 && nnz > 0 && rp && ci && v);
+    return amg_setup(ctx, amg, n, nnz, rp, ci, v);
+}
+
+cfa_status cfa_amg_apply(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(amg && r && z && amg->coarse_n > 0);
+    return amg_vcycle(ctx, amg, r, z, nullptr);
+}
+
+cfa_status cfa_amg_info(const cfa_amg* amg, int* num_levels, int* coarse_n, double* setup_ms) {
+    if (!amg) return CFA_BAD_ARG;
+    if (num_levels) *num_levels = (int)amg->levels.size() + 1;
+    if (coarse_n) *coarse_n = amg->coarse_n;
+    if (setup_ms) *setup_ms = amg->setup_ms;
+    return CFA_OK;
+}
+
+cfa_status cfa_amg_level(const cfa_amg* amg, int l, int* info, const int** agg, const int** Arp, const int** Aci,
+                         const double** Av, const int** Prp, const int** Pci, const double** Pv, const int** Rrp,
+                         const int** Rci, const double** Rv, double* omega) {
+    if (!amg || l < 0 || l >= (int)amg->levels.size()) return CFA_BAD_ARG;
+    const AmgLevel& L = amg->levels[l];
+    if (info) { info[0] = L.A.rows; info[1] = L.A.nnz; info[2] = L.P.cols; info[3] = L.P.nnz; info[4] = L.R.nnz; }
+    if (agg) *agg = L.agg.p;
+    if (Arp) *Arp = L.A.rp.p;
+    if (Aci) *Aci = L.A.ci.p;
+    if (Av) *Av = L.A.v.p;
+    if (Prp) *Prp = L.P.rp.p;
+    if (Pci) *Pci = L.P.ci.p;
+    if (Pv) *Pv = L.P.v.p;
+    if (Rrp) *Rrp = L.R.rp.p;
+    if (Rci) *Rci = L.R.ci.p;
+    if (Rv) *Rv = L.R.v.p;
+    if (omega) *omega = L.omega;
+    return CFA_OK;
+}
+
+cfa_status cfa_amg_coarse_inverse(const cfa_amg* amg, const double** inv) {
+    if (!amg || !inv) return CFA_BAD_ARG;
+    *inv = amg->coarse_inv.p;
+    return CFA_OK;
+}
+
+}  // extern "C"

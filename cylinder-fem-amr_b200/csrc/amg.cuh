@@ -1,0 +1,48 @@
+// SA-AMG handle (AmgPreconditioner, src/cfa/linalg.cuh:939-1432).
+#pragma once
+
+#include <vector>
+
+#include "internal.cuh"
+
+namespace cfa {
+
+struct DCsr {
+    int rows = 0, cols = 0, nnz = 0;
+    int tpr = 1;                   // threads per row of the V-cycle kernels
+    DevBuf<int> rp, ci;
+    DevBuf<double> v;              // FP64 values (setup arithmetic)
+    DevBuf<float> v32;             // FP32 copy (mixed precision)
+};
+
+struct AmgLevel {
+    DCsr A, P, R;
+    DevBuf<double> dinv;
+    DevBuf<float> dinv32;
+    double omega = 0.0;
+    DevBuf<int> agg;
+    // V-cycle vectors in the hierarchy precision: x, t (Jacobi ping-pong), b, r
+    DevBuf<double> x64, t64, b64, r64;
+    DevBuf<float> x32, t32, b32, r32;
+};
+
+}  // namespace cfa
+
+struct cfa_amg {
+    cfa_amg_opts opts{};
+    std::vector<cfa::AmgLevel> levels;   // levels with a prolongator (reference: levels)
+    int coarse_n = 0;
+    cfa::DevBuf<double> coarse_inv;      // dense inverse of the coarsest operator, row-major
+    cfa::DevBuf<double> cb64, cx64;      // coarsest right-hand side / solution (FP64)
+    cfa::DevBuf<float> cb32, cx32;
+    double setup_ms = 0.0;
+    int version = 0;                     // bumped by every setup (graph caches key on it)
+    std::vector<double> host_x0;         // 1 + 0.1 sin(1 + i), the power-iteration start vector
+    cfa::DevBuf<double> x0;
+};
+
+namespace cfa {
+// One symmetric V-cycle z = M^-1 r (FP64 in/out). Kernels return at once while *done != 0
+// (done nullable).
+cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done);
+}  // namespace cfa

@@ -1,0 +1,281 @@
+// Multicolour ILU(0): colouring and split pattern on the host exactly as
+// MulticolourIlu0::set_pattern (src/cfa/linalg.cuh:456-528); factor colour by colour in FP64
+// (k_ilu0_factor_colour, :366-392); sweeps colour by colour with one thread per row handling
+// both right-hand sides, so the factors are read once per apply (the reference's
+// k_ilu0_lower/upper_colour, :406-433, use a thread per row and component and read them twice).
+#include <algorithm>
+
+#include "ilu.cuh"
+
+namespace cfa {
+
+constexpr int kIluMaxRow = 32;   // ILU_MAX_ROW (src/cfa/linalg.cuh:361)
+
+// Row i of colour c: for its L entries k in elimination order, l_ik = a_ik / u_kk and
+// a_ij -= l_ik u_kj within the pattern. Same arithmetic and order as the reference kernel.
+__global__ void k_ilu_factor_colour(int m, const int* __restrict__ rows, const int* __restrict__ rp,
+                                    const int* __restrict__ ci, const int* __restrict__ colour,
+                                    const int* __restrict__ diag, double* __restrict__ lu) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    const int i = rows[t];
+    const int s = rp[i], len = rp[i + 1] - s;
+    const int cii = colour[i];
+    int cols[kIluMaxRow], ccol[kIluMaxRow];
+    double a[kIluMaxRow];
+    for (int q = 0; q < len; ++q) { cols[q] = ci[s + q]; ccol[q] = colour[cols[q]]; a[q] = lu[s + q]; }
+    for (int c = 0; c < cii; ++c) {
+        for (int q = 0; q < len; ++q) {
+            if (ccol[q] != c) continue;
+            const int k = cols[q];
+            const double lik = a[q] / lu[diag[k]];
+            a[q] = lik;
+            for (int mm = rp[k]; mm < rp[k + 1]; ++mm) {
+                const int j = ci[mm];
+                for (int b = 0; b < len; ++b)
+                    if (cols[b] == j) { if (ccol[b] > c) a[b] -= lik * lu[mm]; break; }
+            }
+        }
+    }
+    for (int q = 0; q < len; ++q) lu[s + q] = a[q];
+}
+
+// k_ilu0_gather (src/cfa/linalg.cuh:395-402), in the factor precision
+template <class T>
+__global__ void k_ilu_gather(int nl, int nu, int n, const int* __restrict__ l_src, const int* __restrict__ u_src,
+                             const int* __restrict__ d_src, const double* __restrict__ lu, T* __restrict__ lv,
+                             T* __restrict__ uv, T* __restrict__ dinv) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < nl) lv[e] = (T)lu[l_src[e]];
+    if (e < nu) uv[e] = (T)lu[u_src[e]];
+    if (e < n) dinv[e] = (T)(1.0 / lu[d_src[e]]);
+}
+
+// Forward sweep of one colour for NR right-hand sides: y_i = r_i - sum_L l_ie y_e (unit L); the
+// last colour also divides by u_ii. T: factor/work precision; FP64 output written when a row is
+// final (last colour here, else in the backward sweep).
+template <class T, int NR>
+__global__ void k_ilu_lower(int m, int n, const int* __restrict__ rows, const int* __restrict__ lp,
+                            const int* __restrict__ lc, const T* __restrict__ lv, const T* __restrict__ dinv,
+                            int last, const double* __restrict__ r, T* __restrict__ w, double* __restrict__ z,
+                            const int* __restrict__ done) {
+    if (done && *done) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    const int i = rows[t];
+    T acc[NR];
+#pragma unroll
+    for (int c = 0; c < NR; ++c) acc[c] = (T)r[(size_t)c * n + i];
+    for (int e = lp[t]; e < lp[t + 1]; ++e) {
+        const T l = lv[e];
+        const int j = lc[e];
+#pragma unroll
+        for (int c = 0; c < NR; ++c) acc[c] -= l * w[(size_t)c * n + j];
+    }
+    if (last) {
+        const T d = dinv[t];
+#pragma unroll
+        for (int c = 0; c < NR; ++c) {
+            acc[c] = acc[c] * d;
+            z[(size_t)c * n + i] = (double)acc[c];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < NR; ++c) w[(size_t)c * n + i] = acc[c];
+}
+
+// Backward sweep of one colour: z_i = (y_i - sum_U u_ie z_e) / u_ii
+template <class T, int NR>
+__global__ void k_ilu_upper(int m, int n, const int* __restrict__ rows, const int* __restrict__ up,
+                            const int* __restrict__ uc, const T* __restrict__ uv, const T* __restrict__ dinv,
+                            T* __restrict__ w, double* __restrict__ z, const int* __restrict__ done) {
+    if (done && *done) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    const int i = rows[t];
+    T acc[NR];
+#pragma unroll
+    for (int c = 0; c < NR; ++c) acc[c] = w[(size_t)c * n + i];
+    for (int e = up[t]; e < up[t + 1]; ++e) {
+        const T u = uv[e];
+        const int j = uc[e];
+#pragma unroll
+        for (int c = 0; c < NR; ++c) acc[c] -= u * w[(size_t)c * n + j];
+    }
+    const T d = dinv[t];
+#pragma unroll
+    for (int c = 0; c < NR; ++c) {
+        acc[c] = acc[c] * d;
+        w[(size_t)c * n + i] = acc[c];
+        z[(size_t)c * n + i] = (double)acc[c];
+    }
+}
+
+template <class T, int NR>
+static void sweeps(cfa_ctx* ctx, const cfa_ilu* h, const T* lv, const T* uv, const T* dinv, T* w,
+                   const double* r, double* z, const int* done) {
+    const int n = h->n;
+    for (int c = 0; c < h->nc; ++c) {
+        const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
+        if (m == 0) continue;
+        CFA_LAUNCH(ctx, (k_ilu_lower<T, NR>), ceil_div(m, kThreads), kThreads, 0, m, n, h->rows.p + cs, h->lp.p + cs,
+                   h->lc.p, lv, dinv + cs, c == h->nc - 1 ? 1 : 0, r, w, z, done);
+    }
+    for (int c = h->nc - 2; c >= 0; --c) {
+        const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
+        if (m == 0) continue;
+        CFA_LAUNCH(ctx, (k_ilu_upper<T, NR>), ceil_div(m, kThreads), kThreads, 0, m, n, h->rows.p + cs, h->up.p + cs,
+                   h->uc.p, uv, dinv + cs, w, z, done);
+    }
+}
+
+cfa_status ilu_apply(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z, int nrhs, const int* done) {
+    if (h->precision == CFA_MIXED) {
+        float* w = const_cast<cfa_ilu*>(h)->work32.p;
+        if (nrhs == 1) sweeps<float, 1>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r, z, done);
+        else sweeps<float, 2>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r, z, done);
+    } else {
+        // FP64: the sweeps work in place in z (as the reference)
+        if (nrhs == 1) sweeps<double, 1>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, z, r, z, done);
+        else sweeps<double, 2>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, z, r, z, done);
+    }
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+}  // namespace cfa
+
+using namespace cfa;
+
+extern "C" {
+
+cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, const int* d_rp, const int* d_ci,
+                          cfa_precision precision, cfa_ilu** out) {
+    if (!ctx || !out) return CFA_BAD_ARG;
+    CFA_ARG(n > 0 && rp && ci && d_rp && d_ci);
+    CFA_ARG(precision == CFA_FP64 || precision == CFA_MIXED);
+    *out = nullptr;
+    const int nnz = rp[n];
+    std::vector<int> colour(n, -1), diag(n, -1), mark;
+    int nc = 0;
+    for (int i = 0; i < n; ++i) {
+        if (rp[i + 1] - rp[i] > kIluMaxRow)
+            return set_error(ctx, CFA_ROW_TOO_LONG, "ILU row longer than 32 entries", __FILE__, __LINE__);
+        for (int a = rp[i]; a < rp[i + 1]; ++a) {
+            const int c = colour[ci[a]];
+            if (c >= 0) mark[c] = i;
+            if (ci[a] == i) diag[i] = a;
+        }
+        int c = 0;
+        while (c < nc && mark[c] == i) ++c;
+        if (c == nc) { ++nc; mark.push_back(-1); }
+        colour[i] = c;
+    }
+    auto* h = new cfa_ilu();
+    h->n = n; h->nnz = nnz; h->nc = nc; h->precision = precision; h->rp = d_rp; h->ci = d_ci;
+    h->colour_start.assign(nc + 1, 0);
+    for (int i = 0; i < n; ++i) h->colour_start[colour[i] + 1]++;
+    for (int c = 0; c < nc; ++c) h->colour_start[c + 1] += h->colour_start[c];
+    std::vector<int> rows(n), fill(h->colour_start.begin(), h->colour_start.end() - 1);
+    for (int i = 0; i < n; ++i) rows[fill[colour[i]]++] = i;
+    std::vector<int> lp(n + 1, 0), up(n + 1, 0);
+    for (int t = 0; t < n; ++t) {
+        const int i = rows[t];
+        int l = 0, u = 0;
+        for (int a = rp[i]; a < rp[i + 1]; ++a) {
+            if (ci[a] == i) continue;
+            if (colour[ci[a]] < colour[i]) ++l; else ++u;
+        }
+        lp[t + 1] = l; up[t + 1] = u;
+    }
+    for (int t = 0; t < n; ++t) { lp[t + 1] += lp[t]; up[t + 1] += up[t]; }
+    h->nl = lp[n]; h->nu = up[n];
+    std::vector<int> lc(h->nl), uc(h->nu), l_src(h->nl), u_src(h->nu), d_src(n);
+    for (int t = 0; t < n; ++t) {
+        const int i = rows[t];
+        int l = lp[t], u = up[t];
+        for (int a = rp[i]; a < rp[i + 1]; ++a) {
+            const int j = ci[a];
+            if (j == i) d_src[t] = a;
+            else if (colour[j] < colour[i]) { lc[l] = j; l_src[l++] = a; }
+            else { uc[u] = j; u_src[u++] = a; }
+        }
+    }
+    cudaError_t e = cudaSuccess;
+    auto up_int = [&](DevBuf<int>& d, const std::vector<int>& v) {
+        if (e != cudaSuccess) return;
+        e = d.ensure(std::max<size_t>(v.size(), 1));
+        if (e == cudaSuccess && !v.empty())
+            e = cudaMemcpyAsync(d.p, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+    };
+    up_int(h->rows, rows); up_int(h->colour, colour); up_int(h->diag, diag); up_int(h->lp, lp); up_int(h->up, up);
+    up_int(h->lc, lc); up_int(h->uc, uc); up_int(h->l_src, l_src); up_int(h->u_src, u_src); up_int(h->d_src, d_src);
+    if (e == cudaSuccess) e = h->lu.ensure(nnz);
+    if (precision == CFA_MIXED) {
+        if (e == cudaSuccess) e = h->lv32.ensure(std::max(h->nl, 1));
+        if (e == cudaSuccess) e = h->uv32.ensure(std::max(h->nu, 1));
+        if (e == cudaSuccess) e = h->dinv32.ensure(n);
+        if (e == cudaSuccess) e = h->work32.ensure(2 * (size_t)n);
+    } else {
+        if (e == cudaSuccess) e = h->lv64.ensure(std::max(h->nl, 1));
+        if (e == cudaSuccess) e = h->uv64.ensure(std::max(h->nu, 1));
+        if (e == cudaSuccess) e = h->dinv64.ensure(n);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        delete h;
+        return set_error(ctx, CFA_CUDA_ERROR, cudaGetErrorString(e), __FILE__, __LINE__);
+    }
+    *out = h;
+    return CFA_OK;
+}
+
+cfa_status cfa_ilu_destroy(cfa_ilu* ilu) {
+    delete ilu;
+    return CFA_OK;
+}
+
+cfa_status cfa_ilu_factor(cfa_ctx* ctx, cfa_ilu* h, const double* val) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(h && val);
+    CFA_CUDA(cudaMemcpyAsync(h->lu.p, val, (size_t)h->nnz * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    for (int c = 1; c < h->nc; ++c) {
+        const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
+        if (m == 0) continue;
+        CFA_LAUNCH(ctx, k_ilu_factor_colour, ceil_div(m, 128), 128, 0, m, h->rows.p + cs, h->rp, h->ci, h->colour.p,
+                   h->diag.p, h->lu.p);
+    }
+    const int len = std::max(h->n, std::max(h->nl, h->nu));
+    if (h->precision == CFA_MIXED)
+        CFA_LAUNCH(ctx, k_ilu_gather<float>, ceil_div(len, kThreads), kThreads, 0, h->nl, h->nu, h->n, h->l_src.p,
+                   h->u_src.p, h->d_src.p, h->lu.p, h->lv32.p, h->uv32.p, h->dinv32.p);
+    else
+        CFA_LAUNCH(ctx, k_ilu_gather<double>, ceil_div(len, kThreads), kThreads, 0, h->nl, h->nu, h->n, h->l_src.p,
+                   h->u_src.p, h->d_src.p, h->lu.p, h->lv64.p, h->uv64.p, h->dinv64.p);
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+cfa_status cfa_ilu_apply(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z, int nrhs) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(h && r && z && (nrhs == 1 || nrhs == 2));
+    CFA_ARG(r != z);
+    return ilu_apply(ctx, h, r, z, nrhs, nullptr);
+}
+
+cfa_status cfa_ilu_colours(const cfa_ilu* h, int* n_colours, int* colour_start) {
+    if (!h) return CFA_BAD_ARG;
+    if (n_colours) *n_colours = h->nc;
+    if (colour_start) std::copy(h->colour_start.begin(), h->colour_start.end(), colour_start);
+    return CFA_OK;
+}
+
+cfa_status cfa_ilu_device_arrays(const cfa_ilu* h, const int** colour, const int** rows, const double** lu) {
+    if (!h) return CFA_BAD_ARG;
+    if (colour) *colour = h->colour.p;
+    if (rows) *rows = h->rows.p;
+    if (lu) *lu = h->lu.p;
+    return CFA_OK;
+}
+
+}  // extern "C"

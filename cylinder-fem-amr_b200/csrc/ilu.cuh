@@ -1,0 +1,26 @@
+// Multicolour ILU(0) handle (MulticolourIlu0, src/cfa/linalg.cuh:435-568).
+#pragma once
+
+#include <vector>
+
+#include "internal.cuh"
+
+struct cfa_ilu {
+    int n = 0, nnz = 0, nc = 0, nl = 0, nu = 0;
+    cfa_precision precision = CFA_FP64;
+    const int* rp = nullptr;          // device pattern (caller-owned)
+    const int* ci = nullptr;
+    std::vector<int> colour_start;    // host, nc + 1
+    cfa::DevBuf<int> rows, colour, diag, lp, up, lc, uc, l_src, u_src, d_src;
+    cfa::DevBuf<double> lu;           // FP64 factor on the CSR pattern
+    cfa::DevBuf<double> lv64, uv64, dinv64;
+    cfa::DevBuf<float> lv32, uv32, dinv32;
+    cfa::DevBuf<float> work32;        // FP32 sweep vectors (mixed precision), nrhs * n
+};
+
+namespace cfa {
+// z = (LU)^-1 r, nrhs in {1, 2} vectors of stride n. FP64 in/out; internal precision of the
+// handle. `done` (nullable): device flag, the sweep kernels return at once when it is set and
+// `active` (nullable, 2 ints) masks components (inactive: z left unchanged).
+cfa_status ilu_apply(cfa_ctx* ctx, const cfa_ilu* ilu, const double* r, double* z, int nrhs, const int* done);
+}  // namespace cfa

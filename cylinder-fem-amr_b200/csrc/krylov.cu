@@ -1,0 +1,1166 @@
+// Krylov solvers with every scalar on the device.
+//
+// The reference drives PCG and BiCGSTAB from the host and copies each dot product back, with a
+// blocking D2H copy per dot (3 per CG iteration, 4 per BiCGSTAB2 iteration; src/cfa/linalg.cuh:
+// 172-177, :674-679). Here each dot product is fused into the kernel that produces its operand:
+// every block publishes fixed-order partials, the last block to finish sums them in a fixed
+// order and computes the recurrence scalars (alpha, beta, omega, stopping flags) into a state
+// struct in device memory that the following kernels read. A solve is one CUDA graph: the
+// initialisation kernels followed by a conditional WHILE node whose body is one iteration; the
+// body's kernels clear the condition when the solve stops, so the loop runs on the device with
+// no host round trip. Results are deterministic run to run.
+#include <algorithm>
+#include <cstring>
+#include <cstdlib>
+
+#include "amg.cuh"
+#include "ilu.cuh"
+#include "mesh.cuh"
+
+namespace cfa {
+
+// =============================================================================================
+// shared pieces
+// =============================================================================================
+struct CondArg {
+    cudaGraphConditionalHandle handle;
+    int use;
+};
+
+__device__ __forceinline__ void set_cond(CondArg c, unsigned v) {
+    if (c.use) cudaGraphSetConditional(c.handle, v);
+}
+
+#define ROWS_BEGIN(TPR, n)                                                                        \
+    {                                                                                             \
+        const int lane = threadIdx.x % (TPR);                                                     \
+        const int gw_ = (blockIdx.x * blockDim.x + threadIdx.x) / 32;                             \
+        const int nw_ = gridDim.x * blockDim.x / 32;                                              \
+        constexpr int rpw_ = 32 / (TPR);                                                          \
+        for (int base_ = gw_ * rpw_; base_ < (n); base_ += nw_ * rpw_) {                          \
+            const int row = base_ + (threadIdx.x & 31) / (TPR);                                   \
+            const bool valid = row < (n);
+
+#define ROWS_END \
+        }        \
+    }
+
+template <int TPR>
+__device__ __forceinline__ double group_reduce(double s) {
+#pragma unroll
+    for (int o = TPR / 2; o > 0; o /= 2) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
+    return s;
+}
+
+// plain SpMV (k_spmv_csr / k_spmv_csr_multi semantics), NR right-hand sides of stride n
+template <int TPR, int NR>
+__global__ void k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
+                       const double* __restrict__ x, double* __restrict__ y) {
+    ROWS_BEGIN(TPR, n)
+    double s[NR];
+#pragma unroll
+    for (int c = 0; c < NR; ++c) s[c] = 0.0;
+    if (valid)
+        for (int k = rp[row] + lane; k < rp[row + 1]; k += TPR) {
+            const double a = val[k];
+            const int j = ci[k];
+#pragma unroll
+            for (int c = 0; c < NR; ++c) s[c] += a * x[(size_t)c * n + j];
+        }
+#pragma unroll
+    for (int c = 0; c < NR; ++c) s[c] = group_reduce<TPR>(s[c]);
+    if (valid && lane == 0)
+#pragma unroll
+        for (int c = 0; c < NR; ++c) y[(size_t)c * n + row] = s[c];
+    ROWS_END
+}
+
+// Operator pass 1 (OSS only): pn = z + beta p (beta NULL: pn = z), g = M_L^-1 B pn (k_oss_apply_B,
+// src/cfa/fem_kernels.cuh:855-868), pn written for the own row when p_new != NULL.
+template <int TPR>
+__global__ void k_op_b(int n, int nnz, const int* __restrict__ rp, const int* __restrict__ ci,
+                       const double* __restrict__ oss, const double* __restrict__ inv_m, const double* __restrict__ z,
+                       const double* __restrict__ p, const double* __restrict__ beta_ptr, double* __restrict__ p_new,
+                       double* __restrict__ gx, double* __restrict__ gy, const int* __restrict__ done) {
+    if (done && *done) return;
+    const double beta = beta_ptr ? *beta_ptr : 0.0;
+    const double* Bx = oss;
+    const double* By = oss + nnz;
+    ROWS_BEGIN(TPR, n)
+    double sx = 0.0, sy = 0.0;
+    if (valid)
+        for (int k = rp[row] + lane; k < rp[row + 1]; k += TPR) {
+            const int j = ci[k];
+            const double pj = beta_ptr ? z[j] + beta * p[j] : z[j];
+            sx += Bx[k] * pj;
+            sy += By[k] * pj;
+        }
+    sx = group_reduce<TPR>(sx);
+    sy = group_reduce<TPR>(sy);
+    if (valid && lane == 0) {
+        const double im = inv_m[row];
+        gx[row] = sx * im;
+        gy[row] = sy * im;
+        if (p_new) p_new[row] = beta_ptr ? z[row] + beta * p[row] : z[row];
+    }
+    ROWS_END
+}
+
+// CG state (all on the device)
+struct CgState {
+    double bnorm, tol, rz, alpha, beta, rel, zero;
+    int iter, max_iter, done, converged, status, nullb;
+};
+
+// Operator pass 2: q = K pn - [not Dirichlet] (B^T_x g_x + B^T_y g_y) (k_spmv_csr + k_oss_apply_BT,
+// src/cfa/fem_kernels.cuh:871-885). FUSEP: pn = z + beta p computed on the fly (no OSS pass 1),
+// written to p_new for the own row. DOT: pq = pn . q in the last block, alpha = rz / pq and
+// the breakdown guard |pq| < 1e-30 of solve_pcg (src/cfa/linalg.cuh:232-236).
+template <int TPR, bool OSS, bool FUSEP, bool DOT>
+__global__ void __launch_bounds__(kThreads)
+k_op_k(int n, int nnz, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ K,
+       const double* __restrict__ oss, const int* __restrict__ tag, OutletBc bc, const double* __restrict__ z,
+       const double* __restrict__ p, const double* __restrict__ beta_ptr, double* __restrict__ pn_buf,
+       const double* __restrict__ gx, const double* __restrict__ gy, double* __restrict__ q, CgState* __restrict__ st,
+       double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond, const int* __restrict__ done) {
+    if (done && *done) return;
+    __shared__ double sh[kWarps];
+    const double beta = (FUSEP && beta_ptr) ? *beta_ptr : 0.0;
+    const double* BTx = oss + 2 * (size_t)nnz;
+    const double* BTy = oss + 3 * (size_t)nnz;
+    double acc = 0.0;
+    ROWS_BEGIN(TPR, n)
+    double s = 0.0, so = 0.0;
+    if (valid) {
+        for (int k = rp[row] + lane; k < rp[row + 1]; k += TPR) {
+            const int j = ci[k];
+            const double pj = FUSEP ? (beta_ptr ? z[j] + beta * p[j] : z[j]) : pn_buf[j];
+            s += K[k] * pj;
+            if (OSS) so += BTx[k] * gx[j] + BTy[k] * gy[j];
+        }
+    }
+    s = group_reduce<TPR>(s);
+    if (OSS) so = group_reduce<TPR>(so);
+    if (valid && lane == 0) {
+        if (OSS && !pressure_dirichlet(row, tag[row], bc)) s -= so;
+        q[row] = s;
+        const double pi = FUSEP ? (beta_ptr ? z[row] + beta * p[row] : z[row]) : pn_buf[row];
+        if (FUSEP && pn_buf) pn_buf[row] = pi;
+        if (DOT) acc += pi * s;
+    }
+    ROWS_END
+    if (!DOT) return;
+    double v[1] = {acc};
+    block_sum<1>(v, sh);
+    if (publish_partials<1>(v, part, counter)) {
+        reduce_partials<1>(v, part, counter, sh);
+        if (threadIdx.x == 0) {
+            const double pq = v[0];
+            if (fabs(pq) < 1.0e-30) {
+                st->done = 1;
+                st->converged = 0;
+                st->status = CFA_BREAKDOWN;
+                set_cond(cond, 0);
+            } else {
+                st->alpha = st->rz / pq;
+            }
+        }
+    }
+}
+
+// ||b|| (solve_pcg :205-209)
+__global__ void __launch_bounds__(kThreads)
+k_cg_bnorm(int n, const double* __restrict__ b, CgState* __restrict__ st, double* __restrict__ part,
+           unsigned int* __restrict__ counter, CondArg cond) {
+    __shared__ double sh[kWarps];
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] += b[i] * b[i];
+    block_sum<1>(v, sh);
+    if (publish_partials<1>(v, part, counter)) {
+        reduce_partials<1>(v, part, counter, sh);
+        if (threadIdx.x == 0) {
+            st->bnorm = sqrt(v[0]);
+            st->iter = 0;
+            st->done = 0;
+            st->converged = 1;
+            st->status = 0;
+            st->nullb = 0;
+            st->rel = 0.0;
+            st->beta = 0.0;
+            st->zero = 0.0;
+            if (st->bnorm < 1.0e-14) {
+                st->done = 1;
+                st->nullb = 1;
+                set_cond(cond, 0);
+            }
+        }
+    }
+}
+
+// r = b - q, ||r|| test (:213-218)
+__global__ void __launch_bounds__(kThreads)
+k_cg_resid0(int n, const double* __restrict__ b, const double* __restrict__ q, double* __restrict__ r,
+            CgState* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+    if (st->done) return;
+    __shared__ double sh[kWarps];
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double ri = b[i] + -1.0 * q[i];
+        r[i] = ri;
+        v[0] += ri * ri;
+    }
+    block_sum<1>(v, sh);
+    if (publish_partials<1>(v, part, counter)) {
+        reduce_partials<1>(v, part, counter, sh);
+        if (threadIdx.x == 0) {
+            const double rn = sqrt(v[0]);
+            if (rn < st->tol * st->bnorm) {
+                st->done = 1;
+                st->converged = 1;
+                set_cond(cond, 0);
+            }
+        }
+    }
+}
+
+__global__ void k_cg_nullx(int n, double* __restrict__ x, double* __restrict__ p0, const CgState* __restrict__ st) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (st->nullb) x[i] = 0.0;
+    p0[i] = 0.0;
+}
+
+// 1 / diag (k_extract_inv_diag, src/cfa/linalg.cuh:28-48)
+__global__ void k_inv_diag(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
+                           double* __restrict__ dinv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = 1.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) if (ci[k] == i) { d = val[k]; break; }
+    dinv[i] = (fabs(d) > 1.0e-14) ? (1.0 / d) : 1.0;
+}
+
+// x += alpha pn, r -= alpha q, p = pn, ||r|| test (:237-247); JAC: z = D^-1 r and r.z -> beta
+template <bool JAC>
+__global__ void __launch_bounds__(kThreads)
+k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ pn, double* __restrict__ p,
+            const double* __restrict__ q, const double* __restrict__ dinv, double* __restrict__ z,
+            CgState* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+    if (st->done) return;
+    __shared__ double sh[2 * kWarps];
+    const double alpha = st->alpha;
+    double v[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double pi = pn[i];
+        x[i] += alpha * pi;
+        const double ri = r[i] + -alpha * q[i];
+        r[i] = ri;
+        p[i] = pi;
+        v[0] += ri * ri;
+        if (JAC) {
+            const double zi = dinv[i] * ri;
+            z[i] = zi;
+            v[1] += ri * zi;
+        }
+    }
+    block_sum<2>(v, sh);
+    if (publish_partials<2>(v, part, counter)) {
+        reduce_partials<2>(v, part, counter, sh);
+        if (threadIdx.x == 0) {
+            const double rn = sqrt(v[0]);
+            st->rel = rn / st->bnorm;
+            const int it = st->iter + 1;
+            st->iter = it;
+            if (rn < st->tol * st->bnorm) {
+                st->done = 1;
+                st->converged = 1;
+                set_cond(cond, 0);
+            } else if (it >= st->max_iter) {
+                st->done = 1;
+                st->converged = 0;
+                st->status = CFA_NOT_CONVERGED;
+                set_cond(cond, 0);
+            } else if (JAC) {
+                const double rz_new = v[1];
+                st->beta = rz_new / (st->rz + 1.0e-30);
+                st->rz = rz_new;
+            }
+        }
+    }
+}
+
+// r.z after the preconditioner: first = initial rz (p = z); else beta = rz_new / (rz + 1e-30)
+__global__ void __launch_bounds__(kThreads)
+k_cg_rz(int n, const double* __restrict__ r, const double* __restrict__ z, int first, CgState* __restrict__ st,
+        double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+    if (st->done) return;
+    __shared__ double sh[kWarps];
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] += r[i] * z[i];
+    block_sum<1>(v, sh);
+    if (publish_partials<1>(v, part, counter)) {
+        reduce_partials<1>(v, part, counter, sh);
+        if (threadIdx.x == 0) {
+            if (first) {
+                st->rz = v[0];
+                st->beta = 0.0;
+                set_cond(cond, 1);
+            } else {
+                st->beta = v[0] / (st->rz + 1.0e-30);
+                st->rz = v[0];
+            }
+        }
+    }
+}
+
+// =============================================================================================
+// two-component BiCGSTAB (GpuBicgstab2::solve, src/cfa/linalg.cuh:656-754)
+// =============================================================================================
+struct B2State {
+    double tol;
+    double rn0[2], bd[2], rho[2], rho_old[2], alpha[2], omega[2], rel[2];
+    double cb[2], co[2], ca[2], a1[2], a2[2], cw[2];
+    int active[2], iters[2], conv[2], s_done[2];
+    int iter, max_iter, done, pad;
+};
+
+__device__ __forceinline__ void b2_stop(B2State* st, int c, int it, int ok) {
+    st->active[c] = 0;
+    st->iters[c] = it;
+    st->conv[c] = ok;
+}
+
+// start of an iteration (:699-707): breakdown on rho, p-update coefficients
+__device__ __forceinline__ void b2_begin_iteration(B2State* st, CondArg cond) {
+    const int iter = st->iter;
+    if (iter >= st->max_iter) { st->done = 1; set_cond(cond, 0); return; }
+    for (int c = 0; c < 2; ++c) {
+        st->cb[c] = 0.0;
+        st->co[c] = 0.0;
+        if (st->active[c] && fabs(st->rho[c]) < st->bd[c]) b2_stop(st, c, iter, 0);
+        if (st->active[c] && iter > 0) {
+            st->cb[c] = (st->rho[c] / st->rho_old[c]) * (st->alpha[c] / (st->omega[c] + 1.0e-30));
+            st->co[c] = st->omega[c];
+        }
+    }
+    if (!(st->active[0] || st->active[1])) { st->done = 1; set_cond(cond, 0); }
+}
+
+// v = A x (x = [x_u | x_v] given as two pointers), r = b - v, r0 = p = r, v = 0, ||r|| (:681-697)
+template <int TPR>
+__global__ void __launch_bounds__(kThreads)
+k_b2_init(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
+          const double* __restrict__ xu, const double* __restrict__ xv, const double* __restrict__ bu,
+          const double* __restrict__ bv, double* __restrict__ r, double* __restrict__ r0, double* __restrict__ p,
+          double* __restrict__ vv, B2State* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter,
+          CondArg cond) {
+    __shared__ double sh[2 * kWarps];
+    double acc[2] = {0.0, 0.0};
+    ROWS_BEGIN(TPR, n)
+    double su = 0.0, sv = 0.0;
+    if (valid)
+        for (int k = rp[row] + lane; k < rp[row + 1]; k += TPR) {
+            const double a = val[k];
+            const int j = ci[k];
+            su += a * xu[j];
+            sv += a * xv[j];
+        }
+    su = group_reduce<TPR>(su);
+    sv = group_reduce<TPR>(sv);
+    if (valid && lane == 0) {
+        const double ru = bu[row] - 1.0 * su, rv = bv[row] - 1.0 * sv;
+        r[row] = ru; r[n + row] = rv;
+        r0[row] = ru; r0[n + row] = rv;
+        p[row] = ru; p[n + row] = rv;
+        vv[row] = 0.0; vv[n + row] = 0.0;
+        acc[0] += ru * ru;
+        acc[1] += rv * rv;
+    }
+    ROWS_END
+    block_sum<2>(acc, sh);
+    if (publish_partials<2>(acc, part, counter)) {
+        reduce_partials<2>(acc, part, counter, sh);
+        if (threadIdx.x == 0) {
+            for (int c = 0; c < 2; ++c) {
+                st->rn0[c] = sqrt(acc[c]);
+                st->rho[c] = acc[c];
+                st->bd[c] = 1.0e-30 * st->rn0[c] * st->rn0[c] + 1.0e-300;
+                st->rho_old[c] = 1.0; st->alpha[c] = 1.0; st->omega[c] = 1.0;
+                st->iters[c] = 0; st->conv[c] = 1; st->rel[c] = 0.0; st->s_done[c] = 0;
+                st->active[c] = st->rn0[c] >= 1.0e-13;
+            }
+            st->iter = 0;
+            st->done = 0;
+            set_cond(cond, 1);
+            b2_begin_iteration(st, cond);
+        }
+    }
+}
+
+// p = r + cb (p - co v) (k_bicg2_p)
+__global__ void k_b2_p(int n, const double* __restrict__ r, const double* __restrict__ v, double* __restrict__ p,
+                       const B2State* __restrict__ st) {
+    if (st->done) return;
+    const double cb0 = st->cb[0], cb1 = st->cb[1], co0 = st->co[0], co1 = st->co[1];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * n; i += gridDim.x * blockDim.x) {
+        const int c = i >= n;
+        p[i] = r[i] + (c ? cb1 : cb0) * (p[i] - (c ? co1 : co0) * v[i]);
+    }
+}
+
+// v = A phat, r0 . v -> alpha (:711-719)
+template <int TPR>
+__global__ void __launch_bounds__(kThreads)
+k_b2_v(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
+       const double* __restrict__ phat, const double* __restrict__ r0, double* __restrict__ vv, B2State* __restrict__ st,
+       double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+    if (st->done) return;
+    __shared__ double sh[2 * kWarps];
+    double acc[2] = {0.0, 0.0};
+    ROWS_BEGIN(TPR, n)
+    double su = 0.0, sv = 0.0;
+    if (valid)
+        for (int k = rp[row] + lane; k < rp[row + 1]; k += TPR) {
+            const double a = val[k];
+            const int j = ci[k];
+            su += a * phat[j];
+            sv += a * phat[n + j];
+        }
+    su = group_reduce<TPR>(su);
+    sv = group_reduce<TPR>(sv);
+    if (valid && lane == 0) {
+        vv[row] = su;
+        vv[n + row] = sv;
+        acc[0] += r0[row] * su;
+        acc[1] += r0[n + row] * sv;
+    }
+    ROWS_END
+    block_sum<2>(acc, sh);
+    if (publish_partials<2>(acc, part, counter)) {
+        reduce_partials<2>(acc, part, counter, sh);
+        if (threadIdx.x == 0) {
+            const int iter = st->iter;
+            for (int c = 0; c < 2; ++c) {
+                st->ca[c] = 0.0;
+                if (st->active[c] && fabs(acc[c]) < st->bd[c]) b2_stop(st, c, iter, 0);
+                if (st->active[c]) { st->alpha[c] = st->rho[c] / acc[c]; st->ca[c] = st->alpha[c]; }
+            }
+            if (!(st->active[0] || st->active[1])) { st->done = 1; set_cond(cond, 0); }
+        }
+    }
+}
+
+// s = r - ca v (k_bicg2_s)
+__global__ void k_b2_s(int n, const double* __restrict__ r, const double* __restrict__ v, double* __restrict__ s,
+                       const B2State* __restrict__ st) {
+    if (st->done) return;
+    const double a0 = st->ca[0], a1 = st->ca[1];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * n; i += gridDim.x * blockDim.x)
+        s[i] = r[i] - (i >= n ? a1 : a0) * v[i];
+}
+
+// t = A shat; s.s, t.t, t.s -> omega, s-stop (:723-736)
+template <int TPR>
+__global__ void __launch_bounds__(kThreads)
+k_b2_t(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
+       const double* __restrict__ shat, const double* __restrict__ s, double* __restrict__ t, B2State* __restrict__ st,
+       double* __restrict__ part, unsigned int* __restrict__ counter) {
+    if (st->done) return;
+    __shared__ double sh[6 * kWarps];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    ROWS_BEGIN(TPR, n)
+    double su = 0.0, sv = 0.0;
+    if (valid)
+        for (int k = rp[row] + lane; k < rp[row + 1]; k += TPR) {
+            const double a = val[k];
+            const int j = ci[k];
+            su += a * shat[j];
+            sv += a * shat[n + j];
+        }
+    su = group_reduce<TPR>(su);
+    sv = group_reduce<TPR>(sv);
+    if (valid && lane == 0) {
+        t[row] = su;
+        t[n + row] = sv;
+        const double s0 = s[row], s1 = s[n + row];
+        acc[0] += s0 * s0; acc[1] += s1 * s1;
+        acc[2] += su * su; acc[3] += sv * sv;
+        acc[4] += su * s0; acc[5] += sv * s1;
+    }
+    ROWS_END
+    block_sum<6>(acc, sh);
+    if (publish_partials<6>(acc, part, counter)) {
+        reduce_partials<6>(acc, part, counter, sh);
+        if (threadIdx.x == 0) {
+            for (int c = 0; c < 2; ++c) {
+                st->a1[c] = 0.0; st->a2[c] = 0.0; st->cw[c] = 0.0; st->s_done[c] = 0;
+                if (!st->active[c]) continue;
+                st->a1[c] = st->alpha[c];
+                const double s_norm = sqrt(acc[c]);
+                if (s_norm < st->tol * st->rn0[c] || s_norm < 1.0e-11) { st->s_done[c] = 1; continue; }
+                const double tt = acc[2 + c];
+                st->omega[c] = (tt > st->bd[c]) ? (acc[4 + c] / tt) : 0.0;
+                st->a2[c] = st->omega[c];
+                st->cw[c] = st->omega[c];
+            }
+        }
+    }
+}
+
+// x += a1 phat + a2 shat, r = s - cw t; r.r, r0.r -> stop tests, rho (:737-750); then the
+// start of the next iteration
+__global__ void __launch_bounds__(kThreads)
+k_b2_xr(int n, double* __restrict__ xu, double* __restrict__ xv, const double* __restrict__ phat,
+        const double* __restrict__ shat, const double* __restrict__ s, const double* __restrict__ t,
+        double* __restrict__ r, const double* __restrict__ r0, B2State* __restrict__ st, double* __restrict__ part,
+        unsigned int* __restrict__ counter, CondArg cond) {
+    if (st->done) return;
+    __shared__ double sh[4 * kWarps];
+    const double a10 = st->a1[0], a11 = st->a1[1], a20 = st->a2[0], a21 = st->a2[1], w0 = st->cw[0], w1 = st->cw[1];
+    double acc[4] = {0, 0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        xu[i] += a10 * phat[i] + a20 * shat[i];
+        xv[i] += a11 * phat[n + i] + a21 * shat[n + i];
+        const double ru = s[i] - w0 * t[i], rv = s[n + i] - w1 * t[n + i];
+        r[i] = ru;
+        r[n + i] = rv;
+        acc[0] += ru * ru; acc[1] += rv * rv;
+        acc[2] += r0[i] * ru; acc[3] += r0[n + i] * rv;
+    }
+    block_sum<4>(acc, sh);
+    if (publish_partials<4>(acc, part, counter)) {
+        reduce_partials<4>(acc, part, counter, sh);
+        if (threadIdx.x == 0) {
+            const int iter = st->iter;
+            for (int c = 0; c < 2; ++c) if (st->s_done[c] && st->active[c]) b2_stop(st, c, iter + 1, 1);
+            if (!(st->active[0] || st->active[1])) {
+                st->done = 1;
+                set_cond(cond, 0);
+            } else {
+                for (int c = 0; c < 2; ++c) {
+                    if (!st->active[c]) continue;
+                    const double r_norm = sqrt(acc[c]);
+                    st->rel[c] = r_norm / st->rn0[c];
+                    if (r_norm < st->tol * st->rn0[c] || r_norm < 1.0e-11) { b2_stop(st, c, iter + 1, 1); continue; }
+                    st->rho_old[c] = st->rho[c];
+                    st->rho[c] = acc[2 + c];
+                    if (iter + 1 == st->max_iter) b2_stop(st, c, st->max_iter, 0);
+                }
+                st->iter = iter + 1;
+                if (!(st->active[0] || st->active[1])) { st->done = 1; set_cond(cond, 0); }
+                else b2_begin_iteration(st, cond);
+            }
+        }
+    }
+}
+
+// =============================================================================================
+// Jacobi BiCGSTAB (GpuLinearSolver::solve_bicgstab, :261-347), host-driven like the reference
+// but with the fused dot kernels (kept simple: it is the non-default solver and a test oracle).
+// =============================================================================================
+__global__ void __launch_bounds__(kThreads)
+k_dot(int n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out,
+      double* __restrict__ part, unsigned int* __restrict__ counter) {
+    __shared__ double sh[kWarps];
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] += a[i] * b[i];
+    block_sum<1>(v, sh);
+    if (publish_partials<1>(v, part, counter)) {
+        reduce_partials<1>(v, part, counter, sh);
+        if (threadIdx.x == 0) *out = v[0];
+    }
+}
+
+__global__ void k_axpby(int n, double a, const double* __restrict__ x, double b, const double* __restrict__ y,
+                        double* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = a * x[i] + b * y[i];
+}
+__global__ void k_axpy(int n, double a, const double* __restrict__ x, double* __restrict__ y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += a * x[i];
+}
+__global__ void k_vmul(int n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = a[i] * b[i];
+}
+__global__ void k_bicg_p(int n, const double* __restrict__ r, const double* __restrict__ v, double beta, double omega,
+                         double* __restrict__ p) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        p[i] = r[i] + beta * (p[i] - omega * v[i]);
+}
+
+// =============================================================================================
+// solver workspaces and graphs
+// =============================================================================================
+// Operator row shape: TPR from the mean row length (P1: about 7 per row)
+static int op_tpr(int n, long long nnz) {
+    const double per_row = n > 0 ? (double)nnz / n : 1.0;
+    if (per_row <= 2.5) return 2;
+    if (per_row <= 5.0) return 4;
+    if (per_row <= 12.0) return 8;
+    return 16;
+}
+
+#define OP_TPR_SWITCH(tpr, ...)                                                                \
+    do {                                                                                       \
+        switch (tpr) {                                                                         \
+            case 2: { constexpr int TPR = 2; __VA_ARGS__; } break;                              \
+            case 4: { constexpr int TPR = 4; __VA_ARGS__; } break;                              \
+            case 8: { constexpr int TPR = 8; __VA_ARGS__; } break;                              \
+            default: { constexpr int TPR = 16; __VA_ARGS__; } break;                            \
+        }                                                                                      \
+    } while (0)
+
+struct GraphCache {
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    std::vector<const void*> key;
+    long long init_kernels = 0, body_kernels = 0;
+    void reset() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        key.clear();
+    }
+    ~GraphCache() { reset(); }
+};
+
+struct PcgWork {
+    int cap = 0;
+    DevBuf<double> r, z, p, pn, q, gx, gy, dinv;
+    DevBuf<CgState> st;
+    DevBuf<double> part;
+    DevBuf<unsigned int> counter;
+    GraphCache graph;
+};
+
+struct B2Work {
+    int cap = 0;
+    DevBuf<double> r, r0, p, v, s, t, phat, shat;
+    DevBuf<B2State> st;
+    DevBuf<double> part;
+    DevBuf<unsigned int> counter;
+    GraphCache graph;
+};
+
+struct SolverWork {
+    PcgWork pcg;
+    B2Work b2;
+};
+
+static SolverWork* work(cfa_ctx* ctx) {
+    if (!ctx->work) ctx->work = new SolverWork();
+    return ctx->work;
+}
+
+void free_solver_work(cfa_ctx* ctx) {
+    delete ctx->work;
+    ctx->work = nullptr;
+}
+
+static bool graphs_enabled() {
+    const char* e = std::getenv("CFA_GRAPHS");
+    return !(e && e[0] == '0');
+}
+
+// Captures `init` then a WHILE node with `body` into `gc` (the init kernels set the condition).
+template <class Init, class Body>
+static cfa_status build_graph(cfa_ctx* ctx, GraphCache& gc, Init init, Body body) {
+    gc.reset();
+    cudaGraph_t g = nullptr;
+    CFA_CUDA(cudaGraphCreate(&g, 0));
+    gc.graph = g;
+    cudaGraphConditionalHandle handle;
+    CFA_CUDA(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
+    CondArg cond{handle, 1};
+    // init part, captured into g (launch counts of captures are added per replay instead)
+    long long l0 = ctx->launches;
+    CFA_CUDA(cudaStreamBeginCaptureToGraph(ctx->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    cfa_status s = init(cond);
+    cudaGraph_t captured = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &captured);
+    gc.init_kernels = ctx->launches - l0;
+    ctx->launches = l0;
+    if (s != CFA_OK) return s;
+    CFA_CUDA(e);
+    // the WHILE node depends on every leaf of the init part
+    size_t nn = 0;
+    CFA_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    CFA_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+    std::vector<cudaGraphNode_t> leaves;
+    for (cudaGraphNode_t nd : nodes) {
+        size_t ndep = 0;
+        CFA_CUDA(cudaGraphNodeGetDependentNodes(nd, nullptr, &ndep));
+        if (ndep == 0) leaves.push_back(nd);
+    }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    CFA_CUDA(cudaGraphAddNode(&wnode, g, leaves.data(), leaves.size(), &cp));
+    cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+    l0 = ctx->launches;
+    CFA_CUDA(cudaStreamBeginCaptureToGraph(ctx->stream, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    s = body(cond);
+    e = cudaStreamEndCapture(ctx->stream, &captured);
+    gc.body_kernels = ctx->launches - l0;
+    ctx->launches = l0;
+    if (s != CFA_OK) return s;
+    CFA_CUDA(e);
+    CFA_CUDA(cudaGraphInstantiate(&gc.exec, g, 0));
+    return CFA_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// PCG
+// ---------------------------------------------------------------------------------------------
+struct PcgArgs {
+    int n, nnz;
+    const int *rp, *ci;
+    const double* val;
+    const double *b;
+    double* x;
+    const cfa_oss_operator* oss;
+    cfa_amg* amg;
+    int max_iter;
+    double tol;
+};
+
+static cfa_status pcg_operator(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, const double* z, const double* p,
+                               const double* beta_ptr, double* pn, double* q, bool dot, CondArg cond,
+                               const int* done) {
+    const int tpr = op_tpr(a.n, a.nnz);
+    const int grid = row_grid(ctx, a.n, tpr);
+    CgState* st = W.st.p;
+    if (a.oss) {
+        const cfa_mesh* m = a.oss->mesh;
+        OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_op_b<TPR>), grid, kThreads, 0, a.n, a.nnz, a.rp, a.ci, a.oss->d_oss_val,
+                                      a.oss->d_inv_m, z, p, beta_ptr, pn, W.gx.p, W.gy.p, done));
+        if (dot)
+            OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_op_k<TPR, true, false, true>), grid, kThreads, 0, a.n, a.nnz, a.rp,
+                                          a.ci, a.val, a.oss->d_oss_val, m->tag, m->bc, z, p, beta_ptr, pn, W.gx.p,
+                                          W.gy.p, q, st, W.part.p, W.counter.p, cond, done));
+        else
+            OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_op_k<TPR, true, false, false>), grid, kThreads, 0, a.n, a.nnz, a.rp,
+                                          a.ci, a.val, a.oss->d_oss_val, m->tag, m->bc, z, p, beta_ptr, pn, W.gx.p,
+                                          W.gy.p, q, st, W.part.p, W.counter.p, cond, done));
+    } else {
+        OutletBc nobc;
+        if (dot)
+            OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_op_k<TPR, false, true, true>), grid, kThreads, 0, a.n, a.nnz, a.rp,
+                                          a.ci, a.val, (const double*)nullptr, (const int*)nullptr, nobc, z, p, beta_ptr,
+                                          pn, (const double*)nullptr, (const double*)nullptr, q, st, W.part.p,
+                                          W.counter.p, cond, done));
+        else
+            OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_op_k<TPR, false, true, false>), grid, kThreads, 0, a.n, a.nnz, a.rp,
+                                          a.ci, a.val, (const double*)nullptr, (const int*)nullptr, nobc, z, p, beta_ptr,
+                                          pn, (const double*)nullptr, (const double*)nullptr, q, st, W.part.p,
+                                          W.counter.p, cond, done));
+    }
+    return CFA_OK;
+}
+
+static cfa_status pcg_init(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg cond) {
+    const int n = a.n;
+    const int gv = row_grid(ctx, n, 1);
+    CgState* st = W.st.p;
+    const int* done = &st->done;
+    CFA_LAUNCH(ctx, k_cg_bnorm, gv, kThreads, 0, n, a.b, st, W.part.p, W.counter.p, cond);
+    if (!a.amg) CFA_LAUNCH(ctx, k_inv_diag, ceil_div(n, kThreads), kThreads, 0, n, a.rp, a.ci, a.val, W.dinv.p);
+    // q = A x (pn scratch receives x)
+    CFA_PROPAGATE(pcg_operator(ctx, W, a, a.x, a.x, nullptr, W.pn.p, W.q.p, false, cond, done));
+    CFA_LAUNCH(ctx, k_cg_resid0, gv, kThreads, 0, n, a.b, W.q.p, W.r.p, st, W.part.p, W.counter.p, cond);
+    if (a.amg) CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done));
+    else CFA_LAUNCH(ctx, k_vmul, gv, kThreads, 0, n, W.dinv.p, W.r.p, W.z.p);
+    CFA_LAUNCH(ctx, k_cg_nullx, ceil_div(n, kThreads), kThreads, 0, n, a.x, W.p.p, st);
+    CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, 1, st, W.part.p, W.counter.p, cond);
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+static cfa_status pcg_body(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg cond) {
+    const int n = a.n;
+    const int gv = row_grid(ctx, n, 1);
+    CgState* st = W.st.p;
+    const int* done = &st->done;
+    // q = A pn with pn = z + beta p
+    CFA_PROPAGATE(pcg_operator(ctx, W, a, W.z.p, W.p.p, &st->beta, W.pn.p, W.q.p, true, cond, done));
+    if (a.amg) {
+        CFA_LAUNCH(ctx, k_cg_update<false>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p,
+                   (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond);
+        CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done));
+        CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, 0, st, W.part.p, W.counter.p, cond);
+    } else {
+        CFA_LAUNCH(ctx, k_cg_update<true>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p, W.dinv.p, W.z.p, st,
+                   W.part.p, W.counter.p, cond);
+    }
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* rep) {
+    PcgWork& W = work(ctx)->pcg;
+    const int n = a.n;
+    if (n > W.cap) {
+        W.graph.reset();
+        for (DevBuf<double>* b : {&W.r, &W.z, &W.p, &W.pn, &W.q, &W.gx, &W.gy, &W.dinv}) CFA_CUDA(b->ensure(n));
+        CFA_CUDA(W.st.ensure(1));
+        CFA_CUDA(W.counter.ensure(1));
+        CFA_CUDA(cudaMemsetAsync(W.counter.p, 0, sizeof(unsigned int), ctx->stream));
+        W.cap = n;
+    }
+    CFA_CUDA(W.part.ensure(8 * (size_t)row_grid(ctx, n, 1) + 64));
+    // parameters
+    CgState init{};
+    init.tol = a.tol;
+    init.max_iter = a.max_iter;
+    CFA_CUDA(cudaMemcpyAsync(W.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
+    CFA_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+    long long extra_body = 0;
+    if (graphs_enabled()) {
+        std::vector<const void*> key = {a.rp, a.ci, a.val, a.b, a.x, a.oss ? a.oss->d_oss_val : nullptr,
+                                        a.oss ? a.oss->d_inv_m : nullptr, a.oss ? (const void*)a.oss->mesh : nullptr,
+                                        a.amg, (const void*)(intptr_t)(a.amg ? a.amg->version : 0),
+                                        (const void*)(intptr_t)n, (const void*)(intptr_t)a.nnz};
+        if (!W.graph.exec || W.graph.key != key) {
+            CFA_PROPAGATE(build_graph(ctx, W.graph, [&](CondArg c) { return pcg_init(ctx, W, a, c); },
+                                      [&](CondArg c) { return pcg_body(ctx, W, a, c); }));
+            W.graph.key = key;
+        }
+        CFA_CUDA(cudaGraphLaunch(W.graph.exec, ctx->stream));
+        extra_body = W.graph.body_kernels;
+        ctx->launches += W.graph.init_kernels;
+    } else {
+        CondArg none{0, 0};
+        const long long l0 = ctx->launches;
+        CFA_PROPAGATE(pcg_init(ctx, W, a, none));
+        (void)l0;
+        int polled = 0;
+        for (int it = 0; it < a.max_iter; ++it) {
+            CFA_PROPAGATE(pcg_body(ctx, W, a, none));
+            if (++polled == 8 || it + 1 == a.max_iter) {
+                polled = 0;
+                int d = 0;
+                CFA_CUDA(cudaMemcpyAsync(&d, &W.st.p->done, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+                CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+                if (d) break;
+            }
+        }
+    }
+    CFA_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    CgState h;
+    CFA_CUDA(cudaMemcpyAsync(&h, W.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    CFA_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->launches += extra_body * (long long)(h.iter + (h.status == CFA_BREAKDOWN ? 1 : 0));
+    if (rep) {
+        rep->iterations[0] = h.iter;
+        rep->iterations[1] = 0;
+        rep->converged[0] = h.converged;
+        rep->converged[1] = 1;
+        rep->rel_residual[0] = h.rel;
+        rep->rel_residual[1] = 0.0;
+        rep->solve_ms = ms;
+    }
+    if (h.status == CFA_BREAKDOWN) return CFA_BREAKDOWN;
+    return h.converged ? CFA_OK : CFA_NOT_CONVERGED;
+}
+
+// ---------------------------------------------------------------------------------------------
+// BiCGSTAB2
+// ---------------------------------------------------------------------------------------------
+struct B2Args {
+    int n, nnz;
+    const int *rp, *ci;
+    const double* val;
+    const double *bu, *bv;
+    double *xu, *xv;
+    const cfa_ilu* ilu;
+    int max_iter;
+    double tol;
+};
+
+static cfa_status b2_init(cfa_ctx* ctx, B2Work& W, const B2Args& a, CondArg cond) {
+    const int tpr = op_tpr(a.n, a.nnz);
+    const int grid = row_grid(ctx, a.n, tpr);
+    OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_init<TPR>), grid, kThreads, 0, a.n, a.rp, a.ci, a.val, (const double*)a.xu,
+                                  (const double*)a.xv, a.bu, a.bv, W.r.p, W.r0.p, W.p.p, W.v.p, W.st.p, W.part.p,
+                                  W.counter.p, cond));
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+static cfa_status b2_body(cfa_ctx* ctx, B2Work& W, const B2Args& a, CondArg cond) {
+    const int n = a.n;
+    const int tpr = op_tpr(a.n, a.nnz);
+    const int grid = row_grid(ctx, n, tpr);
+    const int gv = row_grid(ctx, 2LL * n, 1);
+    const int* done = &W.st.p->done;
+    CFA_LAUNCH(ctx, k_b2_p, gv, kThreads, 0, n, W.r.p, W.v.p, W.p.p, W.st.p);
+    CFA_PROPAGATE(ilu_apply(ctx, a.ilu, W.p.p, W.phat.p, 2, done));
+    OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_v<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, W.phat.p, W.r0.p, W.v.p,
+                                  W.st.p, W.part.p, W.counter.p, cond));
+    CFA_LAUNCH(ctx, k_b2_s, gv, kThreads, 0, n, W.r.p, W.v.p, W.s.p, W.st.p);
+    CFA_PROPAGATE(ilu_apply(ctx, a.ilu, W.s.p, W.shat.p, 2, done));
+    OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_t<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, W.shat.p, W.s.p, W.t.p,
+                                  W.st.p, W.part.p, W.counter.p));
+    CFA_LAUNCH(ctx, k_b2_xr, row_grid(ctx, n, 1), kThreads, 0, n, a.xu, a.xv, W.phat.p, W.shat.p, W.s.p, W.t.p, W.r.p,
+               W.r0.p, W.st.p, W.part.p, W.counter.p, cond);
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+static cfa_status b2_solve(cfa_ctx* ctx, const B2Args& a, cfa_solve_report* rep) {
+    B2Work& W = work(ctx)->b2;
+    const int n = a.n;
+    if (n > W.cap) {
+        W.graph.reset();
+        for (DevBuf<double>* b : {&W.r, &W.r0, &W.p, &W.v, &W.s, &W.t, &W.phat, &W.shat}) CFA_CUDA(b->ensure(2 * (size_t)n));
+        CFA_CUDA(W.st.ensure(1));
+        CFA_CUDA(W.counter.ensure(1));
+        CFA_CUDA(cudaMemsetAsync(W.counter.p, 0, sizeof(unsigned int), ctx->stream));
+        W.cap = n;
+    }
+    CFA_CUDA(W.part.ensure(8 * (size_t)row_grid(ctx, 2LL * n, 1) + 64));
+    B2State init{};
+    init.tol = a.tol;
+    init.max_iter = a.max_iter;
+    CFA_CUDA(cudaMemcpyAsync(W.st.p, &init, sizeof(B2State), cudaMemcpyHostToDevice, ctx->stream));
+    CFA_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+    long long extra_body = 0;
+    if (graphs_enabled()) {
+        std::vector<const void*> key = {a.rp, a.ci, a.val, a.bu, a.bv, a.xu, a.xv, a.ilu,
+                                        (const void*)(intptr_t)n, (const void*)(intptr_t)a.nnz};
+        if (!W.graph.exec || W.graph.key != key) {
+            CFA_PROPAGATE(build_graph(ctx, W.graph, [&](CondArg c) { return b2_init(ctx, W, a, c); },
+                                      [&](CondArg c) { return b2_body(ctx, W, a, c); }));
+            W.graph.key = key;
+        }
+        CFA_CUDA(cudaGraphLaunch(W.graph.exec, ctx->stream));
+        extra_body = W.graph.body_kernels;
+        ctx->launches += W.graph.init_kernels;
+    } else {
+        CondArg none{0, 0};
+        CFA_PROPAGATE(b2_init(ctx, W, a, none));
+        int polled = 0;
+        for (int it = 0; it < a.max_iter; ++it) {
+            CFA_PROPAGATE(b2_body(ctx, W, a, none));
+            if (++polled == 4 || it + 1 == a.max_iter) {
+                polled = 0;
+                int d = 0;
+                CFA_CUDA(cudaMemcpyAsync(&d, &W.st.p->done, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+                CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+                if (d) break;
+            }
+        }
+    }
+    CFA_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    B2State h;
+    CFA_CUDA(cudaMemcpyAsync(&h, W.st.p, sizeof(B2State), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    CFA_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->launches += extra_body * (long long)(h.iter + 1);
+    if (rep) {
+        for (int c = 0; c < 2; ++c) {
+            rep->iterations[c] = h.iters[c];
+            rep->converged[c] = h.conv[c];
+            rep->rel_residual[c] = h.rel[c];
+        }
+        rep->solve_ms = ms;
+    }
+    return (h.conv[0] && h.conv[1]) ? CFA_OK : CFA_NOT_CONVERGED;
+}
+
+}  // namespace cfa
+
+using namespace cfa;
+
+extern "C" {
+
+cfa_status cfa_spmv(cfa_ctx* ctx, int n, const int* rp, const int* ci, const double* val, const double* x, double* y) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(n > 0 && rp && ci && val && x && y);
+    const int tpr = 4;
+    CFA_LAUNCH(ctx, (k_spmv<4, 1>), row_grid(ctx, n, tpr), kThreads, 0, n, rp, ci, val, x, y);
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+cfa_status cfa_spmv_multi(cfa_ctx* ctx, int n, int nrhs, const int* rp, const int* ci, const double* val,
+                          const double* x, double* y) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(n > 0 && (nrhs == 1 || nrhs == 2) && rp && ci && val && x && y);
+    if (nrhs == 1) CFA_LAUNCH(ctx, (k_spmv<4, 1>), row_grid(ctx, n, 4), kThreads, 0, n, rp, ci, val, x, y);
+    else CFA_LAUNCH(ctx, (k_spmv<4, 2>), row_grid(ctx, n, 4), kThreads, 0, n, rp, ci, val, x, y);
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+cfa_status cfa_pressure_operator(cfa_ctx* ctx, int n, int nnz, const int* rp, const int* ci, const double* val,
+                                 const cfa_oss_operator* oss, const double* x, double* y) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(n > 0 && nnz > 0 && rp && ci && val && x && y);
+    CFA_ARG(!oss || (oss->mesh && oss->d_oss_val && oss->d_inv_m && oss->mesh->n == n));
+    PcgWork& W = work(ctx)->pcg;
+    if (n > W.cap) {
+        W.graph.reset();
+        for (DevBuf<double>* b : {&W.r, &W.z, &W.p, &W.pn, &W.q, &W.gx, &W.gy, &W.dinv}) CFA_CUDA(b->ensure(n));
+        CFA_CUDA(W.st.ensure(1));
+        CFA_CUDA(W.counter.ensure(1));
+        CFA_CUDA(cudaMemsetAsync(W.counter.p, 0, sizeof(unsigned int), ctx->stream));
+        W.cap = n;
+    }
+    PcgArgs a{n, nnz, rp, ci, val, nullptr, nullptr, oss, nullptr, 0, 0.0};
+    CondArg none{0, 0};
+    CFA_PROPAGATE(pcg_operator(ctx, W, a, x, x, nullptr, W.pn.p, y, false, none, nullptr));
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+cfa_status cfa_oss_apply(cfa_ctx* ctx, const cfa_mesh* m, const double* oss_val, const double* inv_m, const double* in,
+                         double* out) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(m && oss_val && inv_m && in && out);
+    // out -= B^T M^-1 B in: pass 1 into the PCG scratch g, pass 2 with K = 0 contributions
+    PcgWork& W = work(ctx)->pcg;
+    const int n = m->n;
+    if (n > W.cap) {
+        W.graph.reset();
+        for (DevBuf<double>* b : {&W.r, &W.z, &W.p, &W.pn, &W.q, &W.gx, &W.gy, &W.dinv}) CFA_CUDA(b->ensure(n));
+        CFA_CUDA(W.st.ensure(1));
+        CFA_CUDA(W.counter.ensure(1));
+        CFA_CUDA(cudaMemsetAsync(W.counter.p, 0, sizeof(unsigned int), ctx->stream));
+        W.cap = n;
+    }
+    DevBuf<double> zeroK;
+    CFA_CUDA(zeroK.ensure(std::max(m->nnz, 1)));
+    CFA_CUDA(cudaMemsetAsync(zeroK.p, 0, (size_t)m->nnz * sizeof(double), ctx->stream));
+    cfa_oss_operator op{m, oss_val, inv_m};
+    PcgArgs a{n, m->nnz, m->rp, m->ci, zeroK.p, nullptr, nullptr, &op, nullptr, 0, 0.0};
+    CondArg none{0, 0};
+    CFA_PROPAGATE(pcg_operator(ctx, W, a, in, in, nullptr, W.pn.p, W.q.p, false, none, nullptr));
+    // out += q (q = -B^T g on non-Dirichlet rows, 0 elsewhere)
+    CFA_LAUNCH(ctx, k_axpy, row_grid(ctx, n, 1), kThreads, 0, n, 1.0, (const double*)W.q.p, out);
+    CFA_CHECK_LAUNCH();
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    return CFA_OK;
+}
+
+cfa_status cfa_pcg_solve(cfa_ctx* ctx, int n, const int* rp, const int* ci, const double* val, const double* b,
+                         double* x, const cfa_oss_operator* oss, cfa_amg* amg, const cfa_solve_opts* opts,
+                         cfa_solve_report* rep) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(n > 0 && rp && ci && val && b && x && opts && opts->max_iter >= 0);
+    CFA_ARG(!oss || (oss->mesh && oss->d_oss_val && oss->d_inv_m && oss->mesh->n == n));
+    CFA_ARG(!amg || (amg->coarse_n > 0 && (amg->levels.empty() ? amg->coarse_n == n : amg->levels[0].A.rows == n)));
+    int nnz = 0;
+    CFA_CUDA(cudaMemcpyAsync(&nnz, rp + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    PcgArgs a{n, nnz, rp, ci, val, b, x, oss, amg, opts->max_iter, opts->tol};
+    if (opts->max_iter == 0) {
+        if (rep) { *rep = cfa_solve_report{}; rep->converged[0] = 0; rep->converged[1] = 1; }
+        return CFA_NOT_CONVERGED;
+    }
+    return pcg_solve(ctx, a, rep);
+}
+
+cfa_status cfa_bicgstab2_solve(cfa_ctx* ctx, int n, const int* rp, const int* ci, const double* val, const double* bu,
+                               const double* bv, double* xu, double* xv, const cfa_ilu* ilu, const cfa_solve_opts* opts,
+                               cfa_solve_report* rep) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(n > 0 && rp && ci && val && bu && bv && xu && xv && ilu && opts && ilu->n == n && opts->max_iter > 0);
+    B2Args a{n, ilu->nnz, rp, ci, val, bu, bv, xu, xv, ilu, opts->max_iter, opts->tol};
+    return b2_solve(ctx, a, rep);
+}
+
+cfa_status cfa_bicgstab_solve(cfa_ctx* ctx, int n, const int* rp, const int* ci, const double* val, const double* b,
+                              double* x, const cfa_solve_opts* opts, cfa_solve_report* rep) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(n > 0 && rp && ci && val && b && x && opts);
+    DevBuf<double> r, r0, p, v, s, t, phat, shat, dinv, dots;
+    for (DevBuf<double>* buf : {&r, &r0, &p, &v, &s, &t, &phat, &shat, &dinv}) CFA_CUDA(buf->ensure(n));
+    CFA_CUDA(dots.ensure(8));
+    DevBuf<unsigned int> counter;
+    CFA_CUDA(counter.ensure(1));
+    CFA_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned int), ctx->stream));
+    const int gv = row_grid(ctx, n, 1);
+    DevBuf<double> part;
+    CFA_CUDA(part.ensure(gv + 16));
+    auto spmv = [&](const double* in, double* out) {
+        CFA_LAUNCH(ctx, (k_spmv<4, 1>), row_grid(ctx, n, 4), kThreads, 0, n, rp, ci, val, in, out);
+    };
+    auto dot = [&](const double* aa, const double* bb) -> double {
+        CFA_LAUNCH(ctx, k_dot, gv, kThreads, 0, n, aa, bb, dots.p, part.p, counter.p);
+        double h = 0.0;
+        cudaMemcpyAsync(&h, dots.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+        return h;
+    };
+    CFA_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+    CFA_LAUNCH(ctx, k_inv_diag, ceil_div(n, kThreads), kThreads, 0, n, rp, ci, val, dinv.p);
+    spmv(x, v.p);
+    CFA_LAUNCH(ctx, k_axpby, gv, kThreads, 0, n, 1.0, b, -1.0, (const double*)v.p, r.p);
+    CFA_CUDA(cudaMemcpyAsync(r0.p, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(p.p, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CFA_CUDA(cudaMemsetAsync(v.p, 0, n * sizeof(double), ctx->stream));
+    const double r_norm0 = std::sqrt(dot(r.p, r.p));
+    int iter = 0;
+    bool fin = false;
+    double rel = 0.0;
+    if (r_norm0 < 1.0e-13) {
+        fin = true;
+    } else {
+        double rho_old = 1.0, alpha = 1.0, omega = 1.0;
+        const double breakdown = 1.0e-30 * r_norm0 * r_norm0 + 1.0e-300;
+        for (; iter < opts->max_iter; ++iter) {
+            const double rho_new = dot(r0.p, r.p);
+            if (std::fabs(rho_new) < breakdown) break;
+            if (iter > 0) {
+                const double beta = (rho_new / rho_old) * (alpha / (omega + 1.0e-30));
+                CFA_LAUNCH(ctx, k_bicg_p, gv, kThreads, 0, n, (const double*)r.p, (const double*)v.p, beta, omega, p.p);
+            }
+            CFA_LAUNCH(ctx, k_vmul, gv, kThreads, 0, n, (const double*)dinv.p, (const double*)p.p, phat.p);
+            spmv(phat.p, v.p);
+            const double r0v = dot(r0.p, v.p);
+            if (std::fabs(r0v) < breakdown) break;
+            alpha = rho_new / r0v;
+            CFA_LAUNCH(ctx, k_axpby, gv, kThreads, 0, n, 1.0, (const double*)r.p, -alpha, (const double*)v.p, s.p);
+            const double s_norm = std::sqrt(dot(s.p, s.p));
+            if (s_norm < opts->tol * r_norm0 || s_norm < 1.0e-11) {
+                CFA_LAUNCH(ctx, k_axpy, gv, kThreads, 0, n, alpha, (const double*)phat.p, x);
+                ++iter;
+                fin = true;
+                break;
+            }
+            CFA_LAUNCH(ctx, k_vmul, gv, kThreads, 0, n, (const double*)dinv.p, (const double*)s.p, shat.p);
+            spmv(shat.p, t.p);
+            const double tt = dot(t.p, t.p);
+            omega = (tt > breakdown) ? (dot(t.p, s.p) / tt) : 0.0;
+            CFA_LAUNCH(ctx, k_axpy, gv, kThreads, 0, n, alpha, (const double*)phat.p, x);
+            CFA_LAUNCH(ctx, k_axpy, gv, kThreads, 0, n, omega, (const double*)shat.p, x);
+            CFA_LAUNCH(ctx, k_axpby, gv, kThreads, 0, n, 1.0, (const double*)s.p, -omega, (const double*)t.p, r.p);
+            const double r_norm = std::sqrt(dot(r.p, r.p));
+            rel = r_norm / r_norm0;
+            if (r_norm < opts->tol * r_norm0 || r_norm < 1.0e-11) { ++iter; fin = true; break; }
+            rho_old = rho_new;
+        }
+    }
+    CFA_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    CFA_CHECK_LAUNCH();
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    if (rep) {
+        rep->iterations[0] = iter; rep->iterations[1] = 0;
+        rep->converged[0] = fin; rep->converged[1] = 1;
+        rep->rel_residual[0] = rel; rep->rel_residual[1] = 0.0;
+        rep->solve_ms = ms;
+    }
+    return fin ? CFA_OK : CFA_NOT_CONVERGED;
+}
+
+}  // extern "C"

@@ -1,0 +1,103 @@
+"""One time step's solve path through the C ABI, in the order of the reference driver's Steps A
+and B (src/cylinder_fem_amr.cu:300-475):
+
+  A. momentum assembly + BCs (one row pass), ILU(0) factor, two-component BiCGSTAB;
+  B. OSS weights s_K, G(p^n), pressure system (PPE + BCs + OSS operator, one row pass), PCG with
+     the OSS term and SA-AMG.
+
+The AMG hierarchy is built by ``amg_setup()`` (the driver rebuilds it every ``amg_rebuild`` = 50
+steps, src/cfa/options.cuh:26); ``run()`` does one step. Every ``run()`` starts from the same
+state (u* = u^n, dp = 0), so repeated steps do identical work. All device memory is allocated
+here once; ``run()`` allocates nothing.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+import cfa_b200 as cfa
+
+
+class SolveStep:
+    def __init__(self, mesh, u_n, v_n, p_n, precision=cfa.FP64, dt=1e-3, nu=1e-3, rho=1.0, tau_time=1e-3,
+                 stab=0.3, u_max=1.5, H=1.0, tol=1e-10, max_it_mom=1000, max_it_p=4000, ctx=None, dm=None):
+        import torch
+        self.ctx = ctx or cfa.default_context()
+        self.dm = dm or cfa.DeviceMesh(self.ctx, mesh)
+        n, ne, nnz = self.dm.n, self.dm.ne, self.dm.nnz
+        self.n, self.ne, self.nnz = n, ne, nnz
+        dev = "cuda"
+        f64 = dict(dtype=torch.float64, device=dev)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+        self.u_n, self.v_n, self.p_n = t(u_n), t(v_n), t(p_n)
+        self.u_prev, self.v_prev = self.u_n.clone(), self.v_n.clone()
+        self.u, self.v = self.u_n.clone(), self.v_n.clone()      # u*, v* (initial guess u^n)
+        self.A = torch.zeros(nnz, **f64)
+        self.rhs_u, self.rhs_v, self.mass = torch.zeros(n, **f64), torch.zeros(n, **f64), torch.zeros(n, **f64)
+        self.elem_s = torch.zeros(ne, **f64)
+        self.gpx, self.gpy = torch.zeros(n, **f64), torch.zeros(n, **f64)
+        self.Kp = torch.zeros(nnz, **f64)
+        self.rhs_p, self.div, self.dp = torch.zeros(n, **f64), torch.zeros(n, **f64), torch.zeros(n, **f64)
+        self.oss_val = torch.zeros(4 * nnz, **f64)
+        self.inv_m = torch.zeros(n, **f64)
+        self.prm = cfa.bdf2_params(dt, nu, rho, tau_time, 0.5, True)
+        self.dt, self.nu, self.rho, self.stab, self.u_max, self.H = dt, nu, rho, stab, u_max, H
+        self.dt_proj = (2.0 / 3.0) * dt
+        self.tol, self.max_it_mom, self.max_it_p = tol, max_it_mom, max_it_p
+        rp_h, ci_h = self.dm.host_pattern()
+        self.ilu = cfa.MulticolourIlu0(self.ctx, precision)
+        self.ilu.set_pattern(n, rp_h, ci_h, self.dm.rp, self.dm.ci)
+        self.mom = cfa.GpuBicgstab2(self.ctx)
+        self.solver = cfa.GpuLinearSolver(self.ctx)
+        self.amg = cfa.AmgPreconditioner(self.ctx, precision)
+        self.oss = cfa.oss_operator(self.dm, self.oss_val, self.inv_m) if stab > 0.0 else None
+        self.precision = precision
+        self.it_p = 0
+
+    def reset(self):
+        self.u.copy_(self.u_n)
+        self.v.copy_(self.v_n)
+        self.dp.zero_()
+
+    def assemble_momentum(self):
+        c, d = self.ctx, self.dm
+        cfa.assemble_momentum(c, d, self.u_n, self.v_n, self.u_prev, self.v_prev, self.p_n, self.prm, self.A,
+                              self.rhs_u, self.rhs_v, self.mass, self.u, self.v, u_max=self.u_max, H=self.H)
+
+    def solve_momentum(self):
+        self.ilu.factor(self.A)
+        self.mom.solve(self.n, self.dm.rp, self.dm.ci, self.A, self.rhs_u, self.rhs_v, self.u, self.v,
+                       self.max_it_mom, self.tol, self.ilu)
+
+    def assemble_pressure(self):
+        c, d = self.ctx, self.dm
+        if self.stab > 0.0:
+            cfa.oss_weights(c, d, self.u, self.v, self.dt_proj, self.rho, self.nu, self.stab, self.elem_s)
+            cfa.scalar_gradient(c, d, self.p_n, self.elem_s, self.gpx, self.gpy)
+        cfa.assemble_pressure_system(c, d, self.u, self.v, self.p_n, self.gpx, self.gpy, self.mass, self.elem_s,
+                                     self.dt_proj, self.rho, self.stab, self.Kp, self.rhs_p, self.div, self.dp,
+                                     self.oss_val, self.inv_m)
+
+    def solve_pressure(self):
+        self.it_p = self.solver.solve_pcg(self.n, self.dm.rp, self.dm.ci, self.Kp, self.rhs_p, self.dp, self.max_it_p,
+                                          self.tol, self.oss, self.amg)
+
+    def amg_setup(self) -> float:
+        """Assembles the pressure operator of this state and builds the hierarchy; returns ms."""
+        self.reset()
+        self.assemble_momentum()
+        self.solve_momentum()
+        self.assemble_pressure()
+        self.amg.setup(self.n, self.nnz, self.dm.rp, self.dm.ci, self.Kp)
+        return self.amg.setup_ms
+
+    def run(self):
+        self.reset()
+        self.assemble_momentum()
+        self.solve_momentum()
+        self.assemble_pressure()
+        self.solve_pressure()
+
+    def report(self) -> dict:
+        return dict(it_u=self.mom.iters[0], it_v=self.mom.iters[1], it_p=self.it_p,
+                    conv=[bool(self.mom.converged[0]), bool(self.mom.converged[1]), bool(self.solver.converged)],
+                    rel=[self.mom.last_rel_residual[0], self.mom.last_rel_residual[1], self.solver.last_rel_residual])

@@ -1,0 +1,270 @@
+/*
+ * cfa_b200 -- B200 (sm_100a) implementation of the per-timestep solve path of the P1-P1
+ * projection solver: element assembly of the momentum and pressure (PPE + OSS) systems, the
+ * multicolour-ILU(0) two-component BiCGSTAB for momentum and the SA-AMG-preconditioned CG for
+ * the pressure.
+ *
+ * C ABI: plain pointers and sizes. Every pointer named d_* (or documented as device memory) is
+ * device memory owned by the caller, exactly as in the reference driver, which cudaMallocs the
+ * mesh, CSR and solution arrays itself (src/cfa/device.cuh:21-115). Solver handles own their
+ * workspaces. Every call is asynchronous on the context's CUDA stream unless it says it
+ * synchronises; calls returning a report synchronise.
+ *
+ * Layouts are the reference's: int32 CSR (row_ptr[n+1], sorted unique col_ind[nnz], diagonal
+ * present), one value array per matrix, u and v sharing the momentum matrix, the OSS operator as
+ * [Bx | By | BTx | BTy] (4 nnz doubles, src/cfa/fem_kernels.cuh:799-806), multicolour ILU rows in
+ * colour order with split L/U (src/cfa/linalg.cuh:435-447), triangles as 3 ints per element.
+ *
+ * Errors are returned as cfa_status (the reference exits the process instead,
+ * src/cfa/common.cuh:33-41); cfa_ctx_last_error() holds the message.
+ */
+#ifndef CFA_B200_H
+#define CFA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    CFA_OK = 0,
+    CFA_NOT_CONVERGED = 1,  /* solve stopped at max_iter (reference: converged = false)        */
+    CFA_BREAKDOWN = 2,      /* Krylov breakdown guard hit (reference: converged = false)       */
+    CFA_ROW_TOO_LONG = 3,   /* ILU row above 32 entries (reference exits, linalg.cuh:464-467)  */
+    CFA_COARSE_NOT_SPD = 4, /* AMG coarsest operator not SPD (reference exits, :1399-1402)     */
+    CFA_CUDA_ERROR = 5,
+    CFA_TIMEOUT = 6,        /* a bounded device wait gave up                                   */
+    CFA_BAD_ARG = 7,
+    CFA_NO_MEMORY = 8
+} cfa_status;
+
+typedef enum {
+    CFA_FP64 = 0,   /* preconditioner stored and applied in FP64 (the reference)              */
+    CFA_MIXED = 1   /* preconditioner stored and applied in FP32 inside FP64 Krylov iterations */
+} cfa_precision;
+
+typedef struct cfa_ctx cfa_ctx;
+typedef struct cfa_mesh cfa_mesh;
+typedef struct cfa_ilu cfa_ilu;
+typedef struct cfa_amg cfa_amg;
+
+/* ---------------------------------------------------------------------------------------------
+ * context: one per CUDA stream (cudaStream_t passed as void*, NULL = legacy default stream)
+ * ------------------------------------------------------------------------------------------- */
+cfa_status cfa_ctx_create(void* cuda_stream, cfa_ctx** out);
+cfa_status cfa_ctx_destroy(cfa_ctx* ctx);
+const char* cfa_ctx_last_error(const cfa_ctx* ctx);
+const char* cfa_status_string(cfa_status s);
+/* Kernels launched through this context since creation (all of them are this library's). */
+long long cfa_ctx_kernel_launches(const cfa_ctx* ctx);
+/* Synchronises the context's stream. */
+cfa_status cfa_ctx_sync(cfa_ctx* ctx);
+
+/* ---------------------------------------------------------------------------------------------
+ * CSR pattern of the P1 mesh graph: node i's row holds i and the vertices of its elements,
+ * sorted and unique. Replaces build_csr_and_boundary_topology (src/cfa/mesh.cuh:198-249).
+ * cfa_csr_count fills d_row_ptr and returns nnz (synchronises); cfa_csr_fill fills d_col_ind.
+ * ------------------------------------------------------------------------------------------- */
+cfa_status cfa_csr_count(cfa_ctx* ctx, int n_nodes, int n_elems, const int* d_elem_v, int* d_row_ptr,
+                         int* nnz_out);
+cfa_status cfa_csr_fill(cfa_ctx* ctx, int n_nodes, int n_elems, const int* d_elem_v,
+                        const int* d_row_ptr, int* d_col_ind);
+
+/* ---------------------------------------------------------------------------------------------
+ * mesh: the device mesh and pattern of DeviceMeshBuffers (src/cfa/device.cuh:21-59) plus the
+ * assembly plan built from them (node-to-element incidence and CSR scatter positions, which
+ * replace find_csr_index, src/cfa/fem_kernels.cuh:12-28). The arrays stay owned by the caller
+ * and must outlive the handle. Synchronises.
+ * ------------------------------------------------------------------------------------------- */
+cfa_status cfa_mesh_create(cfa_ctx* ctx, int n_nodes, int n_elems, const int* d_elem_v,
+                           const double* d_x, const double* d_y, const int* d_bc_tag,
+                           const int* d_row_ptr, const int* d_col_ind, cfa_mesh** out);
+cfa_status cfa_mesh_destroy(cfa_mesh* mesh);
+/* Outlet condition of src/cfa/common.cuh:76-89 (c_outlet_dirichlet, c_pressure_pin,
+ * c_outlet_scale). Default: p = 0 Dirichlet on BC_OUTLET nodes. */
+cfa_status cfa_mesh_set_outlet(cfa_mesh* mesh, int outlet_dirichlet, int pressure_pin, double outlet_scale);
+
+/* ---------------------------------------------------------------------------------------------
+ * assembly (atomic-free, deterministic: every entry is summed over its elements in ascending
+ * element order). Outputs are overwritten (the reference memsets them and accumulates).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct {
+    double dt, nu, rho;
+    double a0, a1, a2;      /* du/dt ~ a0 u* - (a1 u^n + a2 u^{n-1})           */
+    double c1, c2;          /* advecting velocity w = c1 u^n + c2 u^{n-1}        */
+    double tau_time;        /* SUPG tau time scale T                             */
+    double skew_coef;       /* 0.5 skew-symmetric convection, 0 convective form  */
+} cfa_momentum_params;
+
+typedef struct {
+    double u_max;           /* inflow peak: u = 4 u_max y (H - y) / H^2 on BC_INLET */
+    double H;               /* channel height                                        */
+} cfa_momentum_bc;
+
+/* k_assemble_momentum_fem (src/cfa/fem_kernels.cuh:40-181) with the lumped mass. If bc is not
+ * NULL, k_apply_bc_momentum (:411-453) is applied in the same pass (then d_u, d_v receive the
+ * Dirichlet values; otherwise they are not touched and may be NULL). */
+cfa_status cfa_assemble_momentum(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_u_old,
+                                 const double* d_v_old, const double* d_u_prev, const double* d_v_prev,
+                                 const double* d_p_old, const cfa_momentum_params* prm,
+                                 const cfa_momentum_bc* bc, double* d_A_val, double* d_rhs_u,
+                                 double* d_rhs_v, double* d_mass_lumped, double* d_u, double* d_v);
+/* k_apply_bc_momentum (src/cfa/fem_kernels.cuh:411-453) alone. */
+cfa_status cfa_apply_bc_momentum(cfa_ctx* ctx, const cfa_mesh* mesh, const cfa_momentum_bc* bc,
+                                 double* d_A_val, double* d_rhs_u, double* d_rhs_v, double* d_u,
+                                 double* d_v);
+/* k_assemble_lumped_mass (src/cfa/fem_kernels.cuh:890-909). */
+cfa_status cfa_lumped_mass(cfa_ctx* ctx, const cfa_mesh* mesh, double* d_mass_lumped);
+/* k_compute_oss_weights (src/cfa/fem_kernels.cuh:697-719): s_K per element. */
+cfa_status cfa_oss_weights(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_u_star,
+                           const double* d_v_star, double dt, double rho, double nu, double stab,
+                           double* d_elem_s);
+/* k_accumulate_scalar_gradient (src/cfa/fem_kernels.cuh:726-757): G(f) numerators, weights
+ * sqrt(s_K) (d_elem_s NULL: weight 1). Overwrites d_gx, d_gy. */
+cfa_status cfa_scalar_gradient(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_f,
+                               const double* d_elem_s, double* d_gx, double* d_gy);
+/* k_assemble_pressure_poisson (src/cfa/fem_kernels.cuh:201-282); with apply_bc != 0 also
+ * apply_bc_pressure (:519-531) in the same pass, which then writes d_dp on Dirichlet rows.
+ * With the pinned outlet (cfa_mesh_set_outlet) the RHS mean removal needs apply_bc != 0. */
+cfa_status cfa_assemble_ppe(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_u_star,
+                            const double* d_v_star, const double* d_p_old, const double* d_gp_x,
+                            const double* d_gp_y, const double* d_mass_lumped, const double* d_elem_s,
+                            double dt, double rho, double stab, int apply_bc, double* d_Kp_val,
+                            double* d_rhs_p, double* d_div_num, double* d_dp);
+/* apply_bc_pressure (src/cfa/fem_kernels.cuh:460-531) alone. */
+cfa_status cfa_apply_bc_pressure(cfa_ctx* ctx, const cfa_mesh* mesh, double* d_Kp_val,
+                                 double* d_rhs_p, double* d_dp, const double* d_mass_lumped);
+/* assemble_oss_projection (src/cfa/device.cuh:304-314): B, B^T into d_oss_val (4 nnz) and
+ * 1/max(m, 1e-14) into d_inv_m. */
+cfa_status cfa_assemble_oss(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_elem_s,
+                            const double* d_mass_lumped, double* d_oss_val, double* d_inv_m);
+/* The pressure system of one step in one row pass: k_assemble_pressure_poisson +
+ * apply_bc_pressure + assemble_oss_projection (the driver's sequence at
+ * src/cylinder_fem_amr.cu:412-441). With stab = 0 the OSS outputs are not written. */
+cfa_status cfa_assemble_pressure_system(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_u_star,
+                                        const double* d_v_star, const double* d_p_old,
+                                        const double* d_gp_x, const double* d_gp_y,
+                                        const double* d_mass_lumped, const double* d_elem_s, double dt,
+                                        double rho, double stab, double* d_Kp_val, double* d_rhs_p,
+                                        double* d_div_num, double* d_dp, double* d_oss_val,
+                                        double* d_inv_m);
+/* apply_oss_projection (src/cfa/device.cuh:316-323): d_out -= B^T M^-1 B d_in, Dirichlet rows
+ * untouched. */
+cfa_status cfa_oss_apply(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_oss_val,
+                         const double* d_inv_m, const double* d_in, double* d_out);
+
+/* ---------------------------------------------------------------------------------------------
+ * sparse kernels
+ * ------------------------------------------------------------------------------------------- */
+/* k_spmv_csr (src/cfa/linalg.cuh:8-26): y = A x, FP64. */
+cfa_status cfa_spmv(cfa_ctx* ctx, int n, const int* d_row_ptr, const int* d_col_ind,
+                    const double* d_val, const double* d_x, double* d_y);
+/* k_spmv_csr_multi (src/cfa/linalg.cuh:572-581): nrhs vectors of stride n, A read once. */
+cfa_status cfa_spmv_multi(cfa_ctx* ctx, int n, int nrhs, const int* d_row_ptr, const int* d_col_ind,
+                          const double* d_val, const double* d_x, double* d_y);
+
+/* ---------------------------------------------------------------------------------------------
+ * multicolour ILU(0): MulticolourIlu0 (src/cfa/linalg.cuh:435-568)
+ * ------------------------------------------------------------------------------------------- */
+/* set_pattern (:456-528): greedy colouring in node order (bit-exact with the reference) from the
+ * host copy of the pattern; d_row_ptr/d_col_ind are the same pattern on the device and must
+ * outlive the handle. Synchronises. CFA_ROW_TOO_LONG above 32 entries per row. */
+cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* h_row_ptr, const int* h_col_ind,
+                          const int* d_row_ptr, const int* d_col_ind, cfa_precision precision,
+                          cfa_ilu** out);
+cfa_status cfa_ilu_destroy(cfa_ilu* ilu);
+/* factor (:531-541): ILU(0) of d_val in colour order, in FP64; the split factors are then kept in
+ * the handle's precision. */
+cfa_status cfa_ilu_factor(cfa_ctx* ctx, cfa_ilu* ilu, const double* d_val);
+/* apply (:544-555): z = (LU)^-1 r for nrhs vectors of stride n. */
+cfa_status cfa_ilu_apply(cfa_ctx* ctx, const cfa_ilu* ilu, const double* d_r, double* d_z, int nrhs);
+/* n_colours and colour_start (host, n_colours + 1 entries, may be NULL). */
+cfa_status cfa_ilu_colours(const cfa_ilu* ilu, int* n_colours, int* colour_start);
+/* Device arrays of the handle (public members d_colour, d_rows, d_lu of the reference class):
+ * colour[n], rows[n] (colour order), lu[nnz] (FP64 factor on the CSR pattern). */
+cfa_status cfa_ilu_device_arrays(const cfa_ilu* ilu, const int** d_colour, const int** d_rows,
+                                 const double** d_lu);
+
+/* ---------------------------------------------------------------------------------------------
+ * solvers
+ * ------------------------------------------------------------------------------------------- */
+typedef struct {
+    int max_iter;
+    double tol;             /* relative tolerance, the reference's stopping rules */
+} cfa_solve_opts;
+
+typedef struct {
+    int iterations[2];      /* [0] = the (u) system, [1] = v for the two-component solve */
+    int converged[2];
+    double rel_residual[2]; /* the reference's last_rel_residual */
+    double solve_ms;        /* device time of the solve (CUDA events) */
+} cfa_solve_report;
+
+/* Two-component BiCGSTAB, right MC-ILU(0): GpuBicgstab2::solve (src/cfa/linalg.cuh:656-754).
+ * Per-component stop |r| < tol |r0| or |r| < 1e-11, breakdown 1e-30 r0^2 + 1e-300. x_u, x_v are
+ * the initial guesses and receive the solutions. Synchronises (report). Returns CFA_OK when both
+ * components converged, else CFA_NOT_CONVERGED (details in the report). */
+cfa_status cfa_bicgstab2_solve(cfa_ctx* ctx, int n, const int* d_row_ptr, const int* d_col_ind,
+                               const double* d_val, const double* d_b_u, const double* d_b_v,
+                               double* d_x_u, double* d_x_v, const cfa_ilu* ilu,
+                               const cfa_solve_opts* opts, cfa_solve_report* report);
+/* Jacobi BiCGSTAB: GpuLinearSolver::solve_bicgstab (src/cfa/linalg.cuh:261-347). */
+cfa_status cfa_bicgstab_solve(cfa_ctx* ctx, int n, const int* d_row_ptr, const int* d_col_ind,
+                              const double* d_val, const double* d_b, double* d_x,
+                              const cfa_solve_opts* opts, cfa_solve_report* report);
+
+/* SA-AMG: AmgPreconditioner (src/cfa/linalg.cuh:939-1432) */
+typedef struct {
+    double theta;           /* strength threshold (0.08)          */
+    int smooth_steps;       /* Jacobi sweeps per side (2)         */
+    int coarse_target;      /* dense solve below this size (300)  */
+    int max_levels;         /* (15)                               */
+    cfa_precision precision;
+} cfa_amg_opts;
+void cfa_amg_default_opts(cfa_amg_opts* opts);
+cfa_status cfa_amg_create(cfa_ctx* ctx, const cfa_amg_opts* opts, cfa_amg** out);
+cfa_status cfa_amg_destroy(cfa_amg* amg);
+/* setup (:995-1060): hierarchy of the device matrix; FP64 setup arithmetic in the reference's
+ * order (aggregates, P, R and Galerkin operators bit-exact with the reference's host setup).
+ * Synchronises. CFA_COARSE_NOT_SPD if the coarsest operator is not SPD. */
+cfa_status cfa_amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* d_row_ptr,
+                         const int* d_col_ind, const double* d_val);
+/* apply (:1161-1168): one symmetric V-cycle, z = M^-1 r. */
+cfa_status cfa_amg_apply(cfa_ctx* ctx, cfa_amg* amg, const double* d_r, double* d_z);
+/* num_levels() (reference: levels with P + the coarsest), coarse_n, setup time [ms] */
+cfa_status cfa_amg_info(const cfa_amg* amg, int* num_levels, int* coarse_n, double* setup_ms);
+/* Level l (0 <= l < num_levels - 1): info = {rows, A nnz, P cols, P nnz, R nnz}; FP64 device
+ * arrays of A, P, R (any pointer argument may be NULL), the aggregate of every row, omega. */
+cfa_status cfa_amg_level(const cfa_amg* amg, int l, int* info, const int** d_agg,
+                         const int** d_A_rp, const int** d_A_ci, const double** d_A_v,
+                         const int** d_P_rp, const int** d_P_ci, const double** d_P_v,
+                         const int** d_R_rp, const int** d_R_ci, const double** d_R_v, double* omega);
+/* dense inverse of the coarsest operator (device, coarse_n^2 FP64, row-major) */
+cfa_status cfa_amg_coarse_inverse(const cfa_amg* amg, const double** d_inv);
+
+/* The assembled OSS term of the pressure operator (apply_oss_projection,
+ * src/cfa/device.cuh:316-323): A x = K x - B^T M^-1 B x on non-Dirichlet rows. */
+typedef struct {
+    const cfa_mesh* mesh;   /* boundary tags and outlet rule */
+    const double* d_oss_val;
+    const double* d_inv_m;
+} cfa_oss_operator;
+
+/* PCG: GpuLinearSolver::solve_pcg (src/cfa/linalg.cuh:183-256). The OSS term and the AMG are
+ * handles instead of std::function callbacks (oss / amg NULL: plain CSR operator / Jacobi).
+ * Warm start from d_x; stop when |r| < tol |b|; x = 0 and 0 iterations when |b| < 1e-14.
+ * Synchronises (report). CFA_NOT_CONVERGED / CFA_BREAKDOWN as the reference's converged flag. */
+cfa_status cfa_pcg_solve(cfa_ctx* ctx, int n, const int* d_row_ptr, const int* d_col_ind,
+                         const double* d_val, const double* d_b, double* d_x,
+                         const cfa_oss_operator* oss, cfa_amg* amg, const cfa_solve_opts* opts,
+                         cfa_solve_report* report);
+
+/* The pressure operator alone (operator of cfa_pcg_solve): y = K x (- B^T M^-1 B x).
+ * Asynchronous (nnz passed by the caller). */
+cfa_status cfa_pressure_operator(cfa_ctx* ctx, int n, int nnz, const int* d_row_ptr,
+                                 const int* d_col_ind, const double* d_val,
+                                 const cfa_oss_operator* oss, const double* d_x, double* d_y);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

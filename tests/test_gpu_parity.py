@@ -1,0 +1,556 @@
+"""Parity of the CUDA path (called through the C ABI) with the oracle and with the reference.
+
+Bars (the reference's own): bit-exact CSR patterns, colourings and AMG hierarchies (aggregates,
+P, R, Galerkin operators, omega, coarse inverse); assembled values within 1e-12 per row; ILU
+factors within 1e-12; solutions to the solver tolerance (tol 1e-10: 1e-8 relative); mixed
+precision solves reach the same 1e-10 residual and match the FP64 solution to 1e-7.
+"""
+import numpy as np
+import pytest
+
+import fixtures as F
+from oracle import oracle as O
+from tests.conftest import MeshFromGolden, golden
+from tests.test_oracle import rows_rel_err
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+import cfa_b200 as cfa  # noqa: E402
+
+MESHES = {}
+
+
+def mesh(name):
+    if name not in MESHES:
+        MESHES[name] = F.make_mesh(name)
+    return MESHES[name]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return cfa.default_context()
+
+
+def dev(a, dtype=torch.float64):
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dtype)
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def fields(m):
+    return (F.fourier_field(m.x, m.y, 1), F.fourier_field(m.x, m.y, 2), 0.3 * F.fourier_field(m.x, m.y, 3))
+
+
+# ------------------------------------------------------------------------------------------------
+# a1: CSR pattern
+# ------------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("name", ["tiny", "small", "medium"])
+def test_csr_build_bit_exact(ctx, name):
+    m = mesh(name)
+    rp, ci = cfa.csr_build(ctx, m.n, dev(m.elem_v, torch.int32))
+    orp, oci = O.csr_build(m.n, m.elem_v)
+    assert np.array_equal(host(rp), orp) and np.array_equal(host(ci), oci)
+
+
+def test_csr_build_matches_reference_golden(ctx):
+    g = golden("ref_host_small.npz")
+    m = MeshFromGolden(g)
+    rp, ci = cfa.csr_build(ctx, m.n, dev(m.elem_v, torch.int32))
+    assert np.array_equal(host(rp), g["rp"]) and np.array_equal(host(ci), g["ci"])
+
+
+# ------------------------------------------------------------------------------------------------
+# a3-a9: assembly
+# ------------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("name", ["small", "medium"])
+def test_assembly_matches_oracle(ctx, name):
+    m = mesh(name)
+    dm = cfa.DeviceMesh(ctx, m)
+    rp, ci = dm.host_pattern()
+    n, ne, nnz = m.n, m.ne, dm.nnz
+    u, v, p = fields(m)
+    prm_o, prm = O.bdf2_params(), cfa.bdf2_params()
+    # momentum + BCs
+    A, ru, rv, mass = O.assemble_momentum(m, rp, ci, u, v, u, v, p, prm_o)
+    uu, vv = u.copy(), v.copy()
+    O.apply_bc_momentum(m, rp, ci, A, ru, rv, uu, vv)
+    dA, dru, drv, dmass = (torch.zeros(k, dtype=torch.float64, device="cuda") for k in (nnz, n, n, n))
+    du, dv = dev(u), dev(v)
+    du_old, dv_old, dp_old = dev(u), dev(v), dev(p)
+    cfa.assemble_momentum(ctx, dm, du_old, dv_old, du_old, dv_old, dp_old, prm, dA, dru, drv, dmass, du, dv,
+                          u_max=1.5, H=1.0)
+    assert rows_rel_err(host(dA), A, rp) < 1e-12
+    for got, want in ((dru, ru), (drv, rv), (dmass, mass), (du, uu), (dv, vv)):
+        assert np.abs(host(got) - want).max() <= 1e-12 * max(np.abs(want).max(), 1e-300)
+    # lumped mass kernel (|det|/6 form)
+    dm2 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    cfa.lumped_mass(ctx, dm, dm2)
+    assert np.abs(host(dm2) - O.lumped_mass(m)).max() <= 1e-12 * mass.max()
+    # PPE + OSS with BCs, the driver's Step B
+    dt_proj = 2e-3 / 3
+    s = O.oss_weights(m, uu, vv, dt_proj, 1.0, 1e-3, 0.3)
+    ds = torch.zeros(ne, dtype=torch.float64, device="cuda")
+    cfa.oss_weights(ctx, dm, du, dv, dt_proj, 1.0, 1e-3, 0.3, ds)
+    assert np.abs(host(ds) - s).max() <= 1e-12 * np.abs(s).max()
+    gx, gy = O.scalar_gradient(m, p, s)
+    dgx, dgy = torch.zeros(n, dtype=torch.float64, device="cuda"), torch.zeros(n, dtype=torch.float64, device="cuda")
+    cfa.scalar_gradient(ctx, dm, dp_old, ds, dgx, dgy)
+    assert np.abs(host(dgx) - gx).max() <= 1e-12 * np.abs(gx).max()
+    assert np.abs(host(dgy) - gy).max() <= 1e-12 * np.abs(gy).max()
+    Kp, rhs, div = O.assemble_ppe(m, rp, ci, uu, vv, p, gx, gy, mass, s, dt_proj, 1.0, 0.3)
+    dp0 = np.ones(n)
+    O.apply_bc_pressure(m, rp, ci, Kp, rhs, dp0, mass)
+    oss, inv_m = O.assemble_oss(m, rp, ci, s, mass)
+    dKp, drhs, ddiv = torch.zeros(nnz, dtype=torch.float64, device="cuda"), torch.zeros(n, dtype=torch.float64, device="cuda"), torch.zeros(n, dtype=torch.float64, device="cuda")
+    ddp = torch.ones(n, dtype=torch.float64, device="cuda")
+    doss, dinv = torch.zeros(4 * nnz, dtype=torch.float64, device="cuda"), torch.zeros(n, dtype=torch.float64, device="cuda")
+    cfa.assemble_pressure_system(ctx, dm, du, dv, dp_old, dgx, dgy, dmass, ds, dt_proj, 1.0, 0.3, dKp, drhs, ddiv, ddp,
+                                 doss, dinv)
+    assert rows_rel_err(host(dKp), Kp, rp) < 1e-12
+    assert np.abs(host(drhs) - rhs).max() <= 1e-12 * np.abs(rhs).max()
+    assert np.abs(host(ddiv) - div).max() <= 1e-12 * np.abs(div).max()
+    assert np.array_equal(host(ddp), dp0)
+    hoss = host(doss)
+    for q in range(4):
+        assert rows_rel_err(hoss[q * nnz:(q + 1) * nnz], oss[q * nnz:(q + 1) * nnz], rp) < 1e-11
+    assert np.abs(host(dinv) - inv_m).max() <= 1e-12 * inv_m.max()
+    # the separate drop-in entry points give the same pressure system
+    dKp2, drhs2, ddiv2 = torch.zeros_like(dKp), torch.zeros_like(drhs), torch.zeros_like(ddiv)
+    ddp2 = torch.ones(n, dtype=torch.float64, device="cuda")
+    cfa.assemble_ppe(ctx, dm, du, dv, dp_old, dgx, dgy, dmass, ds, dt_proj, 1.0, 0.3, dKp2, drhs2, ddiv2, ddp2)
+    doss2, dinv2 = torch.zeros_like(doss), torch.zeros_like(dinv)
+    cfa.assemble_oss(ctx, dm, ds, dmass, doss2, dinv2)
+    assert torch.equal(dKp2, dKp) and torch.equal(drhs2, drhs) and torch.equal(doss2, doss)
+    # OSS apply (a8) against the oracle
+    xin = np.random.default_rng(3).uniform(-0.5, 0.5, n)
+    out = np.zeros(n)
+    O.oss_apply(m, rp, ci, oss, inv_m, xin, out)
+    dout = torch.zeros(n, dtype=torch.float64, device="cuda")
+    cfa.oss_apply(ctx, dm, doss, dinv, dev(xin), dout)
+    assert np.abs(host(dout) - out).max() <= 1e-12 * np.abs(out).max()
+
+
+def test_assembly_deterministic(ctx):
+    m = mesh("medium")
+    dm = cfa.DeviceMesh(ctx, m)
+    u, v, p = fields(m)
+    outs = []
+    for _ in range(2):
+        dA = torch.zeros(dm.nnz, dtype=torch.float64, device="cuda")
+        bufs = [torch.zeros(m.n, dtype=torch.float64, device="cuda") for _ in range(3)]
+        cfa.assemble_momentum(ctx, dm, dev(u), dev(v), dev(u), dev(v), dev(p), cfa.bdf2_params(), dA, *bufs,
+                              dev(u), dev(v), u_max=1.5)
+        outs.append(host(dA))
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_assembly_matches_reference_golden(ctx):
+    """The reference's GPU assembly of one step (FP64 atomics) against ours: 1e-12 per row."""
+    g = golden("ref_gpu_small.npz")
+    h = golden("ref_host_small.npz")
+    m = MeshFromGolden(h)
+    dm = cfa.DeviceMesh(ctx, m, dev(h["rp"], torch.int32), dev(h["ci"], torch.int32))
+    rp = h["rp"]
+    n, nnz = m.n, rp[-1]
+    u, v, p = h["u"], h["v"], h["p"]
+    dA, dru, drv, dmass = (torch.zeros(k, dtype=torch.float64, device="cuda") for k in (nnz, n, n, n))
+    cfa.assemble_momentum(ctx, dm, dev(u), dev(v), dev(u), dev(v), dev(p), cfa.bdf2_params(), dA, dru, drv, dmass,
+                          dev(u), dev(v), u_max=1.5)
+    assert rows_rel_err(host(dA), g["step_A_val"], rp) < 1e-12
+    assert np.abs(host(dru) - g["step_rhs_u"]).max() <= 1e-12 * np.abs(g["step_rhs_u"]).max()
+    us, vs = dev(g["step_u"]), dev(g["step_v"])
+    dt_proj = 2e-3 / 3
+    ds = torch.zeros(m.ne, dtype=torch.float64, device="cuda")
+    cfa.oss_weights(ctx, dm, us, vs, dt_proj, 1.0, 1e-3, 0.3, ds)
+    dgx, dgy = torch.zeros(n, dtype=torch.float64, device="cuda"), torch.zeros(n, dtype=torch.float64, device="cuda")
+    cfa.scalar_gradient(ctx, dm, dev(p), ds, dgx, dgy)
+    dKp, drhs, ddiv, ddp = (torch.zeros(k, dtype=torch.float64, device="cuda") for k in (nnz, n, n, n))
+    doss, dinv = torch.zeros(4 * nnz, dtype=torch.float64, device="cuda"), torch.zeros(n, dtype=torch.float64, device="cuda")
+    cfa.assemble_pressure_system(ctx, dm, us, vs, dev(p), dgx, dgy, dmass, ds, dt_proj, 1.0, 0.3, dKp, drhs, ddiv, ddp,
+                                 doss, dinv)
+    assert rows_rel_err(host(dKp), g["step_Kp_val"], rp) < 1e-12
+    assert np.abs(host(drhs) - g["step_rhs_p"]).max() <= 1e-12 * np.abs(g["step_rhs_p"]).max()
+    hoss = host(doss)
+    for q in range(4):
+        assert rows_rel_err(hoss[q * nnz:(q + 1) * nnz], g["step_oss_val"][q * nnz:(q + 1) * nnz], rp) < 1e-11
+
+
+# ------------------------------------------------------------------------------------------------
+# a15-a17: multicolour ILU(0)
+# ------------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
+def test_ilu_colouring_factor_apply(ctx, precision):
+    from tests.golden.make_golden import momentum_ilu_matrix
+    m = mesh("small")
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    n = m.n
+    a, b = momentum_ilu_matrix(rp, ci)
+    oi = O.Ilu(rp, ci)
+    lu, _, _, _ = oi.factor(a)
+    drp, dci = dev(rp, torch.int32), dev(ci, torch.int32)
+    ilu = cfa.MulticolourIlu0(ctx, precision)
+    ilu.set_pattern(n, rp, ci, drp, dci)
+    assert ilu.n_colours == oi.nc and np.array_equal(ilu.colour_start, oi.colour_start)
+    ilu.factor(dev(a))
+    col, rows, dlu = ilu.device_arrays(ci.size)
+    assert np.array_equal(host(col), oi.colour) and np.array_equal(host(rows), oi.rows)
+    assert rows_rel_err(host(dlu), lu, rp) < 1e-12
+    z = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
+    ilu.apply(dev(b), z, nrhs=2)
+    zo = oi.apply(b, nrhs=2)
+    tol = 1e-12 if precision == cfa.FP64 else 1e-5
+    assert np.abs(host(z) - zo).max() <= tol * np.abs(zo).max()
+
+
+def test_ilu_row_too_long_is_an_error(ctx):
+    n = 40
+    rp = np.array([0, n] + list(range(n + 1, 2 * n)), np.int32)   # row 0 full, others diagonal
+    ci = np.array(list(range(n)) + list(range(1, n)), np.int32)
+    ilu = cfa.MulticolourIlu0(ctx)
+    with pytest.raises(cfa.CfaError) as e:
+        ilu.set_pattern(n, rp, ci, dev(rp, torch.int32), dev(ci, torch.int32))
+    assert e.value.status == cfa.CFA_ROW_TOO_LONG
+
+
+# ------------------------------------------------------------------------------------------------
+# a18-a21: two-component BiCGSTAB
+# ------------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
+def test_bicgstab2_matches_oracle(ctx, precision):
+    from tests.golden.make_golden import momentum_ilu_matrix
+    m = mesh("small")
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    n = m.n
+    a, b = momentum_ilu_matrix(rp, ci)
+    oi = O.Ilu(rp, ci)
+    oi.factor(a)
+    xu, xv, reps = O.bicgstab2(rp, ci, a, b[:n], b[n:], np.zeros(n), np.zeros(n), oi, 200, 1e-10)
+    drp, dci = dev(rp, torch.int32), dev(ci, torch.int32)
+    ilu = cfa.MulticolourIlu0(ctx, precision)
+    ilu.set_pattern(n, rp, ci, drp, dci)
+    da = dev(a)
+    ilu.factor(da)
+    s = cfa.GpuBicgstab2(ctx)
+    du, dv = torch.zeros(n, dtype=torch.float64, device="cuda"), torch.zeros(n, dtype=torch.float64, device="cuda")
+    db = dev(b)
+    s.solve(n, drp, dci, da, db[:n], db[n:], du, dv, 200, 1e-10, ilu)
+    assert s.converged == [True, True]
+    x = np.concatenate([host(du), host(dv)])
+    xo = np.concatenate([xu, xv])
+    assert np.abs(x - xo).max() < 1e-8 * np.abs(xo).max()
+    if precision == cfa.FP64:
+        assert abs(s.iters[0] - reps[0].iterations) <= 1 and abs(s.iters[1] - reps[1].iterations) <= 1
+    # true residual of each component
+    for comp, xx, bb in ((0, host(du), b[:n]), (1, host(dv), b[n:])):
+        r = bb - O.spmv(rp, ci, a, xx)
+        assert np.linalg.norm(r) <= 1.5e-10 * np.linalg.norm(bb) or np.linalg.norm(r) < 1e-11
+
+
+def test_bicgstab2_not_converged_status(ctx):
+    from tests.golden.make_golden import momentum_ilu_matrix
+    m = mesh("small")
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    n = m.n
+    a, b = momentum_ilu_matrix(rp, ci)
+    drp, dci, da, db = dev(rp, torch.int32), dev(ci, torch.int32), dev(a), dev(b)
+    ilu = cfa.MulticolourIlu0(ctx)
+    ilu.set_pattern(n, rp, ci, drp, dci)
+    ilu.factor(da)
+    s = cfa.GpuBicgstab2(ctx)
+    du, dv = torch.zeros(n, dtype=torch.float64, device="cuda"), torch.zeros(n, dtype=torch.float64, device="cuda")
+    s.solve(n, drp, dci, da, db[:n], db[n:], du, dv, 2, 1e-14, ilu)
+    assert s.converged == [False, False] and s.iters == [2, 2]
+
+
+def test_bicgstab_jacobi_matches_oracle(ctx):
+    from tests.golden.make_golden import momentum_ilu_matrix
+    m = mesh("small")
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    n = m.n
+    a, b = momentum_ilu_matrix(rp, ci)
+    xo, rep = O.bicgstab(rp, ci, a, b[:n], np.zeros(n), 400, 1e-10)
+    s = cfa.GpuLinearSolver(ctx)
+    dx = torch.zeros(n, dtype=torch.float64, device="cuda")
+    it = s.solve_bicgstab(n, dev(rp, torch.int32), dev(ci, torch.int32), dev(a), dev(b[:n]), dx, 400, 1e-10)
+    assert s.converged and abs(it - rep.iterations) <= 1
+    assert np.abs(host(dx) - xo).max() < 1e-8 * np.abs(xo).max()
+
+
+# ------------------------------------------------------------------------------------------------
+# a22-a25: SA-AMG
+# ------------------------------------------------------------------------------------------------
+def laplacian(rp, ci):
+    from tests.golden.make_golden import shifted_laplacian
+    return shifted_laplacian(rp, ci)
+
+
+def check_hierarchy(amg, oa):
+    assert amg.num_levels() == oa.nlev + 1
+    assert amg.coarse_n == oa.coarse_n
+    for l in range(oa.nlev):
+        L, OL = amg.level(l), oa.level(l)
+        assert L["omega"] == OL["omega"]
+        assert np.array_equal(host(L["agg"]), OL["agg"])
+        for name in ("A", "P", "R"):
+            rp_, ci_, v_ = (host(t) for t in L[name])
+            _, _, orp, oci, ov = OL[name]
+            assert np.array_equal(rp_, orp), (l, name)
+            assert np.array_equal(ci_, oci), (l, name)
+            assert np.array_equal(v_, ov), (l, name)
+    _, inv = oa.coarse()
+    assert np.array_equal(host(amg.coarse_inverse()), inv)
+
+
+@pytest.mark.parametrize("name,which", [("small", "lap"), ("medium", "lap"), ("medium", "ppe")])
+def test_amg_setup_bit_exact(ctx, name, which):
+    m = mesh(name)
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    if which == "lap":
+        a = laplacian(rp, ci)
+    else:
+        from tests.golden.make_golden import oracle_pressure_matrix
+        u, v, p = fields(m)
+        a = oracle_pressure_matrix(m, rp, ci, u, v, p)
+    oa = O.Amg(rp, ci, a)
+    amg = cfa.AmgPreconditioner(ctx)
+    amg.setup(m.n, ci.size, dev(rp, torch.int32), dev(ci, torch.int32), dev(a))
+    check_hierarchy(amg, oa)
+    # V-cycle against the oracle's
+    r = np.sin(0.37 * np.arange(m.n)) + 0.2
+    z = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+    amg.apply(dev(r), z)
+    zo = oa.apply(r)
+    assert np.abs(host(z) - zo).max() <= 1e-12 * np.abs(zo).max()
+    # mixed precision V-cycle: same hierarchy in FP32
+    amg32 = cfa.AmgPreconditioner(ctx, cfa.MIXED)
+    amg32.setup(m.n, ci.size, dev(rp, torch.int32), dev(ci, torch.int32), dev(a))
+    z32 = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+    amg32.apply(dev(r), z32)
+    assert np.abs(host(z32) - zo).max() <= 1e-4 * np.abs(zo).max()
+
+
+def test_amg_matches_reference_golden(ctx):
+    for name in ("tiny", "small"):
+        g = golden(f"ref_host_{name}.npz")
+        rp, ci = g["rp"], g["ci"]
+        for which in ("ppe", "lap"):
+            amg = cfa.AmgPreconditioner(ctx)
+            amg.setup(rp.size - 1, ci.size, dev(rp, torch.int32), dev(ci, torch.int32), dev(g[f"{which}_val"]))
+            assert amg.num_levels() == int(g[f"{which}_levels"][0]) + 1
+            for l in range(int(g[f"{which}_levels"][0])):
+                L = amg.level(l)
+                assert L["omega"] == g[f"{which}_L{l}_omega"][0]
+                for nm in ("A", "P", "R"):
+                    for part, t in zip(("rp", "ci", "v"), L[nm]):
+                        assert np.array_equal(host(t), g[f"{which}_L{l}_{nm}_{part}"]), (name, which, l, nm, part)
+            assert np.array_equal(host(amg.coarse_inverse()).ravel(), g[f"{which}_coarse_inv"])
+
+
+def test_amg_vcycle_matches_reference_gpu_golden(ctx):
+    g = golden("ref_gpu_small.npz")
+    h = golden("ref_host_small.npz")
+    rp, ci = h["rp"], h["ci"]
+    n = rp.size - 1
+    amg = cfa.AmgPreconditioner(ctx)
+    amg.setup(n, ci.size, dev(rp, torch.int32), dev(ci, torch.int32), dev(h["lap_val"]))
+    z = torch.zeros(n, dtype=torch.float64, device="cuda")
+    amg.apply(dev(np.sin(0.37 * np.arange(n)) + 0.2), z)
+    # same hierarchy, same row sums and shuffle tree as the reference's kernels
+    assert np.abs(host(z) - g["lap_vcycle_z"]).max() <= 1e-14 * np.abs(g["lap_vcycle_z"]).max()
+
+
+def test_amg_coarse_not_spd_is_an_error(ctx):
+    m = mesh("tiny")
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    a = -laplacian(rp, ci)            # negative definite: the coarse Cholesky must fail
+    amg = cfa.AmgPreconditioner(ctx)
+    with pytest.raises(cfa.CfaError) as e:
+        amg.setup(m.n, ci.size, dev(rp, torch.int32), dev(ci, torch.int32), dev(a))
+    assert e.value.status == cfa.CFA_COARSE_NOT_SPD
+
+
+# ------------------------------------------------------------------------------------------------
+# a10-a13: PCG (+ OSS + AMG)
+# ------------------------------------------------------------------------------------------------
+def pressure_system(m, rp, ci):
+    u, v, p = fields(m)
+    A, ru, rv, mass = O.assemble_momentum(m, rp, ci, u, v, u, v, p, O.bdf2_params())
+    dt_proj = 2e-3 / 3
+    s = O.oss_weights(m, u, v, dt_proj, 1.0, 1e-3, 0.3)
+    gx, gy = O.scalar_gradient(m, p, s)
+    Kp, rhs, div = O.assemble_ppe(m, rp, ci, u, v, p, gx, gy, mass, s, dt_proj, 1.0, 0.3)
+    dp = np.zeros(m.n)
+    O.apply_bc_pressure(m, rp, ci, Kp, rhs, dp, mass)
+    oss, inv_m = O.assemble_oss(m, rp, ci, s, mass)
+    return Kp, rhs, oss, inv_m
+
+
+@pytest.mark.parametrize("use_oss,use_amg", [(True, True), (False, True), (True, False), (False, False)])
+def test_pcg_matches_oracle(ctx, use_oss, use_amg):
+    m = mesh("small")
+    dm = cfa.DeviceMesh(ctx, m)
+    rp, ci = dm.host_pattern()
+    Kp, rhs, oss, inv_m = pressure_system(m, rp, ci)
+    oa = O.Amg(rp, ci, Kp) if use_amg else None
+    xo, rep = O.pcg(rp, ci, Kp, rhs, np.zeros(m.n), 4000, 1e-10, oss if use_oss else None,
+                    inv_m if use_oss else None, m.tag, oa)
+    dK, db, doss, dinv = dev(Kp), dev(rhs), dev(oss), dev(inv_m)
+    amg = None
+    if use_amg:
+        amg = cfa.AmgPreconditioner(ctx)
+        amg.setup(m.n, ci.size, dm.rp, dm.ci, dK)
+    s = cfa.GpuLinearSolver(ctx)
+    dx = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+    it = s.solve_pcg(m.n, dm.rp, dm.ci, dK, db, dx, 4000, 1e-10, cfa.oss_operator(dm, doss, dinv) if use_oss else None,
+                     amg)
+    assert s.converged and rep.converged
+    assert abs(it - rep.iterations) <= max(2, rep.iterations // 50)
+    assert np.abs(host(dx) - xo).max() < 1e-8 * np.abs(xo).max()
+    # true residual with the oracle operator
+    x = host(dx)
+    Ax = O.spmv(rp, ci, Kp, x)
+    if use_oss:
+        O.oss_apply(m, rp, ci, oss, inv_m, x, Ax)
+    assert np.linalg.norm(rhs - Ax) <= 1.5e-10 * np.linalg.norm(rhs)
+
+
+def test_pcg_mixed_precision_reaches_tolerance(ctx):
+    m = mesh("medium")
+    dm = cfa.DeviceMesh(ctx, m)
+    rp, ci = dm.host_pattern()
+    Kp, rhs, oss, inv_m = pressure_system(m, rp, ci)
+    dK, db, doss, dinv = dev(Kp), dev(rhs), dev(oss), dev(inv_m)
+    op = cfa.oss_operator(dm, doss, dinv)
+    res = {}
+    for prec in (cfa.FP64, cfa.MIXED):
+        amg = cfa.AmgPreconditioner(ctx, prec)
+        amg.setup(m.n, ci.size, dm.rp, dm.ci, dK)
+        s = cfa.GpuLinearSolver(ctx)
+        dx = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+        it = s.solve_pcg(m.n, dm.rp, dm.ci, dK, db, dx, 4000, 1e-10, op, amg)
+        assert s.converged
+        x = host(dx)
+        Ax = O.spmv(rp, ci, Kp, x)
+        O.oss_apply(m, rp, ci, oss, inv_m, x, Ax)
+        assert np.linalg.norm(rhs - Ax) <= 1.5e-10 * np.linalg.norm(rhs)
+        res[prec] = (it, x)
+    assert np.abs(res[cfa.MIXED][1] - res[cfa.FP64][1]).max() < 1e-7 * np.abs(res[cfa.FP64][1]).max()
+    assert res[cfa.MIXED][0] <= res[cfa.FP64][0] + 3
+
+
+def test_pcg_zero_rhs_and_breakdown(ctx):
+    m = mesh("tiny")
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    a = laplacian(rp, ci)
+    s = cfa.GpuLinearSolver(ctx)
+    drp, dci, da = dev(rp, torch.int32), dev(ci, torch.int32), dev(a)
+    dx = torch.ones(m.n, dtype=torch.float64, device="cuda")
+    it = s.solve_pcg(m.n, drp, dci, da, torch.zeros(m.n, dtype=torch.float64, device="cuda"), dx, 100, 1e-10)
+    assert it == 0 and s.converged and float(dx.abs().max()) == 0.0     # reference: x = 0 for |b| < 1e-14
+    # zero operator: p.q = 0 -> breakdown guard, not converged
+    dx.zero_()
+    it = s.solve_pcg(m.n, drp, dci, torch.zeros_like(da), dev(np.ones(m.n)), dx, 100, 1e-10)
+    assert not s.converged and it == 0
+
+
+def test_pcg_matches_reference_gpu_golden(ctx):
+    g = golden("ref_gpu_small.npz")
+    h = golden("ref_host_small.npz")
+    rp, ci = h["rp"], h["ci"]
+    n = rp.size - 1
+    amg = cfa.AmgPreconditioner(ctx)
+    drp, dci, da = dev(rp, torch.int32), dev(ci, torch.int32), dev(h["lap_val"])
+    amg.setup(n, ci.size, drp, dci, da)
+    s = cfa.GpuLinearSolver(ctx)
+    dx = torch.zeros(n, dtype=torch.float64, device="cuda")
+    it = s.solve_pcg(n, drp, dci, da, dev(np.cos(0.11 * np.arange(n))), dx, 400, 1e-10, None, amg)
+    assert s.converged and abs(it - g["lap_pcg_info"][0]) <= 1
+    assert np.abs(host(dx) - g["lap_pcg_x"]).max() < 1e-8 * np.abs(g["lap_pcg_x"]).max()
+
+
+# ------------------------------------------------------------------------------------------------
+# the whole step
+# ------------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
+def test_step_matches_oracle(ctx, precision):
+    import step as S
+    m = mesh("medium")
+    u, v, p = fields(m)
+    st = S.SolveStep(m, u, v, p, precision=precision, ctx=ctx)
+    st.amg_setup()
+    st.run()
+    rep = st.report()
+    assert all(rep["conv"]), rep
+    rp, ci = st.dm.host_pattern()
+    A, ru, rv, mass = O.assemble_momentum(m, rp, ci, u, v, u, v, p, O.bdf2_params())
+    uu, vv = u.copy(), v.copy()
+    O.apply_bc_momentum(m, rp, ci, A, ru, rv, uu, vv)
+    oi = O.Ilu(rp, ci)
+    oi.factor(A)
+    xu, xv, reps = O.bicgstab2(rp, ci, A, ru, rv, uu, vv, oi, 1000, 1e-10)
+    assert np.abs(host(st.u) - xu).max() < 1e-8 * np.abs(xu).max()
+    assert np.abs(host(st.v) - xv).max() < 1e-8 * np.abs(xv).max()
+    us, vs = host(st.u), host(st.v)
+    dt_proj = 2e-3 / 3
+    s = O.oss_weights(m, us, vs, dt_proj, 1.0, 1e-3, 0.3)
+    gx, gy = O.scalar_gradient(m, p, s)
+    Kp, rhs, div = O.assemble_ppe(m, rp, ci, us, vs, p, gx, gy, mass, s, dt_proj, 1.0, 0.3)
+    dp = np.zeros(m.n)
+    O.apply_bc_pressure(m, rp, ci, Kp, rhs, dp, mass)
+    oss, inv_m = O.assemble_oss(m, rp, ci, s, mass)
+    oa = O.Amg(rp, ci, Kp)
+    xo, repo = O.pcg(rp, ci, Kp, rhs, dp, 4000, 1e-10, oss, inv_m, m.tag, oa)
+    assert np.abs(host(st.dp) - xo).max() < 1e-7 * np.abs(xo).max()
+
+
+def test_step_matches_reference_gpu_golden(ctx):
+    import step as S
+    g = golden("ref_gpu_small.npz")
+    h = golden("ref_host_small.npz")
+    m = MeshFromGolden(h)
+    st = S.SolveStep(m, h["u"], h["v"], h["p"], ctx=ctx)
+    st.amg_setup()
+    st.run()
+    rep = st.report()
+    assert all(rep["conv"])
+    for k, t in (("step_u", st.u), ("step_v", st.v), ("step_dp", st.dp)):
+        ref = g[k]
+        assert np.abs(host(t) - ref).max() < 1e-7 * np.abs(ref).max(), k
+    assert abs(rep["it_p"] - int(g["step_its"][2])) <= 2
+
+
+def test_step_live_reference_harness(ctx):
+    """When the reference's CUDA build is present (oracle/_ref), run one of its steps on the same
+    inputs in this process and compare the solutions."""
+    import ctypes as C
+    import os
+    from oracle import build as B
+    if not os.path.exists(B.REF_LIB):
+        pytest.skip("reference harness not built")
+    import step as S
+    R = O.ref()
+    m = mesh("medium")
+    u, v, p = fields(m)
+    ev = np.ascontiguousarray(m.elem_v, np.int32)
+    tag = np.ascontiguousarray(m.tag, np.int32)
+    h = C.c_void_p(R.ref_step_create(m.n, m.ne, O._p(ev), O._p(m.x), O._p(m.y), O._p(tag), O._p(u), O._p(v), O._p(p),
+                                     C.c_double(1e-3), C.c_double(1e-3), C.c_double(1.0), C.c_double(1.5),
+                                     C.c_double(1.0), C.c_double(1e-3), C.c_double(0.3), C.c_double(1e-10), 1000, 4000))
+    R.ref_step_amg_setup(h)
+    its, conv, rel = np.zeros(3, np.int32), np.zeros(3, np.int32), np.zeros(3)
+    ru, rv, rdp = np.zeros(m.n), np.zeros(m.n), np.zeros(m.n)
+    R.ref_step_run(h, O._p(its), O._p(conv), O._p(rel), O._p(ru), O._p(rv), O._p(rdp))
+    R.ref_step_free(h)
+    st = S.SolveStep(m, u, v, p, ctx=ctx)
+    st.amg_setup()
+    st.run()
+    assert all(conv) and all(st.report()["conv"])
+    assert np.abs(host(st.u) - ru).max() < 1e-8 * np.abs(ru).max()
+    assert np.abs(host(st.dp) - rdp).max() < 1e-7 * np.abs(rdp).max()
