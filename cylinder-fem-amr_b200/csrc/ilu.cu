@@ -171,6 +171,8 @@ cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, con
         if (c == nc) { ++nc; mark.push_back(-1); }
         colour[i] = c;
     }
+    for (int r = 0; r < n; ++r)
+        if (diag[r] < 0) return set_error(ctx, CFA_BAD_ARG, "ILU pattern row without a diagonal", __FILE__, __LINE__);
     auto* h = new cfa_ilu();
     h->n = n; h->nnz = nnz; h->nc = nc; h->precision = precision; h->rp = d_rp; h->ci = d_ci;
     h->colour_start.assign(nc + 1, 0);

@@ -811,7 +811,7 @@ static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* re
         CFA_CUDA(cudaMemsetAsync(W.counter.p, 0, sizeof(unsigned int), ctx->stream));
         W.cap = n;
     }
-    CFA_CUDA(W.part.ensure(8 * (size_t)row_grid(ctx, n, 1) + 64));
+    CFA_CUDA(W.part.ensure(8 * 8 * (size_t)ctx->num_sms + 64));   // NV <= 8 partials x max grid
     // parameters
     CgState init{};
     init.tol = a.tol;
@@ -924,7 +924,7 @@ static cfa_status b2_solve(cfa_ctx* ctx, const B2Args& a, cfa_solve_report* rep)
         CFA_CUDA(cudaMemsetAsync(W.counter.p, 0, sizeof(unsigned int), ctx->stream));
         W.cap = n;
     }
-    CFA_CUDA(W.part.ensure(8 * (size_t)row_grid(ctx, 2LL * n, 1) + 64));
+    CFA_CUDA(W.part.ensure(8 * 8 * (size_t)ctx->num_sms + 64));   // NV <= 8 partials x max grid
     B2State init{};
     init.tol = a.tol;
     init.max_iter = a.max_iter;
