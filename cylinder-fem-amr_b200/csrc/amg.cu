@@ -635,7 +635,7 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
     const auto t0 = std::chrono::steady_clock::now();
     const cfa_amg_opts& o = amg->opts;
     amg->levels.clear();
-    amg->version++;
+    amg->version = next_uid();
     DCsr A;
     CFA_PROPAGATE(copy_csr(ctx, n, nnz, d_rp, d_ci, d_v, A));
     while (A.rows > o.coarse_target && (int)amg->levels.size() < o.max_levels - 1) {

@@ -2,6 +2,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include "internal.cuh"
@@ -16,6 +17,11 @@ cfa_status set_error(cfa_ctx* ctx, cfa_status s, const char* what, const char* f
         ctx->err = buf;
     }
     return s;
+}
+
+long long next_uid() {
+    static std::atomic<long long> uid{0};
+    return ++uid;
 }
 
 cfa_status ensure_partials(cfa_ctx* ctx, size_t count) {
@@ -265,6 +271,7 @@ cfa_status cfa_mesh_create(cfa_ctx* ctx, int n, int ne, const int* d_ev, const d
     if (!ctx || !out) return CFA_BAD_ARG;
     CFA_ARG(n > 0 && ne > 0 && d_ev && d_x && d_y && d_tag && d_rp && d_ci);
     auto* m = new cfa_mesh();
+    m->uid = next_uid();
     m->n = n;
     m->ne = ne;
     m->ev = d_ev;

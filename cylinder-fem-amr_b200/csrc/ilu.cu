@@ -174,6 +174,7 @@ cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, con
     for (int r = 0; r < n; ++r)
         if (diag[r] < 0) return set_error(ctx, CFA_BAD_ARG, "ILU pattern row without a diagonal", __FILE__, __LINE__);
     auto* h = new cfa_ilu();
+    h->uid = next_uid();
     h->n = n; h->nnz = nnz; h->nc = nc; h->precision = precision; h->rp = d_rp; h->ci = d_ci;
     h->colour_start.assign(nc + 1, 0);
     for (int i = 0; i < n; ++i) h->colour_start[colour[i] + 1]++;

@@ -7,6 +7,7 @@
 
 struct cfa_ilu {
     int n = 0, nnz = 0, nc = 0, nl = 0, nu = 0;
+    long long uid = 0;
     cfa_precision precision = CFA_FP64;
     const int* rp = nullptr;          // device pattern (caller-owned)
     const int* ci = nullptr;

@@ -126,6 +126,9 @@ inline int threads_per_row(int rows, long long nnz) {
 
 cfa_status ensure_partials(cfa_ctx* ctx, size_t count);
 void free_solver_work(cfa_ctx* ctx);
+// Process-unique id for handles and hierarchy versions: cached solve graphs key on it, because a
+// new handle can be allocated at the address of a freed one.
+long long next_uid();
 
 // ---------------------------------------------------------------------------------------------
 // device helpers

@@ -820,9 +820,12 @@ static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* re
     CFA_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
     long long extra_body = 0;
     if (graphs_enabled()) {
+        const cfa_mesh* om = a.oss ? a.oss->mesh : nullptr;
         std::vector<const void*> key = {a.rp, a.ci, a.val, a.b, a.x, a.oss ? a.oss->d_oss_val : nullptr,
-                                        a.oss ? a.oss->d_inv_m : nullptr, a.oss ? (const void*)a.oss->mesh : nullptr,
-                                        a.amg, (const void*)(intptr_t)(a.amg ? a.amg->version : 0),
+                                        a.oss ? a.oss->d_inv_m : nullptr, (const void*)(intptr_t)(om ? om->uid : 0),
+                                        (const void*)(intptr_t)(om ? om->bc.outlet_dirichlet : 0),
+                                        (const void*)(intptr_t)(om ? om->bc.pin : 0),
+                                        (const void*)(intptr_t)(a.amg ? a.amg->version : 0),
                                         (const void*)(intptr_t)n, (const void*)(intptr_t)a.nnz};
         if (!W.graph.exec || W.graph.key != key) {
             CFA_PROPAGATE(build_graph(ctx, W.graph, [&](CondArg c) { return pcg_init(ctx, W, a, c); },
@@ -932,7 +935,7 @@ static cfa_status b2_solve(cfa_ctx* ctx, const B2Args& a, cfa_solve_report* rep)
     CFA_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
     long long extra_body = 0;
     if (graphs_enabled()) {
-        std::vector<const void*> key = {a.rp, a.ci, a.val, a.bu, a.bv, a.xu, a.xv, a.ilu,
+        std::vector<const void*> key = {a.rp, a.ci, a.val, a.bu, a.bv, a.xu, a.xv, (const void*)(intptr_t)a.ilu->uid,
                                         (const void*)(intptr_t)n, (const void*)(intptr_t)a.nnz};
         if (!W.graph.exec || W.graph.key != key) {
             CFA_PROPAGATE(build_graph(ctx, W.graph, [&](CondArg c) { return b2_init(ctx, W, a, c); },

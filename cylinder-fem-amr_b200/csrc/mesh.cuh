@@ -24,6 +24,7 @@ __device__ __forceinline__ bool pressure_dirichlet(int i, int tag, const OutletB
 
 struct cfa_mesh {
     int n = 0, ne = 0, nnz = 0;
+    long long uid = 0;
     const int* ev = nullptr;     // [3 ne]
     const double* x = nullptr;
     const double* y = nullptr;

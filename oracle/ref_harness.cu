@@ -1,7 +1,7 @@
 // Reference harness -- TEST INFRASTRUCTURE ONLY.
 //
 // Compiles the reference solver's own translation unit (the file `cylinder_fem_amr.cu` of the
-// reference project, found through the include path given by oracle/Makefile; nothing of it is
+// reference project, found through the include path given by oracle/build.py; nothing of it is
 // copied here) with CFA_NO_MAIN, the same mechanism as the reference's tests/test_cfa.cu:10-11,
 // and exposes its functions and classes behind extern "C" entry points taking host arrays:
 //   * host-only reference code (runs without a GPU): the CSR build, csr_multiply/csr_transpose,
@@ -393,49 +393,13 @@ static void ref_reset(RefStep* S) {
     CUDA_CHECK(cudaDeviceSynchronize());
 }
 
-// Assembles the pressure operator once (for the AMG setup) and returns the setup time [ms].
-double ref_step_amg_setup(void* h) {
-    auto* S = static_cast<RefStep*>(h);
+// Step A (src/cylinder_fem_amr.cu:300-384): momentum assembly + BCs, ILU factor, BiCGSTAB2.
+static void ref_step_momentum(RefStep* S) {
     DeviceMeshBuffers& g = S->g;
-    ref_reset(S);
-    CUDA_CHECK(cudaMemset(g.d_Kp_val, 0, g.nnz * sizeof(double)));
-    CUDA_CHECK(cudaMemset(g.d_rhs_p, 0, g.n_nodes * sizeof(double)));
-    CUDA_CHECK(cudaMemset(g.d_div_num, 0, g.n_nodes * sizeof(double)));
-    CUDA_CHECK(cudaMemset(g.d_grad_dp_x, 0, g.n_nodes * sizeof(double)));
-    CUDA_CHECK(cudaMemset(g.d_grad_dp_y, 0, g.n_nodes * sizeof(double)));
-    CUDA_CHECK(cudaMemset(g.d_mass_lumped, 0, g.n_nodes * sizeof(double)));
-    const int tb = 256, be = (g.n_elems + tb - 1) / tb;
-    const double dt_proj = (2.0 / 3.0) * S->dt;
-    k_assemble_lumped_mass<<<be, tb>>>(g.n_elems, g.d_elem_v, g.d_x, g.d_y, g.d_mass_lumped);
-    k_compute_oss_weights<<<be, tb>>>(g.n_elems, g.d_elem_v, g.d_x, g.d_y, g.d_u, g.d_v, dt_proj,
-                                      S->rho, S->nu, S->stab, g.d_elem_s);
-    k_accumulate_scalar_gradient<<<be, tb>>>(g.n_elems, g.d_elem_v, g.d_x, g.d_y, g.d_p, g.d_elem_s,
-                                             g.d_grad_dp_x, g.d_grad_dp_y);
-    k_assemble_pressure_poisson<<<be, tb>>>(g.n_elems, g.d_elem_v, g.d_x, g.d_y, g.d_u, g.d_v, g.d_p,
-                                            g.d_grad_dp_x, g.d_grad_dp_y, g.d_mass_lumped, g.d_elem_s,
-                                            dt_proj, S->rho, S->stab, g.d_row_ptr, g.d_col_ind,
-                                            g.d_Kp_val, g.d_rhs_p, g.d_div_num);
-    apply_bc_pressure(g.n_nodes, g.d_bc_tag, g.d_row_ptr, g.d_col_ind, g.d_Kp_val, g.d_rhs_p, g.d_dp,
-                      g.d_mass_lumped);
-    CUDA_CHECK(cudaDeviceSynchronize());
-    S->amg.setup(g.n_nodes, g.nnz, g.d_row_ptr, g.d_col_ind, g.d_Kp_val);
-    CUDA_CHECK(cudaDeviceSynchronize());
-    return S->amg.setup_ms;
-}
-
-// Runs one step; returns its wall time [ms] (host clock with device syncs, as the reference times
-// its phases). it[0..2] = momentum u, v and pressure iterations; conv[0..2] converged flags.
-// If out_u/out_v/out_p are given, the solved u*, v* and dp are returned.
-double ref_step_run(void* h, int* it, int* conv, double* rel, double* out_u, double* out_v, double* out_dp) {
-    auto* S = static_cast<RefStep*>(h);
-    DeviceMeshBuffers& g = S->g;
-    ref_reset(S);
     const int n = g.n_nodes, ne = g.n_elems, nnz = g.nnz, tb = 256;
     const int bn = (n + tb - 1) / tb, be = (ne + tb - 1) / tb;
-    const double dt = S->dt, dt_proj = (2.0 / 3.0) * dt;
+    const double dt = S->dt;
     const double a0 = 1.5 / dt, a1 = 2.0 / dt, a2 = -0.5 / dt, c1 = 2.0, c2 = -1.0;
-    auto t0 = std::chrono::steady_clock::now();
-    // Step A
     CUDA_CHECK(cudaMemset(g.d_A_val, 0, nnz * sizeof(double)));
     CUDA_CHECK(cudaMemset(g.d_rhs_u, 0, n * sizeof(double)));
     CUDA_CHECK(cudaMemset(g.d_rhs_v, 0, n * sizeof(double)));
@@ -450,7 +414,14 @@ double ref_step_run(void* h, int* it, int* conv, double* rel, double* out_u, dou
     S->mom.solve(n, g.d_row_ptr, g.d_col_ind, g.d_A_val, g.d_rhs_u, g.d_rhs_v, g.d_u, g.d_v,
                  S->max_it_mom, S->tol, S->ilu);
     CUDA_CHECK(cudaDeviceSynchronize());
-    // Step B
+}
+
+// Step B assembly (src/cylinder_fem_amr.cu:387-441): OSS weights, G(p^n), PPE + BCs, OSS operator.
+static void ref_step_pressure_assembly(RefStep* S) {
+    DeviceMeshBuffers& g = S->g;
+    const int n = g.n_nodes, ne = g.n_elems, nnz = g.nnz, tb = 256;
+    const int be = (ne + tb - 1) / tb;
+    const double dt_proj = (2.0 / 3.0) * S->dt;
     CUDA_CHECK(cudaMemset(g.d_Kp_val, 0, nnz * sizeof(double)));
     CUDA_CHECK(cudaMemset(g.d_rhs_p, 0, n * sizeof(double)));
     CUDA_CHECK(cudaMemset(g.d_div_num, 0, n * sizeof(double)));
@@ -469,13 +440,40 @@ double ref_step_run(void* h, int* it, int* conv, double* rel, double* out_u, dou
                                             g.d_Kp_val, g.d_rhs_p, g.d_div_num);
     apply_bc_pressure(n, g.d_bc_tag, g.d_row_ptr, g.d_col_ind, g.d_Kp_val, g.d_rhs_p, g.d_dp, g.d_mass_lumped);
     if (oss) assemble_oss_projection(g);
+}
+
+// Builds the AMG hierarchy as the driver does every amg_rebuild steps: from this step's pressure
+// operator, i.e. after the momentum solve (src/cylinder_fem_amr.cu:445-452). Returns setup ms.
+double ref_step_amg_setup(void* h) {
+    auto* S = static_cast<RefStep*>(h);
+    DeviceMeshBuffers& g = S->g;
+    ref_reset(S);
+    ref_step_momentum(S);
+    ref_step_pressure_assembly(S);
+    CUDA_CHECK(cudaDeviceSynchronize());
+    S->amg.setup(g.n_nodes, g.nnz, g.d_row_ptr, g.d_col_ind, g.d_Kp_val);
+    CUDA_CHECK(cudaDeviceSynchronize());
+    return S->amg.setup_ms;
+}
+
+// Runs one step; returns its wall time [ms] (host clock with device syncs, as the reference times
+// its phases). it[0..2] = momentum u, v and pressure iterations; conv[0..2] converged flags.
+// If out_u/out_v/out_dp are given, the solved u*, v* and dp are returned.
+double ref_step_run(void* h, int* it, int* conv, double* rel, double* out_u, double* out_v, double* out_dp) {
+    auto* S = static_cast<RefStep*>(h);
+    DeviceMeshBuffers& g = S->g;
+    ref_reset(S);
+    const int n = g.n_nodes;
+    auto t0 = std::chrono::steady_clock::now();
+    ref_step_momentum(S);
+    ref_step_pressure_assembly(S);
     std::function<void(const double*, double*)> oss_op = [&g](const double* in, double* out) {
         apply_oss_projection(g, in, out);
     };
     std::function<void(const double*, double*)> prec = [S](const double* r, double* z) { S->amg.apply(r, z); };
     const bool use_amg = !S->amg.levels.empty() || S->amg.coarse_n > 0;
     int it_p = S->solver.solve_pcg(n, g.d_row_ptr, g.d_col_ind, g.d_Kp_val, g.d_rhs_p, g.d_dp, S->max_it_p,
-                                   S->tol, oss ? &oss_op : nullptr, use_amg ? &prec : nullptr);
+                                   S->tol, S->stab > 0.0 ? &oss_op : nullptr, use_amg ? &prec : nullptr);
     CUDA_CHECK(cudaDeviceSynchronize());
     double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (it) { it[0] = S->mom.iters[0]; it[1] = S->mom.iters[1]; it[2] = it_p; }
