@@ -128,6 +128,7 @@ def time_operator(cfa, st, reps, flush):
     x = st.dp.clone().normal_()
     y = torch.empty_like(x)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    cfa.pressure_operator_prepare(st.ctx, st.dm.rp, st.dm.ci, st.Kp, st.oss)
     for _ in range(3):
         cfa.pressure_operator(st.ctx, st.dm.rp, st.dm.ci, st.Kp, x, y, st.oss)
     total = 0.0

@@ -182,9 +182,12 @@ class DeviceMesh:
             raise CfaError(s, "cfa_mesh_set_outlet")
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().cfa_mesh_destroy(self.h)
-            self.h = None
+        try:
+            if getattr(self, "h", None):
+                lib().cfa_mesh_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------------------------
@@ -250,6 +253,11 @@ def spmv_multi(ctx, rp, ci, val, x, y, nrhs):
     ctx.check(lib().cfa_spmv_multi(ctx.h, rp.numel() - 1, nrhs, ptr(rp), ptr(ci), ptr(val), ptr(x), ptr(y)))
 
 
+def pressure_operator_prepare(ctx, rp, ci, val, oss=None):
+    ctx.check(lib().cfa_pressure_operator_prepare(ctx.h, rp.numel() - 1, ci.numel(), ptr(rp), ptr(ci), ptr(val),
+                                                  C.byref(oss) if oss is not None else None))
+
+
 def pressure_operator(ctx, rp, ci, val, x, y, oss=None):
     ctx.check(lib().cfa_pressure_operator(ctx.h, rp.numel() - 1, ci.numel(), ptr(rp), ptr(ci), ptr(val),
                                           C.byref(oss) if oss is not None else None, ptr(x), ptr(y)))
@@ -305,9 +313,12 @@ class MulticolourIlu0:
             _dev_view(lu.value, nnz, torch.float64)
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().cfa_ilu_destroy(self.h)
-            self.h = None
+        try:
+            if getattr(self, "h", None):
+                lib().cfa_ilu_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
 
 
 class GpuBicgstab2:
@@ -397,9 +408,12 @@ class AmgPreconditioner:
         return _dev_view(p.value, cn * cn, torch.float64).reshape(cn, cn)
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().cfa_amg_destroy(self.h)
-            self.h = None
+        try:
+            if getattr(self, "h", None):
+                lib().cfa_amg_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
 
 
 class GpuLinearSolver:

@@ -11,30 +11,29 @@ namespace cfa {
 
 constexpr int kIluMaxRow = 32;   // ILU_MAX_ROW (src/cfa/linalg.cuh:361)
 
-// Row i of colour c: for its L entries k in elimination order, l_ik = a_ik / u_kk and
-// a_ij -= l_ik u_kj within the pattern. Same arithmetic and order as the reference kernel.
+// Row i of colour c (k_ilu0_factor_colour, src/cfa/linalg.cuh:363-392): for its L entries k in
+// elimination order, l_ik = a_ik / u_kk and a_ij -= l_ik u_kj within the pattern. The matching of
+// row k's columns against row i's pattern is done once per pattern (the elimination program
+// built in cfa_ilu_create), so the arithmetic -- the same operations in the same order as the
+// reference kernel -- is a plain gather loop.
 __global__ void k_ilu_factor_colour(int m, const int* __restrict__ rows, const int* __restrict__ rp,
-                                    const int* __restrict__ ci, const int* __restrict__ colour,
-                                    const int* __restrict__ diag, double* __restrict__ lu) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= m) return;
+                                    const int* __restrict__ ep, const int4* __restrict__ elim,
+                                    const int2* __restrict__ upd, int t0, double* __restrict__ lu) {
+    const int tl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tl >= m) return;
+    const int t = t0 + tl;
     const int i = rows[t];
     const int s = rp[i], len = rp[i + 1] - s;
-    const int cii = colour[i];
-    int cols[kIluMaxRow], ccol[kIluMaxRow];
     double a[kIluMaxRow];
-    for (int q = 0; q < len; ++q) { cols[q] = ci[s + q]; ccol[q] = colour[cols[q]]; a[q] = lu[s + q]; }
-    for (int c = 0; c < cii; ++c) {
-        for (int q = 0; q < len; ++q) {
-            if (ccol[q] != c) continue;
-            const int k = cols[q];
-            const double lik = a[q] / lu[diag[k]];
-            a[q] = lik;
-            for (int mm = rp[k]; mm < rp[k + 1]; ++mm) {
-                const int j = ci[mm];
-                for (int b = 0; b < len; ++b)
-                    if (cols[b] == j) { if (ccol[b] > c) a[b] -= lik * lu[mm]; break; }
-            }
+    for (int q = 0; q < len; ++q) a[q] = lu[s + q];
+    const int e1 = ep[t + 1];
+    for (int e = ep[t]; e < e1; ++e) {
+        const int4 el = elim[e];
+        const double lik = a[el.x] / lu[el.y];
+        a[el.x] = lik;
+        for (int u = el.z; u < el.w; ++u) {
+            const int2 up = upd[u];
+            a[up.x] -= lik * lu[up.y];
         }
     }
     for (int q = 0; q < len; ++q) lu[s + q] = a[q];
@@ -204,6 +203,35 @@ cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, con
             else { uc[u] = j; u_src[u++] = a; }
         }
     }
+    // elimination program (symbolic ILU(0)): the operation sequence of the reference's factor kernel
+    std::vector<int> ep(n + 1, 0);
+    std::vector<int4> elim;
+    std::vector<int2> updv;
+    elim.reserve((size_t)h->nl);
+    for (int t = 0; t < n; ++t) {
+        const int i = rows[t];
+        const int s0 = rp[i], len = rp[i + 1] - s0, cii = colour[i];
+        for (int c = 0; c < cii; ++c) {
+            for (int q = 0; q < len; ++q) {
+                const int k = ci[s0 + q];
+                if (colour[k] != c) continue;
+                int4 el;
+                el.x = q;
+                el.y = diag[k];
+                el.z = (int)updv.size();
+                for (int mm = rp[k]; mm < rp[k + 1]; ++mm) {
+                    const int j = ci[mm];
+                    for (int b = 0; b < len; ++b)
+                        if (ci[s0 + b] == j) { if (colour[j] > c) updv.push_back(make_int2(b, mm)); break; }
+                }
+                el.w = (int)updv.size();
+                elim.push_back(el);
+            }
+        }
+        ep[t + 1] = (int)elim.size();
+    }
+    h->n_elim = (int)elim.size();
+    h->n_upd = (int)updv.size();
     cudaError_t e = cudaSuccess;
     auto up_int = [&](DevBuf<int>& d, const std::vector<int>& v) {
         if (e != cudaSuccess) return;
@@ -213,6 +241,13 @@ cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, con
     };
     up_int(h->rows, rows); up_int(h->colour, colour); up_int(h->diag, diag); up_int(h->lp, lp); up_int(h->up, up);
     up_int(h->lc, lc); up_int(h->uc, uc); up_int(h->l_src, l_src); up_int(h->u_src, u_src); up_int(h->d_src, d_src);
+    up_int(h->ep, ep);
+    if (e == cudaSuccess) e = h->elim.ensure(std::max<size_t>(elim.size(), 1));
+    if (e == cudaSuccess && !elim.empty())
+        e = cudaMemcpyAsync(h->elim.p, elim.data(), elim.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = h->upd.ensure(std::max<size_t>(updv.size(), 1));
+    if (e == cudaSuccess && !updv.empty())
+        e = cudaMemcpyAsync(h->upd.p, updv.data(), updv.size() * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = h->lu.ensure(nnz);
     if (precision == CFA_MIXED) {
         if (e == cudaSuccess) e = h->lv32.ensure(std::max(h->nl, 1));
@@ -245,8 +280,8 @@ cfa_status cfa_ilu_factor(cfa_ctx* ctx, cfa_ilu* h, const double* val) {
     for (int c = 1; c < h->nc; ++c) {
         const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
         if (m == 0) continue;
-        CFA_LAUNCH(ctx, k_ilu_factor_colour, ceil_div(m, 128), 128, 0, m, h->rows.p + cs, h->rp, h->ci, h->colour.p,
-                   h->diag.p, h->lu.p);
+        CFA_LAUNCH(ctx, k_ilu_factor_colour, ceil_div(m, 128), 128, 0, m, (const int*)h->rows.p, h->rp,
+                   (const int*)h->ep.p, (const int4*)h->elim.p, (const int2*)h->upd.p, cs, h->lu.p);
     }
     const int len = std::max(h->n, std::max(h->nl, h->nu));
     if (h->precision == CFA_MIXED)

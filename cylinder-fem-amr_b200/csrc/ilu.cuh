@@ -17,6 +17,13 @@ struct cfa_ilu {
     cfa::DevBuf<double> lv64, uv64, dinv64;
     cfa::DevBuf<float> lv32, uv32, dinv32;
     cfa::DevBuf<float> work32;        // FP32 sweep vectors (mixed precision), nrhs * n
+    // symbolic factorization (elimination program), rows in colour order:
+    // elim[ep[t] .. ep[t+1]) = {local index q of l_ik in row i, CSR position of u_kk, first update},
+    // upd[elim.ub .. next.ub) = {local index b in row i, CSR position m in row k}: a_ib -= l_ik lu_m
+    cfa::DevBuf<int> ep;              // [n + 1]
+    cfa::DevBuf<int4> elim;           // {q, dk, ub, 0}
+    cfa::DevBuf<int2> upd;            // {b, m}
+    int n_elim = 0, n_upd = 0;
 };
 
 namespace cfa {

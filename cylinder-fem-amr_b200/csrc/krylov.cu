@@ -16,6 +16,7 @@
 #include "amg.cuh"
 #include "ilu.cuh"
 #include "mesh.cuh"
+#include "tiled.cuh"
 
 namespace cfa {
 
@@ -168,6 +169,109 @@ k_op_k(int n, int nnz, const int* __restrict__ rp, const int* __restrict__ ci, c
     }
 }
 
+// ---- tile-streamed forms of the two operator passes (tiled.cuh) ----
+// pass 1: tiles of {Bx, By}; pn = z + beta p (beta NULL: pn = z)
+template <int TPR>
+__global__ void __launch_bounds__(kTileThreads)
+k_opt_b(TileView tv, const double* __restrict__ inv_m, const double* __restrict__ z, const double* __restrict__ p,
+        const double* __restrict__ beta_ptr, double* __restrict__ p_new, double* __restrict__ gx,
+        double* __restrict__ gy, const int* __restrict__ done) {
+    if (done && *done) return;
+    extern __shared__ __align__(128) unsigned char tsmem[];
+    const bool fuse = beta_ptr != nullptr;
+    const double beta = fuse ? *beta_ptr : 0.0;
+    tile_loop(tv, tsmem, [&](int, int r0, int nr, const unsigned char* ch) {
+        const int* rr = reinterpret_cast<const int*>(ch);
+        const int ne = rr[nr];
+        const int* cs = reinterpret_cast<const int*>(ch + tile_ci_off(nr));
+        const double* bx = reinterpret_cast<const double*>(ch + tile_val_off(nr, ne, 8, 0));
+        const double* by = reinterpret_cast<const double*>(ch + tile_val_off(nr, ne, 8, 1));
+        for (int base = 0; base < nr; base += kTileThreads / TPR) {
+            const int lr = base + (int)threadIdx.x / TPR, lane = threadIdx.x % TPR;
+            const bool valid = lr < nr;
+            double sx = 0.0, sy = 0.0;
+            if (valid)
+                for (int e = rr[lr] + lane; e < rr[lr + 1]; e += TPR) {
+                    const int j = cs[e];
+                    const double pj = fuse ? z[j] + beta * p[j] : z[j];
+                    sx += bx[e] * pj;
+                    sy += by[e] * pj;
+                }
+            sx = group_reduce<TPR>(sx);
+            sy = group_reduce<TPR>(sy);
+            if (valid && lane == 0) {
+                const int row = r0 + lr;
+                const double im = inv_m[row];
+                gx[row] = sx * im;
+                gy[row] = sy * im;
+                if (p_new) p_new[row] = fuse ? z[row] + beta * p[row] : z[row];
+            }
+        }
+    });
+}
+
+// pass 2: tiles of {K, BTx, BTy} (OSS) or {K}; FUSEP as k_op_k; DOT: pn.q -> alpha
+template <int TPR, bool OSS, bool FUSEP, bool DOT>
+__global__ void __launch_bounds__(kTileThreads)
+k_opt_k(TileView tv, const int* __restrict__ tag, OutletBc bc, const double* __restrict__ z,
+        const double* __restrict__ p, const double* __restrict__ beta_ptr, double* __restrict__ pn_buf,
+        const double* __restrict__ gx, const double* __restrict__ gy, double* __restrict__ q, CgState* __restrict__ st,
+        double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond, const int* __restrict__ done) {
+    if (done && *done) return;
+    extern __shared__ __align__(128) unsigned char tsmem[];
+    __shared__ double sh[kWarps];
+    const bool fuse = FUSEP && beta_ptr != nullptr;
+    const double beta = fuse ? *beta_ptr : 0.0;
+    double acc = 0.0;
+    tile_loop(tv, tsmem, [&](int, int r0, int nr, const unsigned char* ch) {
+        const int* rr = reinterpret_cast<const int*>(ch);
+        const int ne = rr[nr];
+        const int* cs = reinterpret_cast<const int*>(ch + tile_ci_off(nr));
+        const double* kv = reinterpret_cast<const double*>(ch + tile_val_off(nr, ne, 8, 0));
+        const double* btx = reinterpret_cast<const double*>(ch + tile_val_off(nr, ne, 8, 1));
+        const double* bty = reinterpret_cast<const double*>(ch + tile_val_off(nr, ne, 8, 2));
+        for (int base = 0; base < nr; base += kTileThreads / TPR) {
+            const int lr = base + (int)threadIdx.x / TPR, lane = threadIdx.x % TPR;
+            const bool valid = lr < nr;
+            double s = 0.0, so = 0.0;
+            if (valid)
+                for (int e = rr[lr] + lane; e < rr[lr + 1]; e += TPR) {
+                    const int j = cs[e];
+                    const double pj = FUSEP ? (fuse ? z[j] + beta * p[j] : z[j]) : pn_buf[j];
+                    s += kv[e] * pj;
+                    if (OSS) so += btx[e] * gx[j] + bty[e] * gy[j];
+                }
+            s = group_reduce<TPR>(s);
+            if (OSS) so = group_reduce<TPR>(so);
+            if (valid && lane == 0) {
+                const int row = r0 + lr;
+                if (OSS && !pressure_dirichlet(row, tag[row], bc)) s -= so;
+                q[row] = s;
+                const double pi = FUSEP ? (fuse ? z[row] + beta * p[row] : z[row]) : pn_buf[row];
+                if (FUSEP && pn_buf) pn_buf[row] = pi;
+                if (DOT) acc += pi * s;
+            }
+        }
+    });
+    if (!DOT) return;
+    double v[1] = {acc};
+    block_sum<1>(v, sh);
+    if (publish_partials<1>(v, part, counter)) {
+        reduce_partials<1>(v, part, counter, sh);
+        if (threadIdx.x == 0) {
+            const double pq = v[0];
+            if (fabs(pq) < 1.0e-30) {
+                st->done = 1;
+                st->converged = 0;
+                st->status = CFA_BREAKDOWN;
+                set_cond(cond, 0);
+            } else {
+                st->alpha = st->rz / pq;
+            }
+        }
+    }
+}
+
 // ||b|| (solve_pcg :205-209)
 __global__ void __launch_bounds__(kThreads)
 k_cg_bnorm(int n, const double* __restrict__ b, CgState* __restrict__ st, double* __restrict__ part,
@@ -290,23 +394,32 @@ k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, const double*
 }
 
 // r.z after the preconditioner: first = initial rz (p = z); else beta = rz_new / (rz + 1e-30)
+// (solve_pcg, :249-252). With `flexible` (an FP32 preconditioner, which is not exactly the same
+// linear operator at every application) beta is the Polak-Ribiere form
+// z_new.(r_new - r_old) / rz_old = -alpha z_new.q / rz_old, which keeps CG's convergence rate;
+// for a fixed preconditioner both forms are equal in exact arithmetic.
 __global__ void __launch_bounds__(kThreads)
-k_cg_rz(int n, const double* __restrict__ r, const double* __restrict__ z, int first, CgState* __restrict__ st,
-        double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+k_cg_rz(int n, const double* __restrict__ r, const double* __restrict__ z, const double* __restrict__ q, int first,
+        int flexible, CgState* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter,
+        CondArg cond) {
     if (st->done) return;
-    __shared__ double sh[kWarps];
-    double v[1] = {0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] += r[i] * z[i];
-    block_sum<1>(v, sh);
-    if (publish_partials<1>(v, part, counter)) {
-        reduce_partials<1>(v, part, counter, sh);
+    __shared__ double sh[2 * kWarps];
+    double v[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double zi = z[i];
+        v[0] += r[i] * zi;
+        if (flexible) v[1] += zi * q[i];
+    }
+    block_sum<2>(v, sh);
+    if (publish_partials<2>(v, part, counter)) {
+        reduce_partials<2>(v, part, counter, sh);
         if (threadIdx.x == 0) {
             if (first) {
                 st->rz = v[0];
                 st->beta = 0.0;
                 set_cond(cond, 1);
             } else {
-                st->beta = v[0] / (st->rz + 1.0e-30);
+                st->beta = flexible ? -st->alpha * v[1] / (st->rz + 1.0e-30) : v[0] / (st->rz + 1.0e-30);
                 st->rz = v[0];
             }
         }
@@ -628,6 +741,12 @@ struct PcgWork {
     int cap = 0;
     DevBuf<double> r, z, p, pn, q, gx, gy, dinv;
     DevBuf<CgState> st;
+    // tile-streamed copy of the operator (pass 1: Bx, By; pass 2: K [, BTx, BTy])
+    TiledCsr tb, tk;
+    std::vector<const void*> tile_key;
+    std::vector<const void*> prepared;   // operator whose values the tiles hold (standalone apply)
+    bool tiled = false;
+    DevBuf<int> err;
     DevBuf<double> part;
     DevBuf<unsigned int> counter;
     GraphCache graph;
@@ -728,9 +847,52 @@ struct PcgArgs {
     double tol;
 };
 
+#define TILE_TPR_SWITCH(tpr, ...)                                                              \
+    do {                                                                                       \
+        switch (tpr) {                                                                         \
+            case 1: { constexpr int TPR = 1; __VA_ARGS__; } break;                              \
+            case 2: { constexpr int TPR = 2; __VA_ARGS__; } break;                              \
+            case 4: { constexpr int TPR = 4; __VA_ARGS__; } break;                              \
+            case 8: { constexpr int TPR = 8; __VA_ARGS__; } break;                              \
+            case 16: { constexpr int TPR = 16; __VA_ARGS__; } break;                            \
+            default: { constexpr int TPR = 32; __VA_ARGS__; } break;                            \
+        }                                                                                      \
+    } while (0)
+
+// Launches tiled pass 2 for one template configuration
+template <bool OSS, bool FUSEP, bool DOT>
+static void launch_opt_k(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, const double* z, const double* p,
+                         const double* beta_ptr, double* pn, double* q, CondArg cond, const int* done) {
+    const cfa_mesh* m = a.oss ? a.oss->mesh : nullptr;
+    OutletBc bc = m ? m->bc : OutletBc{};
+    const TileView tv = W.tk.view(W.err.p);
+    TileLaunch L;
+    TILE_TPR_SWITCH(W.tk.tile_rows >= 256 ? 1 : std::min(32, kTileThreads / W.tk.tile_rows),
+        L = tile_launch(ctx, W.tk, (const void*)k_opt_k<TPR, OSS, FUSEP, DOT>);
+        CFA_LAUNCH(ctx, (k_opt_k<TPR, OSS, FUSEP, DOT>), L.grid, kTileThreads, L.smem, tv,
+                   m ? m->tag : (const int*)nullptr, bc, z, p, beta_ptr, pn, (const double*)W.gx.p,
+                   (const double*)W.gy.p, q, W.st.p, W.part.p, W.counter.p, cond, done));
+}
+
 static cfa_status pcg_operator(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, const double* z, const double* p,
                                const double* beta_ptr, double* pn, double* q, bool dot, CondArg cond,
                                const int* done) {
+    if (W.tiled) {
+        if (a.oss) {
+            const TileView tv = W.tb.view(W.err.p);
+            TileLaunch L;
+            TILE_TPR_SWITCH(W.tb.tile_rows >= 256 ? 1 : std::min(32, kTileThreads / W.tb.tile_rows),
+                L = tile_launch(ctx, W.tb, (const void*)k_opt_b<TPR>);
+                CFA_LAUNCH(ctx, (k_opt_b<TPR>), L.grid, kTileThreads, L.smem, tv, a.oss->d_inv_m, z, p, beta_ptr, pn,
+                           W.gx.p, W.gy.p, done));
+            if (dot) launch_opt_k<true, false, true>(ctx, W, a, z, p, beta_ptr, pn, q, cond, done);
+            else launch_opt_k<true, false, false>(ctx, W, a, z, p, beta_ptr, pn, q, cond, done);
+        } else {
+            if (dot) launch_opt_k<false, true, true>(ctx, W, a, z, p, beta_ptr, pn, q, cond, done);
+            else launch_opt_k<false, true, false>(ctx, W, a, z, p, beta_ptr, pn, q, cond, done);
+        }
+        return CFA_OK;
+    }
     const int tpr = op_tpr(a.n, a.nnz);
     const int grid = row_grid(ctx, a.n, tpr);
     CgState* st = W.st.p;
@@ -767,6 +929,16 @@ static cfa_status pcg_init(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg c
     const int gv = row_grid(ctx, n, 1);
     CgState* st = W.st.p;
     const int* done = &st->done;
+    if (W.tiled) {   // this solve's operator values into the tile-streamed layout
+        if (a.oss) {
+            const double* o = a.oss->d_oss_val;
+            const size_t nz = (size_t)a.nnz;
+            CFA_PROPAGATE(pack_tiled(ctx, a.rp, a.ci, o, o + nz, nullptr, W.tb));
+            CFA_PROPAGATE(pack_tiled(ctx, a.rp, a.ci, a.val, o + 2 * nz, o + 3 * nz, W.tk));
+        } else {
+            CFA_PROPAGATE(pack_tiled(ctx, a.rp, a.ci, a.val, nullptr, nullptr, W.tk));
+        }
+    }
     CFA_LAUNCH(ctx, k_cg_bnorm, gv, kThreads, 0, n, a.b, st, W.part.p, W.counter.p, cond);
     if (!a.amg) CFA_LAUNCH(ctx, k_inv_diag, ceil_div(n, kThreads), kThreads, 0, n, a.rp, a.ci, a.val, W.dinv.p);
     // q = A x (pn scratch receives x)
@@ -775,7 +947,8 @@ static cfa_status pcg_init(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg c
     if (a.amg) CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done));
     else CFA_LAUNCH(ctx, k_vmul, gv, kThreads, 0, n, W.dinv.p, W.r.p, W.z.p);
     CFA_LAUNCH(ctx, k_cg_nullx, ceil_div(n, kThreads), kThreads, 0, n, a.x, W.p.p, st);
-    CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, 1, st, W.part.p, W.counter.p, cond);
+    CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 1, 0, st, W.part.p,
+               W.counter.p, cond);
     CFA_CHECK_LAUNCH();
     return CFA_OK;
 }
@@ -791,7 +964,9 @@ static cfa_status pcg_body(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg c
         CFA_LAUNCH(ctx, k_cg_update<false>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p,
                    (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond);
         CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done));
-        CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, 0, st, W.part.p, W.counter.p, cond);
+        const int flexible = a.amg->opts.precision == CFA_MIXED ? 1 : 0;
+        CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, flexible, st, W.part.p,
+                   W.counter.p, cond);
     } else {
         CFA_LAUNCH(ctx, k_cg_update<true>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p, W.dinv.p, W.z.p, st,
                    W.part.p, W.counter.p, cond);
@@ -800,9 +975,13 @@ static cfa_status pcg_body(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg c
     return CFA_OK;
 }
 
-static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* rep) {
-    PcgWork& W = work(ctx)->pcg;
-    const int n = a.n;
+static std::vector<const void*> operator_key(int n, int nnz, const int* rp, const int* ci, const double* val,
+                                             const cfa_oss_operator* oss) {
+    return {rp, ci, val, oss ? oss->d_oss_val : nullptr, oss ? oss->d_inv_m : nullptr,
+            (const void*)(intptr_t)(oss ? oss->mesh->uid : 0), (const void*)(intptr_t)n, (const void*)(intptr_t)nnz};
+}
+
+static cfa_status ensure_pcg_vectors(cfa_ctx* ctx, PcgWork& W, int n) {
     if (n > W.cap) {
         W.graph.reset();
         for (DevBuf<double>* b : {&W.r, &W.z, &W.p, &W.pn, &W.q, &W.gx, &W.gy, &W.dinv}) CFA_CUDA(b->ensure(n));
@@ -811,7 +990,64 @@ static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* re
         CFA_CUDA(cudaMemsetAsync(W.counter.p, 0, sizeof(unsigned int), ctx->stream));
         W.cap = n;
     }
-    CFA_CUDA(W.part.ensure(8 * 8 * (size_t)ctx->num_sms + 64));   // NV <= 8 partials x max grid
+    if (!W.err.p) {
+        CFA_CUDA(W.err.ensure(1));
+        CFA_CUDA(cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream));
+    }
+    CFA_CUDA(W.part.ensure(8 * 8 * (size_t)ctx->num_sms + 64));
+    return CFA_OK;
+}
+
+static bool tiles_enabled() {
+    const char* e = std::getenv("CFA_TILES");
+    return !(e && e[0] == '0');
+}
+
+template <int TPR>
+static void allow_operator_tpr() {
+    allow_tile_kernel((const void*)k_opt_b<TPR>);
+    allow_tile_kernel((const void*)k_opt_k<TPR, true, false, true>);
+    allow_tile_kernel((const void*)k_opt_k<TPR, true, false, false>);
+    allow_tile_kernel((const void*)k_opt_k<TPR, false, true, true>);
+    allow_tile_kernel((const void*)k_opt_k<TPR, false, true, false>);
+}
+
+static void allow_operator_kernels() {
+    static bool done = false;
+    if (done) return;
+    allow_operator_tpr<1>(); allow_operator_tpr<2>(); allow_operator_tpr<4>();
+    allow_operator_tpr<8>(); allow_operator_tpr<16>(); allow_operator_tpr<32>();
+    done = true;
+}
+
+// Plans the tile-streamed operator for this pattern (host row pointer needed: one sync).
+static cfa_status plan_operator_tiles(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a) {
+    W.tiled = tiles_enabled();
+    if (!W.tiled) return CFA_OK;
+    allow_operator_kernels();
+    std::vector<const void*> key = {a.rp, a.ci, (const void*)(intptr_t)a.n, (const void*)(intptr_t)a.nnz,
+                                    (const void*)(intptr_t)(a.oss ? 1 : 0)};
+    if (key == W.tile_key) return CFA_OK;
+    std::vector<int> h_rp(a.n + 1);
+    CFA_CUDA(cudaMemcpyAsync(h_rp.data(), a.rp, (a.n + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (a.oss) {
+        CFA_PROPAGATE(plan_tiled(ctx, h_rp.data(), a.n, 2, 8, W.tb));
+        CFA_PROPAGATE(plan_tiled(ctx, h_rp.data(), a.n, 3, 8, W.tk));
+    } else {
+        CFA_PROPAGATE(plan_tiled(ctx, h_rp.data(), a.n, 1, 8, W.tk));
+    }
+    W.tile_key = key;
+    W.graph.reset();
+    return CFA_OK;
+}
+
+static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* rep) {
+    PcgWork& W = work(ctx)->pcg;
+    const int n = a.n;
+    CFA_PROPAGATE(ensure_pcg_vectors(ctx, W, n));
+    CFA_PROPAGATE(plan_operator_tiles(ctx, W, a));
+    W.prepared.clear();
     // parameters
     CgState init{};
     init.tol = a.tol;
@@ -854,8 +1090,14 @@ static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* re
     }
     CFA_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     CgState h;
+    int h_err = 0;
     CFA_CUDA(cudaMemcpyAsync(&h, W.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(&h_err, W.err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (h_err) {
+        cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream);
+        return set_error(ctx, CFA_TIMEOUT, "a bounded wait of a tile pipeline timed out", __FILE__, __LINE__);
+    }
     float ms = 0.f;
     CFA_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     ctx->launches += extra_body * (long long)(h.iter + (h.status == CFA_BREAKDOWN ? 1 : 0));
@@ -1003,20 +1245,36 @@ cfa_status cfa_spmv_multi(cfa_ctx* ctx, int n, int nrhs, const int* rp, const in
     return CFA_OK;
 }
 
+cfa_status cfa_pressure_operator_prepare(cfa_ctx* ctx, int n, int nnz, const int* rp, const int* ci, const double* val,
+                                         const cfa_oss_operator* oss) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(n > 0 && nnz > 0 && rp && ci && val);
+    CFA_ARG(!oss || (oss->mesh && oss->d_oss_val && oss->d_inv_m && oss->mesh->n == n));
+    PcgWork& W = work(ctx)->pcg;
+    CFA_PROPAGATE(ensure_pcg_vectors(ctx, W, n));
+    PcgArgs a{n, nnz, rp, ci, val, nullptr, nullptr, oss, nullptr, 0, 0.0};
+    CFA_PROPAGATE(plan_operator_tiles(ctx, W, a));
+    W.prepared.clear();
+    if (!W.tiled) return CFA_OK;
+    if (oss) {
+        const double* o = oss->d_oss_val;
+        CFA_PROPAGATE(pack_tiled(ctx, rp, ci, o, o + (size_t)nnz, nullptr, W.tb));
+        CFA_PROPAGATE(pack_tiled(ctx, rp, ci, val, o + 2 * (size_t)nnz, o + 3 * (size_t)nnz, W.tk));
+    } else {
+        CFA_PROPAGATE(pack_tiled(ctx, rp, ci, val, nullptr, nullptr, W.tk));
+    }
+    W.prepared = operator_key(n, nnz, rp, ci, val, oss);
+    return CFA_OK;
+}
+
 cfa_status cfa_pressure_operator(cfa_ctx* ctx, int n, int nnz, const int* rp, const int* ci, const double* val,
                                  const cfa_oss_operator* oss, const double* x, double* y) {
     if (!ctx) return CFA_BAD_ARG;
     CFA_ARG(n > 0 && nnz > 0 && rp && ci && val && x && y);
     CFA_ARG(!oss || (oss->mesh && oss->d_oss_val && oss->d_inv_m && oss->mesh->n == n));
     PcgWork& W = work(ctx)->pcg;
-    if (n > W.cap) {
-        W.graph.reset();
-        for (DevBuf<double>* b : {&W.r, &W.z, &W.p, &W.pn, &W.q, &W.gx, &W.gy, &W.dinv}) CFA_CUDA(b->ensure(n));
-        CFA_CUDA(W.st.ensure(1));
-        CFA_CUDA(W.counter.ensure(1));
-        CFA_CUDA(cudaMemsetAsync(W.counter.p, 0, sizeof(unsigned int), ctx->stream));
-        W.cap = n;
-    }
+    CFA_PROPAGATE(ensure_pcg_vectors(ctx, W, n));
+    W.tiled = tiles_enabled() && !W.prepared.empty() && W.prepared == operator_key(n, nnz, rp, ci, val, oss);
     PcgArgs a{n, nnz, rp, ci, val, nullptr, nullptr, oss, nullptr, 0, 0.0};
     CondArg none{0, 0};
     CFA_PROPAGATE(pcg_operator(ctx, W, a, x, x, nullptr, W.pn.p, y, false, none, nullptr));
@@ -1031,14 +1289,8 @@ cfa_status cfa_oss_apply(cfa_ctx* ctx, const cfa_mesh* m, const double* oss_val,
     // out -= B^T M^-1 B in: pass 1 into the PCG scratch g, pass 2 with K = 0 contributions
     PcgWork& W = work(ctx)->pcg;
     const int n = m->n;
-    if (n > W.cap) {
-        W.graph.reset();
-        for (DevBuf<double>* b : {&W.r, &W.z, &W.p, &W.pn, &W.q, &W.gx, &W.gy, &W.dinv}) CFA_CUDA(b->ensure(n));
-        CFA_CUDA(W.st.ensure(1));
-        CFA_CUDA(W.counter.ensure(1));
-        CFA_CUDA(cudaMemsetAsync(W.counter.p, 0, sizeof(unsigned int), ctx->stream));
-        W.cap = n;
-    }
+    CFA_PROPAGATE(ensure_pcg_vectors(ctx, W, n));
+    W.tiled = false;
     DevBuf<double> zeroK;
     CFA_CUDA(zeroK.ensure(std::max(m->nnz, 1)));
     CFA_CUDA(cudaMemsetAsync(zeroK.p, 0, (size_t)m->nnz * sizeof(double), ctx->stream));

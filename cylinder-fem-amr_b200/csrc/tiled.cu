@@ -1,0 +1,106 @@
+// Tile planning and packing for the tile-streamed CSR kernels (tiled.cuh).
+#include <algorithm>
+#include <unordered_map>
+
+#include "tiled.cuh"
+
+namespace cfa {
+
+__global__ void k_pack_tiles(int ntiles, const long long* __restrict__ off, const int* __restrict__ row0,
+                             const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v0,
+                             const double* __restrict__ v1, const double* __restrict__ v2, int nvals, int vbytes,
+                             unsigned char* __restrict__ data) {
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int r0 = row0[t], nr = row0[t + 1] - r0;
+        const int e0 = rp[r0], ne = rp[r0 + nr] - e0;
+        unsigned char* ch = data + off[t];
+        int* rr = reinterpret_cast<int*>(ch);
+        for (int r = threadIdx.x; r <= nr; r += blockDim.x) rr[r] = rp[r0 + r] - e0;
+        int* cs = reinterpret_cast<int*>(ch + tile_ci_off(nr));
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) cs[e] = ci[e0 + e];
+        const double* src[3] = {v0, v1, v2};
+        for (int k = 0; k < nvals; ++k) {
+            unsigned char* vs = ch + tile_val_off(nr, ne, vbytes, k);
+            const double* sv = src[k] + e0;
+            if (vbytes == 8) {
+                double* d = reinterpret_cast<double*>(vs);
+                for (int e = threadIdx.x; e < ne; e += blockDim.x) d[e] = sv[e];
+            } else {
+                float* d = reinterpret_cast<float*>(vs);
+                for (int e = threadIdx.x; e < ne; e += blockDim.x) d[e] = (float)sv[e];
+            }
+        }
+    }
+}
+
+cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T) {
+    int tr = 256;
+    for (;;) {
+        long long mx = 0;
+        for (int r0 = 0; r0 < rows; r0 += tr) {
+            const int r1 = std::min(rows, r0 + tr);
+            mx = std::max(mx, tile_bytes(r1 - r0, h_rp[r1] - h_rp[r0], nvals, vbytes));
+        }
+        if (mx <= kTileBudget || tr <= 1) {
+            T.max_chunk = (int)mx;
+            break;
+        }
+        tr /= 2;
+    }
+    if (T.max_chunk > kTileBudget) return set_error(ctx, CFA_BAD_ARG, "matrix row too long for the tile budget", __FILE__, __LINE__);
+    T.rows = rows;
+    T.nnz = h_rp[rows];
+    T.nvals = nvals;
+    T.vbytes = vbytes;
+    T.tile_rows = tr;
+    T.ntiles = (rows + tr - 1) / tr;
+    std::vector<long long> off(T.ntiles + 1, 0);
+    std::vector<int> row0(T.ntiles + 1), e0(T.ntiles + 1);
+    for (int t = 0; t < T.ntiles; ++t) {
+        const int r0 = t * tr, r1 = std::min(rows, r0 + tr);
+        row0[t] = r0;
+        e0[t] = h_rp[r0];
+        off[t + 1] = off[t] + tile_bytes(r1 - r0, h_rp[r1] - h_rp[r0], nvals, vbytes);
+    }
+    row0[T.ntiles] = rows;
+    e0[T.ntiles] = h_rp[rows];
+    T.bytes = off[T.ntiles];
+    CFA_CUDA(T.data.ensure(T.bytes + 16));
+    CFA_CUDA(T.off.ensure(T.ntiles + 1));
+    CFA_CUDA(T.row0.ensure(T.ntiles + 1));
+    CFA_CUDA(T.e0.ensure(T.ntiles + 1));
+    CFA_CUDA(cudaMemcpyAsync(T.off.p, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(T.row0.p, row0.data(), row0.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(T.e0.p, e0.data(), e0.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    return CFA_OK;
+}
+
+cfa_status pack_tiled(cfa_ctx* ctx, const int* d_rp, const int* d_ci, const double* v0, const double* v1,
+                      const double* v2, TiledCsr& T) {
+    if (T.ntiles == 0) return CFA_OK;
+    const int grid = std::min(T.ntiles, 16 * ctx->num_sms);
+    CFA_LAUNCH(ctx, k_pack_tiles, grid, kTileThreads, 0, T.ntiles, (const long long*)T.off.p, (const int*)T.row0.p,
+               d_rp, d_ci, v0, v1, v2, T.nvals, T.vbytes, T.data.p);
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+void allow_tile_kernel(const void* kernel) {
+    static std::unordered_map<const void*, bool> done;
+    if (done[kernel]) return;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kTileBudget + 64);
+    done[kernel] = true;
+}
+
+TileLaunch tile_launch(const cfa_ctx* ctx, const TiledCsr& T, const void*) {
+    TileLaunch L;
+    L.smem = (int)(2 * align16(T.max_chunk) + 16);
+    const int per_sm = std::max(1, std::min(2048 / kTileThreads, (227 * 1024 - 1024) / std::max(L.smem + 64, 1)));
+    L.grid = std::max(1, std::min(T.ntiles, per_sm * ctx->num_sms));
+    L.tpr = std::max(1, kTileThreads / std::max(T.tile_rows, 1));
+    if (L.tpr > 32) L.tpr = 32;
+    return L;
+}
+
+}  // namespace cfa

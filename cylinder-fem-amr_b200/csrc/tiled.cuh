@@ -1,0 +1,175 @@
+// Tile-streamed CSR: the B200 data path of the bandwidth-bound row kernels.
+//
+// A CSR matrix (with one or more value arrays on the same pattern) is repacked into row tiles.
+// Each tile is one contiguous, 16-byte aligned chunk:
+//     [ row offsets relative to the tile (rows + 1 int32) | column indices (int32) |
+//       value array 0 | value array 1 | ... ]                    (every section 16-byte padded)
+// so a whole tile moves with ONE bulk asynchronous copy (cp.async.bulk, the TMA's 1-D mode)
+// into shared memory. Persistent CTAs walk the tiles (tile = blockIdx.x + k gridDim.x) through a
+// two-stage pipeline: the copy of tile k+1 is in flight while tile k is computed from shared
+// memory; an mbarrier with transaction counting signals arrival. Every wait is bounded: on
+// timeout the kernel records an error code, waits (bounded) for its other copy, and returns.
+// Matrix bytes are read once, fully coalesced, at exactly the algorithmic volume (plus 16-byte
+// padding per section); only the vector gathers x[col] go through L1/L2.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace cfa {
+
+constexpr int kTileThreads = 256;
+constexpr int kTileBudget = 48 * 1024;     // max bytes of one tile (two stages per CTA)
+constexpr unsigned kWaitLimit = 1u << 22;  // bounded mbarrier waits (each try_wait itself blocks a while)
+
+__host__ __device__ inline long long align16(long long b) { return (b + 15) & ~15LL; }
+
+struct TileView {
+    const unsigned char* data = nullptr;
+    const long long* off = nullptr;   // [ntiles + 1] byte offset of each tile chunk
+    const int* row0 = nullptr;        // [ntiles + 1] first row of each tile
+    int ntiles = 0, rows = 0, nvals = 0, vbytes = 8;
+    int max_chunk = 0;                // bytes
+    int* err = nullptr;               // device error word (timeout)
+};
+
+// Host-side description + device buffers of a tiled matrix.
+struct TiledCsr {
+    int rows = 0, nnz = 0, ntiles = 0, nvals = 0, vbytes = 8, tile_rows = 0, max_chunk = 0;
+    long long bytes = 0;
+    DevBuf<unsigned char> data;
+    DevBuf<long long> off;
+    DevBuf<int> row0;
+    DevBuf<int> e0;                   // [ntiles + 1] first CSR entry of each tile
+    TileView view(int* err) const {
+        TileView v;
+        v.data = data.p; v.off = off.p; v.row0 = row0.p; v.ntiles = ntiles; v.rows = rows;
+        v.nvals = nvals; v.vbytes = vbytes; v.max_chunk = max_chunk; v.err = err;
+        return v;
+    }
+};
+
+// Chunk geometry of a tile with nr rows and ne entries
+__host__ __device__ inline long long tile_ci_off(int nr) { return align16(4LL * (nr + 1)); }
+__host__ __device__ inline long long tile_val_off(int nr, int ne, int vbytes, int k) {
+    return tile_ci_off(nr) + align16(4LL * ne) + k * align16((long long)vbytes * ne);
+}
+__host__ __device__ inline long long tile_bytes(int nr, int ne, int nvals, int vbytes) {
+    return tile_val_off(nr, ne, vbytes, nvals);
+}
+
+// Plans the tiles from the host row pointer: tile_rows = 256 rows, halved until every tile fits
+// the budget. Allocates the device buffers (the pattern and values are packed by pack_tiled).
+cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T);
+
+// Packs pattern + values (FP64 sources; converted to float when vbytes == 4) into T.
+// vals[k] may be NULL for k >= nvals. Asynchronous.
+cfa_status pack_tiled(cfa_ctx* ctx, const int* d_rp, const int* d_ci, const double* v0, const double* v1,
+                      const double* v2, TiledCsr& T);
+
+// ---------------------------------------------------------------------------------------------
+// device side: mbarrier + bulk copy
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
+    for (unsigned it = 0; it < kWaitLimit; ++it)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+
+// Issues the copy of tile t into stage s (one thread).
+__device__ __forceinline__ void tile_issue(const TileView& tv, int t, unsigned char* dst, uint64_t* bar) {
+    const long long o0 = tv.off[t], o1 = tv.off[t + 1];
+    const unsigned bytes = (unsigned)(o1 - o0);
+    mbar_expect_tx(bar, bytes);
+    bulk_g2s(dst, tv.data + o0, bytes, bar);
+}
+
+// Runs body(tile, row0, nrows, chunk) for every tile of this CTA (all threads call it; the
+// body must not return early for some threads and must synchronise nothing itself).
+// Dynamic shared memory: 2 * max_chunk bytes, 16-aligned. Returns false on a timeout.
+template <class Body>
+__device__ __forceinline__ bool tile_loop(const TileView& tv, unsigned char* smem, Body&& body) {
+    __shared__ uint64_t bar[2];
+    __shared__ int abort_flag;
+    unsigned char* buf0 = smem;
+    unsigned char* buf1 = smem + align16(tv.max_chunk);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+        abort_flag = 0;
+    }
+    __syncthreads();
+    int t = blockIdx.x;
+    if (t >= tv.ntiles) return true;
+    if (threadIdx.x == 0) tile_issue(tv, t, buf0, &bar[0]);
+    unsigned phase[2] = {0u, 0u};
+    for (int k = 0; t < tv.ntiles; ++k, t += gridDim.x) {
+        const int s = k & 1;
+        const int next = t + gridDim.x;
+        if (threadIdx.x == 0 && next < tv.ntiles) {
+            fence_proxy_async();
+            tile_issue(tv, next, s ? buf0 : buf1, &bar[s ^ 1]);
+        }
+        if (!mbar_wait(&bar[s], phase[s])) {
+            atomicExch(tv.err, (int)CFA_TIMEOUT);
+            abort_flag = 1;
+        }
+        __syncthreads();
+        if (abort_flag) {
+            // let the other stage's copy (if any) land before the CTA exits, bounded
+            if (next < tv.ntiles) mbar_wait(&bar[s ^ 1], phase[s ^ 1]);
+            return false;
+        }
+        phase[s] ^= 1u;
+        const int r0 = tv.row0[t];
+        body(t, r0, tv.row0[t + 1] - r0, s ? buf1 : buf0);
+        __syncthreads();
+    }
+    return true;
+}
+
+// Launch shape of a tile kernel: persistent grid limited by shared memory (two stages).
+struct TileLaunch {
+    int grid = 1, smem = 0, tpr = 1;
+};
+TileLaunch tile_launch(const cfa_ctx* ctx, const TiledCsr& T, const void* kernel);
+// Raises the kernel's dynamic shared memory limit to two tiles of the budget (once per kernel;
+// call outside stream capture).
+void allow_tile_kernel(const void* kernel);
+
+}  // namespace cfa

@@ -258,8 +258,15 @@ cfa_status cfa_pcg_solve(cfa_ctx* ctx, int n, const int* d_row_ptr, const int* d
                          const cfa_oss_operator* oss, cfa_amg* amg, const cfa_solve_opts* opts,
                          cfa_solve_report* report);
 
+/* Snapshots the pressure operator's current values into the context's tile-streamed layout
+ * (the layout cfa_pcg_solve streams each iteration; one synchronisation when the pattern is
+ * new). Call again after the values change. */
+cfa_status cfa_pressure_operator_prepare(cfa_ctx* ctx, int n, int nnz, const int* d_row_ptr,
+                                         const int* d_col_ind, const double* d_val,
+                                         const cfa_oss_operator* oss);
 /* The pressure operator alone (operator of cfa_pcg_solve): y = K x (- B^T M^-1 B x).
- * Asynchronous (nnz passed by the caller). */
+ * Asynchronous (nnz passed by the caller). Uses the tile-streamed kernels when the same operator
+ * was prepared, the row kernels otherwise. */
 cfa_status cfa_pressure_operator(cfa_ctx* ctx, int n, int nnz, const int* d_row_ptr,
                                  const int* d_col_ind, const double* d_val,
                                  const cfa_oss_operator* oss, const double* d_x, double* d_y);
