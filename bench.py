@@ -200,7 +200,7 @@ def run_ours(args, rank, world):
         e2e_ms = e2e_total / args.steps
         op_ms = time_operator(cfa, st, 20, flush) if prec == cfa.FP64 else None
         res[prec_name] = dict(step_ms=step_ms, setup_ms=setup_ms, e2e_ms=e2e_ms, launches=launches,
-                              clocks=clk.summary(), report=reports[-1], op_ms=op_ms, levels=st.amg.num_levels(),
+                              clocks=clk.summary(), report=reports[-1], op_ms=op_ms, levels=st.amg.num_levels(), phases=st.amg.phase_ms,
                               colours=st.ilu.n_colours, nnz=st.nnz, n=st.n)
         del st
     return m, res
@@ -342,7 +342,8 @@ def main():
                    "iterations_mixed": {"u": mixed["report"]["it_u"], "v": mixed["report"]["it_v"], "p": mixed["report"]["it_p"]},
                    "iterations_fp64": {"u": fp64["report"]["it_u"], "v": fp64["report"]["it_v"], "p": fp64["report"]["it_p"]},
                    "converged": mixed["report"]["conv"] + fp64["report"]["conv"],
-                   "amg_levels": mixed["levels"], "ilu_colours": mixed["colours"]},
+                   "amg_levels": mixed["levels"], "ilu_colours": mixed["colours"],
+                   "amg_setup_phases_ms": {k: round(v, 2) for k, v in mixed["phases"].items()}},
         "e2e": {"value": round(e2e, 4), "unit": "ms/step", "h2d_bytes_per_step": 3 * 8 * n, "d2h_bytes_per_step": 3 * 8 * n},
         "gpu_launches": int(mixed["launches"]),
         "roofline": {"bound": "hbm", "kernel": "pressure operator K + OSS (k_op_b + k_op_k), FP64",

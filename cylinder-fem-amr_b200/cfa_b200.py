@@ -400,6 +400,13 @@ class AmgPreconditioner:
                     P=(_dev_view(prp, rows + 1, torch.int32), _dev_view(pci, pnnz, torch.int32), _dev_view(pv, pnnz, torch.float64)),
                     R=(_dev_view(rrp, pcols + 1, torch.int32), _dev_view(rci, rnnz, torch.int32), _dev_view(rv, rnnz, torch.float64)))
 
+    @property
+    def phase_ms(self):
+        out = np.zeros(8)
+        lib().cfa_amg_phases(self.h, ptr(out))
+        return dict(zip(("copy", "rho", "aggregation", "smoothing", "transpose", "galerkin", "tiles", "coarse"),
+                        out.tolist()))
+
     def coarse_inverse(self):
         import torch
         p = C.c_void_p()

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <type_traits>
 
 #include "amg.cuh"
@@ -355,6 +356,73 @@ __global__ void k_vc_dense(int cn, const double* __restrict__ inv, const B* __re
 }
 
 // ---------------------------------------------------------------------------------------------
+// tile-streamed V-cycle kernel (tiled.cuh): one kernel for the five row operations
+// ---------------------------------------------------------------------------------------------
+enum VcOp { VC_PRE = 0, VC_JAC = 1, VC_RES = 2, VC_SPMV = 3, VC_ADD = 4 };
+
+template <int TPR, int OP, class T, class B, class O>
+__global__ void __launch_bounds__(kTileThreads)
+k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b, const T* __restrict__ x,
+      O* __restrict__ y, const int* __restrict__ done) {
+    if (done && *done) return;
+    extern __shared__ __align__(128) unsigned char tsmem[];
+    tile_loop(tv, tsmem, [&](int, int r0, int nr, const unsigned char* ch) {
+        const int* rr = reinterpret_cast<const int*>(ch);
+        const int ne = rr[nr];
+        const int* cs = reinterpret_cast<const int*>(ch + tile_ci_off(nr));
+        const T* vv = reinterpret_cast<const T*>(ch + tile_val_off(nr, ne, (int)sizeof(T), 0));
+        for (int base = 0; base < nr; base += kTileThreads / TPR) {
+            const int lr = base + (int)threadIdx.x / TPR, lane = threadIdx.x % TPR;
+            const bool valid = lr < nr;
+            T s = (T)0;
+            if (valid)
+                for (int e = rr[lr] + lane; e < rr[lr + 1]; e += TPR) {
+                    const int j = cs[e];
+                    if (OP == VC_PRE) s += vv[e] * (omega * dinv[j] * (T)b[j]);
+                    else s += vv[e] * x[j];
+                }
+#pragma unroll
+            for (int o = TPR / 2; o > 0; o /= 2) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
+            if (valid && lane == 0) {
+                const int row = r0 + lr;
+                if (OP == VC_PRE) {
+                    const T x0 = omega * dinv[row] * (T)b[row];
+                    y[row] = (O)(x0 + omega * dinv[row] * ((T)b[row] - s));
+                } else if (OP == VC_JAC) {
+                    y[row] = (O)(x[row] + omega * dinv[row] * ((T)b[row] - s));
+                } else if (OP == VC_RES) {
+                    y[row] = (O)((T)b[row] - s);
+                } else if (OP == VC_SPMV) {
+                    y[row] = (O)s;
+                } else {
+                    y[row] = (O)((T)y[row] + s);
+                }
+            }
+        }
+    });
+}
+
+// Launches (or, dry, only prepares) one tiled V-cycle operation.
+template <int OP, class T, class B, class O>
+static void vct(cfa_ctx* ctx, bool dry, const TiledCsr& M, int* err, const T* dinv, T omega, const B* b, const T* x,
+                O* y, const int* done) {
+    const int tpr = M.tile_rows >= kTileThreads ? 1 : std::min(32, kTileThreads / std::max(M.tile_rows, 1));
+    const TileView tv = M.view(err);
+    const TileLaunch L = tile_launch(ctx, M, nullptr);
+    switch (tpr) {
+#define VCT_CASE(N)                                                                                     \
+    case N:                                                                                             \
+        if (dry) allow_tile_kernel((const void*)k_vct<N, OP, T, B, O>);                                 \
+        else CFA_LAUNCH(ctx, (k_vct<N, OP, T, B, O>), L.grid, kTileThreads, L.smem, tv, dinv, omega, b, x, y, done); \
+        break;
+        VCT_CASE(1) VCT_CASE(2) VCT_CASE(4) VCT_CASE(8) VCT_CASE(16)
+        default:
+        VCT_CASE(32)
+#undef VCT_CASE
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // launch helpers with the TPR dispatch
 // ---------------------------------------------------------------------------------------------
 #define CFA_TPR_SWITCH(tpr, ...)                                                               \
@@ -448,10 +516,60 @@ static void vcycle_level(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     }
 }
 
+// V-cycle on the tile-streamed kernels (dry: prepare the kernels only, no launches)
+template <class T, class B>
+static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* z, const int* done, bool dry) {
+    AmgLevel& L = amg->levels[l];
+    LevelView<T> V = view<T>(L);
+    const int s = amg->opts.smooth_steps;
+    int* err = amg->err.p;
+    const T omega = V.omega;
+    T* x = V.x;
+    T* t = V.t;
+    if (s >= 2) {
+        vct<VC_PRE, T, B, T>(ctx, dry, L.tA, err, V.dinv, omega, b, (const T*)nullptr, x, done);
+    } else if (!dry) {
+        CFA_TPR_SWITCH(L.A.tpr, CFA_LAUNCH(ctx, (k_vc_pre<TPR, T, B>), row_grid(ctx, L.A.rows, L.A.tpr), kThreads, 0,
+                                           L.A.rows, V.Arp, V.Aci, V.Av, V.dinv, V.omega, b, 0, V.x, done));
+    }
+    for (int k = 2; k < s; ++k) {
+        vct<VC_JAC, T, B, T>(ctx, dry, L.tA, err, V.dinv, omega, b, (const T*)x, t, done);
+        std::swap(x, t);
+    }
+    vct<VC_RES, T, B, T>(ctx, dry, L.tA, err, V.dinv, omega, b, (const T*)x, V.r, done);
+    const bool last = l + 1 == (int)amg->levels.size();
+    T* cb = last ? (std::is_same<T, double>::value ? (T*)amg->cb64.p : (T*)amg->cb32.p) : view<T>(amg->levels[l + 1]).b;
+    vct<VC_SPMV, T, T, T>(ctx, dry, L.tR, err, V.dinv, omega, (const T*)nullptr, (const T*)V.r, cb, done);
+    const T* cx;
+    if (!last) {
+        vcycle_tiled<T, T>(ctx, amg, l + 1, cb, nullptr, done, dry);
+        cx = view<T>(amg->levels[l + 1]).x;
+    } else {
+        T* dst = std::is_same<T, double>::value ? (T*)amg->cx64.p : (T*)amg->cx32.p;
+        if (!dry)
+            CFA_LAUNCH(ctx, (k_vc_dense<T, T>), ceil_div((long long)amg->coarse_n * 32, kThreads), kThreads, 0,
+                       amg->coarse_n, amg->coarse_inv.p, (const T*)cb, dst, done);
+        cx = dst;
+    }
+    vct<VC_ADD, T, T, T>(ctx, dry, L.tP, err, V.dinv, omega, (const T*)nullptr, cx, x, done);
+    for (int k = 0; k < s; ++k) {
+        if (l == 0 && k == s - 1) {
+            vct<VC_JAC, T, B, double>(ctx, dry, L.tA, err, V.dinv, omega, b, (const T*)x, z, done);
+        } else {
+            vct<VC_JAC, T, B, T>(ctx, dry, L.tA, err, V.dinv, omega, b, (const T*)x, t, done);
+            std::swap(x, t);
+        }
+    }
+    if (l > 0 && x != V.x && !dry) cudaMemcpyAsync(V.x, x, (size_t)L.A.rows * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream);
+}
+
 cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done) {
     if (amg->levels.empty()) {
         CFA_LAUNCH(ctx, (k_vc_dense<double, double>), ceil_div((long long)amg->coarse_n * 32, kThreads), kThreads, 0,
                    amg->coarse_n, amg->coarse_inv.p, r, z, done);
+    } else if (amg->tiled) {
+        if (amg->opts.precision == CFA_MIXED) vcycle_tiled<float, double>(ctx, amg, 0, r, z, done, false);
+        else vcycle_tiled<double, double>(ctx, amg, 0, r, z, done, false);
     } else if (amg->opts.precision == CFA_MIXED) {
         vcycle_level<float, double>(ctx, amg, 0, r, z, done);
     } else {
@@ -633,11 +751,19 @@ static cfa_status level_vectors(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int n) 
 static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* d_rp, const int* d_ci,
                             const double* d_v) {
     const auto t0 = std::chrono::steady_clock::now();
+    auto tp = t0;
+    auto phase = [&](int ph) {
+        cudaStreamSynchronize(ctx->stream);
+        const auto now = std::chrono::steady_clock::now();
+        amg->phase_ms[ph] += std::chrono::duration<double, std::milli>(now - tp).count();
+        tp = now;
+    };
     const cfa_amg_opts& o = amg->opts;
     amg->levels.clear();
     amg->version = next_uid();
     DCsr A;
     CFA_PROPAGATE(copy_csr(ctx, n, nnz, d_rp, d_ci, d_v, A));
+    phase(0);
     while (A.rows > o.coarse_target && (int)amg->levels.size() < o.max_levels - 1) {
         const int m = A.rows;
         AmgLevel L;
@@ -646,6 +772,7 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
         double rho = 1.0;
         CFA_PROPAGATE(spectral_radius(ctx, amg, A, L.dinv.p, &rho));
         const double omega = 4.0 / (3.0 * rho);
+        phase(1);
         // strength on the device, aggregation on the host
         DevBuf<unsigned char> strong;
         CFA_CUDA(strong.ensure(std::max(A.nnz, 1)));
@@ -674,6 +801,7 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
         CFA_CUDA(cudaMemcpyAsync(L.agg.p, agg.data(), m * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
         CFA_CUDA(cudaMemcpyAsync(d_p0v.p, p0v.data(), m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
         CFA_CUDA(cudaMemcpyAsync(d_p0rp.p, p0rp.data(), (m + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        phase(2);
         // AP0 = A P0, then P = P0 - omega D^-1 A P0
         DCsr AP0;
         CFA_PROPAGATE(spgemm(ctx, m, na, A.rp.p, A.ci.p, A.v.p, d_p0rp.p, L.agg.p, d_p0v.p, AP0));
@@ -695,11 +823,14 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
         CFA_LAUNCH(ctx, k_p_rows, ceil_div(m, kThreads), kThreads, 0, m, AP0.rp.p, AP0.ci.p, AP0.v.p, L.agg.p, d_p0v.p,
                    L.dinv.p, omega, L.P.rp.p, L.P.ci.p, L.P.v.p, cnt.p);
         CFA_CHECK_LAUNCH();
+        phase(3);
         // R = P^T, A_c = R (A P)
         CFA_PROPAGATE(transpose(ctx, L.P, L.R));
+        phase(4);
         DCsr AP, Ac;
         CFA_PROPAGATE(spgemm(ctx, m, na, A.rp.p, A.ci.p, A.v.p, L.P.rp.p, L.P.ci.p, L.P.v.p, AP));
         CFA_PROPAGATE(spgemm(ctx, na, na, L.R.rp.p, L.R.ci.p, L.R.v.p, AP.rp.p, AP.ci.p, AP.v.p, Ac));
+        phase(5);
         L.omega = omega;
         L.A = std::move(A);
         CFA_PROPAGATE(level_vectors(ctx, amg, L, m));
@@ -721,6 +852,7 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
     CFA_CHECK_LAUNCH();
     int h_err = 0;
     CFA_CUDA(cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    phase(7);
     CFA_CUDA(amg->cb64.ensure(cn + 1));
     CFA_CUDA(amg->cx64.ensure(cn + 1));
     if (o.precision == CFA_MIXED) {
@@ -742,6 +874,29 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
         }
     }
     CFA_CHECK_LAUNCH();
+    // tile-streamed copies of every level's A, P, R in the hierarchy precision
+    const char* te = std::getenv("CFA_TILES");
+    amg->tiled = !(te && te[0] == '0') && !amg->levels.empty();
+    if (amg->tiled) {
+        CFA_CUDA(amg->err.ensure(1));
+        CFA_CUDA(cudaMemsetAsync(amg->err.p, 0, sizeof(int), ctx->stream));
+        const int vb = o.precision == CFA_MIXED ? 4 : 8;
+        for (AmgLevel& L : amg->levels) {
+            for (DCsr* M : {&L.A, &L.P, &L.R}) {
+                TiledCsr& T = M == &L.A ? L.tA : M == &L.P ? L.tP : L.tR;
+                std::vector<int> h_rp(M->rows + 1);
+                CFA_CUDA(cudaMemcpyAsync(h_rp.data(), M->rp.p, (M->rows + 1) * sizeof(int), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+                CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+                CFA_PROPAGATE(plan_tiled(ctx, h_rp.data(), M->rows, 1, vb, T));
+                CFA_PROPAGATE(pack_tiled(ctx, M->rp.p, M->ci.p, M->v.p, nullptr, nullptr, T));
+            }
+        }
+        // raise the kernels' shared-memory limits now, outside any stream capture
+        if (o.precision == CFA_MIXED) vcycle_tiled<float, double>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
+        else vcycle_tiled<double, double>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
+    }
+    phase(6);
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     amg->setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (h_err) return set_error(ctx, CFA_COARSE_NOT_SPD, "coarsest AMG operator not SPD", __FILE__, __LINE__);
@@ -818,6 +973,12 @@ cfa_status cfa_amg_level(const cfa_amg* amg, int l, int* info, const int** agg, 
     if (Rci) *Rci = L.R.ci.p;
     if (Rv) *Rv = L.R.v.p;
     if (omega) *omega = L.omega;
+    return CFA_OK;
+}
+
+cfa_status cfa_amg_phases(const cfa_amg* amg, double* ms8) {
+    if (!amg || !ms8) return CFA_BAD_ARG;
+    for (int k = 0; k < 8; ++k) ms8[k] = amg->phase_ms[k];
     return CFA_OK;
 }
 

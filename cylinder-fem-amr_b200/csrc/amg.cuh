@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "internal.cuh"
+#include "tiled.cuh"
 
 namespace cfa {
 
@@ -17,6 +18,7 @@ struct DCsr {
 
 struct AmgLevel {
     DCsr A, P, R;
+    TiledCsr tA, tP, tR;           // tile-streamed copies in the hierarchy precision
     DevBuf<double> dinv;
     DevBuf<float> dinv32;
     double omega = 0.0;
@@ -39,6 +41,12 @@ struct cfa_amg {
     long long version = 0;               // process-unique, renewed by every setup (graph caches key on it)
     std::vector<double> host_x0;         // 1 + 0.1 sin(1 + i), the power-iteration start vector
     cfa::DevBuf<double> x0;
+    bool tiled = false;                  // V-cycle on the tile-streamed kernels
+    // accumulated setup phases [ms] (the reference's phase_ms[], src/cfa/linalg.cuh:970-982):
+    // 0 copy, 1 D^-1 + rho, 2 strength + aggregation, 3 P smoothing, 4 transpose, 5 Galerkin,
+    // 6 tile packing, 7 coarse inverse
+    double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    cfa::DevBuf<int> err;                // tile pipeline error word
 };
 
 namespace cfa {

@@ -191,6 +191,7 @@ k_opt_b(TileView tv, const double* __restrict__ inv_m, const double* __restrict_
             const bool valid = lr < nr;
             double sx = 0.0, sy = 0.0;
             if (valid)
+#pragma unroll 4
                 for (int e = rr[lr] + lane; e < rr[lr + 1]; e += TPR) {
                     const int j = cs[e];
                     const double pj = fuse ? z[j] + beta * p[j] : z[j];
@@ -235,6 +236,7 @@ k_opt_k(TileView tv, const int* __restrict__ tag, OutletBc bc, const double* __r
             const bool valid = lr < nr;
             double s = 0.0, so = 0.0;
             if (valid)
+#pragma unroll 4
                 for (int e = rr[lr] + lane; e < rr[lr + 1]; e += TPR) {
                     const int j = cs[e];
                     const double pj = FUSEP ? (fuse ? z[j] + beta * p[j] : z[j]) : pn_buf[j];
@@ -667,6 +669,110 @@ k_b2_xr(int n, double* __restrict__ xu, double* __restrict__ xv, const double* _
     }
 }
 
+// ---- tile-streamed forms of the BiCGSTAB2 SpMV + dot kernels (tiles of {A}, FP64) ----
+// MODE 0: init  (x -> v = A x, r = b - v, r0 = p = r, v = 0, r.r)
+// MODE 1: v = A phat, r0.v -> alpha
+// MODE 2: t = A shat, s.s t.t t.s -> omega / s-stop
+template <int TPR, int MODE>
+__global__ void __launch_bounds__(kTileThreads)
+k_b2t(TileView tv, int n, const double* __restrict__ xu, const double* __restrict__ xv, const double* __restrict__ bu,
+      const double* __restrict__ bv, const double* __restrict__ in, const double* __restrict__ aux,
+      double* __restrict__ out, double* __restrict__ r, double* __restrict__ r0, double* __restrict__ p,
+      B2State* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+    if (MODE != 0 && st->done) return;
+    extern __shared__ __align__(128) unsigned char tsmem[];
+    constexpr int NV = MODE == 2 ? 6 : 2;
+    __shared__ double sh[NV * kWarps];
+    double acc[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+    const double* x0 = MODE == 0 ? xu : in;
+    const double* x1 = MODE == 0 ? xv : in + n;
+    tile_loop(tv, tsmem, [&](int, int r0_, int nr, const unsigned char* ch) {
+        const int* rr = reinterpret_cast<const int*>(ch);
+        const int ne = rr[nr];
+        const int* cs = reinterpret_cast<const int*>(ch + tile_ci_off(nr));
+        const double* av = reinterpret_cast<const double*>(ch + tile_val_off(nr, ne, 8, 0));
+        for (int base = 0; base < nr; base += kTileThreads / TPR) {
+            const int lr = base + (int)threadIdx.x / TPR, lane = threadIdx.x % TPR;
+            const bool valid = lr < nr;
+            double su = 0.0, sv = 0.0;
+            if (valid)
+#pragma unroll 4
+                for (int e = rr[lr] + lane; e < rr[lr + 1]; e += TPR) {
+                    const double a = av[e];
+                    const int j = cs[e];
+                    su += a * x0[j];
+                    sv += a * x1[j];
+                }
+            su = group_reduce<TPR>(su);
+            sv = group_reduce<TPR>(sv);
+            if (valid && lane == 0) {
+                const int row = r0_ + lr;
+                if (MODE == 0) {
+                    const double ru = bu[row] - 1.0 * su, rv = bv[row] - 1.0 * sv;
+                    r[row] = ru; r[n + row] = rv;
+                    r0[row] = ru; r0[n + row] = rv;
+                    p[row] = ru; p[n + row] = rv;
+                    out[row] = 0.0; out[n + row] = 0.0;
+                    acc[0] += ru * ru;
+                    acc[1] += rv * rv;
+                } else if (MODE == 1) {
+                    out[row] = su;
+                    out[n + row] = sv;
+                    acc[0] += aux[row] * su;
+                    acc[1] += aux[n + row] * sv;
+                } else {
+                    out[row] = su;
+                    out[n + row] = sv;
+                    const double s0 = aux[row], s1 = aux[n + row];
+                    acc[0] += s0 * s0; acc[1] += s1 * s1;
+                    acc[2 % NV] += su * su; acc[3 % NV] += sv * sv;
+                    acc[4 % NV] += su * s0; acc[5 % NV] += sv * s1;
+                }
+            }
+        }
+    });
+    block_sum<NV>(acc, sh);
+    if (!publish_partials<NV>(acc, part, counter)) return;
+    reduce_partials<NV>(acc, part, counter, sh);
+    if (threadIdx.x != 0) return;
+    if (MODE == 0) {
+        for (int c = 0; c < 2; ++c) {
+            st->rn0[c] = sqrt(acc[c]);
+            st->rho[c] = acc[c];
+            st->bd[c] = 1.0e-30 * st->rn0[c] * st->rn0[c] + 1.0e-300;
+            st->rho_old[c] = 1.0; st->alpha[c] = 1.0; st->omega[c] = 1.0;
+            st->iters[c] = 0; st->conv[c] = 1; st->rel[c] = 0.0; st->s_done[c] = 0;
+            st->active[c] = st->rn0[c] >= 1.0e-13;
+        }
+        st->iter = 0;
+        st->done = 0;
+        set_cond(cond, 1);
+        b2_begin_iteration(st, cond);
+    } else if (MODE == 1) {
+        const int iter = st->iter;
+        for (int c = 0; c < 2; ++c) {
+            st->ca[c] = 0.0;
+            if (st->active[c] && fabs(acc[c]) < st->bd[c]) b2_stop(st, c, iter, 0);
+            if (st->active[c]) { st->alpha[c] = st->rho[c] / acc[c]; st->ca[c] = st->alpha[c]; }
+        }
+        if (!(st->active[0] || st->active[1])) { st->done = 1; set_cond(cond, 0); }
+    } else {
+        for (int c = 0; c < 2; ++c) {
+            st->a1[c] = 0.0; st->a2[c] = 0.0; st->cw[c] = 0.0; st->s_done[c] = 0;
+            if (!st->active[c]) continue;
+            st->a1[c] = st->alpha[c];
+            const double s_norm = sqrt(acc[c]);
+            if (s_norm < st->tol * st->rn0[c] || s_norm < 1.0e-11) { st->s_done[c] = 1; continue; }
+            const double tt = acc[2 + c];
+            st->omega[c] = (tt > st->bd[c]) ? (acc[4 + c] / tt) : 0.0;
+            st->a2[c] = st->omega[c];
+            st->cw[c] = st->omega[c];
+        }
+    }
+}
+
 // =============================================================================================
 // Jacobi BiCGSTAB (GpuLinearSolver::solve_bicgstab, :261-347), host-driven like the reference
 // but with the fused dot kernels (kept simple: it is the non-default solver and a test oracle).
@@ -756,6 +862,10 @@ struct B2Work {
     int cap = 0;
     DevBuf<double> r, r0, p, v, s, t, phat, shat;
     DevBuf<B2State> st;
+    TiledCsr tA;                     // tile-streamed copy of the momentum matrix (packed per solve)
+    std::vector<const void*> tile_key;
+    bool tiled = false;
+    DevBuf<int> err;
     DevBuf<double> part;
     DevBuf<unsigned int> counter;
     GraphCache graph;
@@ -1094,7 +1204,12 @@ static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* re
     CFA_CUDA(cudaMemcpyAsync(&h, W.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaMemcpyAsync(&h_err, W.err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (h_err) {
+    int h_amg_err = 0;
+    if (a.amg && a.amg->err.p) {
+        CFA_CUDA(cudaMemcpy(&h_amg_err, a.amg->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h_amg_err) cudaMemsetAsync(a.amg->err.p, 0, sizeof(int), ctx->stream);
+    }
+    if (h_err || h_amg_err) {
         cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream);
         return set_error(ctx, CFA_TIMEOUT, "a bounded wait of a tile pipeline timed out", __FILE__, __LINE__);
     }
@@ -1128,7 +1243,55 @@ struct B2Args {
     double tol;
 };
 
+template <int MODE>
+static void launch_b2t(cfa_ctx* ctx, B2Work& W, const B2Args& a, const double* in, const double* aux, double* out,
+                       CondArg cond) {
+    const TileView tv = W.tA.view(W.err.p);
+    const TileLaunch L = tile_launch(ctx, W.tA, nullptr);
+    TILE_TPR_SWITCH(W.tA.tile_rows >= 256 ? 1 : std::min(32, kTileThreads / W.tA.tile_rows),
+        CFA_LAUNCH(ctx, (k_b2t<TPR, MODE>), L.grid, kTileThreads, L.smem, tv, a.n, (const double*)a.xu,
+                   (const double*)a.xv, a.bu, a.bv, in, aux, out, W.r.p, W.r0.p, W.p.p, W.st.p, W.part.p, W.counter.p,
+                   cond));
+}
+
+template <int TPR>
+static void allow_b2_tpr() {
+    allow_tile_kernel((const void*)k_b2t<TPR, 0>);
+    allow_tile_kernel((const void*)k_b2t<TPR, 1>);
+    allow_tile_kernel((const void*)k_b2t<TPR, 2>);
+}
+
+static cfa_status plan_b2_tiles(cfa_ctx* ctx, B2Work& W, const B2Args& a) {
+    const char* e = std::getenv("CFA_TILES");
+    W.tiled = !(e && e[0] == '0');
+    if (!W.tiled) return CFA_OK;
+    static bool allowed = false;
+    if (!allowed) {
+        allow_b2_tpr<1>(); allow_b2_tpr<2>(); allow_b2_tpr<4>(); allow_b2_tpr<8>(); allow_b2_tpr<16>(); allow_b2_tpr<32>();
+        allowed = true;
+    }
+    if (!W.err.p) {
+        CFA_CUDA(W.err.ensure(1));
+        CFA_CUDA(cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream));
+    }
+    std::vector<const void*> key = {a.rp, a.ci, (const void*)(intptr_t)a.n, (const void*)(intptr_t)a.nnz};
+    if (key == W.tile_key) return CFA_OK;
+    std::vector<int> h_rp(a.n + 1);
+    CFA_CUDA(cudaMemcpyAsync(h_rp.data(), a.rp, (a.n + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    CFA_PROPAGATE(plan_tiled(ctx, h_rp.data(), a.n, 1, 8, W.tA));
+    W.tile_key = key;
+    W.graph.reset();
+    return CFA_OK;
+}
+
 static cfa_status b2_init(cfa_ctx* ctx, B2Work& W, const B2Args& a, CondArg cond) {
+    if (W.tiled) {
+        CFA_PROPAGATE(pack_tiled(ctx, a.rp, a.ci, a.val, nullptr, nullptr, W.tA));
+        launch_b2t<0>(ctx, W, a, nullptr, nullptr, W.v.p, cond);
+        CFA_CHECK_LAUNCH();
+        return CFA_OK;
+    }
     const int tpr = op_tpr(a.n, a.nnz);
     const int grid = row_grid(ctx, a.n, tpr);
     OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_init<TPR>), grid, kThreads, 0, a.n, a.rp, a.ci, a.val, (const double*)a.xu,
@@ -1146,12 +1309,16 @@ static cfa_status b2_body(cfa_ctx* ctx, B2Work& W, const B2Args& a, CondArg cond
     const int* done = &W.st.p->done;
     CFA_LAUNCH(ctx, k_b2_p, gv, kThreads, 0, n, W.r.p, W.v.p, W.p.p, W.st.p);
     CFA_PROPAGATE(ilu_apply(ctx, a.ilu, W.p.p, W.phat.p, 2, done));
-    OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_v<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, W.phat.p, W.r0.p, W.v.p,
-                                  W.st.p, W.part.p, W.counter.p, cond));
+    if (W.tiled) launch_b2t<1>(ctx, W, a, W.phat.p, W.r0.p, W.v.p, cond);
+    else
+        OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_v<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, W.phat.p, W.r0.p,
+                                      W.v.p, W.st.p, W.part.p, W.counter.p, cond));
     CFA_LAUNCH(ctx, k_b2_s, gv, kThreads, 0, n, W.r.p, W.v.p, W.s.p, W.st.p);
     CFA_PROPAGATE(ilu_apply(ctx, a.ilu, W.s.p, W.shat.p, 2, done));
-    OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_t<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, W.shat.p, W.s.p, W.t.p,
-                                  W.st.p, W.part.p, W.counter.p));
+    if (W.tiled) launch_b2t<2>(ctx, W, a, W.shat.p, W.s.p, W.t.p, cond);
+    else
+        OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_t<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, W.shat.p, W.s.p,
+                                      W.t.p, W.st.p, W.part.p, W.counter.p));
     CFA_LAUNCH(ctx, k_b2_xr, row_grid(ctx, n, 1), kThreads, 0, n, a.xu, a.xv, W.phat.p, W.shat.p, W.s.p, W.t.p, W.r.p,
                W.r0.p, W.st.p, W.part.p, W.counter.p, cond);
     CFA_CHECK_LAUNCH();
@@ -1170,6 +1337,7 @@ static cfa_status b2_solve(cfa_ctx* ctx, const B2Args& a, cfa_solve_report* rep)
         W.cap = n;
     }
     CFA_CUDA(W.part.ensure(8 * 8 * (size_t)ctx->num_sms + 64));   // NV <= 8 partials x max grid
+    CFA_PROPAGATE(plan_b2_tiles(ctx, W, a));
     B2State init{};
     init.tol = a.tol;
     init.max_iter = a.max_iter;
@@ -1204,8 +1372,14 @@ static cfa_status b2_solve(cfa_ctx* ctx, const B2Args& a, cfa_solve_report* rep)
     }
     CFA_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     B2State h;
+    int h_err = 0;
     CFA_CUDA(cudaMemcpyAsync(&h, W.st.p, sizeof(B2State), cudaMemcpyDeviceToHost, ctx->stream));
+    if (W.err.p) CFA_CUDA(cudaMemcpyAsync(&h_err, W.err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (h_err) {
+        cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream);
+        return set_error(ctx, CFA_TIMEOUT, "a bounded wait of a tile pipeline timed out", __FILE__, __LINE__);
+    }
     float ms = 0.f;
     CFA_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     ctx->launches += extra_body * (long long)(h.iter + 1);

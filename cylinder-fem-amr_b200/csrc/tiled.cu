@@ -33,8 +33,9 @@ __global__ void k_pack_tiles(int ntiles, const long long* __restrict__ off, cons
     }
 }
 
-cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T) {
-    int tr = 256;
+cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T,
+                      int max_tile_rows) {
+    int tr = std::max(1, std::min(kTileThreads, max_tile_rows));
     for (;;) {
         long long mx = 0;
         for (int r0 = 0; r0 < rows; r0 += tr) {

@@ -60,9 +60,11 @@ __host__ __device__ inline long long tile_bytes(int nr, int ne, int nvals, int v
     return tile_val_off(nr, ne, vbytes, nvals);
 }
 
-// Plans the tiles from the host row pointer: tile_rows = 256 rows, halved until every tile fits
-// the budget. Allocates the device buffers (the pattern and values are packed by pack_tiled).
-cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T);
+// Plans the tiles from the host row pointer: tile_rows = max_tile_rows (64: four lanes per row
+// with 256 threads, which keeps several gathers per thread in flight), halved until every tile
+// fits the budget. Allocates the device buffers (the pattern and values are packed by pack_tiled).
+cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T,
+                      int max_tile_rows = 64);
 
 // Packs pattern + values (FP64 sources; converted to float when vbytes == 4) into T.
 // vals[k] may be NULL for k >= nvals. Asynchronous.

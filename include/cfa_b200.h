@@ -238,6 +238,10 @@ cfa_status cfa_amg_level(const cfa_amg* amg, int l, int* info, const int** d_agg
                          const int** d_A_rp, const int** d_A_ci, const double** d_A_v,
                          const int** d_P_rp, const int** d_P_ci, const double** d_P_v,
                          const int** d_R_rp, const int** d_R_ci, const double** d_R_v, double* omega);
+/* Accumulated setup phase times [ms] over all setups (the reference's phase_ms[],
+ * src/cfa/linalg.cuh:970-982): copy, D^-1 + rho, strength + aggregation, P smoothing, transpose,
+ * Galerkin products, tile packing, coarse inverse. */
+cfa_status cfa_amg_phases(const cfa_amg* amg, double* ms8);
 /* dense inverse of the coarsest operator (device, coarse_n^2 FP64, row-major) */
 cfa_status cfa_amg_coarse_inverse(const cfa_amg* amg, const double** d_inv);
 

@@ -362,8 +362,8 @@ def test_amg_vcycle_matches_reference_gpu_golden(ctx):
     amg.setup(n, ci.size, dev(rp, torch.int32), dev(ci, torch.int32), dev(h["lap_val"]))
     z = torch.zeros(n, dtype=torch.float64, device="cuda")
     amg.apply(dev(np.sin(0.37 * np.arange(n)) + 0.2), z)
-    # same hierarchy, same row sums and shuffle tree as the reference's kernels
-    assert np.abs(host(z) - g["lap_vcycle_z"]).max() <= 1e-14 * np.abs(g["lap_vcycle_z"]).max()
+    # bit-identical hierarchy; the V-cycle's row sums are ordered differently (tile kernels)
+    assert np.abs(host(z) - g["lap_vcycle_z"]).max() <= 1e-12 * np.abs(g["lap_vcycle_z"]).max()
 
 
 def test_amg_coarse_not_spd_is_an_error(ctx):
