@@ -360,7 +360,7 @@ __global__ void k_vc_dense(int cn, const double* __restrict__ inv, const B* __re
 // ---------------------------------------------------------------------------------------------
 enum VcOp { VC_PRE = 0, VC_JAC = 1, VC_RES = 2, VC_SPMV = 3, VC_ADD = 4 };
 
-template <int TPR, int OP, class T, class B, class O>
+template <int TPR, int OP, class V, class T, class B, class O>
 __global__ void __launch_bounds__(kTileThreads)
 k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b, const T* __restrict__ x,
       O* __restrict__ y, const int* __restrict__ done) {
@@ -370,16 +370,17 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
         const int* rr = reinterpret_cast<const int*>(ch);
         const int ne = rr[nr];
         const int* cs = reinterpret_cast<const int*>(ch + tile_ci_off(nr));
-        const T* vv = reinterpret_cast<const T*>(ch + tile_val_off(nr, ne, (int)sizeof(T), 0));
+        const V* vv = reinterpret_cast<const V*>(ch + tile_val_off(nr, ne, (int)sizeof(V), 0));
         for (int base = 0; base < nr; base += kTileThreads / TPR) {
             const int lr = base + (int)threadIdx.x / TPR, lane = threadIdx.x % TPR;
             const bool valid = lr < nr;
             T s = (T)0;
             if (valid)
+#pragma unroll 4
                 for (int e = rr[lr] + lane; e < rr[lr + 1]; e += TPR) {
                     const int j = cs[e];
-                    if (OP == VC_PRE) s += vv[e] * (omega * dinv[j] * (T)b[j]);
-                    else s += vv[e] * x[j];
+                    if (OP == VC_PRE) s += (T)vv[e] * (omega * dinv[j] * (T)b[j]);
+                    else s += (T)vv[e] * x[j];
                 }
 #pragma unroll
             for (int o = TPR / 2; o > 0; o /= 2) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
@@ -402,8 +403,8 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
     });
 }
 
-// Launches (or, dry, only prepares) one tiled V-cycle operation.
-template <int OP, class T, class B, class O>
+// Launches (or, dry, only prepares) one tiled V-cycle operation; values of type V in the tiles.
+template <int OP, class V, class T, class B, class O>
 static void vct(cfa_ctx* ctx, bool dry, const TiledCsr& M, int* err, const T* dinv, T omega, const B* b, const T* x,
                 O* y, const int* done) {
     const int tpr = M.tile_rows >= kTileThreads ? 1 : std::min(32, kTileThreads / std::max(M.tile_rows, 1));
@@ -412,8 +413,8 @@ static void vct(cfa_ctx* ctx, bool dry, const TiledCsr& M, int* err, const T* di
     switch (tpr) {
 #define VCT_CASE(N)                                                                                     \
     case N:                                                                                             \
-        if (dry) allow_tile_kernel((const void*)k_vct<N, OP, T, B, O>);                                 \
-        else CFA_LAUNCH(ctx, (k_vct<N, OP, T, B, O>), L.grid, kTileThreads, L.smem, tv, dinv, omega, b, x, y, done); \
+        if (dry) allow_tile_kernel((const void*)k_vct<N, OP, V, T, B, O>);                              \
+        else CFA_LAUNCH(ctx, (k_vct<N, OP, V, T, B, O>), L.grid, kTileThreads, L.smem, tv, dinv, omega, b, x, y, done); \
         break;
         VCT_CASE(1) VCT_CASE(2) VCT_CASE(4) VCT_CASE(8) VCT_CASE(16)
         default:
@@ -516,51 +517,53 @@ static void vcycle_level(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     }
 }
 
-// V-cycle on the tile-streamed kernels (dry: prepare the kernels only, no launches)
-template <class T, class B>
-static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* z, const int* done, bool dry) {
+// V-cycle on the tile-streamed kernels: values V (FP32 in mixed precision) in the tiles, vectors
+// and arithmetic in FP64 (dry: prepare the kernels only, no launches)
+template <class V>
+static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const double* b, double* z, const int* done, bool dry) {
+    using T = double;
     AmgLevel& L = amg->levels[l];
-    LevelView<T> V = view<T>(L);
     const int s = amg->opts.smooth_steps;
     int* err = amg->err.p;
-    const T omega = V.omega;
-    T* x = V.x;
-    T* t = V.t;
+    const T omega = L.omega;
+    const T* dinv = L.dinv.p;
+    T* x = L.x64.p;
+    T* t = L.t64.p;
     if (s >= 2) {
-        vct<VC_PRE, T, B, T>(ctx, dry, L.tA, err, V.dinv, omega, b, (const T*)nullptr, x, done);
+        vct<VC_PRE, V, T, T, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)nullptr, x, done);
     } else if (!dry) {
-        CFA_TPR_SWITCH(L.A.tpr, CFA_LAUNCH(ctx, (k_vc_pre<TPR, T, B>), row_grid(ctx, L.A.rows, L.A.tpr), kThreads, 0,
-                                           L.A.rows, V.Arp, V.Aci, V.Av, V.dinv, V.omega, b, 0, V.x, done));
+        CFA_TPR_SWITCH(L.A.tpr, CFA_LAUNCH(ctx, (k_vc_pre<TPR, T, T>), row_grid(ctx, L.A.rows, L.A.tpr), kThreads, 0,
+                                           L.A.rows, L.A.rp.p, L.A.ci.p, L.A.v.p, dinv, omega, b, 0, x, done));
     }
     for (int k = 2; k < s; ++k) {
-        vct<VC_JAC, T, B, T>(ctx, dry, L.tA, err, V.dinv, omega, b, (const T*)x, t, done);
+        vct<VC_JAC, V, T, T, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, t, done);
         std::swap(x, t);
     }
-    vct<VC_RES, T, B, T>(ctx, dry, L.tA, err, V.dinv, omega, b, (const T*)x, V.r, done);
+    vct<VC_RES, V, T, T, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, L.r64.p, done);
     const bool last = l + 1 == (int)amg->levels.size();
-    T* cb = last ? (std::is_same<T, double>::value ? (T*)amg->cb64.p : (T*)amg->cb32.p) : view<T>(amg->levels[l + 1]).b;
-    vct<VC_SPMV, T, T, T>(ctx, dry, L.tR, err, V.dinv, omega, (const T*)nullptr, (const T*)V.r, cb, done);
+    T* cb = last ? amg->cb64.p : amg->levels[l + 1].b64.p;
+    vct<VC_SPMV, V, T, T, T>(ctx, dry, L.tR, err, dinv, omega, (const T*)nullptr, (const T*)L.r64.p, cb, done);
     const T* cx;
     if (!last) {
-        vcycle_tiled<T, T>(ctx, amg, l + 1, cb, nullptr, done, dry);
-        cx = view<T>(amg->levels[l + 1]).x;
+        vcycle_tiled<V>(ctx, amg, l + 1, cb, nullptr, done, dry);
+        cx = amg->levels[l + 1].x64.p;
     } else {
-        T* dst = std::is_same<T, double>::value ? (T*)amg->cx64.p : (T*)amg->cx32.p;
         if (!dry)
             CFA_LAUNCH(ctx, (k_vc_dense<T, T>), ceil_div((long long)amg->coarse_n * 32, kThreads), kThreads, 0,
-                       amg->coarse_n, amg->coarse_inv.p, (const T*)cb, dst, done);
-        cx = dst;
+                       amg->coarse_n, amg->coarse_inv.p, (const T*)cb, amg->cx64.p, done);
+        cx = amg->cx64.p;
     }
-    vct<VC_ADD, T, T, T>(ctx, dry, L.tP, err, V.dinv, omega, (const T*)nullptr, cx, x, done);
+    vct<VC_ADD, V, T, T, T>(ctx, dry, L.tP, err, dinv, omega, (const T*)nullptr, cx, x, done);
     for (int k = 0; k < s; ++k) {
         if (l == 0 && k == s - 1) {
-            vct<VC_JAC, T, B, double>(ctx, dry, L.tA, err, V.dinv, omega, b, (const T*)x, z, done);
+            vct<VC_JAC, V, T, T, double>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, z, done);
         } else {
-            vct<VC_JAC, T, B, T>(ctx, dry, L.tA, err, V.dinv, omega, b, (const T*)x, t, done);
+            vct<VC_JAC, V, T, T, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, t, done);
             std::swap(x, t);
         }
     }
-    if (l > 0 && x != V.x && !dry) cudaMemcpyAsync(V.x, x, (size_t)L.A.rows * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream);
+    if (l > 0 && x != L.x64.p && !dry)
+        cudaMemcpyAsync(L.x64.p, x, (size_t)L.A.rows * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream);
 }
 
 cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done) {
@@ -568,8 +571,8 @@ cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, co
         CFA_LAUNCH(ctx, (k_vc_dense<double, double>), ceil_div((long long)amg->coarse_n * 32, kThreads), kThreads, 0,
                    amg->coarse_n, amg->coarse_inv.p, r, z, done);
     } else if (amg->tiled) {
-        if (amg->opts.precision == CFA_MIXED) vcycle_tiled<float, double>(ctx, amg, 0, r, z, done, false);
-        else vcycle_tiled<double, double>(ctx, amg, 0, r, z, done, false);
+        if (amg->opts.precision == CFA_MIXED) vcycle_tiled<float>(ctx, amg, 0, r, z, done, false);
+        else vcycle_tiled<double>(ctx, amg, 0, r, z, done, false);
     } else if (amg->opts.precision == CFA_MIXED) {
         vcycle_level<float, double>(ctx, amg, 0, r, z, done);
     } else {
@@ -748,6 +751,11 @@ static cfa_status level_vectors(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int n) 
     return CFA_OK;
 }
 
+static cfa_status level_vectors64(cfa_ctx* ctx, AmgLevel& L, int n) {
+    CFA_CUDA(L.x64.ensure(n)); CFA_CUDA(L.t64.ensure(n)); CFA_CUDA(L.b64.ensure(n)); CFA_CUDA(L.r64.ensure(n));
+    return CFA_OK;
+}
+
 static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* d_rp, const int* d_ci,
                             const double* d_v) {
     const auto t0 = std::chrono::steady_clock::now();
@@ -893,8 +901,9 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
             }
         }
         // raise the kernels' shared-memory limits now, outside any stream capture
-        if (o.precision == CFA_MIXED) vcycle_tiled<float, double>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
-        else vcycle_tiled<double, double>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
+        for (AmgLevel& L : amg->levels) CFA_PROPAGATE(level_vectors64(ctx, L, L.A.rows));
+        if (o.precision == CFA_MIXED) vcycle_tiled<float>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
+        else vcycle_tiled<double>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
     }
     phase(6);
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -53,9 +53,9 @@ __global__ void k_ilu_gather(int nl, int nu, int n, const int* __restrict__ l_sr
 // Forward sweep of one colour for NR right-hand sides: y_i = r_i - sum_L l_ie y_e (unit L); the
 // last colour also divides by u_ii. T: factor/work precision; FP64 output written when a row is
 // final (last colour here, else in the backward sweep).
-template <class T, int NR>
+template <class V, class T, int NR>
 __global__ void k_ilu_lower(int m, int n, const int* __restrict__ rows, const int* __restrict__ lp,
-                            const int* __restrict__ lc, const T* __restrict__ lv, const T* __restrict__ dinv,
+                            const int* __restrict__ lc, const V* __restrict__ lv, const V* __restrict__ dinv,
                             int last, const double* __restrict__ r, T* __restrict__ w, double* __restrict__ z,
                             const int* __restrict__ done) {
     if (done && *done) return;
@@ -66,13 +66,13 @@ __global__ void k_ilu_lower(int m, int n, const int* __restrict__ rows, const in
 #pragma unroll
     for (int c = 0; c < NR; ++c) acc[c] = (T)r[(size_t)c * n + i];
     for (int e = lp[t]; e < lp[t + 1]; ++e) {
-        const T l = lv[e];
+        const T l = (T)lv[e];
         const int j = lc[e];
 #pragma unroll
         for (int c = 0; c < NR; ++c) acc[c] -= l * w[(size_t)c * n + j];
     }
     if (last) {
-        const T d = dinv[t];
+        const T d = (T)dinv[t];
 #pragma unroll
         for (int c = 0; c < NR; ++c) {
             acc[c] = acc[c] * d;
@@ -84,9 +84,9 @@ __global__ void k_ilu_lower(int m, int n, const int* __restrict__ rows, const in
 }
 
 // Backward sweep of one colour: z_i = (y_i - sum_U u_ie z_e) / u_ii
-template <class T, int NR>
+template <class V, class T, int NR>
 __global__ void k_ilu_upper(int m, int n, const int* __restrict__ rows, const int* __restrict__ up,
-                            const int* __restrict__ uc, const T* __restrict__ uv, const T* __restrict__ dinv,
+                            const int* __restrict__ uc, const V* __restrict__ uv, const V* __restrict__ dinv,
                             T* __restrict__ w, double* __restrict__ z, const int* __restrict__ done) {
     if (done && *done) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -96,12 +96,12 @@ __global__ void k_ilu_upper(int m, int n, const int* __restrict__ rows, const in
 #pragma unroll
     for (int c = 0; c < NR; ++c) acc[c] = w[(size_t)c * n + i];
     for (int e = up[t]; e < up[t + 1]; ++e) {
-        const T u = uv[e];
+        const T u = (T)uv[e];
         const int j = uc[e];
 #pragma unroll
         for (int c = 0; c < NR; ++c) acc[c] -= u * w[(size_t)c * n + j];
     }
-    const T d = dinv[t];
+    const T d = (T)dinv[t];
 #pragma unroll
     for (int c = 0; c < NR; ++c) {
         acc[c] = acc[c] * d;
@@ -110,33 +110,33 @@ __global__ void k_ilu_upper(int m, int n, const int* __restrict__ rows, const in
     }
 }
 
-template <class T, int NR>
-static void sweeps(cfa_ctx* ctx, const cfa_ilu* h, const T* lv, const T* uv, const T* dinv, T* w,
+template <class V, class T, int NR>
+static void sweeps(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv, const V* dinv, T* w,
                    const double* r, double* z, const int* done) {
     const int n = h->n;
     for (int c = 0; c < h->nc; ++c) {
         const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
         if (m == 0) continue;
-        CFA_LAUNCH(ctx, (k_ilu_lower<T, NR>), ceil_div(m, kThreads), kThreads, 0, m, n, h->rows.p + cs, h->lp.p + cs,
+        CFA_LAUNCH(ctx, (k_ilu_lower<V, T, NR>), ceil_div(m, kThreads), kThreads, 0, m, n, h->rows.p + cs, h->lp.p + cs,
                    h->lc.p, lv, dinv + cs, c == h->nc - 1 ? 1 : 0, r, w, z, done);
     }
     for (int c = h->nc - 2; c >= 0; --c) {
         const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
         if (m == 0) continue;
-        CFA_LAUNCH(ctx, (k_ilu_upper<T, NR>), ceil_div(m, kThreads), kThreads, 0, m, n, h->rows.p + cs, h->up.p + cs,
+        CFA_LAUNCH(ctx, (k_ilu_upper<V, T, NR>), ceil_div(m, kThreads), kThreads, 0, m, n, h->rows.p + cs, h->up.p + cs,
                    h->uc.p, uv, dinv + cs, w, z, done);
     }
 }
 
 cfa_status ilu_apply(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z, int nrhs, const int* done) {
     if (h->precision == CFA_MIXED) {
-        float* w = const_cast<cfa_ilu*>(h)->work32.p;
-        if (nrhs == 1) sweeps<float, 1>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r, z, done);
-        else sweeps<float, 2>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r, z, done);
+        // FP32 factors, FP64 vectors and arithmetic, in place in z
+        if (nrhs == 1) sweeps<float, double, 1>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, z, r, z, done);
+        else sweeps<float, double, 2>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, z, r, z, done);
     } else {
         // FP64: the sweeps work in place in z (as the reference)
-        if (nrhs == 1) sweeps<double, 1>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, z, r, z, done);
-        else sweeps<double, 2>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, z, r, z, done);
+        if (nrhs == 1) sweeps<double, double, 1>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, z, r, z, done);
+        else sweeps<double, double, 2>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, z, r, z, done);
     }
     CFA_CHECK_LAUNCH();
     return CFA_OK;
