@@ -517,6 +517,223 @@ static void vcycle_level(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// coarse tail: the V-cycle below level l0 in ONE cooperative kernel. Each phase is a grid-stride
+// row operation; phases are separated by a grid barrier whose spin is bounded (on timeout the
+// error word is set and every CTA leaves at its next barrier). Mutable vectors are read through
+// L2 (__ldcg) since other CTAs wrote them earlier in the same kernel.
+// ---------------------------------------------------------------------------------------------
+constexpr int kTailMaxLevels = 16;
+constexpr int kTailThreads = 512;
+constexpr int kTailTpr = 8;
+constexpr unsigned kBarrierLimit = 1u << 24;
+
+template <class V>
+struct TailLevel {
+    int n, nc;
+    const int *Arp, *Aci, *Prp, *Pci, *Rrp, *Rci;
+    const V *Av, *Pv, *Rv;
+    const double* dinv;
+    double omega;
+    double *x, *t, *b, *r;
+};
+
+template <class V>
+struct TailArgs {
+    TailLevel<V> lv[kTailMaxLevels];
+    int nlev, s, cn;
+    const double* cinv;
+    double *cb, *cx;
+    unsigned* bar;   // [0] count, [1] generation
+    int* err;
+    const int* done;
+};
+
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err) {
+    __shared__ int failed;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        failed = 0;
+        volatile unsigned* vgen = bar + 1;
+        const unsigned g = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned it = 0;
+            while (*vgen == g) {
+                if (++it > kBarrierLimit) { atomicExch(err, (int)CFA_TIMEOUT); failed = 1; break; }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if (*(volatile int*)err) failed = 1;
+    }
+    __syncthreads();
+    return !failed;
+}
+
+enum TailOp { T_PRE, T_JAC, T_RES, T_SPMV, T_ADD };
+
+// One row operation over all rows of a matrix (grid-stride warps, kTailTpr lanes per row).
+template <int OP, class V>
+__device__ __forceinline__ void tail_rows(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                          const V* __restrict__ val, const double* __restrict__ dinv, double omega,
+                                          const double* b, const double* x, double* y) {
+    constexpr int TPR = kTailTpr;
+    const int lane = threadIdx.x % TPR;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const int nw = gridDim.x * blockDim.x / 32;
+    constexpr int rpw = 32 / TPR;
+    for (int base = gw * rpw; base < n; base += nw * rpw) {
+        const int row = base + (threadIdx.x & 31) / TPR;
+        const bool valid = row < n;
+        double s = 0.0;
+        if (valid)
+            for (int k = rp[row] + lane; k < rp[row + 1]; k += TPR) {
+                const int j = ci[k];
+                if (OP == T_PRE) s += (double)val[k] * (omega * dinv[j] * __ldcg(b + j));
+                else s += (double)val[k] * __ldcg(x + j);
+            }
+#pragma unroll
+        for (int o = TPR / 2; o > 0; o /= 2) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
+        if (valid && lane == 0) {
+            if (OP == T_PRE) {
+                const double bi = __ldcg(b + row);
+                const double x0 = omega * dinv[row] * bi;
+                y[row] = x0 + omega * dinv[row] * (bi - s);
+            } else if (OP == T_JAC) {
+                y[row] = __ldcg(x + row) + omega * dinv[row] * (__ldcg(b + row) - s);
+            } else if (OP == T_RES) {
+                y[row] = __ldcg(b + row) - s;
+            } else if (OP == T_SPMV) {
+                y[row] = s;
+            } else {
+                y[row] = __ldcg(y + row) + s;
+            }
+        }
+    }
+}
+
+template <class V>
+__global__ void __launch_bounds__(kTailThreads) k_vc_tail(TailArgs<V> a) {
+    if (a.done && *a.done) return;
+    const int L = a.nlev, s = a.s;
+    // down
+    for (int l = 0; l < L; ++l) {
+        const TailLevel<V>& v = a.lv[l];
+        double* x = v.x;
+        double* t = v.t;
+        if (s >= 2) tail_rows<T_PRE, V>(v.n, v.Arp, v.Aci, v.Av, v.dinv, v.omega, v.b, nullptr, x);
+        else {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.n; i += gridDim.x * blockDim.x)
+                x[i] = v.omega * v.dinv[i] * __ldcg(v.b + i);
+        }
+        if (!grid_barrier(a.bar, a.err)) return;
+        for (int k = 2; k < s; ++k) {
+            tail_rows<T_JAC, V>(v.n, v.Arp, v.Aci, v.Av, v.dinv, v.omega, v.b, x, t);
+            double* tmp = x; x = t; t = tmp;
+            if (!grid_barrier(a.bar, a.err)) return;
+        }
+        if (x != v.x) {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.n; i += gridDim.x * blockDim.x) v.x[i] = __ldcg(x + i);
+            if (!grid_barrier(a.bar, a.err)) return;
+        }
+        tail_rows<T_RES, V>(v.n, v.Arp, v.Aci, v.Av, v.dinv, v.omega, v.b, v.x, v.r);
+        if (!grid_barrier(a.bar, a.err)) return;
+        double* cb = (l + 1 < L) ? a.lv[l + 1].b : a.cb;
+        tail_rows<T_SPMV, V>(v.nc, v.Rrp, v.Rci, v.Rv, nullptr, 0.0, nullptr, v.r, cb);
+        if (!grid_barrier(a.bar, a.err)) return;
+    }
+    // coarsest: dense inverse, one warp per row
+    {
+        const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32, nw = gridDim.x * blockDim.x / 32;
+        const int lane = threadIdx.x & 31;
+        for (int i = warp; i < a.cn; i += nw) {
+            double acc = 0.0;
+            for (int j = lane; j < a.cn; j += 32) acc += a.cinv[(size_t)i * a.cn + j] * __ldcg(a.cb + j);
+            acc = warp_sum(acc);
+            if (lane == 0) a.cx[i] = acc;
+        }
+        if (!grid_barrier(a.bar, a.err)) return;
+    }
+    // up
+    for (int l = L - 1; l >= 0; --l) {
+        const TailLevel<V>& v = a.lv[l];
+        const double* cx = (l + 1 < L) ? a.lv[l + 1].x : a.cx;
+        tail_rows<T_ADD, V>(v.n, v.Prp, v.Pci, v.Pv, nullptr, 0.0, nullptr, cx, v.x);
+        if (!grid_barrier(a.bar, a.err)) return;
+        double* x = v.x;
+        double* t = v.t;
+        for (int k = 0; k < s; ++k) {
+            tail_rows<T_JAC, V>(v.n, v.Arp, v.Aci, v.Av, v.dinv, v.omega, v.b, x, t);
+            double* tmp = x; x = t; t = tmp;
+            if (!grid_barrier(a.bar, a.err)) return;
+        }
+        if (x != v.x) {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.n; i += gridDim.x * blockDim.x) v.x[i] = __ldcg(x + i);
+            if (!grid_barrier(a.bar, a.err)) return;
+        }
+    }
+}
+
+template <class V>
+static void launch_tail(cfa_ctx* ctx, cfa_amg* amg, int l0, const int* done) {
+    TailArgs<V> a{};
+    const int L = (int)amg->levels.size() - l0;
+    a.nlev = L;
+    a.s = amg->opts.smooth_steps;
+    a.cn = amg->coarse_n;
+    a.cinv = amg->coarse_inv.p;
+    a.cb = amg->cb64.p;
+    a.cx = amg->cx64.p;
+    a.bar = amg->tail_bar.p;
+    a.err = amg->err.p;
+    a.done = done;
+    for (int k = 0; k < L; ++k) {
+        AmgLevel& Lv = amg->levels[l0 + k];
+        TailLevel<V>& t = a.lv[k];
+        t.n = Lv.A.rows;
+        t.nc = Lv.P.cols;
+        t.Arp = Lv.A.rp.p; t.Aci = Lv.A.ci.p;
+        t.Prp = Lv.P.rp.p; t.Pci = Lv.P.ci.p;
+        t.Rrp = Lv.R.rp.p; t.Rci = Lv.R.ci.p;
+        if constexpr (std::is_same<V, float>::value) { t.Av = Lv.A.v32.p; t.Pv = Lv.P.v32.p; t.Rv = Lv.R.v32.p; }
+        else { t.Av = Lv.A.v.p; t.Pv = Lv.P.v.p; t.Rv = Lv.R.v.p; }
+        t.dinv = Lv.dinv.p;
+        t.omega = Lv.omega;
+        t.x = Lv.x64.p; t.t = Lv.t64.p; t.b = Lv.b64.p; t.r = Lv.r64.p;
+    }
+    void* args[] = {&a};
+    ctx->launches++;
+    cudaLaunchCooperativeKernel((const void*)k_vc_tail<V>, amg->tail_grid, kTailThreads, args, 0, ctx->stream);
+}
+
+// Chooses the first tail level (rows <= tail_rows) and the co-resident grid.
+static cfa_status plan_tail(cfa_ctx* ctx, cfa_amg* amg) {
+    amg->tail_level = -1;
+    const char* e = std::getenv("CFA_TAIL_ROWS");
+    const int tail_rows = e ? std::atoi(e) : 100000;
+    if (tail_rows <= 0 || amg->levels.size() > (size_t)kTailMaxLevels + 1) return CFA_OK;
+    for (int l = 1; l < (int)amg->levels.size(); ++l)
+        if (amg->levels[l].A.rows <= tail_rows) { amg->tail_level = l; break; }
+    if (amg->tail_level < 0 || (int)amg->levels.size() - amg->tail_level > kTailMaxLevels) {
+        amg->tail_level = -1;
+        return CFA_OK;
+    }
+    int per_sm = 0;
+    const void* k = amg->opts.precision == CFA_MIXED ? (const void*)k_vc_tail<float> : (const void*)k_vc_tail<double>;
+    CFA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTailThreads, 0));
+    if (per_sm < 1) { amg->tail_level = -1; return CFA_OK; }
+    amg->tail_grid = std::min(per_sm, 2) * ctx->num_sms;
+    CFA_CUDA(amg->tail_bar.ensure(2));
+    CFA_CUDA(cudaMemsetAsync(amg->tail_bar.p, 0, 2 * sizeof(unsigned), ctx->stream));
+    return CFA_OK;
+}
+
 // V-cycle on the tile-streamed kernels: values V (FP32 in mixed precision) in the tiles, vectors
 // and arithmetic in FP64 (dry: prepare the kernels only, no launches)
 template <class V>
@@ -544,7 +761,10 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const double* b, dou
     T* cb = last ? amg->cb64.p : amg->levels[l + 1].b64.p;
     vct<VC_SPMV, V, T, T, T>(ctx, dry, L.tR, err, dinv, omega, (const T*)nullptr, (const T*)L.r64.p, cb, done);
     const T* cx;
-    if (!last) {
+    if (!last && l + 1 == amg->tail_level) {
+        if (!dry) launch_tail<V>(ctx, amg, l + 1, done);
+        cx = amg->levels[l + 1].x64.p;
+    } else if (!last) {
         vcycle_tiled<V>(ctx, amg, l + 1, cb, nullptr, done, dry);
         cx = amg->levels[l + 1].x64.p;
     } else {
@@ -902,6 +1122,7 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
         }
         // raise the kernels' shared-memory limits now, outside any stream capture
         for (AmgLevel& L : amg->levels) CFA_PROPAGATE(level_vectors64(ctx, L, L.A.rows));
+        CFA_PROPAGATE(plan_tail(ctx, amg));
         if (o.precision == CFA_MIXED) vcycle_tiled<float>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
         else vcycle_tiled<double>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
     }

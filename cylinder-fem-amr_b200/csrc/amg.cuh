@@ -46,6 +46,10 @@ struct cfa_amg {
     // 0 copy, 1 D^-1 + rho, 2 strength + aggregation, 3 P smoothing, 4 transpose, 5 Galerkin,
     // 6 tile packing, 7 coarse inverse
     double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    // coarse tail: levels >= tail_level run inside one cooperative kernel (grid barriers)
+    int tail_level = -1;
+    int tail_grid = 0;
+    cfa::DevBuf<unsigned> tail_bar;      // {count, generation}
     cfa::DevBuf<int> err;                // tile pipeline error word
 };
 

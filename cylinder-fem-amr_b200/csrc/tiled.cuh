@@ -31,6 +31,7 @@ struct TileView {
     const long long* off = nullptr;   // [ntiles + 1] byte offset of each tile chunk
     const int* row0 = nullptr;        // [ntiles + 1] first row of each tile
     int ntiles = 0, rows = 0, nvals = 0, vbytes = 8;
+    int tile_rows = 0;                // rows of every tile but the last (tile t starts at t * tile_rows)
     int max_chunk = 0;                // bytes
     int* err = nullptr;               // device error word (timeout)
 };
@@ -46,7 +47,7 @@ struct TiledCsr {
     TileView view(int* err) const {
         TileView v;
         v.data = data.p; v.off = off.p; v.row0 = row0.p; v.ntiles = ntiles; v.rows = rows;
-        v.nvals = nvals; v.vbytes = vbytes; v.max_chunk = max_chunk; v.err = err;
+        v.nvals = nvals; v.vbytes = vbytes; v.max_chunk = max_chunk; v.err = err; v.tile_rows = tile_rows;
         return v;
     }
 };
@@ -158,8 +159,8 @@ __device__ __forceinline__ bool tile_loop(const TileView& tv, unsigned char* sme
             return false;
         }
         phase[s] ^= 1u;
-        const int r0 = tv.row0[t];
-        body(t, r0, tv.row0[t + 1] - r0, s ? buf1 : buf0);
+        const int r0 = t * tv.tile_rows;
+        body(t, r0, min(tv.tile_rows, tv.rows - r0), s ? buf1 : buf0);
         __syncthreads();
     }
     return true;
