@@ -33,6 +33,7 @@ for _p in (ROOT, PKG):
         sys.path.insert(0, _p)
 
 AMG_REBUILD = 50          # src/cfa/options.cuh:26
+SETUP_REPS = 3
 STAB, DT, NU, U_MAX, TOL = 0.3, 1e-3, 1e-3, 1.5, 1e-10
 METRIC = "pressure+momentum solve ms/step & HBM GB/s, mixed vs FP64 at 1e-10 rel res"
 
@@ -46,28 +47,40 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling (every 100 ms) while the timed regions run: one sampler process for
+    the whole run; samples taken between start() and pause() are kept."""
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.path = os.path.join("/tmp", f"cfa_clocks_{os.getpid()}.csv")
+        self.windows = []
+        self.t0 = None
 
-    def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-        try:
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=self.f, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
-        return self
+    def start(self):
+        if self.proc is None:
+            q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            try:
+                self.f = open(self.path, "w")
+                self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                              "--format=csv,noheader,nounits", "-lms", "100"],
+                                             stdout=self.f, stderr=subprocess.DEVNULL)
+                time.sleep(0.3)
+            except Exception:
+                self.proc = False
+        self.t0 = time.time()
 
-    def __exit__(self, *a):
-        if self.proc is not None:
+    def pause(self):
+        if self.t0 is not None:
+            self.windows.append((self.t0, time.time() + 0.1))
+            self.t0 = None
+
+    def stop(self):
+        self.pause()
+        if self.proc:
+            time.sleep(0.2)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -76,24 +89,33 @@ class ClockSampler:
             self.f.close()
 
     def summary(self):
-        if self.proc is None or not os.path.exists(self.path):
+        if not self.proc or not os.path.exists(self.path):
             return None
-        sm, mx, reasons = [], 0.0, set()
+        import datetime
+        sm, mx, reasons, n_all = [], 0.0, set(), 0
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
             try:
-                sm.append(float(f[1]))
-                mx = max(mx, float(f[2]))
+                clk, cmax = float(f[1]), float(f[2])
             except ValueError:
                 continue
+            try:
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                ts = None   # unknown format: keep the sample
+            n_all += 1
+            if ts is not None and not any(a <= ts <= b for a, b in self.windows):
+                continue
+            sm.append(clk)
+            mx = max(mx, cmax)
             for k, nm in enumerate(names):
                 if f[5 + k].lower().startswith("active"):
                     reasons.add(nm)
         if not sm:
-            return None
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "samples_total": n_all}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
@@ -152,9 +174,25 @@ def run_ours(args, rank, world):
     ctx = cfa.Context()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
     res = {}
+    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
     for prec_name, prec in (("fp64", cfa.FP64), ("mixed", cfa.MIXED)):
         st = S.SolveStep(m, u, v, p, precision=prec, ctx=ctx, dt=DT, nu=NU, stab=STAB, u_max=U_MAX, tol=TOL)
-        setup_ms = st.amg_setup()
+        # AMG setup: one untimed setup (first-touch allocations), then the mean of SETUP_REPS
+        st.amg_setup()
+        ph0 = dict(st.amg.phase_ms)
+        setup_ms = sum(st.amg_setup() for _ in range(SETUP_REPS)) / SETUP_REPS
+        phases = {k: (v - ph0.get(k, 0.0)) / SETUP_REPS for k, v in st.amg.phase_ms.items()}
+        if args.profile:
+            for _ in range(args.warmup):
+                st.run()
+            torch.cuda.synchronize()
+            torch.cuda.profiler.start()
+            st.run()
+            torch.cuda.synchronize()
+            torch.cuda.profiler.stop()
+            print(json.dumps({"profile": prec_name, "report": st.report(), "launches": ctx.launches}))
+            del st
+            continue
         for _ in range(args.warmup):
             st.run()
         torch.cuda.synchronize()
@@ -164,15 +202,16 @@ def run_ours(args, rank, world):
         total = 0.0
         l0 = ctx.launches
         reports = []
-        with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
-            for _ in range(args.steps):
-                l2_flush(flush)
-                ev[0].record()
-                st.run()
-                ev[1].record()
-                ev[1].synchronize()
-                total += ev[0].elapsed_time(ev[1])
-                reports.append(st.report())
+        clk.start()
+        for _ in range(args.steps):
+            l2_flush(flush)
+            ev[0].record()
+            st.run()
+            ev[1].record()
+            ev[1].synchronize()
+            total += ev[0].elapsed_time(ev[1])
+            reports.append(st.report())
+        clk.pause()
         launches = ctx.launches - l0
         torch.cuda.synchronize()
         step_ms = total / args.steps
@@ -182,6 +221,7 @@ def run_ours(args, rank, world):
         hp = torch.from_numpy(p).pin_memory()
         outs = [torch.empty(m.n, dtype=torch.float64).pin_memory() for _ in range(3)]
         e2e_total = 0.0
+        clk.start()
         for _ in range(args.steps):
             l2_flush(flush)
             ev[0].record()
@@ -197,12 +237,15 @@ def run_ours(args, rank, world):
             ev[1].record()
             ev[1].synchronize()
             e2e_total += ev[0].elapsed_time(ev[1])
+        clk.pause()
         e2e_ms = e2e_total / args.steps
         op_ms = time_operator(cfa, st, 20, flush) if prec == cfa.FP64 else None
         res[prec_name] = dict(step_ms=step_ms, setup_ms=setup_ms, e2e_ms=e2e_ms, launches=launches,
-                              clocks=clk.summary(), report=reports[-1], op_ms=op_ms, levels=st.amg.num_levels(), phases=st.amg.phase_ms,
+                              report=reports[-1], op_ms=op_ms, levels=st.amg.num_levels(), phases=phases,
                               colours=st.ilu.n_colours, nnz=st.nnz, n=st.n)
         del st
+    clk.stop()
+    res["clocks"] = clk.summary()
     return m, res
 
 
@@ -259,11 +302,13 @@ def run_reference(args):
         R.ref_step_run(h, O._p(its), O._p(conv), O._p(rel), None, None, None)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     total = 0.0
-    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
-        for _ in range(args.steps):
-            flush.add_(1.0)
-            torch.cuda.synchronize()
-            total += R.ref_step_run(h, O._p(its), O._p(conv), O._p(rel), None, None, None)
+    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
+    clk.start()
+    for _ in range(args.steps):
+        flush.add_(1.0)
+        torch.cuda.synchronize()
+        total += R.ref_step_run(h, O._p(its), O._p(conv), O._p(rel), None, None, None)
+    clk.stop()
     R.ref_step_free(h)
     step_ms = total / args.steps
     value = step_ms + setup_ms / AMG_REBUILD
@@ -288,11 +333,13 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c1")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="one step per precision between cudaProfilerStart/Stop (for ncu --profile-from-start off); no JSON line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -308,6 +355,8 @@ def main():
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     m, res = run_ours(args, rank, world)
+    if args.profile:
+        return
     mixed, fp64 = res["mixed"], res["fp64"]
     value = mixed["step_ms"] + mixed["setup_ms"] / AMG_REBUILD
     value64 = fp64["step_ms"] + fp64["setup_ms"] / AMG_REBUILD
@@ -329,7 +378,7 @@ def main():
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get(f"pressure_operator_{args.workload}")
     cpu = None if args.no_cpu else cpu_baseline(m, *workload_inputs(args.workload)[1:])
-    clocks = mixed["clocks"]
+    clocks = res["clocks"]
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": "ms/step", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(value, 4), "higher_is_better": False, "scaling": "weak",

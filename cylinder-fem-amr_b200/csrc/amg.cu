@@ -374,6 +374,15 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
         for (int base = 0; base < nr; base += kTileThreads / TPR) {
             const int lr = base + (int)threadIdx.x / TPR, lane = threadIdx.x % TPR;
             const bool valid = lr < nr;
+            const int row = r0 + lr;
+            // the row's own operands, loaded before the gathers so both round trips overlap
+            T di = (T)0, bi = (T)0, xi = (T)0;
+            if (valid && lane == 0) {
+                if (OP == VC_PRE || OP == VC_JAC) di = dinv[row];
+                if (OP == VC_PRE || OP == VC_JAC || OP == VC_RES) bi = (T)b[row];
+                if (OP == VC_JAC) xi = x[row];
+                if (OP == VC_ADD) xi = (T)y[row];
+            }
             T s = (T)0;
             if (valid)
 #pragma unroll 4
@@ -385,18 +394,17 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
 #pragma unroll
             for (int o = TPR / 2; o > 0; o /= 2) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
             if (valid && lane == 0) {
-                const int row = r0 + lr;
                 if (OP == VC_PRE) {
-                    const T x0 = omega * dinv[row] * (T)b[row];
-                    y[row] = (O)(x0 + omega * dinv[row] * ((T)b[row] - s));
+                    const T x0 = omega * di * bi;
+                    y[row] = (O)(x0 + omega * di * (bi - s));
                 } else if (OP == VC_JAC) {
-                    y[row] = (O)(x[row] + omega * dinv[row] * ((T)b[row] - s));
+                    y[row] = (O)(xi + omega * di * (bi - s));
                 } else if (OP == VC_RES) {
-                    y[row] = (O)((T)b[row] - s);
+                    y[row] = (O)(bi - s);
                 } else if (OP == VC_SPMV) {
                     y[row] = (O)s;
                 } else {
-                    y[row] = (O)((T)y[row] + s);
+                    y[row] = (O)(xi + s);
                 }
             }
         }
@@ -518,15 +526,19 @@ static void vcycle_level(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
 }
 
 // ---------------------------------------------------------------------------------------------
-// coarse tail: the V-cycle below level l0 in ONE cooperative kernel. Each phase is a grid-stride
-// row operation; phases are separated by a grid barrier whose spin is bounded (on timeout the
-// error word is set and every CTA leaves at its next barrier). Mutable vectors are read through
-// L2 (__ldcg) since other CTAs wrote them earlier in the same kernel.
+// coarse tail: the V-cycle below level l0 in ONE kernel launched as a single thread-block
+// cluster (16 CTAs x 1024 threads, one CTA per SM). Each phase is a cluster-stride row
+// operation; phases are separated by the hardware cluster barrier (barrier.cluster with
+// release/acquire semantics), so no software spin is involved. Mutable vectors are read through
+// L2 (__ldcg) since other CTAs of the cluster wrote them earlier in the same kernel.
 // ---------------------------------------------------------------------------------------------
 constexpr int kTailMaxLevels = 16;
-constexpr int kTailThreads = 512;
+constexpr int kTailThreads = 1024;
 constexpr int kTailTpr = 8;
-constexpr unsigned kBarrierLimit = 1u << 24;
+
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
 
 template <class V>
 struct TailLevel {
@@ -544,37 +556,9 @@ struct TailArgs {
     int nlev, s, cn;
     const double* cinv;
     double *cb, *cx;
-    unsigned* bar;   // [0] count, [1] generation
     int* err;
     const int* done;
 };
-
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err) {
-    __shared__ int failed;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        failed = 0;
-        volatile unsigned* vgen = bar + 1;
-        const unsigned g = *vgen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u);
-        if (arrived == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            unsigned it = 0;
-            while (*vgen == g) {
-                if (++it > kBarrierLimit) { atomicExch(err, (int)CFA_TIMEOUT); failed = 1; break; }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        if (*(volatile int*)err) failed = 1;
-    }
-    __syncthreads();
-    return !failed;
-}
 
 enum TailOp { T_PRE, T_JAC, T_RES, T_SPMV, T_ADD };
 
@@ -619,7 +603,7 @@ __device__ __forceinline__ void tail_rows(int n, const int* __restrict__ rp, con
 }
 
 template <class V>
-__global__ void __launch_bounds__(kTailThreads) k_vc_tail(TailArgs<V> a) {
+__global__ void __launch_bounds__(kTailThreads, 1) k_vc_tail(TailArgs<V> a) {
     if (a.done && *a.done) return;
     const int L = a.nlev, s = a.s;
     // down
@@ -632,21 +616,21 @@ __global__ void __launch_bounds__(kTailThreads) k_vc_tail(TailArgs<V> a) {
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.n; i += gridDim.x * blockDim.x)
                 x[i] = v.omega * v.dinv[i] * __ldcg(v.b + i);
         }
-        if (!grid_barrier(a.bar, a.err)) return;
+        cluster_sync_all();
         for (int k = 2; k < s; ++k) {
             tail_rows<T_JAC, V>(v.n, v.Arp, v.Aci, v.Av, v.dinv, v.omega, v.b, x, t);
             double* tmp = x; x = t; t = tmp;
-            if (!grid_barrier(a.bar, a.err)) return;
+            cluster_sync_all();
         }
         if (x != v.x) {
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.n; i += gridDim.x * blockDim.x) v.x[i] = __ldcg(x + i);
-            if (!grid_barrier(a.bar, a.err)) return;
+            cluster_sync_all();
         }
         tail_rows<T_RES, V>(v.n, v.Arp, v.Aci, v.Av, v.dinv, v.omega, v.b, v.x, v.r);
-        if (!grid_barrier(a.bar, a.err)) return;
+        cluster_sync_all();
         double* cb = (l + 1 < L) ? a.lv[l + 1].b : a.cb;
         tail_rows<T_SPMV, V>(v.nc, v.Rrp, v.Rci, v.Rv, nullptr, 0.0, nullptr, v.r, cb);
-        if (!grid_barrier(a.bar, a.err)) return;
+        cluster_sync_all();
     }
     // coarsest: dense inverse, one warp per row
     {
@@ -658,24 +642,24 @@ __global__ void __launch_bounds__(kTailThreads) k_vc_tail(TailArgs<V> a) {
             acc = warp_sum(acc);
             if (lane == 0) a.cx[i] = acc;
         }
-        if (!grid_barrier(a.bar, a.err)) return;
+        cluster_sync_all();
     }
     // up
     for (int l = L - 1; l >= 0; --l) {
         const TailLevel<V>& v = a.lv[l];
         const double* cx = (l + 1 < L) ? a.lv[l + 1].x : a.cx;
         tail_rows<T_ADD, V>(v.n, v.Prp, v.Pci, v.Pv, nullptr, 0.0, nullptr, cx, v.x);
-        if (!grid_barrier(a.bar, a.err)) return;
+        cluster_sync_all();
         double* x = v.x;
         double* t = v.t;
         for (int k = 0; k < s; ++k) {
             tail_rows<T_JAC, V>(v.n, v.Arp, v.Aci, v.Av, v.dinv, v.omega, v.b, x, t);
             double* tmp = x; x = t; t = tmp;
-            if (!grid_barrier(a.bar, a.err)) return;
+            cluster_sync_all();
         }
         if (x != v.x) {
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.n; i += gridDim.x * blockDim.x) v.x[i] = __ldcg(x + i);
-            if (!grid_barrier(a.bar, a.err)) return;
+            cluster_sync_all();
         }
     }
 }
@@ -690,7 +674,6 @@ static void launch_tail(cfa_ctx* ctx, cfa_amg* amg, int l0, const int* done) {
     a.cinv = amg->coarse_inv.p;
     a.cb = amg->cb64.p;
     a.cx = amg->cx64.p;
-    a.bar = amg->tail_bar.p;
     a.err = amg->err.p;
     a.done = done;
     for (int k = 0; k < L; ++k) {
@@ -707,30 +690,55 @@ static void launch_tail(cfa_ctx* ctx, cfa_amg* amg, int l0, const int* done) {
         t.omega = Lv.omega;
         t.x = Lv.x64.p; t.t = Lv.t64.p; t.b = Lv.b64.p; t.r = Lv.r64.p;
     }
-    void* args[] = {&a};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(amg->tail_grid, 1, 1);
+    cfg.blockDim = dim3(kTailThreads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = amg->tail_grid;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     ctx->launches++;
-    cudaLaunchCooperativeKernel((const void*)k_vc_tail<V>, amg->tail_grid, kTailThreads, args, 0, ctx->stream);
+    cudaLaunchKernelEx(&cfg, k_vc_tail<V>, a);
 }
 
-// Chooses the first tail level (rows <= tail_rows) and the co-resident grid.
+// Chooses the first tail level (rows <= tail_rows, default: one row per thread of the cluster) and
+// the cluster size (16 CTAs where the GPU allows a non-portable cluster of 16, else 8).
 static cfa_status plan_tail(cfa_ctx* ctx, cfa_amg* amg) {
     amg->tail_level = -1;
+    const void* k = amg->opts.precision == CFA_MIXED ? (const void*)k_vc_tail<float> : (const void*)k_vc_tail<double>;
+    int csize = 0;
+    for (int c : {16, 8}) {
+        if (c == 16) cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(c, 1, 1);
+        cfg.blockDim = dim3(kTailThreads, 1, 1);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = c;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, k, &cfg) == cudaSuccess && nclusters > 0) { csize = c; break; }
+        cudaGetLastError();
+    }
+    if (csize == 0) return CFA_OK;
     const char* e = std::getenv("CFA_TAIL_ROWS");
-    const int tail_rows = e ? std::atoi(e) : 100000;
-    if (tail_rows <= 0 || amg->levels.size() > (size_t)kTailMaxLevels + 1) return CFA_OK;
+    const int tail_rows = e ? std::atoi(e) : csize * kTailThreads;
+    if (tail_rows <= 0) return CFA_OK;
     for (int l = 1; l < (int)amg->levels.size(); ++l)
         if (amg->levels[l].A.rows <= tail_rows) { amg->tail_level = l; break; }
     if (amg->tail_level < 0 || (int)amg->levels.size() - amg->tail_level > kTailMaxLevels) {
         amg->tail_level = -1;
         return CFA_OK;
     }
-    int per_sm = 0;
-    const void* k = amg->opts.precision == CFA_MIXED ? (const void*)k_vc_tail<float> : (const void*)k_vc_tail<double>;
-    CFA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTailThreads, 0));
-    if (per_sm < 1) { amg->tail_level = -1; return CFA_OK; }
-    amg->tail_grid = std::min(per_sm, 2) * ctx->num_sms;
-    CFA_CUDA(amg->tail_bar.ensure(2));
-    CFA_CUDA(cudaMemsetAsync(amg->tail_bar.p, 0, 2 * sizeof(unsigned), ctx->stream));
+    amg->tail_grid = csize;
     return CFA_OK;
 }
 
@@ -805,55 +813,52 @@ cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, co
 // =============================================================================================
 // setup driver
 // =============================================================================================
-// Exact-order SpGEMM C = A B into C (device CSR).
-static cfa_status spgemm(cfa_ctx* ctx, int ar, int bc, const int* arp, const int* aci, const double* av, const int* brp,
-                         const int* bci, const double* bv, DCsr& C) {
-    DevBuf<int> ub, cnt;
-    DevBuf<long long> off;
-    CFA_CUDA(ub.ensure(ar + 1));
-    CFA_CUDA(off.ensure(ar + 1));
-    CFA_CUDA(cnt.ensure(ar + 1));
-    CFA_CUDA(cudaMemsetAsync(ub.p + ar, 0, sizeof(int), ctx->stream));
-    CFA_LAUNCH(ctx, k_sg_ub, ceil_div(ar, kThreads), kThreads, 0, ar, arp, aci, brp, ub.p);
-    // 64-bit offsets of the per-row scratch regions (host scan)
-    std::vector<int> h_ub(ar + 1);
-    CFA_CUDA(cudaMemcpyAsync(h_ub.data(), ub.p, (ar + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+// Exact-order SpGEMM C = A B into C (device CSR), temporaries from the setup scratch.
+static cfa_status spgemm(cfa_ctx* ctx, SetupScratch& S, int ar, int bc, const int* arp, const int* aci, const double* av,
+                         const int* brp, const int* bci, const double* bv, DCsr& C) {
+    CFA_CUDA(S.sg_ub.ensure(ar + 1));
+    CFA_CUDA(S.sg_off.ensure(ar + 1));
+    CFA_CUDA(S.sg_cnt.ensure(ar + 1));
+    CFA_CUDA(S.h_ub.ensure(ar + 1));
+    CFA_CUDA(S.h_off.ensure(ar + 1));
+    CFA_CUDA(S.h_cnt.ensure(ar + 1));
+    CFA_LAUNCH(ctx, k_sg_ub, ceil_div(ar, kThreads), kThreads, 0, ar, arp, aci, brp, S.sg_ub.p);
+    CFA_CUDA(cudaMemcpyAsync(S.h_ub.p, S.sg_ub.p, ar * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-    std::vector<long long> h_off(ar + 1, 0);
-    for (int i = 0; i < ar; ++i) h_off[i + 1] = h_off[i] + h_ub[i];
+    long long* h_off = S.h_off.p;
+    h_off[0] = 0;
+    for (int i = 0; i < ar; ++i) h_off[i + 1] = h_off[i] + S.h_ub.p[i];
     const long long total = h_off[ar];
-    CFA_CUDA(cudaMemcpyAsync(off.p, h_off.data(), (ar + 1) * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
-    DevBuf<int> scol;
-    DevBuf<double> sval;
-    CFA_CUDA(scol.ensure(std::max<long long>(total, 1)));
-    CFA_CUDA(sval.ensure(std::max<long long>(total, 1)));
-    CFA_LAUNCH(ctx, k_sg_accum, ceil_div(ar, 128), 128, 0, ar, arp, aci, av, brp, bci, bv, off.p, scol.p, sval.p, cnt.p);
-    std::vector<int> h_cnt(ar);
-    CFA_CUDA(cudaMemcpyAsync(h_cnt.data(), cnt.p, ar * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(S.sg_off.p, h_off, (ar + 1) * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
+    CFA_CUDA(S.sg_scol.ensure(std::max<long long>(total, 1)));
+    CFA_CUDA(S.sg_sval.ensure(std::max<long long>(total, 1)));
+    CFA_LAUNCH(ctx, k_sg_accum, ceil_div(ar, 128), 128, 0, ar, arp, aci, av, brp, bci, bv, (const long long*)S.sg_off.p,
+               S.sg_scol.p, S.sg_sval.p, S.sg_cnt.p);
+    CFA_CUDA(cudaMemcpyAsync(S.h_cnt.p, S.sg_cnt.p, ar * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-    std::vector<int> h_rp(ar + 1, 0);
-    for (int i = 0; i < ar; ++i) h_rp[i + 1] = h_rp[i] + h_cnt[i];
+    int* h_rp = S.h_ub.p;   // reuse: C row pointer
+    h_rp[0] = 0;
+    for (int i = 0; i < ar; ++i) h_rp[i + 1] = h_rp[i] + S.h_cnt.p[i];
     C.rows = ar;
     C.cols = bc;
     C.nnz = h_rp[ar];
     CFA_CUDA(C.rp.ensure(ar + 1));
     CFA_CUDA(C.ci.ensure(std::max(C.nnz, 1)));
     CFA_CUDA(C.v.ensure(std::max(C.nnz, 1)));
-    CFA_CUDA(cudaMemcpyAsync(C.rp.p, h_rp.data(), (ar + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    CFA_LAUNCH(ctx, k_sg_copy, ceil_div(ar, kThreads), kThreads, 0, ar, off.p, scol.p, sval.p, C.rp.p, C.ci.p, C.v.p);
+    CFA_CUDA(cudaMemcpyAsync(C.rp.p, h_rp, (ar + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CFA_LAUNCH(ctx, k_sg_copy, ceil_div(ar, kThreads), kThreads, 0, ar, (const long long*)S.sg_off.p,
+               (const int*)S.sg_scol.p, (const double*)S.sg_sval.p, (const int*)C.rp.p, C.ci.p, C.v.p);
     CFA_CHECK_LAUNCH();
-    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     return CFA_OK;
 }
 
 // T = A^T (csr_transpose, :847-862): entries of each column in ascending row order
-static cfa_status transpose(cfa_ctx* ctx, const DCsr& A, DCsr& T) {
+static cfa_status transpose(cfa_ctx* ctx, SetupScratch& S, const DCsr& A, DCsr& T) {
     const int m = A.nnz;
-    DevBuf<int> keys_out, idx, perm, row_of;
-    CFA_CUDA(keys_out.ensure(std::max(m, 1)));
-    CFA_CUDA(idx.ensure(std::max(m, 1)));
-    CFA_CUDA(perm.ensure(std::max(m, 1)));
-    CFA_CUDA(row_of.ensure(std::max(m, 1)));
+    CFA_CUDA(S.tr_keys.ensure(std::max(m, 1)));
+    CFA_CUDA(S.tr_idx.ensure(std::max(m, 1)));
+    CFA_CUDA(S.tr_perm.ensure(std::max(m, 1)));
+    CFA_CUDA(S.tr_row_of.ensure(std::max(m, 1)));
     T.rows = A.cols;
     T.cols = A.rows;
     T.nnz = m;
@@ -861,29 +866,28 @@ static cfa_status transpose(cfa_ctx* ctx, const DCsr& A, DCsr& T) {
     CFA_CUDA(T.ci.ensure(std::max(m, 1)));
     CFA_CUDA(T.v.ensure(std::max(m, 1)));
     if (m > 0) {
-        CFA_LAUNCH(ctx, k_iota, ceil_div(m, kThreads), kThreads, 0, m, idx.p);
-        CFA_LAUNCH(ctx, k_entry_rows, ceil_div(A.rows, kThreads), kThreads, 0, A.rows, A.rp.p, row_of.p);
+        CFA_LAUNCH(ctx, k_iota, ceil_div(m, kThreads), kThreads, 0, m, S.tr_idx.p);
+        CFA_LAUNCH(ctx, k_entry_rows, ceil_div(A.rows, kThreads), kThreads, 0, A.rows, (const int*)A.rp.p, S.tr_row_of.p);
         int bits = 1;
         while ((1LL << bits) <= A.cols) ++bits;
         size_t tmp_bytes = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, A.ci.p, keys_out.p, idx.p, perm.p, m, 0, bits, ctx->stream);
-        DevBuf<char> tmp;
-        CFA_CUDA(tmp.ensure(tmp_bytes + 16));
-        CFA_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, A.ci.p, keys_out.p, idx.p, perm.p, m, 0, bits,
-                                                 ctx->stream));
+        cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, A.ci.p, S.tr_keys.p, S.tr_idx.p, S.tr_perm.p, m, 0, bits,
+                                        ctx->stream);
+        CFA_CUDA(S.cub_tmp.ensure(tmp_bytes + 16));
+        CFA_CUDA(cub::DeviceRadixSort::SortPairs(S.cub_tmp.p, tmp_bytes, A.ci.p, S.tr_keys.p, S.tr_idx.p, S.tr_perm.p, m,
+                                                 0, bits, ctx->stream));
         ctx->launches += 4;
-        CFA_LAUNCH(ctx, k_transpose_fill, ceil_div(m, kThreads), kThreads, 0, m, perm.p, row_of.p, A.v.p, T.ci.p, T.v.p);
+        CFA_LAUNCH(ctx, k_transpose_fill, ceil_div(m, kThreads), kThreads, 0, m, (const int*)S.tr_perm.p,
+                   (const int*)S.tr_row_of.p, (const double*)A.v.p, T.ci.p, T.v.p);
     }
-    CFA_LAUNCH(ctx, k_ptr_from_sorted, ceil_div(m + 1, kThreads), kThreads, 0, A.cols, m, keys_out.p, T.rp.p);
+    CFA_LAUNCH(ctx, k_ptr_from_sorted, ceil_div(m + 1, kThreads), kThreads, 0, A.cols, m, (const int*)S.tr_keys.p, T.rp.p);
     CFA_CHECK_LAUNCH();
-    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     return CFA_OK;
 }
 
 // Greedy 3-phase aggregation of smoothed_prolongator (:1321-1348) on the host strength flags.
-static int aggregate_host(int n, const std::vector<int>& rp, const std::vector<int>& ci,
-                          const std::vector<unsigned char>& strong, std::vector<int>& agg) {
-    agg.assign(n, -1);
+static int aggregate_host(int n, const int* rp, const int* ci, const unsigned char* strong, int* agg) {
+    for (int i = 0; i < n; ++i) agg[i] = -1;
     int na = 0;
     for (int i = 0; i < n; ++i) {
         if (agg[i] >= 0) continue;
@@ -895,13 +899,13 @@ static int aggregate_host(int n, const std::vector<int>& rp, const std::vector<i
         for (int a = rp[i]; a < rp[i + 1]; ++a) if (strong[a]) agg[ci[a]] = na;
         ++na;
     }
-    std::vector<int> agg2(agg);
+    std::vector<int> agg2(agg, agg + n);
     for (int i = 0; i < n; ++i) {
         if (agg[i] >= 0) continue;
         for (int a = rp[i]; a < rp[i + 1]; ++a)
             if (strong[a] && agg[ci[a]] >= 0) { agg2[i] = agg[ci[a]]; break; }
     }
-    agg.swap(agg2);
+    std::copy(agg2.begin(), agg2.end(), agg);
     for (int i = 0; i < n; ++i) {
         if (agg[i] >= 0) continue;
         agg[i] = na;
@@ -932,33 +936,46 @@ static cfa_status to_float(cfa_ctx* ctx, DCsr& M) {
     return CFA_OK;
 }
 
+// 1 + 0.1 sin(1 + i) for i < n: the power-iteration start vector (host libm, as the reference),
+// computed once per process.
+static const std::vector<double>& start_vector(int n) {
+    static std::vector<double> x0;
+    if ((int)x0.size() < n) {
+        const size_t old = x0.size();
+        x0.resize(n);
+        for (size_t i = old; i < (size_t)n; ++i) x0[i] = 1.0 + 0.1 * std::sin(1.0 + (double)i);
+    }
+    return x0;
+}
+
 // rho(D^-1 A) by 20 power iterations (spectral_radius_DinvA, :1276-1304), on the device.
 static cfa_status spectral_radius(cfa_ctx* ctx, cfa_amg* amg, const DCsr& A, const double* dinv, double* rho) {
+    SetupScratch& S = amg->scratch;
     const int n = A.rows, nch = (n + 4095) / 4096;
-    if ((int)amg->host_x0.size() < n) {
-        const size_t old = amg->host_x0.size();
-        amg->host_x0.resize(n);
-        for (size_t i = old; i < (size_t)n; ++i) amg->host_x0[i] = 1.0 + 0.1 * std::sin(1.0 + (double)i);
+    if (!amg->x0.p || amg->x0.cap < (size_t)n) {
+        const std::vector<double>& h = start_vector(n);
         CFA_CUDA(amg->x0.ensure(n));
-        CFA_CUDA(cudaMemcpyAsync(amg->x0.p, amg->host_x0.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        CFA_CUDA(cudaMemcpy(amg->x0.p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice));
     }
-    DevBuf<double> x, y, py, px, st;
-    CFA_CUDA(x.ensure(n));
-    CFA_CUDA(y.ensure(n));
-    CFA_CUDA(py.ensure(nch));
-    CFA_CUDA(px.ensure(nch));
-    CFA_CUDA(st.ensure(2));
-    CFA_CUDA(cudaMemcpyAsync(x.p, amg->x0.p, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CFA_CUDA(S.pow_x.ensure(n));
+    CFA_CUDA(S.pow_y.ensure(n));
+    CFA_CUDA(S.pow_py.ensure(nch));
+    CFA_CUDA(S.pow_px.ensure(nch));
+    CFA_CUDA(S.pow_st.ensure(2));
+    CFA_CUDA(S.h_st.ensure(2));
+    CFA_CUDA(cudaMemcpyAsync(S.pow_x.p, amg->x0.p, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     for (int it = 0; it < 20; ++it) {
-        CFA_LAUNCH(ctx, k_pow_y, ceil_div(n, kThreads), kThreads, 0, n, A.rp.p, A.ci.p, A.v.p, dinv, x.p, y.p);
-        CFA_LAUNCH(ctx, k_pow_chunks, ceil_div(nch, 64), 64, 0, n, nch, x.p, y.p, py.p, px.p);
-        CFA_LAUNCH(ctx, k_pow_finish, 1, 32, 0, nch, py.p, px.p, st.p);
-        CFA_LAUNCH(ctx, k_pow_scale, ceil_div(n, kThreads), kThreads, 0, n, y.p, st.p, x.p);
+        CFA_LAUNCH(ctx, k_pow_y, ceil_div(n, kThreads), kThreads, 0, n, (const int*)A.rp.p, (const int*)A.ci.p,
+                   (const double*)A.v.p, dinv, (const double*)S.pow_x.p, S.pow_y.p);
+        CFA_LAUNCH(ctx, k_pow_chunks, ceil_div(nch, 64), 64, 0, n, nch, (const double*)S.pow_x.p,
+                   (const double*)S.pow_y.p, S.pow_py.p, S.pow_px.p);
+        CFA_LAUNCH(ctx, k_pow_finish, 1, 32, 0, nch, (const double*)S.pow_py.p, (const double*)S.pow_px.p, S.pow_st.p);
+        CFA_LAUNCH(ctx, k_pow_scale, ceil_div(n, kThreads), kThreads, 0, n, (const double*)S.pow_y.p,
+                   (const double*)S.pow_st.p, S.pow_x.p);
     }
-    double h[2];
-    CFA_CUDA(cudaMemcpyAsync(h, st.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(S.h_st.p, S.pow_st.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-    *rho = std::max(h[1], 1.0e-12) * 1.05;
+    *rho = std::max(S.h_st.p[1], 1.0e-12) * 1.05;
     return CFA_OK;
 }
 
@@ -987,89 +1004,108 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
         tp = now;
     };
     const cfa_amg_opts& o = amg->opts;
+    // the previous hierarchy's levels are recycled: their buffers only grow (the reference keeps
+    // them as `spare`, src/cfa/linalg.cuh:964, :1266-1272)
+    std::vector<AmgLevel> pool = std::move(amg->levels);
     amg->levels.clear();
-    amg->version = next_uid();
-    DCsr A;
-    CFA_PROPAGATE(copy_csr(ctx, n, nnz, d_rp, d_ci, d_v, A));
-    phase(0);
-    while (A.rows > o.coarse_target && (int)amg->levels.size() < o.max_levels - 1) {
-        const int m = A.rows;
+    auto take = [&](size_t l) {
         AmgLevel L;
+        if (l < pool.size()) L = std::move(pool[l]);
+        else if (l == pool.size() && amg->coarse_holder.A.rp.p) L.A = std::move(amg->coarse_holder.A);
+        return L;
+    };
+    amg->version = next_uid();
+    AmgLevel cur = take(0);
+    CFA_PROPAGATE(copy_csr(ctx, n, nnz, d_rp, d_ci, d_v, cur.A));
+    phase(0);
+    for (;;) {
+        DCsr& A = cur.A;
+        if (!(A.rows > o.coarse_target && (int)amg->levels.size() < o.max_levels - 1)) break;
+        const int m = A.rows;
+        AmgLevel& L = cur;
         CFA_CUDA(L.dinv.ensure(m));
         CFA_LAUNCH(ctx, k_amg_dinv, ceil_div(m, kThreads), kThreads, 0, m, A.rp.p, A.ci.p, A.v.p, L.dinv.p);
         double rho = 1.0;
         CFA_PROPAGATE(spectral_radius(ctx, amg, A, L.dinv.p, &rho));
         const double omega = 4.0 / (3.0 * rho);
         phase(1);
-        // strength on the device, aggregation on the host
-        DevBuf<unsigned char> strong;
-        CFA_CUDA(strong.ensure(std::max(A.nnz, 1)));
+        // strength on the device, aggregation on the host (pinned staging)
+        SetupScratch& S = amg->scratch;
+        CFA_CUDA(S.strong.ensure(std::max(A.nnz, 1)));
         CFA_LAUNCH(ctx, k_strength, ceil_div(m, kThreads), kThreads, 0, m, A.rp.p, A.ci.p, A.v.p, L.dinv.p, o.theta,
-                   strong.p);
-        std::vector<int> h_rp(m + 1), h_ci(A.nnz);
-        std::vector<unsigned char> h_strong(A.nnz);
-        CFA_CUDA(cudaMemcpyAsync(h_rp.data(), A.rp.p, (m + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-        CFA_CUDA(cudaMemcpyAsync(h_ci.data(), A.ci.p, (size_t)A.nnz * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-        CFA_CUDA(cudaMemcpyAsync(h_strong.data(), strong.p, (size_t)A.nnz, cudaMemcpyDeviceToHost, ctx->stream));
+                   S.strong.p);
+        CFA_CUDA(S.h_rp.ensure(m + 1));
+        CFA_CUDA(S.h_ci.ensure(std::max(A.nnz, 1)));
+        CFA_CUDA(S.h_strong.ensure(std::max(A.nnz, 1)));
+        CFA_CUDA(cudaMemcpyAsync(S.h_rp.p, A.rp.p, (m + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CFA_CUDA(cudaMemcpyAsync(S.h_ci.p, A.ci.p, (size_t)A.nnz * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CFA_CUDA(cudaMemcpyAsync(S.h_strong.p, S.strong.p, (size_t)A.nnz, cudaMemcpyDeviceToHost, ctx->stream));
         CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-        std::vector<int> agg;
-        const int na = aggregate_host(m, h_rp, h_ci, h_strong, agg);
+        CFA_CUDA(S.h_agg.ensure(m));
+        const int na = aggregate_host(m, S.h_rp.p, S.h_ci.p, S.h_strong.p, S.h_agg.p);
         if (na >= (int)(0.85 * m) || na == 0) break;   // coarsening stalled (:1019)
+        const int* agg = S.h_agg.p;
         std::vector<int> size(na, 0);
         for (int i = 0; i < m; ++i) size[agg[i]]++;
-        std::vector<double> p0v(m);
-        std::vector<int> p0rp(m + 1);
-        for (int i = 0; i < m; ++i) { p0v[i] = 1.0 / std::sqrt((double)size[agg[i]]); p0rp[i] = i; }
-        p0rp[m] = m;
-        DevBuf<double> d_p0v;
-        DevBuf<int> d_p0rp;
+        CFA_CUDA(S.h_p0v.ensure(m));
+        CFA_CUDA(S.h_p0rp.ensure(m + 1));
+        for (int i = 0; i < m; ++i) { S.h_p0v.p[i] = 1.0 / std::sqrt((double)size[agg[i]]); S.h_p0rp.p[i] = i; }
+        S.h_p0rp.p[m] = m;
         CFA_CUDA(L.agg.ensure(m));
-        CFA_CUDA(d_p0v.ensure(m));
-        CFA_CUDA(d_p0rp.ensure(m + 1));
-        CFA_CUDA(cudaMemcpyAsync(L.agg.p, agg.data(), m * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-        CFA_CUDA(cudaMemcpyAsync(d_p0v.p, p0v.data(), m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-        CFA_CUDA(cudaMemcpyAsync(d_p0rp.p, p0rp.data(), (m + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        CFA_CUDA(S.p0v.ensure(m));
+        CFA_CUDA(S.p0rp.ensure(m + 1));
+        DevBuf<double>& d_p0v = S.p0v;
+        DevBuf<int>& d_p0rp = S.p0rp;
+        CFA_CUDA(cudaMemcpyAsync(L.agg.p, agg, m * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        CFA_CUDA(cudaMemcpyAsync(d_p0v.p, S.h_p0v.p, m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        CFA_CUDA(cudaMemcpyAsync(d_p0rp.p, S.h_p0rp.p, (m + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
         phase(2);
         // AP0 = A P0, then P = P0 - omega D^-1 A P0
-        DCsr AP0;
-        CFA_PROPAGATE(spgemm(ctx, m, na, A.rp.p, A.ci.p, A.v.p, d_p0rp.p, L.agg.p, d_p0v.p, AP0));
-        DevBuf<int> cnt;
+        DCsr& AP0 = S.AP0;
+        CFA_PROPAGATE(spgemm(ctx, S, m, na, A.rp.p, A.ci.p, A.v.p, d_p0rp.p, L.agg.p, d_p0v.p, AP0));
+        DevBuf<int>& cnt = S.cnt;
         CFA_CUDA(cnt.ensure(m));
         CFA_LAUNCH(ctx, k_p_rows, ceil_div(m, kThreads), kThreads, 0, m, AP0.rp.p, AP0.ci.p, AP0.v.p, L.agg.p, d_p0v.p,
                    L.dinv.p, omega, (const int*)nullptr, (int*)nullptr, (double*)nullptr, cnt.p);
-        std::vector<int> h_cnt(m), h_prp(m + 1, 0);
-        CFA_CUDA(cudaMemcpyAsync(h_cnt.data(), cnt.p, m * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CFA_CUDA(S.h_cnt.ensure(m));
+        CFA_CUDA(S.h_rp.ensure(m + 1));
+        CFA_CUDA(cudaMemcpyAsync(S.h_cnt.p, cnt.p, m * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-        for (int i = 0; i < m; ++i) h_prp[i + 1] = h_prp[i] + h_cnt[i];
+        int* h_prp = S.h_rp.p;
+        h_prp[0] = 0;
+        for (int i = 0; i < m; ++i) h_prp[i + 1] = h_prp[i] + S.h_cnt.p[i];
         L.P.rows = m;
         L.P.cols = na;
         L.P.nnz = h_prp[m];
         CFA_CUDA(L.P.rp.ensure(m + 1));
         CFA_CUDA(L.P.ci.ensure(std::max(L.P.nnz, 1)));
         CFA_CUDA(L.P.v.ensure(std::max(L.P.nnz, 1)));
-        CFA_CUDA(cudaMemcpyAsync(L.P.rp.p, h_prp.data(), (m + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        CFA_CUDA(cudaMemcpyAsync(L.P.rp.p, h_prp, (m + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
         CFA_LAUNCH(ctx, k_p_rows, ceil_div(m, kThreads), kThreads, 0, m, AP0.rp.p, AP0.ci.p, AP0.v.p, L.agg.p, d_p0v.p,
                    L.dinv.p, omega, L.P.rp.p, L.P.ci.p, L.P.v.p, cnt.p);
         CFA_CHECK_LAUNCH();
         phase(3);
         // R = P^T, A_c = R (A P)
-        CFA_PROPAGATE(transpose(ctx, L.P, L.R));
+        CFA_PROPAGATE(transpose(ctx, S, L.P, L.R));
         phase(4);
-        DCsr AP, Ac;
-        CFA_PROPAGATE(spgemm(ctx, m, na, A.rp.p, A.ci.p, A.v.p, L.P.rp.p, L.P.ci.p, L.P.v.p, AP));
-        CFA_PROPAGATE(spgemm(ctx, na, na, L.R.rp.p, L.R.ci.p, L.R.v.p, AP.rp.p, AP.ci.p, AP.v.p, Ac));
+        AmgLevel next = take(amg->levels.size() + 1);
+        DCsr& AP = S.AP;
+        CFA_PROPAGATE(spgemm(ctx, S, m, na, A.rp.p, A.ci.p, A.v.p, L.P.rp.p, L.P.ci.p, L.P.v.p, AP));
+        CFA_PROPAGATE(spgemm(ctx, S, na, na, L.R.rp.p, L.R.ci.p, L.R.v.p, AP.rp.p, AP.ci.p, AP.v.p, next.A));
         phase(5);
         L.omega = omega;
-        L.A = std::move(A);
         CFA_PROPAGATE(level_vectors(ctx, amg, L, m));
-        amg->levels.push_back(std::move(L));
-        A = std::move(Ac);
+        amg->levels.push_back(std::move(cur));
+        cur = std::move(next);
     }
     // coarsest level: dense Cholesky inverse on the device
+    amg->coarse_holder = std::move(cur);
+    DCsr& A = amg->coarse_holder.A;
     const int cn = A.rows;
     amg->coarse_n = cn;
-    DevBuf<double> M, colbuf;
-    DevBuf<int> err;
+    DevBuf<double>& M = amg->scratch.M;
+    DevBuf<double>& colbuf = amg->scratch.colbuf;
+    DevBuf<int>& err = amg->scratch.ierr;
     CFA_CUDA(M.ensure((size_t)cn * cn + 1));
     CFA_CUDA(colbuf.ensure((size_t)cn * cn + 1));
     CFA_CUDA(amg->coarse_inv.ensure((size_t)cn * cn + 1));
@@ -1112,11 +1148,12 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
         for (AmgLevel& L : amg->levels) {
             for (DCsr* M : {&L.A, &L.P, &L.R}) {
                 TiledCsr& T = M == &L.A ? L.tA : M == &L.P ? L.tP : L.tR;
-                std::vector<int> h_rp(M->rows + 1);
-                CFA_CUDA(cudaMemcpyAsync(h_rp.data(), M->rp.p, (M->rows + 1) * sizeof(int), cudaMemcpyDeviceToHost,
+                HostBuf<int>& hr = amg->scratch.h_rp;
+                CFA_CUDA(hr.ensure(M->rows + 1));
+                CFA_CUDA(cudaMemcpyAsync(hr.p, M->rp.p, (M->rows + 1) * sizeof(int), cudaMemcpyDeviceToHost,
                                          ctx->stream));
                 CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-                CFA_PROPAGATE(plan_tiled(ctx, h_rp.data(), M->rows, 1, vb, T));
+                CFA_PROPAGATE(plan_tiled(ctx, hr.p, M->rows, 1, vb, T));
                 CFA_PROPAGATE(pack_tiled(ctx, M->rp.p, M->ci.p, M->v.p, nullptr, nullptr, T));
             }
         }

@@ -28,9 +28,44 @@ struct AmgLevel {
     DevBuf<float> x32, t32, b32, r32;
 };
 
+// Pinned, grow-only host buffer
+template <class T>
+struct HostBuf {
+    T* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t count) {
+        if (count <= cap && p) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        const size_t c = count + count / 2 + 64;
+        cudaError_t e = cudaMallocHost(&p, c * sizeof(T));
+        cap = e == cudaSuccess ? c : 0;
+        return e;
+    }
+    ~HostBuf() { if (p) cudaFreeHost(p); }
+    HostBuf() = default;
+    HostBuf(const HostBuf&) = delete;
+    HostBuf& operator=(const HostBuf&) = delete;
+};
+
+// Setup temporaries, kept across setups (grow-only): no allocation in a repeated setup.
+struct SetupScratch {
+    DevBuf<int> sg_ub, sg_cnt, sg_scol, tr_keys, tr_idx, tr_perm, tr_row_of, cnt, p0rp, ierr;
+    DevBuf<long long> sg_off;
+    DevBuf<double> sg_sval, pow_x, pow_y, pow_py, pow_px, pow_st, p0v, M, colbuf;
+    DevBuf<unsigned char> strong;
+    DevBuf<char> cub_tmp;
+    HostBuf<int> h_rp, h_ci, h_cnt, h_ub, h_agg, h_p0rp;
+    HostBuf<long long> h_off;
+    HostBuf<unsigned char> h_strong;
+    HostBuf<double> h_p0v, h_st;
+    DCsr AP0, AP;
+};
+
 }  // namespace cfa
 
 struct cfa_amg {
+    cfa::SetupScratch scratch;
     cfa_amg_opts opts{};
     std::vector<cfa::AmgLevel> levels;   // levels with a prolongator (reference: levels)
     int coarse_n = 0;
@@ -46,10 +81,10 @@ struct cfa_amg {
     // 0 copy, 1 D^-1 + rho, 2 strength + aggregation, 3 P smoothing, 4 transpose, 5 Galerkin,
     // 6 tile packing, 7 coarse inverse
     double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    // coarse tail: levels >= tail_level run inside one cooperative kernel (grid barriers)
+    // coarse tail: levels >= tail_level run inside one kernel launched as one thread-block cluster
     int tail_level = -1;
     int tail_grid = 0;
-    cfa::DevBuf<unsigned> tail_bar;      // {count, generation}
+    cfa::AmgLevel coarse_holder;         // the coarsest operator (its buffers recycled by the next setup)
     cfa::DevBuf<int> err;                // tile pipeline error word
 };
 

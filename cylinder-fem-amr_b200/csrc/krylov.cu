@@ -189,6 +189,13 @@ k_opt_b(TileView tv, const double* __restrict__ inv_m, const double* __restrict_
         for (int base = 0; base < nr; base += kTileThreads / TPR) {
             const int lr = base + (int)threadIdx.x / TPR, lane = threadIdx.x % TPR;
             const bool valid = lr < nr;
+            const int row = r0 + lr;
+            double im = 0.0, zi = 0.0, pi = 0.0;
+            if (valid && lane == 0) {
+                im = inv_m[row];
+                zi = z[row];
+                if (fuse) pi = p[row];
+            }
             double sx = 0.0, sy = 0.0;
             if (valid)
 #pragma unroll 4
@@ -201,11 +208,9 @@ k_opt_b(TileView tv, const double* __restrict__ inv_m, const double* __restrict_
             sx = group_reduce<TPR>(sx);
             sy = group_reduce<TPR>(sy);
             if (valid && lane == 0) {
-                const int row = r0 + lr;
-                const double im = inv_m[row];
                 gx[row] = sx * im;
                 gy[row] = sy * im;
-                if (p_new) p_new[row] = fuse ? z[row] + beta * p[row] : z[row];
+                if (p_new) p_new[row] = fuse ? zi + beta * pi : zi;
             }
         }
     });
@@ -234,6 +239,13 @@ k_opt_k(TileView tv, const int* __restrict__ tag, OutletBc bc, const double* __r
         for (int base = 0; base < nr; base += kTileThreads / TPR) {
             const int lr = base + (int)threadIdx.x / TPR, lane = threadIdx.x % TPR;
             const bool valid = lr < nr;
+            const int row = r0 + lr;
+            bool dir = true;
+            double pi = 0.0;
+            if (valid && lane == 0) {
+                if (OSS) dir = pressure_dirichlet(row, tag[row], bc);
+                pi = FUSEP ? (fuse ? z[row] + beta * p[row] : z[row]) : pn_buf[row];
+            }
             double s = 0.0, so = 0.0;
             if (valid)
 #pragma unroll 4
@@ -246,10 +258,8 @@ k_opt_k(TileView tv, const int* __restrict__ tag, OutletBc bc, const double* __r
             s = group_reduce<TPR>(s);
             if (OSS) so = group_reduce<TPR>(so);
             if (valid && lane == 0) {
-                const int row = r0 + lr;
-                if (OSS && !pressure_dirichlet(row, tag[row], bc)) s -= so;
+                if (OSS && !dir) s -= so;
                 q[row] = s;
-                const double pi = FUSEP ? (fuse ? z[row] + beta * p[row] : z[row]) : pn_buf[row];
                 if (FUSEP && pn_buf) pn_buf[row] = pi;
                 if (DOT) acc += pi * s;
             }
