@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cstring>
 #include <cstdlib>
+#include <mutex>
 
 #include "amg.cuh"
 #include "ilu.cuh"
@@ -1600,6 +1601,93 @@ cfa_status cfa_bicgstab_solve(cfa_ctx* ctx, int n, const int* rp, const int* ci,
         rep->solve_ms = ms;
     }
     return fin ? CFA_OK : CFA_NOT_CONVERGED;
+}
+
+}  // extern "C"
+
+// =============================================================================================
+// cfa_oss_apply_noalloc: the OSS apply with its intermediate vector in static device memory
+// =============================================================================================
+namespace cfa {
+
+// Largest mesh (nodes) cfa_oss_apply_noalloc accepts; its scratch is 2 * kOssStaticRows doubles
+// (8 MiB), reserved when the library's device code is loaded on a device.
+constexpr int kOssStaticRows = 1 << 19;
+
+// g = M_L^-1 B x of the OSS apply: [0, n) the x component, [kOssStaticRows, + n) the y component.
+// Nothing in it needs to start at zero: each call writes every entry it later reads.
+static __device__ __align__(256) double g_oss_static[2 * kOssStaticRows];
+
+// Pass 2 of the OSS apply on its own: out -= B^T_x g_x + B^T_y g_y on rows that are not pressure
+// Dirichlet rows (k_oss_apply_BT, src/cfa/fem_kernels.cuh:871-885); the same per-row summation
+// order as the operator kernel of cfa_oss_apply.
+template <int TPR>
+__global__ void k_oss_bt_sub(int n, int nnz, const int* __restrict__ rp, const int* __restrict__ ci,
+                             const double* __restrict__ oss, const int* __restrict__ tag, OutletBc bc,
+                             const double* __restrict__ gx, const double* __restrict__ gy, double* __restrict__ out) {
+    const double* BTx = oss + 2 * (size_t)nnz;
+    const double* BTy = oss + 3 * (size_t)nnz;
+    ROWS_BEGIN(TPR, n)
+    double so = 0.0;
+    if (valid)
+        for (int k = rp[row] + lane; k < rp[row + 1]; k += TPR) {
+            const int j = ci[k];
+            so += BTx[k] * gx[j] + BTy[k] * gy[j];
+        }
+    so = group_reduce<TPR>(so);
+    if (valid && lane == 0 && !pressure_dirichlet(row, tag[row], bc)) out[row] -= so;
+    ROWS_END
+}
+
+// Device address of g_oss_static on each device, looked up once per device (with that device
+// current) on the first call there.
+static cfa_status oss_static_scratch(cfa_ctx* ctx, double** out) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static double* addr[kMaxDevices] = {};
+    if (ctx->device < 0 || ctx->device >= kMaxDevices)
+        return set_error(ctx, CFA_BAD_ARG, "device ordinal out of range", __FILE__, __LINE__);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[ctx->device]) {
+        int cur = 0;
+        CFA_CUDA(cudaGetDevice(&cur));
+        if (cur != ctx->device) CFA_CUDA(cudaSetDevice(ctx->device));
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_oss_static);
+        if (cur != ctx->device) CFA_CUDA(cudaSetDevice(cur));
+        if (e != cudaSuccess) return set_error(ctx, CFA_CUDA_ERROR, cudaGetErrorString(e), __FILE__, __LINE__);
+        addr[ctx->device] = static_cast<double*>(p);
+    }
+    *out = addr[ctx->device];
+    return CFA_OK;
+}
+
+}  // namespace cfa
+
+extern "C" {
+
+cfa_status cfa_oss_apply_noalloc(cfa_ctx* ctx, const cfa_mesh* m, const double* oss_val, const double* inv_m,
+                                 const double* in, double* out) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(m && oss_val && inv_m && in && out);
+    const int n = m->n;
+    if (n > kOssStaticRows)
+        return set_error(ctx, CFA_BAD_ARG,
+                         "cfa_oss_apply_noalloc: the mesh has more nodes than its static scratch holds (524288)",
+                         __FILE__, __LINE__);
+    double* g = nullptr;
+    CFA_PROPAGATE(oss_static_scratch(ctx, &g));
+    double* gx = g;
+    double* gy = g + kOssStaticRows;
+    const int tpr = op_tpr(n, m->nnz);
+    const int grid = row_grid(ctx, n, tpr);
+    OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_op_b<TPR>), grid, kThreads, 0, n, m->nnz, m->rp, m->ci, oss_val, inv_m, in,
+                                  (const double*)nullptr, (const double*)nullptr, (double*)nullptr, gx, gy,
+                                  (const int*)nullptr));
+    OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_oss_bt_sub<TPR>), grid, kThreads, 0, n, m->nnz, m->rp, m->ci, oss_val,
+                                  m->tag, m->bc, (const double*)gx, (const double*)gy, out));
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
 }
 
 }  // extern "C"

@@ -151,6 +151,22 @@ cfa_status cfa_assemble_pressure_system(cfa_ctx* ctx, const cfa_mesh* mesh, cons
  * untouched. */
 cfa_status cfa_oss_apply(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_oss_val,
                          const double* d_inv_m, const double* d_in, double* d_out);
+/* cfa_oss_apply without any device allocation. This entry point has no counterpart in the
+ * reference. It is for callers that must not allocate device memory while they run: for example,
+ * a time-step loop whose device memory is all handed to another allocator, or one that cannot
+ * afford the device-wide synchronisation that cudaFree (and cudaMalloc, at times) implies.
+ * cfa_oss_apply grows a workspace on first use; this entry point keeps the intermediate vector
+ * g = M^-1 B d_in in a fixed static device array instead, and it does not synchronise.
+ * Limit: mesh->n <= 524288 nodes (the array is 8 MiB); larger meshes get CFA_BAD_ARG.
+ * Nothing needs to start at zero: every call writes each scratch entry it reads.
+ * Setup: the first call on each device looks up the array's address (with that device made
+ * current for the lookup) and must come before any stream capture on that device.
+ * There is one array per device and process: calls in flight at the same time on one device (two
+ * streams, contexts or threads) race on it. Order such calls, e.g. on one stream or with events.
+ * Result: the same d_out as cfa_oss_apply (same per-row summation order). Asynchronous on the
+ * context's stream. */
+cfa_status cfa_oss_apply_noalloc(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_oss_val,
+                                 const double* d_inv_m, const double* d_in, double* d_out);
 
 /* ---------------------------------------------------------------------------------------------
  * sparse kernels
