@@ -384,13 +384,31 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
                 if (OP == VC_ADD) xi = (T)y[row];
             }
             T s = (T)0;
-            if (valid)
-#pragma unroll 4
-                for (int e = rr[lr] + lane; e < rr[lr + 1]; e += TPR) {
-                    const int j = cs[e];
-                    if (OP == VC_PRE) s += (T)vv[e] * (omega * dinv[j] * (T)b[j]);
-                    else s += (T)vv[e] * x[j];
+            if (valid) {
+                const int end = rr[lr + 1];
+                for (int e0 = rr[lr] + lane; e0 < end; e0 += kGatherBatch * TPR) {
+                    // all loads of the batch first, then the sums in entry order
+                    V a[kGatherBatch];
+                    T g0[kGatherBatch];
+                    B g1[kGatherBatch];
+#pragma unroll
+                    for (int u = 0; u < kGatherBatch; ++u) {
+                        const int e = e0 + u * TPR;
+                        if (e < end) {
+                            const int j = cs[e];
+                            a[u] = vv[e];
+                            if (OP == VC_PRE) { g0[u] = dinv[j]; g1[u] = b[j]; }
+                            else g0[u] = x[j];
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kGatherBatch; ++u)
+                        if (e0 + u * TPR < end) {
+                            if (OP == VC_PRE) s += (T)a[u] * (omega * g0[u] * (T)g1[u]);
+                            else s += (T)a[u] * g0[u];
+                        }
                 }
+            }
 #pragma unroll
             for (int o = TPR / 2; o > 0; o /= 2) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
             if (valid && lane == 0) {
@@ -415,7 +433,7 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
 template <int OP, class V, class T, class B, class O>
 static void vct(cfa_ctx* ctx, bool dry, const TiledCsr& M, int* err, const T* dinv, T omega, const B* b, const T* x,
                 O* y, const int* done) {
-    const int tpr = M.tile_rows >= kTileThreads ? 1 : std::min(32, kTileThreads / std::max(M.tile_rows, 1));
+    const int tpr = M.tpr;
     const TileView tv = M.view(err);
     const TileLaunch L = tile_launch(ctx, M, nullptr);
     switch (tpr) {
@@ -706,10 +724,16 @@ static void launch_tail(cfa_ctx* ctx, cfa_amg* amg, int l0, const int* done) {
     cudaLaunchKernelEx(&cfg, k_vc_tail<V>, a);
 }
 
-// Chooses the first tail level (rows <= tail_rows, default: one row per thread of the cluster) and
-// the cluster size (16 CTAs where the GPU allows a non-portable cluster of 16, else 8).
+// The coarse tail is opt-in (CFA_TAIL_ROWS = largest level, in rows, that it takes over): on the
+// P1 pressure hierarchies measured (400k nodes: levels of 67k, 8.2k, 1.1k rows and a 230-row
+// coarse solve), one 16-SM cluster is no faster than the grid-wide kernels per level, whose
+// launches the solve graph already pipelines. Picks the cluster size (16 CTAs where the GPU
+// allows a non-portable cluster of 16, else 8).
 static cfa_status plan_tail(cfa_ctx* ctx, cfa_amg* amg) {
     amg->tail_level = -1;
+    const char* e = std::getenv("CFA_TAIL_ROWS");
+    const int tail_rows = e ? std::atoi(e) : 0;
+    if (tail_rows <= 0) return CFA_OK;
     const void* k = amg->opts.precision == CFA_MIXED ? (const void*)k_vc_tail<float> : (const void*)k_vc_tail<double>;
     int csize = 0;
     for (int c : {16, 8}) {
@@ -729,9 +753,6 @@ static cfa_status plan_tail(cfa_ctx* ctx, cfa_amg* amg) {
         cudaGetLastError();
     }
     if (csize == 0) return CFA_OK;
-    const char* e = std::getenv("CFA_TAIL_ROWS");
-    const int tail_rows = e ? std::atoi(e) : csize * kTailThreads;
-    if (tail_rows <= 0) return CFA_OK;
     for (int l = 1; l < (int)amg->levels.size(); ++l)
         if (amg->levels[l].A.rows <= tail_rows) { amg->tail_level = l; break; }
     if (amg->tail_level < 0 || (int)amg->levels.size() - amg->tail_level > kTailMaxLevels) {

@@ -50,6 +50,9 @@ __global__ void k_ilu_gather(int nl, int nu, int n, const int* __restrict__ l_sr
     if (e < n) dinv[e] = (T)(1.0 / lu[d_src[e]]);
 }
 
+// entries of a row whose loads the sweeps issue together
+constexpr int kIluBatch = 4;
+
 // Forward sweep of one colour for NR right-hand sides: y_i = r_i - sum_L l_ie y_e (unit L); the
 // last colour also divides by u_ii. T: factor/work precision; FP64 output written when a row is
 // final (last colour here, else in the backward sweep).
@@ -65,11 +68,24 @@ __global__ void k_ilu_lower(int m, int n, const int* __restrict__ rows, const in
     T acc[NR];
 #pragma unroll
     for (int c = 0; c < NR; ++c) acc[c] = (T)r[(size_t)c * n + i];
-    for (int e = lp[t]; e < lp[t + 1]; ++e) {
-        const T l = (T)lv[e];
-        const int j = lc[e];
+    const int end = lp[t + 1];
+    for (int e0 = lp[t]; e0 < end; e0 += kIluBatch) {
+        // the loads of a batch of entries first, then the updates in entry order
+        V l[kIluBatch];
+        T g[kIluBatch][NR];
 #pragma unroll
-        for (int c = 0; c < NR; ++c) acc[c] -= l * w[(size_t)c * n + j];
+        for (int u = 0; u < kIluBatch; ++u)
+            if (e0 + u < end) {
+                const int j = lc[e0 + u];
+                l[u] = lv[e0 + u];
+#pragma unroll
+                for (int c = 0; c < NR; ++c) g[u][c] = w[(size_t)c * n + j];
+            }
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (e0 + u < end)
+#pragma unroll
+                for (int c = 0; c < NR; ++c) acc[c] -= (T)l[u] * g[u][c];
     }
     if (last) {
         const T d = (T)dinv[t];
@@ -95,11 +111,23 @@ __global__ void k_ilu_upper(int m, int n, const int* __restrict__ rows, const in
     T acc[NR];
 #pragma unroll
     for (int c = 0; c < NR; ++c) acc[c] = w[(size_t)c * n + i];
-    for (int e = up[t]; e < up[t + 1]; ++e) {
-        const T u = (T)uv[e];
-        const int j = uc[e];
+    const int end = up[t + 1];
+    for (int e0 = up[t]; e0 < end; e0 += kIluBatch) {
+        V uu[kIluBatch];
+        T g[kIluBatch][NR];
 #pragma unroll
-        for (int c = 0; c < NR; ++c) acc[c] -= u * w[(size_t)c * n + j];
+        for (int u = 0; u < kIluBatch; ++u)
+            if (e0 + u < end) {
+                const int j = uc[e0 + u];
+                uu[u] = uv[e0 + u];
+#pragma unroll
+                for (int c = 0; c < NR; ++c) g[u][c] = w[(size_t)c * n + j];
+            }
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (e0 + u < end)
+#pragma unroll
+                for (int c = 0; c < NR; ++c) acc[c] -= (T)uu[u] * g[u][c];
     }
     const T d = (T)dinv[t];
 #pragma unroll

@@ -198,14 +198,31 @@ k_opt_b(TileView tv, const double* __restrict__ inv_m, const double* __restrict_
                 if (fuse) pi = p[row];
             }
             double sx = 0.0, sy = 0.0;
-            if (valid)
-#pragma unroll 4
-                for (int e = rr[lr] + lane; e < rr[lr + 1]; e += TPR) {
-                    const int j = cs[e];
-                    const double pj = fuse ? z[j] + beta * p[j] : z[j];
-                    sx += bx[e] * pj;
-                    sy += by[e] * pj;
+            if (valid) {
+                constexpr int U = kGatherBatch / 2;
+                const int end = rr[lr + 1];
+                for (int e0 = rr[lr] + lane; e0 < end; e0 += U * TPR) {
+                    double ax[U], ay[U], gz[U], gp[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int e = e0 + u * TPR;
+                        if (e < end) {
+                            const int j = cs[e];
+                            ax[u] = bx[e];
+                            ay[u] = by[e];
+                            gz[u] = z[j];
+                            if (fuse) gp[u] = p[j];
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+                        if (e0 + u * TPR < end) {
+                            const double pj = fuse ? gz[u] + beta * gp[u] : gz[u];
+                            sx += ax[u] * pj;
+                            sy += ay[u] * pj;
+                        }
                 }
+            }
             sx = group_reduce<TPR>(sx);
             sy = group_reduce<TPR>(sy);
             if (valid && lane == 0) {
@@ -248,14 +265,40 @@ k_opt_k(TileView tv, const int* __restrict__ tag, OutletBc bc, const double* __r
                 pi = FUSEP ? (fuse ? z[row] + beta * p[row] : z[row]) : pn_buf[row];
             }
             double s = 0.0, so = 0.0;
-            if (valid)
-#pragma unroll 4
-                for (int e = rr[lr] + lane; e < rr[lr + 1]; e += TPR) {
-                    const int j = cs[e];
-                    const double pj = FUSEP ? (fuse ? z[j] + beta * p[j] : z[j]) : pn_buf[j];
-                    s += kv[e] * pj;
-                    if (OSS) so += btx[e] * gx[j] + bty[e] * gy[j];
+            if (valid) {
+                constexpr int U = kGatherBatch / 2;
+                const int end = rr[lr + 1];
+                for (int e0 = rr[lr] + lane; e0 < end; e0 += U * TPR) {
+                    double ak[U], g0[U], g1[U], ax[U], ay[U], hx[U], hy[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int e = e0 + u * TPR;
+                        if (e < end) {
+                            const int j = cs[e];
+                            ak[u] = kv[e];
+                            if (FUSEP) {
+                                g0[u] = z[j];
+                                if (fuse) g1[u] = p[j];
+                            } else {
+                                g0[u] = pn_buf[j];
+                            }
+                            if (OSS) {
+                                ax[u] = btx[e];
+                                ay[u] = bty[e];
+                                hx[u] = gx[j];
+                                hy[u] = gy[j];
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+                        if (e0 + u * TPR < end) {
+                            const double pj = (FUSEP && fuse) ? g0[u] + beta * g1[u] : g0[u];
+                            s += ak[u] * pj;
+                            if (OSS) so += ax[u] * hx[u] + ay[u] * hy[u];
+                        }
                 }
+            }
             s = group_reduce<TPR>(s);
             if (OSS) so = group_reduce<TPR>(so);
             if (valid && lane == 0) {
@@ -708,14 +751,28 @@ k_b2t(TileView tv, int n, const double* __restrict__ xu, const double* __restric
             const int lr = base + (int)threadIdx.x / TPR, lane = threadIdx.x % TPR;
             const bool valid = lr < nr;
             double su = 0.0, sv = 0.0;
-            if (valid)
-#pragma unroll 4
-                for (int e = rr[lr] + lane; e < rr[lr + 1]; e += TPR) {
-                    const double a = av[e];
-                    const int j = cs[e];
-                    su += a * x0[j];
-                    sv += a * x1[j];
+            if (valid) {
+                const int end = rr[lr + 1];
+                for (int e0 = rr[lr] + lane; e0 < end; e0 += kGatherBatch * TPR) {
+                    double a[kGatherBatch], g0[kGatherBatch], g1[kGatherBatch];
+#pragma unroll
+                    for (int u = 0; u < kGatherBatch; ++u) {
+                        const int e = e0 + u * TPR;
+                        if (e < end) {
+                            const int j = cs[e];
+                            a[u] = av[e];
+                            g0[u] = x0[j];
+                            g1[u] = x1[j];
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kGatherBatch; ++u)
+                        if (e0 + u * TPR < end) {
+                            su += a[u] * g0[u];
+                            sv += a[u] * g1[u];
+                        }
                 }
+            }
             su = group_reduce<TPR>(su);
             sv = group_reduce<TPR>(sv);
             if (valid && lane == 0) {
@@ -988,7 +1045,7 @@ static void launch_opt_k(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, const doubl
     OutletBc bc = m ? m->bc : OutletBc{};
     const TileView tv = W.tk.view(W.err.p);
     TileLaunch L;
-    TILE_TPR_SWITCH(W.tk.tile_rows >= 256 ? 1 : std::min(32, kTileThreads / W.tk.tile_rows),
+    TILE_TPR_SWITCH(W.tk.tpr,
         L = tile_launch(ctx, W.tk, (const void*)k_opt_k<TPR, OSS, FUSEP, DOT>);
         CFA_LAUNCH(ctx, (k_opt_k<TPR, OSS, FUSEP, DOT>), L.grid, kTileThreads, L.smem, tv,
                    m ? m->tag : (const int*)nullptr, bc, z, p, beta_ptr, pn, (const double*)W.gx.p,
@@ -1002,7 +1059,7 @@ static cfa_status pcg_operator(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, const
         if (a.oss) {
             const TileView tv = W.tb.view(W.err.p);
             TileLaunch L;
-            TILE_TPR_SWITCH(W.tb.tile_rows >= 256 ? 1 : std::min(32, kTileThreads / W.tb.tile_rows),
+            TILE_TPR_SWITCH(W.tb.tpr,
                 L = tile_launch(ctx, W.tb, (const void*)k_opt_b<TPR>);
                 CFA_LAUNCH(ctx, (k_opt_b<TPR>), L.grid, kTileThreads, L.smem, tv, a.oss->d_inv_m, z, p, beta_ptr, pn,
                            W.gx.p, W.gy.p, done));
@@ -1259,7 +1316,7 @@ static void launch_b2t(cfa_ctx* ctx, B2Work& W, const B2Args& a, const double* i
                        CondArg cond) {
     const TileView tv = W.tA.view(W.err.p);
     const TileLaunch L = tile_launch(ctx, W.tA, nullptr);
-    TILE_TPR_SWITCH(W.tA.tile_rows >= 256 ? 1 : std::min(32, kTileThreads / W.tA.tile_rows),
+    TILE_TPR_SWITCH(W.tA.tpr,
         CFA_LAUNCH(ctx, (k_b2t<TPR, MODE>), L.grid, kTileThreads, L.smem, tv, a.n, (const double*)a.xu,
                    (const double*)a.xv, a.bu, a.bv, in, aux, out, W.r.p, W.r0.p, W.p.p, W.st.p, W.part.p, W.counter.p,
                    cond));

@@ -33,9 +33,11 @@ __global__ void k_pack_tiles(int ntiles, const long long* __restrict__ off, cons
     }
 }
 
-cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T,
-                      int max_tile_rows) {
-    int tr = std::max(1, std::min(kTileThreads, max_tile_rows));
+cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T) {
+    const double per_row = rows > 0 ? (double)h_rp[rows] / rows : 1.0;
+    int tpr = 1;
+    while (tpr < 32 && per_row > (double)kGatherBatch * tpr) tpr *= 2;
+    int tr = kTileThreads / tpr;
     for (;;) {
         long long mx = 0;
         for (int r0 = 0; r0 < rows; r0 += tr) {
@@ -46,8 +48,14 @@ cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vb
             T.max_chunk = (int)mx;
             break;
         }
-        tr /= 2;
+        if (tpr < 32) {
+            tpr *= 2;
+            tr = kTileThreads / tpr;
+        } else {
+            tr /= 2;
+        }
     }
+    T.tpr = tpr;
     if (T.max_chunk > kTileBudget) return set_error(ctx, CFA_BAD_ARG, "matrix row too long for the tile budget", __FILE__, __LINE__);
     T.rows = rows;
     T.nnz = h_rp[rows];
@@ -90,17 +98,16 @@ cfa_status pack_tiled(cfa_ctx* ctx, const int* d_rp, const int* d_ci, const doub
 void allow_tile_kernel(const void* kernel) {
     static std::unordered_map<const void*, bool> done;
     if (done[kernel]) return;
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kTileBudget + 64);
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileStages * kTileBudget + 64);
     done[kernel] = true;
 }
 
 TileLaunch tile_launch(const cfa_ctx* ctx, const TiledCsr& T, const void*) {
     TileLaunch L;
-    L.smem = (int)(2 * align16(T.max_chunk) + 16);
+    L.smem = (int)(kTileStages * align16(T.max_chunk) + 16);
     const int per_sm = std::max(1, std::min(2048 / kTileThreads, (227 * 1024 - 1024) / std::max(L.smem + 64, 1)));
     L.grid = std::max(1, std::min(T.ntiles, per_sm * ctx->num_sms));
-    L.tpr = std::max(1, kTileThreads / std::max(T.tile_rows, 1));
-    if (L.tpr > 32) L.tpr = 32;
+    L.tpr = T.tpr;
     return L;
 }
 

@@ -6,11 +6,13 @@
 //       value array 0 | value array 1 | ... ]                    (every section 16-byte padded)
 // so a whole tile moves with ONE bulk asynchronous copy (cp.async.bulk, the TMA's 1-D mode)
 // into shared memory. Persistent CTAs walk the tiles (tile = blockIdx.x + k gridDim.x) through a
-// two-stage pipeline: the copy of tile k+1 is in flight while tile k is computed from shared
-// memory; an mbarrier with transaction counting signals arrival. Every wait is bounded: on
-// timeout the kernel records an error code, waits (bounded) for its other copy, and returns.
-// Matrix bytes are read once, fully coalesced, at exactly the algorithmic volume (plus 16-byte
-// padding per section); only the vector gathers x[col] go through L1/L2.
+// kTileStages-deep pipeline: the copies of the next kTileStages - 1 tiles are in flight while
+// tile k is computed from shared memory; an mbarrier with transaction counting signals arrival.
+// Every wait is bounded: on timeout the kernel records an error code, waits (bounded) for its
+// other copies, and returns. Matrix bytes are read once, fully coalesced, at exactly the
+// algorithmic volume (plus 16-byte padding per section); only the vector gathers x[col] go
+// through L1/L2. The row kernels issue the gathers of up to kGatherBatch entries of a lane before
+// they use any of them, so a row costs one L2 round trip instead of one per entry.
 #pragma once
 
 #include <cstdint>
@@ -21,7 +23,9 @@
 namespace cfa {
 
 constexpr int kTileThreads = 256;
-constexpr int kTileBudget = 48 * 1024;     // max bytes of one tile (two stages per CTA)
+constexpr int kTileStages = 3;             // tiles in flight per CTA
+constexpr int kTileBudget = 36 * 1024;     // max bytes of one tile (kTileStages per CTA: two CTAs per SM at most)
+constexpr int kGatherBatch = 8;            // entries per lane whose gathers are issued together
 constexpr unsigned kWaitLimit = 1u << 22;  // bounded mbarrier waits (each try_wait itself blocks a while)
 
 __host__ __device__ inline long long align16(long long b) { return (b + 15) & ~15LL; }
@@ -39,6 +43,7 @@ struct TileView {
 // Host-side description + device buffers of a tiled matrix.
 struct TiledCsr {
     int rows = 0, nnz = 0, ntiles = 0, nvals = 0, vbytes = 8, tile_rows = 0, max_chunk = 0;
+    int tpr = 1;                      // lanes per row of the kernels (tile_rows = kTileThreads / tpr)
     long long bytes = 0;
     DevBuf<unsigned char> data;
     DevBuf<long long> off;
@@ -61,11 +66,11 @@ __host__ __device__ inline long long tile_bytes(int nr, int ne, int nvals, int v
     return tile_val_off(nr, ne, vbytes, nvals);
 }
 
-// Plans the tiles from the host row pointer: tile_rows = max_tile_rows (64: four lanes per row
-// with 256 threads, which keeps several gathers per thread in flight), halved until every tile
-// fits the budget. Allocates the device buffers (the pattern and values are packed by pack_tiled).
-cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T,
-                      int max_tile_rows = 64);
+// Plans the tiles from the host row pointer: tpr (lanes per row) is the smallest power of two
+// with at most about kGatherBatch entries per lane on average, raised until a tile of
+// kTileThreads / tpr rows fits kTileBudget (at tpr = 32 the tile rows are halved instead).
+// Allocates the device buffers (the pattern and values are packed by pack_tiled).
+cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T);
 
 // Packs pattern + values (FP64 sources; converted to float when vbytes == 4) into T.
 // vals[k] may be NULL for k >= nvals. Asynchronous.
@@ -123,55 +128,66 @@ __device__ __forceinline__ void tile_issue(const TileView& tv, int t, unsigned c
 
 // Runs body(tile, row0, nrows, chunk) for every tile of this CTA (all threads call it; the
 // body must not return early for some threads and must synchronise nothing itself).
-// Dynamic shared memory: 2 * max_chunk bytes, 16-aligned. Returns false on a timeout.
+// Dynamic shared memory: kTileStages * align16(max_chunk) bytes. Returns false on a timeout.
 template <class Body>
 __device__ __forceinline__ bool tile_loop(const TileView& tv, unsigned char* smem, Body&& body) {
-    __shared__ uint64_t bar[2];
+    constexpr int S = kTileStages;
+    __shared__ uint64_t bar[S];
     __shared__ int abort_flag;
-    unsigned char* buf0 = smem;
-    unsigned char* buf1 = smem + align16(tv.max_chunk);
+    const long long stride = align16(tv.max_chunk);
     if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+#pragma unroll
+        for (int k = 0; k < S; ++k) mbar_init(&bar[k], 1);
         mbar_fence_init();
         abort_flag = 0;
     }
     __syncthreads();
-    int t = blockIdx.x;
-    if (t >= tv.ntiles) return true;
-    if (threadIdx.x == 0) tile_issue(tv, t, buf0, &bar[0]);
-    unsigned phase[2] = {0u, 0u};
-    for (int k = 0; t < tv.ntiles; ++k, t += gridDim.x) {
-        const int s = k & 1;
-        const int next = t + gridDim.x;
-        if (threadIdx.x == 0 && next < tv.ntiles) {
-            fence_proxy_async();
-            tile_issue(tv, next, s ? buf0 : buf1, &bar[s ^ 1]);
+    const int t0 = blockIdx.x;
+    if (t0 >= tv.ntiles) return true;
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < S - 1; ++k) {
+            const int t = t0 + k * (int)gridDim.x;
+            if (t < tv.ntiles) tile_issue(tv, t, smem + k * stride, &bar[k]);
         }
-        if (!mbar_wait(&bar[s], phase[s])) {
+    unsigned phase = 0u;   // bit k: parity of the next completion of stage k
+    int s = 0;             // stage of tile t
+    for (int t = t0; t < tv.ntiles; t += gridDim.x) {
+        // refill the stage consumed in the previous iteration with the tile S - 1 ahead
+        const int sn = s == 0 ? S - 1 : s - 1;
+        const int tn = t + (S - 1) * (int)gridDim.x;
+        if (threadIdx.x == 0 && tn < tv.ntiles) {
+            fence_proxy_async();
+            tile_issue(tv, tn, smem + sn * stride, &bar[sn]);
+        }
+        if (!mbar_wait(&bar[s], (phase >> s) & 1u)) {
             atomicExch(tv.err, (int)CFA_TIMEOUT);
             abort_flag = 1;
         }
         __syncthreads();
         if (abort_flag) {
-            // let the other stage's copy (if any) land before the CTA exits, bounded
-            if (next < tv.ntiles) mbar_wait(&bar[s ^ 1], phase[s ^ 1]);
+            // let the copies still in flight land before the CTA exits, bounded
+            for (int k = 0; k < S; ++k) {
+                const int sk = (s + k) % S;
+                if (t + k * (int)gridDim.x < tv.ntiles) mbar_wait(&bar[sk], (phase >> sk) & 1u);
+            }
             return false;
         }
-        phase[s] ^= 1u;
+        phase ^= 1u << s;
         const int r0 = t * tv.tile_rows;
-        body(t, r0, min(tv.tile_rows, tv.rows - r0), s ? buf1 : buf0);
+        body(t, r0, min(tv.tile_rows, tv.rows - r0), smem + s * stride);
         __syncthreads();
+        s = s + 1 == S ? 0 : s + 1;
     }
     return true;
 }
 
-// Launch shape of a tile kernel: persistent grid limited by shared memory (two stages).
+// Launch shape of a tile kernel: persistent grid limited by shared memory (kTileStages tiles).
 struct TileLaunch {
     int grid = 1, smem = 0, tpr = 1;
 };
 TileLaunch tile_launch(const cfa_ctx* ctx, const TiledCsr& T, const void* kernel);
-// Raises the kernel's dynamic shared memory limit to two tiles of the budget (once per kernel;
+// Raises the kernel's dynamic shared memory limit to kTileStages tiles of the budget (once per kernel;
 // call outside stream capture).
 void allow_tile_kernel(const void* kernel);
 

@@ -366,6 +366,29 @@ def test_amg_vcycle_matches_reference_gpu_golden(ctx):
     assert np.abs(host(z) - g["lap_vcycle_z"]).max() <= 1e-12 * np.abs(g["lap_vcycle_z"]).max()
 
 
+@pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
+def test_amg_cluster_tail_matches_level_kernels(ctx, precision, monkeypatch):
+    """The opt-in coarse tail (one thread-block cluster for the levels below CFA_TAIL_ROWS rows)
+    gives the V-cycle of the per-level kernels."""
+    m = mesh("medium")
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    val = laplacian(rp, ci)
+    r = dev(np.cos(0.11 * np.arange(m.n)))
+    out = []
+    for tail in (None, "7000"):   # tail from level 1 (6.4k rows) down
+        if tail is None:
+            monkeypatch.delenv("CFA_TAIL_ROWS", raising=False)
+        else:
+            monkeypatch.setenv("CFA_TAIL_ROWS", tail)
+        amg = cfa.AmgPreconditioner(ctx, precision=precision)
+        amg.setup(m.n, ci.size, dev(rp, torch.int32), dev(ci, torch.int32), dev(val))
+        assert amg.num_levels() >= 3
+        z = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+        amg.apply(r, z)
+        out.append(host(z))
+    assert np.abs(out[1] - out[0]).max() <= 1e-12 * np.abs(out[0]).max()
+
+
 def test_amg_coarse_not_spd_is_an_error(ctx):
     m = mesh("tiny")
     rp, ci = O.csr_build(m.n, m.elem_v)
