@@ -263,6 +263,13 @@ def pressure_operator(ctx, rp, ci, val, x, y, oss=None):
                                           C.byref(oss) if oss is not None else None, ptr(x), ptr(y)))
 
 
+def pressure_operator_layout(ctx):
+    """(passes, stored_nnz) of the prepared pressure operator."""
+    passes, nz = C.c_int(), C.c_longlong()
+    ctx.check(lib().cfa_pressure_operator_layout(ctx.h, C.byref(passes), C.byref(nz)))
+    return passes.value, nz.value
+
+
 def oss_operator(mesh: DeviceMesh, oss_val, inv_m) -> OssOperator:
     return OssOperator(mesh.h.value, oss_val.data_ptr(), inv_m.data_ptr())
 
@@ -366,6 +373,18 @@ class AmgPreconditioner:
 
     def apply(self, r, z):
         self.ctx.check(lib().cfa_amg_apply(self.ctx.h, self.h, ptr(r), ptr(z)))
+
+    def remap(self, n, nnz, d_rp, d_ci, d_val, h_rp, h_ci, new_to_old):
+        """remap (src/cfa/linalg.cuh:1074-1157): host pattern and new_to_old as numpy int32."""
+        h_rp = np.ascontiguousarray(h_rp, np.int32)
+        h_ci = np.ascontiguousarray(h_ci, np.int32)
+        n2o = np.ascontiguousarray(new_to_old, np.int32)
+        self.ctx.check(lib().cfa_amg_remap(self.ctx.h, self._handle(), n, nnz, ptr(d_rp), ptr(d_ci), ptr(d_val),
+                                           ptr(h_rp), ptr(h_ci), ptr(n2o)))
+
+    @property
+    def remaps(self) -> int:
+        return int(lib().cfa_amg_remaps(self.h)) if self.h else 0
 
     def _info(self):
         nl, cn, ms = C.c_int(), C.c_int(), C.c_double()

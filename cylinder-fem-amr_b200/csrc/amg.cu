@@ -20,6 +20,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
+#include <mutex>
 #include <type_traits>
 
 #include "amg.cuh"
@@ -958,15 +959,17 @@ static cfa_status to_float(cfa_ctx* ctx, DCsr& M) {
 }
 
 // 1 + 0.1 sin(1 + i) for i < n: the power-iteration start vector (host libm, as the reference),
-// computed once per process.
-static const std::vector<double>& start_vector(int n) {
+// computed once per process (shared by the threads of all contexts).
+static std::vector<double> start_vector(int n) {
+    static std::mutex mu;
     static std::vector<double> x0;
+    std::lock_guard<std::mutex> lock(mu);
     if ((int)x0.size() < n) {
         const size_t old = x0.size();
         x0.resize(n);
         for (size_t i = old; i < (size_t)n; ++i) x0[i] = 1.0 + 0.1 * std::sin(1.0 + (double)i);
     }
-    return x0;
+    return std::vector<double>(x0.begin(), x0.begin() + n);
 }
 
 // rho(D^-1 A) by 20 power iterations (spectral_radius_DinvA, :1276-1304), on the device.
@@ -974,7 +977,7 @@ static cfa_status spectral_radius(cfa_ctx* ctx, cfa_amg* amg, const DCsr& A, con
     SetupScratch& S = amg->scratch;
     const int n = A.rows, nch = (n + 4095) / 4096;
     if (!amg->x0.p || amg->x0.cap < (size_t)n) {
-        const std::vector<double>& h = start_vector(n);
+        const std::vector<double> h = start_vector(n);
         CFA_CUDA(amg->x0.ensure(n));
         CFA_CUDA(cudaMemcpy(amg->x0.p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice));
     }
@@ -1011,6 +1014,47 @@ static cfa_status level_vectors(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int n) 
 
 static cfa_status level_vectors64(cfa_ctx* ctx, AmgLevel& L, int n) {
     CFA_CUDA(L.x64.ensure(n)); CFA_CUDA(L.t64.ensure(n)); CFA_CUDA(L.b64.ensure(n)); CFA_CUDA(L.r64.ensure(n));
+    return CFA_OK;
+}
+
+// Kernel shapes of one level, its FP32 copies (mixed precision) and its tile-streamed A, P, R in
+// the hierarchy precision.
+static cfa_status prepare_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L) {
+    const cfa_amg_opts& o = amg->opts;
+    L.A.tpr = threads_per_row(L.A.rows, L.A.nnz);
+    L.P.tpr = threads_per_row(L.P.rows, L.P.nnz);
+    L.R.tpr = threads_per_row(L.R.rows, L.R.nnz);
+    if (o.precision == CFA_MIXED) {
+        CFA_PROPAGATE(to_float(ctx, L.A));
+        CFA_PROPAGATE(to_float(ctx, L.P));
+        CFA_PROPAGATE(to_float(ctx, L.R));
+        CFA_CUDA(L.dinv32.ensure(L.A.rows));
+        CFA_LAUNCH(ctx, k_to_float, std::min(ceil_div(L.A.rows, kThreads), 8 * ctx->num_sms), kThreads, 0,
+                   (long long)L.A.rows, L.dinv.p, L.dinv32.p);
+    }
+    CFA_CHECK_LAUNCH();
+    if (!amg->tiled) return CFA_OK;
+    const int vb = o.precision == CFA_MIXED ? 4 : 8;
+    for (DCsr* M : {&L.A, &L.P, &L.R}) {
+        TiledCsr& T = M == &L.A ? L.tA : M == &L.P ? L.tP : L.tR;
+        HostBuf<int>& hr = amg->scratch.h_rp;
+        CFA_CUDA(hr.ensure(M->rows + 1));
+        CFA_CUDA(cudaMemcpyAsync(hr.p, M->rp.p, (M->rows + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+        CFA_PROPAGATE(plan_tiled(ctx, hr.p, M->rows, 1, vb, T));
+        CFA_PROPAGATE(pack_tiled(ctx, M->rp.p, M->ci.p, M->v.p, nullptr, nullptr, T));
+    }
+    return level_vectors64(ctx, L, L.A.rows);
+}
+
+// The V-cycle's coarse tail plan, and the kernels' shared-memory limits raised now, outside any
+// stream capture (a dry V-cycle).
+static cfa_status prepare_vcycle(cfa_ctx* ctx, cfa_amg* amg) {
+    if (!amg->tiled) return CFA_OK;
+    CFA_PROPAGATE(plan_tail(ctx, amg));
+    if (amg->opts.precision == CFA_MIXED) vcycle_tiled<float>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
+    else vcycle_tiled<double>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
+    CFA_CHECK_LAUNCH();
     return CFA_OK;
 }
 
@@ -1144,46 +1188,15 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
         CFA_CUDA(amg->cb32.ensure(cn + 1));
         CFA_CUDA(amg->cx32.ensure(cn + 1));
     }
-    // precision and kernel shapes of the V-cycle
-    for (AmgLevel& L : amg->levels) {
-        L.A.tpr = threads_per_row(L.A.rows, L.A.nnz);
-        L.P.tpr = threads_per_row(L.P.rows, L.P.nnz);
-        L.R.tpr = threads_per_row(L.R.rows, L.R.nnz);
-        if (o.precision == CFA_MIXED) {
-            CFA_PROPAGATE(to_float(ctx, L.A));
-            CFA_PROPAGATE(to_float(ctx, L.P));
-            CFA_PROPAGATE(to_float(ctx, L.R));
-            CFA_CUDA(L.dinv32.ensure(L.A.rows));
-            CFA_LAUNCH(ctx, k_to_float, std::min(ceil_div(L.A.rows, kThreads), 8 * ctx->num_sms), kThreads, 0,
-                       (long long)L.A.rows, L.dinv.p, L.dinv32.p);
-        }
-    }
-    CFA_CHECK_LAUNCH();
-    // tile-streamed copies of every level's A, P, R in the hierarchy precision
+    // precision, kernel shapes and tile-streamed copies of the V-cycle
     const char* te = std::getenv("CFA_TILES");
     amg->tiled = !(te && te[0] == '0') && !amg->levels.empty();
     if (amg->tiled) {
         CFA_CUDA(amg->err.ensure(1));
         CFA_CUDA(cudaMemsetAsync(amg->err.p, 0, sizeof(int), ctx->stream));
-        const int vb = o.precision == CFA_MIXED ? 4 : 8;
-        for (AmgLevel& L : amg->levels) {
-            for (DCsr* M : {&L.A, &L.P, &L.R}) {
-                TiledCsr& T = M == &L.A ? L.tA : M == &L.P ? L.tP : L.tR;
-                HostBuf<int>& hr = amg->scratch.h_rp;
-                CFA_CUDA(hr.ensure(M->rows + 1));
-                CFA_CUDA(cudaMemcpyAsync(hr.p, M->rp.p, (M->rows + 1) * sizeof(int), cudaMemcpyDeviceToHost,
-                                         ctx->stream));
-                CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-                CFA_PROPAGATE(plan_tiled(ctx, hr.p, M->rows, 1, vb, T));
-                CFA_PROPAGATE(pack_tiled(ctx, M->rp.p, M->ci.p, M->v.p, nullptr, nullptr, T));
-            }
-        }
-        // raise the kernels' shared-memory limits now, outside any stream capture
-        for (AmgLevel& L : amg->levels) CFA_PROPAGATE(level_vectors64(ctx, L, L.A.rows));
-        CFA_PROPAGATE(plan_tail(ctx, amg));
-        if (o.precision == CFA_MIXED) vcycle_tiled<float>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
-        else vcycle_tiled<double>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
     }
+    for (AmgLevel& L : amg->levels) CFA_PROPAGATE(prepare_level(ctx, amg, L));
+    CFA_PROPAGATE(prepare_vcycle(ctx, amg));
     phase(6);
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     amg->setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -1194,6 +1207,112 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
 }  // namespace cfa
 
 using namespace cfa;
+
+// AmgPreconditioner::remap (src/cfa/linalg.cuh:1074-1157). The prolongator of a new node is the
+// mean of the rows of its graph neighbours that already have one, built pass by pass outwards on
+// the host in node order (the reference's host algorithm; equal columns are summed in the order
+// they were gathered, a stable sort), uploaded, transposed on the device in the setup's exact
+// order; level 0 takes the new operator and its inverse diagonal. remapped = false when it set
+// the hierarchy up anew instead (no levels, or new nodes none of whose neighbours has a row).
+static cfa_status amg_remap(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* d_rp, const int* d_ci,
+                            const double* d_v, const int* h_rp, const int* h_ci, const int* n2o, bool& remapped) {
+    remapped = false;
+    if (amg->levels.empty()) return amg_setup(ctx, amg, n, nnz, d_rp, d_ci, d_v);
+    const auto t0 = std::chrono::steady_clock::now();
+    AmgLevel& L = amg->levels[0];
+    const int old_rows = L.P.rows;
+    for (int i = 0; i < n; ++i)
+        if (n2o[i] < -1 || n2o[i] >= old_rows)
+            return set_error(ctx, CFA_BAD_ARG, "new_to_old entry outside the old level-0 rows", __FILE__, __LINE__);
+    // the current level-0 prolongator on the host
+    std::vector<int> prp(old_rows + 1), pci(std::max(L.P.nnz, 1));
+    std::vector<double> pv(std::max(L.P.nnz, 1));
+    CFA_CUDA(cudaMemcpyAsync(prp.data(), L.P.rp.p, (old_rows + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(pci.data(), L.P.ci.p, (size_t)L.P.nnz * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(pv.data(), L.P.v.p, (size_t)L.P.nnz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    // rows of new nodes, pass by pass from neighbours set in earlier passes
+    std::vector<int> extra_of(n, -1), ex_rp(1, 0), pending, still, set_now;
+    std::vector<std::pair<int, double>> ex, acc;
+    std::vector<char> has_row(n);
+    for (int i = 0; i < n; ++i) {
+        has_row[i] = n2o[i] >= 0;
+        if (n2o[i] < 0) pending.push_back(i);
+    }
+    while (!pending.empty()) {
+        still.clear();
+        set_now.clear();
+        for (int i : pending) {
+            acc.clear();
+            int cnt = 0;
+            for (int a = h_rp[i]; a < h_rp[i + 1]; ++a) {
+                const int k = h_ci[a];
+                if (k == i || !has_row[k]) continue;
+                ++cnt;
+                if (n2o[k] >= 0) {
+                    const int j = n2o[k];
+                    for (int b = prp[j]; b < prp[j + 1]; ++b) acc.push_back({pci[b], pv[b]});
+                } else {
+                    for (int b = ex_rp[extra_of[k]]; b < ex_rp[extra_of[k] + 1]; ++b) acc.push_back(ex[b]);
+                }
+            }
+            if (cnt == 0) { still.push_back(i); continue; }
+            std::stable_sort(acc.begin(), acc.end(),
+                             [](const std::pair<int, double>& x, const std::pair<int, double>& y) { return x.first < y.first; });
+            const size_t row0 = ex.size();
+            for (const auto& e : acc) {
+                if (ex.size() > row0 && ex.back().first == e.first) ex.back().second += e.second;
+                else ex.push_back(e);
+            }
+            for (size_t q = row0; q < ex.size(); ++q) ex[q].second /= cnt;
+            extra_of[i] = (int)ex_rp.size() - 1;
+            ex_rp.push_back((int)ex.size());
+            set_now.push_back(i);
+        }
+        if (set_now.empty()) return amg_setup(ctx, amg, n, nnz, d_rp, d_ci, d_v);   // isolated new nodes
+        for (int i : set_now) has_row[i] = 1;
+        pending.swap(still);
+    }
+    std::vector<int> nrp(n + 1, 0);
+    for (int i = 0; i < n; ++i)
+        nrp[i + 1] = nrp[i] + (n2o[i] >= 0 ? prp[n2o[i] + 1] - prp[n2o[i]] : ex_rp[extra_of[i] + 1] - ex_rp[extra_of[i]]);
+    const int pnnz = nrp[n];
+    std::vector<int> nci(std::max(pnnz, 1));
+    std::vector<double> nv(std::max(pnnz, 1));
+    for (int i = 0; i < n; ++i) {
+        int o = nrp[i];
+        if (n2o[i] >= 0) {
+            for (int b = prp[n2o[i]]; b < prp[n2o[i] + 1]; ++b, ++o) { nci[o] = pci[b]; nv[o] = pv[b]; }
+        } else {
+            for (int b = ex_rp[extra_of[i]]; b < ex_rp[extra_of[i] + 1]; ++b, ++o) { nci[o] = ex[b].first; nv[o] = ex[b].second; }
+        }
+    }
+    // level 0: new operator, inverse diagonal, P (uploaded), R = P^T
+    amg->version = next_uid();
+    L.P.rows = n;
+    L.P.nnz = pnnz;
+    CFA_CUDA(L.P.rp.ensure(n + 1));
+    CFA_CUDA(L.P.ci.ensure(std::max(pnnz, 1)));
+    CFA_CUDA(L.P.v.ensure(std::max(pnnz, 1)));
+    CFA_CUDA(cudaMemcpyAsync(L.P.rp.p, nrp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(L.P.ci.p, nci.data(), (size_t)pnnz * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(L.P.v.p, nv.data(), (size_t)pnnz * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CFA_PROPAGATE(transpose(ctx, amg->scratch, L.P, L.R));
+    CFA_PROPAGATE(copy_csr(ctx, n, nnz, d_rp, d_ci, d_v, L.A));
+    CFA_CUDA(L.dinv.ensure(n));
+    CFA_LAUNCH(ctx, k_amg_dinv, ceil_div(n, kThreads), kThreads, 0, n, L.A.rp.p, L.A.ci.p, L.A.v.p, L.dinv.p);
+    CFA_CUDA(L.agg.ensure(n));
+    CFA_CUDA(cudaMemsetAsync(L.agg.p, 0xff, (size_t)n * sizeof(int), ctx->stream));   // no aggregates after a remap
+    CFA_PROPAGATE(level_vectors(ctx, amg, L, n));
+    if (amg->tiled) CFA_CUDA(cudaMemsetAsync(amg->err.p, 0, sizeof(int), ctx->stream));
+    CFA_PROPAGATE(prepare_level(ctx, amg, L));
+    CFA_PROPAGATE(prepare_vcycle(ctx, amg));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    amg->remaps++;
+    amg->setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    remapped = true;
+    return CFA_OK;
+}
 
 extern "C" {
 
@@ -1229,6 +1348,16 @@ cfa_status cfa_amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* 
     CFA_ARG(amg && n > 0 && nnz > 0 && rp && ci && v);
     return amg_setup(ctx, amg, n, nnz, rp, ci, v);
 }
+
+cfa_status cfa_amg_remap(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* rp, const int* ci, const double* v,
+                         const int* h_rp, const int* h_ci, const int* h_new_to_old) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(amg && n > 0 && nnz > 0 && rp && ci && v && h_rp && h_ci && h_new_to_old);
+    bool remapped = false;
+    return amg_remap(ctx, amg, n, nnz, rp, ci, v, h_rp, h_ci, h_new_to_old, remapped);
+}
+
+int cfa_amg_remaps(const cfa_amg* amg) { return amg ? amg->remaps : 0; }
 
 cfa_status cfa_amg_apply(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z) {
     if (!ctx) return CFA_BAD_ARG;

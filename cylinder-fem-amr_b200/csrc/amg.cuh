@@ -73,6 +73,7 @@ struct cfa_amg {
     cfa::DevBuf<double> cb64, cx64;      // coarsest right-hand side / solution (FP64)
     cfa::DevBuf<float> cb32, cx32;
     double setup_ms = 0.0;
+    int remaps = 0;                      // remap() calls that reused the hierarchy
     long long version = 0;               // process-unique, renewed by every setup (graph caches key on it)
     std::vector<double> host_x0;         // 1 + 0.1 sin(1 + i), the power-iteration start vector
     cfa::DevBuf<double> x0;

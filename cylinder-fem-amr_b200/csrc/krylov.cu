@@ -9,6 +9,8 @@
 // initialisation kernels followed by a conditional WHILE node whose body is one iteration; the
 // body's kernels clear the condition when the solve stops, so the loop runs on the device with
 // no host round trip. Results are deterministic run to run.
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <cstring>
 #include <cstdlib>
@@ -166,6 +168,104 @@ k_op_k(int n, int nnz, const int* __restrict__ rp, const int* __restrict__ ci, c
             } else {
                 st->alpha = st->rz / pq;
             }
+        }
+    }
+}
+
+// ---- the OSS operator assembled into one matrix ----
+// A = K - diag(not Dirichlet) B^T M^-1 B (apply_oss_projection, src/cfa/device.cuh:316-323, with
+// k_oss_apply_B / k_oss_apply_BT, src/cfa/fem_kernels.cuh:855-885, applied to the operator
+// instead of a vector): one row pass of about 19 entries per row instead of two passes over
+// K, Bx, By, BTx, BTy (7 entries each). The pattern of row i is the two-ring of node i, the
+// union of the K rows of its neighbours.
+constexpr int kRing2Max = 96;
+
+// Sorted union of the K rows of the neighbours of row i in buf; -1 when longer than kRing2Max.
+__device__ int ring2_row(int i, const int* __restrict__ rp, const int* __restrict__ ci, int* buf) {
+    int len = 0;
+    for (int e = rp[i]; e < rp[i + 1]; ++e) {
+        const int k = ci[e];
+        for (int f = rp[k]; f < rp[k + 1]; ++f) {
+            const int j = ci[f];
+            int q = len;
+            while (q > 0 && buf[q - 1] > j) --q;
+            if (q > 0 && buf[q - 1] == j) continue;
+            if (len == kRing2Max) return -1;
+            for (int r = len; r > q; --r) buf[r] = buf[r - 1];
+            buf[q] = j;
+            ++len;
+        }
+    }
+    return len;
+}
+
+__global__ void k_ring2_count(int n, const int* __restrict__ rp, const int* __restrict__ ci, int* __restrict__ cnt,
+                              int* __restrict__ err) {
+    int buf[kRing2Max];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    if (i == n) { cnt[n] = 0; return; }
+    const int len = ring2_row(i, rp, ci, buf);
+    if (len < 0) { atomicExch(err, 1); cnt[i] = 0; return; }
+    cnt[i] = len;
+}
+
+__global__ void k_ring2_fill(int n, const int* __restrict__ rp, const int* __restrict__ ci, const int* __restrict__ rp2,
+                             int* __restrict__ ci2) {
+    int buf[kRing2Max];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int len = ring2_row(i, rp, ci, buf);
+    for (int q = 0; q < len; ++q) ci2[rp2[i] + q] = buf[q];
+}
+
+// Values of the fused operator, written straight into the value section of its tiles. One warp
+// per row, one lane per entry (i, j) of the two-ring row: the entry is K_ij minus the sum over
+// k in N(i) with j in N(k), k ascending, of BTx_ik m_k^-1 Bx_kj + BTy_ik m_k^-1 By_kj. The rows of
+// the neighbours k are read by every lane at once (broadcast); no atomics, a fixed order.
+__global__ void __launch_bounds__(kThreads)
+k_oss_fuse(int n, int nnz, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ K,
+           const double* __restrict__ oss, const int* __restrict__ tag, OutletBc bc, const double* __restrict__ inv_m,
+           const int* __restrict__ rp2, const int* __restrict__ ci2, TileView tv, unsigned char* __restrict__ data) {
+    const int lane = threadIdx.x & 31;
+    const int nw = gridDim.x * blockDim.x / 32;
+    const double* Bx = oss;
+    const double* By = oss + nnz;
+    const double* BTx = oss + 2 * (size_t)nnz;
+    const double* BTy = oss + 3 * (size_t)nnz;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < n; i += nw) {
+        const int t = i / tv.tile_rows;
+        const int r0 = t * tv.tile_rows;
+        const int nr = min(tv.tile_rows, n - r0);
+        const int e0 = rp2[r0], ne = rp2[r0 + nr] - e0;
+        double* dst = reinterpret_cast<double*>(data + tv.off[t] + tile_val_off(nr, ne, 8, 0)) + (rp2[i] - e0);
+        const int b2 = rp2[i], len = rp2[i + 1] - b2;
+        const bool oss_row = !pressure_dirichlet(i, tag[i], bc);
+        const int a0 = rp[i], a1 = rp[i + 1];
+        for (int q = lane; q - lane < len; q += 32) {
+            const bool on = q < len;
+            const int j = on ? ci2[b2 + q] : -1;
+            double acc = 0.0;
+            // K_ij (j in N(i))
+            for (int a = a0; a < a1; ++a)
+                if (ci[a] == j) acc = K[a];
+            if (oss_row)
+                for (int a = a0; a < a1; ++a) {
+                    const int k = ci[a];
+                    const int f0 = rp[k], f1 = rp[k + 1];
+                    // j in row k (sorted): binary search
+                    int lo = f0, hi = f1 - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (ci[mid] < j) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    if (on && lo < f1 && ci[lo] == j) {
+                        const double im = inv_m[k];
+                        acc -= (BTx[a] * im) * Bx[lo] + (BTy[a] * im) * By[lo];
+                    }
+                }
+            if (on) dst[q] = acc;
         }
     }
 }
@@ -915,8 +1015,12 @@ struct PcgWork {
     int cap = 0;
     DevBuf<double> r, z, p, pn, q, gx, gy, dinv;
     DevBuf<CgState> st;
-    // tile-streamed copy of the operator (pass 1: Bx, By; pass 2: K [, BTx, BTy])
+    // tile-streamed copy of the operator: K - B^T M^-1 B as one matrix on the two-ring pattern
+    // (fused), else pass 1: Bx, By; pass 2: K [, BTx, BTy]
     TiledCsr tb, tk;
+    bool fused = false;
+    DevBuf<int> rp2, ci2, cnt2;       // two-ring pattern of the fused OSS operator
+    DevBuf<unsigned char> scan_tmp;
     std::vector<const void*> tile_key;
     std::vector<const void*> prepared;   // operator whose values the tiles hold (standalone apply)
     bool tiled = false;
@@ -1056,7 +1160,7 @@ static cfa_status pcg_operator(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, const
                                const double* beta_ptr, double* pn, double* q, bool dot, CondArg cond,
                                const int* done) {
     if (W.tiled) {
-        if (a.oss) {
+        if (a.oss && !W.fused) {
             const TileView tv = W.tb.view(W.err.p);
             TileLaunch L;
             TILE_TPR_SWITCH(W.tb.tpr,
@@ -1102,21 +1206,31 @@ static cfa_status pcg_operator(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, const
     return CFA_OK;
 }
 
+// This operator's values into the tile-streamed layout (fused: the K - B^T M^-1 B values).
+static cfa_status pack_operator(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a) {
+    if (a.oss && W.fused) {
+        const cfa_mesh* m = a.oss->mesh;
+        CFA_LAUNCH(ctx, k_oss_fuse, row_grid(ctx, a.n, 32), kThreads, 0, a.n, a.nnz, a.rp, a.ci, a.val,
+                   a.oss->d_oss_val, m->tag, m->bc, a.oss->d_inv_m, (const int*)W.rp2.p, (const int*)W.ci2.p,
+                   W.tk.view(W.err.p), W.tk.data.p);
+    } else if (a.oss) {
+        const double* o = a.oss->d_oss_val;
+        const size_t nz = (size_t)a.nnz;
+        CFA_PROPAGATE(pack_tiled(ctx, a.rp, a.ci, o, o + nz, nullptr, W.tb));
+        CFA_PROPAGATE(pack_tiled(ctx, a.rp, a.ci, a.val, o + 2 * nz, o + 3 * nz, W.tk));
+    } else {
+        CFA_PROPAGATE(pack_tiled(ctx, a.rp, a.ci, a.val, nullptr, nullptr, W.tk));
+    }
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
 static cfa_status pcg_init(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg cond) {
     const int n = a.n;
     const int gv = row_grid(ctx, n, 1);
     CgState* st = W.st.p;
     const int* done = &st->done;
-    if (W.tiled) {   // this solve's operator values into the tile-streamed layout
-        if (a.oss) {
-            const double* o = a.oss->d_oss_val;
-            const size_t nz = (size_t)a.nnz;
-            CFA_PROPAGATE(pack_tiled(ctx, a.rp, a.ci, o, o + nz, nullptr, W.tb));
-            CFA_PROPAGATE(pack_tiled(ctx, a.rp, a.ci, a.val, o + 2 * nz, o + 3 * nz, W.tk));
-        } else {
-            CFA_PROPAGATE(pack_tiled(ctx, a.rp, a.ci, a.val, nullptr, nullptr, W.tk));
-        }
-    }
+    if (W.tiled) CFA_PROPAGATE(pack_operator(ctx, W, a));   // this solve's operator values
     CFA_LAUNCH(ctx, k_cg_bnorm, gv, kThreads, 0, n, a.b, st, W.part.p, W.counter.p, cond);
     if (!a.amg) CFA_LAUNCH(ctx, k_inv_diag, ceil_div(n, kThreads), kThreads, 0, n, a.rp, a.ci, a.val, W.dinv.p);
     // q = A x (pn scratch receives x)
@@ -1191,11 +1305,43 @@ static void allow_operator_tpr() {
 }
 
 static void allow_operator_kernels() {
-    static bool done = false;
-    if (done) return;
-    allow_operator_tpr<1>(); allow_operator_tpr<2>(); allow_operator_tpr<4>();
-    allow_operator_tpr<8>(); allow_operator_tpr<16>(); allow_operator_tpr<32>();
-    done = true;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        allow_operator_tpr<1>(); allow_operator_tpr<2>(); allow_operator_tpr<4>();
+        allow_operator_tpr<8>(); allow_operator_tpr<16>(); allow_operator_tpr<32>();
+    });
+}
+
+static bool oss_fused_enabled() {
+    const char* e = std::getenv("CFA_OSS_FUSED");
+    return !(e && e[0] == '0');
+}
+
+// Two-ring pattern (rp2, ci2) of the fused OSS operator; ok = false when a row is longer than
+// kRing2Max (the operator then stays in two passes).
+static cfa_status plan_ring2(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, bool& ok) {
+    const int n = a.n;
+    ok = false;
+    CFA_CUDA(W.cnt2.ensure(n + 1));
+    CFA_CUDA(W.rp2.ensure(n + 1));
+    CFA_CUDA(W.err.ensure(1));
+    CFA_CUDA(cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream));
+    CFA_LAUNCH(ctx, k_ring2_count, ceil_div(n + 1, kThreads), kThreads, 0, n, a.rp, a.ci, W.cnt2.p, W.err.p);
+    size_t tmp = 0;
+    CFA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, W.cnt2.p, W.rp2.p, n + 1, ctx->stream));
+    CFA_CUDA(W.scan_tmp.ensure(tmp + 16));
+    CFA_CUDA(cub::DeviceScan::ExclusiveSum(W.scan_tmp.p, tmp, W.cnt2.p, W.rp2.p, n + 1, ctx->stream));
+    int h[2] = {0, 0};
+    CFA_CUDA(cudaMemcpyAsync(&h[0], W.err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(&h[1], W.rp2.p + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    CFA_CUDA(cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream));
+    if (h[0]) return CFA_OK;
+    CFA_CUDA(W.ci2.ensure(std::max(h[1], 1)));
+    CFA_LAUNCH(ctx, k_ring2_fill, ceil_div(n, kThreads), kThreads, 0, n, a.rp, a.ci, (const int*)W.rp2.p, W.ci2.p);
+    CFA_CHECK_LAUNCH();
+    ok = true;
+    return CFA_OK;
 }
 
 // Plans the tile-streamed operator for this pattern (host row pointer needed: one sync).
@@ -1209,10 +1355,24 @@ static cfa_status plan_operator_tiles(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a
     std::vector<int> h_rp(a.n + 1);
     CFA_CUDA(cudaMemcpyAsync(h_rp.data(), a.rp, (a.n + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (a.oss) {
+    W.fused = false;
+    if (a.oss && oss_fused_enabled()) {
+        bool ok = false;
+        CFA_PROPAGATE(plan_ring2(ctx, W, a, ok));
+        if (ok) {
+            std::vector<int> h_rp2(a.n + 1);
+            CFA_CUDA(cudaMemcpyAsync(h_rp2.data(), W.rp2.p, (a.n + 1) * sizeof(int), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+            CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+            CFA_PROPAGATE(plan_tiled(ctx, h_rp2.data(), a.n, 1, 8, W.tk));
+            CFA_PROPAGATE(pack_tiled(ctx, W.rp2.p, W.ci2.p, nullptr, nullptr, nullptr, W.tk));   // pattern only
+            W.fused = true;
+        }
+    }
+    if (a.oss && !W.fused) {
         CFA_PROPAGATE(plan_tiled(ctx, h_rp.data(), a.n, 2, 8, W.tb));
         CFA_PROPAGATE(plan_tiled(ctx, h_rp.data(), a.n, 3, 8, W.tk));
-    } else {
+    } else if (!a.oss) {
         CFA_PROPAGATE(plan_tiled(ctx, h_rp.data(), a.n, 1, 8, W.tk));
     }
     W.tile_key = key;
@@ -1333,11 +1493,10 @@ static cfa_status plan_b2_tiles(cfa_ctx* ctx, B2Work& W, const B2Args& a) {
     const char* e = std::getenv("CFA_TILES");
     W.tiled = !(e && e[0] == '0');
     if (!W.tiled) return CFA_OK;
-    static bool allowed = false;
-    if (!allowed) {
+    static std::once_flag once;
+    std::call_once(once, [] {
         allow_b2_tpr<1>(); allow_b2_tpr<2>(); allow_b2_tpr<4>(); allow_b2_tpr<8>(); allow_b2_tpr<16>(); allow_b2_tpr<32>();
-        allowed = true;
-    }
+    });
     if (!W.err.p) {
         CFA_CUDA(W.err.ensure(1));
         CFA_CUDA(cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream));
@@ -1498,14 +1657,18 @@ cfa_status cfa_pressure_operator_prepare(cfa_ctx* ctx, int n, int nnz, const int
     CFA_PROPAGATE(plan_operator_tiles(ctx, W, a));
     W.prepared.clear();
     if (!W.tiled) return CFA_OK;
-    if (oss) {
-        const double* o = oss->d_oss_val;
-        CFA_PROPAGATE(pack_tiled(ctx, rp, ci, o, o + (size_t)nnz, nullptr, W.tb));
-        CFA_PROPAGATE(pack_tiled(ctx, rp, ci, val, o + 2 * (size_t)nnz, o + 3 * (size_t)nnz, W.tk));
-    } else {
-        CFA_PROPAGATE(pack_tiled(ctx, rp, ci, val, nullptr, nullptr, W.tk));
-    }
+    CFA_PROPAGATE(pack_operator(ctx, W, a));
     W.prepared = operator_key(n, nnz, rp, ci, val, oss);
+    return CFA_OK;
+}
+
+cfa_status cfa_pressure_operator_layout(const cfa_ctx* ctx, int* passes, long long* stored_nnz) {
+    if (!ctx || !ctx->work) return CFA_BAD_ARG;
+    const PcgWork& W = ctx->work->pcg;
+    if (W.prepared.empty()) return CFA_BAD_ARG;
+    const bool two = W.tiled && W.tb.nnz > 0 && !W.fused;
+    if (passes) *passes = two ? 2 : 1;
+    if (stored_nnz) *stored_nnz = W.tk.nnz;
     return CFA_OK;
 }
 

@@ -1,5 +1,6 @@
 // Tile planning and packing for the tile-streamed CSR kernels (tiled.cuh).
 #include <algorithm>
+#include <mutex>
 #include <unordered_map>
 
 #include "tiled.cuh"
@@ -20,6 +21,7 @@ __global__ void k_pack_tiles(int ntiles, const long long* __restrict__ off, cons
         for (int e = threadIdx.x; e < ne; e += blockDim.x) cs[e] = ci[e0 + e];
         const double* src[3] = {v0, v1, v2};
         for (int k = 0; k < nvals; ++k) {
+            if (!src[k]) continue;   // value section left to its producer
             unsigned char* vs = ch + tile_val_off(nr, ne, vbytes, k);
             const double* sv = src[k] + e0;
             if (vbytes == 8) {
@@ -96,7 +98,9 @@ cfa_status pack_tiled(cfa_ctx* ctx, const int* d_rp, const int* d_ci, const doub
 }
 
 void allow_tile_kernel(const void* kernel) {
+    static std::mutex mu;
     static std::unordered_map<const void*, bool> done;
+    std::lock_guard<std::mutex> lock(mu);
     if (done[kernel]) return;
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileStages * kTileBudget + 64);
     done[kernel] = true;

@@ -73,7 +73,7 @@ __host__ __device__ inline long long tile_bytes(int nr, int ne, int nvals, int v
 cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T);
 
 // Packs pattern + values (FP64 sources; converted to float when vbytes == 4) into T.
-// vals[k] may be NULL for k >= nvals. Asynchronous.
+// A NULL source leaves its value section to be filled by its producer. Asynchronous.
 cfa_status pack_tiled(cfa_ctx* ctx, const int* d_rp, const int* d_ci, const double* v0, const double* v1,
                       const double* v2, TiledCsr& T);
 

@@ -249,6 +249,23 @@ def refine_region(mesh: Mesh, max_gen: int, radius: float = 0.3, band=(0.4, 0.6)
         mesh = nvb_round(mesh, mark)
 
 
+def refine_blob(mesh: Mesh, centre=(1.0, 0.3), radius: float = 0.05, rounds: int = 2):
+    """One remesh of an adaptive run: ``rounds`` NVB rounds on the elements whose centroid lies
+    within ``radius`` of ``centre``, then renumbered. Returns the new mesh and new_to_old, the old
+    index of every kept node (-1 for a new node), matched by exact coordinates as the reference's
+    remap test does (tests/test_cfa.cu:395-401)."""
+    old = mesh
+    for _ in range(rounds):
+        t = mesh.tri
+        cx = (mesh.x[t[:, 0]] + mesh.x[t[:, 1]] + mesh.x[t[:, 2]]) / 3.0
+        cy = (mesh.y[t[:, 0]] + mesh.y[t[:, 1]] + mesh.y[t[:, 2]]) / 3.0
+        mesh = nvb_round(mesh, np.hypot(cx - centre[0], cy - centre[1]) < radius)
+    mesh = renumber(mesh)
+    index = {xy: i for i, xy in enumerate(zip(old.x.tolist(), old.y.tolist()))}
+    new_to_old = np.array([index.get(xy, -1) for xy in zip(mesh.x.tolist(), mesh.y.tolist())], np.int32)
+    return mesh, new_to_old
+
+
 # ----------------------------------------------------------------------------------------------
 # named workloads
 # ----------------------------------------------------------------------------------------------

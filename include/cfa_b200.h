@@ -244,6 +244,18 @@ cfa_status cfa_amg_destroy(cfa_amg* amg);
  * Synchronises. CFA_COARSE_NOT_SPD if the coarsest operator is not SPD. */
 cfa_status cfa_amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* d_row_ptr,
                          const int* d_col_ind, const double* d_val);
+/* remap (:1074-1157): carries the hierarchy over to a new mesh. Level 0 takes the new operator,
+ * its inverse diagonal and a prolongator built from the old one: a kept node (h_new_to_old[i] =
+ * its old row) keeps its row, a new node (-1) gets the mean of the rows of its graph neighbours
+ * that already have one, pass by pass outwards. Levels >= 1, omega and the coarse inverse stay.
+ * h_rp/h_ci: host copy of the new operator's pattern. Sets the hierarchy up anew (as setup) when
+ * nothing can be reused: no levels, or new nodes none of whose neighbours has a row.
+ * Synchronises. */
+cfa_status cfa_amg_remap(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* d_row_ptr,
+                         const int* d_col_ind, const double* d_val, const int* h_row_ptr,
+                         const int* h_col_ind, const int* h_new_to_old);
+/* remaps: remap() calls that reused the hierarchy (the reference's `remaps`). */
+int cfa_amg_remaps(const cfa_amg* amg);
 /* apply (:1161-1168): one symmetric V-cycle, z = M^-1 r. */
 cfa_status cfa_amg_apply(cfa_ctx* ctx, cfa_amg* amg, const double* d_r, double* d_z);
 /* num_levels() (reference: levels with P + the coarsest), coarse_n, setup time [ms] */
@@ -284,6 +296,11 @@ cfa_status cfa_pcg_solve(cfa_ctx* ctx, int n, const int* d_row_ptr, const int* d
 cfa_status cfa_pressure_operator_prepare(cfa_ctx* ctx, int n, int nnz, const int* d_row_ptr,
                                          const int* d_col_ind, const double* d_val,
                                          const cfa_oss_operator* oss);
+/* Layout of the prepared pressure operator (diagnostic of this library; no counterpart in the
+ * reference): passes = 1 when K - B^T M^-1 B is stored as one matrix on the two-ring pattern (or
+ * there is no OSS term), 2 for the two-pass apply; stored_nnz = entries of the matrix streamed in
+ * the (last) pass. CFA_BAD_ARG before cfa_pressure_operator_prepare. */
+cfa_status cfa_pressure_operator_layout(const cfa_ctx* ctx, int* passes, long long* stored_nnz);
 /* The pressure operator alone (operator of cfa_pcg_solve): y = K x (- B^T M^-1 B x).
  * Asynchronous (nnz passed by the caller). Uses the tile-streamed kernels when the same operator
  * was prepared, the row kernels otherwise. */

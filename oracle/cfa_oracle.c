@@ -1056,6 +1056,145 @@ void or_amg_free(or_amg* h) {
     free(h);
 }
 
+/* AmgPreconditioner::remap (src/cfa/linalg.cuh:1074-1157): level 0 takes the new operator, its
+ * inverse diagonal and a prolongator whose rows come from the old one (kept node: its old row;
+ * new node: the mean of the rows of its graph neighbours that already have one, pass by pass
+ * outwards); levels >= 1, omega and the coarse inverse stay. Rows of new nodes are summed in
+ * column order with equal columns in accumulation order (a stable sort; the reference's
+ * std::sort leaves the order of equal columns unspecified, so its sums may differ in the last
+ * bit). Returns 1, or 0 when there is nothing to reuse (no levels, or new nodes without any
+ * neighbour that has a row): the caller then sets the hierarchy up anew. */
+typedef struct { int c; double v; } cv_pair;
+
+static void pair_msort(cv_pair* a, cv_pair* tmp, int n) {
+    if (n < 2) return;
+    int h = n / 2;
+    pair_msort(a, tmp, h);
+    pair_msort(a + h, tmp, n - h);
+    int i = 0, j = h, k = 0;
+    while (i < h && j < n) tmp[k++] = (a[j].c < a[i].c) ? a[j++] : a[i++];
+    while (i < h) tmp[k++] = a[i++];
+    while (j < n) tmp[k++] = a[j++];
+    memcpy(a, tmp, sizeof(cv_pair) * (size_t)n);
+}
+
+int or_amg_remap(or_amg* h, int n, const int* rp, const int* ci, const double* val, const int* new_to_old) {
+    if (h->nlev == 0) return 0;
+    const hcsr* Po = &h->L[0].P;
+    int* extra_of = (int*)xmalloc(sizeof(int) * (size_t)(n + 1));
+    char* has_row = (char*)xmalloc((size_t)n + 1);
+    int* pending = (int*)xmalloc(sizeof(int) * (size_t)(n + 1));
+    int* still = (int*)xmalloc(sizeof(int) * (size_t)(n + 1));
+    int* set_now = (int*)xmalloc(sizeof(int) * (size_t)(n + 1));
+    int np = 0;
+    for (int i = 0; i < n; ++i) {
+        extra_of[i] = -1;
+        has_row[i] = new_to_old[i] >= 0;
+        if (new_to_old[i] < 0) pending[np++] = i;
+    }
+    /* rows of new nodes: ex_rp[r] .. ex_rp[r + 1] in ex (grown geometrically) */
+    int nex = 0, ex_cap = 1024, rp_cap = 256;
+    cv_pair* ex = (cv_pair*)xmalloc(sizeof(cv_pair) * (size_t)ex_cap);
+    int* ex_rp = (int*)xmalloc(sizeof(int) * (size_t)rp_cap);
+    ex_rp[0] = 0;
+    int acc_cap = 256;
+    cv_pair* acc = (cv_pair*)xmalloc(sizeof(cv_pair) * (size_t)acc_cap);
+    cv_pair* tmp = (cv_pair*)xmalloc(sizeof(cv_pair) * (size_t)acc_cap);
+    int ok = 1;
+    while (np > 0) {
+        int ns = 0, nset = 0;
+        for (int q = 0; q < np; ++q) {
+            const int i = pending[q];
+            int na = 0, cnt = 0;
+            for (int a = rp[i]; a < rp[i + 1]; ++a) {
+                const int k = ci[a];
+                if (k == i || !has_row[k]) continue;
+                ++cnt;
+                const cv_pair* src;
+                cv_pair one;
+                int len;
+                int j = new_to_old[k];
+                int b0, b1;
+                if (j >= 0) { b0 = Po->rp[j]; b1 = Po->rp[j + 1]; len = b1 - b0; }
+                else { b0 = ex_rp[extra_of[k]]; b1 = ex_rp[extra_of[k] + 1]; len = b1 - b0; }
+                if (na + len > acc_cap) {
+                    while (na + len > acc_cap) acc_cap *= 2;
+                    acc = (cv_pair*)realloc(acc, sizeof(cv_pair) * (size_t)acc_cap);
+                    tmp = (cv_pair*)realloc(tmp, sizeof(cv_pair) * (size_t)acc_cap);
+                }
+                for (int b = b0; b < b1; ++b) {
+                    if (j >= 0) { one.c = Po->ci[b]; one.v = Po->v[b]; src = &one; }
+                    else src = &ex[b];
+                    acc[na++] = *src;
+                }
+            }
+            if (cnt == 0) { still[ns++] = i; continue; }
+            pair_msort(acc, tmp, na);
+            int nr = 0;
+            for (int e = 0; e < na; ++e) {
+                if (nr > 0 && acc[nr - 1].c == acc[e].c) acc[nr - 1].v += acc[e].v;
+                else acc[nr++] = acc[e];
+            }
+            for (int e = 0; e < nr; ++e) acc[e].v /= cnt;
+            if (nex + 2 > rp_cap) { rp_cap *= 2; ex_rp = (int*)realloc(ex_rp, sizeof(int) * (size_t)rp_cap); }
+            if (ex_rp[nex] + nr > ex_cap) {
+                while (ex_rp[nex] + nr > ex_cap) ex_cap *= 2;
+                ex = (cv_pair*)realloc(ex, sizeof(cv_pair) * (size_t)ex_cap);
+            }
+            memcpy(ex + ex_rp[nex], acc, sizeof(cv_pair) * (size_t)nr);
+            ex_rp[nex + 1] = ex_rp[nex] + nr;
+            extra_of[i] = nex++;
+            set_now[nset++] = i;
+        }
+        if (nset == 0) { ok = 0; break; }
+        for (int q = 0; q < nset; ++q) has_row[set_now[q]] = 1;
+        memcpy(pending, still, sizeof(int) * (size_t)ns);
+        np = ns;
+    }
+    if (ok) {
+        hcsr P;
+        P.rows = n; P.cols = Po->cols;
+        P.rp = (int*)xcalloc((size_t)n + 1, sizeof(int));
+        for (int i = 0; i < n; ++i) {
+            const int j = new_to_old[i];
+            P.rp[i + 1] = P.rp[i] + (j >= 0 ? Po->rp[j + 1] - Po->rp[j] : ex_rp[extra_of[i] + 1] - ex_rp[extra_of[i]]);
+        }
+        P.ci = (int*)xmalloc(sizeof(int) * (size_t)(P.rp[n] + 1));
+        P.v = (double*)xmalloc(sizeof(double) * (size_t)(P.rp[n] + 1));
+        for (int i = 0; i < n; ++i) {
+            const int j = new_to_old[i];
+            int o = P.rp[i];
+            if (j >= 0) {
+                for (int b = Po->rp[j]; b < Po->rp[j + 1]; ++b, ++o) { P.ci[o] = Po->ci[b]; P.v[o] = Po->v[b]; }
+            } else {
+                for (int b = ex_rp[extra_of[i]]; b < ex_rp[extra_of[i] + 1]; ++b, ++o) { P.ci[o] = ex[b].c; P.v[o] = ex[b].v; }
+            }
+        }
+        or_level* L = &h->L[0];
+        hcsr R = csr_tr(&P);
+        hcsr_free(&L->A); hcsr_free(&L->P); hcsr_free(&L->R);
+        L->A = hcsr_copy(n, rp, ci, val);
+        L->P = P;
+        L->R = R;
+        free(L->dinv); free(L->agg); free(L->x); free(L->b); free(L->r); free(L->Ax);
+        L->dinv = (double*)xmalloc(sizeof(double) * (size_t)(n + 1));
+        for (int i = 0; i < n; ++i) {
+            double d = 0.0;
+            for (int a = rp[i]; a < rp[i + 1]; ++a) if (ci[a] == i) d = val[a];
+            L->dinv[i] = (fabs(d) > 1.0e-300) ? 1.0 / d : 1.0;
+        }
+        L->agg = (int*)xmalloc(sizeof(int) * (size_t)(n + 1));
+        for (int i = 0; i < n; ++i) L->agg[i] = -1;
+        L->x = (double*)xcalloc((size_t)n + 1, sizeof(double));
+        L->b = (double*)xcalloc((size_t)n + 1, sizeof(double));
+        L->r = (double*)xcalloc((size_t)n + 1, sizeof(double));
+        L->Ax = (double*)xcalloc((size_t)n + 1, sizeof(double));
+    }
+    free(extra_of); free(has_row); free(pending); free(still); free(set_now);
+    free(ex); free(ex_rp); free(acc); free(tmp);
+    return ok;
+}
+
 /* ============================================================================================
  * Krylov solvers
  * ========================================================================================== */

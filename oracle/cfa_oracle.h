@@ -79,6 +79,8 @@ void or_amg_level_dinv(const or_amg* h, int l, double* dinv);
 int  or_amg_coarse_n(const or_amg* h);
 void or_amg_coarse(const or_amg* h, double* Ac_dense, double* inv);
 void or_amg_apply(const or_amg* h, const double* r, double* z);
+/* remap (src/cfa/linalg.cuh:1074-1157) onto a new operator; 0: set the hierarchy up anew */
+int  or_amg_remap(or_amg* h, int n, const int* rp, const int* ci, const double* val, const int* new_to_old);
 void or_amg_free(or_amg* h);
 
 /* Reference host SpGEMM and transpose (src/cfa/linalg.cuh:799-862) on plain CSR arrays.

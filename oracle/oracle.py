@@ -246,6 +246,26 @@ class Ilu:
 
 class Amg:
     def __init__(self, rp, ci, val, theta=0.08, smooth_steps=2, coarse_target=300, max_levels=15):
+        self.opts = (theta, smooth_steps, coarse_target, max_levels)
+        self.remaps = 0
+        self._setup(rp, ci, val)
+
+    def remap(self, rp, ci, val, new_to_old):
+        """AmgPreconditioner::remap (src/cfa/linalg.cuh:1074-1157); sets up anew when nothing can be
+        reused, as the reference does."""
+        rp, ci, val, n2o = i32(rp), i32(ci), f64(val), i32(new_to_old)
+        n = rp.size - 1
+        if lib().or_amg_remap(self.h, n, _p(rp), _p(ci), _p(val), _p(n2o)):
+            self.rp, self.ci, self.val, self.n = rp, ci, val, n
+            self.remaps += 1
+            return True
+        lib().or_amg_free(self.h)
+        self.h = None
+        self._setup(rp, ci, val)
+        return False
+
+    def _setup(self, rp, ci, val):
+        theta, smooth_steps, coarse_target, max_levels = self.opts
         self.rp, self.ci, self.val = i32(rp), i32(ci), f64(val)
         n = self.rp.size - 1
         h = lib().or_amg_setup(n, _p(self.rp), _p(self.ci), _p(self.val), C.c_double(theta), smooth_steps,

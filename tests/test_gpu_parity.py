@@ -389,6 +389,58 @@ def test_amg_cluster_tail_matches_level_kernels(ctx, precision, monkeypatch):
     assert np.abs(out[1] - out[0]).max() <= 1e-12 * np.abs(out[0]).max()
 
 
+@pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
+def test_amg_remap_matches_oracle(ctx, precision):
+    """remap (a24) against the oracle's restatement: the level-0 prolongator and restriction
+    bit-exact, the V-cycle within 1e-12 (FP64) / 1e-6 (FP32 hierarchy); an unchanged mesh gives the
+    setup's V-cycle; the remapped hierarchy after a local refinement solves to 1e-10 within the
+    reference's iteration bound."""
+    from tests.golden.make_golden import shifted_laplacian
+    m = mesh("medium")
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    a = shifted_laplacian(rp, ci)
+    drp, dci, da = dev(rp, torch.int32), dev(ci, torch.int32), dev(a)
+    amg = cfa.AmgPreconditioner(ctx, precision=precision)
+    amg.setup(m.n, ci.size, drp, dci, da)
+    r = dev(np.sin(0.37 * np.arange(m.n)) + 0.2)
+    z0 = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+    amg.apply(r, z0)
+    amg.remap(m.n, ci.size, drp, dci, da, rp, ci, np.arange(m.n))
+    assert amg.remaps == 1
+    z1 = torch.zeros_like(z0)
+    amg.apply(r, z1)
+    assert torch.equal(z0, z1)
+    m2, n2o = F.refine_blob(m, radius=0.08, rounds=3)
+    rp2, ci2 = O.csr_build(m2.n, m2.elem_v)
+    a2 = shifted_laplacian(rp2, ci2)
+    drp2, dci2, da2 = dev(rp2, torch.int32), dev(ci2, torch.int32), dev(a2)
+    amg.remap(m2.n, ci2.size, drp2, dci2, da2, rp2, ci2, n2o)
+    assert amg.remaps == 2
+    oa = O.Amg(rp, ci, a)
+    assert oa.remap(rp2, ci2, a2, n2o)
+    want, got = oa.level(0), amg.level(0)
+    for name in ("P", "R"):
+        wr, wc, (wrp, wci, wv) = want[name][0], want[name][1], want[name][2:]
+        grp, gci, gv = (host(t) for t in got[name])
+        assert np.array_equal(grp, wrp) and np.array_equal(gci, wci) and np.array_equal(gv, wv)
+    r2 = np.sin(0.29 * np.arange(m2.n)) + 0.1
+    z = torch.zeros(m2.n, dtype=torch.float64, device="cuda")
+    amg.apply(dev(r2), z)
+    zo = oa.apply(r2)
+    tol = 1e-12 if precision == cfa.FP64 else 1e-6
+    assert np.abs(host(z) - zo).max() <= tol * np.abs(zo).max()
+    s = cfa.GpuLinearSolver(ctx)
+    b = dev(np.cos(0.11 * np.arange(m2.n)))
+    x = torch.zeros(m2.n, dtype=torch.float64, device="cuda")
+    it_remap = s.solve_pcg(m2.n, drp2, dci2, da2, b, x, 400, 1e-10, None, amg)
+    assert s.converged
+    fresh = cfa.AmgPreconditioner(ctx, precision=precision)
+    fresh.setup(m2.n, ci2.size, drp2, dci2, da2)
+    x.zero_()
+    it_setup = s.solve_pcg(m2.n, drp2, dci2, da2, b, x, 400, 1e-10, None, fresh)
+    assert s.converged and it_remap <= 3 * it_setup + 5
+
+
 def test_amg_coarse_not_spd_is_an_error(ctx):
     m = mesh("tiny")
     rp, ci = O.csr_build(m.n, m.elem_v)
@@ -442,6 +494,35 @@ def test_pcg_matches_oracle(ctx, use_oss, use_amg):
     if use_oss:
         O.oss_apply(m, rp, ci, oss, inv_m, x, Ax)
     assert np.linalg.norm(rhs - Ax) <= 1.5e-10 * np.linalg.norm(rhs)
+
+
+@pytest.mark.parametrize("name,outlet_dirichlet", [("small", 0), ("medium", 0), ("medium", 1)])
+def test_pressure_operator_fused_oss_matches_oracle(name, outlet_dirichlet, monkeypatch):
+    """K - B^T M^-1 B assembled into one two-ring matrix (the default) and the two-pass apply
+    against the oracle's K x and apply_oss_projection: 1e-13 of the largest entry."""
+    m = mesh(name)
+    results = []
+    for fused in ("1", "0"):
+        monkeypatch.setenv("CFA_OSS_FUSED", fused)
+        c = cfa.Context(stream=cfa.default_context().stream)   # a fresh context plans its operator anew
+        dm = cfa.DeviceMesh(c, m)
+        pin = int(np.argmax(m.x)) if outlet_dirichlet else -1
+        if outlet_dirichlet:
+            dm.set_outlet(1, pin, 1.0)
+        rp, ci = dm.host_pattern()
+        Kp, rhs, oss, inv_m = pressure_system(m, rp, ci)
+        x = np.sin(0.3 * np.arange(m.n)) + 0.1
+        want = O.spmv(rp, ci, Kp, x)
+        O.oss_apply(m, rp, ci, oss, inv_m, x, want, outlet_dirichlet=outlet_dirichlet, pin=pin)
+        dK, doss, dinv = dev(Kp), dev(oss), dev(inv_m)
+        op = cfa.oss_operator(dm, doss, dinv)
+        cfa.pressure_operator_prepare(c, dm.rp, dm.ci, dK, op)
+        y = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+        cfa.pressure_operator(c, dm.rp, dm.ci, dK, dev(x), y, op)
+        got = host(y)
+        assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+        results.append(got)
+    assert np.abs(results[0] - results[1]).max() <= 1e-13 * np.abs(results[1]).max()
 
 
 def test_pcg_mixed_precision_reaches_tolerance(ctx):

@@ -153,6 +153,39 @@ def test_amg_setup_and_pcg_restated():
     assert np.linalg.norm(r) < 1.01e-10 * np.linalg.norm(b)
 
 
+def test_amg_remap_restated():
+    """test_amg_remap (tests/test_cfa.cu:372-437): remapping onto an unchanged mesh gives the
+    setup's V-cycle; after a local refinement (new nodes) the remapped hierarchy reaches 1e-10
+    with at most 3x + 5 the iterations of a fresh setup."""
+    from tests.golden.make_golden import shifted_laplacian
+    m = F.make_mesh("medium")
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    a = shifted_laplacian(rp, ci)
+    amg = O.Amg(rp, ci, a)
+    assert amg.nlev + 1 > 2
+    r = np.sin(0.37 * np.arange(m.n)) + 0.2
+    z_setup = amg.apply(r)
+    assert amg.remap(rp, ci, a, np.arange(m.n)) and amg.remaps == 1
+    z_remap = amg.apply(r)
+    assert np.abs(z_remap - z_setup).max() <= 1e-14 * np.abs(z_setup).max()
+    m2, n2o = F.refine_blob(m, radius=0.08, rounds=3)
+    assert m2.n > m.n and (n2o < 0).any() and (n2o >= 0).sum() == m.n
+    rp2, ci2 = O.csr_build(m2.n, m2.elem_v)
+    a2 = shifted_laplacian(rp2, ci2)
+    assert amg.remap(rp2, ci2, a2, n2o) and amg.remaps == 2
+    b = np.cos(0.11 * np.arange(m2.n))
+    x, rep = O.pcg(rp2, ci2, a2, b, np.zeros(m2.n), 400, 1e-10, amg=amg)
+    x2, rep2 = O.pcg(rp2, ci2, a2, b, np.zeros(m2.n), 400, 1e-10, amg=O.Amg(rp2, ci2, a2))
+    assert rep.converged and rep2.converged
+    assert rep.iterations <= 3 * rep2.iterations + 5
+    # a hierarchy without levels has nothing to reuse: remap sets it up anew
+    t = F.make_mesh("tiny")
+    trp, tci = O.csr_build(t.n, t.elem_v)
+    small = O.Amg(trp, tci, shifted_laplacian(trp, tci), coarse_target=t.n)
+    assert small.nlev == 0 and not small.remap(trp, tci, shifted_laplacian(trp, tci), np.arange(t.n))
+    assert small.remaps == 0
+
+
 def test_pcg_oss_amg_step():
     """The pressure solve of a synthetic step: PCG + OSS + AMG reaches 1e-10 with far fewer
     iterations than Jacobi, and both agree."""
