@@ -337,6 +337,135 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------------------------------------
+# bandwidth stress (c2): ~4M vertices, repeated solves with perturbed right-hand sides
+# ------------------------------------------------------------------------------------------------
+def vcycle_bytes(levels, coarse_n, vb):
+    """Algorithmic bytes of one V(2,2) cycle of the tile kernels: per level with n rows, z entries
+    of A and q of P (= of R), values of vb bytes: pre-smoothing (initial guess fused), residual,
+    restriction, prolongation-add and two post-smoothing sweeps, each reading its matrix once
+    (column index + value, row offsets) and its vectors (8 bytes per entry read or written);
+    the dense coarse solve reads its inverse."""
+    total = 0
+    for (n, z, nc, q) in levels:
+        mat_a = z * (vb + 4) + 4 * (n + 1)
+        total += mat_a + 8 * n * 4                       # pre: b, dinv, b (own), x write
+        total += mat_a + 8 * n * 3                       # residual: x, b, r write
+        total += q * (vb + 4) + 4 * (nc + 1) + 8 * n + 8 * nc          # restriction
+        total += q * (vb + 4) + 4 * (n + 1) + 8 * nc + 16 * n          # prolongation-add
+        total += 2 * (mat_a + 8 * n * 4)                 # two Jacobi sweeps: x, b, dinv, out
+    return total + 8 * coarse_n * coarse_n + 16 * coarse_n
+
+
+def run_stress(args, rank, world):
+    import torch
+    import cfa_b200 as cfa
+    import step as S
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    m, u, v, p = workload_inputs("c2")
+    ctx = cfa.Context()
+    st = S.SolveStep(m, u, v, p, precision=cfa.MIXED, ctx=ctx, dt=DT, nu=NU, stab=STAB, u_max=U_MAX, tol=TOL)
+    st.amg_setup()
+    base_u, base_v, base_p = st.rhs_u.clone(), st.rhs_v.clone(), st.rhs_p.clone()
+    n, nnz = st.n, st.nnz
+    solves = max(args.steps, 1)
+
+    def perturbed(k):
+        g = torch.Generator(device="cuda")
+        g.manual_seed(k)
+        st.rhs_u.copy_(base_u + 1e-3 * torch.randn(n, generator=g, device="cuda", dtype=torch.float64))
+        st.rhs_v.copy_(base_v + 1e-3 * torch.randn(n, generator=g, device="cuda", dtype=torch.float64))
+        st.rhs_p.copy_(base_p + 1e-3 * torch.randn(n, generator=g, device="cuda", dtype=torch.float64))
+        st.u.copy_(st.u_n)
+        st.v.copy_(st.v_n)
+        st.dp.zero_()
+
+    for k in range(args.warmup):
+        perturbed(1000 + k)
+        st.solve_momentum()
+        st.solve_pressure()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
+    clk.start()
+    total, its = 0.0, []
+    l0 = ctx.launches
+    for k in range(solves):
+        perturbed(k)
+        ev[0].record()
+        st.solve_momentum()
+        st.solve_pressure()
+        ev[1].record()
+        ev[1].synchronize()
+        total += ev[0].elapsed_time(ev[1])
+        r = st.report()
+        its.append((r["it_u"], r["it_v"], r["it_p"]))
+    launches = ctx.launches - l0
+    # per-kernel bandwidth: each path applied alone, repeated, timed by events on the context stream
+    reps = 20
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        acc = 0.0
+        for _ in range(reps):
+            flush.add_(1.0)
+            ev[0].record()
+            fn()
+            ev[1].record()
+            ev[1].synchronize()
+            acc += ev[0].elapsed_time(ev[1])
+        return acc / reps * 1e3
+
+    hbm, peak_kind = peaks()
+    x = torch.randn(n, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    cfa.pressure_operator_prepare(ctx, st.dm.rp, st.dm.ci, st.Kp, st.oss)
+    passes, stored = cfa.pressure_operator_layout(ctx)
+    t_op = timed(lambda: cfa.pressure_operator(ctx, st.dm.rp, st.dm.ci, st.Kp, x, y, st.oss))
+    b_op = operator_bytes(n, nnz, passes, stored)
+    z = torch.empty_like(x)
+    t_vc = timed(lambda: st.amg.apply(x, z))
+    levels = []
+    for l in range(st.amg.num_levels() - 1):
+        d = st.amg.level(l)
+        levels.append((d["rows"], int(d["A"][1].numel()), d["pcols"], int(d["P"][1].numel())))
+    b_vc = vcycle_bytes(levels, st.amg.coarse_n, 4)
+    x2 = torch.randn(2 * n, dtype=torch.float64, device="cuda")
+    z2 = torch.empty_like(x2)
+    t_ilu = timed(lambda: st.ilu.apply(x2, z2, 2))
+    b_ilu = (nnz - n) * (4 + 4) + n * 4 + 4 * n + 8 * (n + 1) + 2 * n * 8 * 4
+    t_spmv = timed(lambda: cfa.spmv_multi(ctx, st.dm.rp, st.dm.ci, st.A, x2, z2, 2))
+    b_spmv = nnz * 12 + 4 * (n + 1) + 4 * n * 8
+    clk.stop()
+    kern = {}
+    for name, b, t in (("pressure_operator", b_op, t_op), ("vcycle_fp32", b_vc, t_vc), ("ilu_apply_2rhs_fp32", b_ilu, t_ilu),
+                       ("momentum_spmv_2rhs", b_spmv, t_spmv)):
+        gbs = b / (t * 1e-6) / 1e9
+        kern[name] = {"bytes": int(b), "us": round(t, 2), "gbs": round(gbs, 1), "frac": round(gbs / hbm, 4)}
+    ms = total / solves
+    line = {
+        "metric": "pressure+momentum solve ms per repeated solve & HBM GB/s per kernel (c2, mixed, 1e-10 rel res)",
+        "value": round(ms, 3), "unit": "ms/solve pair", "n_gpus": 1, "steps": solves, "warmup": args.warmup,
+        "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 outer / f32 preconditioners", "data": "synthetic",
+        "config": {"workload": f"c2: uniform NVB mesh n={n}, nnz={nnz}; {solves} solves, RHS + N(0, 1e-3) noise "
+                               "seeded by the solve index (momentum BiCGSTAB2 + pressure PCG)",
+                   "l2": "inputs larger than L2", "iterations_median": [int(np.median([i[c] for i in its])) for c in range(3)],
+                   "amg_levels": st.amg.num_levels(), "pressure_operator_passes": passes},
+        "kernels": kern,
+        "roofline": {"bound": "hbm", "kernel": "pressure operator (K - B^T M^-1 B, one pass), FP64",
+                     "achieved": kern["pressure_operator"]["gbs"], "peak": hbm, "unit": "GB/s",
+                     "frac": kern["pressure_operator"]["frac"], "traffic": None, "peak_kind": peak_kind},
+        "e2e": {"value": round(ms, 3), "unit": "ms/solve pair", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 48},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------------------------------------
 # batched systems (c4): 64 independent system pairs, 5k-500k vertices, LPT over GPUs
 # ------------------------------------------------------------------------------------------------
 def run_batch(args, rank, world):
@@ -426,6 +555,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     if args.workload == "c4":
         run_batch(args, rank, world)
+        return
+    if args.workload == "c2":
+        if rank == 0:
+            run_stress(args, rank, world)
         return
     m, res = run_ours(args, rank, world)
     if args.profile:

@@ -245,6 +245,43 @@ def oss_apply(ctx, m: DeviceMesh, oss_val, inv_m, x, out):
     ctx.check(lib().cfa_oss_apply(ctx.h, m.h, ptr(oss_val), ptr(inv_m), ptr(x), ptr(out)))
 
 
+def stiffness_apply(ctx, m: DeviceMesh, f, c, out):
+    ctx.check(lib().cfa_stiffness_apply(ctx.h, m.h, ptr(f), C.c_double(c), ptr(out)))
+
+
+def grad_dp_vorticity(ctx, m: DeviceMesh, dp, u, v, gdx, gdy, vort_num):
+    ctx.check(lib().cfa_grad_dp_vorticity(ctx.h, m.h, ptr(dp), ptr(u), ptr(v), ptr(gdx), ptr(gdy), ptr(vort_num)))
+
+
+def velocity_pressure_correction(ctx, m: DeviceMesh, dt, rho, p_update, rot_coeff, div_num, mass, gdx, gdy,
+                                 vort_num, dp, u, v, p, vort=None):
+    ctx.check(lib().cfa_velocity_pressure_correction(ctx.h, m.h, C.c_double(dt), C.c_double(rho),
+                                                     C.c_double(p_update), C.c_double(rot_coeff), ptr(div_num),
+                                                     ptr(mass), ptr(gdx), ptr(gdy), ptr(vort_num), ptr(dp), ptr(u),
+                                                     ptr(v), ptr(p), ptr(vort)))
+
+
+def project_step(ctx, m: DeviceMesh, dt_proj, rho, rot_coeff, rotational_from_dp, mass, dp, div_num, gdx, gdy,
+                 vort_num, u, v, p, vort=None):
+    ctx.check(lib().cfa_project_step(ctx.h, m.h, C.c_double(dt_proj), C.c_double(rho), C.c_double(rot_coeff),
+                                     int(rotational_from_dp), ptr(mass), ptr(dp), ptr(div_num), ptr(gdx), ptr(gdy),
+                                     ptr(vort_num), ptr(u), ptr(v), ptr(p), ptr(vort)))
+
+
+def volume_forces(ctx, m: DeviceMesh, u, v, u_old, v_old, u_prev, v_prev, p, b0, b1, b2, nu, rho, out2):
+    ctx.check(lib().cfa_volume_forces(ctx.h, m.h, ptr(u), ptr(v), ptr(u_old), ptr(v_old), ptr(u_prev), ptr(v_prev),
+                                      ptr(p), C.c_double(b0), C.c_double(b1), C.c_double(b2), C.c_double(nu),
+                                      C.c_double(rho), ptr(out2)))
+
+
+def amr_indicators(ctx, m: DeviceMesh, u, v, u_max, H, mass, grad_rec, elem_error):
+    """k_accumulate_recovered_gradient + k_compute_amr_error_indicator: grad_rec [4 n] and
+    elem_error [2 ne] (device, overwritten)."""
+    ctx.check(lib().cfa_recovered_gradient(ctx.h, m.h, ptr(u), ptr(v), C.c_double(u_max), C.c_double(H),
+                                           ptr(grad_rec)))
+    ctx.check(lib().cfa_amr_error_indicator(ctx.h, m.h, ptr(grad_rec), ptr(mass), ptr(elem_error)))
+
+
 def spmv(ctx, rp, ci, val, x, y):
     ctx.check(lib().cfa_spmv(ctx.h, rp.numel() - 1, ptr(rp), ptr(ci), ptr(val), ptr(x), ptr(y)))
 

@@ -101,3 +101,101 @@ class SolveStep:
         return dict(it_u=self.mom.iters[0], it_v=self.mom.iters[1], it_p=self.it_p,
                     conv=[bool(self.mom.converged[0]), bool(self.mom.converged[1]), bool(self.solver.converged)],
                     rel=[self.mom.last_rel_residual[0], self.mom.last_rel_residual[1], self.solver.last_rel_residual])
+
+
+class TimeStepper:
+    """The reference driver's time loop on one fixed mesh (src/cylinder_fem_amr.cu:276-520):
+    BDF2 incremental pressure correction in rotational form, first step backward Euler.
+
+      history: u_prev <- u_old <- u;
+      A. momentum assembly + BCs, ILU(0), BiCGSTAB2 (u, v) from u^n;
+      B. OSS weights, G(p^n), pressure system, AMG rebuilt every ``amg_rebuild`` steps, PCG from
+         the last dp;
+      C. div_num = -(dt'/rho) K dp (rotational term from the increment), grad dp, vorticity,
+         u -= dt'/rho M^-1 grad dp, p += dp - rho nu M^-1 div_num;
+      D. volume-integral drag and lift, C_D = force_scale F_x, C_L = force_scale F_y.
+
+    Everything stays on the device; ``step()`` returns (C_D, C_L) (one 16-byte read per step)."""
+
+    def __init__(self, mesh, u0, v0, p0, precision=cfa.FP64, dt=1e-3, nu=1e-3, rho=1.0, tau_time=1e-3, stab=0.3,
+                 u_max=1.5, H=1.0, u_mean=1.0, diameter=0.2, tol_mom=1e-7, tol_p=1e-7, max_it_mom=150,
+                 max_it_p=4000, amg_rebuild=50, rotational=True, bdf2=True, ctx=None, dm=None):
+        import torch
+        self.ctx = ctx or cfa.default_context()
+        self.dm = dm or cfa.DeviceMesh(self.ctx, mesh)
+        n, ne, nnz = self.dm.n, self.dm.ne, self.dm.nnz
+        self.n, self.ne, self.nnz = n, ne, nnz
+        f64 = dict(dtype=torch.float64, device="cuda")
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to("cuda")
+        self.u, self.v, self.p = t(u0), t(v0), t(p0)
+        self.u_old, self.v_old = self.u.clone(), self.v.clone()
+        self.u_prev, self.v_prev = self.u.clone(), self.v.clone()
+        z = lambda k: torch.zeros(k, **f64)
+        self.A, self.rhs_u, self.rhs_v, self.mass = z(nnz), z(n), z(n), z(n)
+        self.elem_s, self.gpx, self.gpy = z(ne), z(n), z(n)
+        self.Kp, self.rhs_p, self.div, self.dp = z(nnz), z(n), z(n), z(n)
+        self.oss_val, self.inv_m = z(4 * nnz), z(n)
+        self.vort_num, self.vort = z(n), z(n)
+        self.forces = z(2)
+        self.dt, self.nu, self.rho, self.tau_time, self.stab = dt, nu, rho, tau_time, stab
+        self.u_max, self.H = u_max, H
+        self.force_scale = -2.0 / (u_mean * u_mean * diameter)
+        self.tol_mom, self.tol_p, self.max_it_mom, self.max_it_p = tol_mom, tol_p, max_it_mom, max_it_p
+        self.amg_rebuild, self.rotational, self.bdf2 = amg_rebuild, rotational, bdf2
+        rp_h, ci_h = self.dm.host_pattern()
+        self.ilu = cfa.MulticolourIlu0(self.ctx, precision)
+        self.ilu.set_pattern(n, rp_h, ci_h, self.dm.rp, self.dm.ci)
+        self.mom = cfa.GpuBicgstab2(self.ctx)
+        self.solver = cfa.GpuLinearSolver(self.ctx)
+        self.amg = cfa.AmgPreconditioner(self.ctx, precision)
+        self.oss = cfa.oss_operator(self.dm, self.oss_val, self.inv_m) if stab > 0.0 else None
+        self.step_no = 0
+        self.amg_built = None
+        self.iters = []
+
+    def coefficients(self):
+        """(dt', a0, a1, a2, c1, c2) of this step (src/cylinder_fem_amr.cu:288-294)."""
+        dt = self.dt
+        bdf2 = self.bdf2 and self.step_no > 1
+        if bdf2:
+            return (2.0 / 3.0) * dt, 1.5 / dt, 2.0 / dt, -0.5 / dt, 2.0, -1.0
+        return dt, 1.0 / dt, 1.0 / dt, 0.0, 1.0, 0.0
+
+    def step(self):
+        c, d = self.ctx, self.dm
+        self.step_no += 1
+        dt_proj, a0, a1, a2, c1, c2 = self.coefficients()
+        self.u_prev.copy_(self.u_old)
+        self.v_prev.copy_(self.v_old)
+        self.u_old.copy_(self.u)
+        self.v_old.copy_(self.v)
+        # A
+        prm = cfa.MomentumParams(self.dt, self.nu, self.rho, a0, a1, a2, c1, c2,
+                            self.tau_time if self.tau_time > 0.0 else self.dt, 0.5)
+        cfa.assemble_momentum(c, d, self.u_old, self.v_old, self.u_prev, self.v_prev, self.p, prm, self.A,
+                              self.rhs_u, self.rhs_v, self.mass, self.u, self.v, u_max=self.u_max, H=self.H)
+        self.ilu.factor(self.A)
+        self.mom.solve(self.n, d.rp, d.ci, self.A, self.rhs_u, self.rhs_v, self.u, self.v, self.max_it_mom,
+                       self.tol_mom, self.ilu)
+        # B
+        if self.stab > 0.0:
+            cfa.oss_weights(c, d, self.u, self.v, dt_proj, self.rho, self.nu, self.stab, self.elem_s)
+            cfa.scalar_gradient(c, d, self.p, self.elem_s, self.gpx, self.gpy)
+        cfa.assemble_pressure_system(c, d, self.u, self.v, self.p, self.gpx, self.gpy, self.mass, self.elem_s,
+                                     dt_proj, self.rho, self.stab, self.Kp, self.rhs_p, self.div, self.dp,
+                                     self.oss_val, self.inv_m)
+        if self.amg_built is None or self.step_no - self.amg_built >= self.amg_rebuild:
+            self.amg.setup(self.n, self.nnz, d.rp, d.ci, self.Kp)
+            self.amg_built = self.step_no
+        it_p = self.solver.solve_pcg(self.n, d.rp, d.ci, self.Kp, self.rhs_p, self.dp, self.max_it_p, self.tol_p,
+                                     self.oss, self.amg)
+        self.iters.append((self.mom.iters[0], self.mom.iters[1], it_p))
+        # C
+        rot_coeff = self.rho * self.nu if self.rotational else 0.0
+        cfa.project_step(c, d, dt_proj, self.rho, rot_coeff, True, self.mass, self.dp, self.div, self.gpx, self.gpy,
+                         self.vort_num, self.u, self.v, self.p, self.vort)
+        # D
+        cfa.volume_forces(c, d, self.u, self.v, self.u_old, self.v_old, self.u_prev, self.v_prev, self.p, a0, -a1,
+                          -a2, self.nu, self.rho, self.forces)
+        f = self.forces.cpu().numpy()
+        return self.force_scale * f[0], self.force_scale * f[1]

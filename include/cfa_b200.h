@@ -169,6 +169,55 @@ cfa_status cfa_oss_apply_noalloc(cfa_ctx* ctx, const cfa_mesh* mesh, const doubl
                                  const double* d_inv_m, const double* d_in, double* d_out);
 
 /* ---------------------------------------------------------------------------------------------
+ * after the solves (the driver's Steps C and D, src/cylinder_fem_amr.cu:462-513); node sums are
+ * gathered over each node's elements in ascending element order (the reference scatters them
+ * with atomics), so results are deterministic.
+ * ------------------------------------------------------------------------------------------- */
+/* k_stiffness_apply (src/cfa/fem_kernels.cuh:618-637): d_out[i] += c (grad N_i, grad f). */
+cfa_status cfa_stiffness_apply(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_f, double c,
+                               double* d_out);
+/* k_accumulate_grad_dp_and_vorticity (src/cfa/fem_kernels.cuh:536-575): the lumped-mass
+ * numerators of grad dp and of the vorticity dv/dx - du/dy. Overwrites the three outputs (the
+ * reference accumulates into zeroed arrays). */
+cfa_status cfa_grad_dp_vorticity(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_dp,
+                                 const double* d_u, const double* d_v, double* d_grad_dp_x,
+                                 double* d_grad_dp_y, double* d_vort_num);
+/* k_velocity_pressure_correction (src/cfa/fem_kernels.cuh:585-610): vort = vort_num / m,
+ * p += p_update (dp - rot_coeff div_num / m), u -= (dt/rho) grad_dp_x / m and likewise v on
+ * interior nodes and on a natural outlet. d_vort may be NULL. */
+cfa_status cfa_velocity_pressure_correction(cfa_ctx* ctx, const cfa_mesh* mesh, double dt, double rho,
+                                            double p_update, double rot_coeff, const double* d_div_num,
+                                            const double* d_mass_lumped, const double* d_grad_dp_x,
+                                            const double* d_grad_dp_y, const double* d_vort_num,
+                                            const double* d_dp, double* d_u, double* d_v, double* d_p,
+                                            double* d_vort);
+/* Step C in two passes: with rotational_from_dp, div_num = -(dt_proj/rho) K dp (the driver's
+ * k_stiffness_apply on a zeroed div_num, src/cylinder_fem_amr.cu:467-472; otherwise div_num is
+ * used as the PPE assembly left it), then grad dp and vorticity, then the correction with
+ * p_update = 1. */
+cfa_status cfa_project_step(cfa_ctx* ctx, const cfa_mesh* mesh, double dt_proj, double rho,
+                            double rot_coeff, int rotational_from_dp, const double* d_mass_lumped,
+                            const double* d_dp, double* d_div_num, double* d_grad_dp_x,
+                            double* d_grad_dp_y, double* d_vort_num, double* d_u, double* d_v,
+                            double* d_p, double* d_vort);
+/* k_volume_forces (src/cfa/fem_kernels.cuh:1046-1123): volume-integral drag and lift into
+ * d_out2[0..1] (device; overwritten), du/dt = b0 u + b1 u_old + b2 u_prev. */
+cfa_status cfa_volume_forces(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_u, const double* d_v,
+                             const double* d_u_old, const double* d_v_old, const double* d_u_prev,
+                             const double* d_v_prev, const double* d_p, double b0, double b1, double b2,
+                             double nu, double rho, double* d_out2);
+
+/* AMR refinement indicators (the remesh side of the path). k_accumulate_recovered_gradient
+ * (src/cfa/fem_kernels.cuh:911-968): d_grad_rec[4 n] = [du'/dx | du'/dy | dv/dx | dv/dy]
+ * numerators of the disturbance velocity u' = u - 4 U y (H - y) / H^2 (overwritten). */
+cfa_status cfa_recovered_gradient(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_u, const double* d_v,
+                                  double u_max, double H, double* d_grad_rec);
+/* k_compute_amr_error_indicator (src/cfa/fem_kernels.cuh:995-1035): d_elem_error[2 ne] =
+ * [h_K max |omega - omega_P| | P1 interpolation-error estimate]. */
+cfa_status cfa_amr_error_indicator(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_grad_rec,
+                                   const double* d_mass_lumped, double* d_elem_error);
+
+/* ---------------------------------------------------------------------------------------------
  * sparse kernels
  * ------------------------------------------------------------------------------------------- */
 /* k_spmv_csr (src/cfa/linalg.cuh:8-26): y = A x, FP64. */

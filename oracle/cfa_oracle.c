@@ -312,6 +312,147 @@ void or_scalar_gradient(int ne, const int* ev, const double* x, const double* y,
     }
 }
 
+/* k_stiffness_apply (src/cfa/fem_kernels.cuh:618-637): out_i += c area (dN_i . grad f) */
+void or_stiffness_apply(int ne, const int* ev, const double* x, const double* y, const double* f, double c,
+                        double* out) {
+    for (int e = 0; e < ne; ++e) {
+        const int nd[3] = {ev[3 * e], ev[3 * e + 1], ev[3 * e + 2]};
+        geom g = elem_geom(nd, x, y);
+        if (!g.ok) continue;
+        double gx = f[nd[0]] * g.dNdx[0] + f[nd[1]] * g.dNdx[1] + f[nd[2]] * g.dNdx[2];
+        double gy = f[nd[0]] * g.dNdy[0] + f[nd[1]] * g.dNdy[1] + f[nd[2]] * g.dNdy[2];
+        for (int a = 0; a < 3; ++a) out[nd[a]] += c * g.area * (g.dNdx[a] * gx + g.dNdy[a] * gy);
+    }
+}
+
+/* k_accumulate_grad_dp_and_vorticity (src/cfa/fem_kernels.cuh:536-575); accumulated */
+void or_grad_dp_vorticity(int ne, const int* ev, const double* x, const double* y, const double* dp,
+                          const double* u, const double* v, double* gdx, double* gdy, double* vort_num) {
+    for (int e = 0; e < ne; ++e) {
+        const int nd[3] = {ev[3 * e], ev[3 * e + 1], ev[3 * e + 2]};
+        geom g = elem_geom(nd, x, y);
+        if (!g.ok) continue;
+        double dpdx = dp[nd[0]] * g.dNdx[0] + dp[nd[1]] * g.dNdx[1] + dp[nd[2]] * g.dNdx[2];
+        double dpdy = dp[nd[0]] * g.dNdy[0] + dp[nd[1]] * g.dNdy[1] + dp[nd[2]] * g.dNdy[2];
+        double dvdx = v[nd[0]] * g.dNdx[0] + v[nd[1]] * g.dNdx[1] + v[nd[2]] * g.dNdx[2];
+        double dudy = u[nd[0]] * g.dNdy[0] + u[nd[1]] * g.dNdy[1] + u[nd[2]] * g.dNdy[2];
+        double w = g.area / 3.0;
+        for (int a = 0; a < 3; ++a) {
+            gdx[nd[a]] += w * dpdx;
+            gdy[nd[a]] += w * dpdy;
+            vort_num[nd[a]] += w * (dvdx - dudy);
+        }
+    }
+}
+
+/* k_velocity_pressure_correction (src/cfa/fem_kernels.cuh:585-610) */
+void or_velocity_pressure_correction(int n, const int* tag, int outlet_dirichlet, double dt, double rho,
+                                     double p_update, double rot_coeff, const double* div_num,
+                                     const double* mass, const double* gdx, const double* gdy,
+                                     const double* vort_num, const double* dp, double* u, double* v, double* p,
+                                     double* vort) {
+    for (int i = 0; i < n; ++i) {
+        double m_i = fmax(mass[i], 1.0e-14);
+        vort[i] = vort_num[i] / m_i;
+        p[i] += p_update * (dp[i] - rot_coeff * div_num[i] / m_i);
+        if (tag[i] == BC_INTERIOR || (tag[i] == BC_OUTLET && !outlet_dirichlet)) {
+            u[i] -= (dt / rho) * (gdx[i] / m_i);
+            v[i] -= (dt / rho) * (gdy[i] / m_i);
+        }
+    }
+}
+
+/* k_volume_forces (src/cfa/fem_kernels.cuh:1046-1123): out[0..1] accumulated */
+void or_volume_forces(int ne, const int* ev, const int* tag, const double* x, const double* y, const double* u,
+                      const double* v, const double* u_old, const double* v_old, const double* u_prev,
+                      const double* v_prev, const double* p, double b0, double b1, double b2, double nu,
+                      double rho, double* out) {
+    for (int e = 0; e < ne; ++e) {
+        const int nd[3] = {ev[3 * e], ev[3 * e + 1], ev[3 * e + 2]};
+        double phi[3];
+        int touches = 0;
+        for (int a = 0; a < 3; ++a) {
+            phi[a] = tag[nd[a]] == BC_CYLINDER ? 1.0 : 0.0;
+            touches = touches || phi[a] > 0.0;
+        }
+        if (!touches) continue;
+        geom g = elem_geom(nd, x, y);
+        if (!g.ok) continue;
+        double ue[3], ve[3], ute[3], vte[3];
+        double dudx = 0.0, dudy = 0.0, dvdx = 0.0, dvdy = 0.0, dphidx = 0.0, dphidy = 0.0, p_bar = 0.0;
+        for (int a = 0; a < 3; ++a) {
+            ue[a] = u[nd[a]];
+            ve[a] = v[nd[a]];
+            ute[a] = b0 * ue[a] + b1 * u_old[nd[a]] + b2 * u_prev[nd[a]];
+            vte[a] = b0 * ve[a] + b1 * v_old[nd[a]] + b2 * v_prev[nd[a]];
+            dudx += ue[a] * g.dNdx[a]; dudy += ue[a] * g.dNdy[a];
+            dvdx += ve[a] * g.dNdx[a]; dvdy += ve[a] * g.dNdy[a];
+            dphidx += phi[a] * g.dNdx[a]; dphidy += phi[a] * g.dNdy[a];
+            p_bar += p[nd[a]] / 3.0;
+        }
+        double fx = 0.0, fy = 0.0;
+        for (int a = 0; a < 3; ++a) {
+            int b = (a + 1) % 3;
+            double phi_m = 0.5 * (phi[a] + phi[b]);
+            if (phi_m == 0.0) continue;
+            double um = 0.5 * (ue[a] + ue[b]), vm = 0.5 * (ve[a] + ve[b]);
+            fx += (0.5 * (ute[a] + ute[b]) + (um * dudx + vm * dudy)) * phi_m;
+            fy += (0.5 * (vte[a] + vte[b]) + (um * dvdx + vm * dvdy)) * phi_m;
+        }
+        fx *= g.area / 3.0;
+        fy *= g.area / 3.0;
+        fx += g.area * (nu * (dudx * dphidx + dudy * dphidy) - (p_bar / rho) * dphidx);
+        fy += g.area * (nu * (dvdx * dphidx + dvdy * dphidy) - (p_bar / rho) * dphidy);
+        out[0] += fx;
+        out[1] += fy;
+    }
+}
+
+/* k_accumulate_recovered_gradient (src/cfa/fem_kernels.cuh:911-968); grad_rec accumulated */
+void or_recovered_gradient(int n, int ne, const int* ev, const double* x, const double* y, const double* u,
+                           const double* v, double u_max, double H, double* grad_rec) {
+    for (int e = 0; e < ne; ++e) {
+        const int nd[3] = {ev[3 * e], ev[3 * e + 1], ev[3 * e + 2]};
+        geom g = elem_geom(nd, x, y);
+        if (!g.ok) continue;
+        double ud[3];
+        for (int a = 0; a < 3; ++a) ud[a] = u[nd[a]] - 4.0 * u_max * y[nd[a]] * (H - y[nd[a]]) / (H * H);
+        double gc[4] = {ud[0] * g.dNdx[0] + ud[1] * g.dNdx[1] + ud[2] * g.dNdx[2],
+                        ud[0] * g.dNdy[0] + ud[1] * g.dNdy[1] + ud[2] * g.dNdy[2],
+                        v[nd[0]] * g.dNdx[0] + v[nd[1]] * g.dNdx[1] + v[nd[2]] * g.dNdx[2],
+                        v[nd[0]] * g.dNdy[0] + v[nd[1]] * g.dNdy[1] + v[nd[2]] * g.dNdy[2]};
+        double w = g.area / 3.0;
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 4; ++c) grad_rec[(size_t)c * n + nd[a]] += w * gc[c];
+    }
+}
+
+/* k_compute_amr_error_indicator (src/cfa/fem_kernels.cuh:995-1035) */
+void or_amr_error_indicator(int n, int ne, const int* ev, const double* x, const double* y, const double* grad_rec,
+                            const double* mass, double* elem_error) {
+    for (int e = 0; e < ne; ++e) {
+        const int nd[3] = {ev[3 * e], ev[3 * e + 1], ev[3 * e + 2]};
+        double G[3][4];
+        for (int a = 0; a < 3; ++a) {
+            double inv_m = 1.0 / fmax(mass[nd[a]], 1.0e-14);
+            for (int c = 0; c < 4; ++c) G[a][c] = grad_rec[(size_t)c * n + nd[a]] * inv_m;
+        }
+        double x0 = x[nd[0]], y0 = y[nd[0]];
+        double area = 0.5 * fabs((x[nd[1]] - x0) * (y[nd[2]] - y0) - (x[nd[2]] - x0) * (y[nd[1]] - y0));
+        double omega = 0.0, eta_i = 0.0;
+        for (int a = 0; a < 3; ++a) {
+            omega = fmax(omega, fabs(G[a][2] - G[a][1]));
+            int b = (a + 1) % 3;
+            double ex = x[nd[b]] - x[nd[a]], ey = y[nd[b]] - y[nd[a]];
+            double eu = (G[b][0] - G[a][0]) * ex + (G[b][1] - G[a][1]) * ey;
+            double evv = (G[b][2] - G[a][2]) * ex + (G[b][3] - G[a][3]) * ey;
+            eta_i = fmax(eta_i, 0.125 * sqrt(eu * eu + evv * evv));
+        }
+        elem_error[e] = sqrt(2.0 * area) * omega;
+        elem_error[ne + e] = eta_i;
+    }
+}
+
 /* k_assemble_oss_operator + k_inverse_lumped_mass (src/cfa/fem_kernels.cuh:807-852),
  * assemble_oss_projection (src/cfa/device.cuh:304-314) */
 void or_assemble_oss(int n, int ne, const int* ev, const double* x, const double* y,

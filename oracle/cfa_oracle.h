@@ -57,6 +57,27 @@ void or_lumped_mass(int n, int ne, const int* elem_v, const double* x, const dou
 void or_spmv(int n, const int* rp, const int* ci, const double* val, const double* x, double* y);
 double or_dot(int n, const double* a, const double* b);
 
+/* after the solves (src/cfa/fem_kernels.cuh:536-637, :1046-1123); outputs accumulated */
+void or_stiffness_apply(int ne, const int* ev, const double* x, const double* y, const double* f, double c,
+                        double* out);
+void or_grad_dp_vorticity(int ne, const int* ev, const double* x, const double* y, const double* dp,
+                          const double* u, const double* v, double* gdx, double* gdy, double* vort_num);
+void or_velocity_pressure_correction(int n, const int* tag, int outlet_dirichlet, double dt, double rho,
+                                     double p_update, double rot_coeff, const double* div_num,
+                                     const double* mass, const double* gdx, const double* gdy,
+                                     const double* vort_num, const double* dp, double* u, double* v, double* p,
+                                     double* vort);
+void or_volume_forces(int ne, const int* ev, const int* tag, const double* x, const double* y, const double* u,
+                      const double* v, const double* u_old, const double* v_old, const double* u_prev,
+                      const double* v_prev, const double* p, double b0, double b1, double b2, double nu,
+                      double rho, double* out);
+
+/* AMR indicators (src/cfa/fem_kernels.cuh:911-1035); grad_rec accumulated */
+void or_recovered_gradient(int n, int ne, const int* ev, const double* x, const double* y, const double* u,
+                           const double* v, double u_max, double H, double* grad_rec);
+void or_amr_error_indicator(int n, int ne, const int* ev, const double* x, const double* y, const double* grad_rec,
+                            const double* mass, double* elem_error);
+
 typedef struct or_ilu or_ilu;
 or_ilu* or_ilu_create(int n, const int* rp, const int* ci);        /* NULL: row longer than 32 */
 int  or_ilu_colours(const or_ilu* h);

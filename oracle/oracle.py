@@ -165,6 +165,51 @@ def lumped_mass(mesh):
     return m
 
 
+def stiffness_apply(mesh, f, c, out):
+    """out += c (grad N_i, grad f) (k_stiffness_apply)."""
+    lib().or_stiffness_apply(mesh.ne, _p(mesh.elem_v), _p(f64(mesh.x)), _p(f64(mesh.y)), _p(f64(f)), C.c_double(c),
+                             _p(out))
+
+
+def grad_dp_vorticity(mesh, dp, u, v):
+    gdx, gdy, vn = np.zeros(mesh.n, _D), np.zeros(mesh.n, _D), np.zeros(mesh.n, _D)
+    lib().or_grad_dp_vorticity(mesh.ne, _p(mesh.elem_v), _p(f64(mesh.x)), _p(f64(mesh.y)), _p(f64(dp)), _p(f64(u)),
+                               _p(f64(v)), _p(gdx), _p(gdy), _p(vn))
+    return gdx, gdy, vn
+
+
+def velocity_pressure_correction(mesh, dt, rho, p_update, rot_coeff, div_num, mass, gdx, gdy, vort_num, dp, u, v, p,
+                                 outlet_dirichlet=0):
+    """u, v, p updated in place (float64 arrays); returns vort."""
+    vort = np.zeros(mesh.n, _D)
+    lib().or_velocity_pressure_correction(mesh.n, _p(i32(mesh.tag)), outlet_dirichlet, C.c_double(dt),
+                                          C.c_double(rho), C.c_double(p_update), C.c_double(rot_coeff),
+                                          _p(f64(div_num)), _p(f64(mass)), _p(f64(gdx)), _p(f64(gdy)),
+                                          _p(f64(vort_num)), _p(f64(dp)), _p(u), _p(v), _p(p), _p(vort))
+    return vort
+
+
+def volume_forces(mesh, u, v, u_old, v_old, u_prev, v_prev, p, b0, b1, b2, nu, rho):
+    out = np.zeros(2, _D)
+    lib().or_volume_forces(mesh.ne, _p(mesh.elem_v), _p(i32(mesh.tag)), _p(f64(mesh.x)), _p(f64(mesh.y)),
+                           _p(f64(u)), _p(f64(v)), _p(f64(u_old)), _p(f64(v_old)), _p(f64(u_prev)), _p(f64(v_prev)),
+                           _p(f64(p)), C.c_double(b0), C.c_double(b1), C.c_double(b2), C.c_double(nu),
+                           C.c_double(rho), _p(out))
+    return out
+
+
+def amr_indicators(mesh, u, v, u_max, H, mass):
+    """(grad_rec [4 n], elem_error [2 ne]) of k_accumulate_recovered_gradient and
+    k_compute_amr_error_indicator."""
+    g = np.zeros(4 * mesh.n, _D)
+    lib().or_recovered_gradient(mesh.n, mesh.ne, _p(mesh.elem_v), _p(f64(mesh.x)), _p(f64(mesh.y)), _p(f64(u)),
+                                _p(f64(v)), C.c_double(u_max), C.c_double(H), _p(g))
+    err = np.zeros(2 * mesh.ne, _D)
+    lib().or_amr_error_indicator(mesh.n, mesh.ne, _p(mesh.elem_v), _p(f64(mesh.x)), _p(f64(mesh.y)), _p(g),
+                                 _p(f64(mass)), _p(err))
+    return g, err
+
+
 def assemble_ppe(mesh, rp, ci, u, v, p, gpx, gpy, mass, elem_s, dt, rho, stab):
     Kp = np.zeros(rp[-1], _D)
     rhs, div = np.zeros(mesh.n, _D), np.zeros(mesh.n, _D)
@@ -343,3 +388,65 @@ def bicgstab2(rp, ci, val, bu, bv, xu0, xv0, ilu, max_iter=150, tol=1e-7):
     lib().or_bicgstab2(n, _p(i32(rp)), _p(i32(ci)), _p(f64(val)), _p(f64(bu)), _p(f64(bv)), _p(xu), _p(xv),
                        max_iter, C.c_double(tol), ilu.h, reps)
     return xu, xv, (reps[0], reps[1])
+
+
+class Stepper:
+    """The reference driver's time loop on a fixed mesh (src/cylinder_fem_amr.cu:276-520), CPU
+    restatement: the oracle of the device time stepper (same steps, same order, same options:
+    BDF2 after a backward Euler first step, rotational pressure update from the increment, OSS,
+    AMG rebuilt every ``amg_rebuild`` steps)."""
+
+    def __init__(self, mesh, u0, v0, p0, dt=1e-3, nu=1e-3, rho=1.0, tau_time=1e-3, stab=0.3, u_max=1.5, H=1.0,
+                 u_mean=1.0, diameter=0.2, tol_mom=1e-7, tol_p=1e-7, max_it_mom=150, max_it_p=4000,
+                 amg_rebuild=50, rotational=True, bdf2=True):
+        self.m = mesh
+        self.rp, self.ci = csr_build(mesh.n, mesh.elem_v)
+        self.u, self.v, self.p = f64(u0).copy(), f64(v0).copy(), f64(p0).copy()
+        self.u_old, self.v_old = self.u.copy(), self.v.copy()
+        self.u_prev, self.v_prev = self.u.copy(), self.v.copy()
+        self.dp = np.zeros(mesh.n)
+        self.dt, self.nu, self.rho, self.tau_time, self.stab = dt, nu, rho, tau_time, stab
+        self.u_max, self.H = u_max, H
+        self.force_scale = -2.0 / (u_mean * u_mean * diameter)
+        self.tol_mom, self.tol_p, self.max_it_mom, self.max_it_p = tol_mom, tol_p, max_it_mom, max_it_p
+        self.amg_rebuild, self.rotational, self.bdf2 = amg_rebuild, rotational, bdf2
+        self.ilu = Ilu(self.rp, self.ci)
+        self.amg, self.amg_built, self.step_no = None, None, 0
+        self.iters = []
+
+    def step(self):
+        m, rp, ci = self.m, self.rp, self.ci
+        self.step_no += 1
+        dt = self.dt
+        if self.bdf2 and self.step_no > 1:
+            dt_proj, a0, a1, a2, c1, c2 = (2.0 / 3.0) * dt, 1.5 / dt, 2.0 / dt, -0.5 / dt, 2.0, -1.0
+        else:
+            dt_proj, a0, a1, a2, c1, c2 = dt, 1.0 / dt, 1.0 / dt, 0.0, 1.0, 0.0
+        self.u_prev, self.v_prev = self.u_old.copy(), self.v_old.copy()
+        self.u_old, self.v_old = self.u.copy(), self.v.copy()
+        prm = MomParams(dt, self.nu, self.rho, a0, a1, a2, c1, c2, self.tau_time if self.tau_time > 0 else dt, 0.5)
+        A, ru, rv, mass = assemble_momentum(m, rp, ci, self.u_old, self.v_old, self.u_prev, self.v_prev, self.p, prm)
+        u, v = self.u_old.copy(), self.v_old.copy()
+        apply_bc_momentum(m, rp, ci, A, ru, rv, u, v, self.u_max, self.H)
+        self.ilu.factor(A)
+        u, v, (ru_rep, rv_rep) = bicgstab2(rp, ci, A, ru, rv, u, v, self.ilu, self.max_it_mom, self.tol_mom)
+        s = oss_weights(m, u, v, dt_proj, self.rho, self.nu, self.stab) if self.stab > 0 else np.zeros(m.ne)
+        gx, gy = scalar_gradient(m, self.p, s) if self.stab > 0 else (np.zeros(m.n), np.zeros(m.n))
+        Kp, rhs, div = assemble_ppe(m, rp, ci, u, v, self.p, gx, gy, mass, s, dt_proj, self.rho, self.stab)
+        apply_bc_pressure(m, rp, ci, Kp, rhs, self.dp, mass)
+        oss, inv_m = assemble_oss(m, rp, ci, s, mass) if self.stab > 0 else (None, None)
+        if self.amg_built is None or self.step_no - self.amg_built >= self.amg_rebuild:
+            self.amg = Amg(rp, ci, Kp)
+            self.amg_built = self.step_no
+        self.dp, prep = pcg(rp, ci, Kp, rhs, self.dp, self.max_it_p, self.tol_p, oss, inv_m, m.tag, self.amg)
+        self.iters.append((ru_rep.iterations, rv_rep.iterations, prep.iterations))
+        div_num = np.zeros(m.n)
+        stiffness_apply(m, self.dp, -dt_proj / self.rho, div_num)
+        gdx, gdy, vn = grad_dp_vorticity(m, self.dp, u, v)
+        rot = self.rho * self.nu if self.rotational else 0.0
+        self.vort = velocity_pressure_correction(m, dt_proj, self.rho, 1.0, rot, div_num, mass, gdx, gdy, vn, self.dp,
+                                                 u, v, self.p)
+        self.u, self.v = u, v
+        f = volume_forces(m, u, v, self.u_old, self.v_old, self.u_prev, self.v_prev, self.p, a0, -a1, -a2, self.nu,
+                          self.rho)
+        return self.force_scale * f[0], self.force_scale * f[1]

@@ -658,3 +658,86 @@ def test_step_live_reference_harness(ctx):
     assert all(conv) and all(st.report()["conv"])
     assert np.abs(host(st.u) - ru).max() < 1e-8 * np.abs(ru).max()
     assert np.abs(host(st.dp) - rdp).max() < 1e-7 * np.abs(rdp).max()
+
+
+# ------------------------------------------------------------------------------------------------
+# f1: after the solves (Steps C and D) and the time loop
+# ------------------------------------------------------------------------------------------------
+def test_post_solve_kernels_match_oracle(ctx):
+    m = mesh("medium")
+    dm = cfa.DeviceMesh(ctx, m)
+    u, v, p = fields(m)
+    rng = np.random.default_rng(5)
+    dp = rng.uniform(-1, 1, m.n)
+    mass = O.lumped_mass(m)
+    # stiffness (adds into out)
+    base = rng.uniform(-1, 1, m.n)
+    want = base.copy()
+    O.stiffness_apply(m, dp, -0.37, want)
+    got = dev(base)
+    cfa.stiffness_apply(ctx, dm, dev(dp), -0.37, got)
+    assert np.abs(host(got) - want).max() <= 1e-12 * np.abs(want).max()
+    # grad dp and vorticity numerators
+    gdx, gdy, vn = O.grad_dp_vorticity(m, dp, u, v)
+    dgx, dgy, dvn = (torch.zeros(m.n, dtype=torch.float64, device="cuda") for _ in range(3))
+    cfa.grad_dp_vorticity(ctx, dm, dev(dp), dev(u), dev(v), dgx, dgy, dvn)
+    for g, w in ((dgx, gdx), (dgy, gdy), (dvn, vn)):
+        assert np.abs(host(g) - w).max() <= 1e-12 * np.abs(w).max()
+    # correction
+    div_num = rng.uniform(-1, 1, m.n) * mass
+    uo, vo, po = u.copy(), v.copy(), p.copy()
+    vort = O.velocity_pressure_correction(m, 2e-3 / 3, 1.0, 1.0, 1e-3, div_num, mass, gdx, gdy, vn, dp, uo, vo, po)
+    du, dv, dpp, dvort = dev(u), dev(v), dev(p), torch.zeros(m.n, dtype=torch.float64, device="cuda")
+    cfa.velocity_pressure_correction(ctx, dm, 2e-3 / 3, 1.0, 1.0, 1e-3, dev(div_num), dev(mass), dev(gdx), dev(gdy),
+                                     dev(vn), dev(dp), du, dv, dpp, dvort)
+    for g, w in ((du, uo), (dv, vo), (dpp, po), (dvort, vort)):
+        assert np.abs(host(g) - w).max() <= 1e-13 * np.abs(w).max()
+    # the fused Step C
+    div2 = np.zeros(m.n)
+    O.stiffness_apply(m, dp, -(2e-3 / 3), div2)
+    u2, v2, p2 = u.copy(), v.copy(), p.copy()
+    vort2 = O.velocity_pressure_correction(m, 2e-3 / 3, 1.0, 1.0, 1e-3, div2, mass, gdx, gdy, vn, dp, u2, v2, p2)
+    du, dv, dpp = dev(u), dev(v), dev(p)
+    bufs = [torch.zeros(m.n, dtype=torch.float64, device="cuda") for _ in range(5)]
+    cfa.project_step(ctx, dm, 2e-3 / 3, 1.0, 1e-3, True, dev(mass), dev(dp), *bufs[:4], du, dv, dpp, bufs[4])
+    for g, w in ((du, u2), (dv, v2), (dpp, p2), (bufs[4], vort2)):
+        assert np.abs(host(g) - w).max() <= 1e-12 * np.abs(w).max()
+    # volume forces
+    up, vp = 0.9 * u, 0.8 * v
+    want = O.volume_forces(m, u, v, 0.95 * u, 0.9 * v, up, vp, p, 1.5e3, -2e3, 0.5e3, 1e-3, 1.0)
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    cfa.volume_forces(ctx, dm, dev(u), dev(v), dev(0.95 * u), dev(0.9 * v), dev(up), dev(vp), dev(p), 1.5e3, -2e3,
+                      0.5e3, 1e-3, 1.0, out)
+    assert np.abs(host(out) - want).max() <= 1e-12 * np.abs(want).max()
+
+
+def test_amr_indicators_match_oracle(ctx):
+    m = mesh("medium")
+    dm = cfa.DeviceMesh(ctx, m)
+    u, v, _ = fields(m)
+    mass = O.lumped_mass(m)
+    g, err = O.amr_indicators(m, u, v, 1.5, 1.0, mass)
+    dg = torch.zeros(4 * m.n, dtype=torch.float64, device="cuda")
+    de = torch.zeros(2 * m.ne, dtype=torch.float64, device="cuda")
+    cfa.amr_indicators(ctx, dm, dev(u), dev(v), 1.5, 1.0, dev(mass), dg, de)
+    assert np.abs(host(dg) - g).max() <= 1e-12 * np.abs(g).max()
+    assert np.abs(host(de) - err).max() <= 1e-11 * np.abs(err).max()
+
+
+@pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
+def test_time_stepper_matches_oracle(ctx, precision):
+    """The device time loop against the oracle's (same steps and options) over 12 BDF2 steps from
+    rest, solves at 1e-12: drag and lift histories within 1e-9 of the drag scale."""
+    import step as S
+    m = mesh("small")
+    z = np.zeros(m.n)
+    kw = dict(dt=5e-3, tol_mom=1e-12, tol_p=1e-12, max_it_mom=400, amg_rebuild=5)
+    ref = O.Stepper(m, z, z, z, **kw)
+    st = S.TimeStepper(m, z, z, z, precision=precision, ctx=ctx, **kw)
+    for k in range(12):
+        want = ref.step()
+        got = st.step()
+        scale = max(1.0, abs(want[0]))
+        assert abs(got[0] - want[0]) <= 1e-9 * scale and abs(got[1] - want[1]) <= 1e-9 * scale, (k, got, want)
+    assert np.abs(host(st.u) - ref.u).max() <= 1e-9 * np.abs(ref.u).max()
+    assert np.abs(host(st.p) - ref.p).max() <= 1e-9 * np.abs(ref.p).max()

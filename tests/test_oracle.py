@@ -186,6 +186,53 @@ def test_amg_remap_restated():
     assert small.remaps == 0
 
 
+def test_post_solve_known_answers():
+    """The kernels after the solves on exact cases: K f = 0 on interior rows for a linear f
+    (k_stiffness_apply), the lumped gradient of a linear dp is its slope on interior nodes and
+    the vorticity of a linear shear is constant (k_accumulate_grad_dp_and_vorticity), and the
+    volume forces of the fluid at rest are zero (test_force_at_rest, tests/test_cfa.cu:171-185)."""
+    m = F.make_mesh("small")
+    inner = m.tag == 0
+    f = 0.7 * m.x - 1.3 * m.y + 0.2
+    out = np.zeros(m.n)
+    O.stiffness_apply(m, f, 1.0, out)
+    assert np.abs(out[inner]).max() < 1e-12 * np.abs(f).max()
+    mass = O.lumped_mass(m)
+    u, v = 0.5 * m.y, -0.25 * m.x
+    gdx, gdy, vn = O.grad_dp_vorticity(m, f, u, v)
+    assert np.abs(gdx[inner] / mass[inner] - 0.7).max() < 1e-12
+    assert np.abs(gdy[inner] / mass[inner] + 1.3).max() < 1e-12
+    assert np.abs(vn / mass - (-0.25 - 0.5)).max() < 1e-12
+    z = np.zeros(m.n)
+    assert np.abs(O.volume_forces(m, z, z, z, z, z, z, z, 1.5e3, -2e3, 0.5e3, 1e-3, 1.0)).max() == 0.0
+
+
+def test_amr_indicators_vanish_for_channel_flow():
+    """k_accumulate_recovered_gradient + k_compute_amr_error_indicator: the undisturbed inflow
+    profile gives exactly zero (the reference's design statement, fem_kernels.cuh:911-918), a
+    disturbed field does not."""
+    m = F.make_mesh("small")
+    mass = O.lumped_mass(m)
+    up = 4 * 1.5 * m.y * (1 - m.y)
+    g, err = O.amr_indicators(m, up, np.zeros(m.n), 1.5, 1.0, mass)
+    assert np.abs(err).max() == 0.0 and np.abs(g).max() == 0.0
+    g, err = O.amr_indicators(m, up + 0.01 * F.fourier_field(m.x, m.y, 4), np.zeros(m.n), 1.5, 1.0, mass)
+    assert err[:m.ne].max() > 0 and err[m.ne:].max() > 0
+
+
+def test_oracle_stepper_reaches_a_steady_drag():
+    """The CPU time loop (the oracle of the device stepper) from rest: the solves converge every
+    step and the drag settles; the lift stays small by symmetry of the inflow."""
+    m = F.make_mesh("small")
+    z = np.zeros(m.n)
+    st = O.Stepper(m, z, z, z, dt=5e-3)
+    hist = [st.step() for _ in range(12)]
+    cd = np.array([h[0] for h in hist])
+    assert all(it[2] > 0 for it in st.iters)
+    assert abs(cd[-1] - cd[-2]) < 0.05 * abs(cd[-1]) and 0.5 < cd[-1] < 5.0
+    assert abs(hist[-1][1]) < 0.05
+
+
 def test_pcg_oss_amg_step():
     """The pressure solve of a synthetic step: PCG + OSS + AMG reaches 1e-10 with far fewer
     iterations than Jacobi, and both agree."""
