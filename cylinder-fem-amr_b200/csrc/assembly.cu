@@ -55,9 +55,9 @@ k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x,
                 const int* __restrict__ pos, const int* __restrict__ rp, const int* __restrict__ ci,
                 const double* __restrict__ u_old, const double* __restrict__ v_old,
                 const double* __restrict__ u_prev, const double* __restrict__ v_prev,
-                const double* __restrict__ p_old, MomParams P, int with_bc, double u_max, double H, OutletBc bc,
-                double* __restrict__ A_val, double* __restrict__ rhs_u, double* __restrict__ rhs_v,
-                double* __restrict__ mass) {
+                const double* __restrict__ p_old, const double* __restrict__ nu_node, MomParams P, int with_bc,
+                double u_max, double H, OutletBc bc, double* __restrict__ A_val, double* __restrict__ rhs_u,
+                double* __restrict__ rhs_v, double* __restrict__ mass) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int r0 = rp[i], len = rp[i + 1] - r0;
@@ -95,9 +95,11 @@ k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x,
         }
         const double vel_mag = sqrt(w_u * w_u + w_v * w_v) + 1.0e-12;
         const double h_K = sqrt(2.0 * area);
+        // element viscosity: the scalar nu, or the mean of a nodal field
+        const double nu = nu_node ? (nu_node[nd[0]] + nu_node[nd[1]] + nu_node[nd[2]]) / 3.0 : P.nu;
         const double term_t = 2.0 / P.tau_time;
         const double term_c = 2.0 * vel_mag / h_K;
-        const double term_d = 4.0 * P.nu / (h_K * h_K);
+        const double term_d = 4.0 * nu / (h_K * h_K);
         const double tau_supg = 1.0 / sqrt(term_t * term_t + term_c * term_c + 9.0 * term_d * term_d);
         const double p0 = p_old[nd[0]], p1 = p_old[nd[1]], p2 = p_old[nd[2]];
         const double dpdx = (p0 * g.dNdx[0] + p1 * g.dNdx[1] + p2 * g.dNdx[2]) / P.rho;
@@ -113,7 +115,7 @@ k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x,
             const double C_ij = (area / 3.0) * ugN[j] + P.skew_coef * div_w * M_ij;
             const double S_ij = area * tau_supg * ugN[a] * ugN[j];
             const double Ms_ij = (area / 3.0) * tau_supg * ugN[a];
-            const double A_ij = P.a0 * (M_ij + Ms_ij) + P.nu * K_ij + C_ij + S_ij;
+            const double A_ij = P.a0 * (M_ij + Ms_ij) + nu * K_ij + C_ij + S_ij;
             const int p = pos[3 * s + j];
             if (local) acc[p - r0] += A_ij; else A_val[p] += A_ij;
             f_u += (M_ij + Ms_ij) * u_h[j];
@@ -365,18 +367,33 @@ using namespace cfa;
 
 extern "C" {
 
+cfa_status cfa_assemble_momentum_nu(cfa_ctx* ctx, const cfa_mesh* m, const double* u_old, const double* v_old,
+                                    const double* u_prev, const double* v_prev, const double* p_old,
+                                    const cfa_momentum_params* prm, const double* nu_node,
+                                    const cfa_momentum_bc* bcp, double* A_val, double* rhs_u, double* rhs_v,
+                                    double* mass, double* u, double* v);
+
 cfa_status cfa_assemble_momentum(cfa_ctx* ctx, const cfa_mesh* m, const double* u_old, const double* v_old,
                                  const double* u_prev, const double* v_prev, const double* p_old,
                                  const cfa_momentum_params* prm, const cfa_momentum_bc* bcp, double* A_val,
                                  double* rhs_u, double* rhs_v, double* mass, double* u, double* v) {
+    return cfa_assemble_momentum_nu(ctx, m, u_old, v_old, u_prev, v_prev, p_old, prm, nullptr, bcp, A_val, rhs_u,
+                                    rhs_v, mass, u, v);
+}
+
+cfa_status cfa_assemble_momentum_nu(cfa_ctx* ctx, const cfa_mesh* m, const double* u_old, const double* v_old,
+                                    const double* u_prev, const double* v_prev, const double* p_old,
+                                    const cfa_momentum_params* prm, const double* nu_node,
+                                    const cfa_momentum_bc* bcp, double* A_val, double* rhs_u, double* rhs_v,
+                                    double* mass, double* u, double* v) {
     if (!ctx) return CFA_BAD_ARG;
     CFA_ARG(m && u_old && v_old && u_prev && v_prev && p_old && prm && A_val && rhs_u && rhs_v && mass);
     CFA_ARG(!bcp || (u && v));
     MomParams P{prm->dt, prm->nu, prm->rho, prm->a0, prm->a1, prm->a2, prm->c1, prm->c2, prm->tau_time, prm->skew_coef};
     const double u_max = bcp ? bcp->u_max : 0.0, H = bcp ? bcp->H : 1.0;
     CFA_LAUNCH(ctx, k_momentum_rows, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y, m->tag,
-               m->inc_ptr.p, m->inc.p, m->pos.p, m->rp, m->ci, u_old, v_old, u_prev, v_prev, p_old, P, bcp ? 1 : 0,
-               u_max, H, m->bc, A_val, rhs_u, rhs_v, mass);
+               m->inc_ptr.p, m->inc.p, m->pos.p, m->rp, m->ci, u_old, v_old, u_prev, v_prev, p_old, nu_node, P,
+               bcp ? 1 : 0, u_max, H, m->bc, A_val, rhs_u, rhs_v, mass);
     if (bcp)   // solution values on Dirichlet nodes after the rows (u may alias u_old)
         CFA_LAUNCH(ctx, k_momentum_bc, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->tag, m->y, m->rp, m->ci,
                    u_max, H, m->bc, 0, A_val, rhs_u, rhs_v, u, v);

@@ -156,6 +156,49 @@ static void sweeps(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv, con
     }
 }
 
+// Position of the mirrored entry (j, i) of every CSR entry (i, j) (binary search in row j);
+// err set when the pattern is not structurally symmetric.
+__global__ void k_mirror_positions(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                   int* __restrict__ tpos, int* __restrict__ err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int a = rp[i]; a < rp[i + 1]; ++a) {
+        const int j = ci[a];
+        int lo = rp[j], hi = rp[j + 1] - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (ci[mid] < i) lo = mid + 1;
+            else hi = mid;
+        }
+        if (lo < rp[j + 1] && ci[lo] == i) tpos[a] = lo;
+        else { tpos[a] = a; atomicExch(err, 1); }
+    }
+}
+
+// The split factor of (LU)^T = (U^T D^-1)(D L^T) in the same colour order (rows in colour c only
+// depend on colours < c in both triangles): unit lower L'_ij = U_ji / U_jj, upper
+// U'_ij = U_ii L_ji, the same diagonal (src/cfa/linalg.cuh:531-541 factor, transposed).
+template <class T>
+__global__ void k_ilu_gather_transposed(int n, const int* __restrict__ rows, const int* __restrict__ lp,
+                                        const int* __restrict__ up, const int* __restrict__ lc,
+                                        const int* __restrict__ l_src, const int* __restrict__ u_src,
+                                        const int* __restrict__ d_src, const int* __restrict__ diag,
+                                        const int* __restrict__ tpos, const double* __restrict__ lu,
+                                        T* __restrict__ lv, T* __restrict__ uv, T* __restrict__ dinv) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const double d = lu[d_src[t]];
+    for (int e = lp[t]; e < lp[t + 1]; ++e) lv[e] = (T)(lu[tpos[l_src[e]]] / lu[diag[lc[e]]]);
+    for (int e = up[t]; e < up[t + 1]; ++e) uv[e] = (T)(d * lu[tpos[u_src[e]]]);
+    dinv[t] = (T)(1.0 / d);
+}
+
+__global__ void k_transpose_values(int nnz, const int* __restrict__ tpos, const double* __restrict__ val,
+                                   double* __restrict__ out) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < nnz) out[a] = val[tpos[a]];
+}
+
 cfa_status ilu_apply(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z, int nrhs, const int* done) {
     if (h->precision == CFA_MIXED) {
         // FP32 factors, FP64 vectors and arithmetic, in place in z
@@ -318,6 +361,59 @@ cfa_status cfa_ilu_factor(cfa_ctx* ctx, cfa_ilu* h, const double* val) {
     else
         CFA_LAUNCH(ctx, k_ilu_gather<double>, ceil_div(len, kThreads), kThreads, 0, h->nl, h->nu, h->n, h->l_src.p,
                    h->u_src.p, h->d_src.p, h->lu.p, h->lv64.p, h->uv64.p, h->dinv64.p);
+    CFA_CHECK_LAUNCH();
+    h->transposed = false;
+    return CFA_OK;
+}
+
+}  // extern "C"
+
+namespace cfa {
+// Mirror positions of the handle's pattern, computed once (synchronises the first time).
+static cfa_status ensure_mirror(cfa_ctx* ctx, cfa_ilu* h) {
+    if (h->tpos.p) return CFA_OK;
+    CFA_CUDA(h->tpos.ensure(std::max(h->nnz, 1)));
+    DevBuf<int> err;
+    CFA_CUDA(err.ensure(1));
+    CFA_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
+    CFA_LAUNCH(ctx, k_mirror_positions, ceil_div(h->n, kThreads), kThreads, 0, h->n, h->rp, h->ci, h->tpos.p, err.p);
+    int herr = 0;
+    CFA_CUDA(cudaMemcpyAsync(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (herr) {
+        h->tpos.release();
+        return set_error(ctx, CFA_BAD_ARG, "pattern not structurally symmetric", __FILE__, __LINE__);
+    }
+    return CFA_OK;
+}
+}  // namespace cfa
+
+extern "C" {
+
+cfa_status cfa_ilu_factor_transposed(cfa_ctx* ctx, cfa_ilu* h, const double* val) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(h && val);
+    CFA_PROPAGATE(ensure_mirror(ctx, h));
+    CFA_PROPAGATE(cfa_ilu_factor(ctx, h, val));
+    if (h->precision == CFA_MIXED)
+        CFA_LAUNCH(ctx, k_ilu_gather_transposed<float>, ceil_div(h->n, kThreads), kThreads, 0, h->n, h->rows.p,
+                   h->lp.p, h->up.p, h->lc.p, h->l_src.p, h->u_src.p, h->d_src.p, h->diag.p, h->tpos.p, h->lu.p,
+                   h->lv32.p, h->uv32.p, h->dinv32.p);
+    else
+        CFA_LAUNCH(ctx, k_ilu_gather_transposed<double>, ceil_div(h->n, kThreads), kThreads, 0, h->n, h->rows.p,
+                   h->lp.p, h->up.p, h->lc.p, h->l_src.p, h->u_src.p, h->d_src.p, h->diag.p, h->tpos.p, h->lu.p,
+                   h->lv64.p, h->uv64.p, h->dinv64.p);
+    CFA_CHECK_LAUNCH();
+    h->transposed = true;
+    return CFA_OK;
+}
+
+cfa_status cfa_csr_transpose_values(cfa_ctx* ctx, cfa_ilu* h, const double* val, double* val_t) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(h && val && val_t && val != val_t);
+    CFA_PROPAGATE(ensure_mirror(ctx, h));
+    CFA_LAUNCH(ctx, k_transpose_values, ceil_div(h->nnz, kThreads), kThreads, 0, h->nnz, (const int*)h->tpos.p, val,
+               val_t);
     CFA_CHECK_LAUNCH();
     return CFA_OK;
 }

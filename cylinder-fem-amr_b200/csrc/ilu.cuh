@@ -24,6 +24,8 @@ struct cfa_ilu {
     cfa::DevBuf<int4> elim;           // {q, dk, ub, 0}
     cfa::DevBuf<int2> upd;            // {b, m}
     int n_elim = 0, n_upd = 0;
+    cfa::DevBuf<int> tpos;            // CSR position of the mirrored entry (j, i) of every (i, j)
+    bool transposed = false;          // the split factor holds (LU)^T (cfa_ilu_factor_transposed)
 };
 
 namespace cfa {

@@ -219,54 +219,73 @@ __global__ void k_ring2_fill(int n, const int* __restrict__ rp, const int* __res
     for (int q = 0; q < len; ++q) ci2[rp2[i] + q] = buf[q];
 }
 
-// Values of the fused operator, written straight into the value section of its tiles. One warp
-// per row, one lane per entry (i, j) of the two-ring row: the entry is K_ij minus the sum over
-// k in N(i) with j in N(k), k ascending, of BTx_ik m_k^-1 Bx_kj + BTy_ik m_k^-1 By_kj. The rows of
-// the neighbours k are read by every lane at once (broadcast); no atomics, a fixed order.
+// Position of column j in the sorted row [f0, f1) of ci, or -1.
+__device__ __forceinline__ int find_in_row(const int* __restrict__ ci, int f0, int f1, int j) {
+    int lo = f0, hi = f1 - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (ci[mid] < j) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < f1 && ci[lo] == j) ? lo : -1;
+}
+
+// Symbolic plan of the fused values, one thread per two-ring entry s = (i, j): its row, the
+// position of j in K's row i (or -1) and, in pass 2, the pairs (a, f) of the products
+// BT_ik m_k^-1 B_kj that reach it: a = (i, k) in K's pattern, f = (k, j), k ascending.
+__global__ void k_ring2_slots(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                              const int* __restrict__ rp2, const int* __restrict__ ci2, int* __restrict__ slot_row,
+                              int* __restrict__ kpos, int* __restrict__ cnt, const int* __restrict__ pair_ptr,
+                              int* __restrict__ pa, int* __restrict__ pf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int s = rp2[i]; s < rp2[i + 1]; ++s) {
+        const int j = ci2[s];
+        int c = pair_ptr ? pair_ptr[s] : 0;
+        if (!pair_ptr) {
+            slot_row[s] = i;
+            kpos[s] = find_in_row(ci, rp[i], rp[i + 1], j);
+        }
+        for (int a = rp[i]; a < rp[i + 1]; ++a) {
+            const int k = ci[a];
+            const int f = find_in_row(ci, rp[k], rp[k + 1], j);
+            if (f < 0) continue;
+            if (pair_ptr) { pa[c] = a; pf[c] = f; }
+            ++c;
+        }
+        if (!pair_ptr) cnt[s] = c;
+    }
+}
+
+// Values of the fused operator, one thread per two-ring entry (i, j), written straight into the
+// value section of its tile: K_ij minus, over its pairs in order (k ascending),
+// BTx_ik m_k^-1 Bx_kj + BTy_ik m_k^-1 By_kj; Dirichlet rows keep K only.
 __global__ void __launch_bounds__(kThreads)
-k_oss_fuse(int n, int nnz, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ K,
+k_oss_fuse(long long nnz2, int n, int nnz, const int* __restrict__ ci, const double* __restrict__ K,
            const double* __restrict__ oss, const int* __restrict__ tag, OutletBc bc, const double* __restrict__ inv_m,
-           const int* __restrict__ rp2, const int* __restrict__ ci2, TileView tv, unsigned char* __restrict__ data) {
-    const int lane = threadIdx.x & 31;
-    const int nw = gridDim.x * blockDim.x / 32;
+           const int* __restrict__ rp2, const int* __restrict__ slot_row, const int* __restrict__ kpos,
+           const int* __restrict__ pair_ptr, const int* __restrict__ pa, const int* __restrict__ pf, TileView tv,
+           unsigned char* __restrict__ data) {
     const double* Bx = oss;
     const double* By = oss + nnz;
     const double* BTx = oss + 2 * (size_t)nnz;
     const double* BTy = oss + 3 * (size_t)nnz;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < n; i += nw) {
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nnz2;
+         s += (long long)gridDim.x * blockDim.x) {
+        const int i = slot_row[s];
+        const int kp = kpos[s];
+        double acc = kp >= 0 ? K[kp] : 0.0;
+        if (!pressure_dirichlet(i, tag[i], bc))
+            for (int q = pair_ptr[s]; q < pair_ptr[s + 1]; ++q) {
+                const int a = pa[q], f = pf[q];
+                const double im = inv_m[ci[a]];
+                acc -= (BTx[a] * im) * Bx[f] + (BTy[a] * im) * By[f];
+            }
         const int t = i / tv.tile_rows;
         const int r0 = t * tv.tile_rows;
         const int nr = min(tv.tile_rows, n - r0);
         const int e0 = rp2[r0], ne = rp2[r0 + nr] - e0;
-        double* dst = reinterpret_cast<double*>(data + tv.off[t] + tile_val_off(nr, ne, 8, 0)) + (rp2[i] - e0);
-        const int b2 = rp2[i], len = rp2[i + 1] - b2;
-        const bool oss_row = !pressure_dirichlet(i, tag[i], bc);
-        const int a0 = rp[i], a1 = rp[i + 1];
-        for (int q = lane; q - lane < len; q += 32) {
-            const bool on = q < len;
-            const int j = on ? ci2[b2 + q] : -1;
-            double acc = 0.0;
-            // K_ij (j in N(i))
-            for (int a = a0; a < a1; ++a)
-                if (ci[a] == j) acc = K[a];
-            if (oss_row)
-                for (int a = a0; a < a1; ++a) {
-                    const int k = ci[a];
-                    const int f0 = rp[k], f1 = rp[k + 1];
-                    // j in row k (sorted): binary search
-                    int lo = f0, hi = f1 - 1;
-                    while (lo < hi) {
-                        const int mid = (lo + hi) >> 1;
-                        if (ci[mid] < j) lo = mid + 1;
-                        else hi = mid;
-                    }
-                    if (on && lo < f1 && ci[lo] == j) {
-                        const double im = inv_m[k];
-                        acc -= (BTx[a] * im) * Bx[lo] + (BTy[a] * im) * By[lo];
-                    }
-                }
-            if (on) dst[q] = acc;
-        }
+        reinterpret_cast<double*>(data + tv.off[t] + tile_val_off(nr, ne, 8, 0))[s - e0] = acc;
     }
 }
 
@@ -1020,6 +1039,7 @@ struct PcgWork {
     TiledCsr tb, tk;
     bool fused = false;
     DevBuf<int> rp2, ci2, cnt2;       // two-ring pattern of the fused OSS operator
+    DevBuf<int> slot_row, kpos, pair_ptr, pa, pf;   // its per-entry plan (k_ring2_slots)
     DevBuf<unsigned char> scan_tmp;
     std::vector<const void*> tile_key;
     std::vector<const void*> prepared;   // operator whose values the tiles hold (standalone apply)
@@ -1210,9 +1230,11 @@ static cfa_status pcg_operator(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, const
 static cfa_status pack_operator(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a) {
     if (a.oss && W.fused) {
         const cfa_mesh* m = a.oss->mesh;
-        CFA_LAUNCH(ctx, k_oss_fuse, row_grid(ctx, a.n, 32), kThreads, 0, a.n, a.nnz, a.rp, a.ci, a.val,
-                   a.oss->d_oss_val, m->tag, m->bc, a.oss->d_inv_m, (const int*)W.rp2.p, (const int*)W.ci2.p,
-                   W.tk.view(W.err.p), W.tk.data.p);
+        const long long nnz2 = W.tk.nnz;
+        CFA_LAUNCH(ctx, k_oss_fuse, (int)std::min<long long>((nnz2 + kThreads - 1) / kThreads, 16LL * ctx->num_sms),
+                   kThreads, 0, nnz2, a.n, a.nnz, a.ci, a.val, a.oss->d_oss_val, m->tag, m->bc, a.oss->d_inv_m,
+                   (const int*)W.rp2.p, (const int*)W.slot_row.p, (const int*)W.kpos.p, (const int*)W.pair_ptr.p,
+                   (const int*)W.pa.p, (const int*)W.pf.p, W.tk.view(W.err.p), W.tk.data.p);
     } else if (a.oss) {
         const double* o = a.oss->d_oss_val;
         const size_t nz = (size_t)a.nnz;
@@ -1337,8 +1359,30 @@ static cfa_status plan_ring2(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, bool& o
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     CFA_CUDA(cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream));
     if (h[0]) return CFA_OK;
-    CFA_CUDA(W.ci2.ensure(std::max(h[1], 1)));
+    const int nnz2 = h[1];
+    CFA_CUDA(W.ci2.ensure(std::max(nnz2, 1)));
     CFA_LAUNCH(ctx, k_ring2_fill, ceil_div(n, kThreads), kThreads, 0, n, a.rp, a.ci, (const int*)W.rp2.p, W.ci2.p);
+    // per-entry plan: row, K position, pair counts, then the pairs
+    CFA_CUDA(W.slot_row.ensure(std::max(nnz2, 1)));
+    CFA_CUDA(W.kpos.ensure(std::max(nnz2, 1)));
+    CFA_CUDA(W.cnt2.ensure(nnz2 + 1));
+    CFA_CUDA(W.pair_ptr.ensure(nnz2 + 1));
+    CFA_CUDA(cudaMemsetAsync(W.cnt2.p + nnz2, 0, sizeof(int), ctx->stream));
+    CFA_LAUNCH(ctx, k_ring2_slots, ceil_div(n, kThreads), kThreads, 0, n, a.rp, a.ci, (const int*)W.rp2.p,
+               (const int*)W.ci2.p, W.slot_row.p, W.kpos.p, W.cnt2.p, (const int*)nullptr, (int*)nullptr,
+               (int*)nullptr);
+    tmp = 0;
+    CFA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, W.cnt2.p, W.pair_ptr.p, nnz2 + 1, ctx->stream));
+    CFA_CUDA(W.scan_tmp.ensure(tmp + 16));
+    CFA_CUDA(cub::DeviceScan::ExclusiveSum(W.scan_tmp.p, tmp, W.cnt2.p, W.pair_ptr.p, nnz2 + 1, ctx->stream));
+    int npairs = 0;
+    CFA_CUDA(cudaMemcpyAsync(&npairs, W.pair_ptr.p + nnz2, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    CFA_CUDA(W.pa.ensure(std::max(npairs, 1)));
+    CFA_CUDA(W.pf.ensure(std::max(npairs, 1)));
+    CFA_LAUNCH(ctx, k_ring2_slots, ceil_div(n, kThreads), kThreads, 0, n, a.rp, a.ci, (const int*)W.rp2.p,
+               (const int*)W.ci2.p, (int*)nullptr, (int*)nullptr, (int*)nullptr, (const int*)W.pair_ptr.p, W.pa.p,
+               W.pf.p);
     CFA_CHECK_LAUNCH();
     ok = true;
     return CFA_OK;

@@ -108,6 +108,29 @@ cfa_status cfa_assemble_momentum(cfa_ctx* ctx, const cfa_mesh* mesh, const doubl
                                  const double* d_p_old, const cfa_momentum_params* prm,
                                  const cfa_momentum_bc* bc, double* d_A_val, double* d_rhs_u,
                                  double* d_rhs_v, double* d_mass_lumped, double* d_u, double* d_v);
+/* cfa_assemble_momentum with a per-node viscosity field (d_nu_node, n values; the element uses
+ * their mean). The reference has a scalar nu; with d_nu_node NULL this is cfa_assemble_momentum. */
+cfa_status cfa_assemble_momentum_nu(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_u_old,
+                                    const double* d_v_old, const double* d_u_prev, const double* d_v_prev,
+                                    const double* d_p_old, const cfa_momentum_params* prm,
+                                    const double* d_nu_node, const cfa_momentum_bc* bc, double* d_A_val,
+                                    double* d_rhs_u, double* d_rhs_v, double* d_mass_lumped, double* d_u,
+                                    double* d_v);
+/* Adjoint of the momentum predictor (no counterpart in the reference). With x = (u*, v*) the
+ * solution of the system cfa_assemble_momentum_nu built (bc required) and lambda the solution of
+ * A^T lambda_c = dJ/dx_c (cfa_ilu_factor_transposed + cfa_csr_transpose_values +
+ * cfa_bicgstab2_solve), writes dJ/dtheta = sum_c lambda_c^T (db_c/dtheta - dA/dtheta x_c) for
+ * the nodal inputs u_old, v_old, u_prev, v_prev, p_old and, when d_nu_node is given, the nodal
+ * viscosity (each n values, overwritten); d_scalars2[0] = dJ/du_max (the inflow amplitude),
+ * d_scalars2[1] = dJ/dnu for the scalar viscosity. The element derivatives are exact (forward-mode
+ * dual numbers through the element assembly). Synchronises. */
+cfa_status cfa_momentum_adjoint(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_u_old, const double* d_v_old,
+                                const double* d_u_prev, const double* d_v_prev, const double* d_p_old,
+                                const cfa_momentum_params* prm, const double* d_nu_node,
+                                const cfa_momentum_bc* bc, const double* d_x_u, const double* d_x_v,
+                                const double* d_lambda_u, const double* d_lambda_v, double* d_g_u_old,
+                                double* d_g_v_old, double* d_g_u_prev, double* d_g_v_prev, double* d_g_p_old,
+                                double* d_g_nu_node, double* d_scalars2);
 /* k_apply_bc_momentum (src/cfa/fem_kernels.cuh:411-453) alone. */
 cfa_status cfa_apply_bc_momentum(cfa_ctx* ctx, const cfa_mesh* mesh, const cfa_momentum_bc* bc,
                                  double* d_A_val, double* d_rhs_u, double* d_rhs_v, double* d_u,
@@ -242,6 +265,14 @@ cfa_status cfa_ilu_destroy(cfa_ilu* ilu);
 cfa_status cfa_ilu_factor(cfa_ctx* ctx, cfa_ilu* ilu, const double* d_val);
 /* apply (:544-555): z = (LU)^-1 r for nrhs vectors of stride n. */
 cfa_status cfa_ilu_apply(cfa_ctx* ctx, const cfa_ilu* ilu, const double* d_r, double* d_z, int nrhs);
+/* Adjoint support (no counterpart in the reference): factors d_val as cfa_ilu_factor does and
+ * keeps (LU)^T in the handle, so that cfa_ilu_apply gives z = (LU)^-T r and the handle
+ * preconditions A^T (in the same colour order: (LU)^T = (U^T D^-1)(D L^T)). Needs a structurally
+ * symmetric pattern (CFA_BAD_ARG otherwise; synchronises the first time). cfa_ilu_factor
+ * switches the handle back. */
+cfa_status cfa_ilu_factor_transposed(cfa_ctx* ctx, cfa_ilu* ilu, const double* d_val);
+/* d_val_t = the values of A^T on the same (structurally symmetric) pattern as the handle's. */
+cfa_status cfa_csr_transpose_values(cfa_ctx* ctx, cfa_ilu* ilu, const double* d_val, double* d_val_t);
 /* n_colours and colour_start (host, n_colours + 1 entries, may be NULL). */
 cfa_status cfa_ilu_colours(const cfa_ilu* ilu, int* n_colours, int* colour_start);
 /* Device arrays of the handle (public members d_colour, d_rows, d_lu of the reference class):
