@@ -194,11 +194,32 @@ class DeviceMesh:
 # assembly
 # ---------------------------------------------------------------------------------------------
 def assemble_momentum(ctx, m: DeviceMesh, u_old, v_old, u_prev, v_prev, p_old, prm, A_val, rhs_u, rhs_v, mass,
-                      u=None, v=None, u_max=None, H=1.0):
+                      u=None, v=None, u_max=None, H=1.0, nu_node=None):
     bc = MomentumBc(u_max, H) if u_max is not None else None
-    ctx.check(lib().cfa_assemble_momentum(ctx.h, m.h, ptr(u_old), ptr(v_old), ptr(u_prev), ptr(v_prev), ptr(p_old),
-                                          C.byref(prm), C.byref(bc) if bc is not None else None, ptr(A_val),
-                                          ptr(rhs_u), ptr(rhs_v), ptr(mass), ptr(u), ptr(v)))
+    if nu_node is None:
+        ctx.check(lib().cfa_assemble_momentum(ctx.h, m.h, ptr(u_old), ptr(v_old), ptr(u_prev), ptr(v_prev), ptr(p_old),
+                                              C.byref(prm), C.byref(bc) if bc is not None else None, ptr(A_val),
+                                              ptr(rhs_u), ptr(rhs_v), ptr(mass), ptr(u), ptr(v)))
+    else:
+        ctx.check(lib().cfa_assemble_momentum_nu(ctx.h, m.h, ptr(u_old), ptr(v_old), ptr(u_prev), ptr(v_prev),
+                                                 ptr(p_old), C.byref(prm), ptr(nu_node),
+                                                 C.byref(bc) if bc is not None else None, ptr(A_val), ptr(rhs_u),
+                                                 ptr(rhs_v), ptr(mass), ptr(u), ptr(v)))
+
+
+def momentum_adjoint(ctx, m: DeviceMesh, u_old, v_old, u_prev, v_prev, p_old, prm, u_max, H, x_u, x_v, lam_u, lam_v,
+                     g_u_old, g_v_old, g_u_prev, g_v_prev, g_p_old, scalars2, nu_node=None, g_nu_node=None):
+    """cfa_momentum_adjoint: node gradients (overwritten) and scalars2 = [dJ/du_max, dJ/dnu]."""
+    bc = MomentumBc(u_max, H)
+    ctx.check(lib().cfa_momentum_adjoint(ctx.h, m.h, ptr(u_old), ptr(v_old), ptr(u_prev), ptr(v_prev), ptr(p_old),
+                                         C.byref(prm), ptr(nu_node), C.byref(bc), ptr(x_u), ptr(x_v), ptr(lam_u),
+                                         ptr(lam_v), ptr(g_u_old), ptr(g_v_old), ptr(g_u_prev), ptr(g_v_prev),
+                                         ptr(g_p_old), ptr(g_nu_node), ptr(scalars2)))
+
+
+def transpose_values(ctx, ilu, val, val_t):
+    """Values of A^T on the (symmetric) pattern of the ILU handle."""
+    ctx.check(lib().cfa_csr_transpose_values(ctx.h, ilu.h, ptr(val), ptr(val_t)))
 
 
 def apply_bc_momentum(ctx, m: DeviceMesh, A_val, rhs_u, rhs_v, u, v, u_max, H=1.0):
@@ -348,6 +369,10 @@ class MulticolourIlu0:
 
     def apply(self, r, z, nrhs=1):
         self.ctx.check(lib().cfa_ilu_apply(self.ctx.h, self.h, ptr(r), ptr(z), nrhs))
+
+    def factor_transposed(self, d_val):
+        """Factor A and keep (LU)^T: the handle then preconditions A^T."""
+        self.ctx.check(lib().cfa_ilu_factor_transposed(self.ctx.h, self.h, ptr(d_val)))
 
     def device_arrays(self, nnz):
         import torch
