@@ -217,6 +217,25 @@ def momentum_adjoint(ctx, m: DeviceMesh, u_old, v_old, u_prev, v_prev, p_old, pr
                                          ptr(g_p_old), ptr(g_nu_node), ptr(scalars2)))
 
 
+def ppe_rhs_adjoint(ctx, m: DeviceMesh, lam_p, dt_proj, rho, g_u, g_v):
+    ctx.check(lib().cfa_ppe_rhs_adjoint(ctx.h, m.h, ptr(lam_p), C.c_double(dt_proj), C.c_double(rho), ptr(g_u),
+                                        ptr(g_v)))
+
+
+def projection_adjoint(ctx, m: DeviceMesh, dt_proj, rho, nu, mass, g_u_new, g_v_new, g_p_new, g_dp):
+    ctx.check(lib().cfa_projection_adjoint(ctx.h, m.h, C.c_double(dt_proj), C.c_double(rho), C.c_double(nu), ptr(mass),
+                                           ptr(g_u_new), ptr(g_v_new), ptr(g_p_new), ptr(g_dp)))
+
+
+def volume_forces_adjoint(ctx, m: DeviceMesh, u, v, u_old, v_old, u_prev, v_prev, p, b0, b1, b2, nu, rho, wx, wy,
+                          g_u, g_v, g_u_old, g_v_old, g_u_prev, g_v_prev, g_p):
+    ctx.check(lib().cfa_volume_forces_adjoint(ctx.h, m.h, ptr(u), ptr(v), ptr(u_old), ptr(v_old), ptr(u_prev),
+                                              ptr(v_prev), ptr(p), C.c_double(b0), C.c_double(b1), C.c_double(b2),
+                                              C.c_double(nu), C.c_double(rho), C.c_double(wx), C.c_double(wy),
+                                              ptr(g_u), ptr(g_v), ptr(g_u_old), ptr(g_v_old), ptr(g_u_prev),
+                                              ptr(g_v_prev), ptr(g_p)))
+
+
 def transpose_values(ctx, ilu, val, val_t):
     """Values of A^T on the (symmetric) pattern of the ILU handle."""
     ctx.check(lib().cfa_csr_transpose_values(ctx.h, ilu.h, ptr(val), ptr(val_t)))

@@ -16,73 +16,89 @@
 
 namespace cfa {
 
-constexpr int kAdjDirs = 16;   // u^n[3] v^n[3] u^{n-1}[3] v^{n-1}[3] p^n[3] nu_e
+constexpr int kAdjDirs = 16;   // momentum: u^n[3] v^n[3] u^{n-1}[3] v^{n-1}[3] p^n[3] nu_e
+constexpr int kForceDirs = 21;  // forces: u[3] v[3] u_old[3] v_old[3] u_prev[3] v_prev[3] p[3]
 
-struct Dual {
+template <int N>
+struct DualN {
     double v;
-    double d[kAdjDirs];
+    double d[N];
 };
+using Dual = DualN<kAdjDirs>;
+using DualF = DualN<kForceDirs>;
 
-__device__ __forceinline__ Dual dconst(double a) {
-    Dual r;
+template <int N>
+__device__ __forceinline__ DualN<N> dconst_n(double a) {
+    DualN<N> r;
     r.v = a;
 #pragma unroll
-    for (int k = 0; k < kAdjDirs; ++k) r.d[k] = 0.0;
+    for (int k = 0; k < N; ++k) r.d[k] = 0.0;
     return r;
 }
-__device__ __forceinline__ Dual dvar(double a, int dir) {
-    Dual r = dconst(a);
+template <int N>
+__device__ __forceinline__ DualN<N> dvar_n(double a, int dir) {
+    DualN<N> r = dconst_n<N>(a);
     r.d[dir] = 1.0;
     return r;
 }
-__device__ __forceinline__ Dual operator+(const Dual& a, const Dual& b) {
-    Dual r;
+__device__ __forceinline__ Dual dconst(double a) { return dconst_n<kAdjDirs>(a); }
+__device__ __forceinline__ Dual dvar(double a, int dir) { return dvar_n<kAdjDirs>(a, dir); }
+template <int N>
+__device__ __forceinline__ DualN<N> operator+(const DualN<N>& a, const DualN<N>& b) {
+    DualN<N> r;
     r.v = a.v + b.v;
 #pragma unroll
-    for (int k = 0; k < kAdjDirs; ++k) r.d[k] = a.d[k] + b.d[k];
+    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] + b.d[k];
     return r;
 }
-__device__ __forceinline__ Dual operator-(const Dual& a, const Dual& b) {
-    Dual r;
+template <int N>
+__device__ __forceinline__ DualN<N> operator-(const DualN<N>& a, const DualN<N>& b) {
+    DualN<N> r;
     r.v = a.v - b.v;
 #pragma unroll
-    for (int k = 0; k < kAdjDirs; ++k) r.d[k] = a.d[k] - b.d[k];
+    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] - b.d[k];
     return r;
 }
-__device__ __forceinline__ Dual operator*(const Dual& a, const Dual& b) {
-    Dual r;
+template <int N>
+__device__ __forceinline__ DualN<N> operator*(const DualN<N>& a, const DualN<N>& b) {
+    DualN<N> r;
     r.v = a.v * b.v;
 #pragma unroll
-    for (int k = 0; k < kAdjDirs; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
     return r;
 }
-__device__ __forceinline__ Dual operator*(double s, const Dual& a) {
-    Dual r;
+template <int N>
+__device__ __forceinline__ DualN<N> operator*(double s, const DualN<N>& a) {
+    DualN<N> r;
     r.v = s * a.v;
 #pragma unroll
-    for (int k = 0; k < kAdjDirs; ++k) r.d[k] = s * a.d[k];
+    for (int k = 0; k < N; ++k) r.d[k] = s * a.d[k];
     return r;
 }
-__device__ __forceinline__ Dual operator/(const Dual& a, double s) { return (1.0 / s) * a; }
-__device__ __forceinline__ Dual operator+(const Dual& a, double s) {
-    Dual r = a;
+template <int N>
+__device__ __forceinline__ DualN<N> operator/(const DualN<N>& a, double s) { return (1.0 / s) * a; }
+template <int N>
+__device__ __forceinline__ DualN<N> operator+(const DualN<N>& a, double s) {
+    DualN<N> r = a;
     r.v += s;
     return r;
 }
-__device__ __forceinline__ Dual dsqrt(const Dual& a) {
-    Dual r;
+template <int N>
+__device__ __forceinline__ DualN<N> dsqrt(const DualN<N>& a) {
+    DualN<N> r;
     r.v = sqrt(a.v);
     const double g = r.v > 0.0 ? 0.5 / r.v : 0.0;   // |w| at w = 0: the zero subgradient
 #pragma unroll
-    for (int k = 0; k < kAdjDirs; ++k) r.d[k] = g * a.d[k];
+    for (int k = 0; k < N; ++k) r.d[k] = g * a.d[k];
     return r;
 }
-__device__ __forceinline__ Dual drecip(const Dual& a) {
-    Dual r;
+template <int N>
+__device__ __forceinline__ DualN<N> drecip(const DualN<N>& a) {
+    DualN<N> r;
     r.v = 1.0 / a.v;
     const double g = -r.v * r.v;
 #pragma unroll
-    for (int k = 0; k < kAdjDirs; ++k) r.d[k] = g * a.d[k];
+    for (int k = 0; k < N; ++k) r.d[k] = g * a.d[k];
     return r;
 }
 
@@ -224,6 +240,158 @@ k_momentum_adjoint_scalars(int n, int ne, const int* __restrict__ tag, const dou
     }
 }
 
+// Pressure step without OSS (stab = 0): rhs_i = -(rho/dt') sum_e (|K|/3) div u*_e on rows that
+// are not pressure-Dirichlet (k_assemble_pressure_poisson, fem_kernels.cuh:201-282, with
+// apply_bc_pressure). Adds R^T lambda_p to g_u, g_v (per node, gathering its elements).
+__global__ void k_ppe_rhs_adjoint(int n, const int* __restrict__ ev, const double* __restrict__ x,
+                                  const double* __restrict__ y, const int* __restrict__ tag, OutletBc bc,
+                                  const int* __restrict__ inc_ptr, const int* __restrict__ inc,
+                                  const double* __restrict__ lam_p, double c, double* __restrict__ g_u,
+                                  double* __restrict__ g_v) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double su = 0.0, sv = 0.0;
+    for (int k = inc_ptr[j]; k < inc_ptr[j + 1]; ++k) {
+        const int e = inc[k] >> 2, b = inc[k] & 3;
+        const int nd[3] = {ev[3 * e], ev[3 * e + 1], ev[3 * e + 2]};
+        const double x0 = x[nd[0]], y0 = y[nd[0]], x1 = x[nd[1]], y1 = y[nd[1]], x2 = x[nd[2]], y2 = y[nd[2]];
+        const double area = 0.5 * fabs((x1 - x0) * (y2 - y0) - (x2 - x0) * (y1 - y0));
+        if (area < 1.0e-14) continue;
+        const double inv2A = 1.0 / (2.0 * area);
+        const double dNdx[3] = {(y1 - y2) * inv2A, (y2 - y0) * inv2A, (y0 - y1) * inv2A};
+        const double dNdy[3] = {(x2 - x1) * inv2A, (x0 - x2) * inv2A, (x1 - x0) * inv2A};
+        double l = 0.0;
+        for (int a = 0; a < 3; ++a)
+            if (!pressure_dirichlet(nd[a], tag[nd[a]], bc)) l += lam_p[nd[a]];
+        const double w = c * (area / 3.0) * l;
+        su += w * dNdx[b];
+        sv += w * dNdy[b];
+    }
+    g_u[j] += su;
+    g_v[j] += sv;
+}
+
+// Projection (k_velocity_pressure_correction with the rotational term from the increment):
+// u' = u* - (dt'/rho) M^-1 G_x dp on interior nodes and a natural outlet, p' = p + dp + nu dt'
+// M^-1 K dp. Given the adjoints of u', v', p': g_dp = p'bar + nu dt' K (p'bar / m)
+// - (dt'/rho) (G_x^T (mask u'bar / m) + G_y^T (mask v'bar / m)) (overwritten).
+__global__ void k_projection_adjoint(int n, const int* __restrict__ ev, const double* __restrict__ x,
+                                     const double* __restrict__ y, const int* __restrict__ tag, OutletBc bc,
+                                     const int* __restrict__ inc_ptr, const int* __restrict__ inc,
+                                     const double* __restrict__ mass, double dt, double rho, double nu,
+                                     const double* __restrict__ gu, const double* __restrict__ gv,
+                                     const double* __restrict__ gp, double* __restrict__ g_dp) {
+    const int k0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k0 >= n) return;
+    double s = 0.0;
+    for (int q = inc_ptr[k0]; q < inc_ptr[k0 + 1]; ++q) {
+        const int e = inc[q] >> 2, b = inc[q] & 3;
+        const int nd[3] = {ev[3 * e], ev[3 * e + 1], ev[3 * e + 2]};
+        const double x0 = x[nd[0]], y0 = y[nd[0]], x1 = x[nd[1]], y1 = y[nd[1]], x2 = x[nd[2]], y2 = y[nd[2]];
+        const double area = 0.5 * fabs((x1 - x0) * (y2 - y0) - (x2 - x0) * (y1 - y0));
+        if (area < 1.0e-14) continue;
+        const double inv2A = 1.0 / (2.0 * area);
+        const double dNdx[3] = {(y1 - y2) * inv2A, (y2 - y0) * inv2A, (y0 - y1) * inv2A};
+        const double dNdy[3] = {(x2 - x1) * inv2A, (x0 - x2) * inv2A, (x1 - x0) * inv2A};
+        double psx = 0.0, psy = 0.0, au = 0.0, av = 0.0;
+        for (int a = 0; a < 3; ++a) {
+            const int i = nd[a];
+            const double m_i = fmax(mass[i], 1.0e-14);
+            const double psi = gp[i] / m_i;
+            psx += psi * dNdx[a];
+            psy += psi * dNdy[a];
+            const int t = tag[i];
+            if (t == BC_INTERIOR || (t == BC_OUTLET && !bc.outlet_dirichlet)) {
+                au += gu[i] / m_i;
+                av += gv[i] / m_i;
+            }
+        }
+        s += nu * dt * area * (dNdx[b] * psx + dNdy[b] * psy);
+        s -= (dt / rho) * (area / 3.0) * (dNdx[b] * au + dNdy[b] * av);
+    }
+    g_dp[k0] = gp[k0] + s;
+}
+
+// Volume forces (k_volume_forces, fem_kernels.cuh:1046-1123): per element the derivatives of
+// wx F_x + wy F_y with respect to its 21 nodal inputs (dual numbers through the same formula).
+__global__ void __launch_bounds__(128)
+k_forces_adjoint_elems(int ne, const int* __restrict__ ev, const int* __restrict__ tag, const double* __restrict__ x,
+                       const double* __restrict__ y, const double* __restrict__ u, const double* __restrict__ v,
+                       const double* __restrict__ u_old, const double* __restrict__ v_old,
+                       const double* __restrict__ u_prev, const double* __restrict__ v_prev,
+                       const double* __restrict__ p, double b0, double b1, double b2, double nu, double rho, double wx,
+                       double wy, double* __restrict__ g_elem) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    double* g = g_elem + (size_t)e * kForceDirs;
+    const int nd[3] = {ev[3 * e], ev[3 * e + 1], ev[3 * e + 2]};
+    double phi[3];
+    bool touches = false;
+    for (int a = 0; a < 3; ++a) {
+        phi[a] = tag[nd[a]] == BC_CYLINDER ? 1.0 : 0.0;
+        touches = touches || phi[a] > 0.0;
+    }
+    const double x0 = x[nd[0]], y0 = y[nd[0]], x1 = x[nd[1]], y1 = y[nd[1]], x2 = x[nd[2]], y2 = y[nd[2]];
+    const double area = 0.5 * fabs((x1 - x0) * (y2 - y0) - (x2 - x0) * (y1 - y0));
+    if (!touches || area < 1.0e-14) {
+        for (int k = 0; k < kForceDirs; ++k) g[k] = 0.0;
+        return;
+    }
+    const double inv2A = 1.0 / (2.0 * area);
+    const double dNdx[3] = {(y1 - y2) * inv2A, (y2 - y0) * inv2A, (y0 - y1) * inv2A};
+    const double dNdy[3] = {(x2 - x1) * inv2A, (x0 - x2) * inv2A, (x1 - x0) * inv2A};
+    DualF ue[3], ve[3], ute[3], vte[3];
+    DualF dudx = dconst_n<kForceDirs>(0.0), dudy = dudx, dvdx = dudx, dvdy = dudx, p_bar = dudx;
+    double dphidx = 0.0, dphidy = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        ue[a] = dvar_n<kForceDirs>(u[nd[a]], a);
+        ve[a] = dvar_n<kForceDirs>(v[nd[a]], 3 + a);
+        ute[a] = b0 * ue[a] + b1 * dvar_n<kForceDirs>(u_old[nd[a]], 6 + a) +
+                 b2 * dvar_n<kForceDirs>(u_prev[nd[a]], 12 + a);
+        vte[a] = b0 * ve[a] + b1 * dvar_n<kForceDirs>(v_old[nd[a]], 9 + a) +
+                 b2 * dvar_n<kForceDirs>(v_prev[nd[a]], 15 + a);
+        dudx = dudx + dNdx[a] * ue[a];
+        dudy = dudy + dNdy[a] * ue[a];
+        dvdx = dvdx + dNdx[a] * ve[a];
+        dvdy = dvdy + dNdy[a] * ve[a];
+        dphidx += phi[a] * dNdx[a];
+        dphidy += phi[a] * dNdy[a];
+        p_bar = p_bar + dvar_n<kForceDirs>(p[nd[a]], 18 + a) / 3.0;
+    }
+    DualF fx = dconst_n<kForceDirs>(0.0), fy = fx;
+    for (int a = 0; a < 3; ++a) {
+        const int b = (a + 1) % 3;
+        const double phi_m = 0.5 * (phi[a] + phi[b]);
+        if (phi_m == 0.0) continue;
+        const DualF um = 0.5 * (ue[a] + ue[b]), vm = 0.5 * (ve[a] + ve[b]);
+        fx = fx + phi_m * (0.5 * (ute[a] + ute[b]) + (um * dudx + vm * dudy));
+        fy = fy + phi_m * (0.5 * (vte[a] + vte[b]) + (um * dvdx + vm * dvdy));
+    }
+    fx = (area / 3.0) * fx;
+    fy = (area / 3.0) * fy;
+    fx = fx + area * ((nu * dphidx) * dudx + (nu * dphidy) * dudy - (dphidx / rho) * p_bar);
+    fy = fy + area * ((nu * dphidx) * dvdx + (nu * dphidy) * dvdy - (dphidy / rho) * p_bar);
+    for (int k = 0; k < kForceDirs; ++k) g[k] = wx * fx.d[k] + wy * fy.d[k];
+}
+
+// Node sums of the element force derivatives into seven nodal gradients (added to).
+__global__ void k_forces_adjoint_nodes(int n, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
+                                       const double* __restrict__ g_elem, double* __restrict__ g_u,
+                                       double* __restrict__ g_v, double* __restrict__ g_u_old,
+                                       double* __restrict__ g_v_old, double* __restrict__ g_u_prev,
+                                       double* __restrict__ g_v_prev, double* __restrict__ g_p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int k = inc_ptr[i]; k < inc_ptr[i + 1]; ++k) {
+        const int e = inc[k] >> 2, a = inc[k] & 3;
+        const double* g = g_elem + (size_t)e * kForceDirs;
+        for (int q = 0; q < 7; ++q) s[q] += g[3 * q + a];
+    }
+    g_u[i] += s[0]; g_v[i] += s[1]; g_u_old[i] += s[2]; g_v_old[i] += s[3];
+    g_u_prev[i] += s[4]; g_v_prev[i] += s[5]; g_p[i] += s[6];
+}
+
 }  // namespace cfa
 
 using namespace cfa;
@@ -250,6 +418,48 @@ cfa_status cfa_momentum_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const double* u
     CFA_PROPAGATE(ensure_partials(ctx, 2 * (size_t)grid + 2));
     CFA_LAUNCH(ctx, k_momentum_adjoint_scalars, grid, kThreads, 0, m->n, m->ne, m->tag, m->y, bcp->H, m->bc, lam_u,
                (const double*)g_elem.p, ctx->d_part, ctx->d_counters, d_scalars2);
+    CFA_CHECK_LAUNCH();
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));   // g_elem is released on return
+    return CFA_OK;
+}
+
+cfa_status cfa_ppe_rhs_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const double* lam_p, double dt_proj, double rho,
+                               double* g_u, double* g_v) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(m && lam_p && g_u && g_v && dt_proj > 0.0);
+    CFA_ARG(!m->bc.outlet_dirichlet);
+    CFA_LAUNCH(ctx, k_ppe_rhs_adjoint, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y, m->tag, m->bc,
+               m->inc_ptr.p, m->inc.p, lam_p, -(rho / dt_proj), g_u, g_v);
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+cfa_status cfa_projection_adjoint(cfa_ctx* ctx, const cfa_mesh* m, double dt_proj, double rho, double nu,
+                                  const double* mass_lumped, const double* g_u_new, const double* g_v_new,
+                                  const double* g_p_new, double* g_dp) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(m && mass_lumped && g_u_new && g_v_new && g_p_new && g_dp && g_dp != g_p_new);
+    CFA_LAUNCH(ctx, k_projection_adjoint, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y, m->tag,
+               m->bc, m->inc_ptr.p, m->inc.p, mass_lumped, dt_proj, rho, nu, g_u_new, g_v_new, g_p_new, g_dp);
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+cfa_status cfa_volume_forces_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const double* u, const double* v,
+                                     const double* u_old, const double* v_old, const double* u_prev,
+                                     const double* v_prev, const double* p, double b0, double b1, double b2,
+                                     double nu, double rho, double wx, double wy, double* g_u, double* g_v,
+                                     double* g_u_old, double* g_v_old, double* g_u_prev, double* g_v_prev,
+                                     double* g_p) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(m && u && v && u_old && v_old && u_prev && v_prev && p && g_u && g_v && g_u_old && g_v_old && g_u_prev &&
+            g_v_prev && g_p);
+    DevBuf<double> g_elem;
+    CFA_CUDA(g_elem.ensure((size_t)std::max(m->ne, 1) * kForceDirs));
+    CFA_LAUNCH(ctx, k_forces_adjoint_elems, ceil_div(m->ne, 128), 128, 0, m->ne, m->ev, m->tag, m->x, m->y, u, v,
+               u_old, v_old, u_prev, v_prev, p, b0, b1, b2, nu, rho, wx, wy, g_elem.p);
+    CFA_LAUNCH(ctx, k_forces_adjoint_nodes, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->inc_ptr.p, m->inc.p,
+               (const double*)g_elem.p, g_u, g_v, g_u_old, g_v_old, g_u_prev, g_v_prev, g_p);
     CFA_CHECK_LAUNCH();
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));   // g_elem is released on return
     return CFA_OK;

@@ -131,6 +131,26 @@ cfa_status cfa_momentum_adjoint(cfa_ctx* ctx, const cfa_mesh* mesh, const double
                                 const double* d_lambda_u, const double* d_lambda_v, double* d_g_u_old,
                                 double* d_g_v_old, double* d_g_u_prev, double* d_g_v_prev, double* d_g_p_old,
                                 double* d_g_nu_node, double* d_scalars2);
+/* Adjoint pieces of the rest of a step (no counterpart in the reference; the pressure step
+ * without OSS, stab = 0, and the default p = 0 outlet). cfa_ppe_rhs_adjoint adds R^T lambda_p to
+ * d_g_u, d_g_v, where rhs_p = R (u*, v*) is the PPE right-hand side -(rho/dt') (N_i, div u*) on
+ * rows that are not Dirichlet. */
+cfa_status cfa_ppe_rhs_adjoint(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_lambda_p, double dt_proj,
+                               double rho, double* d_g_u, double* d_g_v);
+/* Adjoint of cfa_project_step with the rotational term from the increment: given the adjoints of
+ * the corrected u, v, p, writes the adjoint of dp (overwritten); those of u* and p^n are the
+ * corrected ones unchanged (the caller passes them through). */
+cfa_status cfa_projection_adjoint(cfa_ctx* ctx, const cfa_mesh* mesh, double dt_proj, double rho, double nu,
+                                  const double* d_mass_lumped, const double* d_g_u_new, const double* d_g_v_new,
+                                  const double* d_g_p_new, double* d_g_dp);
+/* Adds the derivatives of wx F_x + wy F_y (cfa_volume_forces) with respect to its seven nodal
+ * inputs to the seven gradients. Synchronises. */
+cfa_status cfa_volume_forces_adjoint(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_u, const double* d_v,
+                                     const double* d_u_old, const double* d_v_old, const double* d_u_prev,
+                                     const double* d_v_prev, const double* d_p, double b0, double b1, double b2,
+                                     double nu, double rho, double wx, double wy, double* d_g_u, double* d_g_v,
+                                     double* d_g_u_old, double* d_g_v_old, double* d_g_u_prev,
+                                     double* d_g_v_prev, double* d_g_p);
 /* k_apply_bc_momentum (src/cfa/fem_kernels.cuh:411-453) alone. */
 cfa_status cfa_apply_bc_momentum(cfa_ctx* ctx, const cfa_mesh* mesh, const cfa_momentum_bc* bc,
                                  double* d_A_val, double* d_rhs_u, double* d_rhs_v, double* d_u,
