@@ -466,6 +466,63 @@ def run_stress(args, rank, world):
 
 
 # ------------------------------------------------------------------------------------------------
+# adjoint (c3): gradient of the mean drag over 200 BDF2 steps on the c1 mesh
+# ------------------------------------------------------------------------------------------------
+def run_adjoint(args):
+    import torch
+    import adjoint as AD
+    import cfa_b200 as cfa
+    import fixtures as F
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    m = F.make_mesh("c1")
+    steps = 200
+    u0 = 4 * U_MAX * m.y * (1 - m.y)
+    z = np.zeros(m.n)
+    nu_node = np.full(m.n, NU)
+
+    def make(prec):
+        return AD.DragAdjoint(m, u0, z, z, nu_node, u_max=U_MAX, steps=steps, dt=5e-3, nu=NU, precision=prec,
+                              checkpoint=20, tol=1e-12)
+
+    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
+    adj = make(cfa.MIXED)
+    adj.objective()                                   # warm-up: setup, graphs
+    torch.cuda.synchronize()
+    clk.start()
+    t0 = time.perf_counter()
+    J = adj.objective()
+    torch.cuda.synchronize()
+    t_fwd = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    J2, g_nu, g_u = adj.gradient()
+    torch.cuda.synchronize()
+    t_grad = (time.perf_counter() - t0) * 1e3
+    clk.stop()
+    h = 1e-6 * U_MAX
+    fd = (adj.objective(U_MAX + h) - adj.objective(U_MAX - h)) / (2 * h)
+    ref = make(cfa.FP64)
+    J64, g64, gu64 = ref.gradient()
+    line = {
+        "metric": "adjoint gradient of the mean drag over 200 BDF2 steps (c1 mesh), wall ms per gradient",
+        "value": round(t_grad, 1), "unit": "ms/gradient", "n_gpus": 1, "steps": steps, "warmup": 1,
+        "ms_per_step": round(t_grad / steps, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 outer / f32 preconditioners", "data": "synthetic",
+        "config": {"workload": f"c3: c1 mesh n={m.n}, dt 5e-3, U 1.5, nu 1e-3, from the inflow profile, "
+                               "OSS off (stab 0), checkpoints every 20 steps, solves to 1e-12",
+                   "forward_ms": round(t_fwd, 1), "J_mean_drag": J,
+                   "dJ_dU": g_u, "dJ_dU_central_fd_h1e-6": fd, "fd_rel_diff": abs(g_u - fd) / abs(fd),
+                   "dJ_dnu_norm": float(torch.linalg.norm(g_nu)),
+                   "fp64_grad_rel_diff": float(torch.abs(g_nu - g64).max() / torch.abs(g64).max()),
+                   "fp64_dJ_dU_rel_diff": abs(g_u - gu64) / abs(gu64)},
+        "e2e": {"value": round(t_grad, 1), "unit": "ms/gradient", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8},
+        "gpu_launches": None,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------------------------------------
 # batched systems (c4): 64 independent system pairs, 5k-500k vertices, LPT over GPUs
 # ------------------------------------------------------------------------------------------------
 def run_batch(args, rank, world):
@@ -559,6 +616,10 @@ def main():
     if args.workload == "c2":
         if rank == 0:
             run_stress(args, rank, world)
+        return
+    if args.workload == "c3":
+        if rank == 0:
+            run_adjoint(args)
         return
     m, res = run_ours(args, rank, world)
     if args.profile:

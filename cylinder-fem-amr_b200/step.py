@@ -199,3 +199,57 @@ class TimeStepper:
                           -a2, self.nu, self.rho, self.forces)
         f = self.forces.cpu().numpy()
         return self.force_scale * f[0], self.force_scale * f[1]
+
+
+def project_divergence_free(ctx, dm, dt, u, v, p, mass, amg=None, tol=1e-8, rho=1.0):
+    """project_divergence_free (src/cfa/device.cuh:413-461): K phi = -(rho/dt) (N_i, div u) with the
+    outlet rows eliminated, then u -= (dt/rho) M^-1 grad phi (p unchanged). u, v updated in place;
+    returns (PCG iterations, nodal vorticity of the projected field). amg: a hierarchy of K to
+    reuse (set up here when it has none yet)."""
+    import torch
+    n, nnz, ne = dm.n, dm.nnz, dm.ne
+    z = lambda k: torch.zeros(k, dtype=torch.float64, device="cuda")
+    Kp, rhs, div, phi = z(nnz), z(n), z(n), z(n)
+    gx, gy, vn, vort = z(n), z(n), z(n), z(n)
+    cfa.lumped_mass(ctx, dm, mass)
+    cfa.assemble_pressure_system(ctx, dm, u, v, p, gx, gy, mass, z(ne), dt, rho, 0.0, Kp, rhs, div, phi, z(4 * nnz),
+                                 z(n))
+    if amg is not None and amg.h is None:
+        amg.setup(n, nnz, dm.rp, dm.ci, Kp)
+    it = cfa.GpuLinearSolver(ctx).solve_pcg(n, dm.rp, dm.ci, Kp, rhs, phi, 4000, tol, None, amg)
+    cfa.grad_dp_vorticity(ctx, dm, phi, u, v, gx, gy, vn)
+    cfa.velocity_pressure_correction(ctx, dm, dt, rho, 0.0, 0.0, div, mass, gx, gy, vn, phi, u, v, p, vort)
+    return it, vort
+
+
+def project_scheme_consistent(ctx, dm, dt_proj, stab, nu, u_old, v_old, u, v, p, amg=None, both_levels=True,
+                              tol=1e-8, rho=1.0):
+    """project_scheme_consistent (src/cfa/device.cuh:337-405): after a remesh, each velocity level
+    (u^{n-1} and u^n, or u^n only) is projected with the time step's own pressure operator (PPE
+    with the OSS term for weights of the current u, G(p^n)), p unchanged. Fields updated in place;
+    returns the PCG iterations. The AMG hierarchy is set up on the first level's operator."""
+    import torch
+    n, nnz, ne = dm.n, dm.nnz, dm.ne
+    z = lambda k: torch.zeros(k, dtype=torch.float64, device="cuda")
+    mass, elem_s, Kp, rhs, div, dp = z(n), z(ne), z(nnz), z(n), z(n), z(n)
+    gpx, gpy, gx, gy, vn, vort = z(n), z(n), z(n), z(n), z(n), z(n)
+    oss_val, inv_m = z(4 * nnz), z(n)
+    cfa.lumped_mass(ctx, dm, mass)
+    if stab > 0.0:
+        cfa.oss_weights(ctx, dm, u, v, dt_proj, rho, nu, stab, elem_s)
+    oss = cfa.oss_operator(dm, oss_val, inv_m) if stab > 0.0 else None
+    solver = cfa.GpuLinearSolver(ctx)
+    iters = 0
+    levels = ((u_old, v_old), (u, v)) if both_levels else ((u, v),)
+    for k, (fu, fv) in enumerate(levels):
+        dp.zero_()
+        if stab > 0.0:
+            cfa.scalar_gradient(ctx, dm, p, elem_s, gpx, gpy)
+        cfa.assemble_pressure_system(ctx, dm, fu, fv, p, gpx, gpy, mass, elem_s, dt_proj, rho, stab, Kp, rhs, div, dp,
+                                     oss_val, inv_m)
+        if amg is not None and k == 0:
+            amg.setup(n, nnz, dm.rp, dm.ci, Kp)
+        iters += solver.solve_pcg(n, dm.rp, dm.ci, Kp, rhs, dp, 4000, tol, oss, amg)
+        cfa.grad_dp_vorticity(ctx, dm, dp, fu, fv, gx, gy, vn)
+        cfa.velocity_pressure_correction(ctx, dm, dt_proj, rho, 0.0, 0.0, div, mass, gx, gy, vn, dp, fu, fv, p, vort)
+    return iters

@@ -450,3 +450,37 @@ class Stepper:
         f = volume_forces(m, u, v, self.u_old, self.v_old, self.u_prev, self.v_prev, self.p, a0, -a1, -a2, self.nu,
                           self.rho)
         return self.force_scale * f[0], self.force_scale * f[1]
+
+
+def project_divergence_free(mesh, rp, ci, dt, u, v, tol=1e-8, rho=1.0):
+    """project_divergence_free (src/cfa/device.cuh:413-461): u, v updated in place; returns phi."""
+    n = mesh.n
+    mass = lumped_mass(mesh)
+    z = np.zeros(n)
+    Kp, rhs, div = assemble_ppe(mesh, rp, ci, u, v, z, z, z, mass, np.zeros(mesh.ne), dt, rho, 0.0)
+    phi = np.zeros(n)
+    apply_bc_pressure(mesh, rp, ci, Kp, rhs, phi, mass)
+    phi, rep = pcg(rp, ci, Kp, rhs, phi, 4000, tol, amg=Amg(rp, ci, Kp))
+    gx, gy, vn = grad_dp_vorticity(mesh, phi, u, v)
+    velocity_pressure_correction(mesh, dt, rho, 0.0, 0.0, div, mass, gx, gy, vn, phi, u, v, np.zeros(n))
+    return phi
+
+
+def project_scheme_consistent(mesh, rp, ci, dt_proj, stab, nu, levels, p, tol=1e-8, rho=1.0):
+    """project_scheme_consistent (src/cfa/device.cuh:337-405): each (u, v) pair of `levels`
+    projected in place with the step's pressure operator; p unchanged."""
+    n = mesh.n
+    mass = lumped_mass(mesh)
+    s = oss_weights(mesh, levels[-1][0], levels[-1][1], dt_proj, rho, nu, stab) if stab > 0 else np.zeros(mesh.ne)
+    oss, inv_m = assemble_oss(mesh, rp, ci, s, mass) if stab > 0 else (None, None)
+    amg = None
+    for k, (u, v) in enumerate(levels):
+        gx, gy = scalar_gradient(mesh, p, s) if stab > 0 else (np.zeros(n), np.zeros(n))
+        Kp, rhs, div = assemble_ppe(mesh, rp, ci, u, v, p, gx, gy, mass, s, dt_proj, rho, stab)
+        dp = np.zeros(n)
+        apply_bc_pressure(mesh, rp, ci, Kp, rhs, dp, mass)
+        if k == 0:
+            amg = Amg(rp, ci, Kp)
+        dp, rep = pcg(rp, ci, Kp, rhs, dp, 4000, tol, oss, inv_m, mesh.tag, amg)
+        gdx, gdy, vn = grad_dp_vorticity(mesh, dp, u, v)
+        velocity_pressure_correction(mesh, dt_proj, rho, 0.0, 0.0, div, mass, gdx, gdy, vn, dp, u, v, p.copy())

@@ -741,3 +741,33 @@ def test_time_stepper_matches_oracle(ctx, precision):
         assert abs(got[0] - want[0]) <= 1e-9 * scale and abs(got[1] - want[1]) <= 1e-9 * scale, (k, got, want)
     assert np.abs(host(st.u) - ref.u).max() <= 1e-9 * np.abs(ref.u).max()
     assert np.abs(host(st.p) - ref.p).max() <= 1e-9 * np.abs(ref.p).max()
+
+
+# ------------------------------------------------------------------------------------------------
+# f2: re-projection of transferred velocities after a remesh
+# ------------------------------------------------------------------------------------------------
+def test_reprojection_matches_oracle(ctx):
+    import step as S
+    m = mesh("small")
+    dm = cfa.DeviceMesh(ctx, m)
+    rp, ci = dm.host_pattern()
+    u, v, p = fields(m)
+    # divergence-free projection (plain PPE), p unchanged
+    uo, vo = u.copy(), v.copy()
+    O.project_divergence_free(m, rp, ci, 1e-3, uo, vo, tol=1e-12)
+    du, dv, dpp = dev(u), dev(v), dev(p)
+    mass = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+    it, vort = S.project_divergence_free(ctx, dm, 1e-3, du, dv, dpp, mass, amg=cfa.AmgPreconditioner(ctx), tol=1e-12)
+    assert it > 0
+    assert np.abs(host(du) - uo).max() <= 1e-9 * np.abs(uo).max()
+    assert np.abs(host(dv) - vo).max() <= 1e-9 * np.abs(vo).max()
+    assert np.array_equal(host(dpp), p)
+    # scheme-consistent projection of both levels with the OSS operator
+    u1, v1 = 0.9 * u, 0.9 * v
+    lv = [(u1.copy(), v1.copy()), (u.copy(), v.copy())]
+    O.project_scheme_consistent(m, rp, ci, 2e-3 / 3, 0.3, 1e-3, lv, p, tol=1e-12)
+    du1, dv1, du, dv = dev(u1), dev(v1), dev(u), dev(v)
+    S.project_scheme_consistent(ctx, dm, 2e-3 / 3, 0.3, 1e-3, du1, dv1, du, dv, dev(p),
+                                amg=cfa.AmgPreconditioner(ctx), tol=1e-12)
+    for g, w in ((du1, lv[0][0]), (dv1, lv[0][1]), (du, lv[1][0]), (dv, lv[1][1])):
+        assert np.abs(host(g) - w).max() <= 1e-9 * np.abs(w).max()
