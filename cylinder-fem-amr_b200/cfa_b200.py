@@ -366,15 +366,17 @@ class MulticolourIlu0:
         self.colour_start = []
 
     def set_pattern(self, n, rp_host, ci_host, d_rp, d_ci):
-        if self.h is not None:
-            lib().cfa_ilu_destroy(self.h)
-            self.h = None
+        """A new pattern; the handle (and its device buffers) is kept across calls."""
         rp_h = np.ascontiguousarray(rp_host, dtype=np.int32)
         ci_h = np.ascontiguousarray(ci_host, dtype=np.int32)
-        h = C.c_void_p()
-        self.ctx.check(lib().cfa_ilu_create(self.ctx.h, n, ptr(rp_h), ptr(ci_h), ptr(d_rp), ptr(d_ci), self.precision,
-                                            C.byref(h)))
-        self.h = h
+        if self.h is None:
+            h = C.c_void_p()
+            self.ctx.check(lib().cfa_ilu_create(self.ctx.h, n, ptr(rp_h), ptr(ci_h), ptr(d_rp), ptr(d_ci),
+                                                self.precision, C.byref(h)))
+            self.h = h
+        else:
+            self.ctx.check(lib().cfa_ilu_set_pattern(self.ctx.h, self.h, n, ptr(rp_h), ptr(ci_h), ptr(d_rp),
+                                                     ptr(d_ci)))
         self.n = n
         nc = C.c_int()
         lib().cfa_ilu_colours(self.h, C.byref(nc), None)
@@ -540,6 +542,25 @@ class GpuLinearSolver:
         self.ctx.check(lib().cfa_pcg_solve(self.ctx.h, n, ptr(d_rp), ptr(d_ci), ptr(d_val), ptr(d_b), ptr(d_x),
                                            C.byref(oss) if oss is not None else None, amg.h if amg is not None else None,
                                            C.byref(opts), C.byref(rep)),
+                       allow=(CFA_OK, CFA_NOT_CONVERGED, CFA_BREAKDOWN))
+        self.converged = bool(rep.converged[0])
+        self.last_rel_residual = rep.rel_residual[0]
+        self.solve_ms = rep.solve_ms
+        return rep.iterations[0]
+
+    def solve_pcg_host_ops(self, n, d_rp, d_ci, d_val, d_b, d_x, max_iter=400, tol=1e-7, extra_op=None,
+                           amg: AmgPreconditioner | None = None, precond=None) -> int:
+        """solve_pcg with the reference's std::function hooks as Python callables
+        f(in_ptr, out_ptr) on device addresses: extra_op adds its operator into out, precond
+        writes out = M^-1 in (cfa_pcg_solve_host_ops). They run on the host between the
+        library's launches and must enqueue their work on this context's stream."""
+        cb = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_void_p)
+        hooks = [cb(lambda i, o, u, f=f: f(i, o)) if f is not None else None for f in (extra_op, precond)]
+        rep = SolveReport()
+        opts = SolveOpts(max_iter, tol)
+        self.ctx.check(lib().cfa_pcg_solve_host_ops(self.ctx.h, n, ptr(d_rp), ptr(d_ci), ptr(d_val), ptr(d_b),
+                                                    ptr(d_x), hooks[0], None, amg.h if amg is not None else None,
+                                                    hooks[1], None, C.byref(opts), C.byref(rep)),
                        allow=(CFA_OK, CFA_NOT_CONVERGED, CFA_BREAKDOWN))
         self.converged = bool(rep.converged[0])
         self.last_rel_residual = rep.rel_residual[0]

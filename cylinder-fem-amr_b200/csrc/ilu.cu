@@ -164,6 +164,11 @@ __global__ void k_mirror_positions(int n, const int* __restrict__ rp, const int*
     if (i >= n) return;
     for (int a = rp[i]; a < rp[i + 1]; ++a) {
         const int j = ci[a];
+        if (j < 0 || j >= n) {   // not a pattern of n rows
+            tpos[a] = a;
+            atomicExch(err, 1);
+            continue;
+        }
         int lo = rp[j], hi = rp[j + 1] - 1;
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
@@ -213,19 +218,12 @@ cfa_status ilu_apply(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z,
     return CFA_OK;
 }
 
-}  // namespace cfa
-
-using namespace cfa;
-
-extern "C" {
-
-cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, const int* d_rp, const int* d_ci,
-                          cfa_precision precision, cfa_ilu** out) {
-    if (!ctx || !out) return CFA_BAD_ARG;
-    CFA_ARG(n > 0 && rp && ci && d_rp && d_ci);
-    CFA_ARG(precision == CFA_FP64 || precision == CFA_MIXED);
-    *out = nullptr;
+// set_pattern (src/cfa/linalg.cuh:456-528) into handle h, reusing its device buffers (they grow
+// geometrically, as the reference's cap_n / cap_nnz)
+static cfa_status ilu_pattern(cfa_ctx* ctx, cfa_ilu* h, int n, const int* rp, const int* ci, const int* d_rp,
+                              const int* d_ci) {
     const int nnz = rp[n];
+    const cfa_precision precision = h->precision;
     std::vector<int> colour(n, -1), diag(n, -1), mark;
     int nc = 0;
     for (int i = 0; i < n; ++i) {
@@ -243,9 +241,12 @@ cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, con
     }
     for (int r = 0; r < n; ++r)
         if (diag[r] < 0) return set_error(ctx, CFA_BAD_ARG, "ILU pattern row without a diagonal", __FILE__, __LINE__);
-    auto* h = new cfa_ilu();
     h->uid = next_uid();
-    h->n = n; h->nnz = nnz; h->nc = nc; h->precision = precision; h->rp = d_rp; h->ci = d_ci;
+    h->n = n; h->nnz = nnz; h->nc = nc;
+    (void)d_rp;
+    (void)d_ci;
+    h->mirror = false;
+    h->transposed = false;
     h->colour_start.assign(nc + 1, 0);
     for (int i = 0; i < n; ++i) h->colour_start[colour[i] + 1]++;
     for (int c = 0; c < nc; ++c) h->colour_start[c + 1] += h->colour_start[c];
@@ -290,10 +291,12 @@ cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, con
                 el.x = q;
                 el.y = diag[k];
                 el.z = (int)updv.size();
-                for (int mm = rp[k]; mm < rp[k + 1]; ++mm) {
-                    const int j = ci[mm];
-                    for (int b = 0; b < len; ++b)
-                        if (ci[s0 + b] == j) { if (colour[j] > c) updv.push_back(make_int2(b, mm)); break; }
+                // rows k and i are sorted: one merge finds the common columns, in row k's order
+                for (int mm = rp[k], b = 0; mm < rp[k + 1] && b < len;) {
+                    const int j = ci[mm], cb = ci[s0 + b];
+                    if (cb < j) { ++b; continue; }
+                    if (cb == j && colour[j] > c) updv.push_back(make_int2(b, mm));
+                    ++mm;
                 }
                 el.w = (int)updv.size();
                 elim.push_back(el);
@@ -310,6 +313,13 @@ cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, con
         if (e == cudaSuccess && !v.empty())
             e = cudaMemcpyAsync(d.p, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
     };
+    // the handle's own copy of the pattern (the reference keeps the caller's device arrays; a
+    // copy leaves nothing for the caller to keep alive)
+    const std::vector<int> rp_v(rp, rp + n + 1), ci_v(ci, ci + nnz);
+    up_int(h->own_rp, rp_v);
+    up_int(h->own_ci, ci_v);
+    h->rp = h->own_rp.p;
+    h->ci = h->own_ci.p;
     up_int(h->rows, rows); up_int(h->colour, colour); up_int(h->diag, diag); up_int(h->lp, lp); up_int(h->up, up);
     up_int(h->lc, lc); up_int(h->uc, uc); up_int(h->l_src, l_src); up_int(h->u_src, u_src); up_int(h->d_src, d_src);
     up_int(h->ep, ep);
@@ -331,12 +341,39 @@ cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, con
         if (e == cudaSuccess) e = h->dinv64.ensure(n);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) {
+    if (e != cudaSuccess) return set_error(ctx, CFA_CUDA_ERROR, cudaGetErrorString(e), __FILE__, __LINE__);
+    return CFA_OK;
+}
+
+
+}  // namespace cfa
+
+using namespace cfa;
+
+extern "C" {
+
+cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, const int* d_rp, const int* d_ci,
+                          cfa_precision precision, cfa_ilu** out) {
+    if (!ctx || !out) return CFA_BAD_ARG;
+    CFA_ARG(n > 0 && rp && ci && d_rp && d_ci);
+    CFA_ARG(precision == CFA_FP64 || precision == CFA_MIXED);
+    *out = nullptr;
+    auto* h = new cfa_ilu();
+    h->precision = precision;
+    const cfa_status st = ilu_pattern(ctx, h, n, rp, ci, d_rp, d_ci);
+    if (st != CFA_OK) {
         delete h;
-        return set_error(ctx, CFA_CUDA_ERROR, cudaGetErrorString(e), __FILE__, __LINE__);
+        return st;
     }
     *out = h;
     return CFA_OK;
+}
+
+cfa_status cfa_ilu_set_pattern(cfa_ctx* ctx, cfa_ilu* h, int n, const int* rp, const int* ci, const int* d_rp,
+                               const int* d_ci) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(h && n > 0 && rp && ci && d_rp && d_ci);
+    return ilu_pattern(ctx, h, n, rp, ci, d_rp, d_ci);
 }
 
 cfa_status cfa_ilu_destroy(cfa_ilu* ilu) {
@@ -371,7 +408,7 @@ cfa_status cfa_ilu_factor(cfa_ctx* ctx, cfa_ilu* h, const double* val) {
 namespace cfa {
 // Mirror positions of the handle's pattern, computed once (synchronises the first time).
 static cfa_status ensure_mirror(cfa_ctx* ctx, cfa_ilu* h) {
-    if (h->tpos.p) return CFA_OK;
+    if (h->mirror) return CFA_OK;
     CFA_CUDA(h->tpos.ensure(std::max(h->nnz, 1)));
     DevBuf<int> err;
     CFA_CUDA(err.ensure(1));
@@ -380,10 +417,8 @@ static cfa_status ensure_mirror(cfa_ctx* ctx, cfa_ilu* h) {
     int herr = 0;
     CFA_CUDA(cudaMemcpyAsync(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (herr) {
-        h->tpos.release();
-        return set_error(ctx, CFA_BAD_ARG, "pattern not structurally symmetric", __FILE__, __LINE__);
-    }
+    if (herr) return set_error(ctx, CFA_BAD_ARG, "pattern not structurally symmetric", __FILE__, __LINE__);
+    h->mirror = true;
     return CFA_OK;
 }
 }  // namespace cfa

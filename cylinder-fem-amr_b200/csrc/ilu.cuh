@@ -9,8 +9,9 @@ struct cfa_ilu {
     int n = 0, nnz = 0, nc = 0, nl = 0, nu = 0;
     long long uid = 0;
     cfa_precision precision = CFA_FP64;
-    const int* rp = nullptr;          // device pattern (caller-owned)
+    const int* rp = nullptr;          // device pattern (the handle's copy below)
     const int* ci = nullptr;
+    cfa::DevBuf<int> own_rp, own_ci;
     std::vector<int> colour_start;    // host, nc + 1
     cfa::DevBuf<int> rows, colour, diag, lp, up, lc, uc, l_src, u_src, d_src;
     cfa::DevBuf<double> lu;           // FP64 factor on the CSR pattern
@@ -25,6 +26,7 @@ struct cfa_ilu {
     cfa::DevBuf<int2> upd;            // {b, m}
     int n_elim = 0, n_upd = 0;
     cfa::DevBuf<int> tpos;            // CSR position of the mirrored entry (j, i) of every (i, j)
+    bool mirror = false;              // tpos holds the current pattern's mirror positions
     bool transposed = false;          // the split factor holds (LU)^T (cfa_ilu_factor_transposed)
 };
 

@@ -601,6 +601,32 @@ k_cg_rz(int n, const double* __restrict__ r, const double* __restrict__ z, const
     }
 }
 
+// pq = pn . q when a host-side operator added its part to q after the operator kernel; alpha and
+// the breakdown guard as in k_op_k's DOT epilogue (solve_pcg, src/cfa/linalg.cuh:231-236)
+__global__ void __launch_bounds__(kThreads)
+k_cg_pq(int n, const double* __restrict__ pn, const double* __restrict__ q, CgState* __restrict__ st,
+        double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+    if (st->done) return;
+    __shared__ double sh[kWarps];
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] += pn[i] * q[i];
+    block_sum<1>(v, sh);
+    if (publish_partials<1>(v, part, counter)) {
+        reduce_partials<1>(v, part, counter, sh);
+        if (threadIdx.x == 0) {
+            const double pq = v[0];
+            if (fabs(pq) < 1.0e-30) {
+                st->done = 1;
+                st->converged = 0;
+                st->status = CFA_BREAKDOWN;
+                set_cond(cond, 0);
+            } else {
+                st->alpha = st->rz / pq;
+            }
+        }
+    }
+}
+
 // =============================================================================================
 // two-component BiCGSTAB (GpuBicgstab2::solve, src/cfa/linalg.cuh:656-754)
 // =============================================================================================
@@ -1147,6 +1173,13 @@ struct PcgArgs {
     cfa_amg* amg;
     int max_iter;
     double tol;
+    // host-side hooks (cfa_pcg_solve_host_ops): extra adds its operator into out, prec replaces
+    // the AMG / Jacobi preconditioner
+    cfa_host_op extra = nullptr;
+    void* extra_user = nullptr;
+    cfa_host_op prec = nullptr;
+    void* prec_user = nullptr;
+    bool host_ops() const { return extra || prec; }
 };
 
 #define TILE_TPR_SWITCH(tpr, ...)                                                              \
@@ -1254,12 +1287,22 @@ static cfa_status pcg_init(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg c
     const int* done = &st->done;
     if (W.tiled) CFA_PROPAGATE(pack_operator(ctx, W, a));   // this solve's operator values
     CFA_LAUNCH(ctx, k_cg_bnorm, gv, kThreads, 0, n, a.b, st, W.part.p, W.counter.p, cond);
-    if (!a.amg) CFA_LAUNCH(ctx, k_inv_diag, ceil_div(n, kThreads), kThreads, 0, n, a.rp, a.ci, a.val, W.dinv.p);
+    if (!a.amg && !a.prec) CFA_LAUNCH(ctx, k_inv_diag, ceil_div(n, kThreads), kThreads, 0, n, a.rp, a.ci, a.val, W.dinv.p);
     // q = A x (pn scratch receives x)
     CFA_PROPAGATE(pcg_operator(ctx, W, a, a.x, a.x, nullptr, W.pn.p, W.q.p, false, cond, done));
+    if (a.extra) {
+        CFA_CHECK_LAUNCH();
+        a.extra(a.x, W.q.p, a.extra_user);
+    }
     CFA_LAUNCH(ctx, k_cg_resid0, gv, kThreads, 0, n, a.b, W.q.p, W.r.p, st, W.part.p, W.counter.p, cond);
-    if (a.amg) CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done));
-    else CFA_LAUNCH(ctx, k_vmul, gv, kThreads, 0, n, W.dinv.p, W.r.p, W.z.p);
+    if (a.prec) {
+        CFA_CHECK_LAUNCH();
+        a.prec(W.r.p, W.z.p, a.prec_user);
+    } else if (a.amg) {
+        CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done));
+    } else {
+        CFA_LAUNCH(ctx, k_vmul, gv, kThreads, 0, n, W.dinv.p, W.r.p, W.z.p);
+    }
     CFA_LAUNCH(ctx, k_cg_nullx, ceil_div(n, kThreads), kThreads, 0, n, a.x, W.p.p, st);
     CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 1, 0, st, W.part.p,
                W.counter.p, cond);
@@ -1272,13 +1315,25 @@ static cfa_status pcg_body(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg c
     const int gv = row_grid(ctx, n, 1);
     CgState* st = W.st.p;
     const int* done = &st->done;
-    // q = A pn with pn = z + beta p
-    CFA_PROPAGATE(pcg_operator(ctx, W, a, W.z.p, W.p.p, &st->beta, W.pn.p, W.q.p, true, cond, done));
-    if (a.amg) {
+    // q = A pn with pn = z + beta p (with a host-side extra operator: K pn here, its part added on
+    // the host, then pn . q)
+    CFA_PROPAGATE(pcg_operator(ctx, W, a, W.z.p, W.p.p, &st->beta, W.pn.p, W.q.p, !a.extra, cond, done));
+    if (a.extra) {
+        CFA_CHECK_LAUNCH();
+        a.extra(W.pn.p, W.q.p, a.extra_user);
+        CFA_LAUNCH(ctx, k_cg_pq, gv, kThreads, 0, n, (const double*)W.pn.p, (const double*)W.q.p, st, W.part.p,
+                   W.counter.p, cond);
+    }
+    if (a.amg || a.prec) {
         CFA_LAUNCH(ctx, k_cg_update<false>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p,
                    (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond);
-        CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done));
-        const int flexible = a.amg->opts.precision == CFA_MIXED ? 1 : 0;
+        if (a.prec) {
+            CFA_CHECK_LAUNCH();
+            a.prec(W.r.p, W.z.p, a.prec_user);
+        } else {
+            CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done));
+        }
+        const int flexible = (a.amg && a.amg->opts.precision == CFA_MIXED) ? 1 : 0;
         CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, flexible, st, W.part.p,
                    W.counter.p, cond);
     } else {
@@ -1437,7 +1492,7 @@ static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* re
     CFA_CUDA(cudaMemcpyAsync(W.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
     CFA_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
     long long extra_body = 0;
-    if (graphs_enabled()) {
+    if (graphs_enabled() && !a.host_ops()) {
         const cfa_mesh* om = a.oss ? a.oss->mesh : nullptr;
         std::vector<const void*> key = {a.rp, a.ci, a.val, a.b, a.x, a.oss ? a.oss->d_oss_val : nullptr,
                                         a.oss ? a.oss->d_inv_m : nullptr, (const void*)(intptr_t)(om ? om->uid : 0),
@@ -1765,6 +1820,28 @@ cfa_status cfa_pcg_solve(cfa_ctx* ctx, int n, const int* rp, const int* ci, cons
     CFA_CUDA(cudaMemcpyAsync(&nnz, rp + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     PcgArgs a{n, nnz, rp, ci, val, b, x, oss, amg, opts->max_iter, opts->tol};
+    if (opts->max_iter == 0) {
+        if (rep) { *rep = cfa_solve_report{}; rep->converged[0] = 0; rep->converged[1] = 1; }
+        return CFA_NOT_CONVERGED;
+    }
+    return pcg_solve(ctx, a, rep);
+}
+
+cfa_status cfa_pcg_solve_host_ops(cfa_ctx* ctx, int n, const int* rp, const int* ci, const double* val,
+                                  const double* b, double* x, cfa_host_op extra_op, void* extra_user, cfa_amg* amg,
+                                  cfa_host_op precond, void* precond_user, const cfa_solve_opts* opts,
+                                  cfa_solve_report* rep) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(n > 0 && rp && ci && val && b && x && opts && opts->max_iter >= 0 && !(amg && precond));
+    CFA_ARG(!amg || (amg->coarse_n > 0 && (amg->levels.empty() ? amg->coarse_n == n : amg->levels[0].A.rows == n)));
+    int nnz = 0;
+    CFA_CUDA(cudaMemcpyAsync(&nnz, rp + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    PcgArgs a{n, nnz, rp, ci, val, b, x, nullptr, amg, opts->max_iter, opts->tol};
+    a.extra = extra_op;
+    a.extra_user = extra_user;
+    a.prec = precond;
+    a.prec_user = precond_user;
     if (opts->max_iter == 0) {
         if (rep) { *rep = cfa_solve_report{}; rep->converged[0] = 0; rep->converged[1] = 1; }
         return CFA_NOT_CONVERGED;

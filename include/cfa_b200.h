@@ -274,12 +274,18 @@ cfa_status cfa_spmv_multi(cfa_ctx* ctx, int n, int nrhs, const int* d_row_ptr, c
  * multicolour ILU(0): MulticolourIlu0 (src/cfa/linalg.cuh:435-568)
  * ------------------------------------------------------------------------------------------- */
 /* set_pattern (:456-528): greedy colouring in node order (bit-exact with the reference) from the
- * host copy of the pattern; d_row_ptr/d_col_ind are the same pattern on the device and must
- * outlive the handle. Synchronises. CFA_ROW_TOO_LONG above 32 entries per row. */
+ * host copy of the pattern; d_row_ptr/d_col_ind are the same pattern on the device (kept for the
+ * reference's signature: the handle uploads its own copy from the host arrays, so nothing of the
+ * caller's needs to outlive the call). Synchronises. CFA_ROW_TOO_LONG above 32 entries per row. */
 cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* h_row_ptr, const int* h_col_ind,
                           const int* d_row_ptr, const int* d_col_ind, cfa_precision precision,
                           cfa_ilu** out);
 cfa_status cfa_ilu_destroy(cfa_ilu* ilu);
+/* set_pattern (:456-528) on an existing handle (a new mesh after a remesh): as cfa_ilu_create,
+ * keeping the handle's precision and reusing its device buffers. On failure the handle holds no
+ * usable pattern until a successful call. */
+cfa_status cfa_ilu_set_pattern(cfa_ctx* ctx, cfa_ilu* ilu, int n, const int* h_row_ptr, const int* h_col_ind,
+                               const int* d_row_ptr, const int* d_col_ind);
 /* factor (:531-541): ILU(0) of d_val in colour order, in FP64; the split factors are then kept in
  * the handle's precision. */
 cfa_status cfa_ilu_factor(cfa_ctx* ctx, cfa_ilu* ilu, const double* d_val);
@@ -389,6 +395,25 @@ cfa_status cfa_pcg_solve(cfa_ctx* ctx, int n, const int* d_row_ptr, const int* d
                          const double* d_val, const double* d_b, double* d_x,
                          const cfa_oss_operator* oss, cfa_amg* amg, const cfa_solve_opts* opts,
                          cfa_solve_report* report);
+
+/* Host-side operator hook: a preconditioner writes d_out = M^-1 d_in; an extra operator adds its
+ * part into d_out. Called on the host between this library's launches; the work it enqueues must
+ * run after the context stream's earlier work and before its later work (true for the legacy
+ * default stream when the context owns its stream, cfa_ctx_create(NULL, ...), and for the
+ * context stream itself). */
+typedef void (*cfa_host_op)(const double* d_in, double* d_out, void* user);
+
+/* PCG with the reference's std::function hooks kept as host callbacks (GpuLinearSolver::solve_pcg,
+ * src/cfa/linalg.cuh:183-256, extra_op and precond): A p = K p, then extra_op(p, A p) adds the
+ * matrix-free part; precond, when set, replaces the AMG / Jacobi preconditioner (amg and precond
+ * are exclusive). The kernels of cfa_pcg_solve without the CUDA graph (callbacks cannot be
+ * captured); the stopping test stays on the device, polled every 8 iterations. No counterpart
+ * as a separate entry point in the reference: it is solve_pcg with arbitrary closures. */
+cfa_status cfa_pcg_solve_host_ops(cfa_ctx* ctx, int n, const int* d_row_ptr, const int* d_col_ind,
+                                  const double* d_val, const double* d_b, double* d_x,
+                                  cfa_host_op extra_op, void* extra_user, cfa_amg* amg,
+                                  cfa_host_op precond, void* precond_user, const cfa_solve_opts* opts,
+                                  cfa_solve_report* report);
 
 /* Snapshots the pressure operator's current values into the context's tile-streamed layout
  * (the layout cfa_pcg_solve streams each iteration; one synchronisation when the pattern is

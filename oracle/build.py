@@ -7,11 +7,19 @@
   nothing of it is copied into this repository). Built only where that tree exists; the built
   library travels with the repository to GPU machines.
 
-Run as ``python oracle/build.py [oracle|ref|all]``.
+* ``oracle/_ref/cfa_ref_driver``: the reference's application, built by the one-line recipe of
+  its README (``nvcc -O3 -std=c++17 ... src/cylinder_fem_amr.cu``) for sm_100a.
+* ``oracle/_ref/cfa_dropin_driver``: the same unmodified application source built against this
+  repository's solvers: a temporary mirror of the reference's ``src/`` whose files are links to
+  the originals except ``cfa/linalg.cuh``, which links to ``cylinder-fem-amr_b200/shim/cfa/
+  linalg.cuh``; linked with ``libcfa_b200.so``. The mirror is removed after the build.
+
+Run as ``python oracle/build.py [oracle|ref|drivers|all]``.
 """
 from __future__ import annotations
 
 import os
+import shutil
 import subprocess
 import sys
 
@@ -19,6 +27,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REFERENCE_SRC = "/root/reference/src"
 ORACLE_LIB = os.path.join(HERE, "_build", "libcfa_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libcfa_ref.so")
+REF_DRIVER = os.path.join(HERE, "_ref", "cfa_ref_driver")
+DROPIN_DRIVER = os.path.join(HERE, "_ref", "cfa_dropin_driver")
+ROOT = os.path.dirname(HERE)
+PKG = os.path.join(ROOT, "cylinder-fem-amr_b200")
+SHIM = os.path.join(PKG, "shim", "cfa", "linalg.cuh")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 
@@ -57,9 +70,49 @@ def build_ref(force: bool = False) -> str | None:
     return REF_LIB
 
 
+def _driver_cmd(src: str, out: str, extra: list[str]) -> list[str]:
+    return [NVCC, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "shared",
+            "-Xcompiler", "-fopenmp", *extra, src, "-o", out, "-lgomp"]
+
+
+def build_drivers(force: bool = False) -> tuple[str | None, str | None]:
+    """The reference application as it ships, and the same source on this repository's solvers.
+    Returns (stock, drop-in) paths, None where neither the reference tree nor a prebuilt binary
+    exists."""
+    main = os.path.join(REFERENCE_SRC, "cylinder_fem_amr.cu")
+    if not os.path.exists(main):
+        return (REF_DRIVER if os.path.exists(REF_DRIVER) else None,
+                DROPIN_DRIVER if os.path.exists(DROPIN_DRIVER) else None)
+    cfa_dir = os.path.join(REFERENCE_SRC, "cfa")
+    deps = [main] + [os.path.join(cfa_dir, f) for f in os.listdir(cfa_dir)]
+    os.makedirs(os.path.dirname(REF_DRIVER), exist_ok=True)
+    if force or _stale(REF_DRIVER, deps):
+        subprocess.check_call(_driver_cmd(main, REF_DRIVER, []))
+    lib = os.path.join(PKG, "libcfa_b200.so")
+    header = os.path.join(ROOT, "include", "cfa_b200.h")
+    if force or _stale(DROPIN_DRIVER, deps + [SHIM, lib, header]):
+        mirror = os.path.join(HERE, "_ref", "mirror")
+        if os.path.isdir(mirror):
+            shutil.rmtree(mirror)
+        os.makedirs(os.path.join(mirror, "cfa"))
+        try:
+            os.symlink(main, os.path.join(mirror, "cylinder_fem_amr.cu"))
+            for f in os.listdir(cfa_dir):
+                target = SHIM if f == "linalg.cuh" else os.path.join(cfa_dir, f)
+                os.symlink(target, os.path.join(mirror, "cfa", f))
+            extra = ["-I", os.path.join(ROOT, "include"), "-L", PKG, "-lcfa_b200",
+                     "-Xlinker", "-rpath,$ORIGIN/../../cylinder-fem-amr_b200"]
+            subprocess.check_call(_driver_cmd(os.path.join(mirror, "cylinder_fem_amr.cu"), DROPIN_DRIVER, extra))
+        finally:
+            shutil.rmtree(mirror)
+    return REF_DRIVER, DROPIN_DRIVER
+
+
 if __name__ == "__main__":
     what = sys.argv[1] if len(sys.argv) > 1 else "all"
     if what in ("oracle", "all"):
         print(build_oracle(force=True))
     if what in ("ref", "all"):
         print(build_ref(force=True))
+    if what in ("drivers", "all"):
+        print(build_drivers(force=True))

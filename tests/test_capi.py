@@ -41,3 +41,33 @@ def test_status_strings_and_null_handles():
     assert lib.cfa_ctx_create(None, None) == 7          # CFA_BAD_ARG, no GPU work
     assert lib.cfa_mesh_destroy(None) == 0
     assert lib.cfa_amg_info(None, None, None, None) == 7
+
+
+def test_shim_covers_the_reference_solver_interface():
+    """The drop-in header keeps the reference's class and member names (src/cfa/linalg.cuh) and
+    calls only entry points this library exports."""
+    shim = open(os.path.join(ROOT, "cylinder-fem-amr_b200", "shim", "cfa", "linalg.cuh")).read()
+    for name in ("class GpuLinearSolver", "class MulticolourIlu0", "class GpuBicgstab2", "class AmgPreconditioner",
+                 "int solve_pcg(", "int solve_bicgstab(", "void set_pattern(", "void factor(", "void apply(",
+                 "void setup(", "void remap(", "int num_levels()", "__global__ void k_axpy(", "PH_COUNT",
+                 "last_rel_residual", "colour_ms", "n_colours", "colour_start", "setup_ms", "phase_ms", "remaps",
+                 "coarse_n", "iters[2]"):
+        assert name in shim, name
+    called = set(re.findall(r"\b(cfa_[a-z0-9_]+)\s*\(", shim))
+    assert called <= set(declared()), called - set(declared())
+
+
+def test_dropin_application_links_this_library():
+    """The reference application built on the shim (oracle/build.py drivers) imports the solver
+    entry points from libcfa_b200 and carries none of the reference's solver kernels."""
+    import shutil
+    import subprocess
+    exe = os.path.join(ROOT, "oracle", "_ref", "cfa_dropin_driver")
+    if not os.path.exists(exe) or not shutil.which("nm"):
+        pytest.skip("drop-in application not built")
+    dyn = subprocess.run(["nm", "-D", "--undefined-only", exe], capture_output=True, text=True).stdout
+    for name in ("cfa_pcg_solve_host_ops", "cfa_bicgstab2_solve", "cfa_amg_setup", "cfa_ilu_set_pattern"):
+        assert name in dyn, name
+    syms = subprocess.run(["nm", "-C", exe], capture_output=True, text=True).stdout
+    for kernel in ("k_ilu0_lower_colour", "k_csr_op", "k_multidot2_partial", "k_spmv_csr_multi"):
+        assert kernel not in syms, kernel

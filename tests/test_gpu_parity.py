@@ -209,6 +209,37 @@ def test_ilu_colouring_factor_apply(ctx, precision):
     assert np.abs(host(z) - zo).max() <= tol * np.abs(zo).max()
 
 
+@pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
+def test_ilu_set_pattern_reuses_the_handle(ctx, precision):
+    """set_pattern on a handle that held another (larger) pattern gives the same colouring, factor
+    and sweeps as a fresh handle, and the transposed factor follows the new pattern."""
+    from tests.golden.make_golden import momentum_ilu_matrix
+    big, m = mesh("medium"), mesh("small")
+    rpb, cib = O.csr_build(big.n, big.elem_v)
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    a, b = momentum_ilu_matrix(rp, ci)
+    drp, dci = dev(rp, torch.int32), dev(ci, torch.int32)
+    drpb, dcib = dev(rpb, torch.int32), dev(cib, torch.int32)   # device patterns outlive their use
+    reused = cfa.MulticolourIlu0(ctx, precision)
+    reused.set_pattern(big.n, rpb, cib, drpb, dcib)
+    ab, _ = momentum_ilu_matrix(rpb, cib)
+    reused.factor_transposed(dev(ab))
+    reused.set_pattern(m.n, rp, ci, drp, dci)
+    fresh = cfa.MulticolourIlu0(ctx, precision)
+    fresh.set_pattern(m.n, rp, ci, drp, dci)
+    assert reused.n_colours == fresh.n_colours and np.array_equal(reused.colour_start, fresh.colour_start)
+    out = []
+    for ilu in (reused, fresh):
+        ilu.factor(dev(a))
+        z = torch.zeros(2 * m.n, dtype=torch.float64, device="cuda")
+        ilu.apply(dev(b), z, nrhs=2)
+        ilu.factor_transposed(dev(a))
+        zt = torch.zeros(2 * m.n, dtype=torch.float64, device="cuda")
+        ilu.apply(dev(b), zt, nrhs=2)
+        out.append((host(z), host(zt)))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
 def test_ilu_row_too_long_is_an_error(ctx):
     n = 40
     rp = np.array([0, n] + list(range(n + 1, 2 * n)), np.int32)   # row 0 full, others diagonal
@@ -494,6 +525,41 @@ def test_pcg_matches_oracle(ctx, use_oss, use_amg):
     if use_oss:
         O.oss_apply(m, rp, ci, oss, inv_m, x, Ax)
     assert np.linalg.norm(rhs - Ax) <= 1.5e-10 * np.linalg.norm(rhs)
+
+
+@pytest.mark.parametrize("host_prec", [False, True])
+def test_pcg_host_ops_match_handles(ctx, host_prec):
+    """solve_pcg with the OSS term (and optionally the preconditioner) as host callbacks, the way
+    the reference's std::function hooks call them, against the solve with handles."""
+    import ctypes as C
+    m = mesh("small")
+    dm = cfa.DeviceMesh(ctx, m)
+    rp, ci = dm.host_pattern()
+    Kp, rhs, oss, inv_m = pressure_system(m, rp, ci)
+    dK, db, doss, dinv = dev(Kp), dev(rhs), dev(oss), dev(inv_m)
+    amg = cfa.AmgPreconditioner(ctx)
+    amg.setup(m.n, ci.size, dm.rp, dm.ci, dK)
+    s = cfa.GpuLinearSolver(ctx)
+    x0 = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+    it0 = s.solve_pcg(m.n, dm.rp, dm.ci, dK, db, x0, 4000, 1e-10, cfa.oss_operator(dm, doss, dinv), amg)
+    cb = cfa.Context(stream=ctx.stream)   # the callbacks' own context, on the same stream
+    L = cfa.lib()
+    calls = {"extra": 0, "prec": 0}
+
+    def extra(i, o):
+        calls["extra"] += 1
+        cb.check(L.cfa_oss_apply(cb.h, dm.h, cfa.ptr(doss), cfa.ptr(dinv), C.c_void_p(i), C.c_void_p(o)))
+
+    def prec(i, o):
+        calls["prec"] += 1
+        cb.check(L.cfa_amg_apply(cb.h, amg.h, C.c_void_p(i), C.c_void_p(o)))
+
+    x1 = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+    it1 = s.solve_pcg_host_ops(m.n, dm.rp, dm.ci, dK, db, x1, 4000, 1e-10, extra_op=extra,
+                               amg=None if host_prec else amg, precond=prec if host_prec else None)
+    assert s.converged and abs(it1 - it0) <= 2
+    assert calls["extra"] >= it1 + 1 and (calls["prec"] >= it1 if host_prec else calls["prec"] == 0)
+    assert torch.abs(x1 - x0).max().item() <= 1e-8 * torch.abs(x0).max().item()
 
 
 @pytest.mark.parametrize("name,outlet_dirichlet", [("small", 0), ("medium", 0), ("medium", 1)])
