@@ -1,8 +1,11 @@
-// Multicolour ILU(0): colouring and split pattern on the host exactly as
-// MulticolourIlu0::set_pattern (src/cfa/linalg.cuh:456-528); factor colour by colour in FP64
+// Multicolour ILU(0): the greedy colouring on the host exactly as MulticolourIlu0::set_pattern
+// (src/cfa/linalg.cuh:456-528), the split pattern and elimination program from it on the
+// device (k_ilu_program); factor colour by colour in FP64
 // (k_ilu0_factor_colour, :366-392); sweeps colour by colour with one thread per row handling
 // both right-hand sides, so the factors are read once per apply (the reference's
 // k_ilu0_lower/upper_colour, :406-433, use a thread per row and component and read them twice).
+#include <cub/cub.cuh>
+
 #include <algorithm>
 
 #include "ilu.cuh"
@@ -218,12 +221,72 @@ cfa_status ilu_apply(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z,
     return CFA_OK;
 }
 
+// Split pattern and elimination program of row t (rows in colour order), counted (FILL false)
+// or written (FILL true) at the offsets lp[t], up[t] (= ep[t]: one elimination entry per L
+// entry) and uo[t]. The L entries are taken colour by colour and, within a colour, in column
+// order, and row k's matches in its own order: the operation sequence of the reference's
+// k_ilu0_factor_colour (src/cfa/linalg.cuh:366-392). Thread per row.
+template <bool FILL>
+__global__ void k_ilu_program(int n, const int* __restrict__ rows, const int* __restrict__ rp,
+                              const int* __restrict__ ci, const int* __restrict__ colour, const int* __restrict__ diag,
+                              int* __restrict__ lcnt, int* __restrict__ ucnt, int* __restrict__ ocnt,
+                              const int* __restrict__ lp, const int* __restrict__ up, const int* __restrict__ uo,
+                              int* __restrict__ lc, int* __restrict__ uc, int* __restrict__ l_src,
+                              int* __restrict__ u_src, int* __restrict__ d_src, int4* __restrict__ elim,
+                              int2* __restrict__ upd) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = rows[t];
+    const int s0 = rp[i], len = rp[i + 1] - s0, cii = colour[i];
+    int l = FILL ? lp[t] : 0, u = FILL ? up[t] : 0;
+    for (int a = s0; a < s0 + len; ++a) {
+        const int j = ci[a];
+        if (j == i) {
+            if (FILL) d_src[t] = a;
+        } else if (colour[j] < cii) {
+            if (FILL) { lc[l] = j; l_src[l] = a; }
+            ++l;
+        } else {
+            if (FILL) { uc[u] = j; u_src[u] = a; }
+            ++u;
+        }
+    }
+    int e = FILL ? lp[t] : 0, o = FILL ? uo[t] : 0;
+    for (int c = 0; c < cii; ++c) {
+        for (int q = 0; q < len; ++q) {
+            const int k = ci[s0 + q];
+            if (colour[k] != c) continue;
+            const int o0 = o;
+            // rows k and i are sorted: one merge finds the common columns
+            for (int mm = rp[k], b = 0; mm < rp[k + 1] && b < len;) {
+                const int j = ci[mm], cb = ci[s0 + b];
+                if (cb < j) { ++b; continue; }
+                if (cb == j && colour[j] > c) {
+                    if (FILL) upd[o] = make_int2(b, mm);
+                    ++o;
+                }
+                ++mm;
+            }
+            if (FILL) elim[e] = make_int4(q, diag[k], o0, o);
+            ++e;
+        }
+    }
+    if (!FILL) {
+        lcnt[t] = l;
+        ucnt[t] = u;
+        ocnt[t] = o;
+    }
+}
+
 // set_pattern (src/cfa/linalg.cuh:456-528) into handle h, reusing its device buffers (they grow
-// geometrically, as the reference's cap_n / cap_nnz)
+// geometrically, as the reference's cap_n / cap_nnz). The greedy colouring (sequential by
+// definition) runs on the host in node order; the split pattern and the elimination program
+// are built on the device from it.
 static cfa_status ilu_pattern(cfa_ctx* ctx, cfa_ilu* h, int n, const int* rp, const int* ci, const int* d_rp,
                               const int* d_ci) {
+    (void)d_rp;
+    (void)d_ci;
     const int nnz = rp[n];
-    const cfa_precision precision = h->precision;
     std::vector<int> colour(n, -1), diag(n, -1), mark;
     int nc = 0;
     for (int i = 0; i < n; ++i) {
@@ -242,9 +305,9 @@ static cfa_status ilu_pattern(cfa_ctx* ctx, cfa_ilu* h, int n, const int* rp, co
     for (int r = 0; r < n; ++r)
         if (diag[r] < 0) return set_error(ctx, CFA_BAD_ARG, "ILU pattern row without a diagonal", __FILE__, __LINE__);
     h->uid = next_uid();
-    h->n = n; h->nnz = nnz; h->nc = nc;
-    (void)d_rp;
-    (void)d_ci;
+    h->n = n;
+    h->nnz = nnz;
+    h->nc = nc;
     h->mirror = false;
     h->transposed = false;
     h->colour_start.assign(nc + 1, 0);
@@ -252,99 +315,82 @@ static cfa_status ilu_pattern(cfa_ctx* ctx, cfa_ilu* h, int n, const int* rp, co
     for (int c = 0; c < nc; ++c) h->colour_start[c + 1] += h->colour_start[c];
     std::vector<int> rows(n), fill(h->colour_start.begin(), h->colour_start.end() - 1);
     for (int i = 0; i < n; ++i) rows[fill[colour[i]]++] = i;
-    std::vector<int> lp(n + 1, 0), up(n + 1, 0);
-    for (int t = 0; t < n; ++t) {
-        const int i = rows[t];
-        int l = 0, u = 0;
-        for (int a = rp[i]; a < rp[i + 1]; ++a) {
-            if (ci[a] == i) continue;
-            if (colour[ci[a]] < colour[i]) ++l; else ++u;
-        }
-        lp[t + 1] = l; up[t + 1] = u;
-    }
-    for (int t = 0; t < n; ++t) { lp[t + 1] += lp[t]; up[t + 1] += up[t]; }
-    h->nl = lp[n]; h->nu = up[n];
-    std::vector<int> lc(h->nl), uc(h->nu), l_src(h->nl), u_src(h->nu), d_src(n);
-    for (int t = 0; t < n; ++t) {
-        const int i = rows[t];
-        int l = lp[t], u = up[t];
-        for (int a = rp[i]; a < rp[i + 1]; ++a) {
-            const int j = ci[a];
-            if (j == i) d_src[t] = a;
-            else if (colour[j] < colour[i]) { lc[l] = j; l_src[l++] = a; }
-            else { uc[u] = j; u_src[u++] = a; }
-        }
-    }
-    // elimination program (symbolic ILU(0)): the operation sequence of the reference's factor kernel
-    std::vector<int> ep(n + 1, 0);
-    std::vector<int4> elim;
-    std::vector<int2> updv;
-    elim.reserve((size_t)h->nl);
-    for (int t = 0; t < n; ++t) {
-        const int i = rows[t];
-        const int s0 = rp[i], len = rp[i + 1] - s0, cii = colour[i];
-        for (int c = 0; c < cii; ++c) {
-            for (int q = 0; q < len; ++q) {
-                const int k = ci[s0 + q];
-                if (colour[k] != c) continue;
-                int4 el;
-                el.x = q;
-                el.y = diag[k];
-                el.z = (int)updv.size();
-                // rows k and i are sorted: one merge finds the common columns, in row k's order
-                for (int mm = rp[k], b = 0; mm < rp[k + 1] && b < len;) {
-                    const int j = ci[mm], cb = ci[s0 + b];
-                    if (cb < j) { ++b; continue; }
-                    if (cb == j && colour[j] > c) updv.push_back(make_int2(b, mm));
-                    ++mm;
-                }
-                el.w = (int)updv.size();
-                elim.push_back(el);
-            }
-        }
-        ep[t + 1] = (int)elim.size();
-    }
-    h->n_elim = (int)elim.size();
-    h->n_upd = (int)updv.size();
-    cudaError_t e = cudaSuccess;
-    auto up_int = [&](DevBuf<int>& d, const std::vector<int>& v) {
-        if (e != cudaSuccess) return;
-        e = d.ensure(std::max<size_t>(v.size(), 1));
-        if (e == cudaSuccess && !v.empty())
-            e = cudaMemcpyAsync(d.p, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
-    };
+
     // the handle's own copy of the pattern (the reference keeps the caller's device arrays; a
-    // copy leaves nothing for the caller to keep alive)
-    const std::vector<int> rp_v(rp, rp + n + 1), ci_v(ci, ci + nnz);
-    up_int(h->own_rp, rp_v);
-    up_int(h->own_ci, ci_v);
+    // copy leaves nothing for the caller to keep alive), the colouring and the row order
+    auto up_int = [&](DevBuf<int>& d, const int* v, size_t count) -> cudaError_t {
+        cudaError_t e = d.ensure(std::max<size_t>(count, 1));
+        if (e == cudaSuccess && count)
+            e = cudaMemcpyAsync(d.p, v, count * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+        return e;
+    };
+    CFA_CUDA(up_int(h->own_rp, rp, (size_t)n + 1));
+    CFA_CUDA(up_int(h->own_ci, ci, (size_t)nnz));
     h->rp = h->own_rp.p;
     h->ci = h->own_ci.p;
-    up_int(h->rows, rows); up_int(h->colour, colour); up_int(h->diag, diag); up_int(h->lp, lp); up_int(h->up, up);
-    up_int(h->lc, lc); up_int(h->uc, uc); up_int(h->l_src, l_src); up_int(h->u_src, u_src); up_int(h->d_src, d_src);
-    up_int(h->ep, ep);
-    if (e == cudaSuccess) e = h->elim.ensure(std::max<size_t>(elim.size(), 1));
-    if (e == cudaSuccess && !elim.empty())
-        e = cudaMemcpyAsync(h->elim.p, elim.data(), elim.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = h->upd.ensure(std::max<size_t>(updv.size(), 1));
-    if (e == cudaSuccess && !updv.empty())
-        e = cudaMemcpyAsync(h->upd.p, updv.data(), updv.size() * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = h->lu.ensure(nnz);
-    if (precision == CFA_MIXED) {
-        if (e == cudaSuccess) e = h->lv32.ensure(std::max(h->nl, 1));
-        if (e == cudaSuccess) e = h->uv32.ensure(std::max(h->nu, 1));
-        if (e == cudaSuccess) e = h->dinv32.ensure(n);
-        if (e == cudaSuccess) e = h->work32.ensure(2 * (size_t)n);
+    CFA_CUDA(up_int(h->rows, rows.data(), n));
+    CFA_CUDA(up_int(h->colour, colour.data(), n));
+    CFA_CUDA(up_int(h->diag, diag.data(), n));
+
+    // counts, offsets (exclusive sums into lp, up, ep and the update offsets), totals
+    DevBuf<int> cnt;   // lcnt | ucnt | ocnt, n + 1 each
+    CFA_CUDA(cnt.ensure(3 * ((size_t)n + 1)));
+    int* lcnt = cnt.p;
+    int* ucnt = cnt.p + (n + 1);
+    int* ocnt = cnt.p + 2 * (size_t)(n + 1);
+    CFA_CUDA(cudaMemsetAsync(cnt.p, 0, 3 * ((size_t)n + 1) * sizeof(int), ctx->stream));
+    CFA_CUDA(h->lp.ensure(n + 1));
+    CFA_CUDA(h->up.ensure(n + 1));
+    CFA_CUDA(h->ep.ensure(n + 1));
+    DevBuf<int> uo;
+    CFA_CUDA(uo.ensure(n + 1));
+    CFA_LAUNCH(ctx, k_ilu_program<false>, ceil_div(n, kThreads), kThreads, 0, n, (const int*)h->rows.p, h->rp, h->ci,
+               (const int*)h->colour.p, (const int*)h->diag.p, lcnt, ucnt, ocnt, (const int*)nullptr,
+               (const int*)nullptr, (const int*)nullptr, (int*)nullptr, (int*)nullptr, (int*)nullptr, (int*)nullptr,
+               (int*)nullptr, (int4*)nullptr, (int2*)nullptr);
+    size_t tmp_bytes = 0;
+    CFA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, lcnt, h->lp.p, n + 1, ctx->stream));
+    DevBuf<unsigned char> tmp;
+    CFA_CUDA(tmp.ensure(std::max<size_t>(tmp_bytes, 1)));
+    CFA_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tmp_bytes, lcnt, h->lp.p, n + 1, ctx->stream));
+    CFA_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tmp_bytes, ucnt, h->up.p, n + 1, ctx->stream));
+    CFA_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tmp_bytes, ocnt, uo.p, n + 1, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(h->ep.p, h->lp.p, ((size_t)n + 1) * sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
+    int tot[3] = {0, 0, 0};
+    CFA_CUDA(cudaMemcpyAsync(&tot[0], h->lp.p + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(&tot[1], h->up.p + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(&tot[2], uo.p + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    h->nl = tot[0];
+    h->nu = tot[1];
+    h->n_elim = tot[0];
+    h->n_upd = tot[2];
+
+    for (DevBuf<int>* b : {&h->lc, &h->l_src}) CFA_CUDA(b->ensure(std::max(h->nl, 1)));
+    for (DevBuf<int>* b : {&h->uc, &h->u_src}) CFA_CUDA(b->ensure(std::max(h->nu, 1)));
+    CFA_CUDA(h->d_src.ensure(n));
+    CFA_CUDA(h->elim.ensure(std::max(h->n_elim, 1)));
+    CFA_CUDA(h->upd.ensure(std::max(h->n_upd, 1)));
+    CFA_LAUNCH(ctx, k_ilu_program<true>, ceil_div(n, kThreads), kThreads, 0, n, (const int*)h->rows.p, h->rp, h->ci,
+               (const int*)h->colour.p, (const int*)h->diag.p, (int*)nullptr, (int*)nullptr, (int*)nullptr,
+               (const int*)h->lp.p, (const int*)h->up.p, (const int*)uo.p, h->lc.p, h->uc.p, h->l_src.p, h->u_src.p,
+               h->d_src.p, h->elim.p, h->upd.p);
+    CFA_CUDA(h->lu.ensure(nnz));
+    if (h->precision == CFA_MIXED) {
+        CFA_CUDA(h->lv32.ensure(std::max(h->nl, 1)));
+        CFA_CUDA(h->uv32.ensure(std::max(h->nu, 1)));
+        CFA_CUDA(h->dinv32.ensure(n));
+        CFA_CUDA(h->work32.ensure(2 * (size_t)n));
     } else {
-        if (e == cudaSuccess) e = h->lv64.ensure(std::max(h->nl, 1));
-        if (e == cudaSuccess) e = h->uv64.ensure(std::max(h->nu, 1));
-        if (e == cudaSuccess) e = h->dinv64.ensure(n);
+        CFA_CUDA(h->lv64.ensure(std::max(h->nl, 1)));
+        CFA_CUDA(h->uv64.ensure(std::max(h->nu, 1)));
+        CFA_CUDA(h->dinv64.ensure(n));
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) return set_error(ctx, CFA_CUDA_ERROR, cudaGetErrorString(e), __FILE__, __LINE__);
+    CFA_CHECK_LAUNCH();
+    // the scratch buffers (cnt, uo, tmp) are released on return: wait for the kernels using them
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     return CFA_OK;
 }
-
 
 }  // namespace cfa
 

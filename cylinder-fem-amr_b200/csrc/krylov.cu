@@ -1056,6 +1056,19 @@ struct GraphCache {
     ~GraphCache() { reset(); }
 };
 
+// A straight-line captured graph (no conditional node), replayed while its key holds
+struct SegGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void*> key;
+    long long kernels = 0;
+    void reset() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        key.clear();
+    }
+    ~SegGraph() { reset(); }
+};
+
 struct PcgWork {
     int cap = 0;
     DevBuf<double> r, z, p, pn, q, gx, gy, dinv;
@@ -1074,6 +1087,8 @@ struct PcgWork {
     DevBuf<double> part;
     DevBuf<unsigned int> counter;
     GraphCache graph;
+    SegGraph seg[3];   // the pieces of one iteration between host hooks (cfa_pcg_solve_host_ops)
+    DevBuf<unsigned long long> fp;
 };
 
 struct B2Work {
@@ -1163,6 +1178,30 @@ static cfa_status build_graph(cfa_ctx* ctx, GraphCache& gc, Init init, Body body
 // ---------------------------------------------------------------------------------------------
 // PCG
 // ---------------------------------------------------------------------------------------------
+// Order-free fingerprint of a CSR pattern: the sum (mod 2^64) of a 64-bit mix of every
+// (position, value) of row_ptr and col_ind; the mix is the splitmix64 finalizer (Steele, Lea and
+// Flood, "Fast splittable pseudorandom number generators", OOPSLA 2014).
+__device__ __forceinline__ unsigned long long fp_mix(unsigned long long z) {
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+__global__ void k_pattern_fingerprint(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                      unsigned long long* __restrict__ out) {
+    const long long total = (long long)n + 1 + rp[n];
+    unsigned long long h = 0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
+         k += (long long)gridDim.x * blockDim.x) {
+        if (k <= n) h += fp_mix(((unsigned long long)k << 32) ^ (unsigned)rp[k]);
+        else h += fp_mix((((unsigned long long)(k - n - 1)) << 32) ^ (unsigned)ci[k - n - 1] ^ 0xa5a5a5a5a5a5a5a5ull);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o /= 2) h += __shfl_down_sync(0xffffffffu, h, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, h);
+}
+
 struct PcgArgs {
     int n, nnz;
     const int *rp, *ci;
@@ -1179,6 +1218,7 @@ struct PcgArgs {
     void* extra_user = nullptr;
     cfa_host_op prec = nullptr;
     void* prec_user = nullptr;
+    unsigned long long fp = 0;   // fingerprint of the pattern (rp, ci): plans follow its content
     bool host_ops() const { return extra || prec; }
 };
 
@@ -1310,37 +1350,94 @@ static cfa_status pcg_init(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg c
     return CFA_OK;
 }
 
-static cfa_status pcg_body(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg cond) {
+// One iteration in the pieces that the host hooks separate: piece 0 is the operator (with the
+// dot unless an extra operator follows), then extra(pn, q); piece 1 is pq, the update and the
+// preconditioner unless it is a host hook, then prec(r, z); piece 2 is r.z after a host
+// preconditioner (empty otherwise).
+static bool pcg_piece_empty(const PcgArgs& a, int piece) { return piece == 2 && !a.prec; }
+
+static cfa_status pcg_piece(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, int piece, CondArg cond) {
     const int n = a.n;
     const int gv = row_grid(ctx, n, 1);
     CgState* st = W.st.p;
     const int* done = &st->done;
-    // q = A pn with pn = z + beta p (with a host-side extra operator: K pn here, its part added on
-    // the host, then pn . q)
-    CFA_PROPAGATE(pcg_operator(ctx, W, a, W.z.p, W.p.p, &st->beta, W.pn.p, W.q.p, !a.extra, cond, done));
-    if (a.extra) {
-        CFA_CHECK_LAUNCH();
-        a.extra(W.pn.p, W.q.p, a.extra_user);
-        CFA_LAUNCH(ctx, k_cg_pq, gv, kThreads, 0, n, (const double*)W.pn.p, (const double*)W.q.p, st, W.part.p,
-                   W.counter.p, cond);
-    }
-    if (a.amg || a.prec) {
-        CFA_LAUNCH(ctx, k_cg_update<false>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p,
-                   (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond);
-        if (a.prec) {
-            CFA_CHECK_LAUNCH();
-            a.prec(W.r.p, W.z.p, a.prec_user);
+    if (piece == 0) {
+        // q = A pn with pn = z + beta p
+        CFA_PROPAGATE(pcg_operator(ctx, W, a, W.z.p, W.p.p, &st->beta, W.pn.p, W.q.p, !a.extra, cond, done));
+    } else if (piece == 1) {
+        if (a.extra)
+            CFA_LAUNCH(ctx, k_cg_pq, gv, kThreads, 0, n, (const double*)W.pn.p, (const double*)W.q.p, st, W.part.p,
+                       W.counter.p, cond);
+        if (a.amg || a.prec) {
+            CFA_LAUNCH(ctx, k_cg_update<false>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p,
+                       (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond);
+            if (!a.prec) {
+                CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done));
+                const int flexible = a.amg->opts.precision == CFA_MIXED ? 1 : 0;
+                CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, flexible, st,
+                           W.part.p, W.counter.p, cond);
+            }
         } else {
-            CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done));
+            CFA_LAUNCH(ctx, k_cg_update<true>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p, W.dinv.p, W.z.p,
+                       st, W.part.p, W.counter.p, cond);
         }
-        const int flexible = (a.amg && a.amg->opts.precision == CFA_MIXED) ? 1 : 0;
-        CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, flexible, st, W.part.p,
+    } else if (a.prec) {
+        CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, 0, st, W.part.p,
                    W.counter.p, cond);
-    } else {
-        CFA_LAUNCH(ctx, k_cg_update<true>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p, W.dinv.p, W.z.p, st,
-                   W.part.p, W.counter.p, cond);
     }
     CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+static void pcg_hook(const PcgArgs& a, PcgWork& W, int after_piece) {
+    if (after_piece == 0 && a.extra) a.extra(W.pn.p, W.q.p, a.extra_user);
+    if (after_piece == 1 && a.prec) a.prec(W.r.p, W.z.p, a.prec_user);
+}
+
+static cfa_status pcg_body(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg cond) {
+    for (int piece = 0; piece < 3; ++piece) {
+        if (pcg_piece_empty(a, piece)) continue;
+        CFA_PROPAGATE(pcg_piece(ctx, W, a, piece, cond));
+        pcg_hook(a, W, piece);
+    }
+    return CFA_OK;
+}
+
+// Replays `sg` (capturing it first when its key changed)
+template <class F>
+static cfa_status run_segment(cfa_ctx* ctx, SegGraph& sg, const std::vector<const void*>& key, F fn) {
+    if (!sg.exec || sg.key != key) {
+        sg.reset();
+        const long long l0 = ctx->launches;
+        CFA_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        const cfa_status s = fn();
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        sg.kernels = ctx->launches - l0;
+        ctx->launches = l0;
+        if (s != CFA_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            if (s != CFA_OK) return s;
+            CFA_CUDA(e);
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&sg.exec, g, 0);
+        cudaGraphDestroy(g);
+        CFA_CUDA(ei);
+        sg.key = key;
+    }
+    CFA_CUDA(cudaGraphLaunch(sg.exec, ctx->stream));
+    ctx->launches += sg.kernels;
+    return CFA_OK;
+}
+
+// The iteration with host hooks: each piece a captured graph, the hooks called between them
+static cfa_status pcg_body_segments(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, const std::vector<const void*>& key) {
+    CondArg none{0, 0};
+    for (int piece = 0; piece < 3; ++piece) {
+        if (pcg_piece_empty(a, piece)) continue;
+        CFA_PROPAGATE(run_segment(ctx, W.seg[piece], key, [&] { return pcg_piece(ctx, W, a, piece, none); }));
+        pcg_hook(a, W, piece);
+    }
     return CFA_OK;
 }
 
@@ -1353,6 +1450,7 @@ static std::vector<const void*> operator_key(int n, int nnz, const int* rp, cons
 static cfa_status ensure_pcg_vectors(cfa_ctx* ctx, PcgWork& W, int n) {
     if (n > W.cap) {
         W.graph.reset();
+        for (SegGraph& g : W.seg) g.reset();
         for (DevBuf<double>* b : {&W.r, &W.z, &W.p, &W.pn, &W.q, &W.gx, &W.gy, &W.dinv}) CFA_CUDA(b->ensure(n));
         CFA_CUDA(W.st.ensure(1));
         CFA_CUDA(W.counter.ensure(1));
@@ -1449,7 +1547,7 @@ static cfa_status plan_operator_tiles(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a
     if (!W.tiled) return CFA_OK;
     allow_operator_kernels();
     std::vector<const void*> key = {a.rp, a.ci, (const void*)(intptr_t)a.n, (const void*)(intptr_t)a.nnz,
-                                    (const void*)(intptr_t)(a.oss ? 1 : 0)};
+                                    (const void*)(intptr_t)(a.oss ? 1 : 0), (const void*)(uintptr_t)a.fp};
     if (key == W.tile_key) return CFA_OK;
     std::vector<int> h_rp(a.n + 1);
     CFA_CUDA(cudaMemcpyAsync(h_rp.data(), a.rp, (a.n + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1476,6 +1574,23 @@ static cfa_status plan_operator_tiles(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a
     }
     W.tile_key = key;
     W.graph.reset();
+    for (SegGraph& g : W.seg) g.reset();
+    return CFA_OK;
+}
+
+// nnz = rp[n] and the pattern's fingerprint, one synchronisation
+static cfa_status pattern_info(cfa_ctx* ctx, int n, const int* rp, const int* ci, int& nnz, unsigned long long& fp) {
+    PcgWork& W = work(ctx)->pcg;
+    CFA_CUDA(W.fp.ensure(1));
+    CFA_CUDA(cudaMemsetAsync(W.fp.p, 0, sizeof(unsigned long long), ctx->stream));
+    CFA_LAUNCH(ctx, k_pattern_fingerprint, std::min(ceil_div(8 * n + 1, kThreads), 4 * ctx->num_sms), kThreads, 0, n, rp,
+               ci, W.fp.p);
+    CFA_CUDA(cudaMemcpyAsync(&ctx->h_pinned[0], W.fp.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    CFA_CUDA(cudaMemcpyAsync(&ctx->h_pinned[1], rp + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(&fp, &ctx->h_pinned[0], sizeof(fp));
+    std::memcpy(&nnz, &ctx->h_pinned[1], sizeof(nnz));
     return CFA_OK;
 }
 
@@ -1492,14 +1607,16 @@ static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* re
     CFA_CUDA(cudaMemcpyAsync(W.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
     CFA_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
     long long extra_body = 0;
+    const cfa_mesh* om = a.oss ? a.oss->mesh : nullptr;
+    const std::vector<const void*> key = {a.rp, a.ci, a.val, a.b, a.x, a.oss ? a.oss->d_oss_val : nullptr,
+                                          a.oss ? a.oss->d_inv_m : nullptr, (const void*)(intptr_t)(om ? om->uid : 0),
+                                          (const void*)(intptr_t)(om ? om->bc.outlet_dirichlet : 0),
+                                          (const void*)(intptr_t)(om ? om->bc.pin : 0),
+                                          (const void*)(intptr_t)(a.amg ? a.amg->version : 0),
+                                          (const void*)(intptr_t)n, (const void*)(intptr_t)a.nnz,
+                                          (const void*)(intptr_t)((a.extra ? 1 : 0) | (a.prec ? 2 : 0)),
+                                          (const void*)(uintptr_t)a.fp};
     if (graphs_enabled() && !a.host_ops()) {
-        const cfa_mesh* om = a.oss ? a.oss->mesh : nullptr;
-        std::vector<const void*> key = {a.rp, a.ci, a.val, a.b, a.x, a.oss ? a.oss->d_oss_val : nullptr,
-                                        a.oss ? a.oss->d_inv_m : nullptr, (const void*)(intptr_t)(om ? om->uid : 0),
-                                        (const void*)(intptr_t)(om ? om->bc.outlet_dirichlet : 0),
-                                        (const void*)(intptr_t)(om ? om->bc.pin : 0),
-                                        (const void*)(intptr_t)(a.amg ? a.amg->version : 0),
-                                        (const void*)(intptr_t)n, (const void*)(intptr_t)a.nnz};
         if (!W.graph.exec || W.graph.key != key) {
             CFA_PROPAGATE(build_graph(ctx, W.graph, [&](CondArg c) { return pcg_init(ctx, W, a, c); },
                                       [&](CondArg c) { return pcg_body(ctx, W, a, c); }));
@@ -1514,8 +1631,10 @@ static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* re
         CFA_PROPAGATE(pcg_init(ctx, W, a, none));
         (void)l0;
         int polled = 0;
+        const bool segments = graphs_enabled();   // host hooks: one graph per piece of the iteration
         for (int it = 0; it < a.max_iter; ++it) {
-            CFA_PROPAGATE(pcg_body(ctx, W, a, none));
+            if (segments) CFA_PROPAGATE(pcg_body_segments(ctx, W, a, key));
+            else CFA_PROPAGATE(pcg_body(ctx, W, a, none));
             if (++polled == 8 || it + 1 == a.max_iter) {
                 polled = 0;
                 int d = 0;
@@ -1600,7 +1719,10 @@ static cfa_status plan_b2_tiles(cfa_ctx* ctx, B2Work& W, const B2Args& a) {
         CFA_CUDA(W.err.ensure(1));
         CFA_CUDA(cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream));
     }
-    std::vector<const void*> key = {a.rp, a.ci, (const void*)(intptr_t)a.n, (const void*)(intptr_t)a.nnz};
+    // the ILU handle's uid changes with every set_pattern, and its pattern is the matrix's, so a
+    // new mesh at the same addresses gets a new plan
+    std::vector<const void*> key = {a.rp, a.ci, (const void*)(intptr_t)a.n, (const void*)(intptr_t)a.nnz,
+                                    (const void*)(intptr_t)a.ilu->uid};
     if (key == W.tile_key) return CFA_OK;
     std::vector<int> h_rp(a.n + 1);
     CFA_CUDA(cudaMemcpyAsync(h_rp.data(), a.rp, (a.n + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1752,7 +1874,12 @@ cfa_status cfa_pressure_operator_prepare(cfa_ctx* ctx, int n, int nnz, const int
     CFA_ARG(!oss || (oss->mesh && oss->d_oss_val && oss->d_inv_m && oss->mesh->n == n));
     PcgWork& W = work(ctx)->pcg;
     CFA_PROPAGATE(ensure_pcg_vectors(ctx, W, n));
+    int nnz_dev = 0;
+    unsigned long long fp = 0;
+    CFA_PROPAGATE(pattern_info(ctx, n, rp, ci, nnz_dev, fp));
+    CFA_ARG(nnz_dev == nnz);
     PcgArgs a{n, nnz, rp, ci, val, nullptr, nullptr, oss, nullptr, 0, 0.0};
+    a.fp = fp;
     CFA_PROPAGATE(plan_operator_tiles(ctx, W, a));
     W.prepared.clear();
     if (!W.tiled) return CFA_OK;
@@ -1817,9 +1944,10 @@ cfa_status cfa_pcg_solve(cfa_ctx* ctx, int n, const int* rp, const int* ci, cons
     CFA_ARG(!oss || (oss->mesh && oss->d_oss_val && oss->d_inv_m && oss->mesh->n == n));
     CFA_ARG(!amg || (amg->coarse_n > 0 && (amg->levels.empty() ? amg->coarse_n == n : amg->levels[0].A.rows == n)));
     int nnz = 0;
-    CFA_CUDA(cudaMemcpyAsync(&nnz, rp + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    unsigned long long fp = 0;
+    CFA_PROPAGATE(pattern_info(ctx, n, rp, ci, nnz, fp));
     PcgArgs a{n, nnz, rp, ci, val, b, x, oss, amg, opts->max_iter, opts->tol};
+    a.fp = fp;
     if (opts->max_iter == 0) {
         if (rep) { *rep = cfa_solve_report{}; rep->converged[0] = 0; rep->converged[1] = 1; }
         return CFA_NOT_CONVERGED;
@@ -1835,9 +1963,10 @@ cfa_status cfa_pcg_solve_host_ops(cfa_ctx* ctx, int n, const int* rp, const int*
     CFA_ARG(n > 0 && rp && ci && val && b && x && opts && opts->max_iter >= 0 && !(amg && precond));
     CFA_ARG(!amg || (amg->coarse_n > 0 && (amg->levels.empty() ? amg->coarse_n == n : amg->levels[0].A.rows == n)));
     int nnz = 0;
-    CFA_CUDA(cudaMemcpyAsync(&nnz, rp + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    unsigned long long fp = 0;
+    CFA_PROPAGATE(pattern_info(ctx, n, rp, ci, nnz, fp));
     PcgArgs a{n, nnz, rp, ci, val, b, x, nullptr, amg, opts->max_iter, opts->tol};
+    a.fp = fp;
     a.extra = extra_op;
     a.extra_user = extra_user;
     a.prec = precond;

@@ -562,6 +562,34 @@ def test_pcg_host_ops_match_handles(ctx, host_prec):
     assert torch.abs(x1 - x0).max().item() <= 1e-8 * torch.abs(x0).max().item()
 
 
+def test_pcg_new_pattern_at_the_same_addresses(ctx):
+    """A different pattern with the same n and nnz written into the same device arrays (a remesh
+    that lands on recycled buffers) is solved with its own tile plan, not the cached one."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    m = mesh("small")
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    perm = np.random.default_rng(5).permutation(m.n).astype(np.int32)
+    rp2, ci2 = O.csr_build(m.n, perm[m.elem_v])
+    assert ci2.size == ci.size and not np.array_equal(rp, rp2)
+    drp, dci = dev(rp, torch.int32), dev(ci, torch.int32)
+    dval = torch.zeros(ci.size, dtype=torch.float64, device="cuda")
+    b = F.fourier_field(m.x, m.y, 4)
+    db = dev(b)
+    s = cfa.GpuLinearSolver(ctx)
+    for r, c in ((rp, ci), (rp2, ci2)):
+        rows = np.repeat(np.arange(m.n), np.diff(r))
+        val = np.where(c == rows, np.diff(r)[rows].astype(np.float64), -1.0)   # SPD, diagonally dominant
+        drp.copy_(torch.from_numpy(r))
+        dci.copy_(torch.from_numpy(c))
+        dval.copy_(torch.from_numpy(val))
+        x = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+        s.solve_pcg(m.n, drp, dci, dval, db, x, 2000, 1e-12)
+        assert s.converged
+        want = spl.spsolve(sp.csr_matrix((val, c, r), shape=(m.n, m.n)).tocsc(), b)
+        assert np.abs(host(x) - want).max() <= 1e-9 * np.abs(want).max()
+
+
 @pytest.mark.parametrize("name,outlet_dirichlet", [("small", 0), ("medium", 0), ("medium", 1)])
 def test_pressure_operator_fused_oss_matches_oracle(name, outlet_dirichlet, monkeypatch):
     """K - B^T M^-1 B assembled into one two-ring matrix (the default) and the two-pass apply
