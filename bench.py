@@ -339,21 +339,25 @@ def run_reference(args):
 # ------------------------------------------------------------------------------------------------
 # bandwidth stress (c2): ~4M vertices, repeated solves with perturbed right-hand sides
 # ------------------------------------------------------------------------------------------------
-def vcycle_bytes(levels, coarse_n, vb):
+def vcycle_bytes(levels, coarse_n, vb, eb=8):
     """Algorithmic bytes of one V(2,2) cycle of the tile kernels: per level with n rows, z entries
-    of A and q of P (= of R), values of vb bytes: pre-smoothing (initial guess fused), residual,
-    restriction, prolongation-add and two post-smoothing sweeps, each reading its matrix once
-    (column index + value, row offsets) and its vectors (8 bytes per entry read or written);
-    the dense coarse solve reads its inverse."""
+    of A and q of P (= of R), values of vb bytes, vectors of eb bytes (8, or 4 for the FP32 V-cycle
+    of mixed precision, whose level 0 still reads the FP64 right-hand side and writes the FP64
+    result): pre-smoothing (initial guess fused), residual, restriction, prolongation-add and two
+    post-smoothing sweeps, each reading its matrix once (column index + value, row offsets) and
+    its vectors once per entry read or written; the dense coarse solve reads its FP64 inverse."""
     total = 0
-    for (n, z, nc, q) in levels:
+    for lvl, (n, z, nc, q) in enumerate(levels):
+        bb = 8 if lvl == 0 else eb                       # the level's right-hand side
+        zb = 8 if lvl == 0 else eb                       # the last sweep's output
         mat_a = z * (vb + 4) + 4 * (n + 1)
-        total += mat_a + 8 * n * 4                       # pre: b, dinv, b (own), x write
-        total += mat_a + 8 * n * 3                       # residual: x, b, r write
-        total += q * (vb + 4) + 4 * (nc + 1) + 8 * n + 8 * nc          # restriction
-        total += q * (vb + 4) + 4 * (n + 1) + 8 * nc + 16 * n          # prolongation-add
-        total += 2 * (mat_a + 8 * n * 4)                 # two Jacobi sweeps: x, b, dinv, out
-    return total + 8 * coarse_n * coarse_n + 16 * coarse_n
+        total += mat_a + n * (bb + eb + bb + eb)         # pre: b, dinv (gathered), b (own), x write
+        total += mat_a + n * (eb + bb + eb)              # residual: x, b, r write
+        total += q * (vb + 4) + 4 * (nc + 1) + eb * n + eb * nc          # restriction
+        total += q * (vb + 4) + 4 * (n + 1) + eb * nc + 2 * eb * n       # prolongation-add
+        total += mat_a + n * (eb + bb + eb + eb)         # Jacobi sweep: x, b, dinv, out
+        total += mat_a + n * (eb + bb + eb + zb)         # last sweep
+    return total + 8 * coarse_n * coarse_n + 2 * eb * coarse_n
 
 
 def run_stress(args, rank, world):
@@ -431,7 +435,8 @@ def run_stress(args, rank, world):
     for l in range(st.amg.num_levels() - 1):
         d = st.amg.level(l)
         levels.append((d["rows"], int(d["A"][1].numel()), d["pcols"], int(d["P"][1].numel())))
-    b_vc = vcycle_bytes(levels, st.amg.coarse_n, 4)
+    fp32_vectors = os.environ.get("CFA_VCYCLE_FP64", "0") != "1"   # the mixed V-cycle's vectors
+    b_vc = vcycle_bytes(levels, st.amg.coarse_n, 4, 4 if fp32_vectors else 8)
     x2 = torch.randn(2 * n, dtype=torch.float64, device="cuda")
     z2 = torch.empty_like(x2)
     t_ilu = timed(lambda: st.ilu.apply(x2, z2, 2))

@@ -764,56 +764,97 @@ static cfa_status plan_tail(cfa_ctx* ctx, cfa_amg* amg) {
     return CFA_OK;
 }
 
-// V-cycle on the tile-streamed kernels: values V (FP32 in mixed precision) in the tiles, vectors
-// and arithmetic in FP64 (dry: prepare the kernels only, no launches)
-template <class V>
-static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const double* b, double* z, const int* done, bool dry) {
-    using T = double;
+// Level vectors of the tiled V-cycle in the vector type T
+template <class T>
+struct TVec;
+template <>
+struct TVec<double> {
+    static double* x(AmgLevel& L) { return L.x64.p; }
+    static double* t(AmgLevel& L) { return L.t64.p; }
+    static double* b(AmgLevel& L) { return L.b64.p; }
+    static double* r(AmgLevel& L) { return L.r64.p; }
+    static const double* dinv(AmgLevel& L) { return L.dinv.p; }
+    static double* cb(cfa_amg* a) { return a->cb64.p; }
+    static double* cx(cfa_amg* a) { return a->cx64.p; }
+};
+template <>
+struct TVec<float> {
+    static float* x(AmgLevel& L) { return L.x32.p; }
+    static float* t(AmgLevel& L) { return L.t32.p; }
+    static float* b(AmgLevel& L) { return L.b32.p; }
+    static float* r(AmgLevel& L) { return L.r32.p; }
+    static const float* dinv(AmgLevel& L) { return L.dinv32.p; }
+    static float* cb(cfa_amg* a) { return a->cb32.p; }
+    static float* cx(cfa_amg* a) { return a->cx32.p; }
+};
+
+// V-cycle on the tile-streamed kernels: values V in the tiles (FP32 in mixed precision), vectors
+// and arithmetic in T (FP64; FP32 too in mixed precision unless CFA_VCYCLE_FP64 is set), the
+// right-hand side of the level in B (level 0: the caller's FP64 r) (dry: prepare the kernels
+// only, no launches)
+template <class V, class T, class B>
+static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* z, const int* done, bool dry) {
     AmgLevel& L = amg->levels[l];
     const int s = amg->opts.smooth_steps;
     int* err = amg->err.p;
-    const T omega = L.omega;
-    const T* dinv = L.dinv.p;
-    T* x = L.x64.p;
-    T* t = L.t64.p;
+    const T omega = (T)L.omega;
+    const T* dinv = TVec<T>::dinv(L);
+    T* x = TVec<T>::x(L);
+    T* t = TVec<T>::t(L);
     if (s >= 2) {
-        vct<VC_PRE, V, T, T, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)nullptr, x, done);
+        vct<VC_PRE, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)nullptr, x, done);
     } else if (!dry) {
-        CFA_TPR_SWITCH(L.A.tpr, CFA_LAUNCH(ctx, (k_vc_pre<TPR, T, T>), row_grid(ctx, L.A.rows, L.A.tpr), kThreads, 0,
-                                           L.A.rows, L.A.rp.p, L.A.ci.p, L.A.v.p, dinv, omega, b, 0, x, done));
+        CFA_TPR_SWITCH(L.A.tpr, CFA_LAUNCH(ctx, (k_vc_pre<TPR, T, B>), row_grid(ctx, L.A.rows, L.A.tpr), kThreads, 0,
+                                           L.A.rows, L.A.rp.p, L.A.ci.p,
+                                           (const T*)(std::is_same<T, float>::value ? (const void*)L.A.v32.p
+                                                                                    : (const void*)L.A.v.p),
+                                           dinv, omega, b, 0, x, done));
     }
     for (int k = 2; k < s; ++k) {
-        vct<VC_JAC, V, T, T, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, t, done);
+        vct<VC_JAC, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, t, done);
         std::swap(x, t);
     }
-    vct<VC_RES, V, T, T, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, L.r64.p, done);
+    vct<VC_RES, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, TVec<T>::r(L), done);
     const bool last = l + 1 == (int)amg->levels.size();
-    T* cb = last ? amg->cb64.p : amg->levels[l + 1].b64.p;
-    vct<VC_SPMV, V, T, T, T>(ctx, dry, L.tR, err, dinv, omega, (const T*)nullptr, (const T*)L.r64.p, cb, done);
+    T* cb = last ? TVec<T>::cb(amg) : TVec<T>::b(amg->levels[l + 1]);
+    vct<VC_SPMV, V, T, T, T>(ctx, dry, L.tR, err, dinv, omega, (const T*)nullptr, (const T*)TVec<T>::r(L), cb, done);
     const T* cx;
-    if (!last && l + 1 == amg->tail_level) {
+    if (!last && l + 1 == amg->tail_level && std::is_same<T, double>::value) {
         if (!dry) launch_tail<V>(ctx, amg, l + 1, done);
-        cx = amg->levels[l + 1].x64.p;
+        cx = TVec<T>::x(amg->levels[l + 1]);
     } else if (!last) {
-        vcycle_tiled<V>(ctx, amg, l + 1, cb, nullptr, done, dry);
-        cx = amg->levels[l + 1].x64.p;
+        vcycle_tiled<V, T, T>(ctx, amg, l + 1, cb, nullptr, done, dry);
+        cx = TVec<T>::x(amg->levels[l + 1]);
     } else {
         if (!dry)
             CFA_LAUNCH(ctx, (k_vc_dense<T, T>), ceil_div((long long)amg->coarse_n * 32, kThreads), kThreads, 0,
-                       amg->coarse_n, amg->coarse_inv.p, (const T*)cb, amg->cx64.p, done);
-        cx = amg->cx64.p;
+                       amg->coarse_n, amg->coarse_inv.p, (const T*)cb, TVec<T>::cx(amg), done);
+        cx = TVec<T>::cx(amg);
     }
     vct<VC_ADD, V, T, T, T>(ctx, dry, L.tP, err, dinv, omega, (const T*)nullptr, cx, x, done);
     for (int k = 0; k < s; ++k) {
         if (l == 0 && k == s - 1) {
-            vct<VC_JAC, V, T, T, double>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, z, done);
+            vct<VC_JAC, V, T, B, double>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, z, done);
         } else {
-            vct<VC_JAC, V, T, T, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, t, done);
+            vct<VC_JAC, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, t, done);
             std::swap(x, t);
         }
     }
-    if (l > 0 && x != L.x64.p && !dry)
-        cudaMemcpyAsync(L.x64.p, x, (size_t)L.A.rows * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream);
+    if (l > 0 && x != TVec<T>::x(L) && !dry)
+        cudaMemcpyAsync(TVec<T>::x(L), x, (size_t)L.A.rows * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream);
+}
+
+// mixed precision: the whole V-cycle in FP32 (CFA_VCYCLE_FP64=1 keeps FP64 vectors)
+static bool vcycle_fp32(const cfa_amg* amg) {
+    if (amg->opts.precision != CFA_MIXED) return false;
+    const char* e = std::getenv("CFA_VCYCLE_FP64");
+    return !(e && e[0] == '1');
+}
+
+static void vcycle_tiled_top(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, bool dry) {
+    if (amg->opts.precision != CFA_MIXED) vcycle_tiled<double, double, double>(ctx, amg, 0, r, z, done, dry);
+    else if (vcycle_fp32(amg)) vcycle_tiled<float, float, double>(ctx, amg, 0, r, z, done, dry);
+    else vcycle_tiled<float, double, double>(ctx, amg, 0, r, z, done, dry);
 }
 
 cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done) {
@@ -821,8 +862,7 @@ cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, co
         CFA_LAUNCH(ctx, (k_vc_dense<double, double>), ceil_div((long long)amg->coarse_n * 32, kThreads), kThreads, 0,
                    amg->coarse_n, amg->coarse_inv.p, r, z, done);
     } else if (amg->tiled) {
-        if (amg->opts.precision == CFA_MIXED) vcycle_tiled<float>(ctx, amg, 0, r, z, done, false);
-        else vcycle_tiled<double>(ctx, amg, 0, r, z, done, false);
+        vcycle_tiled_top(ctx, amg, r, z, done, false);
     } else if (amg->opts.precision == CFA_MIXED) {
         vcycle_level<float, double>(ctx, amg, 0, r, z, done);
     } else {
@@ -1044,6 +1084,7 @@ static cfa_status prepare_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L) {
         CFA_PROPAGATE(plan_tiled(ctx, hr.p, M->rows, 1, vb, T));
         CFA_PROPAGATE(pack_tiled(ctx, M->rp.p, M->ci.p, M->v.p, nullptr, nullptr, T));
     }
+    if (o.precision == CFA_MIXED) CFA_PROPAGATE(level_vectors(ctx, amg, L, L.A.rows));   // FP32 V-cycle vectors
     return level_vectors64(ctx, L, L.A.rows);
 }
 
@@ -1052,8 +1093,7 @@ static cfa_status prepare_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L) {
 static cfa_status prepare_vcycle(cfa_ctx* ctx, cfa_amg* amg) {
     if (!amg->tiled) return CFA_OK;
     CFA_PROPAGATE(plan_tail(ctx, amg));
-    if (amg->opts.precision == CFA_MIXED) vcycle_tiled<float>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
-    else vcycle_tiled<double>(ctx, amg, 0, nullptr, nullptr, nullptr, true);
+    vcycle_tiled_top(ctx, amg, nullptr, nullptr, nullptr, true);
     CFA_CHECK_LAUNCH();
     return CFA_OK;
 }

@@ -640,7 +640,9 @@ def test_pcg_mixed_precision_reaches_tolerance(ctx):
         assert np.linalg.norm(rhs - Ax) <= 1.5e-10 * np.linalg.norm(rhs)
         res[prec] = (it, x)
     assert np.abs(res[cfa.MIXED][1] - res[cfa.FP64][1]).max() < 1e-7 * np.abs(res[cfa.FP64][1]).max()
-    assert res[cfa.MIXED][0] <= res[cfa.FP64][0] + 3
+    # the FP32 V-cycle (values, vectors and arithmetic) is a preconditioner accurate to ~1e-7; at a
+    # 1e-10 tolerance the flexible CG takes up to about an eighth more iterations
+    assert res[cfa.MIXED][0] <= 1.15 * res[cfa.FP64][0] + 3
 
 
 def test_pcg_zero_rhs_and_breakdown(ctx):
