@@ -13,6 +13,11 @@
   repository's solvers: a temporary mirror of the reference's ``src/`` whose files are links to
   the originals except ``cfa/linalg.cuh``, which links to ``cylinder-fem-amr_b200/shim/cfa/
   linalg.cuh``; linked with ``libcfa_b200.so``. The mirror is removed after the build.
+* ``oracle/_ref/cfa_swap_driver``: as the drop-in, with the driver's Step A and B call sites
+  (assembly, boundary conditions, OSS terms and the PPE solve) switched to the shim's
+  ``cfa_swap`` functions: the mirror's ``cylinder_fem_amr.cu`` is a copy of the reference's with
+  the eight call-site substitutions of ``SWAP_SITES`` applied (each anchor must occur exactly
+  once), removed with the mirror after the build.
 
 Run as ``python oracle/build.py [oracle|ref|drivers|all]``.
 """
@@ -70,6 +75,21 @@ def build_ref(force: bool = False) -> str | None:
     return REF_LIB
 
 
+SWAP_DRIVER = os.path.join(HERE, "_ref", "cfa_swap_driver")
+# call sites of the driver's Steps A and B -> the shim's cfa_swap functions (same arguments,
+# the driver's DeviceMeshBuffers in front)
+SWAP_SITES = [
+    ("k_assemble_momentum_fem<<<blocks_elems, threads>>>(", "cfa_swap::assemble_momentum(gpu_buf, "),
+    ("k_apply_bc_momentum<<<blocks_nodes, threads>>>(", "cfa_swap::apply_bc_momentum(gpu_buf, "),
+    ("k_compute_oss_weights<<<blocks_elems, threads>>>(", "cfa_swap::oss_weights(gpu_buf, "),
+    ("k_accumulate_scalar_gradient<<<blocks_elems, threads>>>(", "cfa_swap::scalar_gradient(gpu_buf, "),
+    ("k_assemble_pressure_poisson<<<blocks_elems, threads>>>(", "cfa_swap::assemble_pressure_poisson(gpu_buf, "),
+    ("apply_bc_pressure(n_nodes, gpu_buf.d_bc_tag", "cfa_swap::apply_bc_pressure(gpu_buf, n_nodes, gpu_buf.d_bc_tag"),
+    ("if (oss) assemble_oss_projection(gpu_buf);", "if (oss) cfa_swap::assemble_oss_projection(gpu_buf);"),
+    ("int it_p = solver.solve_pcg(", "int it_p = cfa_swap::solve_pcg(solver, gpu_buf, "),
+]
+
+
 def _driver_cmd(src: str, out: str, extra: list[str]) -> list[str]:
     return [NVCC, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "shared",
             "-Xcompiler", "-fopenmp", *extra, src, "-o", out, "-lgomp"]
@@ -90,19 +110,30 @@ def build_drivers(force: bool = False) -> tuple[str | None, str | None]:
         subprocess.check_call(_driver_cmd(main, REF_DRIVER, []))
     lib = os.path.join(PKG, "libcfa_b200.so")
     header = os.path.join(ROOT, "include", "cfa_b200.h")
-    if force or _stale(DROPIN_DRIVER, deps + [SHIM, lib, header]):
+    for out, swap in ((DROPIN_DRIVER, False), (SWAP_DRIVER, True)):
+        if not (force or _stale(out, deps + [SHIM, lib, header, os.path.abspath(__file__)])):
+            continue
         mirror = os.path.join(HERE, "_ref", "mirror")
         if os.path.isdir(mirror):
             shutil.rmtree(mirror)
         os.makedirs(os.path.join(mirror, "cfa"))
         try:
-            os.symlink(main, os.path.join(mirror, "cylinder_fem_amr.cu"))
+            if swap:
+                text = open(main).read()
+                for anchor, repl in SWAP_SITES:
+                    if text.count(anchor) != 1:
+                        raise RuntimeError(f"call site not found exactly once: {anchor}")
+                    text = text.replace(anchor, repl)
+                with open(os.path.join(mirror, "cylinder_fem_amr.cu"), "w") as f:
+                    f.write(text)
+            else:
+                os.symlink(main, os.path.join(mirror, "cylinder_fem_amr.cu"))
             for f in os.listdir(cfa_dir):
                 target = SHIM if f == "linalg.cuh" else os.path.join(cfa_dir, f)
                 os.symlink(target, os.path.join(mirror, "cfa", f))
             extra = ["-I", os.path.join(ROOT, "include"), "-L", PKG, "-lcfa_b200",
                      "-Xlinker", "-rpath,$ORIGIN/../../cylinder-fem-amr_b200"]
-            subprocess.check_call(_driver_cmd(os.path.join(mirror, "cylinder_fem_amr.cu"), DROPIN_DRIVER, extra))
+            subprocess.check_call(_driver_cmd(os.path.join(mirror, "cylinder_fem_amr.cu"), out, extra))
         finally:
             shutil.rmtree(mirror)
     return REF_DRIVER, DROPIN_DRIVER

@@ -2,11 +2,13 @@
 
 ``oracle/_ref/cfa_ref_driver`` is the reference's own program (src/cylinder_fem_amr.cu built by
 its README recipe); ``oracle/_ref/cfa_dropin_driver`` is the same source compiled against the
-shim header ``cylinder-fem-amr_b200/shim/cfa/linalg.cuh`` and linked with ``libcfa_b200.so``
-(``oracle/build.py drivers``). Both run the DFG 2D-2 cylinder case on a uniform level-3 mesh
-(the reference's U3 run, 29k nodes) and with adaptive refinement (its A1 settings, a remesh
-every 10 steps), and their force histories (``<prefix>_forces.csv``, 10 significant digits),
-meshes and iteration counts are compared row by row.
+shim header ``cylinder-fem-amr_b200/shim/cfa/linalg.cuh`` and linked with ``libcfa_b200.so``;
+``oracle/_ref/cfa_swap_driver`` additionally has the driver's Step A and B call sites switched to
+this library's assembly and handle-based PPE solve (``oracle/build.py drivers``). Each runs the
+DFG 2D-2 cylinder case on a uniform level-3 mesh (the reference's U3 run, 29k nodes) and with
+adaptive refinement (its A1 settings, a remesh every 10 steps), and the force histories
+(``<prefix>_forces.csv``, 10 significant digits), meshes and iteration counts are compared with
+the stock program's row by row.
 """
 import csv
 import os
@@ -21,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(os.path.dirname(HERE), "oracle", "_ref")
 STOCK = os.path.join(REF_DIR, "cfa_ref_driver")
 DROPIN = os.path.join(REF_DIR, "cfa_dropin_driver")
+SWAP = os.path.join(REF_DIR, "cfa_swap_driver")
 
 torch = pytest.importorskip("torch")
 if not torch.cuda.is_available():
@@ -64,12 +67,25 @@ def compare(a, b):
     return out, same_mesh
 
 
+_STOCK_RUNS = {}
+
+
+def stock(case, tmp_path_factory):
+    if case not in _STOCK_RUNS:
+        _STOCK_RUNS[case] = run(STOCK, case, tmp_path_factory.mktemp("stock"))
+    return _STOCK_RUNS[case]
+
+
 @pytest.mark.parametrize("case", ["U3", "A1"])
-def test_unmodified_application_on_b200_solvers(case, tmp_path):
-    ref_rows, ref_it, ref_wall, _ = run(STOCK, case, tmp_path)
-    new_rows, new_it, new_wall, out = run(DROPIN, case, tmp_path)
+@pytest.mark.parametrize("build", ["dropin", "swap"])
+def test_unmodified_application_on_b200_solvers(build, case, tmp_path, tmp_path_factory):
+    binary = DROPIN if build == "dropin" else SWAP
+    if not os.path.exists(binary):
+        pytest.skip(f"{binary} not built")
+    ref_rows, ref_it, ref_wall, _ = stock(case, tmp_path_factory)
+    new_rows, new_it, new_wall, out = run(binary, case, tmp_path)
     diff, same_mesh = compare(ref_rows, new_rows)
-    print(f"{case}: wall {ref_wall} s (reference) vs {new_wall} s (drop-in); max rel diff {diff}; "
+    print(f"{case}: wall {ref_wall} s (reference) vs {new_wall} s ({build}); max rel diff {diff}; "
           f"same meshes {same_mesh}")
     assert same_mesh
     # Iteration counts of the printed steps. Momentum: within one of the reference's at every
