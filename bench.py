@@ -486,9 +486,11 @@ def run_adjoint(args):
     z = np.zeros(m.n)
     nu_node = np.full(m.n, NU)
 
+    stab = args.stab
+
     def make(prec):
         return AD.DragAdjoint(m, u0, z, z, nu_node, u_max=U_MAX, steps=steps, dt=5e-3, nu=NU, precision=prec,
-                              checkpoint=20, tol=1e-12)
+                              checkpoint=20, tol=1e-12, stab=stab)
 
     clk = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
     adj = make(cfa.MIXED)
@@ -514,7 +516,7 @@ def run_adjoint(args):
         "ms_per_step": round(t_grad / steps, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 outer / f32 preconditioners", "data": "synthetic",
         "config": {"workload": f"c3: c1 mesh n={m.n}, dt 5e-3, U 1.5, nu 1e-3, from the inflow profile, "
-                               "OSS off (stab 0), checkpoints every 20 steps, solves to 1e-12",
+                               f"OSS stab {stab:g}, checkpoints every 20 steps, solves to 1e-12",
                    "forward_ms": round(t_fwd, 1), "J_mean_drag": J,
                    "dJ_dU": g_u, "dJ_dU_central_fd_h1e-6": fd, "fd_rel_diff": abs(g_u - fd) / abs(fd),
                    "dJ_dnu_norm": float(torch.linalg.norm(g_nu)),
@@ -599,6 +601,8 @@ def main():
     ap.add_argument("--workload", default="c1")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--streams", type=int, default=4, help="concurrent streams per GPU (c4)")
+    ap.add_argument("--stab", type=float, default=STAB,
+                    help="c3: OSS pressure stabilisation of the differentiated loop (0.3, the reference's default)")
     ap.add_argument("--profile", action="store_true",
                     help="one step per precision between cudaProfilerStart/Stop (for ncu --profile-from-start off); no JSON line")
     args = ap.parse_args()

@@ -3,12 +3,14 @@
     J = (1/N) sum_{n=1..N} C_D^n,   C_D = force_scale F_x  (k_volume_forces)
 
 with respect to a per-node viscosity field of the momentum equation and the inflow amplitude U,
-for the loop of ``step.TimeStepper`` without the OSS term (stab = 0; the PPE matrix is then the
-stiffness matrix with the outlet rows eliminated, and the rotational pressure update takes the
-scalar viscosity).
+for the loop of ``step.TimeStepper`` (the rotational pressure update takes the scalar viscosity,
+as do the OSS weights). With the OSS pressure stabilisation (stab > 0) the pressure operator is
+(1 + s_K) K - B^T M^-1 B with weights s_K of u*, and its right-hand side carries the OSS terms of
+p^n; their derivatives go through cfa_oss_adjoint.
 
-Every solve's backward is the transposed solve: the pressure operator is symmetric, so the PCG
-with the same AMG serves; the momentum system uses BiCGSTAB2 on A^T with the transposed
+Every solve's backward is the transposed solve: the pressure operator acts symmetrically on the
+rows that are not Dirichlet (the adjoint right-hand side is zeroed on the Dirichlet rows, whose
+multipliers no derivative uses), so the PCG with the same operator and AMG serves; the momentum system uses BiCGSTAB2 on A^T with the transposed
 multicolour ILU. The assembly and the other kernels have adjoint kernels in the library
 (cfa_momentum_adjoint, cfa_ppe_rhs_adjoint, cfa_projection_adjoint, cfa_volume_forces_adjoint).
 The forward sweep keeps the state every ``checkpoint`` steps; the backward sweep recomputes each
@@ -27,7 +29,7 @@ import cfa_b200 as cfa
 class DragAdjoint:
     def __init__(self, mesh, u0, v0, p0, nu_node, u_max=1.5, steps=10, dt=5e-3, nu=1e-3, rho=1.0, tau_time=1e-3,
                  H=1.0, u_mean=1.0, diameter=0.2, precision=cfa.MIXED, tol=1e-12, checkpoint=20, ctx=None,
-                 direct=False):
+                 direct=False, stab=0.0):
         import torch
         self.torch = torch
         self.ctx = ctx or cfa.default_context()
@@ -47,7 +49,11 @@ class DragAdjoint:
         self.A, self.AT, self.ru, self.rv, self.mass = z(nnz), z(nnz), z(n), z(n), z(n)
         self.Kp, self.rhs_p, self.div, self.elem_s = z(nnz), z(n), z(n), z(ne)
         self.gdx, self.gdy, self.vort_num, self.vort, self.forces = z(n), z(n), z(n), z(n), z(2)
-        self.oss_dummy, self.inv_m_dummy = z(4 * nnz), z(n)
+        self.stab = float(stab)
+        self.oss_val, self.inv_m = z(4 * nnz), z(n)
+        self.oss = cfa.oss_operator(self.dm, self.oss_val, self.inv_m) if self.stab > 0.0 else None
+        tag = np.ascontiguousarray(mesh.tag)
+        self.non_dirichlet = t((tag != 2).astype(np.float64))   # BC_OUTLET: p = 0 (the default outlet)
         rp, ci = self.dm.host_pattern()
         self.rp_h, self.ci_h = rp, ci
         self.ilu = cfa.MulticolourIlu0(self.ctx, precision)
@@ -70,11 +76,22 @@ class DragAdjoint:
         dt_p, a0, a1, a2, c1, c2 = self.coefficients(k)
         return cfa.MomentumParams(self.dt, self.nu, self.rho, a0, a1, a2, c1, c2, self.tau_time, 0.5)
 
-    def _lu_solve(self, vals, rhs_list):
+    def _lu_solve(self, vals, rhs_list, oss=False):
+        """Sparse direct solves with the matrix vals on the pattern; oss: the pressure operator,
+        vals - [rows not Dirichlet] B^T M^-1 B from the assembled OSS arrays."""
         import scipy.sparse as sp
         import scipy.sparse.linalg as spl
-        A = sp.csr_matrix((vals.cpu().numpy(), self.ci_h, self.rp_h), shape=(self.n, self.n)).tocsc()
-        lu = spl.splu(A)
+        shape = (self.n, self.n)
+        A = sp.csr_matrix((vals.cpu().numpy(), self.ci_h, self.rp_h), shape=shape)
+        if oss:
+            o = self.oss_val.cpu().numpy()
+            nnz = self.nnz
+            Bx = sp.csr_matrix((o[:nnz], self.ci_h, self.rp_h), shape=shape)
+            By = sp.csr_matrix((o[nnz:2 * nnz], self.ci_h, self.rp_h), shape=shape)
+            Mi = sp.diags(self.inv_m.cpu().numpy())
+            S = Bx.T @ Mi @ Bx + By.T @ Mi @ By
+            A = A - sp.diags(self.non_dirichlet.cpu().numpy()) @ S
+        lu = spl.splu(A.tocsc())
         return [self.torch.from_numpy(lu.solve(r.cpu().numpy())).to("cuda") for r in rhs_list]
 
     def _assemble_momentum(self, k, u_n, v_n, u_nm1, v_nm1, p_n, x_u, x_v, u_max):
@@ -83,12 +100,26 @@ class DragAdjoint:
 
     def _pressure_system(self, k, x_u, x_v, p_n, dp):
         dt_p = self.coefficients(k)[0]
+        if self.stab > 0.0:
+            cfa.oss_weights(self.ctx, self.dm, x_u, x_v, dt_p, self.rho, self.nu, self.stab, self.elem_s)
+            cfa.scalar_gradient(self.ctx, self.dm, p_n, self.elem_s, self.gdx, self.gdy)
         cfa.assemble_pressure_system(self.ctx, self.dm, x_u, x_v, p_n, self.gdx, self.gdy, self.mass, self.elem_s,
-                                     dt_p, self.rho, 0.0, self.Kp, self.rhs_p, self.div, dp, self.oss_dummy,
-                                     self.inv_m_dummy)
+                                     dt_p, self.rho, self.stab, self.Kp, self.rhs_p, self.div, dp, self.oss_val,
+                                     self.inv_m)
         if not self.amg_ready and not self.direct:
-            self.amg.setup(self.n, self.nnz, self.dm.rp, self.dm.ci, self.Kp)   # K: the same every step
+            # built once: the stiffness part of the operator of the first step (with OSS a fixed
+            # SPD preconditioner for every step, as the reference reuses it between rebuilds)
+            self.amg.setup(self.n, self.nnz, self.dm.rp, self.dm.ci, self.Kp)
             self.amg_ready = True
+
+    def _pressure_solve(self, rhs, x):
+        """x = A^-1 rhs with this step's pressure operator (iterative: warm start from x)."""
+        if self.direct:
+            (sol,) = self._lu_solve(self.Kp, [rhs], oss=self.stab > 0.0)
+            x.copy_(sol)
+        else:
+            self.pcg.solve_pcg(self.n, self.dm.rp, self.dm.ci, self.Kp, rhs, x, 4000, self.tol, self.oss, self.amg)
+        return x
 
     def step(self, k, state, u_max=None):
         """Step k from state (u^n, v^n, u^{n-1}, v^{n-1}, p^n, dp warm start); returns the new state
@@ -106,10 +137,7 @@ class DragAdjoint:
             self.mom.solve(self.n, self.dm.rp, self.dm.ci, self.A, self.ru, self.rv, x_u, x_v, 2000, self.tol, self.ilu)
         dp = dp_prev.clone()
         self._pressure_system(k, x_u, x_v, p_n, dp)
-        if self.direct:
-            (dp,) = self._lu_solve(self.Kp, [self.rhs_p])
-        else:
-            self.pcg.solve_pcg(self.n, self.dm.rp, self.dm.ci, self.Kp, self.rhs_p, dp, 4000, self.tol, None, self.amg)
+        self._pressure_solve(self.rhs_p, dp)
         u, v, p = x_u.clone(), x_v.clone(), p_n.clone()
         cfa.project_step(self.ctx, self.dm, dt_p, self.rho, self.rho * self.nu, True, self.mass, dp, self.div, self.gdx,
                          self.gdy, self.vort_num, u, v, p, self.vort)
@@ -172,14 +200,15 @@ class DragAdjoint:
                 cfa.projection_adjoint(self.ctx, self.dm, dt_p, self.rho, self.nu, self.mass, gU, gV, gP, g_dp)
                 g_us, g_vs = gU.clone(), gV.clone()
                 gP1 += gP
-                # B: pressure solve (symmetric) and its right-hand side
+                # B: pressure solve (the operator on the rows that are not Dirichlet) and its
+                # right-hand side; with OSS also the weights' and the OSS right-hand side's terms
                 self._pressure_system(k, rec["x_u"], rec["x_v"], rec["p_n"], rec["dp"].clone())
-                if self.direct:
-                    (lam_p,) = self._lu_solve(self.Kp, [g_dp])
-                else:
-                    lam_p.zero_()
-                    self.pcg.solve_pcg(n, self.dm.rp, self.dm.ci, self.Kp, g_dp, lam_p, 4000, self.tol, None, self.amg)
+                lam_p.zero_()
+                self._pressure_solve(g_dp * self.non_dirichlet, lam_p)
                 cfa.ppe_rhs_adjoint(self.ctx, self.dm, lam_p, dt_p, self.rho, g_us, g_vs)
+                if self.stab > 0.0:
+                    cfa.oss_adjoint(self.ctx, self.dm, rec["x_u"], rec["x_v"], dt_p, self.rho, self.nu, self.stab,
+                                    self.elem_s, self.mass, lam_p, rec["p_n"], rec["dp"], g_us, g_vs, gP1)
                 # A: momentum, transposed solve and the assembly derivatives
                 xu0, xv0 = rec["u_n"].clone(), rec["v_n"].clone()
                 self._assemble_momentum(k, rec["u_n"], rec["v_n"], rec["u_nm1"], rec["v_nm1"], rec["p_n"], xu0, xv0,

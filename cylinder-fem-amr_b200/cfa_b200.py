@@ -222,6 +222,14 @@ def ppe_rhs_adjoint(ctx, m: DeviceMesh, lam_p, dt_proj, rho, g_u, g_v):
                                         ptr(g_v)))
 
 
+def oss_adjoint(ctx, m: DeviceMesh, u_star, v_star, dt_proj, rho, nu, stab, elem_s, mass, lam_p, p_old, dp, g_u, g_v,
+                g_p):
+    """Adds the OSS terms' derivatives of lambda^T (rhs_p - A dp) to g_u, g_v (u*, v*) and g_p (p^n)."""
+    ctx.check(lib().cfa_oss_adjoint(ctx.h, m.h, ptr(u_star), ptr(v_star), C.c_double(dt_proj), C.c_double(rho),
+                                    C.c_double(nu), C.c_double(stab), ptr(elem_s), ptr(mass), ptr(lam_p), ptr(p_old),
+                                    ptr(dp), ptr(g_u), ptr(g_v), ptr(g_p)))
+
+
 def projection_adjoint(ctx, m: DeviceMesh, dt_proj, rho, nu, mass, g_u_new, g_v_new, g_p_new, g_dp):
     ctx.check(lib().cfa_projection_adjoint(ctx.h, m.h, C.c_double(dt_proj), C.c_double(rho), C.c_double(nu), ptr(mass),
                                            ptr(g_u_new), ptr(g_v_new), ptr(g_p_new), ptr(g_dp)))

@@ -392,6 +392,99 @@ __global__ void k_forces_adjoint_nodes(int n, const int* __restrict__ inc_ptr, c
     g_u_prev[i] += s[4]; g_v_prev[i] += s[5]; g_p[i] += s[6];
 }
 
+// ---- the OSS terms of the pressure step (stab > 0) ----
+// With s_K the OSS weights of u* (k_compute_oss_weights, src/cfa/fem_kernels.cuh:697-719) and
+// G(f)_k = sum_{K ∋ k} sqrt(s_K) |K|/3 grad f|K (k_accumulate_scalar_gradient, :726-757), the
+// pressure step's matrix is (1 + s_K) K - [rows not Dirichlet] B^T M^-1 B and its right-hand side
+// carries -[s_K |K| grad N_i . grad p^n - |K| grad N_i . sqrt(s_K)/3 sum_{k in K} G(p^n)_k / m_k]
+// (k_assemble_pressure_poisson, :201-282; k_assemble_oss_operator). With the solution dp zero on
+// Dirichlet rows and l the pressure adjoint with its Dirichlet entries zeroed, the s-dependent part
+// of l^T (rhs_p - A dp) is -Phi(l, q), q = p^n + dp, where
+//   Phi(l, q) = sum_K s_K |K| grad l|K . grad q|K - sum_k G(l)_k . G(q)_k / m_k.
+// Per element: g_s = -dPhi/ds_K, mapped to u*, v* through ds_K/du*_j (the weight's formula,
+// differentiated by hand; the zero subgradient where |u-bar| = 0); per vertex: -dPhi/dq_j, the
+// p^n gradient. Five values per element: d/du and d/dv (equal for its three vertices), d/dp0..2.
+__global__ void __launch_bounds__(kThreads)
+k_oss_adjoint_elems(int ne, const int* __restrict__ ev, const double* __restrict__ x, const double* __restrict__ y,
+                    const double* __restrict__ us, const double* __restrict__ vs, const double* __restrict__ elem_s,
+                    const double* __restrict__ mass, const double* __restrict__ lam, const double* __restrict__ q,
+                    const double* __restrict__ glx, const double* __restrict__ gly, const double* __restrict__ gqx,
+                    const double* __restrict__ gqy, double dt, double rho, double nu, double stab,
+                    double* __restrict__ g_elem) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    double* g = g_elem + (size_t)e * 5;
+    const int nd[3] = {ev[3 * e], ev[3 * e + 1], ev[3 * e + 2]};
+    const double x0 = x[nd[0]], y0 = y[nd[0]], x1 = x[nd[1]], y1 = y[nd[1]], x2 = x[nd[2]], y2 = y[nd[2]];
+    const double area = 0.5 * fabs((x1 - x0) * (y2 - y0) - (x2 - x0) * (y1 - y0));
+    const double sK = elem_s[e];
+    if (area < 1.0e-14 || !(sK > 0.0)) {
+        for (int k = 0; k < 5; ++k) g[k] = 0.0;
+        return;
+    }
+    const double inv2A = 1.0 / (2.0 * area);
+    const double dNdx[3] = {(y1 - y2) * inv2A, (y2 - y0) * inv2A, (y0 - y1) * inv2A};
+    const double dNdy[3] = {(x2 - x1) * inv2A, (x0 - x2) * inv2A, (x1 - x0) * inv2A};
+    double lx = 0.0, ly = 0.0, qx = 0.0, qy = 0.0, slx = 0.0, sly = 0.0, sqx = 0.0, sqy = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        const int k = nd[a];
+        lx += lam[k] * dNdx[a];
+        ly += lam[k] * dNdy[a];
+        qx += q[k] * dNdx[a];
+        qy += q[k] * dNdy[a];
+        const double im = 1.0 / fmax(mass[k], 1.0e-14);
+        slx += glx[k] * im;
+        sly += gly[k] * im;
+        sqx += gqx[k] * im;
+        sqy += gqy[k] * im;
+    }
+    const double rs = sqrt(sK);
+    // dPhi/ds_K: the s_K K term, and sqrt(s_K) in G(l)_k and G(q)_k of the element's vertices
+    const double dphi = area * (lx * qx + ly * qy) - area / (6.0 * rs) * (lx * sqx + ly * sqy + slx * qx + sly * qy);
+    const double gs = -dphi;
+    // s_K = rho tau / dt, tau = stab / (rho (4 nu / h^2 + 2 |u-bar| / h) + 1e-300), h = sqrt(2 |K|)
+    const double h = sqrt(2.0 * area);
+    const double ub = (us[nd[0]] + us[nd[1]] + us[nd[2]]) / 3.0;
+    const double vb = (vs[nd[0]] + vs[nd[1]] + vs[nd[2]]) / 3.0;
+    const double nrm = sqrt(ub * ub + vb * vb);
+    const double den = rho * (4.0 * nu / (h * h) + 2.0 * nrm / h) + 1.0e-300;
+    const double ds_dnrm = (rho / dt) * (-stab / (den * den)) * (rho * 2.0 / h);
+    const double c = nrm > 0.0 ? gs * ds_dnrm / (3.0 * nrm) : 0.0;
+    g[0] = c * ub;
+    g[1] = c * vb;
+    // -dPhi/dq_j
+    for (int j = 0; j < 3; ++j)
+        g[2 + j] = -(sK * area * (lx * dNdx[j] + ly * dNdy[j]) - rs * (area / 3.0) * (dNdx[j] * slx + dNdy[j] * sly));
+}
+
+__global__ void k_oss_adjoint_nodes(int n, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
+                                    const double* __restrict__ g_elem, double* __restrict__ g_u,
+                                    double* __restrict__ g_v, double* __restrict__ g_p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double su = 0.0, sv = 0.0, sp = 0.0;
+    for (int k = inc_ptr[i]; k < inc_ptr[i + 1]; ++k) {
+        const int e = inc[k] >> 2, a = inc[k] & 3;
+        const double* g = g_elem + (size_t)e * 5;
+        su += g[0];
+        sv += g[1];
+        sp += g[2 + a];
+    }
+    g_u[i] += su;
+    g_v[i] += sv;
+    g_p[i] += sp;
+}
+
+// l = lambda with its Dirichlet entries zeroed, q = p^n + dp
+__global__ void k_oss_adjoint_inputs(int n, const int* __restrict__ tag, OutletBc bc, const double* __restrict__ lam,
+                                     const double* __restrict__ p_old, const double* __restrict__ dp,
+                                     double* __restrict__ l, double* __restrict__ q) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    l[i] = pressure_dirichlet(i, tag[i], bc) ? 0.0 : lam[i];
+    q[i] = p_old[i] + dp[i];
+}
+
 }  // namespace cfa
 
 using namespace cfa;
@@ -431,6 +524,31 @@ cfa_status cfa_ppe_rhs_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const double* la
     CFA_LAUNCH(ctx, k_ppe_rhs_adjoint, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y, m->tag, m->bc,
                m->inc_ptr.p, m->inc.p, lam_p, -(rho / dt_proj), g_u, g_v);
     CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+cfa_status cfa_oss_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const double* u_star, const double* v_star, double dt_proj,
+                           double rho, double nu, double stab, const double* elem_s, const double* mass_lumped,
+                           const double* lam_p, const double* p_old, const double* dp, double* g_u, double* g_v,
+                           double* g_p) {
+    if (!ctx) return CFA_BAD_ARG;
+    CFA_ARG(m && u_star && v_star && elem_s && mass_lumped && lam_p && p_old && dp && g_u && g_v && g_p);
+    CFA_ARG(dt_proj > 0.0 && stab > 0.0 && !m->bc.outlet_dirichlet);
+    const int n = m->n, ne = m->ne;
+    DevBuf<double> buf;   // l, q, G(l) x/y, G(q) x/y, per-element values
+    CFA_CUDA(buf.ensure(6 * (size_t)n + 5 * (size_t)ne));
+    double *l = buf.p, *q = buf.p + n, *glx = buf.p + 2 * (size_t)n, *gly = buf.p + 3 * (size_t)n;
+    double *gqx = buf.p + 4 * (size_t)n, *gqy = buf.p + 5 * (size_t)n, *ge = buf.p + 6 * (size_t)n;
+    CFA_LAUNCH(ctx, k_oss_adjoint_inputs, ceil_div(n, kThreads), kThreads, 0, n, m->tag, m->bc, lam_p, p_old, dp, l, q);
+    CFA_PROPAGATE(cfa_scalar_gradient(ctx, m, l, elem_s, glx, gly));
+    CFA_PROPAGATE(cfa_scalar_gradient(ctx, m, q, elem_s, gqx, gqy));
+    CFA_LAUNCH(ctx, k_oss_adjoint_elems, ceil_div(ne, kThreads), kThreads, 0, ne, m->ev, m->x, m->y, u_star, v_star,
+               elem_s, mass_lumped, (const double*)l, (const double*)q, (const double*)glx, (const double*)gly,
+               (const double*)gqx, (const double*)gqy, dt_proj, rho, nu, stab, ge);
+    CFA_LAUNCH(ctx, k_oss_adjoint_nodes, ceil_div(n, kThreads), kThreads, 0, n, m->inc_ptr.p, m->inc.p,
+               (const double*)ge, g_u, g_v, g_p);
+    CFA_CHECK_LAUNCH();
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));   // buf is released on return
     return CFA_OK;
 }
 

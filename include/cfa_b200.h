@@ -137,6 +137,16 @@ cfa_status cfa_momentum_adjoint(cfa_ctx* ctx, const cfa_mesh* mesh, const double
  * rows that are not Dirichlet. */
 cfa_status cfa_ppe_rhs_adjoint(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_lambda_p, double dt_proj,
                                double rho, double* d_g_u, double* d_g_v);
+/* Adjoint of the OSS terms of the pressure step (stab > 0, the default p = 0 outlet; no
+ * counterpart in the reference). Given the pressure adjoint lambda (the solution of A lambda = g
+ * with g zeroed on Dirichlet rows, A the step's operator (1 + s) K - B^T M^-1 B), the step's u*,
+ * its OSS weights d_elem_s (cfa_oss_weights), p^n and the solution dp, adds the derivatives of
+ * lambda^T (rhs_p - A dp) through the weights to d_g_u, d_g_v (u*, v*) and through the OSS
+ * right-hand side to d_g_p (p^n). Synchronises. */
+cfa_status cfa_oss_adjoint(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_u_star, const double* d_v_star,
+                           double dt_proj, double rho, double nu, double stab, const double* d_elem_s,
+                           const double* d_mass_lumped, const double* d_lambda_p, const double* d_p_old,
+                           const double* d_dp, double* d_g_u, double* d_g_v, double* d_g_p);
 /* Adjoint of cfa_project_step with the rotational term from the increment: given the adjoints of
  * the corrected u, v, p, writes the adjoint of dp (overwritten); those of u* and p^n are the
  * corrected ones unchanged (the caller passes them through). */
