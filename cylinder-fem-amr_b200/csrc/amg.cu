@@ -49,19 +49,32 @@ __global__ void k_pow_y(int n, const int* __restrict__ rp, const int* __restrict
     y[i] = __dmul_rn(dinv[i], s);
 }
 
-__global__ void k_pow_chunks(int n, int nch, const double* __restrict__ x, const double* __restrict__ y,
-                             double* __restrict__ py, double* __restrict__ px) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+// One block per chunk of kPowChunk rows: the chunk's x and y are staged in shared memory by the
+// whole block (coalesced), then two threads of different warps run the two sums, each strictly
+// in row order as the reference's per-chunk loop does.
+constexpr int kPowChunk = 4096;
+constexpr int kPowThreads = 256;
+
+__global__ void __launch_bounds__(kPowThreads)
+k_pow_chunks(int n, int nch, const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ py,
+             double* __restrict__ px) {
+    extern __shared__ double pow_sm[];   // [2 * kPowChunk]: y then x
+    const int c = blockIdx.x;
     if (c >= nch) return;
-    double sy = 0.0, sx = 0.0;
-    const int e = min(n, (c + 1) * 4096);
-    for (int i = c * 4096; i < e; ++i) {
-        const double yi = y[i], xi = x[i];
-        sy = __dadd_rn(sy, __dmul_rn(yi, yi));
-        sx = __dadd_rn(sx, __dmul_rn(xi, xi));
+    const int b = c * kPowChunk, m = min(n, b + kPowChunk) - b;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        pow_sm[i] = y[b + i];
+        pow_sm[kPowChunk + i] = x[b + i];
     }
-    py[c] = sy;
-    px[c] = sx;
+    __syncthreads();
+    if (threadIdx.x == 0 || threadIdx.x == 32) {
+        const double* v = pow_sm + (threadIdx.x == 0 ? 0 : kPowChunk);
+        double acc = 0.0;
+#pragma unroll 8
+        for (int i = 0; i < m; ++i) acc = __dadd_rn(acc, __dmul_rn(v[i], v[i]));
+        if (threadIdx.x == 0) py[c] = acc;
+        else px[c] = acc;
+    }
 }
 
 __global__ void k_pow_finish(int nch, const double* __restrict__ py, const double* __restrict__ px, double* __restrict__ st) {
@@ -1015,7 +1028,12 @@ static std::vector<double> start_vector(int n) {
 // rho(D^-1 A) by 20 power iterations (spectral_radius_DinvA, :1276-1304), on the device.
 static cfa_status spectral_radius(cfa_ctx* ctx, cfa_amg* amg, const DCsr& A, const double* dinv, double* rho) {
     SetupScratch& S = amg->scratch;
-    const int n = A.rows, nch = (n + 4095) / 4096;
+    const int n = A.rows, nch = (n + kPowChunk - 1) / kPowChunk;
+    static std::once_flag smem_once;
+    std::call_once(smem_once, [] {
+        cudaFuncSetAttribute(k_pow_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(2 * kPowChunk * sizeof(double)));
+    });
     if (!amg->x0.p || amg->x0.cap < (size_t)n) {
         const std::vector<double> h = start_vector(n);
         CFA_CUDA(amg->x0.ensure(n));
@@ -1031,8 +1049,8 @@ static cfa_status spectral_radius(cfa_ctx* ctx, cfa_amg* amg, const DCsr& A, con
     for (int it = 0; it < 20; ++it) {
         CFA_LAUNCH(ctx, k_pow_y, ceil_div(n, kThreads), kThreads, 0, n, (const int*)A.rp.p, (const int*)A.ci.p,
                    (const double*)A.v.p, dinv, (const double*)S.pow_x.p, S.pow_y.p);
-        CFA_LAUNCH(ctx, k_pow_chunks, ceil_div(nch, 64), 64, 0, n, nch, (const double*)S.pow_x.p,
-                   (const double*)S.pow_y.p, S.pow_py.p, S.pow_px.p);
+        CFA_LAUNCH(ctx, k_pow_chunks, nch, kPowThreads, 2 * kPowChunk * sizeof(double), n, nch,
+                   (const double*)S.pow_x.p, (const double*)S.pow_y.p, S.pow_py.p, S.pow_px.p);
         CFA_LAUNCH(ctx, k_pow_finish, 1, 32, 0, nch, (const double*)S.pow_py.p, (const double*)S.pow_px.p, S.pow_st.p);
         CFA_LAUNCH(ctx, k_pow_scale, ceil_div(n, kThreads), kThreads, 0, n, (const double*)S.pow_y.p,
                    (const double*)S.pow_st.p, S.pow_x.p);
