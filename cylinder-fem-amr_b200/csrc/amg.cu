@@ -114,34 +114,194 @@ __global__ void k_sg_ub(int rows, const int* __restrict__ arp, const int* __rest
     ub[i] = s;
 }
 
-__global__ void k_sg_accum(int rows, const int* __restrict__ arp, const int* __restrict__ aci, const double* __restrict__ av,
-                           const int* __restrict__ brp, const int* __restrict__ bci, const double* __restrict__ bv,
-                           const long long* __restrict__ off, int* __restrict__ scol, double* __restrict__ sval,
-                           int* __restrict__ cnt) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= rows) return;
-    int* cols = scol + off[i];
-    double* vals = sval + off[i];
-    int m = 0;
+// Accumulation of C = A B, a warp per row of C: the row's products are generated in order
+// (a-major, b-minor) into shared memory, the first occurrence of every column is marked, each lane
+// then sums one column's products in product order (first touch 0.0 + prod, then += prod: per entry
+// the operations and their order of csr_multiply's dense accumulator), and the columns are written
+// sorted into the row's slice of the scratch. Rows with more than kSgCap products are left to
+// k_sg_accum_big.
+constexpr int kSgWarps = 8;
+constexpr int kSgCap = 512;
+
+__global__ void __launch_bounds__(kSgWarps * 32)
+k_sg_accum_warp(int rows, const int* __restrict__ arp, const int* __restrict__ aci, const double* __restrict__ av,
+                const int* __restrict__ brp, const int* __restrict__ bci, const double* __restrict__ bv,
+                const long long* __restrict__ off, const int* __restrict__ ub, int* __restrict__ scol,
+                double* __restrict__ sval, int* __restrict__ cnt) {
+    extern __shared__ __align__(16) unsigned char sg_sm[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* pv = reinterpret_cast<double*>(sg_sm) + (size_t)w * kSgCap;
+    int* pc = reinterpret_cast<int*>(sg_sm + sizeof(double) * kSgWarps * kSgCap) + (size_t)w * kSgCap;
+    int* uq = reinterpret_cast<int*>(sg_sm + (sizeof(double) + sizeof(int)) * kSgWarps * kSgCap) + (size_t)w * kSgCap;
+    const int i = blockIdx.x * kSgWarps + w;
+    if (i >= rows) return;   // warp-uniform
+    int* gcols = scol + off[i];
+    double* gvals = sval + off[i];
+    const int np = ub[i];
+    if (np > kSgCap) return;   // k_sg_accum_big takes the row
+    // 1. the products in order
+    int base = 0;
     for (int a = arp[i]; a < arp[i + 1]; ++a) {
         const int k = aci[a];
         const double x = av[a];
-        for (int b = brp[k]; b < brp[k + 1]; ++b) {
-            const int j = bci[b];
-            const double prod = __dmul_rn(x, bv[b]);
-            int lo = 0, hi = m;
-            while (lo < hi) { const int mid = (lo + hi) >> 1; if (cols[mid] < j) lo = mid + 1; else hi = mid; }
-            if (lo < m && cols[lo] == j) {
-                vals[lo] = __dadd_rn(vals[lo], prod);
+        const int b0 = brp[k], len = brp[k + 1] - b0;
+        for (int q = lane; q < len; q += 32) {
+            pc[base + q] = bci[b0 + q];
+            pv[base + q] = __dmul_rn(x, bv[b0 + q]);
+        }
+        base += len;
+    }
+    __syncwarp();
+    // 2. first occurrences, compacted in product order
+    int u = 0;
+    for (int p0 = 0; p0 < np; p0 += 32) {
+        const int p = p0 + lane;
+        bool first = false;
+        if (p < np) {
+            const int c = pc[p];
+            first = true;
+            for (int q = 0; q < p; ++q)
+                if (pc[q] == c) { first = false; break; }
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, first);
+        if (first) uq[u + __popc(mask & ((1u << lane) - 1u))] = p;
+        u += __popc(mask);
+    }
+    __syncwarp();
+    // 3. one column per lane: its products summed in product order; 4. written at its rank
+    for (int k0 = 0; k0 < u; k0 += 32) {
+        const int k = k0 + lane;
+        const bool has = k < u;
+        const int p1 = has ? uq[k] : np;
+        const int c = has ? pc[p1] : 0;
+        double acc = 0.0;
+        if (has) {
+            acc = __dadd_rn(0.0, pv[p1]);
+            for (int p = p1 + 1; p < np; ++p)
+                if (pc[p] == c) acc = __dadd_rn(acc, pv[p]);
+            int rank = 0;
+            for (int q = 0; q < u; ++q) rank += pc[uq[q]] < c;
+            gcols[rank] = c;
+            gvals[rank] = acc;
+        }
+    }
+    if (lane == 0) cnt[i] = u;
+}
+
+// The rows of C with more than kSgCap products, a block per row. With C's columns below
+// kSgDenseCols: the products are staged in order, kSgChunk at a time, and thread t accumulates the
+// columns c with c % blockDim.x == t into a dense accumulator, visiting the products in order (so
+// per entry: first touch 0.0 + prod, then += prod in product order); the touched columns are
+// written in ascending order. Wider C: thread 0 runs the same arithmetic as a sorted insertion
+// into the row's slice.
+constexpr int kSgBigThreads = 1024;
+constexpr int kSgChunk = 4096;
+constexpr int kSgDenseCols = 16384;
+
+__global__ void __launch_bounds__(kSgBigThreads)
+k_sg_accum_big(const int* __restrict__ big, int bc, const int* __restrict__ arp, const int* __restrict__ aci,
+               const double* __restrict__ av, const int* __restrict__ brp, const int* __restrict__ bci,
+               const double* __restrict__ bv, const long long* __restrict__ off, int* __restrict__ scol,
+               double* __restrict__ sval, int* __restrict__ cnt) {
+    extern __shared__ __align__(16) unsigned char sgb_sm[];
+    double* acc = reinterpret_cast<double*>(sgb_sm);                                   // [kSgDenseCols]
+    double* pv = acc + kSgDenseCols;                                                   // [kSgChunk]
+    int* pc = reinterpret_cast<int*>(pv + kSgChunk);                                   // [kSgChunk]
+    unsigned* bits = reinterpret_cast<unsigned*>(pc + kSgChunk);                       // [kSgDenseCols / 32]
+    int* wpre = reinterpret_cast<int*>(bits + kSgDenseCols / 32);                      // [kSgDenseCols / 32 + 1]
+    const int i = big[blockIdx.x];
+    int* gcols = scol + off[i];
+    double* gvals = sval + off[i];
+    if (bc > kSgDenseCols) {
+        if (threadIdx.x == 0) {
+            int m = 0;
+            for (int a = arp[i]; a < arp[i + 1]; ++a) {
+                const int k = aci[a];
+                const double x = av[a];
+                for (int b = brp[k]; b < brp[k + 1]; ++b) {
+                    const int j = bci[b];
+                    const double prod = __dmul_rn(x, bv[b]);
+                    int lo = 0, hi = m;
+                    while (lo < hi) { const int mid = (lo + hi) >> 1; if (gcols[mid] < j) lo = mid + 1; else hi = mid; }
+                    if (lo < m && gcols[lo] == j) {
+                        gvals[lo] = __dadd_rn(gvals[lo], prod);
+                    } else {
+                        for (int q = m; q > lo; --q) { gcols[q] = gcols[q - 1]; gvals[q] = gvals[q - 1]; }
+                        gcols[lo] = j;
+                        gvals[lo] = __dadd_rn(0.0, prod);
+                        ++m;
+                    }
+                }
+            }
+            cnt[i] = m;
+        }
+        return;
+    }
+    const int nw = (bc + 31) / 32;
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) bits[w] = 0u;
+    __syncthreads();
+    // this thread's columns, accumulated over one staged chunk of products
+    auto process = [&](int np) {
+        for (int p = 0; p < np; ++p) {
+            const int c = pc[p];
+            if (c % kSgBigThreads != (int)threadIdx.x) continue;
+            const unsigned bit = 1u << (c & 31);
+            if (bits[c >> 5] & bit) {
+                acc[c] = __dadd_rn(acc[c], pv[p]);
             } else {
-                for (int q = m; q > lo; --q) { cols[q] = cols[q - 1]; vals[q] = vals[q - 1]; }
-                cols[lo] = j;
-                vals[lo] = __dadd_rn(0.0, prod);   // acc[j] = 0.0; acc[j] += ...
-                ++m;
+                acc[c] = __dadd_rn(0.0, pv[p]);
+                atomicOr(&bits[c >> 5], bit);
+            }
+        }
+    };
+    int fill = 0;
+    for (int a = arp[i]; a < arp[i + 1]; ++a) {
+        const int k = aci[a];
+        const double x = av[a];
+        int b0 = brp[k];
+        const int b1 = brp[k + 1];
+        while (b0 < b1) {
+            const int take = min(b1 - b0, kSgChunk - fill);
+            for (int q = threadIdx.x; q < take; q += blockDim.x) {
+                pc[fill + q] = bci[b0 + q];
+                pv[fill + q] = __dmul_rn(x, bv[b0 + q]);
+            }
+            fill += take;
+            b0 += take;
+            if (fill == kSgChunk) {
+                __syncthreads();
+                process(fill);
+                __syncthreads();
+                fill = 0;
             }
         }
     }
-    cnt[i] = m;
+    __syncthreads();
+    process(fill);
+    __syncthreads();
+    // touched columns in ascending order: per-word counts, an exclusive scan, then the writes
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int w = 0; w < nw; ++w) {
+            wpre[w] = run;
+            run += __popc(bits[w]);
+        }
+        wpre[nw] = run;
+        cnt[i] = run;
+    }
+    __syncthreads();
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+        unsigned m = bits[w];
+        int r = wpre[w];
+        while (m) {
+            const int bpos = __ffs(m) - 1;
+            const int c = w * 32 + bpos;
+            gcols[r] = c;
+            gvals[r] = acc[c];
+            ++r;
+            m &= m - 1u;
+        }
+    }
 }
 
 __global__ void k_sg_copy(int rows, const long long* __restrict__ off, const int* __restrict__ scol,
@@ -907,8 +1067,29 @@ static cfa_status spgemm(cfa_ctx* ctx, SetupScratch& S, int ar, int bc, const in
     CFA_CUDA(cudaMemcpyAsync(S.sg_off.p, h_off, (ar + 1) * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
     CFA_CUDA(S.sg_scol.ensure(std::max<long long>(total, 1)));
     CFA_CUDA(S.sg_sval.ensure(std::max<long long>(total, 1)));
-    CFA_LAUNCH(ctx, k_sg_accum, ceil_div(ar, 128), 128, 0, ar, arp, aci, av, brp, bci, bv, (const long long*)S.sg_off.p,
-               S.sg_scol.p, S.sg_sval.p, S.sg_cnt.p);
+    constexpr int sg_smem = kSgWarps * kSgCap * (int)(sizeof(double) + 2 * sizeof(int));
+    static std::once_flag sg_once;
+    std::call_once(sg_once, [] {
+        cudaFuncSetAttribute(k_sg_accum_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, sg_smem);
+    });
+    CFA_LAUNCH(ctx, k_sg_accum_warp, ceil_div(ar, kSgWarps), kSgWarps * 32, sg_smem, ar, arp, aci, av, brp, bci, bv,
+               (const long long*)S.sg_off.p, (const int*)S.sg_ub.p, S.sg_scol.p, S.sg_sval.p, S.sg_cnt.p);
+    // the rows with more products than the warp kernel stages
+    std::vector<int> big;
+    for (int i = 0; i < ar; ++i)
+        if (S.h_ub.p[i] > kSgCap) big.push_back(i);
+    if (!big.empty()) {
+        constexpr int big_smem = (kSgDenseCols + kSgChunk) * (int)sizeof(double) + kSgChunk * (int)sizeof(int) +
+                                 (kSgDenseCols / 32) * (int)sizeof(unsigned) + (kSgDenseCols / 32 + 1) * (int)sizeof(int);
+        static std::once_flag big_once;
+        std::call_once(big_once, [] {
+            cudaFuncSetAttribute(k_sg_accum_big, cudaFuncAttributeMaxDynamicSharedMemorySize, big_smem);
+        });
+        CFA_CUDA(S.sg_big.ensure(big.size()));
+        CFA_CUDA(cudaMemcpyAsync(S.sg_big.p, big.data(), big.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        CFA_LAUNCH(ctx, k_sg_accum_big, (int)big.size(), kSgBigThreads, big_smem, (const int*)S.sg_big.p, bc, arp, aci,
+                   av, brp, bci, bv, (const long long*)S.sg_off.p, S.sg_scol.p, S.sg_sval.p, S.sg_cnt.p);
+    }
     CFA_CUDA(cudaMemcpyAsync(S.h_cnt.p, S.sg_cnt.p, ar * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     int* h_rp = S.h_ub.p;   // reuse: C row pointer

@@ -50,7 +50,7 @@ struct HostBuf {
 
 // Setup temporaries, kept across setups (grow-only): no allocation in a repeated setup.
 struct SetupScratch {
-    DevBuf<int> sg_ub, sg_cnt, sg_scol, tr_keys, tr_idx, tr_perm, tr_row_of, cnt, p0rp, ierr;
+    DevBuf<int> sg_ub, sg_cnt, sg_scol, sg_big, tr_keys, tr_idx, tr_perm, tr_row_of, cnt, p0rp, ierr;
     DevBuf<long long> sg_off;
     DevBuf<double> sg_sval, pow_x, pow_y, pow_py, pow_px, pow_st, p0v, M, colbuf;
     DevBuf<unsigned char> strong;
