@@ -124,12 +124,14 @@ class BatchReport:
         return float(np.percentile([s.solve_ms for s in self.systems], q)) if self.systems else 0.0
 
 
-def solve_system(ctx: cfa.Context, sysm: BatchSystem, precision: int, tol: float) -> tuple:
-    """The system's solve path on ctx's stream; returns (SolveStep, device ms)."""
+def solve_system(ctx: cfa.Context, sysm: BatchSystem, precision: int, tol: float, reuse=None) -> tuple:
+    """The system's solve path on ctx's stream; returns (SolveStep, device ms). ``reuse``: the
+    previous system's SolveStep on this context, whose solver handles are taken over."""
     import torch
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
-    st = S.SolveStep(sysm.mesh, sysm.u, sysm.v, sysm.p, precision=precision, nu=sysm.nu, tol=tol, ctx=ctx)
+    st = S.SolveStep(sysm.mesh, sysm.u, sysm.v, sysm.p, precision=precision, nu=sysm.nu, tol=tol, ctx=ctx,
+                     reuse=reuse)
     st.amg_setup()          # assembly, ILU factor, BiCGSTAB2, pressure system, AMG setup
     st.solve_pressure()
     ev1.record()
@@ -138,9 +140,28 @@ def solve_system(ctx: cfa.Context, sysm: BatchSystem, precision: int, tol: float
 
 
 class BatchSolver:
+    """Solves batches of systems on ``streams`` worker threads, each with its own context (CUDA
+    stream). The contexts live as long as the solver, so the device blocks and workspaces one
+    batch grew serve the next one (``close()`` releases them)."""
+
     def __init__(self, precision: int = cfa.MIXED, streams: int = 4, tol: float = 1e-10, keep: bool = False):
         self.precision, self.streams, self.tol, self.keep = precision, streams, tol, keep
         self.results = {}     # seed -> (u, v, dp) host arrays when keep
+        self._ctxs = [None] * max(1, streams)
+        self._prev = [None] * max(1, streams)   # each worker's last SolveStep (its handles are reused)
+
+    def close(self):
+        self._prev = [None] * len(self._ctxs)
+        for i, c in enumerate(self._ctxs):
+            if c is not None:
+                c.close()
+                self._ctxs[i] = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def solve(self, systems: list) -> BatchReport:
         import torch
@@ -152,36 +173,43 @@ class BatchSolver:
         reports, errors, lock = [], [], threading.Lock()
         launches = [0]
 
-        def worker():
+        def worker(k):
             torch.cuda.set_device(dev)
-            ctx = cfa.Context()                     # own stream, current in this thread
+            if self._ctxs[k] is None:
+                self._ctxs[k] = cfa.Context()       # own stream, made current in this thread
+            ctx = self._ctxs[k]
+            torch.cuda.set_stream(ctx.stream)
+            launches0 = ctx.launches
+            prev = self._prev[k]
             try:
                 while True:
                     try:
                         sysm = work.get_nowait()
                     except queue.Empty:
                         return
-                    st, ms = solve_system(ctx, sysm, self.precision, self.tol)
+                    st, ms = solve_system(ctx, sysm, self.precision, self.tol, reuse=prev)
+                    prev = None
                     r = st.report()
                     rep = SystemReport(sysm.seed, st.n, st.nnz, ms, r["it_u"], r["it_v"], r["it_p"],
                                        all(r["conv"]), r["rel"])
+                    res = (st.u.cpu().numpy(), st.v.cpu().numpy(), st.dp.cpu().numpy()) if self.keep else None
                     with lock:
                         reports.append(rep)
                         if self.keep:
-                            self.results[sysm.seed] = (st.u.cpu().numpy(), st.v.cpu().numpy(), st.dp.cpu().numpy())
-                    del st
+                            self.results[sysm.seed] = res
+                    prev = st
             except Exception as e:               # reported to the caller after the join
                 with lock:
                     errors.append(e)
             finally:
+                self._prev[k] = prev
                 torch.cuda.current_stream().synchronize()
                 with lock:
-                    launches[0] += ctx.launches
-                ctx.close()
+                    launches[0] += ctx.launches - launches0
 
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        threads = [threading.Thread(target=worker) for _ in range(max(1, self.streams))]
+        threads = [threading.Thread(target=worker, args=(k,)) for k in range(len(self._ctxs))]
         for t in threads:
             t.start()
         for t in threads:

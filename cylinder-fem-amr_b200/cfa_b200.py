@@ -37,6 +37,15 @@ def lib():
     return _lib
 
 
+def mem_cached() -> tuple:
+    """(device bytes, pinned host bytes) held by the library's block cache."""
+    d, h = C.c_size_t(), C.c_size_t()
+    s = lib().cfa_mem_cached(C.byref(d), C.byref(h))
+    if s != CFA_OK:
+        raise CfaError(s, "cfa_mem_cached")
+    return d.value, h.value
+
+
 class CfaError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"cfa status {status}: {msg}")
@@ -114,6 +123,10 @@ class Context:
 
     def sync(self):
         self.check(lib().cfa_ctx_sync(self.h))
+
+    def trim(self):
+        """Synchronises and returns this context's cached device blocks (and the idle ones)."""
+        self.check(lib().cfa_mem_trim(self.h))
 
     def close(self):
         if getattr(self, "h", None):

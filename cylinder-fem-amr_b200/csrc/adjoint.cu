@@ -497,7 +497,7 @@ cfa_status cfa_momentum_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const double* u
                                 const double* x_u, const double* x_v, const double* lam_u, const double* lam_v,
                                 double* g_u_old, double* g_v_old, double* g_u_prev, double* g_v_prev,
                                 double* g_p_old, double* g_nu_node, double* d_scalars2) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && u_old && v_old && u_prev && v_prev && p_old && prm && bcp && x_u && x_v && lam_u && lam_v);
     CFA_ARG(g_u_old && g_v_old && g_u_prev && g_v_prev && g_p_old && d_scalars2 && (!g_nu_node || nu_node));
     AdjParams P{prm->nu, prm->rho, prm->a0, prm->a1, prm->a2, prm->c1, prm->c2, prm->tau_time, prm->skew_coef};
@@ -518,7 +518,7 @@ cfa_status cfa_momentum_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const double* u
 
 cfa_status cfa_ppe_rhs_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const double* lam_p, double dt_proj, double rho,
                                double* g_u, double* g_v) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && lam_p && g_u && g_v && dt_proj > 0.0);
     CFA_ARG(!m->bc.outlet_dirichlet);
     CFA_LAUNCH(ctx, k_ppe_rhs_adjoint, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y, m->tag, m->bc,
@@ -531,7 +531,7 @@ cfa_status cfa_oss_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const double* u_star
                            double rho, double nu, double stab, const double* elem_s, const double* mass_lumped,
                            const double* lam_p, const double* p_old, const double* dp, double* g_u, double* g_v,
                            double* g_p) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && u_star && v_star && elem_s && mass_lumped && lam_p && p_old && dp && g_u && g_v && g_p);
     CFA_ARG(dt_proj > 0.0 && stab > 0.0 && !m->bc.outlet_dirichlet);
     const int n = m->n, ne = m->ne;
@@ -555,7 +555,7 @@ cfa_status cfa_oss_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const double* u_star
 cfa_status cfa_projection_adjoint(cfa_ctx* ctx, const cfa_mesh* m, double dt_proj, double rho, double nu,
                                   const double* mass_lumped, const double* g_u_new, const double* g_v_new,
                                   const double* g_p_new, double* g_dp) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && mass_lumped && g_u_new && g_v_new && g_p_new && g_dp && g_dp != g_p_new);
     CFA_LAUNCH(ctx, k_projection_adjoint, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y, m->tag,
                m->bc, m->inc_ptr.p, m->inc.p, mass_lumped, dt_proj, rho, nu, g_u_new, g_v_new, g_p_new, g_dp);
@@ -569,7 +569,7 @@ cfa_status cfa_volume_forces_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const doub
                                      double nu, double rho, double wx, double wy, double* g_u, double* g_v,
                                      double* g_u_old, double* g_v_old, double* g_u_prev, double* g_v_prev,
                                      double* g_p) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && u && v && u_old && v_old && u_prev && v_prev && p && g_u && g_v && g_u_old && g_v_old && g_u_prev &&
             g_v_prev && g_p);
     DevBuf<double> g_elem;

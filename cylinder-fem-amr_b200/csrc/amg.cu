@@ -1218,7 +1218,8 @@ static cfa_status spectral_radius(cfa_ctx* ctx, cfa_amg* amg, const DCsr& A, con
     if (!amg->x0.p || amg->x0.cap < (size_t)n) {
         const std::vector<double> h = start_vector(n);
         CFA_CUDA(amg->x0.ensure(n));
-        CFA_CUDA(cudaMemcpy(amg->x0.p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+        // pageable source: the call returns once `h` has been staged
+        CFA_CUDA(cudaMemcpyAsync(amg->x0.p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     }
     CFA_CUDA(S.pow_x.ensure(n));
     CFA_CUDA(S.pow_y.ensure(n));
@@ -1565,7 +1566,8 @@ void cfa_amg_default_opts(cfa_amg_opts* o) {
 }
 
 cfa_status cfa_amg_create(cfa_ctx* ctx, const cfa_amg_opts* opts, cfa_amg** out) {
-    if (!ctx || !out) return CFA_BAD_ARG;
+    if (!out) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     auto* a = new cfa_amg();
     if (opts) a->opts = *opts; else cfa_amg_default_opts(&a->opts);
     if (a->opts.smooth_steps < 1 || a->opts.max_levels < 1 ||
@@ -1583,14 +1585,14 @@ cfa_status cfa_amg_destroy(cfa_amg* amg) {
 }
 
 cfa_status cfa_amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* rp, const int* ci, const double* v) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(amg && n > 0 && nnz > 0 && rp && ci && v);
     return amg_setup(ctx, amg, n, nnz, rp, ci, v);
 }
 
 cfa_status cfa_amg_remap(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* rp, const int* ci, const double* v,
                          const int* h_rp, const int* h_ci, const int* h_new_to_old) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(amg && n > 0 && nnz > 0 && rp && ci && v && h_rp && h_ci && h_new_to_old);
     bool remapped = false;
     return amg_remap(ctx, amg, n, nnz, rp, ci, v, h_rp, h_ci, h_new_to_old, remapped);
@@ -1599,7 +1601,7 @@ cfa_status cfa_amg_remap(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const int* 
 int cfa_amg_remaps(const cfa_amg* amg) { return amg ? amg->remaps : 0; }
 
 cfa_status cfa_amg_apply(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(amg && r && z && amg->coarse_n > 0);
     return amg_vcycle(ctx, amg, r, z, nullptr);
 }

@@ -28,21 +28,29 @@ struct AmgLevel {
     DevBuf<float> x32, t32, b32, r32;
 };
 
-// Pinned, grow-only host buffer
+// Pinned, grow-only host buffer (blocks from the pinned cache, pool.cu)
 template <class T>
 struct HostBuf {
     T* p = nullptr;
     size_t cap = 0;
+    size_t bytes = 0;
+    cudaStream_t owner = nullptr;
     cudaError_t ensure(size_t count) {
         if (count <= cap && p) return cudaSuccess;
-        if (p) cudaFreeHost(p);
+        if (p) pinned_release(p, bytes, owner);
         p = nullptr;
-        const size_t c = count + count / 2 + 64;
-        cudaError_t e = cudaMallocHost(&p, c * sizeof(T));
-        cap = e == cudaSuccess ? c : 0;
-        return e;
+        cap = bytes = 0;
+        size_t b = (count + count / 2 + 64) * sizeof(T);
+        void* q = nullptr;
+        cudaError_t e = pinned_alloc(&q, &b);
+        if (e != cudaSuccess) return e;
+        p = static_cast<T*>(q);
+        bytes = b;
+        cap = b / sizeof(T);
+        owner = scope_stream();
+        return cudaSuccess;
     }
-    ~HostBuf() { if (p) cudaFreeHost(p); }
+    ~HostBuf() { if (p) pinned_release(p, bytes, owner); }
     HostBuf() = default;
     HostBuf(const HostBuf&) = delete;
     HostBuf& operator=(const HostBuf&) = delete;

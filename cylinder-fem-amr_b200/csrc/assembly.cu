@@ -386,7 +386,7 @@ cfa_status cfa_assemble_momentum_nu(cfa_ctx* ctx, const cfa_mesh* m, const doubl
                                     const cfa_momentum_params* prm, const double* nu_node,
                                     const cfa_momentum_bc* bcp, double* A_val, double* rhs_u, double* rhs_v,
                                     double* mass, double* u, double* v) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && u_old && v_old && u_prev && v_prev && p_old && prm && A_val && rhs_u && rhs_v && mass);
     CFA_ARG(!bcp || (u && v));
     MomParams P{prm->dt, prm->nu, prm->rho, prm->a0, prm->a1, prm->a2, prm->c1, prm->c2, prm->tau_time, prm->skew_coef};
@@ -403,7 +403,7 @@ cfa_status cfa_assemble_momentum_nu(cfa_ctx* ctx, const cfa_mesh* m, const doubl
 
 cfa_status cfa_apply_bc_momentum(cfa_ctx* ctx, const cfa_mesh* m, const cfa_momentum_bc* bcp, double* A_val,
                                  double* rhs_u, double* rhs_v, double* u, double* v) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && bcp && A_val && rhs_u && rhs_v);
     CFA_LAUNCH(ctx, k_momentum_bc, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->tag, m->y, m->rp, m->ci,
                bcp->u_max, bcp->H, m->bc, 1, A_val, rhs_u, rhs_v, u, v);
@@ -412,7 +412,7 @@ cfa_status cfa_apply_bc_momentum(cfa_ctx* ctx, const cfa_mesh* m, const cfa_mome
 }
 
 cfa_status cfa_lumped_mass(cfa_ctx* ctx, const cfa_mesh* m, double* mass) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && mass);
     CFA_LAUNCH(ctx, k_lumped_mass_rows, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y,
                m->inc_ptr.p, m->inc.p, mass);
@@ -422,7 +422,7 @@ cfa_status cfa_lumped_mass(cfa_ctx* ctx, const cfa_mesh* m, double* mass) {
 
 cfa_status cfa_oss_weights(cfa_ctx* ctx, const cfa_mesh* m, const double* us, const double* vs, double dt,
                            double rho, double nu, double stab, double* elem_s) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && us && vs && elem_s);
     CFA_LAUNCH(ctx, k_oss_weights, ceil_div(m->ne, kThreads), kThreads, 0, m->ne, m->ev, m->x, m->y, us, vs, dt,
                rho, nu, stab, elem_s);
@@ -432,7 +432,7 @@ cfa_status cfa_oss_weights(cfa_ctx* ctx, const cfa_mesh* m, const double* us, co
 
 cfa_status cfa_scalar_gradient(cfa_ctx* ctx, const cfa_mesh* m, const double* f, const double* elem_s, double* gx,
                                double* gy) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && f && gx && gy);
     CFA_LAUNCH(ctx, k_scalar_gradient_rows, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y,
                m->inc_ptr.p, m->inc.p, f, elem_s, gx, gy);
@@ -466,7 +466,7 @@ static cfa_status assemble_pressure(cfa_ctx* ctx, const cfa_mesh* m, const doubl
 cfa_status cfa_assemble_ppe(cfa_ctx* ctx, const cfa_mesh* m, const double* us, const double* vs, const double* p_old,
                             const double* gpx, const double* gpy, const double* mass, const double* elem_s, double dt,
                             double rho, double stab, int apply_bc, double* Kp, double* rhs, double* div, double* dp) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && us && vs && Kp && rhs && div);
     CFA_ARG(!(stab > 0.0) || (p_old && gpx && gpy && mass && elem_s));
     return assemble_pressure(ctx, m, us, vs, p_old, gpx, gpy, mass, elem_s, dt, rho, stab, apply_bc, Kp, rhs, div,
@@ -475,7 +475,7 @@ cfa_status cfa_assemble_ppe(cfa_ctx* ctx, const cfa_mesh* m, const double* us, c
 
 cfa_status cfa_apply_bc_pressure(cfa_ctx* ctx, const cfa_mesh* m, double* Kp, double* rhs, double* dp,
                                  const double* mass) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && Kp && rhs);
     const double* sums = nullptr;
     if (m->bc.outlet_dirichlet) {
@@ -493,7 +493,7 @@ cfa_status cfa_apply_bc_pressure(cfa_ctx* ctx, const cfa_mesh* m, double* Kp, do
 
 cfa_status cfa_assemble_oss(cfa_ctx* ctx, const cfa_mesh* m, const double* elem_s, const double* mass,
                             double* oss_val, double* inv_m) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && elem_s && mass && oss_val && inv_m);
     // The B/B^T rows are produced by the pressure-row pass; K, RHS and div go to scratch here.
     DevBuf<double> scratch;
@@ -513,7 +513,7 @@ cfa_status cfa_assemble_pressure_system(cfa_ctx* ctx, const cfa_mesh* m, const d
                                         const double* mass, const double* elem_s, double dt, double rho,
                                         double stab, double* Kp, double* rhs, double* div, double* dp,
                                         double* oss_val, double* inv_m) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && us && vs && Kp && rhs && div);
     CFA_ARG(!(stab > 0.0) || (p_old && gpx && gpy && mass && elem_s && oss_val && inv_m));
     return assemble_pressure(ctx, m, us, vs, p_old, gpx, gpy, mass, elem_s, dt, rho, stab, 1, Kp, rhs, div, dp,

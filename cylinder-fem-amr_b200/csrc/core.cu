@@ -182,6 +182,8 @@ cfa_status cfa_ctx_create(void* stream, cfa_ctx** out) {
         cfa_ctx_destroy(ctx);
         return CFA_CUDA_ERROR;
     }
+    pool_stream_live(ctx->stream, ctx->device);
+    ctx->pooled = true;
     *out = ctx;
     return CFA_OK;
 }
@@ -189,6 +191,11 @@ cfa_status cfa_ctx_create(void* stream, cfa_ctx** out) {
 cfa_status cfa_ctx_destroy(cfa_ctx* ctx) {
     if (!ctx) return CFA_OK;
     free_solver_work(ctx);
+    if (ctx->pooled) {
+        // the stream's cached blocks become idle once its work has finished
+        cudaStreamSynchronize(ctx->stream);
+        pool_stream_retire(ctx->stream);
+    }
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->d_part) cudaFree(ctx->d_part);
@@ -218,8 +225,20 @@ const char* cfa_status_string(cfa_status s) {
 
 long long cfa_ctx_kernel_launches(const cfa_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+cfa_status cfa_mem_trim(cfa_ctx* ctx) {
+    if (ctx) CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    pool_trim(ctx ? ctx->stream : nullptr);
+    return CFA_OK;
+}
+
+cfa_status cfa_mem_cached(size_t* device_bytes, size_t* pinned_bytes) {
+    if (!device_bytes || !pinned_bytes) return CFA_BAD_ARG;
+    pool_stats(device_bytes, pinned_bytes);
+    return CFA_OK;
+}
+
 cfa_status cfa_ctx_sync(cfa_ctx* ctx) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     return CFA_OK;
 }
@@ -228,7 +247,7 @@ cfa_status cfa_ctx_sync(cfa_ctx* ctx) {
 // C ABI: CSR pattern
 // =============================================================================================
 cfa_status cfa_csr_count(cfa_ctx* ctx, int n, int ne, const int* d_ev, int* d_rp, int* nnz_out) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(n > 0 && ne >= 0 && d_ev && d_rp && nnz_out);
     DevBuf<int> inc_ptr, inc, len, err;
     CFA_PROPAGATE(build_incidence(ctx, n, ne, d_ev, inc_ptr, inc));
@@ -253,7 +272,7 @@ cfa_status cfa_csr_count(cfa_ctx* ctx, int n, int ne, const int* d_ev, int* d_rp
 }
 
 cfa_status cfa_csr_fill(cfa_ctx* ctx, int n, int ne, const int* d_ev, const int* d_rp, int* d_ci) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(n > 0 && ne >= 0 && d_ev && d_rp && d_ci);
     DevBuf<int> inc_ptr, inc;
     CFA_PROPAGATE(build_incidence(ctx, n, ne, d_ev, inc_ptr, inc));
@@ -268,7 +287,8 @@ cfa_status cfa_csr_fill(cfa_ctx* ctx, int n, int ne, const int* d_ev, const int*
 // =============================================================================================
 cfa_status cfa_mesh_create(cfa_ctx* ctx, int n, int ne, const int* d_ev, const double* d_x, const double* d_y,
                            const int* d_tag, const int* d_rp, const int* d_ci, cfa_mesh** out) {
-    if (!ctx || !out) return CFA_BAD_ARG;
+    if (!out) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(n > 0 && ne > 0 && d_ev && d_x && d_y && d_tag && d_rp && d_ci);
     auto* m = new cfa_mesh();
     m->uid = next_uid();

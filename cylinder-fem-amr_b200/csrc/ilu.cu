@@ -400,7 +400,8 @@ extern "C" {
 
 cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, const int* d_rp, const int* d_ci,
                           cfa_precision precision, cfa_ilu** out) {
-    if (!ctx || !out) return CFA_BAD_ARG;
+    if (!out) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(n > 0 && rp && ci && d_rp && d_ci);
     CFA_ARG(precision == CFA_FP64 || precision == CFA_MIXED);
     *out = nullptr;
@@ -417,7 +418,7 @@ cfa_status cfa_ilu_create(cfa_ctx* ctx, int n, const int* rp, const int* ci, con
 
 cfa_status cfa_ilu_set_pattern(cfa_ctx* ctx, cfa_ilu* h, int n, const int* rp, const int* ci, const int* d_rp,
                                const int* d_ci) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(h && n > 0 && rp && ci && d_rp && d_ci);
     return ilu_pattern(ctx, h, n, rp, ci, d_rp, d_ci);
 }
@@ -428,7 +429,7 @@ cfa_status cfa_ilu_destroy(cfa_ilu* ilu) {
 }
 
 cfa_status cfa_ilu_factor(cfa_ctx* ctx, cfa_ilu* h, const double* val) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(h && val);
     CFA_CUDA(cudaMemcpyAsync(h->lu.p, val, (size_t)h->nnz * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     for (int c = 1; c < h->nc; ++c) {
@@ -472,7 +473,7 @@ static cfa_status ensure_mirror(cfa_ctx* ctx, cfa_ilu* h) {
 extern "C" {
 
 cfa_status cfa_ilu_factor_transposed(cfa_ctx* ctx, cfa_ilu* h, const double* val) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(h && val);
     CFA_PROPAGATE(ensure_mirror(ctx, h));
     CFA_PROPAGATE(cfa_ilu_factor(ctx, h, val));
@@ -490,7 +491,7 @@ cfa_status cfa_ilu_factor_transposed(cfa_ctx* ctx, cfa_ilu* h, const double* val
 }
 
 cfa_status cfa_csr_transpose_values(cfa_ctx* ctx, cfa_ilu* h, const double* val, double* val_t) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(h && val && val_t && val != val_t);
     CFA_PROPAGATE(ensure_mirror(ctx, h));
     CFA_LAUNCH(ctx, k_transpose_values, ceil_div(h->nnz, kThreads), kThreads, 0, h->nnz, (const int*)h->tpos.p, val,
@@ -500,7 +501,7 @@ cfa_status cfa_csr_transpose_values(cfa_ctx* ctx, cfa_ilu* h, const double* val,
 }
 
 cfa_status cfa_ilu_apply(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z, int nrhs) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(h && r && z && (nrhs == 1 || nrhs == 2));
     CFA_ARG(r != z);
     return ilu_apply(ctx, h, r, z, nrhs, nullptr);

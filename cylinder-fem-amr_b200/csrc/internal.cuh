@@ -27,6 +27,7 @@ struct SolverWork;
 struct cfa_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;              // created here when the caller passed the legacy stream
+    bool pooled = false;                  // its stream is registered with the block cache
     int device = 0;
     int num_sms = 148;
     std::string err;
@@ -68,34 +69,74 @@ cfa_status set_error(cfa_ctx* ctx, cfa_status s, const char* what, const char* f
 // when it is a template-id with commas).
 #define CFA_LAUNCH(ctx, kernel, grid, block, smem, ...) ::cfa::launch((ctx), kernel, (grid), (block), (smem), __VA_ARGS__)
 
-// Growable device buffer (geometric growth, as the reference's workspaces, linalg.cuh:132-151).
+// Block cache behind the buffers (pool.cu). A scope names the stream (a context's) that the
+// allocations of the current thread are ordered on; CFA_ENTER opens one at every C ABI entry.
+struct StreamScope {
+    cudaStream_t prev_stream;
+    int prev_device;
+    StreamScope(cudaStream_t s, int device);
+    ~StreamScope();
+    StreamScope(const StreamScope&) = delete;
+    StreamScope& operator=(const StreamScope&) = delete;
+};
+cudaStream_t scope_stream();
+void pool_stream_live(cudaStream_t s, int device);
+void pool_stream_retire(cudaStream_t s);    // after the stream has been synchronised
+cudaError_t pool_alloc(void** p, size_t* bytes, cudaStream_t* owner, int* device);
+void pool_release(void* p, size_t bytes, cudaStream_t owner, int device);
+cudaError_t pinned_alloc(void** p, size_t* bytes);
+void pinned_release(void* p, size_t bytes, cudaStream_t owner);
+void pool_trim(cudaStream_t s);
+void pool_stats(size_t* device_cached, size_t* pinned_cached);
+
+#define CFA_ENTER(ctx_)                  \
+    if (!(ctx_)) return CFA_BAD_ARG;     \
+    ::cfa::StreamScope cfa_scope_((ctx_)->stream, (ctx_)->device)
+
+// Growable device buffer (geometric growth, as the reference's workspaces, linalg.cuh:132-151);
+// its blocks come from the cache, ordered on the stream of the scope that allocated them.
 template <class T>
 struct DevBuf {
     T* p = nullptr;
     size_t cap = 0;
+    size_t bytes = 0;
+    cudaStream_t owner = nullptr;
+    int dev = -1;
     cudaError_t ensure(size_t count) {
         if (count <= cap && p) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        size_t c = count + count / 2 + 64;
-        cudaError_t e = cudaMalloc(&p, c * sizeof(T));
-        cap = e == cudaSuccess ? c : 0;
-        return e;
+        release();
+        size_t b = (count + count / 2 + 64) * sizeof(T);
+        void* q = nullptr;
+        cudaError_t e = pool_alloc(&q, &b, &owner, &dev);
+        if (e != cudaSuccess) return e;
+        p = static_cast<T*>(q);
+        bytes = b;
+        cap = b / sizeof(T);
+        return cudaSuccess;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) pool_release(p, bytes, owner, dev);
         p = nullptr;
-        cap = 0;
+        cap = bytes = 0;
+        owner = nullptr;
+        dev = -1;
     }
     ~DevBuf() { release(); }
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : p(o.p), cap(o.cap) { o.p = nullptr; o.cap = 0; }
+    DevBuf(DevBuf&& o) noexcept : p(o.p), cap(o.cap), bytes(o.bytes), owner(o.owner), dev(o.dev) { o.forget(); }
     DevBuf& operator=(DevBuf&& o) noexcept {
-        if (this != &o) { release(); p = o.p; cap = o.cap; o.p = nullptr; o.cap = 0; }
+        if (this != &o) {
+            release();
+            p = o.p; cap = o.cap; bytes = o.bytes; owner = o.owner; dev = o.dev;
+            o.forget();
+        }
         return *this;
     }
+
+  private:
+    void forget() { p = nullptr; cap = bytes = 0; owner = nullptr; dev = -1; }
 };
 
 template <class... P, class... A>

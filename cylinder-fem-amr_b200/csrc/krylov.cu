@@ -1649,12 +1649,11 @@ static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* re
     int h_err = 0;
     CFA_CUDA(cudaMemcpyAsync(&h, W.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaMemcpyAsync(&h_err, W.err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     int h_amg_err = 0;
-    if (a.amg && a.amg->err.p) {
-        CFA_CUDA(cudaMemcpy(&h_amg_err, a.amg->err.p, sizeof(int), cudaMemcpyDeviceToHost));
-        if (h_amg_err) cudaMemsetAsync(a.amg->err.p, 0, sizeof(int), ctx->stream);
-    }
+    if (a.amg && a.amg->err.p)
+        CFA_CUDA(cudaMemcpyAsync(&h_amg_err, a.amg->err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (h_amg_err) cudaMemsetAsync(a.amg->err.p, 0, sizeof(int), ctx->stream);
     if (h_err || h_amg_err) {
         cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream);
         return set_error(ctx, CFA_TIMEOUT, "a bounded wait of a tile pipeline timed out", __FILE__, __LINE__);
@@ -1849,7 +1848,7 @@ using namespace cfa;
 extern "C" {
 
 cfa_status cfa_spmv(cfa_ctx* ctx, int n, const int* rp, const int* ci, const double* val, const double* x, double* y) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(n > 0 && rp && ci && val && x && y);
     const int tpr = 4;
     CFA_LAUNCH(ctx, (k_spmv<4, 1>), row_grid(ctx, n, tpr), kThreads, 0, n, rp, ci, val, x, y);
@@ -1859,7 +1858,7 @@ cfa_status cfa_spmv(cfa_ctx* ctx, int n, const int* rp, const int* ci, const dou
 
 cfa_status cfa_spmv_multi(cfa_ctx* ctx, int n, int nrhs, const int* rp, const int* ci, const double* val,
                           const double* x, double* y) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(n > 0 && (nrhs == 1 || nrhs == 2) && rp && ci && val && x && y);
     if (nrhs == 1) CFA_LAUNCH(ctx, (k_spmv<4, 1>), row_grid(ctx, n, 4), kThreads, 0, n, rp, ci, val, x, y);
     else CFA_LAUNCH(ctx, (k_spmv<4, 2>), row_grid(ctx, n, 4), kThreads, 0, n, rp, ci, val, x, y);
@@ -1869,7 +1868,7 @@ cfa_status cfa_spmv_multi(cfa_ctx* ctx, int n, int nrhs, const int* rp, const in
 
 cfa_status cfa_pressure_operator_prepare(cfa_ctx* ctx, int n, int nnz, const int* rp, const int* ci, const double* val,
                                          const cfa_oss_operator* oss) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(n > 0 && nnz > 0 && rp && ci && val);
     CFA_ARG(!oss || (oss->mesh && oss->d_oss_val && oss->d_inv_m && oss->mesh->n == n));
     PcgWork& W = work(ctx)->pcg;
@@ -1889,7 +1888,8 @@ cfa_status cfa_pressure_operator_prepare(cfa_ctx* ctx, int n, int nnz, const int
 }
 
 cfa_status cfa_pressure_operator_layout(const cfa_ctx* ctx, int* passes, long long* stored_nnz) {
-    if (!ctx || !ctx->work) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
+    if (!ctx->work) return CFA_BAD_ARG;
     const PcgWork& W = ctx->work->pcg;
     if (W.prepared.empty()) return CFA_BAD_ARG;
     const bool two = W.tiled && W.tb.nnz > 0 && !W.fused;
@@ -1900,7 +1900,7 @@ cfa_status cfa_pressure_operator_layout(const cfa_ctx* ctx, int* passes, long lo
 
 cfa_status cfa_pressure_operator(cfa_ctx* ctx, int n, int nnz, const int* rp, const int* ci, const double* val,
                                  const cfa_oss_operator* oss, const double* x, double* y) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(n > 0 && nnz > 0 && rp && ci && val && x && y);
     CFA_ARG(!oss || (oss->mesh && oss->d_oss_val && oss->d_inv_m && oss->mesh->n == n));
     PcgWork& W = work(ctx)->pcg;
@@ -1915,7 +1915,7 @@ cfa_status cfa_pressure_operator(cfa_ctx* ctx, int n, int nnz, const int* rp, co
 
 cfa_status cfa_oss_apply(cfa_ctx* ctx, const cfa_mesh* m, const double* oss_val, const double* inv_m, const double* in,
                          double* out) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && oss_val && inv_m && in && out);
     // out -= B^T M^-1 B in: pass 1 into the PCG scratch g, pass 2 with K = 0 contributions
     PcgWork& W = work(ctx)->pcg;
@@ -1939,7 +1939,7 @@ cfa_status cfa_oss_apply(cfa_ctx* ctx, const cfa_mesh* m, const double* oss_val,
 cfa_status cfa_pcg_solve(cfa_ctx* ctx, int n, const int* rp, const int* ci, const double* val, const double* b,
                          double* x, const cfa_oss_operator* oss, cfa_amg* amg, const cfa_solve_opts* opts,
                          cfa_solve_report* rep) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(n > 0 && rp && ci && val && b && x && opts && opts->max_iter >= 0);
     CFA_ARG(!oss || (oss->mesh && oss->d_oss_val && oss->d_inv_m && oss->mesh->n == n));
     CFA_ARG(!amg || (amg->coarse_n > 0 && (amg->levels.empty() ? amg->coarse_n == n : amg->levels[0].A.rows == n)));
@@ -1959,7 +1959,7 @@ cfa_status cfa_pcg_solve_host_ops(cfa_ctx* ctx, int n, const int* rp, const int*
                                   const double* b, double* x, cfa_host_op extra_op, void* extra_user, cfa_amg* amg,
                                   cfa_host_op precond, void* precond_user, const cfa_solve_opts* opts,
                                   cfa_solve_report* rep) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(n > 0 && rp && ci && val && b && x && opts && opts->max_iter >= 0 && !(amg && precond));
     CFA_ARG(!amg || (amg->coarse_n > 0 && (amg->levels.empty() ? amg->coarse_n == n : amg->levels[0].A.rows == n)));
     int nnz = 0;
@@ -1981,7 +1981,7 @@ cfa_status cfa_pcg_solve_host_ops(cfa_ctx* ctx, int n, const int* rp, const int*
 cfa_status cfa_bicgstab2_solve(cfa_ctx* ctx, int n, const int* rp, const int* ci, const double* val, const double* bu,
                                const double* bv, double* xu, double* xv, const cfa_ilu* ilu, const cfa_solve_opts* opts,
                                cfa_solve_report* rep) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(n > 0 && rp && ci && val && bu && bv && xu && xv && ilu && opts && ilu->n == n && opts->max_iter > 0);
     B2Args a{n, ilu->nnz, rp, ci, val, bu, bv, xu, xv, ilu, opts->max_iter, opts->tol};
     return b2_solve(ctx, a, rep);
@@ -1989,7 +1989,7 @@ cfa_status cfa_bicgstab2_solve(cfa_ctx* ctx, int n, const int* rp, const int* ci
 
 cfa_status cfa_bicgstab_solve(cfa_ctx* ctx, int n, const int* rp, const int* ci, const double* val, const double* b,
                               double* x, const cfa_solve_opts* opts, cfa_solve_report* rep) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(n > 0 && rp && ci && val && b && x && opts);
     DevBuf<double> r, r0, p, v, s, t, phat, shat, dinv, dots;
     for (DevBuf<double>* buf : {&r, &r0, &p, &v, &s, &t, &phat, &shat, &dinv}) CFA_CUDA(buf->ensure(n));
@@ -2138,7 +2138,7 @@ extern "C" {
 
 cfa_status cfa_oss_apply_noalloc(cfa_ctx* ctx, const cfa_mesh* m, const double* oss_val, const double* inv_m,
                                  const double* in, double* out) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && oss_val && inv_m && in && out);
     const int n = m->n;
     if (n > kOssStaticRows)

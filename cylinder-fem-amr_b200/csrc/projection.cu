@@ -213,7 +213,7 @@ using namespace cfa;
 extern "C" {
 
 cfa_status cfa_stiffness_apply(cfa_ctx* ctx, const cfa_mesh* m, const double* f, double c, double* out) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && f && out);
     CFA_LAUNCH(ctx, k_node_gradients, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y, m->inc_ptr.p,
                m->inc.p, f, c, out, (const double*)nullptr, (const double*)nullptr, (const double*)nullptr,
@@ -224,7 +224,7 @@ cfa_status cfa_stiffness_apply(cfa_ctx* ctx, const cfa_mesh* m, const double* f,
 
 cfa_status cfa_grad_dp_vorticity(cfa_ctx* ctx, const cfa_mesh* m, const double* dp, const double* u,
                                  const double* v, double* grad_dp_x, double* grad_dp_y, double* vort_num) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && dp && u && v && grad_dp_x && grad_dp_y && vort_num);
     CFA_LAUNCH(ctx, k_node_gradients, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y, m->inc_ptr.p,
                m->inc.p, (const double*)nullptr, 0.0, (double*)nullptr, dp, u, v, grad_dp_x, grad_dp_y, vort_num);
@@ -237,7 +237,7 @@ cfa_status cfa_velocity_pressure_correction(cfa_ctx* ctx, const cfa_mesh* m, dou
                                             const double* grad_dp_x, const double* grad_dp_y,
                                             const double* vort_num, const double* dp, double* u, double* v,
                                             double* p, double* vort) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && div_num && mass_lumped && grad_dp_x && grad_dp_y && dp && u && v && p && (!vort || vort_num));
     CFA_LAUNCH(ctx, k_correction, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->tag, m->bc, dt, rho, p_update,
                rot_coeff, div_num, mass_lumped, grad_dp_x, grad_dp_y, vort_num, dp, u, v, p, vort);
@@ -249,7 +249,7 @@ cfa_status cfa_project_step(cfa_ctx* ctx, const cfa_mesh* m, double dt_proj, dou
                             int rotational_from_dp, const double* mass_lumped, const double* dp, double* div_num,
                             double* grad_dp_x, double* grad_dp_y, double* vort_num, double* u, double* v, double* p,
                             double* vort) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && mass_lumped && dp && div_num && grad_dp_x && grad_dp_y && vort_num && u && v && p);
     if (rotational_from_dp) CFA_CUDA(cudaMemsetAsync(div_num, 0, (size_t)m->n * sizeof(double), ctx->stream));
     CFA_LAUNCH(ctx, k_node_gradients, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y, m->inc_ptr.p,
@@ -265,7 +265,7 @@ cfa_status cfa_project_step(cfa_ctx* ctx, const cfa_mesh* m, double dt_proj, dou
 cfa_status cfa_volume_forces(cfa_ctx* ctx, const cfa_mesh* m, const double* u, const double* v, const double* u_old,
                              const double* v_old, const double* u_prev, const double* v_prev, const double* p,
                              double b0, double b1, double b2, double nu, double rho, double* d_out2) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && u && v && u_old && v_old && u_prev && v_prev && p && d_out2);
     const int grid = std::min(ceil_div(m->ne, kThreads), 4 * ctx->num_sms);
     CFA_PROPAGATE(ensure_partials(ctx, 2 * (size_t)grid + 2));
@@ -277,7 +277,7 @@ cfa_status cfa_volume_forces(cfa_ctx* ctx, const cfa_mesh* m, const double* u, c
 
 cfa_status cfa_recovered_gradient(cfa_ctx* ctx, const cfa_mesh* m, const double* u, const double* v, double u_max,
                                   double H, double* grad_rec) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && u && v && grad_rec && H > 0.0);
     CFA_LAUNCH(ctx, k_recovered_gradient, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y,
                m->inc_ptr.p, m->inc.p, u, v, u_max, H, grad_rec);
@@ -287,7 +287,7 @@ cfa_status cfa_recovered_gradient(cfa_ctx* ctx, const cfa_mesh* m, const double*
 
 cfa_status cfa_amr_error_indicator(cfa_ctx* ctx, const cfa_mesh* m, const double* grad_rec, const double* mass_lumped,
                                    double* elem_error) {
-    if (!ctx) return CFA_BAD_ARG;
+    CFA_ENTER(ctx);
     CFA_ARG(m && grad_rec && mass_lumped && elem_error);
     CFA_LAUNCH(ctx, k_amr_indicator, ceil_div(m->ne, kThreads), kThreads, 0, m->ne, m->n, m->ev, m->x, m->y, grad_rec,
                mass_lumped, elem_error);

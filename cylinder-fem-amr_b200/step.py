@@ -19,7 +19,11 @@ import cfa_b200 as cfa
 
 class SolveStep:
     def __init__(self, mesh, u_n, v_n, p_n, precision=cfa.FP64, dt=1e-3, nu=1e-3, rho=1.0, tau_time=1e-3,
-                 stab=0.3, u_max=1.5, H=1.0, tol=1e-10, max_it_mom=1000, max_it_p=4000, ctx=None, dm=None):
+                 stab=0.3, u_max=1.5, H=1.0, tol=1e-10, max_it_mom=1000, max_it_p=4000, ctx=None, dm=None,
+                 reuse=None):
+        """``reuse``: an earlier SolveStep on the same context whose ILU, AMG and Krylov handles
+        this one takes over (their device buffers only grow, so a sequence of systems allocates
+        nothing once the largest has been seen); the earlier step must not be used afterwards."""
         import torch
         self.ctx = ctx or cfa.default_context()
         self.dm = dm or cfa.DeviceMesh(self.ctx, mesh)
@@ -44,11 +48,15 @@ class SolveStep:
         self.dt_proj = (2.0 / 3.0) * dt
         self.tol, self.max_it_mom, self.max_it_p = tol, max_it_mom, max_it_p
         rp_h, ci_h = self.dm.host_pattern()
-        self.ilu = cfa.MulticolourIlu0(self.ctx, precision)
+        if reuse is not None and reuse.ctx is self.ctx and reuse.precision == precision:
+            self.ilu, self.mom, self.solver, self.amg = reuse.ilu, reuse.mom, reuse.solver, reuse.amg
+            reuse.ilu = reuse.mom = reuse.solver = reuse.amg = None
+        else:
+            self.ilu = cfa.MulticolourIlu0(self.ctx, precision)
+            self.mom = cfa.GpuBicgstab2(self.ctx)
+            self.solver = cfa.GpuLinearSolver(self.ctx)
+            self.amg = cfa.AmgPreconditioner(self.ctx, precision)
         self.ilu.set_pattern(n, rp_h, ci_h, self.dm.rp, self.dm.ci)
-        self.mom = cfa.GpuBicgstab2(self.ctx)
-        self.solver = cfa.GpuLinearSolver(self.ctx)
-        self.amg = cfa.AmgPreconditioner(self.ctx, precision)
         self.oss = cfa.oss_operator(self.dm, self.oss_val, self.inv_m) if stab > 0.0 else None
         self.precision = precision
         self.it_p = 0

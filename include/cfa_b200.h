@@ -21,6 +21,8 @@
 #ifndef CFA_B200_H
 #define CFA_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -58,6 +60,17 @@ const char* cfa_status_string(cfa_status s);
 long long cfa_ctx_kernel_launches(const cfa_ctx* ctx);
 /* Synchronises the context's stream. */
 cfa_status cfa_ctx_sync(cfa_ctx* ctx);
+
+/* Device memory of the library's buffers comes from a block cache. A block that a resized or
+ * destroyed buffer lets go is reused, in stream order, by later allocations of the context that
+ * allocated it, and becomes free for any context of the device once that context is destroyed
+ * (the reference calls cudaMalloc/cudaFree at every resize, src/cfa/linalg.cuh:131-151, and
+ * cudaFree waits for the whole device). A handle (mesh, ILU, AMG, OSS operator) used from a second
+ * context needs that context ordered after the first (cfa_ctx_sync).
+ * cfa_mem_trim synchronises ctx (may be NULL) and returns the blocks cached for ctx's stream and
+ * the idle ones to the device; cfa_mem_cached reports the device and pinned host bytes held. */
+cfa_status cfa_mem_trim(cfa_ctx* ctx);
+cfa_status cfa_mem_cached(size_t* device_bytes, size_t* pinned_bytes);
 
 /* ---------------------------------------------------------------------------------------------
  * CSR pattern of the P1 mesh graph: node i's row holds i and the vertices of its elements,
