@@ -424,6 +424,221 @@ __global__ void k_chol_inverse(int cn, const double* __restrict__ M, double* __r
     for (int i = 0; i < cn; ++i) inv[(size_t)i * cn + c] = col[i];
 }
 
+// Blocked form of the same Cholesky (dense_spd_inverse, :1396-1410), one CTA. Every entry still
+// receives its terms one at a time in ascending k: s_ij -= L_ik L_jk for k = 0, 1, ..., j-1, then
+// L_ij = s_ij / L_jj (the reference sums the same terms in the same order, left-looking); only
+// the moment each term is applied changes. Panels of kCholPanel columns are factored in shared
+// memory (rows p0.., stride kCholStride); the entries right of a panel then take the panel's terms
+// in ascending k, 4x4 entries per thread. L is written to M (row-major) and to Lt (Lt[k cn + i] =
+// L_ik, both triangles' roles swapped) for the inverse.
+constexpr int kCholPanel = 32;
+constexpr int kCholStride = 33;        // padded row stride of the panel (conflict-free columns)
+constexpr int kCholThreads = 512;
+constexpr int kInvCols = 32;           // columns of the inverse per CTA (one thread each)
+constexpr size_t kCoarseSmemMax = 200 * 1024;
+
+inline size_t chol_smem(int cn) { return (size_t)(cn + 4) * kCholStride * sizeof(double); }
+// x vectors (cn x kInvCols), two staged rows of Lt and the diagonal of L
+inline size_t inv_smem(int cn) { return (size_t)cn * (kInvCols + 3) * sizeof(double); }
+inline bool coarse_blocked(int cn) { return chol_smem(cn) <= kCoarseSmemMax && inv_smem(cn) <= kCoarseSmemMax; }
+
+__global__ void __launch_bounds__(kCholThreads) k_coarse_cholesky(int cn, double* __restrict__ M, double* __restrict__ Lt,
+                                                                   int* __restrict__ err) {
+    extern __shared__ double P[];      // (cn + 4) x kCholStride
+    __shared__ double piv[kCholPanel];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    int bad = 0;
+    for (int p0 = 0; p0 < cn && !bad; p0 += kCholPanel) {
+        const int pw = min(kCholPanel, cn - p0);
+        const int R = cn - p0;
+        // the panel: rows p0..cn-1 of columns p0..p0+pw-1 (+4 zero rows read by the edge tiles)
+        for (int r = warp; r < R + 4; r += nwarps)
+            if (lane < kCholStride) P[r * kCholStride + lane] = (r < R && lane < pw) ? M[(size_t)(p0 + r) * cn + p0 + lane] : 0.0;
+        if (lane == 0)
+            for (int r = warp; r < R + 4; r += nwarps) P[r * kCholStride + 32] = 0.0;
+        __syncthreads();
+        for (int kk = 0; kk < pw; ++kk) {
+            // every thread takes the pivot itself (same value, same rounding): no broadcast step;
+            // the diagonal entry is not read again, the factor goes to piv[] for the write-back
+            const double d = P[kk * kCholStride + kk];
+            if (!(d > 0.0)) { bad = 1; break; }
+            const double l = __dsqrt_rn(d);
+            if (tid == 0) piv[kk] = l;
+            for (int r = kk + 1 + tid; r < R; r += blockDim.x)
+                P[r * kCholStride + kk] = __ddiv_rn(P[r * kCholStride + kk], l);
+            __syncthreads();
+            // term k = p0 + kk for the panel's later columns: lane = column, warps stride the rows,
+            // four rows loaded before any is stored
+            const int c2 = kk + 1 + lane;
+            if (c2 < pw) {
+                const double lc = P[c2 * kCholStride + kk];
+                int r = c2 + warp;
+                for (; r + 3 * nwarps < R; r += 4 * nwarps) {
+                    double a[4], b[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        a[u] = P[(r + u * nwarps) * kCholStride + c2];
+                        b[u] = P[(r + u * nwarps) * kCholStride + kk];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) P[(r + u * nwarps) * kCholStride + c2] = __dsub_rn(a[u], __dmul_rn(b[u], lc));
+                }
+                for (; r < R; r += nwarps)
+                    P[r * kCholStride + c2] = __dsub_rn(P[r * kCholStride + c2], __dmul_rn(P[r * kCholStride + kk], lc));
+            }
+            __syncthreads();
+        }
+        if (bad) break;
+        for (int r = warp; r < R; r += nwarps) {
+            if (lane < pw && r >= lane) {
+                const double v = r == lane ? piv[lane] : P[r * kCholStride + lane];
+                M[(size_t)(p0 + r) * cn + p0 + lane] = v;
+                Lt[(size_t)(p0 + lane) * cn + p0 + r] = v;
+            }
+        }
+        // the panel's terms for the entries (i, j), i >= j >= q0, in ascending k, 4x4 per thread
+        const int q0 = p0 + pw, R2 = cn - q0;
+        if (R2 > 0) {
+            const int nb = (R2 + 3) / 4;
+            const long long T = (long long)nb * (nb + 1) / 2;
+            for (long long tt = tid; tt < T; tt += blockDim.x) {
+                int bi = (int)((sqrt(8.0 * (double)tt + 1.0) - 1.0) * 0.5);
+                while ((long long)bi * (bi + 1) / 2 > tt) --bi;
+                while ((long long)(bi + 1) * (bi + 2) / 2 <= tt) ++bi;
+                const int bj = (int)(tt - (long long)bi * (bi + 1) / 2);
+                const int i0 = q0 + 4 * bi, j0 = q0 + 4 * bj;
+                double acc[4][4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const int i = i0 + a, j = j0 + b;
+                        acc[a][b] = (i < cn && j <= i) ? M[(size_t)i * cn + j] : 0.0;
+                    }
+                const double* pi = P + (size_t)(i0 - p0) * kCholStride;
+                const double* pj = P + (size_t)(j0 - p0) * kCholStride;
+                for (int kk = 0; kk < pw; ++kk) {
+                    double li[4], lj[4];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) {
+                        li[a] = pi[a * kCholStride + kk];
+                        lj[a] = pj[a * kCholStride + kk];
+                    }
+#pragma unroll
+                    for (int a = 0; a < 4; ++a)
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) acc[a][b] = __dsub_rn(acc[a][b], __dmul_rn(li[a], lj[b]));
+                }
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const int i = i0 + a, j = j0 + b;
+                        if (i < cn && j <= i) M[(size_t)i * cn + j] = acc[a][b];
+                    }
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) *err = bad;
+}
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Columns of the inverse from L (:1411-1429), one thread per column c, its vector in shared memory
+// (xs[i kInvCols + lane]). L y = e_c column-oriented: y_k = s_k / L_kk, then s_i -= L_ik y_k for
+// i > k, so every s_i still takes its terms in ascending k (rows i < c are +0.0 in the reference,
+// whose terms with k < c subtract products with +0.0 and change nothing). L^T x = y row-oriented
+// with ascending k, as the reference. The row of Lt each step reads is staged in shared memory by
+// the warp one step ahead (cp.async), so the per-column chains wait only on shared memory.
+__global__ void __launch_bounds__(kInvCols) k_coarse_inverse(int cn, const double* __restrict__ L,
+                                                              const double* __restrict__ Lt, double* __restrict__ inv) {
+    extern __shared__ double sm[];
+    double* xs = sm;                                   // cn x kInvCols
+    double* rows = sm + (size_t)cn * kInvCols;         // 2 x cn
+    double* dg = rows + 2 * (size_t)cn;                // cn
+    const int lane = threadIdx.x;
+    const int c0 = blockIdx.x * kInvCols;
+    const int c = c0 + lane;
+    const bool valid = c < cn;
+    for (int i = lane; i < cn; i += kInvCols) dg[i] = L[(size_t)i * cn + i];
+    for (int i = 0; i < cn; ++i) xs[i * kInvCols + lane] = (i == c) ? 1.0 : 0.0;
+    // forward: step k reads Lt[k][k+1 .. cn-1] (= L_ik, i > k)
+    auto stage_fwd = [&](int k, int buf) {
+        const double* src = Lt + (size_t)k * cn + k + 1;
+        double* dst = rows + (size_t)buf * cn;
+        for (int j = lane; j < cn - k - 1; j += kInvCols) cp_async8(dst + j, src + j);
+        cp_async_commit();
+    };
+    if (c0 < cn) stage_fwd(c0, 0);
+    for (int k = c0; k < cn; ++k) {
+        const int buf = (k - c0) & 1;
+        cp_async_wait_all();
+        __syncwarp();
+        if (k + 1 < cn) stage_fwd(k + 1, buf ^ 1);
+        if (valid && k >= c) {
+            const double y = __ddiv_rn(xs[k * kInvCols + lane], dg[k]);
+            xs[k * kInvCols + lane] = y;
+            const double* lk = rows + (size_t)buf * cn;   // lk[j] = L_ik, i = k + 1 + j
+            int i = k + 1;
+            for (; i + 8 <= cn; i += 8) {   // eight rows loaded before any is stored
+                double xv[8], lv[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    xv[u] = xs[(i + u) * kInvCols + lane];
+                    lv[u] = lk[i + u - k - 1];
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) xs[(i + u) * kInvCols + lane] = __dsub_rn(xv[u], __dmul_rn(lv[u], y));
+            }
+            for (; i < cn; ++i)
+                xs[i * kInvCols + lane] = __dsub_rn(xs[i * kInvCols + lane], __dmul_rn(lk[i - k - 1], y));
+        }
+        __syncwarp();
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    // backward: row i reads Lt[i][i+1 .. cn-1] (= L_ki, k > i)
+    stage_fwd(cn - 1, 0);
+    for (int i = cn - 1; i >= 0; --i) {
+        const int buf = (cn - 1 - i) & 1;
+        cp_async_wait_all();
+        __syncwarp();
+        if (i > 0) stage_fwd(i - 1, buf ^ 1);
+        const double* li = rows + (size_t)buf * cn;       // li[j] = L_ki, k = i + 1 + j
+        double s = xs[i * kInvCols + lane];
+        // the products do not depend on s: those of the next eight terms are formed while the
+        // chain of subtractions runs through the current eight (a +0.0 pad leaves s unchanged)
+        double cur[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int k = i + 1 + u;
+            cur[u] = k < cn ? __dmul_rn(li[k - i - 1], xs[k * kInvCols + lane]) : 0.0;
+        }
+        for (int k0 = i + 1; k0 < cn; k0 += 8) {
+            double nxt[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int k = k0 + 8 + u;
+                nxt[u] = k < cn ? __dmul_rn(li[k - i - 1], xs[k * kInvCols + lane]) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) s = __dsub_rn(s, cur[u]);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) cur[u] = nxt[u];
+        }
+        xs[i * kInvCols + lane] = __ddiv_rn(s, dg[i]);
+        __syncwarp();
+    }
+    if (valid)
+        for (int i = 0; i < cn; ++i) inv[(size_t)i * cn + c] = xs[i * kInvCols + lane];
+}
+
 __global__ void k_to_float(long long n, const double* __restrict__ a, float* __restrict__ b) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         b[i] = (float)a[i];
@@ -1416,8 +1631,19 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
     CFA_CUDA(amg->coarse_inv.ensure((size_t)cn * cn + 1));
     CFA_CUDA(err.ensure(1));
     CFA_LAUNCH(ctx, k_dense_build, ceil_div(cn, 64), 64, 0, cn, A.rp.p, A.ci.p, A.v.p, M.p);
-    CFA_LAUNCH(ctx, k_cholesky, 1, 256, 0, cn, M.p, err.p);
-    CFA_LAUNCH(ctx, k_chol_inverse, ceil_div(cn, 32), 32, 0, cn, M.p, amg->coarse_inv.p, colbuf.p);
+    if (coarse_blocked(cn)) {
+        static std::once_flag coarse_once;
+        std::call_once(coarse_once, [] {
+            cudaFuncSetAttribute(k_coarse_cholesky, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarseSmemMax);
+            cudaFuncSetAttribute(k_coarse_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarseSmemMax);
+        });
+        CFA_LAUNCH(ctx, k_coarse_cholesky, 1, kCholThreads, chol_smem(cn), cn, M.p, colbuf.p, err.p);
+        CFA_LAUNCH(ctx, k_coarse_inverse, ceil_div(cn, kInvCols), kInvCols, inv_smem(cn), cn, (const double*)M.p,
+                   (const double*)colbuf.p, amg->coarse_inv.p);
+    } else {   // coarsest levels beyond the shared-memory panels (cn > ~770): one column per step
+        CFA_LAUNCH(ctx, k_cholesky, 1, 256, 0, cn, M.p, err.p);
+        CFA_LAUNCH(ctx, k_chol_inverse, ceil_div(cn, 32), 32, 0, cn, M.p, amg->coarse_inv.p, colbuf.p);
+    }
     CFA_CHECK_LAUNCH();
     int h_err = 0;
     CFA_CUDA(cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
