@@ -120,6 +120,7 @@ k_momentum_adjoint_elems(int ne, const int* __restrict__ ev, const double* __res
                          const double* __restrict__ p_old, const double* __restrict__ nu_node, AdjParams P,
                          const double* __restrict__ xu, const double* __restrict__ xv,
                          const double* __restrict__ lu, const double* __restrict__ lv, double* __restrict__ g_elem) {
+    CFA_GRID_DEP();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= ne) return;
     const int nd[3] = {ev[3 * e], ev[3 * e + 1], ev[3 * e + 2]};
@@ -196,6 +197,7 @@ __global__ void k_momentum_adjoint_nodes(int n, const int* __restrict__ inc_ptr,
                                          double* __restrict__ g_v_old, double* __restrict__ g_u_prev,
                                          double* __restrict__ g_v_prev, double* __restrict__ g_p_old,
                                          double* __restrict__ g_nu) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -224,6 +226,7 @@ __global__ void __launch_bounds__(kThreads)
 k_momentum_adjoint_scalars(int n, int ne, const int* __restrict__ tag, const double* __restrict__ y, double H,
                            OutletBc bc, const double* __restrict__ lu, const double* __restrict__ g_elem,
                            double* __restrict__ part, unsigned int* __restrict__ counter, double* __restrict__ out) {
+    CFA_GRID_DEP();
     __shared__ double sh[2 * kWarps];
     double v[2] = {0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -248,6 +251,7 @@ __global__ void k_ppe_rhs_adjoint(int n, const int* __restrict__ ev, const doubl
                                   const int* __restrict__ inc_ptr, const int* __restrict__ inc,
                                   const double* __restrict__ lam_p, double c, double* __restrict__ g_u,
                                   double* __restrict__ g_v) {
+    CFA_GRID_DEP();
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     double su = 0.0, sv = 0.0;
@@ -281,6 +285,7 @@ __global__ void k_projection_adjoint(int n, const int* __restrict__ ev, const do
                                      const double* __restrict__ mass, double dt, double rho, double nu,
                                      const double* __restrict__ gu, const double* __restrict__ gv,
                                      const double* __restrict__ gp, double* __restrict__ g_dp) {
+    CFA_GRID_DEP();
     const int k0 = blockIdx.x * blockDim.x + threadIdx.x;
     if (k0 >= n) return;
     double s = 0.0;
@@ -321,6 +326,7 @@ k_forces_adjoint_elems(int ne, const int* __restrict__ ev, const int* __restrict
                        const double* __restrict__ u_prev, const double* __restrict__ v_prev,
                        const double* __restrict__ p, double b0, double b1, double b2, double nu, double rho, double wx,
                        double wy, double* __restrict__ g_elem) {
+    CFA_GRID_DEP();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= ne) return;
     double* g = g_elem + (size_t)e * kForceDirs;
@@ -380,6 +386,7 @@ __global__ void k_forces_adjoint_nodes(int n, const int* __restrict__ inc_ptr, c
                                        double* __restrict__ g_v, double* __restrict__ g_u_old,
                                        double* __restrict__ g_v_old, double* __restrict__ g_u_prev,
                                        double* __restrict__ g_v_prev, double* __restrict__ g_p) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -411,6 +418,7 @@ k_oss_adjoint_elems(int ne, const int* __restrict__ ev, const double* __restrict
                     const double* __restrict__ glx, const double* __restrict__ gly, const double* __restrict__ gqx,
                     const double* __restrict__ gqy, double dt, double rho, double nu, double stab,
                     double* __restrict__ g_elem) {
+    CFA_GRID_DEP();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= ne) return;
     double* g = g_elem + (size_t)e * 5;
@@ -460,6 +468,7 @@ k_oss_adjoint_elems(int ne, const int* __restrict__ ev, const double* __restrict
 __global__ void k_oss_adjoint_nodes(int n, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
                                     const double* __restrict__ g_elem, double* __restrict__ g_u,
                                     double* __restrict__ g_v, double* __restrict__ g_p) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double su = 0.0, sv = 0.0, sp = 0.0;
@@ -479,6 +488,7 @@ __global__ void k_oss_adjoint_nodes(int n, const int* __restrict__ inc_ptr, cons
 __global__ void k_oss_adjoint_inputs(int n, const int* __restrict__ tag, OutletBc bc, const double* __restrict__ lam,
                                      const double* __restrict__ p_old, const double* __restrict__ dp,
                                      double* __restrict__ l, double* __restrict__ q) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     l[i] = pressure_dirichlet(i, tag[i], bc) ? 0.0 : lam[i];

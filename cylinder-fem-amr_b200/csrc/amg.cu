@@ -32,6 +32,7 @@ namespace cfa {
 // =============================================================================================
 __global__ void k_amg_dinv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
                            double* __restrict__ dinv) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double d = 0.0;
@@ -42,6 +43,7 @@ __global__ void k_amg_dinv(int n, const int* __restrict__ rp, const int* __restr
 // power iteration pieces (spectral_radius_DinvA, :1276-1304)
 __global__ void k_pow_y(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
                         const double* __restrict__ dinv, const double* __restrict__ x, double* __restrict__ y) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s = 0.0;
@@ -58,6 +60,7 @@ constexpr int kPowThreads = 256;
 __global__ void __launch_bounds__(kPowThreads)
 k_pow_chunks(int n, int nch, const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ py,
              double* __restrict__ px) {
+    CFA_GRID_DEP();
     extern __shared__ double pow_sm[];   // [2 * kPowChunk]: y then x
     const int c = blockIdx.x;
     if (c >= nch) return;
@@ -78,6 +81,7 @@ k_pow_chunks(int n, int nch, const double* __restrict__ x, const double* __restr
 }
 
 __global__ void k_pow_finish(int nch, const double* __restrict__ py, const double* __restrict__ px, double* __restrict__ st) {
+    CFA_GRID_DEP();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double nrm = 0.0, xn = 0.0;
     for (int c = 0; c < nch; ++c) { nrm = __dadd_rn(nrm, py[c]); xn = __dadd_rn(xn, px[c]); }
@@ -87,6 +91,7 @@ __global__ void k_pow_finish(int nch, const double* __restrict__ py, const doubl
 }
 
 __global__ void k_pow_scale(int n, const double* __restrict__ y, const double* __restrict__ st, double* __restrict__ x) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x[i] = __ddiv_rn(y[i], st[0]);
 }
@@ -94,6 +99,7 @@ __global__ void k_pow_scale(int n, const double* __restrict__ y, const double* _
 // strong connections (smoothed_prolongator, :1310-1319)
 __global__ void k_strength(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
                            const double* __restrict__ dinv, double theta, unsigned char* __restrict__ strong) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double di = __ddiv_rn(1.0, dinv[i]);
@@ -107,6 +113,7 @@ __global__ void k_strength(int n, const int* __restrict__ rp, const int* __restr
 // exact-order SpGEMM (csr_multiply): upper bounds, sorted accumulation, copy
 __global__ void k_sg_ub(int rows, const int* __restrict__ arp, const int* __restrict__ aci, const int* __restrict__ brp,
                         int* __restrict__ ub) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
     int s = 0;
@@ -128,6 +135,7 @@ k_sg_accum_warp(int rows, const int* __restrict__ arp, const int* __restrict__ a
                 const int* __restrict__ brp, const int* __restrict__ bci, const double* __restrict__ bv,
                 const long long* __restrict__ off, const int* __restrict__ ub, int* __restrict__ scol,
                 double* __restrict__ sval, int* __restrict__ cnt) {
+    CFA_GRID_DEP();
     extern __shared__ __align__(16) unsigned char sg_sm[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double* pv = reinterpret_cast<double*>(sg_sm) + (size_t)w * kSgCap;
@@ -203,6 +211,7 @@ k_sg_accum_big(const int* __restrict__ big, int bc, const int* __restrict__ arp,
                const double* __restrict__ av, const int* __restrict__ brp, const int* __restrict__ bci,
                const double* __restrict__ bv, const long long* __restrict__ off, int* __restrict__ scol,
                double* __restrict__ sval, int* __restrict__ cnt) {
+    CFA_GRID_DEP();
     extern __shared__ __align__(16) unsigned char sgb_sm[];
     double* acc = reinterpret_cast<double*>(sgb_sm);                                   // [kSgDenseCols]
     double* pv = acc + kSgDenseCols;                                                   // [kSgChunk]
@@ -307,6 +316,7 @@ k_sg_accum_big(const int* __restrict__ big, int bc, const int* __restrict__ arp,
 __global__ void k_sg_copy(int rows, const long long* __restrict__ off, const int* __restrict__ scol,
                           const double* __restrict__ sval, const int* __restrict__ crp, int* __restrict__ cci,
                           double* __restrict__ cv) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
     const long long o = off[i];
@@ -319,6 +329,7 @@ __global__ void k_p_rows(int n, const int* __restrict__ aprp, const int* __restr
                          const int* __restrict__ agg, const double* __restrict__ p0v, const double* __restrict__ dinv,
                          double omega, const int* __restrict__ prp, int* __restrict__ pci, double* __restrict__ pv,
                          int* __restrict__ cnt) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const bool fill = pci != nullptr;
@@ -343,17 +354,20 @@ __global__ void k_p_rows(int n, const int* __restrict__ aprp, const int* __restr
 }
 
 __global__ void k_entry_rows(int rows, const int* __restrict__ rp, int* __restrict__ row_of) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
     for (int a = rp[i]; a < rp[i + 1]; ++a) row_of[a] = i;
 }
 
 __global__ void k_iota(int n, int* __restrict__ v) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = i;
 }
 
 __global__ void k_ptr_from_sorted(int rows, int m, const int* __restrict__ keys, int* __restrict__ ptr) {
+    CFA_GRID_DEP();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t > m) return;
     const int cur = t < m ? keys[t] : rows;
@@ -363,6 +377,7 @@ __global__ void k_ptr_from_sorted(int rows, int m, const int* __restrict__ keys,
 
 __global__ void k_transpose_fill(int m, const int* __restrict__ perm, const int* __restrict__ row_of,
                                  const double* __restrict__ v, int* __restrict__ tci, double* __restrict__ tv) {
+    CFA_GRID_DEP();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= m) return;
     const int e = perm[t];
@@ -372,6 +387,7 @@ __global__ void k_transpose_fill(int m, const int* __restrict__ perm, const int*
 
 __global__ void k_dense_build(int cn, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
                               double* __restrict__ D) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cn) return;
     for (int q = 0; q < cn; ++q) D[(size_t)i * cn + q] = 0.0;
@@ -380,6 +396,7 @@ __global__ void k_dense_build(int cn, const int* __restrict__ rp, const int* __r
 
 // Cholesky M = L L^T in place, one CTA (dense_spd_inverse, :1396-1410); err = 1 if not SPD
 __global__ void k_cholesky(int cn, double* __restrict__ M, int* __restrict__ err) {
+    CFA_GRID_DEP();
     __shared__ double ljj_s;
     __shared__ int bad;
     if (threadIdx.x == 0) bad = 0;
@@ -408,6 +425,7 @@ __global__ void k_cholesky(int cn, double* __restrict__ M, int* __restrict__ err
 
 // Column c of the inverse from L (:1411-1429)
 __global__ void k_chol_inverse(int cn, const double* __restrict__ M, double* __restrict__ inv, double* __restrict__ colbuf) {
+    CFA_GRID_DEP();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= cn) return;
     double* col = colbuf + (size_t)c * cn;
@@ -444,6 +462,7 @@ inline bool coarse_blocked(int cn) { return chol_smem(cn) <= kCoarseSmemMax && i
 
 __global__ void __launch_bounds__(kCholThreads) k_coarse_cholesky(int cn, double* __restrict__ M, double* __restrict__ Lt,
                                                                    int* __restrict__ err) {
+    CFA_GRID_DEP();
     extern __shared__ double P[];      // (cn + 4) x kCholStride
     __shared__ double piv[kCholPanel];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
@@ -558,6 +577,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // the warp one step ahead (cp.async), so the per-column chains wait only on shared memory.
 __global__ void __launch_bounds__(kInvCols) k_coarse_inverse(int cn, const double* __restrict__ L,
                                                               const double* __restrict__ Lt, double* __restrict__ inv) {
+    CFA_GRID_DEP();
     extern __shared__ double sm[];
     double* xs = sm;                                   // cn x kInvCols
     double* rows = sm + (size_t)cn * kInvCols;         // 2 x cn
@@ -640,6 +660,7 @@ __global__ void __launch_bounds__(kInvCols) k_coarse_inverse(int cn, const doubl
 }
 
 __global__ void k_to_float(long long n, const double* __restrict__ a, float* __restrict__ b) {
+    CFA_GRID_DEP();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         b[i] = (float)a[i];
 }
@@ -676,6 +697,7 @@ template <int TPR, class T, class B>
 __global__ void k_vc_pre(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
                          const T* __restrict__ dinv, T omega, const B* __restrict__ b, int jac, T* __restrict__ xo,
                          const int* __restrict__ done) {
+    CFA_GRID_DEP();
     if (done && *done) return;
     ROW_LOOP_BEGIN(TPR, n)
     if (!jac) {
@@ -702,6 +724,7 @@ template <int TPR, class T, class B, class O>
 __global__ void k_vc_jacobi(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
                             const T* __restrict__ dinv, T omega, const B* __restrict__ b, const T* __restrict__ x,
                             O* __restrict__ y, const int* __restrict__ done) {
+    CFA_GRID_DEP();
     if (done && *done) return;
     ROW_LOOP_BEGIN(TPR, n)
     const T s = group_row_sum<TPR, T, T>(rp, ci, val, x, row, valid, lane);
@@ -713,6 +736,7 @@ __global__ void k_vc_jacobi(int n, const int* __restrict__ rp, const int* __rest
 template <int TPR, class T, class B>
 __global__ void k_vc_resid(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
                            const B* __restrict__ b, const T* __restrict__ x, T* __restrict__ r, const int* __restrict__ done) {
+    CFA_GRID_DEP();
     if (done && *done) return;
     ROW_LOOP_BEGIN(TPR, n)
     const T s = group_row_sum<TPR, T, T>(rp, ci, val, x, row, valid, lane);
@@ -724,6 +748,7 @@ __global__ void k_vc_resid(int n, const int* __restrict__ rp, const int* __restr
 template <int TPR, class T, class Y>
 __global__ void k_vc_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
                           const T* __restrict__ x, int add, Y* __restrict__ y, const int* __restrict__ done) {
+    CFA_GRID_DEP();
     if (done && *done) return;
     ROW_LOOP_BEGIN(TPR, n)
     const T s = group_row_sum<TPR, T, T>(rp, ci, val, x, row, valid, lane);
@@ -735,6 +760,7 @@ __global__ void k_vc_spmv(int n, const int* __restrict__ rp, const int* __restri
 template <class B, class X>
 __global__ void k_vc_dense(int cn, const double* __restrict__ inv, const B* __restrict__ b, X* __restrict__ x,
                            const int* __restrict__ done) {
+    CFA_GRID_DEP();
     if (done && *done) return;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x & 31;
     if (i >= cn) return;
@@ -753,6 +779,7 @@ template <int TPR, int OP, class V, class T, class B, class O>
 __global__ void __launch_bounds__(kTileThreads)
 k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b, const T* __restrict__ x,
       O* __restrict__ y, const int* __restrict__ done) {
+    CFA_GRID_DEP();
     if (done && *done) return;
     extern __shared__ __align__(128) unsigned char tsmem[];
     tile_loop(tv, tsmem, [&](int, int r0, int nr, const unsigned char* ch) {
@@ -1011,6 +1038,7 @@ __device__ __forceinline__ void tail_rows(int n, const int* __restrict__ rp, con
 
 template <class V>
 __global__ void __launch_bounds__(kTailThreads, 1) k_vc_tail(TailArgs<V> a) {
+    CFA_GRID_DEP();
     if (a.done && *a.done) return;
     const int L = a.nlev, s = a.s;
     // down

@@ -58,6 +58,7 @@ k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x,
                 const double* __restrict__ p_old, const double* __restrict__ nu_node, MomParams P, int with_bc,
                 double u_max, double H, OutletBc bc, double* __restrict__ A_val, double* __restrict__ rhs_u,
                 double* __restrict__ rhs_v, double* __restrict__ mass) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int r0 = rp[i], len = rp[i + 1] - r0;
@@ -148,6 +149,7 @@ __global__ void k_momentum_bc(int n, const int* __restrict__ tag, const double* 
                               const int* __restrict__ rp, const int* __restrict__ ci, double u_max, double H,
                               OutletBc bc, int rows_too, double* __restrict__ A_val, double* __restrict__ rhs_u,
                               double* __restrict__ rhs_v, double* __restrict__ u, double* __restrict__ v) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int t = tag[i];
@@ -166,6 +168,7 @@ __global__ void k_momentum_bc(int n, const int* __restrict__ tag, const double* 
 __global__ void k_lumped_mass_rows(int n, const int* __restrict__ ev, const double* __restrict__ x,
                                    const double* __restrict__ y, const int* __restrict__ inc_ptr,
                                    const int* __restrict__ inc, double* __restrict__ m) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s = 0.0;
@@ -183,6 +186,7 @@ __global__ void k_oss_weights(int ne, const int* __restrict__ ev, const double* 
                               const double* __restrict__ y, const double* __restrict__ us,
                               const double* __restrict__ vs, double dt, double rho, double nu, double stab,
                               double* __restrict__ elem_s) {
+    CFA_GRID_DEP();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= ne) return;
     const int n0 = ev[3 * e], n1 = ev[3 * e + 1], n2 = ev[3 * e + 2];
@@ -200,6 +204,7 @@ __global__ void k_scalar_gradient_rows(int n, const int* __restrict__ ev, const 
                                        const int* __restrict__ inc, const double* __restrict__ f,
                                        const double* __restrict__ elem_s, double* __restrict__ gx_out,
                                        double* __restrict__ gy_out) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double sx = 0.0, sy = 0.0;
@@ -235,6 +240,7 @@ k_pressure_rows(int n, int nnz, const int* __restrict__ ev, const double* __rest
                 double stab, int with_bc, OutletBc bc, double* __restrict__ Kp_val, double* __restrict__ rhs_p,
                 double* __restrict__ div_num, double* __restrict__ dp, double* __restrict__ oss_val,
                 double* __restrict__ inv_m) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int r0 = rp[i], len = rp[i + 1] - r0;
@@ -322,6 +328,7 @@ __global__ void k_pressure_bc(int n, const int* __restrict__ tag, const int* __r
                               const int* __restrict__ ci, OutletBc bc, const double* __restrict__ sums,
                               const double* __restrict__ mass, double* __restrict__ Kp_val,
                               double* __restrict__ rhs, double* __restrict__ dp) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (sums) rhs[i] -= sums[0] / sums[1] * mass[i];
@@ -341,6 +348,7 @@ __global__ void k_pressure_bc(int n, const int* __restrict__ tag, const int* __r
 __global__ void __launch_bounds__(kThreads)
 k_sum2(int n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ part,
        unsigned int* __restrict__ counter, double* __restrict__ out) {
+    CFA_GRID_DEP();
     __shared__ double sh[2 * kWarps];
     double v[2] = {0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {

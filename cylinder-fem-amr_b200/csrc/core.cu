@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <cstring>
 
 #include "internal.cuh"
@@ -17,6 +18,14 @@ cfa_status set_error(cfa_ctx* ctx, cfa_status s, const char* what, const char* f
         ctx->err = buf;
     }
     return s;
+}
+
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("CFA_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
 }
 
 long long next_uid() {
@@ -41,6 +50,7 @@ cfa_status ensure_partials(cfa_ctx* ctx, size_t count) {
 // its neighbours in registers/local memory.
 // ---------------------------------------------------------------------------------------------
 __global__ void k_incidence_keys(int ne, const int* __restrict__ ev, int* __restrict__ keys, int* __restrict__ vals) {
+    CFA_GRID_DEP();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 3 * ne) return;
     keys[t] = ev[t];
@@ -48,6 +58,7 @@ __global__ void k_incidence_keys(int ne, const int* __restrict__ ev, int* __rest
 }
 
 __global__ void k_incidence_ptr(int n, int m, const int* __restrict__ sorted_keys, int* __restrict__ ptr) {
+    CFA_GRID_DEP();
     // ptr[i] = first position with key >= i (sorted keys), ptr[n] = m
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t > m) return;
@@ -81,6 +92,7 @@ __device__ __forceinline__ int collect_row(int i, const int* __restrict__ ev, co
 
 __global__ void k_csr_row_len(int n, const int* __restrict__ ev, const int* __restrict__ inc_ptr,
                               const int* __restrict__ inc, int* __restrict__ len, int* __restrict__ err) {
+    CFA_GRID_DEP();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int row[kMaxRowBuild];
@@ -92,6 +104,7 @@ __global__ void k_csr_row_len(int n, const int* __restrict__ ev, const int* __re
 
 __global__ void k_csr_row_fill(int n, const int* __restrict__ ev, const int* __restrict__ inc_ptr,
                                const int* __restrict__ inc, const int* __restrict__ rp, int* __restrict__ ci) {
+    CFA_GRID_DEP();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int row[kMaxRowBuild];
@@ -105,6 +118,7 @@ __global__ void k_csr_row_fill(int n, const int* __restrict__ ev, const int* __r
 __global__ void k_scatter_positions(int n, const int* __restrict__ ev, const int* __restrict__ inc_ptr,
                                     const int* __restrict__ inc, const int* __restrict__ rp,
                                     const int* __restrict__ ci, int* __restrict__ pos, int* __restrict__ err) {
+    CFA_GRID_DEP();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int b0 = rp[i], b1 = rp[i + 1];

@@ -22,6 +22,7 @@ constexpr int kIluMaxRow = 32;   // ILU_MAX_ROW (src/cfa/linalg.cuh:361)
 __global__ void k_ilu_factor_colour(int m, const int* __restrict__ rows, const int* __restrict__ rp,
                                     const int* __restrict__ ep, const int4* __restrict__ elim,
                                     const int2* __restrict__ upd, int t0, double* __restrict__ lu) {
+    CFA_GRID_DEP();
     const int tl = blockIdx.x * blockDim.x + threadIdx.x;
     if (tl >= m) return;
     const int t = t0 + tl;
@@ -47,6 +48,7 @@ template <class T>
 __global__ void k_ilu_gather(int nl, int nu, int n, const int* __restrict__ l_src, const int* __restrict__ u_src,
                              const int* __restrict__ d_src, const double* __restrict__ lu, T* __restrict__ lv,
                              T* __restrict__ uv, T* __restrict__ dinv) {
+    CFA_GRID_DEP();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e < nl) lv[e] = (T)lu[l_src[e]];
     if (e < nu) uv[e] = (T)lu[u_src[e]];
@@ -64,6 +66,7 @@ __global__ void k_ilu_lower(int m, int n, const int* __restrict__ rows, const in
                             const int* __restrict__ lc, const V* __restrict__ lv, const V* __restrict__ dinv,
                             int last, const double* __restrict__ r, T* __restrict__ w, double* __restrict__ z,
                             const int* __restrict__ done) {
+    CFA_GRID_DEP();
     if (done && *done) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= m) return;
@@ -107,6 +110,7 @@ template <class V, class T, int NR>
 __global__ void k_ilu_upper(int m, int n, const int* __restrict__ rows, const int* __restrict__ up,
                             const int* __restrict__ uc, const V* __restrict__ uv, const V* __restrict__ dinv,
                             T* __restrict__ w, double* __restrict__ z, const int* __restrict__ done) {
+    CFA_GRID_DEP();
     if (done && *done) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= m) return;
@@ -163,6 +167,7 @@ static void sweeps(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv, con
 // err set when the pattern is not structurally symmetric.
 __global__ void k_mirror_positions(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                                    int* __restrict__ tpos, int* __restrict__ err) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     for (int a = rp[i]; a < rp[i + 1]; ++a) {
@@ -193,6 +198,7 @@ __global__ void k_ilu_gather_transposed(int n, const int* __restrict__ rows, con
                                         const int* __restrict__ d_src, const int* __restrict__ diag,
                                         const int* __restrict__ tpos, const double* __restrict__ lu,
                                         T* __restrict__ lv, T* __restrict__ uv, T* __restrict__ dinv) {
+    CFA_GRID_DEP();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const double d = lu[d_src[t]];
@@ -203,6 +209,7 @@ __global__ void k_ilu_gather_transposed(int n, const int* __restrict__ rows, con
 
 __global__ void k_transpose_values(int nnz, const int* __restrict__ tpos, const double* __restrict__ val,
                                    double* __restrict__ out) {
+    CFA_GRID_DEP();
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a < nnz) out[a] = val[tpos[a]];
 }
@@ -234,6 +241,7 @@ __global__ void k_ilu_program(int n, const int* __restrict__ rows, const int* __
                               int* __restrict__ lc, int* __restrict__ uc, int* __restrict__ l_src,
                               int* __restrict__ u_src, int* __restrict__ d_src, int4* __restrict__ elim,
                               int2* __restrict__ upd) {
+    CFA_GRID_DEP();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const int i = rows[t];

@@ -60,6 +60,7 @@ __device__ __forceinline__ double group_reduce(double s) {
 template <int TPR, int NR>
 __global__ void k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
                        const double* __restrict__ x, double* __restrict__ y) {
+    CFA_GRID_DEP();
     ROWS_BEGIN(TPR, n)
     double s[NR];
 #pragma unroll
@@ -86,6 +87,7 @@ __global__ void k_op_b(int n, int nnz, const int* __restrict__ rp, const int* __
                        const double* __restrict__ oss, const double* __restrict__ inv_m, const double* __restrict__ z,
                        const double* __restrict__ p, const double* __restrict__ beta_ptr, double* __restrict__ p_new,
                        double* __restrict__ gx, double* __restrict__ gy, const int* __restrict__ done) {
+    CFA_GRID_DEP();
     if (done && *done) return;
     const double beta = beta_ptr ? *beta_ptr : 0.0;
     const double* Bx = oss;
@@ -127,6 +129,7 @@ k_op_k(int n, int nnz, const int* __restrict__ rp, const int* __restrict__ ci, c
        const double* __restrict__ p, const double* __restrict__ beta_ptr, double* __restrict__ pn_buf,
        const double* __restrict__ gx, const double* __restrict__ gy, double* __restrict__ q, CgState* __restrict__ st,
        double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond, const int* __restrict__ done) {
+    CFA_GRID_DEP();
     if (done && *done) return;
     __shared__ double sh[kWarps];
     const double beta = (FUSEP && beta_ptr) ? *beta_ptr : 0.0;
@@ -201,6 +204,7 @@ __device__ int ring2_row(int i, const int* __restrict__ rp, const int* __restric
 
 __global__ void k_ring2_count(int n, const int* __restrict__ rp, const int* __restrict__ ci, int* __restrict__ cnt,
                               int* __restrict__ err) {
+    CFA_GRID_DEP();
     int buf[kRing2Max];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > n) return;
@@ -212,6 +216,7 @@ __global__ void k_ring2_count(int n, const int* __restrict__ rp, const int* __re
 
 __global__ void k_ring2_fill(int n, const int* __restrict__ rp, const int* __restrict__ ci, const int* __restrict__ rp2,
                              int* __restrict__ ci2) {
+    CFA_GRID_DEP();
     int buf[kRing2Max];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -237,6 +242,7 @@ __global__ void k_ring2_slots(int n, const int* __restrict__ rp, const int* __re
                               const int* __restrict__ rp2, const int* __restrict__ ci2, int* __restrict__ slot_row,
                               int* __restrict__ kpos, int* __restrict__ cnt, const int* __restrict__ pair_ptr,
                               int* __restrict__ pa, int* __restrict__ pf) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     for (int s = rp2[i]; s < rp2[i + 1]; ++s) {
@@ -266,6 +272,7 @@ k_oss_fuse(long long nnz2, int n, int nnz, const int* __restrict__ ci, const dou
            const int* __restrict__ rp2, const int* __restrict__ slot_row, const int* __restrict__ kpos,
            const int* __restrict__ pair_ptr, const int* __restrict__ pa, const int* __restrict__ pf, TileView tv,
            unsigned char* __restrict__ data) {
+    CFA_GRID_DEP();
     const double* Bx = oss;
     const double* By = oss + nnz;
     const double* BTx = oss + 2 * (size_t)nnz;
@@ -296,6 +303,7 @@ __global__ void __launch_bounds__(kTileThreads)
 k_opt_b(TileView tv, const double* __restrict__ inv_m, const double* __restrict__ z, const double* __restrict__ p,
         const double* __restrict__ beta_ptr, double* __restrict__ p_new, double* __restrict__ gx,
         double* __restrict__ gy, const int* __restrict__ done) {
+    CFA_GRID_DEP();
     if (done && *done) return;
     extern __shared__ __align__(128) unsigned char tsmem[];
     const bool fuse = beta_ptr != nullptr;
@@ -360,6 +368,7 @@ k_opt_k(TileView tv, const int* __restrict__ tag, OutletBc bc, const double* __r
         const double* __restrict__ p, const double* __restrict__ beta_ptr, double* __restrict__ pn_buf,
         const double* __restrict__ gx, const double* __restrict__ gy, double* __restrict__ q, CgState* __restrict__ st,
         double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond, const int* __restrict__ done) {
+    CFA_GRID_DEP();
     if (done && *done) return;
     extern __shared__ __align__(128) unsigned char tsmem[];
     __shared__ double sh[kWarps];
@@ -451,6 +460,7 @@ k_opt_k(TileView tv, const int* __restrict__ tag, OutletBc bc, const double* __r
 __global__ void __launch_bounds__(kThreads)
 k_cg_bnorm(int n, const double* __restrict__ b, CgState* __restrict__ st, double* __restrict__ part,
            unsigned int* __restrict__ counter, CondArg cond) {
+    CFA_GRID_DEP();
     __shared__ double sh[kWarps];
     double v[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] += b[i] * b[i];
@@ -480,6 +490,7 @@ k_cg_bnorm(int n, const double* __restrict__ b, CgState* __restrict__ st, double
 __global__ void __launch_bounds__(kThreads)
 k_cg_resid0(int n, const double* __restrict__ b, const double* __restrict__ q, double* __restrict__ r,
             CgState* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+    CFA_GRID_DEP();
     if (st->done) return;
     __shared__ double sh[kWarps];
     double v[1] = {0.0};
@@ -503,6 +514,7 @@ k_cg_resid0(int n, const double* __restrict__ b, const double* __restrict__ q, d
 }
 
 __global__ void k_cg_nullx(int n, double* __restrict__ x, double* __restrict__ p0, const CgState* __restrict__ st) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (st->nullb) x[i] = 0.0;
@@ -512,6 +524,7 @@ __global__ void k_cg_nullx(int n, double* __restrict__ x, double* __restrict__ p
 // 1 / diag (k_extract_inv_diag, src/cfa/linalg.cuh:28-48)
 __global__ void k_inv_diag(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
                            double* __restrict__ dinv) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double d = 1.0;
@@ -525,6 +538,7 @@ __global__ void __launch_bounds__(kThreads)
 k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ pn, double* __restrict__ p,
             const double* __restrict__ q, const double* __restrict__ dinv, double* __restrict__ z,
             CgState* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+    CFA_GRID_DEP();
     if (st->done) return;
     __shared__ double sh[2 * kWarps];
     const double alpha = st->alpha;
@@ -577,6 +591,7 @@ __global__ void __launch_bounds__(kThreads)
 k_cg_rz(int n, const double* __restrict__ r, const double* __restrict__ z, const double* __restrict__ q, int first,
         int flexible, CgState* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter,
         CondArg cond) {
+    CFA_GRID_DEP();
     if (st->done) return;
     __shared__ double sh[2 * kWarps];
     double v[2] = {0.0, 0.0};
@@ -606,6 +621,7 @@ k_cg_rz(int n, const double* __restrict__ r, const double* __restrict__ z, const
 __global__ void __launch_bounds__(kThreads)
 k_cg_pq(int n, const double* __restrict__ pn, const double* __restrict__ q, CgState* __restrict__ st,
         double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+    CFA_GRID_DEP();
     if (st->done) return;
     __shared__ double sh[kWarps];
     double v[1] = {0.0};
@@ -668,6 +684,7 @@ k_b2_init(int n, const int* __restrict__ rp, const int* __restrict__ ci, const d
           const double* __restrict__ bv, double* __restrict__ r, double* __restrict__ r0, double* __restrict__ p,
           double* __restrict__ vv, B2State* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter,
           CondArg cond) {
+    CFA_GRID_DEP();
     __shared__ double sh[2 * kWarps];
     double acc[2] = {0.0, 0.0};
     ROWS_BEGIN(TPR, n)
@@ -714,6 +731,7 @@ k_b2_init(int n, const int* __restrict__ rp, const int* __restrict__ ci, const d
 // p = r + cb (p - co v) (k_bicg2_p)
 __global__ void k_b2_p(int n, const double* __restrict__ r, const double* __restrict__ v, double* __restrict__ p,
                        const B2State* __restrict__ st) {
+    CFA_GRID_DEP();
     if (st->done) return;
     const double cb0 = st->cb[0], cb1 = st->cb[1], co0 = st->co[0], co1 = st->co[1];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * n; i += gridDim.x * blockDim.x) {
@@ -728,6 +746,7 @@ __global__ void __launch_bounds__(kThreads)
 k_b2_v(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
        const double* __restrict__ phat, const double* __restrict__ r0, double* __restrict__ vv, B2State* __restrict__ st,
        double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+    CFA_GRID_DEP();
     if (st->done) return;
     __shared__ double sh[2 * kWarps];
     double acc[2] = {0.0, 0.0};
@@ -767,6 +786,7 @@ k_b2_v(int n, const int* __restrict__ rp, const int* __restrict__ ci, const doub
 // s = r - ca v (k_bicg2_s)
 __global__ void k_b2_s(int n, const double* __restrict__ r, const double* __restrict__ v, double* __restrict__ s,
                        const B2State* __restrict__ st) {
+    CFA_GRID_DEP();
     if (st->done) return;
     const double a0 = st->ca[0], a1 = st->ca[1];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * n; i += gridDim.x * blockDim.x)
@@ -779,6 +799,7 @@ __global__ void __launch_bounds__(kThreads)
 k_b2_t(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
        const double* __restrict__ shat, const double* __restrict__ s, double* __restrict__ t, B2State* __restrict__ st,
        double* __restrict__ part, unsigned int* __restrict__ counter) {
+    CFA_GRID_DEP();
     if (st->done) return;
     __shared__ double sh[6 * kWarps];
     double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -828,6 +849,7 @@ k_b2_xr(int n, double* __restrict__ xu, double* __restrict__ xv, const double* _
         const double* __restrict__ shat, const double* __restrict__ s, const double* __restrict__ t,
         double* __restrict__ r, const double* __restrict__ r0, B2State* __restrict__ st, double* __restrict__ part,
         unsigned int* __restrict__ counter, CondArg cond) {
+    CFA_GRID_DEP();
     if (st->done) return;
     __shared__ double sh[4 * kWarps];
     const double a10 = st->a1[0], a11 = st->a1[1], a20 = st->a2[0], a21 = st->a2[1], w0 = st->cw[0], w1 = st->cw[1];
@@ -878,6 +900,7 @@ k_b2t(TileView tv, int n, const double* __restrict__ xu, const double* __restric
       const double* __restrict__ bv, const double* __restrict__ in, const double* __restrict__ aux,
       double* __restrict__ out, double* __restrict__ r, double* __restrict__ r0, double* __restrict__ p,
       B2State* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+    CFA_GRID_DEP();
     if (MODE != 0 && st->done) return;
     extern __shared__ __align__(128) unsigned char tsmem[];
     constexpr int NV = MODE == 2 ? 6 : 2;
@@ -993,6 +1016,7 @@ k_b2t(TileView tv, int n, const double* __restrict__ xu, const double* __restric
 __global__ void __launch_bounds__(kThreads)
 k_dot(int n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out,
       double* __restrict__ part, unsigned int* __restrict__ counter) {
+    CFA_GRID_DEP();
     __shared__ double sh[kWarps];
     double v[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] += a[i] * b[i];
@@ -1005,16 +1029,20 @@ k_dot(int n, const double* __restrict__ a, const double* __restrict__ b, double*
 
 __global__ void k_axpby(int n, double a, const double* __restrict__ x, double b, const double* __restrict__ y,
                         double* __restrict__ out) {
+    CFA_GRID_DEP();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = a * x[i] + b * y[i];
 }
 __global__ void k_axpy(int n, double a, const double* __restrict__ x, double* __restrict__ y) {
+    CFA_GRID_DEP();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += a * x[i];
 }
 __global__ void k_vmul(int n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out) {
+    CFA_GRID_DEP();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = a[i] * b[i];
 }
 __global__ void k_bicg_p(int n, const double* __restrict__ r, const double* __restrict__ v, double beta, double omega,
                          double* __restrict__ p) {
+    CFA_GRID_DEP();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         p[i] = r[i] + beta * (p[i] - omega * v[i]);
 }
@@ -1190,6 +1218,7 @@ __device__ __forceinline__ unsigned long long fp_mix(unsigned long long z) {
 
 __global__ void k_pattern_fingerprint(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                                       unsigned long long* __restrict__ out) {
+    CFA_GRID_DEP();
     const long long total = (long long)n + 1 + rp[n];
     unsigned long long h = 0;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
@@ -2095,6 +2124,7 @@ template <int TPR>
 __global__ void k_oss_bt_sub(int n, int nnz, const int* __restrict__ rp, const int* __restrict__ ci,
                              const double* __restrict__ oss, const int* __restrict__ tag, OutletBc bc,
                              const double* __restrict__ gx, const double* __restrict__ gy, double* __restrict__ out) {
+    CFA_GRID_DEP();
     const double* BTx = oss + 2 * (size_t)nnz;
     const double* BTy = oss + 3 * (size_t)nnz;
     ROWS_BEGIN(TPR, n)

@@ -38,6 +38,7 @@ k_node_gradients(int n, const int* __restrict__ ev, const double* __restrict__ x
                  double* __restrict__ stiff, const double* __restrict__ dp, const double* __restrict__ u,
                  const double* __restrict__ v, double* __restrict__ gdx, double* __restrict__ gdy,
                  double* __restrict__ vort_num) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s = 0.0, sx = 0.0, sy = 0.0, sw = 0.0;
@@ -77,6 +78,7 @@ __global__ void k_correction(int n, const int* __restrict__ tag, OutletBc bc, do
                              const double* __restrict__ gdx, const double* __restrict__ gdy,
                              const double* __restrict__ vort_num, const double* __restrict__ dp, double* __restrict__ u,
                              double* __restrict__ v, double* __restrict__ p, double* __restrict__ vort) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double m_i = fmax(mass[i], 1.0e-14);
@@ -98,6 +100,7 @@ k_volume_forces(int ne, const int* __restrict__ ev, const int* __restrict__ tag,
                 const double* __restrict__ v_prev, const double* __restrict__ p, double b0, double b1, double b2,
                 double nu, double rho, double* __restrict__ part, unsigned int* __restrict__ counter,
                 double* __restrict__ out) {
+    CFA_GRID_DEP();
     __shared__ double sh[2 * kWarps];
     double acc[2] = {0.0, 0.0};
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
@@ -156,6 +159,7 @@ __global__ void __launch_bounds__(kThreads)
 k_recovered_gradient(int n, const int* __restrict__ ev, const double* __restrict__ x, const double* __restrict__ y,
                      const int* __restrict__ inc_ptr, const int* __restrict__ inc, const double* __restrict__ u,
                      const double* __restrict__ v, double u_max, double H, double* __restrict__ grad_rec) {
+    CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s[4] = {0.0, 0.0, 0.0, 0.0};
@@ -183,6 +187,7 @@ k_recovered_gradient(int n, const int* __restrict__ ev, const double* __restrict
 __global__ void k_amr_indicator(int ne, int n, const int* __restrict__ ev, const double* __restrict__ x,
                                 const double* __restrict__ y, const double* __restrict__ grad_rec,
                                 const double* __restrict__ mass, double* __restrict__ elem_error) {
+    CFA_GRID_DEP();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= ne) return;
     const int nd[3] = {ev[3 * e], ev[3 * e + 1], ev[3 * e + 2]};

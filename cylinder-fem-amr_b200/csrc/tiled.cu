@@ -11,6 +11,7 @@ __global__ void k_pack_tiles(int ntiles, const long long* __restrict__ off, cons
                              const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v0,
                              const double* __restrict__ v1, const double* __restrict__ v2, int nvals, int vbytes,
                              unsigned char* __restrict__ data) {
+    CFA_GRID_DEP();
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int r0 = row0[t], nr = row0[t + 1] - r0;
         const int e0 = rp[r0], ne = rp[r0 + nr] - e0;
