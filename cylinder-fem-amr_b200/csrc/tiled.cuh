@@ -160,9 +160,17 @@ __device__ __forceinline__ bool tile_loop(const TileView& tv, unsigned char* sme
             fence_proxy_async();
             tile_issue(tv, tn, smem + sn * stride, &bar[sn]);
         }
-        if (!mbar_wait(&bar[s], (phase >> s) & 1u)) {
-            atomicExch(tv.err, (int)CFA_TIMEOUT);
+        // every thread waits on the stage's mbarrier itself (the wait's acquire makes the copied
+        // bytes visible to it); a warp computes only if all its lanes saw the tile arrive, so the
+        // lane groups of the body stay whole, and the one barrier per tile (the stage's reuse)
+        // also carries a timeout to the whole CTA
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar[s], (phase >> s) & 1u));
+        if (!ok) {
+            if ((threadIdx.x & 31) == 0) atomicExch(tv.err, (int)CFA_TIMEOUT);
             abort_flag = 1;
+        } else {
+            const int r0 = t * tv.tile_rows;
+            body(t, r0, min(tv.tile_rows, tv.rows - r0), smem + s * stride);
         }
         __syncthreads();
         if (abort_flag) {
@@ -174,9 +182,6 @@ __device__ __forceinline__ bool tile_loop(const TileView& tv, unsigned char* sme
             return false;
         }
         phase ^= 1u << s;
-        const int r0 = t * tv.tile_rows;
-        body(t, r0, min(tv.tile_rows, tv.rows - r0), smem + s * stride);
-        __syncthreads();
         s = s + 1 == S ? 0 : s + 1;
     }
     return true;
