@@ -13,8 +13,10 @@ rows that are not Dirichlet (the adjoint right-hand side is zeroed on the Dirich
 multipliers no derivative uses), so the PCG with the same operator and AMG serves; the momentum system uses BiCGSTAB2 on A^T with the transposed
 multicolour ILU. The assembly and the other kernels have adjoint kernels in the library
 (cfa_momentum_adjoint, cfa_ppe_rhs_adjoint, cfa_projection_adjoint, cfa_volume_forces_adjoint).
-The forward sweep keeps the state every ``checkpoint`` steps; the backward sweep recomputes each
-segment's steps from its checkpoint and runs them in reverse.
+The forward sweep keeps the state every ``checkpoint`` steps (and the records of the last segment,
+which the backward sweep needs first); the backward sweep recomputes each earlier segment's steps
+from its checkpoint and runs them in reverse. Every backward solve starts from the solution of
+the step after it (the adjoint fields change little from step to step).
 
 ``direct=True`` solves both systems with a sparse LU on the host instead (for finite-difference
 checks that must not carry an iterative tolerance).
@@ -165,11 +167,15 @@ class DragAdjoint:
         torch = self.torch
         N, K = self.steps, self.checkpoint
         checkpoints = {}
+        last = 1 + K * ((N - 1) // K)     # first step of the last segment: taped in this sweep
+        tape = []
         state, total = self.initial_state(), 0.0
         for k in range(1, N + 1):
             if (k - 1) % K == 0:
                 checkpoints[k] = tuple(t.clone() for t in state)
-            state, _, d = self.step(k, state)
+            state, rec, d = self.step(k, state)
+            if k >= last:
+                tape.append(rec)
             total += d
         J = total / N
         z = self.z
@@ -182,13 +188,17 @@ class DragAdjoint:
         g_dp, lam_p = z(n), z(n)
         gu_o, gv_o, gu_p, gv_p, gp_o, gnu_k = (z(n) for _ in range(6))
         sc = z(2)
+        lam_u, lam_v = z(n), z(n)   # warm starts: each backward solve starts from the later step's
         for start in sorted(checkpoints, reverse=True):
             stop = min(start + K - 1, N)
-            state = tuple(t.clone() for t in checkpoints[start])
-            recs = []
-            for k in range(start, stop + 1):
-                state, rec, _ = self.step(k, state)
-                recs.append(rec)
+            if start == last:
+                recs, tape = tape, []
+            else:
+                state = tuple(t.clone() for t in checkpoints[start])
+                recs = []
+                for k in range(start, stop + 1):
+                    state, rec, _ = self.step(k, state)
+                    recs.append(rec)
             for rec in reversed(recs):
                 k = rec["k"]
                 dt_p, a0, a1, a2, c1, c2 = self.coefficients(k)
@@ -203,7 +213,6 @@ class DragAdjoint:
                 # B: pressure solve (the operator on the rows that are not Dirichlet) and its
                 # right-hand side; with OSS also the weights' and the OSS right-hand side's terms
                 self._pressure_system(k, rec["x_u"], rec["x_v"], rec["p_n"], rec["dp"].clone())
-                lam_p.zero_()
                 self._pressure_solve(g_dp * self.non_dirichlet, lam_p)
                 cfa.ppe_rhs_adjoint(self.ctx, self.dm, lam_p, dt_p, self.rho, g_us, g_vs)
                 if self.stab > 0.0:
@@ -223,7 +232,6 @@ class DragAdjoint:
                 else:
                     cfa.transpose_values(self.ctx, self.ilu, self.A, self.AT)
                     self.ilu.factor_transposed(self.A)
-                    lam_u, lam_v = z(n), z(n)
                     self.mom.solve(n, self.dm.rp, self.dm.ci, self.AT, g_us, g_vs, lam_u, lam_v, 2000, self.tol,
                                    self.ilu)
                 cfa.momentum_adjoint(self.ctx, self.dm, rec["u_n"], rec["v_n"], rec["u_nm1"], rec["v_nm1"],
