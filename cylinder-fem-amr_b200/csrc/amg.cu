@@ -775,13 +775,14 @@ __global__ void k_vc_dense(int cn, const double* __restrict__ inv, const B* __re
 // ---------------------------------------------------------------------------------------------
 enum VcOp { VC_PRE = 0, VC_JAC = 1, VC_RES = 2, VC_SPMV = 3, VC_ADD = 4 };
 
-template <int TPR, int OP, class V, class T, class B, class O>
+template <int TPR, int OP, class V, class T, class B, class O, bool RZ = false>
 __global__ void __launch_bounds__(kTileThreads)
 k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b, const T* __restrict__ x,
-      O* __restrict__ y, const int* __restrict__ done) {
+      O* __restrict__ y, const int* __restrict__ done, RzFuse rzf) {
     CFA_GRID_DEP();
     if (done && *done) return;
     extern __shared__ __align__(128) unsigned char tsmem[];
+    double dots[2] = {0.0, 0.0};   // RZ: this thread's rows of r.z and z.q
     tile_loop(tv, tsmem, [&](int, int r0, int nr, const unsigned char* ch) {
         const int* rr = reinterpret_cast<const int*>(ch);
         const int ne = rr[nr];
@@ -832,7 +833,13 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
                     const T x0 = omega * di * bi;
                     y[row] = (O)(x0 + omega * di * (bi - s));
                 } else if (OP == VC_JAC) {
-                    y[row] = (O)(xi + omega * di * (bi - s));
+                    const O out = (O)(xi + omega * di * (bi - s));
+                    y[row] = out;
+                    if constexpr (RZ) {
+                        const double zr = (double)out;
+                        dots[0] += (double)b[row] * zr;
+                        if (rzf.flexible) dots[1] += zr * rzf.q[row];
+                    }
                 } else if (OP == VC_RES) {
                     y[row] = (O)(bi - s);
                 } else if (OP == VC_SPMV) {
@@ -843,20 +850,43 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
             }
         }
     });
+    if constexpr (RZ) {
+        __shared__ double sh[2 * kWarps];
+        block_sum<2>(dots, sh);
+        if (publish_partials<2>(dots, rzf.part, rzf.counter)) {
+            reduce_partials<2>(dots, rzf.part, rzf.counter, sh);
+            if (threadIdx.x == 0) {
+                const double rz_old = *rzf.rz;
+                *rzf.beta = rzf.flexible ? -(*rzf.alpha) * dots[1] / (rz_old + 1.0e-30) : dots[0] / (rz_old + 1.0e-30);
+                *rzf.rz = dots[0];
+            }
+        }
+    }
 }
 
 // Launches (or, dry, only prepares) one tiled V-cycle operation; values of type V in the tiles.
+// rz: fold the CG's dots into this launch (the level-0 last sweep only).
 template <int OP, class V, class T, class B, class O>
 static void vct(cfa_ctx* ctx, bool dry, const TiledCsr& M, int* err, const T* dinv, T omega, const B* b, const T* x,
-                O* y, const int* done) {
+                O* y, const int* done, const RzFuse* rz = nullptr) {
+    constexpr bool kRz = OP == VC_JAC && std::is_same<O, double>::value && std::is_same<B, double>::value;
     const int tpr = M.tpr;
     const TileView tv = M.view(err);
     const TileLaunch L = tile_launch(ctx, M, nullptr);
+    const RzFuse none{};
     switch (tpr) {
 #define VCT_CASE(N)                                                                                     \
     case N:                                                                                             \
-        if (dry) allow_tile_kernel((const void*)k_vct<N, OP, V, T, B, O>);                              \
-        else CFA_LAUNCH(ctx, (k_vct<N, OP, V, T, B, O>), L.grid, kTileThreads, L.smem, tv, dinv, omega, b, x, y, done); \
+        if (dry) {                                                                                      \
+            allow_tile_kernel((const void*)k_vct<N, OP, V, T, B, O>);                                   \
+            if (kRz) allow_tile_kernel((const void*)k_vct<N, OP, V, T, B, O, kRz>);                     \
+        } else if (kRz && rz) {                                                                         \
+            CFA_LAUNCH(ctx, (k_vct<N, OP, V, T, B, O, kRz>), L.grid, kTileThreads, L.smem, tv, dinv, omega, b, x, y, \
+                       done, *rz);                                                                      \
+        } else {                                                                                        \
+            CFA_LAUNCH(ctx, (k_vct<N, OP, V, T, B, O>), L.grid, kTileThreads, L.smem, tv, dinv, omega, b, x, y, done, \
+                       none);                                                                           \
+        }                                                                                               \
         break;
         VCT_CASE(1) VCT_CASE(2) VCT_CASE(4) VCT_CASE(8) VCT_CASE(16)
         default:
@@ -1209,7 +1239,8 @@ struct TVec<float> {
 // right-hand side of the level in B (level 0: the caller's FP64 r) (dry: prepare the kernels
 // only, no launches)
 template <class V, class T, class B>
-static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* z, const int* done, bool dry) {
+static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* z, const int* done, bool dry,
+                         const RzFuse* rz = nullptr) {
     AmgLevel& L = amg->levels[l];
     const int s = amg->opts.smooth_steps;
     int* err = amg->err.p;
@@ -1250,7 +1281,7 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     vct<VC_ADD, V, T, T, T>(ctx, dry, L.tP, err, dinv, omega, (const T*)nullptr, cx, x, done);
     for (int k = 0; k < s; ++k) {
         if (l == 0 && k == s - 1) {
-            vct<VC_JAC, V, T, B, double>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, z, done);
+            vct<VC_JAC, V, T, B, double>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, z, done, rz);
         } else {
             vct<VC_JAC, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, t, done);
             std::swap(x, t);
@@ -1267,10 +1298,11 @@ static bool vcycle_fp32(const cfa_amg* amg) {
     return !(e && e[0] == '1');
 }
 
-static void vcycle_tiled_top(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, bool dry) {
-    if (amg->opts.precision != CFA_MIXED) vcycle_tiled<double, double, double>(ctx, amg, 0, r, z, done, dry);
-    else if (vcycle_fp32(amg)) vcycle_tiled<float, float, double>(ctx, amg, 0, r, z, done, dry);
-    else vcycle_tiled<float, double, double>(ctx, amg, 0, r, z, done, dry);
+static void vcycle_tiled_top(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, bool dry,
+                             const RzFuse* rz = nullptr) {
+    if (amg->opts.precision != CFA_MIXED) vcycle_tiled<double, double, double>(ctx, amg, 0, r, z, done, dry, rz);
+    else if (vcycle_fp32(amg)) vcycle_tiled<float, float, double>(ctx, amg, 0, r, z, done, dry, rz);
+    else vcycle_tiled<float, double, double>(ctx, amg, 0, r, z, done, dry, rz);
 }
 
 cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done) {
@@ -1285,6 +1317,16 @@ cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, co
         vcycle_level<double, double>(ctx, amg, 0, r, z, done);
     }
     CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+cfa_status amg_vcycle_rz(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, const RzFuse& f,
+                         bool* fused) {
+    *fused = false;
+    if (amg->levels.empty() || !amg->tiled || amg->opts.smooth_steps < 1) return amg_vcycle(ctx, amg, r, z, done);
+    vcycle_tiled_top(ctx, amg, r, z, done, false, &f);
+    CFA_CHECK_LAUNCH();
+    *fused = true;
     return CFA_OK;
 }
 

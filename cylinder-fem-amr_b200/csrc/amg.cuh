@@ -101,4 +101,21 @@ namespace cfa {
 // One symmetric V-cycle z = M^-1 r (FP64 in/out). Kernels return at once while *done != 0
 // (done nullable).
 cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done);
+
+// The CG's dots after the preconditioner (r.z, and z.q for the flexible beta) folded into the
+// V-cycle's last sweep, which already reads r and writes z; its last block finishes them as the
+// CG's own kernel would: beta = flexible ? -alpha (z.q) / rz_old : (r.z) / rz_old, rz = r.z.
+struct RzFuse {
+    const double* q;
+    int flexible;
+    double* rz;
+    double* beta;
+    const double* alpha;
+    double* part;
+    unsigned int* counter;
+};
+// amg_vcycle with the dots fused when the hierarchy runs tile-streamed (*fused = true); otherwise
+// the plain V-cycle (*fused = false) and the caller computes the dots.
+cfa_status amg_vcycle_rz(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, const RzFuse& f,
+                         bool* fused);
 }  // namespace cfa

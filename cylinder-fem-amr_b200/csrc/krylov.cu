@@ -1401,10 +1401,14 @@ static cfa_status pcg_piece(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, int piec
             CFA_LAUNCH(ctx, k_cg_update<false>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p,
                        (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond);
             if (!a.prec) {
-                CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done));
+                // z = M^-1 r with r.z (and z.q) folded into the V-cycle's last sweep where it can be
                 const int flexible = a.amg->opts.precision == CFA_MIXED ? 1 : 0;
-                CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, flexible, st,
-                           W.part.p, W.counter.p, cond);
+                const RzFuse f{W.q.p, flexible, &st->rz, &st->beta, &st->alpha, W.part.p, W.counter.p};
+                bool fused = false;
+                CFA_PROPAGATE(amg_vcycle_rz(ctx, a.amg, W.r.p, W.z.p, done, f, &fused));
+                if (!fused)
+                    CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, flexible, st,
+                               W.part.p, W.counter.p, cond);
             }
         } else {
             CFA_LAUNCH(ctx, k_cg_update<true>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p, W.dinv.p, W.z.p,
