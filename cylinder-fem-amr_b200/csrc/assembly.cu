@@ -74,6 +74,10 @@ k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x,
         }
     }
     double f_u_row = 0.0, f_v_row = 0.0, m_row = 0.0;
+    // reciprocals of the constant and per-launch divisors, taken once (the products differ from
+    // the quotients in the last bit at most; the element formula is division-bound in FP64)
+    constexpr double kThird = 1.0 / 3.0, kSixth = 1.0 / 6.0, kTwelfth = 1.0 / 12.0;
+    const double inv_rho = 1.0 / P.rho, term_t_p = 2.0 / P.tau_time;
     for (int s = inc_ptr[i]; s < inc_ptr[i + 1]; ++s) {
         const int e = inc[s] >> 2, a = inc[s] & 3;
         int nd[3];
@@ -81,7 +85,8 @@ k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x,
         const Geom g = elem_geom(nd, x, y);
         if (!g.ok) continue;
         const double area = g.area;
-        m_row += area / 3.0;
+        const double area3 = area * kThird;
+        m_row += area3;
         if (dir) continue;
         double u_h[3], v_h[3], w_u = 0.0, w_v = 0.0, div_w = 0.0;
 #pragma unroll
@@ -90,39 +95,39 @@ k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x,
             u_h[k] = P.a1 * un + P.a2 * um;
             v_h[k] = P.a1 * vn + P.a2 * vm;
             const double wu = P.c1 * un + P.c2 * um, wv = P.c1 * vn + P.c2 * vm;
-            w_u += wu / 3.0;
-            w_v += wv / 3.0;
+            w_u += wu * kThird;
+            w_v += wv * kThird;
             div_w += wu * g.dNdx[k] + wv * g.dNdy[k];
         }
         const double vel_mag = sqrt(w_u * w_u + w_v * w_v) + 1.0e-12;
         const double h_K = sqrt(2.0 * area);
         // element viscosity: the scalar nu, or the mean of a nodal field
-        const double nu = nu_node ? (nu_node[nd[0]] + nu_node[nd[1]] + nu_node[nd[2]]) / 3.0 : P.nu;
-        const double term_t = 2.0 / P.tau_time;
+        const double nu = nu_node ? (nu_node[nd[0]] + nu_node[nd[1]] + nu_node[nd[2]]) * kThird : P.nu;
+        const double term_t = term_t_p;
         const double term_c = 2.0 * vel_mag / h_K;
         const double term_d = 4.0 * nu / (h_K * h_K);
         const double tau_supg = 1.0 / sqrt(term_t * term_t + term_c * term_c + 9.0 * term_d * term_d);
         const double p0 = p_old[nd[0]], p1 = p_old[nd[1]], p2 = p_old[nd[2]];
-        const double dpdx = (p0 * g.dNdx[0] + p1 * g.dNdx[1] + p2 * g.dNdx[2]) / P.rho;
-        const double dpdy = (p0 * g.dNdy[0] + p1 * g.dNdy[1] + p2 * g.dNdy[2]) / P.rho;
+        const double dpdx = (p0 * g.dNdx[0] + p1 * g.dNdx[1] + p2 * g.dNdx[2]) * inv_rho;
+        const double dpdy = (p0 * g.dNdy[0] + p1 * g.dNdy[1] + p2 * g.dNdy[2]) * inv_rho;
         double ugN[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) ugN[k] = w_u * g.dNdx[k] + w_v * g.dNdy[k];
         double f_u = 0.0, f_v = 0.0;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            const double M_ij = (a == j) ? (area / 6.0) : (area / 12.0);
+            const double M_ij = (a == j) ? (area * kSixth) : (area * kTwelfth);
             const double K_ij = area * (g.dNdx[a] * g.dNdx[j] + g.dNdy[a] * g.dNdy[j]);
-            const double C_ij = (area / 3.0) * ugN[j] + P.skew_coef * div_w * M_ij;
+            const double C_ij = area3 * ugN[j] + P.skew_coef * div_w * M_ij;
             const double S_ij = area * tau_supg * ugN[a] * ugN[j];
-            const double Ms_ij = (area / 3.0) * tau_supg * ugN[a];
+            const double Ms_ij = area3 * tau_supg * ugN[a];
             const double A_ij = P.a0 * (M_ij + Ms_ij) + nu * K_ij + C_ij + S_ij;
             const int p = pos[3 * s + j];
             if (local) acc[p - r0] += A_ij; else A_val[p] += A_ij;
             f_u += (M_ij + Ms_ij) * u_h[j];
             f_v += (M_ij + Ms_ij) * v_h[j];
         }
-        const double tw = (area / 3.0) + area * tau_supg * ugN[a];
+        const double tw = area3 + area * tau_supg * ugN[a];
         f_u -= tw * dpdx;
         f_v -= tw * dpdy;
         f_u_row += f_u;
