@@ -4,6 +4,8 @@
 // atomicAdd into a binary-searched CSR slot (src/cfa/fem_kernels.cuh:40-282, :697-909), there
 // are no atomics and no searches, the result is deterministic, and each CSR value is written
 // exactly once (coalesced along the row).
+#include <mutex>
+
 #include "internal.cuh"
 #include "mesh.cuh"
 
@@ -235,7 +237,15 @@ __global__ void k_scalar_gradient_rows(int n, const int* __restrict__ ev, const 
 // Pressure rows: k_assemble_pressure_poisson (fem_kernels.cuh:201-282) gathered per row; with
 // oss_val the rows of B and B^T of k_assemble_oss_operator (:807-847) and inv_m (:849-852) in
 // the same pass; with with_bc the Dirichlet rows/columns of k_apply_bc_pressure (:460-490).
-__global__ void __launch_bounds__(kThreads)
+// A row of up to kPressCap entries accumulates K, Bx, By, B^T x, B^T y in shared memory laid out
+// [array][slot][thread], so that threads adding to different slots of their rows hit different
+// banks; longer rows accumulate in place in global memory. Every entry takes its terms in the
+// element order of the incidence either way.
+constexpr int kPressThreads = 128;
+constexpr int kPressCap = 16;
+constexpr size_t kPressSmem = (size_t)5 * kPressCap * kPressThreads * sizeof(double);
+
+__global__ void __launch_bounds__(kPressThreads)
 k_pressure_rows(int n, int nnz, const int* __restrict__ ev, const double* __restrict__ x,
                 const double* __restrict__ y, const int* __restrict__ tag, const int* __restrict__ inc_ptr,
                 const int* __restrict__ inc, const int* __restrict__ pos, const int* __restrict__ rp,
@@ -249,18 +259,26 @@ k_pressure_rows(int n, int nnz, const int* __restrict__ ev, const double* __rest
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int r0 = rp[i], len = rp[i + 1] - r0;
-    const bool local = len <= kRowCap;
+    const bool local = len <= kPressCap;
     const bool want_oss = oss_val != nullptr;
-    double accK[kRowCap];
+    extern __shared__ double press_sm[];   // [5][kPressCap][blockDim.x]
+    const int T = blockDim.x, tt = threadIdx.x;
+    double* sK = press_sm + tt;                          // sK[q * T]: K entry q of this row
+    double* sBx = press_sm + 1 * kPressCap * T + tt;
+    double* sBy = press_sm + 2 * kPressCap * T + tt;
+    double* sTx = press_sm + 3 * kPressCap * T + tt;
+    double* sTy = press_sm + 4 * kPressCap * T + tt;
+    double *Bx = oss_val, *By = oss_val + (size_t)nnz, *BTx = oss_val + 2 * (size_t)nnz, *BTy = oss_val + 3 * (size_t)nnz;
     if (local) {
-#pragma unroll
-        for (int q = 0; q < kRowCap; ++q) accK[q] = 0.0;
+        for (int q = 0; q < len; ++q) {
+            sK[q * T] = 0.0;
+            if (want_oss) { sBx[q * T] = 0.0; sBy[q * T] = 0.0; sTx[q * T] = 0.0; sTy[q * T] = 0.0; }
+        }
     } else {
         for (int q = 0; q < len; ++q) Kp_val[r0 + q] = 0.0;
+        if (want_oss)
+            for (int q = 0; q < len; ++q) { Bx[r0 + q] = 0.0; By[r0 + q] = 0.0; BTx[r0 + q] = 0.0; BTy[r0 + q] = 0.0; }
     }
-    double *Bx = oss_val, *By = oss_val + (size_t)nnz, *BTx = oss_val + 2 * (size_t)nnz, *BTy = oss_val + 3 * (size_t)nnz;
-    if (want_oss)
-        for (int q = 0; q < len; ++q) { Bx[r0 + q] = 0.0; By[r0 + q] = 0.0; BTx[r0 + q] = 0.0; BTy[r0 + q] = 0.0; }
     double rhs_row = 0.0, div_row = 0.0;
     for (int k = inc_ptr[i]; k < inc_ptr[i + 1]; ++k) {
         const int e = inc[k] >> 2, a = inc[k] & 3;
@@ -291,7 +309,7 @@ k_pressure_rows(int n, int nnz, const int* __restrict__ ev, const double* __rest
         for (int j = 0; j < 3; ++j) {
             const double K_ij = area * (g.dNdx[a] * g.dNdx[j] + g.dNdy[a] * g.dNdy[j]);
             const int p = pos[3 * k + j];
-            if (local) accK[p - r0] += (1.0 + s) * K_ij; else Kp_val[p] += (1.0 + s) * K_ij;
+            if (local) sK[(p - r0) * T] += (1.0 + s) * K_ij; else Kp_val[p] += (1.0 + s) * K_ij;
         }
         const double stab_i = s * area * (g.dNdx[a] * gx + g.dNdy[a] * gy) - area * (g.dNdx[a] * sx + g.dNdy[a] * sy);
         rhs_row += rhs_contrib - stab_i;
@@ -301,14 +319,32 @@ k_pressure_rows(int n, int nnz, const int* __restrict__ ev, const double* __rest
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
                 const int p = pos[3 * k + j];
-                Bx[p] += w * g.dNdx[j];    // B_ij  = sum_K w_K grad N_j|K   (row i, column j)
-                By[p] += w * g.dNdy[j];
-                BTx[p] += w * g.dNdx[a];   // B^T_ij = B_ji = sum_K w_K grad N_i|K
-                BTy[p] += w * g.dNdy[a];
+                // B_ij = sum_K w_K grad N_j|K (row i, column j); B^T_ij = B_ji = sum_K w_K grad N_i|K
+                if (local) {
+                    const int q = (p - r0) * T;
+                    sBx[q] += w * g.dNdx[j];
+                    sBy[q] += w * g.dNdy[j];
+                    sTx[q] += w * g.dNdx[a];
+                    sTy[q] += w * g.dNdy[a];
+                } else {
+                    Bx[p] += w * g.dNdx[j];
+                    By[p] += w * g.dNdy[j];
+                    BTx[p] += w * g.dNdx[a];
+                    BTy[p] += w * g.dNdy[a];
+                }
             }
         }
     }
-    if (want_oss) inv_m[i] = 1.0 / fmax(mass[i], 1.0e-14);
+    if (want_oss) {
+        inv_m[i] = 1.0 / fmax(mass[i], 1.0e-14);
+        if (local)
+            for (int q = 0; q < len; ++q) {
+                Bx[r0 + q] = sBx[q * T];
+                By[r0 + q] = sBy[q * T];
+                BTx[r0 + q] = sTx[q * T];
+                BTy[r0 + q] = sTy[q * T];
+            }
+    }
     div_num[i] = div_row;
     if (with_bc && pressure_dirichlet(i, tag[i], bc)) {
         for (int q = 0; q < len; ++q) Kp_val[r0 + q] = (ci[r0 + q] == i) ? 1.0 : 0.0;
@@ -317,7 +353,7 @@ k_pressure_rows(int n, int nnz, const int* __restrict__ ev, const double* __rest
         return;
     }
     for (int q = 0; q < len; ++q) {
-        double v = local ? accK[q] : Kp_val[r0 + q];
+        double v = local ? sK[q * T] : Kp_val[r0 + q];
         if (with_bc) {
             const int c = ci[r0 + q];
             if (c != i && pressure_dirichlet(c, tag[c], bc)) v = 0.0;
@@ -461,7 +497,12 @@ static cfa_status assemble_pressure(cfa_ctx* ctx, const cfa_mesh* m, const doubl
     // With the pinned outlet the RHS loses its mean before the BC rows (apply_bc_pressure,
     // fem_kernels.cuh:519-531): assemble without BC, then sums, then the BC kernel.
     const bool split = apply_bc && m->bc.outlet_dirichlet;
-    CFA_LAUNCH(ctx, k_pressure_rows, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->nnz, m->ev, m->x, m->y, m->tag,
+    static std::once_flag press_once;
+    std::call_once(press_once, [] {
+        cudaFuncSetAttribute(k_pressure_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPressSmem);
+    });
+    CFA_LAUNCH(ctx, k_pressure_rows, ceil_div(m->n, kPressThreads), kPressThreads, kPressSmem, m->n, m->nnz, m->ev,
+               m->x, m->y, m->tag,
                m->inc_ptr.p, m->inc.p, m->pos.p, m->rp, m->ci, us, vs, p_old, gpx, gpy, mass, elem_s, dt, rho,
                stab, (apply_bc && !split) ? 1 : 0, m->bc, Kp, rhs, div, dp, oss_val, inv_m);
     if (split) {
