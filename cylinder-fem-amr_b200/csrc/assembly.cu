@@ -11,8 +11,6 @@
 
 namespace cfa {
 
-constexpr int kRowCap = 32;   // rows up to this length accumulate in registers/local memory
-
 struct Geom {
     double area, dNdx[3], dNdy[3];
     bool ok;
@@ -50,7 +48,12 @@ __device__ __forceinline__ double momentum_bc_u(int tag, double yi, double u_max
 }
 
 // Momentum rows: k_assemble_momentum_fem (fem_kernels.cuh:40-181) gathered per row, lumped mass,
-// and (with_bc) the Dirichlet rows of k_apply_bc_momentum (:411-453) on A and the RHS.
+// and (with_bc) the Dirichlet rows of k_apply_bc_momentum (:411-453) on A and the RHS. A row of
+// up to kMomCap entries accumulates in shared memory laid out [slot][thread] (conflict-free for
+// any slot a thread adds to); longer rows in place in global memory. Same addition order.
+constexpr int kMomCap = 16;
+constexpr size_t kMomSmem = (size_t)kMomCap * kThreads * sizeof(double);
+
 __global__ void __launch_bounds__(kThreads)
 k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x, const double* __restrict__ y,
                 const int* __restrict__ tag, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
@@ -65,12 +68,13 @@ k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x,
     if (i >= n) return;
     const int r0 = rp[i], len = rp[i + 1] - r0;
     const bool dir = with_bc && momentum_dirichlet(tag[i], bc);
-    const bool local = len <= kRowCap;
-    double acc[kRowCap];
+    const bool local = len <= kMomCap;
+    extern __shared__ double mom_sm[];   // [kMomCap][blockDim.x]
+    const int T = blockDim.x;
+    double* acc = mom_sm + threadIdx.x;  // acc[q * T]: entry q of this row
     if (!dir) {
         if (local) {
-#pragma unroll
-            for (int q = 0; q < kRowCap; ++q) acc[q] = 0.0;
+            for (int q = 0; q < len; ++q) acc[q * T] = 0.0;
         } else {
             for (int q = 0; q < len; ++q) A_val[r0 + q] = 0.0;
         }
@@ -125,7 +129,7 @@ k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x,
             const double Ms_ij = area3 * tau_supg * ugN[a];
             const double A_ij = P.a0 * (M_ij + Ms_ij) + nu * K_ij + C_ij + S_ij;
             const int p = pos[3 * s + j];
-            if (local) acc[p - r0] += A_ij; else A_val[p] += A_ij;
+            if (local) acc[(p - r0) * T] += A_ij; else A_val[p] += A_ij;
             f_u += (M_ij + Ms_ij) * u_h[j];
             f_v += (M_ij + Ms_ij) * v_h[j];
         }
@@ -145,7 +149,7 @@ k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x,
         return;
     }
     if (local)
-        for (int q = 0; q < len; ++q) A_val[r0 + q] = acc[q];
+        for (int q = 0; q < len; ++q) A_val[r0 + q] = acc[q * T];
     rhs_u[i] = f_u_row;
     rhs_v[i] = f_v_row;
 }
@@ -440,7 +444,7 @@ cfa_status cfa_assemble_momentum_nu(cfa_ctx* ctx, const cfa_mesh* m, const doubl
     CFA_ARG(!bcp || (u && v));
     MomParams P{prm->dt, prm->nu, prm->rho, prm->a0, prm->a1, prm->a2, prm->c1, prm->c2, prm->tau_time, prm->skew_coef};
     const double u_max = bcp ? bcp->u_max : 0.0, H = bcp ? bcp->H : 1.0;
-    CFA_LAUNCH(ctx, k_momentum_rows, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y, m->tag,
+    CFA_LAUNCH(ctx, k_momentum_rows, ceil_div(m->n, kThreads), kThreads, kMomSmem, m->n, m->ev, m->x, m->y, m->tag,
                m->inc_ptr.p, m->inc.p, m->pos.p, m->rp, m->ci, u_old, v_old, u_prev, v_prev, p_old, nu_node, P,
                bcp ? 1 : 0, u_max, H, m->bc, A_val, rhs_u, rhs_v, mass);
     if (bcp)   // solution values on Dirichlet nodes after the rows (u may alias u_old)
