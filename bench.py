@@ -128,6 +128,12 @@ def workload_inputs(name):
     return m, u, v, p
 
 
+def workload_name(name, n, nnz):
+    """The workload string both arms print (the same mesh, the same step)."""
+    kind = "uniform" if name == "c0" else "adaptive"
+    return f"{name}: {kind} NVB mesh n={n}, nnz={nnz}, BDF2 step, OSS 0.3, tol 1e-10"
+
+
 def l2_flush(buf):
     buf.add_(1.0)
 
@@ -315,22 +321,25 @@ def run_reference(args):
         torch.cuda.synchronize()
         total += R.ref_step_run(h, O._p(its), O._p(conv), O._p(rel), None, None, None)
     clk.stop()
+    nnz = R.ref_step_nnz(h)
     R.ref_step_free(h)
     step_ms = total / args.steps
     value = step_ms + setup_ms / AMG_REBUILD
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    threads = int(R.ref_omp_threads())
     return {
         "metric": METRIC, "value": round(value, 4), "unit": "ms/step", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 4),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.workload}: adaptive NVB mesh n={m.n}, BDF2 step, OSS 0.3, tol 1e-10",
+        "config": {"workload": workload_name(args.workload, m.n, nnz),
                    "precision": "fp64 (the reference has no mixed mode)", "l2": "flushed between steps",
                    "amg_setup_ms": round(setup_ms, 3), "amg_rebuild": AMG_REBUILD,
+                   "step_ms_without_setup": round(step_ms, 4), "omp_threads": threads,
                    "iterations": {"u": int(its[0]), "v": int(its[1]), "p": int(its[2])},
                    "converged": [bool(c) for c in conv]},
         "cpu_baseline": {"value": round(value, 4), "unit": "ms/step", "cores": threads, "kind": "reference",
                          "sample": "the reference's own CUDA build (nvcc sm_100a, host-timed steps with its "
-                                   "device syncs) on the same workload; OpenMP host setup threads"},
+                                   "device syncs) on the same workload; AMG setup on the host with the "
+                                   "reference application's OpenMP thread rule (half the logical CPUs, at most 8)"},
         "e2e": {"value": round(value, 4), "unit": "ms/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "clocks": clk.summary(),
     }
@@ -662,7 +671,7 @@ def main():
         "metric": METRIC, "value": round(value, 4), "unit": "ms/step", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(value, 4), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 outer / f32 preconditioners", "data": "synthetic",
-        "config": {"workload": f"{args.workload}: adaptive NVB mesh n={n}, nnz={nnz}, BDF2 step, OSS 0.3, tol 1e-10",
+        "config": {"workload": workload_name(args.workload, n, nnz),
                    "parallelism": "replicas" if world > 1 else "single GPU", "l2": "flushed between steps (256 MB write)",
                    "fp64_ms_per_step": round(value64, 4), "mixed_speedup_vs_fp64": round(value64 / value, 3),
                    "amg_setup_ms": {"mixed": round(mixed["setup_ms"], 3), "fp64": round(fp64["setup_ms"], 3)},

@@ -2143,8 +2143,22 @@ __global__ void k_oss_bt_sub(int n, int nnz, const int* __restrict__ rp, const i
     ROWS_END
 }
 
-// Device address of g_oss_static on each device, looked up once per device (with that device
-// current) on the first call there.
+// Makes a device current for the lifetime of the object and restores the caller's device after.
+struct CurrentDevice {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit CurrentDevice(int device) {
+        err = cudaGetDevice(&prev);
+        if (err == cudaSuccess && prev != device) err = cudaSetDevice(device);
+        else prev = -1;
+    }
+    ~CurrentDevice() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// Device address of g_oss_static on the current device (the context's), looked up on the first
+// call there and kept for the life of the process.
 static cfa_status oss_static_scratch(cfa_ctx* ctx, double** out) {
     constexpr int kMaxDevices = 64;
     static std::mutex mu;
@@ -2153,12 +2167,8 @@ static cfa_status oss_static_scratch(cfa_ctx* ctx, double** out) {
         return set_error(ctx, CFA_BAD_ARG, "device ordinal out of range", __FILE__, __LINE__);
     std::lock_guard<std::mutex> lock(mu);
     if (!addr[ctx->device]) {
-        int cur = 0;
-        CFA_CUDA(cudaGetDevice(&cur));
-        if (cur != ctx->device) CFA_CUDA(cudaSetDevice(ctx->device));
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_oss_static);
-        if (cur != ctx->device) CFA_CUDA(cudaSetDevice(cur));
         if (e != cudaSuccess) return set_error(ctx, CFA_CUDA_ERROR, cudaGetErrorString(e), __FILE__, __LINE__);
         addr[ctx->device] = static_cast<double*>(p);
     }
@@ -2179,6 +2189,11 @@ cfa_status cfa_oss_apply_noalloc(cfa_ctx* ctx, const cfa_mesh* m, const double* 
         return set_error(ctx, CFA_BAD_ARG,
                          "cfa_oss_apply_noalloc: the mesh has more nodes than its static scratch holds (524288)",
                          __FILE__, __LINE__);
+    // the scratch address and the launches belong to the context's device, whichever device the
+    // caller has current
+    CurrentDevice on_device(ctx->device);
+    if (on_device.err != cudaSuccess)
+        return set_error(ctx, CFA_CUDA_ERROR, cudaGetErrorString(on_device.err), __FILE__, __LINE__);
     double* g = nullptr;
     CFA_PROPAGATE(oss_static_scratch(ctx, &g));
     double* gx = g;

@@ -225,8 +225,10 @@ cfa_status cfa_oss_apply(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_oss
  * g = M^-1 B d_in in a fixed static device array instead, and it does not synchronise.
  * Limit: mesh->n <= 524288 nodes (the array is 8 MiB); larger meshes get CFA_BAD_ARG.
  * Nothing needs to start at zero: every call writes each scratch entry it reads.
- * Setup: the first call on each device looks up the array's address (with that device made
- * current for the lookup) and must come before any stream capture on that device.
+ * Setup: the call makes the context's device current for its duration (and restores the
+ * caller's device). The first call on each device looks up the array's address and must come
+ * before any stream capture on that device; the address is kept for the life of the process,
+ * so the entry point must not be called on a device after cudaDeviceReset there.
  * There is one array per device and process: calls in flight at the same time on one device (two
  * streams, contexts or threads) race on it. Order such calls, e.g. on one stream or with events.
  * Result: the same d_out as cfa_oss_apply (same per-row summation order). Asynchronous on the

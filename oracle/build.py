@@ -29,7 +29,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE_SRC = "/root/reference/src"
+# The reference project's src/ tree; CFA_REFERENCE_SRC overrides the default location.
+REFERENCE_SRC = os.environ.get("CFA_REFERENCE_SRC", os.path.join(os.sep, "root", "reference", "src"))
 ORACLE_LIB = os.path.join(HERE, "_build", "libcfa_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libcfa_ref.so")
 REF_DRIVER = os.path.join(HERE, "_ref", "cfa_ref_driver")
@@ -95,10 +96,77 @@ def _driver_cmd(src: str, out: str, extra: list[str]) -> list[str]:
             "-Xcompiler", "-fopenmp", *extra, src, "-o", out, "-lgomp"]
 
 
+# The application's solver tolerances (CG and BiCGSTAB stop at |r| < 1e-7 |b|, the re-projection
+# CG at 1e-8) written as literals at the call sites. The *_tight builds replace them by 1e-10 in
+# both the stock program and the drop-in, so that two builds whose solvers differ only in rounding
+# can be compared where the stopping tolerance no longer sets the size of the difference.
+TIGHT_SITES = {
+    "cylinder_fem_amr.cu": [
+        ("gpu_buf.d_u, gpu_buf.d_v, 150, 1.0e-7, mom_ilu);", "gpu_buf.d_u, gpu_buf.d_v, 150, 1.0e-10, mom_ilu);"),
+        ("gpu_buf.d_Kp_val, gpu_buf.d_rhs_p, gpu_buf.d_dp, 4000, 1.0e-7,",
+         "gpu_buf.d_Kp_val, gpu_buf.d_rhs_p, gpu_buf.d_dp, 4000, 1.0e-10,"),
+    ],
+    "device.cuh": [
+        ("g.d_Kp_val, g.d_rhs_p, g.d_dp, 4000, 1.0e-8,\n                                  oss ?",
+         "g.d_Kp_val, g.d_rhs_p, g.d_dp, 4000, 1.0e-10,\n                                  oss ?"),
+        ("g.d_Kp_val, g.d_rhs_p, g.d_dp, 4000, 1.0e-8,\n                                 nullptr,",
+         "g.d_Kp_val, g.d_rhs_p, g.d_dp, 4000, 1.0e-10,\n                                 nullptr,"),
+    ],
+}
+REF_TIGHT_DRIVER = os.path.join(HERE, "_ref", "cfa_ref_driver_tight")
+DROPIN_TIGHT_DRIVER = os.path.join(HERE, "_ref", "cfa_dropin_driver_tight")
+
+
+def _substitute(text: str, sites: list[tuple[str, str]]) -> str:
+    for anchor, repl in sites:
+        if text.count(anchor) != 1:
+            raise RuntimeError(f"call site not found exactly once: {anchor}")
+        text = text.replace(anchor, repl)
+    return text
+
+
+def _build_mirrored(out: str, shim: bool, swap: bool, tight: bool) -> None:
+    """Builds the application from a temporary mirror of the reference's src/: links to the
+    original files, except cfa/linalg.cuh -> the shim (shim=True) and the files edited at the
+    call sites of SWAP_SITES (swap=True) or TIGHT_SITES (tight=True), which are written as
+    copies. The mirror is removed afterwards."""
+    main = os.path.join(REFERENCE_SRC, "cylinder_fem_amr.cu")
+    cfa_dir = os.path.join(REFERENCE_SRC, "cfa")
+    mirror = os.path.join(HERE, "_ref", "mirror")
+    if os.path.isdir(mirror):
+        shutil.rmtree(mirror)
+    os.makedirs(os.path.join(mirror, "cfa"))
+    try:
+        sites = {}
+        if swap:
+            sites.setdefault("cylinder_fem_amr.cu", []).extend(SWAP_SITES)
+        if tight:
+            for f, s in TIGHT_SITES.items():
+                sites.setdefault(f, []).extend(s)
+        files = [("cylinder_fem_amr.cu", main)] + [(os.path.join("cfa", f), os.path.join(cfa_dir, f))
+                                                  for f in os.listdir(cfa_dir)]
+        for rel, src in files:
+            dst = os.path.join(mirror, rel)
+            if shim and rel == os.path.join("cfa", "linalg.cuh"):
+                os.symlink(SHIM, dst)
+            elif os.path.basename(rel) in sites:
+                with open(dst, "w") as f:
+                    f.write(_substitute(open(src).read(), sites[os.path.basename(rel)]))
+            else:
+                os.symlink(src, dst)
+        extra = []
+        if shim:
+            extra = ["-I", os.path.join(ROOT, "include"), "-L", PKG, "-lcfa_b200",
+                     "-Xlinker", "-rpath,$ORIGIN/../../cylinder-fem-amr_b200"]
+        subprocess.check_call(_driver_cmd(os.path.join(mirror, "cylinder_fem_amr.cu"), out, extra))
+    finally:
+        shutil.rmtree(mirror)
+
+
 def build_drivers(force: bool = False) -> tuple[str | None, str | None]:
-    """The reference application as it ships, and the same source on this repository's solvers.
-    Returns (stock, drop-in) paths, None where neither the reference tree nor a prebuilt binary
-    exists."""
+    """The reference application as it ships, and the same source on this repository's solvers
+    (plus the call-site-swapped build and the two tight-tolerance builds). Returns (stock, drop-in)
+    paths, None where neither the reference tree nor a prebuilt binary exists."""
     main = os.path.join(REFERENCE_SRC, "cylinder_fem_amr.cu")
     if not os.path.exists(main):
         return (REF_DRIVER if os.path.exists(REF_DRIVER) else None,
@@ -108,34 +176,14 @@ def build_drivers(force: bool = False) -> tuple[str | None, str | None]:
     os.makedirs(os.path.dirname(REF_DRIVER), exist_ok=True)
     if force or _stale(REF_DRIVER, deps):
         subprocess.check_call(_driver_cmd(main, REF_DRIVER, []))
+    if force or _stale(REF_TIGHT_DRIVER, deps + [os.path.abspath(__file__)]):
+        _build_mirrored(REF_TIGHT_DRIVER, shim=False, swap=False, tight=True)
     lib = os.path.join(PKG, "libcfa_b200.so")
     header = os.path.join(ROOT, "include", "cfa_b200.h")
-    for out, swap in ((DROPIN_DRIVER, False), (SWAP_DRIVER, True)):
-        if not (force or _stale(out, deps + [SHIM, lib, header, os.path.abspath(__file__)])):
-            continue
-        mirror = os.path.join(HERE, "_ref", "mirror")
-        if os.path.isdir(mirror):
-            shutil.rmtree(mirror)
-        os.makedirs(os.path.join(mirror, "cfa"))
-        try:
-            if swap:
-                text = open(main).read()
-                for anchor, repl in SWAP_SITES:
-                    if text.count(anchor) != 1:
-                        raise RuntimeError(f"call site not found exactly once: {anchor}")
-                    text = text.replace(anchor, repl)
-                with open(os.path.join(mirror, "cylinder_fem_amr.cu"), "w") as f:
-                    f.write(text)
-            else:
-                os.symlink(main, os.path.join(mirror, "cylinder_fem_amr.cu"))
-            for f in os.listdir(cfa_dir):
-                target = SHIM if f == "linalg.cuh" else os.path.join(cfa_dir, f)
-                os.symlink(target, os.path.join(mirror, "cfa", f))
-            extra = ["-I", os.path.join(ROOT, "include"), "-L", PKG, "-lcfa_b200",
-                     "-Xlinker", "-rpath,$ORIGIN/../../cylinder-fem-amr_b200"]
-            subprocess.check_call(_driver_cmd(os.path.join(mirror, "cylinder_fem_amr.cu"), out, extra))
-        finally:
-            shutil.rmtree(mirror)
+    for out, swap, tight in ((DROPIN_DRIVER, False, False), (SWAP_DRIVER, True, False),
+                             (DROPIN_TIGHT_DRIVER, False, True)):
+        if force or _stale(out, deps + [SHIM, lib, header, os.path.abspath(__file__)]):
+            _build_mirrored(out, shim=True, swap=swap, tight=tight)
     return REF_DRIVER, DROPIN_DRIVER
 
 

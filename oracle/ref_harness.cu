@@ -368,6 +368,13 @@ void* ref_step_create(int n, int ne, const int* ev, const double* x, const doubl
                       const double* u, const double* v, const double* p, double dt, double nu,
                       double rho, double u_max, double H, double tau_time, double stab, double tol,
                       int max_it_mom, int max_it_p) {
+#ifdef _OPENMP
+    // The reference application's host-thread rule (src/cylinder_fem_amr.cu:134-138), which
+    // CFA_NO_MAIN skips with the rest of main(): unless OMP_NUM_THREADS is set, half the logical
+    // CPUs, at most 8. Without it the AMG setup's OpenMP loops oversubscribe the host and run
+    // several times slower than in the reference's own program.
+    if (!std::getenv("OMP_NUM_THREADS")) omp_set_num_threads(std::max(1, std::min(8, omp_get_num_procs() / 2)));
+#endif
     auto* S = new RefStep();
     S->mesh = to_mesh(n, ne, ev, x, y, tag);
     S->u0.assign(u, u + n);
@@ -507,5 +514,17 @@ void ref_step_systems(void* h, double* A_val, double* rhs_u, double* rhs_v, doub
 }
 
 void ref_step_free(void* h) { delete static_cast<RefStep*>(h); }
+
+// Stored entries of the step's CSR pattern.
+int ref_step_nnz(void* h) { return static_cast<RefStep*>(h)->g.nnz; }
+
+// Host threads the reference's OpenMP loops (AMG setup) run with.
+int ref_omp_threads() {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
 
 }  // extern "C"

@@ -4,7 +4,10 @@
 its README recipe); ``oracle/_ref/cfa_dropin_driver`` is the same source compiled against the
 shim header ``cylinder-fem-amr_b200/shim/cfa/linalg.cuh`` and linked with ``libcfa_b200.so``;
 ``oracle/_ref/cfa_swap_driver`` additionally has the driver's Step A and B call sites switched to
-this library's assembly and handle-based PPE solve (``oracle/build.py drivers``). Each runs the
+this library's assembly and handle-based PPE solve; ``oracle/_ref/cfa_ref_driver_tight`` and
+``oracle/_ref/cfa_dropin_driver_tight`` are the stock program and the drop-in with the solver
+tolerances at the call sites set to 1e-10 instead of the application's 1e-7 / 1e-8
+(``oracle/build.py drivers``). Each runs the
 DFG 2D-2 cylinder case on a uniform level-3 mesh (the reference's U3 run, 29k nodes) and with
 adaptive refinement (its A1 settings, a remesh every 10 steps), and the force histories
 (``<prefix>_forces.csv``, 10 significant digits), meshes and iteration counts are compared with
@@ -24,6 +27,8 @@ REF_DIR = os.path.join(os.path.dirname(HERE), "oracle", "_ref")
 STOCK = os.path.join(REF_DIR, "cfa_ref_driver")
 DROPIN = os.path.join(REF_DIR, "cfa_dropin_driver")
 SWAP = os.path.join(REF_DIR, "cfa_swap_driver")
+STOCK_TIGHT = os.path.join(REF_DIR, "cfa_ref_driver_tight")
+DROPIN_TIGHT = os.path.join(REF_DIR, "cfa_dropin_driver_tight")
 
 torch = pytest.importorskip("torch")
 if not torch.cuda.is_available():
@@ -70,19 +75,31 @@ def compare(a, b):
 _STOCK_RUNS = {}
 
 
-def stock(case, tmp_path_factory):
-    if case not in _STOCK_RUNS:
-        _STOCK_RUNS[case] = run(STOCK, case, tmp_path_factory.mktemp("stock"))
-    return _STOCK_RUNS[case]
+def stock(case, tmp_path_factory, binary=STOCK):
+    key = (case, binary)
+    if key not in _STOCK_RUNS:
+        _STOCK_RUNS[key] = run(binary, case, tmp_path_factory.mktemp("stock"))
+    return _STOCK_RUNS[key]
+
+
+# Largest force difference allowed, relative to the series' scale. At the application's own
+# tolerances (CG and BiCGSTAB stop at |r| < 1e-7 |b|) a PPE solve that stops one iteration earlier
+# or later than the stock program's moves the solution by about the tolerance, and on A1 that
+# shows in the lift from the first step after the remesh at step 65 on (31 against 32 CG
+# iterations there): measured C_D 3.1e-10, C_L 4.5e-9, dp 4.2e-10. With both programs' tolerances
+# at 1e-10 the same comparison measures C_D 0, C_L 1.1e-11, dp 0 -- the stock program's own
+# run-to-run spread (its assembly sums with atomics), so there the north star's 1e-9 holds.
+FORCE_TOL = {"dropin": 1e-8, "swap": 1e-8, "dropin_tight": 1e-9}
 
 
 @pytest.mark.parametrize("case", ["U3", "A1"])
-@pytest.mark.parametrize("build", ["dropin", "swap"])
+@pytest.mark.parametrize("build", ["dropin", "swap", "dropin_tight"])
 def test_unmodified_application_on_b200_solvers(build, case, tmp_path, tmp_path_factory):
-    binary = DROPIN if build == "dropin" else SWAP
-    if not os.path.exists(binary):
+    binary = {"dropin": DROPIN, "swap": SWAP, "dropin_tight": DROPIN_TIGHT}[build]
+    ref_binary = STOCK_TIGHT if build == "dropin_tight" else STOCK
+    if not (os.path.exists(binary) and os.path.exists(ref_binary)):
         pytest.skip(f"{binary} not built")
-    ref_rows, ref_it, ref_wall, _ = stock(case, tmp_path_factory)
+    ref_rows, ref_it, ref_wall, _ = stock(case, tmp_path_factory, ref_binary)
     new_rows, new_it, new_wall, out = run(binary, case, tmp_path)
     diff, same_mesh = compare(ref_rows, new_rows)
     print(f"{case}: wall {ref_wall} s (reference) vs {new_wall} s ({build}); max rel diff {diff}; "
@@ -90,9 +107,9 @@ def test_unmodified_application_on_b200_solvers(build, case, tmp_path, tmp_path_
     assert same_mesh
     # Iteration counts of the printed steps. Momentum: within one of the reference's at every
     # step. PPE: CG stops at |r| < 1e-7 |b|, and the 2-norm of a CG residual is not monotone;
-    # where it oscillates about the tolerance, rounding decides whether a dip crosses it, a few
-    # iterations early (on A1 each implementation has one such step in 400, 5-6 iterations
-    # short). So: within one at 90 % of the printed steps, and the totals within 1 %.
+    # where it oscillates about the tolerance, rounding decides whether a dip crosses it (on A1
+    # the counts differ at 111 of 400 steps at 1e-7 and at 153 at 1e-10, by one or two). So:
+    # within one at 90 % of the printed steps, and the totals within 1 %.
     assert ref_it.keys() == new_it.keys()
     close = 0
     for s in ref_it:
@@ -102,6 +119,6 @@ def test_unmodified_application_on_b200_solvers(build, case, tmp_path, tmp_path_
     assert close >= 0.9 * len(ref_it)
     tot_ref, tot_new = sum(v[2] for v in ref_it.values()), sum(v[2] for v in new_it.values())
     assert abs(tot_ref - tot_new) <= 0.01 * tot_ref
-    # forces to 1e-7 of their scale (the histories are printed with 10 significant digits)
+    # forces (the histories are printed with 10 significant digits)
     for key, d in diff.items():
-        assert d <= 1e-7, (key, d)
+        assert d <= FORCE_TOL[build], (key, d)

@@ -3,7 +3,8 @@
 Both are called through the C ABI on the same assembled OSS operator. Two calls in a row with
 different inputs check that the static scratch carries nothing from one call to the next.
 Tolerance: 1e-13 relative to the largest |entry| (the two use the same per-row summation order,
-so the results are expected to be identical).
+so the results are expected to be identical). Around those two calls the device's free memory and
+the library's block cache are unchanged: the entry point allocates nothing.
 """
 import ctypes as C
 
@@ -60,12 +61,17 @@ def test_oss_apply_noalloc_matches_oss_apply(name):
         ref = base.clone()
         cfa.oss_apply(ctx, dm, oss, inv_m, x, ref)
         want.append(ref)
-    for x in xs:   # two calls in a row on the same scratch
-        out = base.clone()
+    outs = [base.clone() for _ in xs]
+    torch.cuda.synchronize()
+    # device memory and the library's block cache before and after: the calls allocate nothing
+    free0, cached0 = torch.cuda.mem_get_info()[0], cfa.mem_cached()[0]
+    for x, out in zip(xs, outs):   # two calls in a row on the same scratch
         st = _noalloc(ctx, dm, oss, inv_m, x, out)
         assert st == cfa.CFA_OK, _last_error(ctx)
         got.append(out)
     torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert cfa.mem_cached()[0] == cached0
     for w, g in zip(want, got):
         w, g = w.cpu().numpy(), g.cpu().numpy()
         assert np.abs(g - w).max() <= TOL * np.abs(w).max()
