@@ -251,10 +251,13 @@ def run_ours(args, rank, world):
             e2e_total += ev[0].elapsed_time(ev[1])
         clk.pause()
         e2e_ms = e2e_total / args.steps
+        clk.start()
         op_ms, op_layout = time_operator(cfa, st, 20, flush) if prec == cfa.FP64 else (None, None)
+        kern = kernel_table(cfa, st, flush)[0] if prec == cfa.MIXED else None
+        clk.pause()
         res[prec_name] = dict(step_ms=step_ms, setup_ms=setup_ms, e2e_ms=e2e_ms, launches=launches,
                               report=reports[-1], op_ms=op_ms, op_layout=op_layout, levels=st.amg.num_levels(), phases=phases,
-                              colours=st.ilu.n_colours, nnz=st.nnz, n=st.n)
+                              colours=st.ilu.n_colours, nnz=st.nnz, n=st.n, kernels=kern)
         del st
     clk.stop()
     res["clocks"] = clk.summary()
@@ -369,54 +372,28 @@ def vcycle_bytes(levels, coarse_n, vb, eb=8):
     return total + 8 * coarse_n * coarse_n + 2 * eb * coarse_n
 
 
-def run_stress(args, rank, world):
+def ilu_bytes(n, nnz, vb, wb):
+    """Algorithmic bytes of one two-right-hand-side ILU apply (forward and backward colour sweeps,
+    both right-hand sides interleaved per row): the split factors once ((nnz - n) column indices
+    and values of vb bytes), the diagonal inverse, the row order and the split offsets; the FP64
+    right-hand side read once and the FP64 result written once (16 bytes a row each), the work
+    vector (wb bytes a row for the pair: 16 in FP64, where it is the result itself, 8 in FP32)
+    written by the forward sweep and read and written by the backward sweep."""
+    base = (nnz - n) * (vb + 4) + n * vb + 4 * n + 8 * (n + 1)
+    if wb == 16:                      # in place in the FP64 result: r read, y written, y read, z written
+        return base + 4 * 16 * n
+    return base + 16 * n + wb * n + 2 * wb * n + 16 * n
+
+
+def kernel_table(cfa, st, flush, reps=20):
+    """Per-kernel bandwidth of the four paths the solves spend their time in, each applied alone
+    on the step's own operators, repeated, timed by CUDA events on the context's stream with the
+    L2 flushed before each repetition: the pressure operator (FP64, one pass), the V-cycle (the
+    handle's precision), the momentum ILU apply (interleaved pair, the handle's precision) and the
+    two-right-hand-side momentum SpMV (FP64)."""
     import torch
-    import cfa_b200 as cfa
-    import step as S
-
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    m, u, v, p = workload_inputs("c2")
-    ctx = cfa.Context()
-    st = S.SolveStep(m, u, v, p, precision=cfa.MIXED, ctx=ctx, dt=DT, nu=NU, stab=STAB, u_max=U_MAX, tol=TOL)
-    st.amg_setup()
-    base_u, base_v, base_p = st.rhs_u.clone(), st.rhs_v.clone(), st.rhs_p.clone()
-    n, nnz = st.n, st.nnz
-    solves = max(args.steps, 1)
-
-    def perturbed(k):
-        g = torch.Generator(device="cuda")
-        g.manual_seed(k)
-        st.rhs_u.copy_(base_u + 1e-3 * torch.randn(n, generator=g, device="cuda", dtype=torch.float64))
-        st.rhs_v.copy_(base_v + 1e-3 * torch.randn(n, generator=g, device="cuda", dtype=torch.float64))
-        st.rhs_p.copy_(base_p + 1e-3 * torch.randn(n, generator=g, device="cuda", dtype=torch.float64))
-        st.u.copy_(st.u_n)
-        st.v.copy_(st.v_n)
-        st.dp.zero_()
-
-    for k in range(args.warmup):
-        perturbed(1000 + k)
-        st.solve_momentum()
-        st.solve_pressure()
-    torch.cuda.synchronize()
+    ctx = st.ctx
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
-    clk.start()
-    total, its = 0.0, []
-    l0 = ctx.launches
-    for k in range(solves):
-        perturbed(k)
-        ev[0].record()
-        st.solve_momentum()
-        st.solve_pressure()
-        ev[1].record()
-        ev[1].synchronize()
-        total += ev[0].elapsed_time(ev[1])
-        r = st.report()
-        its.append((r["it_u"], r["it_v"], r["it_p"]))
-    launches = ctx.launches - l0
-    # per-kernel bandwidth: each path applied alone, repeated, timed by events on the context stream
-    reps = 20
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
     def timed(fn):
         fn()
@@ -431,7 +408,9 @@ def run_stress(args, rank, world):
             acc += ev[0].elapsed_time(ev[1])
         return acc / reps * 1e3
 
-    hbm, peak_kind = peaks()
+    hbm, _ = peaks()
+    n, nnz = st.n, st.nnz
+    mixed = st.precision == cfa.MIXED
     x = torch.randn(n, dtype=torch.float64, device="cuda")
     y = torch.empty_like(x)
     cfa.pressure_operator_prepare(ctx, st.dm.rp, st.dm.ci, st.Kp, st.oss)
@@ -441,39 +420,119 @@ def run_stress(args, rank, world):
     z = torch.empty_like(x)
     t_vc = timed(lambda: st.amg.apply(x, z))
     levels = []
-    for l in range(st.amg.num_levels() - 1):
-        d = st.amg.level(l)
+    for lvl in range(st.amg.num_levels() - 1):
+        d = st.amg.level(lvl)
         levels.append((d["rows"], int(d["A"][1].numel()), d["pcols"], int(d["P"][1].numel())))
-    fp32_vectors = os.environ.get("CFA_VCYCLE_FP64", "0") != "1"   # the mixed V-cycle's vectors
-    b_vc = vcycle_bytes(levels, st.amg.coarse_n, 4, 4 if fp32_vectors else 8)
+    fp32_vectors = mixed and os.environ.get("CFA_VCYCLE_FP64", "0") != "1"
+    b_vc = vcycle_bytes(levels, st.amg.coarse_n, 4 if mixed else 8, 4 if fp32_vectors else 8)
     x2 = torch.randn(2 * n, dtype=torch.float64, device="cuda")
     z2 = torch.empty_like(x2)
-    t_ilu = timed(lambda: st.ilu.apply(x2, z2, 2))
-    b_ilu = (nnz - n) * (4 + 4) + n * 4 + 4 * n + 8 * (n + 1) + 2 * n * 8 * 4
+    t_ilu = timed(lambda: st.ilu.apply_interleaved(x2, z2))
+    b_ilu = ilu_bytes(n, nnz, 4 if mixed else 8, 8 if mixed else 16)
     t_spmv = timed(lambda: cfa.spmv_multi(ctx, st.dm.rp, st.dm.ci, st.A, x2, z2, 2))
     b_spmv = nnz * 12 + 4 * (n + 1) + 4 * n * 8
-    clk.stop()
+    tag = "fp32" if mixed else "fp64"
     kern = {}
-    for name, b, t in (("pressure_operator", b_op, t_op), ("vcycle_fp32", b_vc, t_vc), ("ilu_apply_2rhs_fp32", b_ilu, t_ilu),
-                       ("momentum_spmv_2rhs", b_spmv, t_spmv)):
+    for name, b, t in (("pressure_operator_fp64", b_op, t_op), (f"vcycle_{tag}", b_vc, t_vc),
+                       (f"ilu_apply_2rhs_{tag}", b_ilu, t_ilu), ("momentum_spmv_2rhs_fp64", b_spmv, t_spmv)):
         gbs = b / (t * 1e-6) / 1e9
         kern[name] = {"bytes": int(b), "us": round(t, 2), "gbs": round(gbs, 1), "frac": round(gbs / hbm, 4)}
-    ms = total / solves
+    return kern, passes
+
+
+def run_stress(args, rank, world):
+    """c2: repeated momentum + pressure solve pairs on the ~4M-vertex mesh with seeded N(0, 1e-3)
+    right-hand-side noise, mixed precision (the headline) and plain FP64, and the per-kernel
+    bandwidth table of each precision. With --profile, one mixed solve pair runs between
+    cudaProfilerStart/Stop (for ncu --profile-from-start off) and no line is printed."""
+    import torch
+    import cfa_b200 as cfa
+    import step as S
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    m, u, v, p = workload_inputs("c2")
+    ctx = cfa.Context()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    solves = max(args.steps, 1)
+    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
+    legs = {}
+    for prec_name, prec in (("mixed", cfa.MIXED), ("fp64", cfa.FP64)):
+        st = S.SolveStep(m, u, v, p, precision=prec, ctx=ctx, dt=DT, nu=NU, stab=STAB, u_max=U_MAX, tol=TOL)
+        st.amg_setup()
+        base_u, base_v, base_p = st.rhs_u.clone(), st.rhs_v.clone(), st.rhs_p.clone()
+        n, nnz = st.n, st.nnz
+
+        def perturbed(k):
+            g = torch.Generator(device="cuda")
+            g.manual_seed(k)
+            st.rhs_u.copy_(base_u + 1e-3 * torch.randn(n, generator=g, device="cuda", dtype=torch.float64))
+            st.rhs_v.copy_(base_v + 1e-3 * torch.randn(n, generator=g, device="cuda", dtype=torch.float64))
+            st.rhs_p.copy_(base_p + 1e-3 * torch.randn(n, generator=g, device="cuda", dtype=torch.float64))
+            st.u.copy_(st.u_n)
+            st.v.copy_(st.v_n)
+            st.dp.zero_()
+
+        for k in range(args.warmup):
+            perturbed(1000 + k)
+            st.solve_momentum()
+            st.solve_pressure()
+        torch.cuda.synchronize()
+        if args.profile:
+            perturbed(0)
+            torch.cuda.synchronize()
+            torch.cuda.profiler.start()
+            st.solve_momentum()
+            st.solve_pressure()
+            torch.cuda.synchronize()
+            torch.cuda.profiler.stop()
+            print(json.dumps({"profile": "c2 " + prec_name, "report": st.report(), "launches": ctx.launches}))
+            return
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        clk.start()
+        total, its = 0.0, []
+        l0 = ctx.launches
+        for k in range(solves):
+            perturbed(k)
+            ev[0].record()
+            st.solve_momentum()
+            st.solve_pressure()
+            ev[1].record()
+            ev[1].synchronize()
+            total += ev[0].elapsed_time(ev[1])
+            r = st.report()
+            its.append((r["it_u"], r["it_v"], r["it_p"]))
+        launches = ctx.launches - l0
+        kern, passes = kernel_table(cfa, st, flush)
+        clk.pause()
+        legs[prec_name] = dict(ms=total / solves, its=its, launches=launches, kernels=kern, passes=passes,
+                               levels=st.amg.num_levels(), n=n, nnz=nnz)
+        del st
+        torch.cuda.synchronize()
+    clk.stop()
+    hbm, peak_kind = peaks()
+    mx, f64 = legs["mixed"], legs["fp64"]
+    n, nnz = mx["n"], mx["nnz"]
+    kern = mx["kernels"]
     line = {
         "metric": "pressure+momentum solve ms per repeated solve & HBM GB/s per kernel (c2, mixed, 1e-10 rel res)",
-        "value": round(ms, 3), "unit": "ms/solve pair", "n_gpus": 1, "steps": solves, "warmup": args.warmup,
-        "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "value": round(mx["ms"], 3), "unit": "ms/solve pair", "n_gpus": 1, "steps": solves, "warmup": args.warmup,
+        "ms_per_step": round(mx["ms"], 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 outer / f32 preconditioners", "data": "synthetic",
         "config": {"workload": f"c2: uniform NVB mesh n={n}, nnz={nnz}; {solves} solves, RHS + N(0, 1e-3) noise "
                                "seeded by the solve index (momentum BiCGSTAB2 + pressure PCG)",
-                   "l2": "inputs larger than L2", "iterations_median": [int(np.median([i[c] for i in its])) for c in range(3)],
-                   "amg_levels": st.amg.num_levels(), "pressure_operator_passes": passes},
+                   "l2": "inputs larger than L2; kernels timed alone with a 256 MB L2 flush before each",
+                   "iterations_median": [int(np.median([i[c] for i in mx["its"]])) for c in range(3)],
+                   "fp64_ms_per_solve_pair": round(f64["ms"], 3),
+                   "mixed_speedup_vs_fp64": round(f64["ms"] / mx["ms"], 3),
+                   "iterations_median_fp64": [int(np.median([i[c] for i in f64["its"]])) for c in range(3)],
+                   "amg_levels": mx["levels"], "pressure_operator_passes": mx["passes"]},
         "kernels": kern,
+        "kernels_fp64": f64["kernels"],
         "roofline": {"bound": "hbm", "kernel": "pressure operator (K - B^T M^-1 B, one pass), FP64",
-                     "achieved": kern["pressure_operator"]["gbs"], "peak": hbm, "unit": "GB/s",
-                     "frac": kern["pressure_operator"]["frac"], "traffic": None, "peak_kind": peak_kind},
-        "e2e": {"value": round(ms, 3), "unit": "ms/solve pair", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 48},
-        "gpu_launches": int(launches),
+                     "achieved": kern["pressure_operator_fp64"]["gbs"], "peak": hbm, "unit": "GB/s",
+                     "frac": kern["pressure_operator_fp64"]["frac"], "traffic": None, "peak_kind": peak_kind},
+        "e2e": {"value": round(mx["ms"], 3), "unit": "ms/solve pair", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 48},
+        "gpu_launches": int(mx["launches"]),
         "clocks": clk.summary(),
     }
     print(json.dumps(line))
@@ -689,6 +748,7 @@ def main():
                      "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": peak_kind,
                      "bytes_per_launch": op_bytes, "stored_nnz": stored_nnz, "launch_us": round(op_ms * 1e3, 2)},
+        "kernels": mixed["kernels"],
         "cpu_baseline": cpu,
         "clocks": clocks,
     }

@@ -412,6 +412,10 @@ class MulticolourIlu0:
     def apply(self, r, z, nrhs=1):
         self.ctx.check(lib().cfa_ilu_apply(self.ctx.h, self.h, ptr(r), ptr(z), nrhs))
 
+    def apply_interleaved(self, r, z):
+        """Two right-hand sides interleaved per row (r[2i], r[2i + 1]): the momentum solve's sweeps."""
+        self.ctx.check(lib().cfa_ilu_apply_interleaved(self.ctx.h, self.h, ptr(r), ptr(z)))
+
     def factor_transposed(self, d_val):
         """Factor A and keep (LU)^T: the handle then preconditions A^T."""
         self.ctx.check(lib().cfa_ilu_factor_transposed(self.ctx.h, self.h, ptr(d_val)))

@@ -779,11 +779,11 @@ template <int TPR, int OP, class V, class T, class B, class O, bool RZ = false>
 __global__ void __launch_bounds__(kTileThreads)
 k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b, const T* __restrict__ x,
       O* __restrict__ y, const int* __restrict__ done, RzFuse rzf) {
-    CFA_GRID_DEP();
-    if (done && *done) return;
     extern __shared__ __align__(128) unsigned char tsmem[];
     double dots[2] = {0.0, 0.0};   // RZ: this thread's rows of r.z and z.q
-    tile_loop(tv, tsmem, [&](int, int r0, int nr, const unsigned char* ch) {
+    // the level's tiles are packed at setup: their first copies go out before the wait
+    const bool go = tile_loop_dep(tv, tsmem, [&] { return !(done && *done); },
+                                  [&](int, int r0, int nr, const unsigned char* ch) {
         const int* rr = reinterpret_cast<const int*>(ch);
         const int ne = rr[nr];
         const int* cs = reinterpret_cast<const int*>(ch + tile_ci_off(nr));
@@ -850,6 +850,7 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
             }
         }
     });
+    if (!go) return;
     if constexpr (RZ) {
         __shared__ double sh[2 * kWarps];
         block_sum<2>(dots, sh);
@@ -1426,7 +1427,289 @@ static cfa_status transpose(cfa_ctx* ctx, SetupScratch& S, const DCsr& A, DCsr& 
     return CFA_OK;
 }
 
+// ---------------------------------------------------------------------------------------------
+// The greedy 3-phase aggregation (smoothed_prolongator, src/cfa/linalg.cuh:1321-1348) on the
+// device, giving the aggregates of the sequential loop bit for bit.
+//
+// Phase 1 visits nodes in index order; node i becomes a root (a new aggregate with its strong
+// neighbours) iff, when it is visited, neither i nor any strong neighbour j of i is aggregated.
+// "Aggregated when i is visited" only involves roots k < i: i is aggregated iff some root k < i
+// has i as a strong neighbour (k -> i); j is iff j is a root below i, or some root k < i has
+// k -> j. So root(i) depends only on the root status of lower-numbered nodes within two strong
+// hops -- the lexicographically first independent set of that conflict relation. It is found in
+// rounds: an undecided node becomes a non-root as soon as one lower conflict is a root, and a
+// root once all of its lower conflicts are decided non-roots. Every round decides at least the
+// lowest undecided node, states only move from undecided to final, so the rounds may read each
+// other's states at any time. Aggregate ids follow root order (a prefix sum); a non-root takes
+// the id of the root that has it as a strong neighbour (at most one can).
+// Phase 2 (parallel in the reference too) gives an unaggregated node the aggregate of its first
+// aggregated strong neighbour. Phase 3 visits the rest in index order: an unaggregated node
+// starts a new aggregate and claims its unaggregated strong neighbours (all of higher index), so
+// it is a root iff no lower root claims it, and a claimed node belongs to the lowest root that
+// claims it. The strong relation is read as directed (row i's entries), as in the reference:
+// coarse Galerkin operators need not be symmetric to the last bit.
+// ---------------------------------------------------------------------------------------------
+enum : unsigned char { AGG_UNDECIDED = 0, AGG_ROOT = 1, AGG_MEMBER = 2 };
+
+// in-degree of the strong graph (k -> j counted at j)
+__global__ void k_strong_indeg(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                               const unsigned char* __restrict__ strong, int* __restrict__ cnt) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int a = rp[i]; a < rp[i + 1]; ++a)
+        if (strong[a]) atomicAdd(cnt + ci[a], 1);
+}
+
+// in-neighbour lists (their order within a list does not matter to the rounds below)
+__global__ void k_strong_fill(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                              const unsigned char* __restrict__ strong, const int* __restrict__ trp,
+                              int* __restrict__ fill, int* __restrict__ tci) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int a = rp[i]; a < rp[i + 1]; ++a)
+        if (strong[a]) {
+            const int j = ci[a];
+            tci[trp[j] + atomicAdd(fill + j, 1)] = i;
+        }
+}
+
+__device__ __forceinline__ unsigned char agg_state(const unsigned char* st, int k) {
+    return *reinterpret_cast<const volatile unsigned char*>(st + k);
+}
+
+// One round of phase 1. `more` is set when a node is still undecided at the end of its visit.
+__global__ void k_agg_p1_round(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                               const unsigned char* __restrict__ strong, const int* __restrict__ trp,
+                               const int* __restrict__ tci, unsigned char* st, int* __restrict__ more) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || agg_state(st, i) != AGG_UNDECIDED) return;
+    bool pending = false;
+    // a root k < i with k -> i aggregated i before its visit
+    for (int q = trp[i]; q < trp[i + 1]; ++q) {
+        const int k = tci[q];
+        if (k >= i) continue;
+        const unsigned char sk = agg_state(st, k);
+        if (sk == AGG_ROOT) { st[i] = AGG_MEMBER; return; }
+        pending |= sk == AGG_UNDECIDED;
+    }
+    // a strong neighbour j aggregated before i's visit: a root below i, or k -> j from a root k < i
+    for (int a = rp[i]; a < rp[i + 1]; ++a) {
+        if (!strong[a]) continue;
+        const int j = ci[a];
+        if (j < i) {
+            const unsigned char sj = agg_state(st, j);
+            if (sj == AGG_ROOT) { st[i] = AGG_MEMBER; return; }
+            pending |= sj == AGG_UNDECIDED;
+        }
+        for (int q = trp[j]; q < trp[j + 1]; ++q) {
+            const int k = tci[q];
+            if (k >= i) continue;
+            const unsigned char sk = agg_state(st, k);
+            if (sk == AGG_ROOT) { st[i] = AGG_MEMBER; return; }
+            pending |= sk == AGG_UNDECIDED;
+        }
+    }
+    if (!pending) st[i] = AGG_ROOT;
+    else *more = 1;
+}
+
+// Phase 1 ids: a root's from the prefix sum of roots; a member's from the root that has it as a
+// strong neighbour; -1 for the rest.
+__global__ void k_agg_p1_ids(int n, const int* __restrict__ trp, const int* __restrict__ tci,
+                             const unsigned char* __restrict__ st, const int* __restrict__ rank, int* __restrict__ agg) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int a = -1;
+    if (st[i] == AGG_ROOT) {
+        a = rank[i];
+    } else {
+        for (int q = trp[i]; q < trp[i + 1]; ++q) {
+            const int k = tci[q];
+            if (st[k] == AGG_ROOT) { a = rank[k]; break; }
+        }
+    }
+    agg[i] = a;
+}
+
+// Phase 2: the first aggregated strong neighbour (row order) of an unaggregated node; also marks
+// the nodes left for phase 3 (undecided) and the others (member).
+__global__ void k_agg_p2(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                         const unsigned char* __restrict__ strong, const int* __restrict__ agg1, int* __restrict__ agg2,
+                         unsigned char* __restrict__ st3) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int a = agg1[i];
+    if (a < 0)
+        for (int e = rp[i]; e < rp[i + 1]; ++e)
+            if (strong[e] && agg1[ci[e]] >= 0) { a = agg1[ci[e]]; break; }
+    agg2[i] = a;
+    st3[i] = a < 0 ? AGG_UNDECIDED : AGG_MEMBER;
+}
+
+// One round of phase 3: a node left unaggregated is claimed by a lower root k -> i, a root
+// once every lower unaggregated in-neighbour is decided and none is a root.
+__global__ void k_agg_p3_round(int n, const int* __restrict__ trp, const int* __restrict__ tci,
+                               const int* __restrict__ agg2, unsigned char* st, int* __restrict__ more) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || agg_state(st, i) != AGG_UNDECIDED) return;
+    bool pending = false;
+    for (int q = trp[i]; q < trp[i + 1]; ++q) {
+        const int k = tci[q];
+        if (k >= i || agg2[k] >= 0) continue;
+        const unsigned char sk = agg_state(st, k);
+        if (sk == AGG_ROOT) { st[i] = AGG_MEMBER; return; }
+        pending |= sk == AGG_UNDECIDED;
+    }
+    if (!pending) st[i] = AGG_ROOT;
+    else *more = 1;
+}
+
+// Phase 3 ids (after na1 phase-1 aggregates): roots in order; a claimed node takes its lowest
+// claiming root's id. Also counts the aggregate sizes.
+__global__ void k_agg_p3_ids(int n, int na1, const int* __restrict__ trp, const int* __restrict__ tci,
+                             const unsigned char* __restrict__ st, const int* __restrict__ rank,
+                             const int* __restrict__ agg2, int* __restrict__ agg, int* __restrict__ size) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int a = agg2[i];
+    if (a < 0) {
+        if (st[i] == AGG_ROOT) {
+            a = na1 + rank[i];
+        } else {
+            int kmin = n;
+            for (int q = trp[i]; q < trp[i + 1]; ++q) {
+                const int k = tci[q];
+                if (k < kmin && agg2[k] < 0 && st[k] == AGG_ROOT) kmin = k;
+            }
+            a = na1 + rank[kmin];
+        }
+    }
+    agg[i] = a;
+    atomicAdd(size + a, 1);
+}
+
+// Tentative prolongator: P0 row i holds 1 / sqrt(|aggregate of i|) in column agg[i].
+__global__ void k_agg_p0(int n, const int* __restrict__ agg, const int* __restrict__ size, int* __restrict__ p0rp,
+                         double* __restrict__ p0v) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    p0rp[i] = i;
+    if (i < n) p0v[i] = 1.0 / sqrt((double)size[agg[i]]);
+}
+
+
+// exclusive prefix sum of n ints (n + 1 outputs: the total at out[n])
+static cfa_status exclusive_sum(cfa_ctx* ctx, SetupScratch& S, const int* in, int* out, int n) {
+    size_t bytes = 0;
+    CFA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n + 1, ctx->stream));
+    CFA_CUDA(S.cub_tmp.ensure(bytes + 16));
+    CFA_CUDA(cub::DeviceScan::ExclusiveSum(S.cub_tmp.p, bytes, in, out, n + 1, ctx->stream));
+    ctx->launches += 2;
+    return CFA_OK;
+}
+
+__global__ void k_agg_is_root(int n, const unsigned char* __restrict__ st, int* __restrict__ flag) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= n) flag[i] = (i < n && st[i] == AGG_ROOT) ? 1 : 0;
+}
+
+// Runs the rounds of one phase until no node is undecided: rounds are launched in groups of
+// `kAggRoundsPerCheck`, the last of each group reporting whether undecided nodes remain. Every
+// round decides at least the lowest undecided node, so the loop ends; `rounds` counts them.
+template <class Launch>
+static cfa_status agg_rounds(cfa_ctx* ctx, SetupScratch& S, int n, Launch launch_round, int* rounds) {
+    constexpr int kAggRoundsPerCheck = 8;
+    int r = 0;
+    for (;;) {
+        CFA_CUDA(cudaMemsetAsync(S.ag_flag.p, 0, sizeof(int), ctx->stream));
+        for (int k = 0; k < kAggRoundsPerCheck; ++k) launch_round(k + 1 == kAggRoundsPerCheck ? S.ag_flag.p : S.ag_flag.p + 1);
+        r += kAggRoundsPerCheck;
+        CFA_CUDA(cudaMemcpyAsync(S.h_ag.p, S.ag_flag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (S.h_ag.p[0] == 0) break;
+        if (r > n + kAggRoundsPerCheck)
+            return set_error(ctx, CFA_CUDA_ERROR, "aggregation rounds did not finish", __FILE__, __LINE__);
+    }
+    if (rounds) *rounds += r;
+    return CFA_OK;
+}
+
+// The aggregates of A's strong graph (S.strong) into agg[m]; na = their count; the tentative
+// prolongator's row offsets and values into S.p0rp / S.p0v.
+static cfa_status aggregate_device(cfa_ctx* ctx, SetupScratch& S, const DCsr& A, int* agg, int* na_out) {
+    const int n = A.rows;
+    const int g = ceil_div(n, kThreads), g1 = ceil_div(n + 1, kThreads);
+    for (DevBuf<int>* b : {&S.ag_trp, &S.ag_fill, &S.ag_rank, &S.ag_agg1, &S.ag_agg2, &S.ag_size})
+        CFA_CUDA(b->ensure(n + 1));
+    CFA_CUDA(S.ag_tci.ensure(std::max(A.nnz, 1)));
+    CFA_CUDA(S.ag_state.ensure(n));
+    CFA_CUDA(S.ag_flag.ensure(2));
+    CFA_CUDA(S.h_ag.ensure(2));
+    CFA_CUDA(S.p0v.ensure(n));
+    CFA_CUDA(S.p0rp.ensure(n + 1));
+    // in-neighbour lists of the strong graph
+    CFA_CUDA(cudaMemsetAsync(S.ag_fill.p, 0, (n + 1) * sizeof(int), ctx->stream));
+    CFA_LAUNCH(ctx, k_strong_indeg, g, kThreads, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p, S.ag_fill.p);
+    CFA_PROPAGATE(exclusive_sum(ctx, S, S.ag_fill.p, S.ag_trp.p, n));
+    CFA_CUDA(cudaMemsetAsync(S.ag_fill.p, 0, (n + 1) * sizeof(int), ctx->stream));
+    CFA_LAUNCH(ctx, k_strong_fill, g, kThreads, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p,
+               (const int*)S.ag_trp.p, S.ag_fill.p, S.ag_tci.p);
+    // phase 1
+    CFA_CUDA(cudaMemsetAsync(S.ag_state.p, AGG_UNDECIDED, n, ctx->stream));
+    int rounds = 0;
+    CFA_PROPAGATE(agg_rounds(ctx, S, n, [&](int* more) {
+        CFA_LAUNCH(ctx, k_agg_p1_round, g, kThreads, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p,
+                   (const int*)S.ag_trp.p, (const int*)S.ag_tci.p, S.ag_state.p, more);
+    }, &rounds));
+    CFA_LAUNCH(ctx, k_agg_is_root, g1, kThreads, 0, n, (const unsigned char*)S.ag_state.p, S.ag_fill.p);
+    CFA_PROPAGATE(exclusive_sum(ctx, S, S.ag_fill.p, S.ag_rank.p, n));
+    CFA_LAUNCH(ctx, k_agg_p1_ids, g, kThreads, 0, n, (const int*)S.ag_trp.p, (const int*)S.ag_tci.p,
+               (const unsigned char*)S.ag_state.p, (const int*)S.ag_rank.p, S.ag_agg1.p);
+    // phase 2
+    CFA_LAUNCH(ctx, k_agg_p2, g, kThreads, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p,
+               (const int*)S.ag_agg1.p, S.ag_agg2.p, S.ag_state.p);
+    // phase 3 (the number of phase-1 aggregates first: the ids continue from it)
+    CFA_CUDA(cudaMemcpyAsync(S.h_ag.p + 1, S.ag_rank.p + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_PROPAGATE(agg_rounds(ctx, S, n, [&](int* more) {
+        CFA_LAUNCH(ctx, k_agg_p3_round, g, kThreads, 0, n, (const int*)S.ag_trp.p, (const int*)S.ag_tci.p,
+                   (const int*)S.ag_agg2.p, S.ag_state.p, more);
+    }, &rounds));
+    const int na1 = S.h_ag.p[1];
+    CFA_LAUNCH(ctx, k_agg_is_root, g1, kThreads, 0, n, (const unsigned char*)S.ag_state.p, S.ag_fill.p);
+    CFA_PROPAGATE(exclusive_sum(ctx, S, S.ag_fill.p, S.ag_rank.p, n));
+    CFA_CUDA(cudaMemsetAsync(S.ag_size.p, 0, (n + 1) * sizeof(int), ctx->stream));
+    CFA_LAUNCH(ctx, k_agg_p3_ids, g, kThreads, 0, n, na1, (const int*)S.ag_trp.p, (const int*)S.ag_tci.p,
+               (const unsigned char*)S.ag_state.p, (const int*)S.ag_rank.p, (const int*)S.ag_agg2.p, agg,
+               S.ag_size.p);
+    CFA_CUDA(cudaMemcpyAsync(S.h_ag.p, S.ag_rank.p + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_LAUNCH(ctx, k_agg_p0, g1, kThreads, 0, n, (const int*)agg, (const int*)S.ag_size.p, S.p0rp.p, S.p0v.p);
+    CFA_CHECK_LAUNCH();
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    *na_out = na1 + S.h_ag.p[0];
+    return CFA_OK;
+}
+
+
 // Greedy 3-phase aggregation of smoothed_prolongator (:1321-1348) on the host strength flags.
+// CFA_AGG_HOST=0: the aggregation runs as the device rounds; otherwise as the reference's
+// sequential host loop.
+static bool agg_on_host() {
+    static const bool on = [] {
+        const char* e = std::getenv("CFA_AGG_HOST");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 static int aggregate_host(int n, const int* rp, const int* ci, const unsigned char* strong, int* agg) {
     for (int i = 0; i < n; ++i) agg[i] = -1;
     int na = 0;
@@ -1619,36 +1902,42 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
         CFA_PROPAGATE(spectral_radius(ctx, amg, A, L.dinv.p, &rho));
         const double omega = 4.0 / (3.0 * rho);
         phase(1);
-        // strength on the device, aggregation on the host (pinned staging)
+        // strength on the device; aggregation by the sequential host loop or the device rounds
         SetupScratch& S = amg->scratch;
         CFA_CUDA(S.strong.ensure(std::max(A.nnz, 1)));
         CFA_LAUNCH(ctx, k_strength, ceil_div(m, kThreads), kThreads, 0, m, A.rp.p, A.ci.p, A.v.p, L.dinv.p, o.theta,
                    S.strong.p);
-        CFA_CUDA(S.h_rp.ensure(m + 1));
-        CFA_CUDA(S.h_ci.ensure(std::max(A.nnz, 1)));
-        CFA_CUDA(S.h_strong.ensure(std::max(A.nnz, 1)));
-        CFA_CUDA(cudaMemcpyAsync(S.h_rp.p, A.rp.p, (m + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-        CFA_CUDA(cudaMemcpyAsync(S.h_ci.p, A.ci.p, (size_t)A.nnz * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-        CFA_CUDA(cudaMemcpyAsync(S.h_strong.p, S.strong.p, (size_t)A.nnz, cudaMemcpyDeviceToHost, ctx->stream));
-        CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-        CFA_CUDA(S.h_agg.ensure(m));
-        const int na = aggregate_host(m, S.h_rp.p, S.h_ci.p, S.h_strong.p, S.h_agg.p);
-        if (na >= (int)(0.85 * m) || na == 0) break;   // coarsening stalled (:1019)
-        const int* agg = S.h_agg.p;
-        std::vector<int> size(na, 0);
-        for (int i = 0; i < m; ++i) size[agg[i]]++;
-        CFA_CUDA(S.h_p0v.ensure(m));
-        CFA_CUDA(S.h_p0rp.ensure(m + 1));
-        for (int i = 0; i < m; ++i) { S.h_p0v.p[i] = 1.0 / std::sqrt((double)size[agg[i]]); S.h_p0rp.p[i] = i; }
-        S.h_p0rp.p[m] = m;
         CFA_CUDA(L.agg.ensure(m));
-        CFA_CUDA(S.p0v.ensure(m));
-        CFA_CUDA(S.p0rp.ensure(m + 1));
+        int na = 0;
+        if (!agg_on_host()) {
+            CFA_PROPAGATE(aggregate_device(ctx, S, A, L.agg.p, &na));
+            if (na >= (int)(0.85 * m) || na == 0) break;   // coarsening stalled (:1019)
+        } else {
+            CFA_CUDA(S.h_rp.ensure(m + 1));
+            CFA_CUDA(S.h_ci.ensure(std::max(A.nnz, 1)));
+            CFA_CUDA(S.h_strong.ensure(std::max(A.nnz, 1)));
+            CFA_CUDA(cudaMemcpyAsync(S.h_rp.p, A.rp.p, (m + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+            CFA_CUDA(cudaMemcpyAsync(S.h_ci.p, A.ci.p, (size_t)A.nnz * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+            CFA_CUDA(cudaMemcpyAsync(S.h_strong.p, S.strong.p, (size_t)A.nnz, cudaMemcpyDeviceToHost, ctx->stream));
+            CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+            CFA_CUDA(S.h_agg.ensure(m));
+            na = aggregate_host(m, S.h_rp.p, S.h_ci.p, S.h_strong.p, S.h_agg.p);
+            if (na >= (int)(0.85 * m) || na == 0) break;   // coarsening stalled (:1019)
+            const int* agg = S.h_agg.p;
+            std::vector<int> size(na, 0);
+            for (int i = 0; i < m; ++i) size[agg[i]]++;
+            CFA_CUDA(S.h_p0v.ensure(m));
+            CFA_CUDA(S.h_p0rp.ensure(m + 1));
+            for (int i = 0; i < m; ++i) { S.h_p0v.p[i] = 1.0 / std::sqrt((double)size[agg[i]]); S.h_p0rp.p[i] = i; }
+            S.h_p0rp.p[m] = m;
+            CFA_CUDA(S.p0v.ensure(m));
+            CFA_CUDA(S.p0rp.ensure(m + 1));
+            CFA_CUDA(cudaMemcpyAsync(L.agg.p, agg, m * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+            CFA_CUDA(cudaMemcpyAsync(S.p0v.p, S.h_p0v.p, m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            CFA_CUDA(cudaMemcpyAsync(S.p0rp.p, S.h_p0rp.p, (m + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        }
         DevBuf<double>& d_p0v = S.p0v;
         DevBuf<int>& d_p0rp = S.p0rp;
-        CFA_CUDA(cudaMemcpyAsync(L.agg.p, agg, m * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-        CFA_CUDA(cudaMemcpyAsync(d_p0v.p, S.h_p0v.p, m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-        CFA_CUDA(cudaMemcpyAsync(d_p0rp.p, S.h_p0rp.p, (m + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
         phase(2);
         // AP0 = A P0, then P = P0 - omega D^-1 A P0
         DCsr& AP0 = S.AP0;

@@ -62,6 +62,9 @@ struct SetupScratch {
     DevBuf<long long> sg_off;
     DevBuf<double> sg_sval, pow_x, pow_y, pow_py, pow_px, pow_st, p0v, M, colbuf;
     DevBuf<unsigned char> strong;
+    DevBuf<int> ag_trp, ag_tci, ag_fill, ag_rank, ag_agg1, ag_agg2, ag_size, ag_flag;   // device aggregation
+    DevBuf<unsigned char> ag_state;
+    HostBuf<int> h_ag;                  // flag / totals read back by the aggregation rounds
     DevBuf<char> cub_tmp;
     HostBuf<int> h_rp, h_ci, h_cnt, h_ub, h_agg, h_p0rp;
     HostBuf<long long> h_off;

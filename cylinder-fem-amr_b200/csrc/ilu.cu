@@ -7,6 +7,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "ilu.cuh"
 
@@ -163,6 +164,434 @@ static void sweeps(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv, con
     }
 }
 
+// ---- sweeps for the momentum solve's pair of right-hand sides stored interleaved per row ----
+// r[i] = (u_i, v_i) as one double2, so a row's own and gathered accesses of both components are
+// one 16-byte (FP64) or 8-byte (FP32 work vector) load in one sector. Each colour kernel first
+// loads the data that do not change during a solve (its rows, their split-pattern offsets, the
+// first kIluBatch column indices and factor values, the diagonal), then waits for the previous
+// kernel (griddepcontrol.wait), so that with programmatic dependent launch these loads overlap
+// the previous colour's tail. With `early` set, each block also signals its dependents at once
+// (griddepcontrol.launch_dependents), so the next colour's blocks are scheduled, and do their
+// own loads, while this colour still runs. Those loads read only the factors and the pattern,
+// written before the solve began. Streamed data go through the evict-first path (__ldcs) when
+// `stream_hint` is set, so that the work vector stays in L2 across the colour kernels.
+template <class T> struct Pair;
+template <> struct Pair<float> { using type = float2; };
+template <> struct Pair<double> { using type = double2; };
+
+template <class X>
+__device__ __forceinline__ X ld_stream(const X* p, bool hint) { return hint ? __ldcs(p) : __ldg(p); }
+
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Forward sweep of one colour: y_i = r_i - sum_L l_ie y_e for both components (unit L); the last
+// colour also divides by u_ii and writes z. T: sweep arithmetic and work-vector precision (SEP:
+// w is a separate T work vector; otherwise w is z, FP64 in place).
+template <class V, class T, bool SEP>
+__global__ void __launch_bounds__(kThreads)
+k_ilu_lower_pair(int m, const int* __restrict__ rows, const int* __restrict__ lp, const int* __restrict__ lc,
+                 const V* __restrict__ lv, const V* __restrict__ dinv, int last, const double2* __restrict__ r,
+                 typename Pair<T>::type* __restrict__ w, double2* __restrict__ z, const int* __restrict__ done,
+                 int early, int hint) {
+    using T2 = typename Pair<T>::type;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = t < m;
+    int i = 0, b = 0, e = 0;
+    int j[kIluBatch];
+    V l[kIluBatch];
+    V d = V(0);
+    if (valid) {
+        i = ld_stream(rows + t, hint);
+        b = ld_stream(lp + t, hint);
+        e = ld_stream(lp + t + 1, hint);
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (b + u < e) {
+                j[u] = ld_stream(lc + b + u, hint);
+                l[u] = ld_stream(lv + b + u, hint);
+            }
+        if (last) d = ld_stream(dinv + t, hint);
+    }
+    if (early) pdl_launch_dependents();
+    CFA_GRID_DEP();
+    if (done && *done) return;
+    if (!valid) return;
+    const double2 rr = r[i];
+    T a0 = (T)rr.x, a1 = (T)rr.y;
+    {
+        T2 g[kIluBatch];
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (b + u < e) g[u] = w[j[u]];
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (b + u < e) {
+                a0 -= (T)l[u] * g[u].x;
+                a1 -= (T)l[u] * g[u].y;
+            }
+    }
+    for (int e0 = b + kIluBatch; e0 < e; e0 += kIluBatch) {
+        V lq[kIluBatch];
+        T2 g[kIluBatch];
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (e0 + u < e) {
+                lq[u] = ld_stream(lv + e0 + u, hint);
+                g[u] = w[ld_stream(lc + e0 + u, hint)];
+            }
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (e0 + u < e) {
+                a0 -= (T)lq[u] * g[u].x;
+                a1 -= (T)lq[u] * g[u].y;
+            }
+    }
+    if (last) {
+        a0 = a0 * (T)d;
+        a1 = a1 * (T)d;
+        if (SEP) z[i] = make_double2((double)a0, (double)a1);
+    }
+    T2 o;
+    o.x = a0;
+    o.y = a1;
+    w[i] = o;
+}
+
+// Backward sweep of one colour: z_i = (y_i - sum_U u_ie z_e) / u_ii, both components.
+template <class V, class T, bool SEP>
+__global__ void __launch_bounds__(kThreads)
+k_ilu_upper_pair(int m, const int* __restrict__ rows, const int* __restrict__ up, const int* __restrict__ uc,
+                 const V* __restrict__ uv, const V* __restrict__ dinv, typename Pair<T>::type* __restrict__ w,
+                 double2* __restrict__ z, const int* __restrict__ done, int early, int hint) {
+    using T2 = typename Pair<T>::type;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = t < m;
+    int i = 0, b = 0, e = 0;
+    int j[kIluBatch];
+    V q[kIluBatch];
+    V d = V(0);
+    if (valid) {
+        i = ld_stream(rows + t, hint);
+        b = ld_stream(up + t, hint);
+        e = ld_stream(up + t + 1, hint);
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (b + u < e) {
+                j[u] = ld_stream(uc + b + u, hint);
+                q[u] = ld_stream(uv + b + u, hint);
+            }
+        d = ld_stream(dinv + t, hint);
+    }
+    if (early) pdl_launch_dependents();
+    CFA_GRID_DEP();
+    if (done && *done) return;
+    if (!valid) return;
+    const T2 own = w[i];
+    T a0 = own.x, a1 = own.y;
+    {
+        T2 g[kIluBatch];
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (b + u < e) g[u] = w[j[u]];
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (b + u < e) {
+                a0 -= (T)q[u] * g[u].x;
+                a1 -= (T)q[u] * g[u].y;
+            }
+    }
+    for (int e0 = b + kIluBatch; e0 < e; e0 += kIluBatch) {
+        V qq[kIluBatch];
+        T2 g[kIluBatch];
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (e0 + u < e) {
+                qq[u] = ld_stream(uv + e0 + u, hint);
+                g[u] = w[ld_stream(uc + e0 + u, hint)];
+            }
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (e0 + u < e) {
+                a0 -= (T)qq[u] * g[u].x;
+                a1 -= (T)qq[u] * g[u].y;
+            }
+    }
+    a0 = a0 * (T)d;
+    a1 = a1 * (T)d;
+    T2 o;
+    o.x = a0;
+    o.y = a1;
+    w[i] = o;
+    if (SEP) z[i] = make_double2((double)a0, (double)a1);
+}
+
+// Runtime switches of the pair sweeps, read once: CFA_ILU_EARLY=0 drops the early dependent
+// launch, CFA_ILU_HINT=1 turns on the evict-first loads of the streamed factors (measured slower
+// on the c1 and c2 meshes), CFA_ILU_PERM=0 selects the natural-order sweeps below instead of the
+// colour-order ones.
+static int env_flag(const char* name, int def) {
+    const char* e = std::getenv(name);
+    return e ? (e[0] != '0') : def;
+}
+
+template <class V, class T, bool SEP>
+static void sweeps_pair(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv, const V* dinv,
+                        typename Pair<T>::type* w, const double2* r, double2* z, const int* done) {
+    static const int early = env_flag("CFA_ILU_EARLY", 1);
+    static const int hint = env_flag("CFA_ILU_HINT", 0);
+    for (int c = 0; c < h->nc; ++c) {
+        const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
+        if (m == 0) continue;
+        CFA_LAUNCH(ctx, (k_ilu_lower_pair<V, T, SEP>), ceil_div(m, kThreads), kThreads, 0, m, h->rows.p + cs,
+                   h->lp.p + cs, h->lc.p, lv, dinv + cs, c == h->nc - 1 ? 1 : 0, r, w, z, done, early, hint);
+    }
+    for (int c = h->nc - 2; c >= 0; --c) {
+        const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
+        if (m == 0) continue;
+        CFA_LAUNCH(ctx, (k_ilu_upper_pair<V, T, SEP>), ceil_div(m, kThreads), kThreads, 0, m, h->rows.p + cs,
+                   h->up.p + cs, h->uc.p, uv, dinv + cs, w, z, done, early, hint);
+    }
+}
+
+// ---- the same sweeps with the work vector in colour order ----
+// In the reference's natural row order the rows of one colour are scattered over the whole
+// vector, so every colour kernel touches most 32-byte sectors of r, w and z for a sixth of their
+// rows. Here the work vector w is held in colour order (position t = the row's place in `rows`):
+// the first kernel runs over the rows in natural order, reads r coalesced and puts each row's
+// pair at its colour position (colour 0 has no L entries: its forward sweep is this copy); the
+// colour kernels read and write their own rows of w contiguously and gather their neighbours
+// through column indices mapped to colour positions (lcp, ucp); the last kernel runs in natural
+// order again, does colour 0's backward step and writes z coalesced. The arithmetic is that of
+// k_ilu_lower_pair / k_ilu_upper_pair, entry for entry.
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+k_ilu_first_perm(int n, const int* __restrict__ pos, const double2* __restrict__ r, typename Pair<T>::type* __restrict__ w,
+                 const int* __restrict__ done, int early) {
+    using T2 = typename Pair<T>::type;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = i < n ? __ldg(pos + i) : 0;
+    if (early) pdl_launch_dependents();
+    CFA_GRID_DEP();
+    if (done && *done) return;
+    if (i >= n) return;
+    const double2 v = r[i];
+    T2 o;
+    o.x = (T)v.x;
+    o.y = (T)v.y;
+    w[t] = o;
+}
+
+// Forward sweep of colour c (positions cs .. cs + m): y_t = y_t - sum_L l_te y_e; the last
+// colour also divides by u_tt.
+template <class V, class T>
+__global__ void __launch_bounds__(kThreads)
+k_ilu_lower_perm(int m, int cs, const int* __restrict__ lp, const int* __restrict__ lcp, const V* __restrict__ lv,
+                 const V* __restrict__ dinv, int last, typename Pair<T>::type* __restrict__ w,
+                 const int* __restrict__ done, int early) {
+    using T2 = typename Pair<T>::type;
+    const int tl = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = tl < m;
+    const int t = cs + tl;
+    int b = 0, e = 0;
+    int j[kIluBatch];
+    V l[kIluBatch];
+    V d = V(0);
+    if (valid) {
+        b = __ldg(lp + t);
+        e = __ldg(lp + t + 1);
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (b + u < e) {
+                j[u] = __ldg(lcp + b + u);
+                l[u] = __ldg(lv + b + u);
+            }
+        if (last) d = __ldg(dinv + t);
+    }
+    if (early) pdl_launch_dependents();
+    CFA_GRID_DEP();
+    if (done && *done) return;
+    if (!valid) return;
+    const T2 own = w[t];
+    T a0 = own.x, a1 = own.y;
+    {
+        T2 g[kIluBatch];
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (b + u < e) g[u] = w[j[u]];
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (b + u < e) {
+                a0 -= (T)l[u] * g[u].x;
+                a1 -= (T)l[u] * g[u].y;
+            }
+    }
+    for (int e0 = b + kIluBatch; e0 < e; e0 += kIluBatch) {
+        V lq[kIluBatch];
+        T2 g[kIluBatch];
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (e0 + u < e) {
+                lq[u] = __ldg(lv + e0 + u);
+                g[u] = w[__ldg(lcp + e0 + u)];
+            }
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (e0 + u < e) {
+                a0 -= (T)lq[u] * g[u].x;
+                a1 -= (T)lq[u] * g[u].y;
+            }
+    }
+    if (last) {
+        a0 = a0 * (T)d;
+        a1 = a1 * (T)d;
+    }
+    T2 o;
+    o.x = a0;
+    o.y = a1;
+    w[t] = o;
+}
+
+// Backward step of row t: (y_t - sum_U u_te z_e) / u_tt, both components.
+template <class V, class T>
+__device__ __forceinline__ typename Pair<T>::type ilu_upper_row(int t, int b, int e, const int (&j)[kIluBatch],
+                                                               const V (&q)[kIluBatch], V d, const int* __restrict__ ucp,
+                                                               const V* __restrict__ uv,
+                                                               const typename Pair<T>::type* __restrict__ w) {
+    using T2 = typename Pair<T>::type;
+    const T2 own = w[t];
+    T a0 = own.x, a1 = own.y;
+    {
+        T2 g[kIluBatch];
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (b + u < e) g[u] = w[j[u]];
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (b + u < e) {
+                a0 -= (T)q[u] * g[u].x;
+                a1 -= (T)q[u] * g[u].y;
+            }
+    }
+    for (int e0 = b + kIluBatch; e0 < e; e0 += kIluBatch) {
+        V qq[kIluBatch];
+        T2 g[kIluBatch];
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (e0 + u < e) {
+                qq[u] = __ldg(uv + e0 + u);
+                g[u] = w[__ldg(ucp + e0 + u)];
+            }
+#pragma unroll
+        for (int u = 0; u < kIluBatch; ++u)
+            if (e0 + u < e) {
+                a0 -= (T)qq[u] * g[u].x;
+                a1 -= (T)qq[u] * g[u].y;
+            }
+    }
+    T2 o;
+    o.x = a0 * (T)d;
+    o.y = a1 * (T)d;
+    return o;
+}
+
+template <class V>
+__device__ __forceinline__ void ilu_upper_prefetch(int t, const int* __restrict__ up, const int* __restrict__ ucp,
+                                                   const V* __restrict__ uv, const V* __restrict__ dinv, int& b, int& e,
+                                                   int (&j)[kIluBatch], V (&q)[kIluBatch], V& d) {
+    b = __ldg(up + t);
+    e = __ldg(up + t + 1);
+#pragma unroll
+    for (int u = 0; u < kIluBatch; ++u)
+        if (b + u < e) {
+            j[u] = __ldg(ucp + b + u);
+            q[u] = __ldg(uv + b + u);
+        }
+    d = __ldg(dinv + t);
+}
+
+// Backward sweep of colour c >= 1 (positions cs .. cs + m), in place in w.
+template <class V, class T>
+__global__ void __launch_bounds__(kThreads)
+k_ilu_upper_perm(int m, int cs, const int* __restrict__ up, const int* __restrict__ ucp, const V* __restrict__ uv,
+                 const V* __restrict__ dinv, typename Pair<T>::type* __restrict__ w, const int* __restrict__ done,
+                 int early) {
+    const int tl = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = tl < m;
+    const int t = cs + tl;
+    int b = 0, e = 0;
+    int j[kIluBatch];
+    V q[kIluBatch];
+    V d = V(0);
+    if (valid) ilu_upper_prefetch(t, up, ucp, uv, dinv, b, e, j, q, d);
+    if (early) pdl_launch_dependents();
+    CFA_GRID_DEP();
+    if (done && *done) return;
+    if (!valid) return;
+    w[t] = ilu_upper_row<V, T>(t, b, e, j, q, d, ucp, uv, w);
+}
+
+// The last kernel, rows in natural order: colour 0's backward step (positions below c1) from w,
+// every other row's final value copied; z written coalesced in FP64.
+template <class V, class T>
+__global__ void __launch_bounds__(kThreads)
+k_ilu_last_perm(int n, int c1, const int* __restrict__ pos, const int* __restrict__ up, const int* __restrict__ ucp,
+                const V* __restrict__ uv, const V* __restrict__ dinv, const typename Pair<T>::type* __restrict__ w,
+                double2* __restrict__ z, const int* __restrict__ done) {
+    using T2 = typename Pair<T>::type;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const int t = valid ? __ldg(pos + i) : 0;
+    const bool c0 = valid && t < c1;
+    int b = 0, e = 0;
+    int j[kIluBatch];
+    V q[kIluBatch];
+    V d = V(0);
+    if (c0) ilu_upper_prefetch(t, up, ucp, uv, dinv, b, e, j, q, d);
+    CFA_GRID_DEP();
+    if (done && *done) return;
+    if (!valid) return;
+    const T2 o = c0 ? ilu_upper_row<V, T>(t, b, e, j, q, d, ucp, uv, w) : w[t];
+    z[i] = make_double2((double)o.x, (double)o.y);
+}
+
+template <class V, class T>
+static void sweeps_perm(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv, const V* dinv,
+                        typename Pair<T>::type* w, const double2* r, double2* z, const int* done) {
+    static const int early = env_flag("CFA_ILU_EARLY", 1);
+    const int n = h->n;
+    CFA_LAUNCH(ctx, (k_ilu_first_perm<T>), ceil_div(n, kThreads), kThreads, 0, n, (const int*)h->pos.p, r, w, done,
+               early);
+    for (int c = 1; c < h->nc; ++c) {
+        const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
+        if (m == 0) continue;
+        CFA_LAUNCH(ctx, (k_ilu_lower_perm<V, T>), ceil_div(m, kThreads), kThreads, 0, m, cs, (const int*)h->lp.p,
+                   (const int*)h->lcp.p, lv, dinv, c == h->nc - 1 ? 1 : 0, w, done, early);
+    }
+    for (int c = h->nc - 2; c >= 1; --c) {
+        const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
+        if (m == 0) continue;
+        CFA_LAUNCH(ctx, (k_ilu_upper_perm<V, T>), ceil_div(m, kThreads), kThreads, 0, m, cs, (const int*)h->up.p,
+                   (const int*)h->ucp.p, uv, dinv, w, done, early);
+    }
+    CFA_LAUNCH(ctx, (k_ilu_last_perm<V, T>), ceil_div(n, kThreads), kThreads, 0, n, h->colour_start[1],
+               (const int*)h->pos.p, (const int*)h->up.p, (const int*)h->ucp.p, uv, dinv,
+               (const typename Pair<T>::type*)w, z, done);
+}
+
+// pos[rows[t]] = t, and the split pattern's column indices as colour positions
+__global__ void k_ilu_positions(int n, const int* __restrict__ rows, int* __restrict__ pos) {
+    CFA_GRID_DEP();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) pos[rows[t]] = t;
+}
+
+__global__ void k_ilu_map_cols(int count, const int* __restrict__ cols, const int* __restrict__ pos,
+                               int* __restrict__ out) {
+    CFA_GRID_DEP();
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < count) out[e] = pos[cols[e]];
+}
+
 // Position of the mirrored entry (j, i) of every CSR entry (i, j) (binary search in row j);
 // err set when the pattern is not structurally symmetric.
 __global__ void k_mirror_positions(int n, const int* __restrict__ rp, const int* __restrict__ ci,
@@ -223,6 +652,30 @@ cfa_status ilu_apply(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z,
         // FP64: the sweeps work in place in z (as the reference)
         if (nrhs == 1) sweeps<double, double, 1>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, z, r, z, done);
         else sweeps<double, double, 2>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, z, r, z, done);
+    }
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+cfa_status ilu_apply_pair(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z, const int* done) {
+    const double2* r2 = reinterpret_cast<const double2*>(r);
+    double2* z2 = reinterpret_cast<double2*>(z);
+    static const int perm = env_flag("CFA_ILU_PERM", 1);
+    const bool colour_order = perm && h->nc >= 2;
+    if (h->precision == CFA_MIXED) {
+        // FP32 factors, FP32 sweeps on the handle's FP32 work vector; FP64 in and out
+        if (!h->work32.p || h->work32.cap < 2 * (size_t)h->n)
+            return set_error(ctx, CFA_BAD_ARG, "ILU handle without its FP32 work vector", __FILE__, __LINE__);
+        float2* w = reinterpret_cast<float2*>(h->work32.p);
+        if (colour_order) sweeps_perm<float, float>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r2, z2, done);
+        else sweeps_pair<float, float, true>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r2, z2, done);
+    } else if (colour_order) {
+        if (!h->work64.p || h->work64.cap < 2 * (size_t)h->n)
+            return set_error(ctx, CFA_BAD_ARG, "ILU handle without its FP64 work vector", __FILE__, __LINE__);
+        sweeps_perm<double, double>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p,
+                                    reinterpret_cast<double2*>(h->work64.p), r2, z2, done);
+    } else {
+        sweeps_pair<double, double, false>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, z2, r2, z2, done);
     }
     CFA_CHECK_LAUNCH();
     return CFA_OK;
@@ -383,6 +836,17 @@ static cfa_status ilu_pattern(cfa_ctx* ctx, cfa_ilu* h, int n, const int* rp, co
                (const int*)h->colour.p, (const int*)h->diag.p, (int*)nullptr, (int*)nullptr, (int*)nullptr,
                (const int*)h->lp.p, (const int*)h->up.p, (const int*)uo.p, h->lc.p, h->uc.p, h->l_src.p, h->u_src.p,
                h->d_src.p, h->elim.p, h->upd.p);
+    // colour positions of the rows and of the split pattern's columns (the colour-order sweeps)
+    CFA_CUDA(h->pos.ensure(n));
+    CFA_CUDA(h->lcp.ensure(std::max(h->nl, 1)));
+    CFA_CUDA(h->ucp.ensure(std::max(h->nu, 1)));
+    CFA_LAUNCH(ctx, k_ilu_positions, ceil_div(n, kThreads), kThreads, 0, n, (const int*)h->rows.p, h->pos.p);
+    if (h->nl > 0)
+        CFA_LAUNCH(ctx, k_ilu_map_cols, ceil_div(h->nl, kThreads), kThreads, 0, h->nl, (const int*)h->lc.p,
+                   (const int*)h->pos.p, h->lcp.p);
+    if (h->nu > 0)
+        CFA_LAUNCH(ctx, k_ilu_map_cols, ceil_div(h->nu, kThreads), kThreads, 0, h->nu, (const int*)h->uc.p,
+                   (const int*)h->pos.p, h->ucp.p);
     CFA_CUDA(h->lu.ensure(nnz));
     if (h->precision == CFA_MIXED) {
         CFA_CUDA(h->lv32.ensure(std::max(h->nl, 1)));
@@ -393,6 +857,7 @@ static cfa_status ilu_pattern(cfa_ctx* ctx, cfa_ilu* h, int n, const int* rp, co
         CFA_CUDA(h->lv64.ensure(std::max(h->nl, 1)));
         CFA_CUDA(h->uv64.ensure(std::max(h->nu, 1)));
         CFA_CUDA(h->dinv64.ensure(n));
+        CFA_CUDA(h->work64.ensure(2 * (size_t)n));
     }
     CFA_CHECK_LAUNCH();
     // the scratch buffers (cnt, uo, tmp) are released on return: wait for the kernels using them
@@ -513,6 +978,13 @@ cfa_status cfa_ilu_apply(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double
     CFA_ARG(h && r && z && (nrhs == 1 || nrhs == 2));
     CFA_ARG(r != z);
     return ilu_apply(ctx, h, r, z, nrhs, nullptr);
+}
+
+cfa_status cfa_ilu_apply_interleaved(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z) {
+    CFA_ENTER(ctx);
+    CFA_ARG(h && r && z && r != z);
+    CFA_ARG(((uintptr_t)r % 16) == 0 && ((uintptr_t)z % 16) == 0);
+    return ilu_apply_pair(ctx, h, r, z, nullptr);
 }
 
 cfa_status cfa_ilu_colours(const cfa_ilu* h, int* n_colours, int* colour_start) {

@@ -17,7 +17,9 @@ struct cfa_ilu {
     cfa::DevBuf<double> lu;           // FP64 factor on the CSR pattern
     cfa::DevBuf<double> lv64, uv64, dinv64;
     cfa::DevBuf<float> lv32, uv32, dinv32;
-    cfa::DevBuf<float> work32;        // FP32 sweep vectors (mixed precision), nrhs * n
+    cfa::DevBuf<float> work32;        // FP32 sweep work vector of the interleaved pair (mixed), 2 n
+    cfa::DevBuf<double> work64;       // FP64 work vector of the colour-order pair sweeps, 2 n
+    cfa::DevBuf<int> pos, lcp, ucp;   // colour position of each row; lc / uc as colour positions
     // symbolic factorization (elimination program), rows in colour order:
     // elim[ep[t] .. ep[t+1]) = {local index q of l_ik in row i, CSR position of u_kk, first update},
     // upd[elim.ub .. next.ub) = {local index b in row i, CSR position m in row k}: a_ib -= l_ik lu_m
@@ -35,4 +37,8 @@ namespace cfa {
 // handle. `done` (nullable): device flag, the sweep kernels return at once when it is set and
 // `active` (nullable, 2 ints) masks components (inactive: z left unchanged).
 cfa_status ilu_apply(cfa_ctx* ctx, const cfa_ilu* ilu, const double* r, double* z, int nrhs, const int* done);
+// z = (LU)^-1 r for the two components of the momentum solve stored interleaved per row
+// (r[2i], r[2i + 1] = u_i, v_i; 16-byte aligned): FP64 handles sweep in FP64 in place in z, mixed
+// handles sweep in FP32 on the handle's FP32 work vector. FP64 in and out.
+cfa_status ilu_apply_pair(cfa_ctx* ctx, const cfa_ilu* ilu, const double* r, double* z, const int* done);
 }  // namespace cfa

@@ -303,12 +303,15 @@ __global__ void __launch_bounds__(kTileThreads)
 k_opt_b(TileView tv, const double* __restrict__ inv_m, const double* __restrict__ z, const double* __restrict__ p,
         const double* __restrict__ beta_ptr, double* __restrict__ p_new, double* __restrict__ gx,
         double* __restrict__ gy, const int* __restrict__ done) {
-    CFA_GRID_DEP();
-    if (done && *done) return;
     extern __shared__ __align__(128) unsigned char tsmem[];
     const bool fuse = beta_ptr != nullptr;
-    const double beta = fuse ? *beta_ptr : 0.0;
-    tile_loop(tv, tsmem, [&](int, int r0, int nr, const unsigned char* ch) {
+    double beta = 0.0;
+    // the tiles are packed at the start of the solve, ahead of at least one other kernel
+    tile_loop_dep(tv, tsmem, [&] {
+        if (done && *done) return false;
+        if (fuse) beta = *beta_ptr;
+        return true;
+    }, [&](int, int r0, int nr, const unsigned char* ch) {
         const int* rr = reinterpret_cast<const int*>(ch);
         const int ne = rr[nr];
         const int* cs = reinterpret_cast<const int*>(ch + tile_ci_off(nr));
@@ -368,14 +371,17 @@ k_opt_k(TileView tv, const int* __restrict__ tag, OutletBc bc, const double* __r
         const double* __restrict__ p, const double* __restrict__ beta_ptr, double* __restrict__ pn_buf,
         const double* __restrict__ gx, const double* __restrict__ gy, double* __restrict__ q, CgState* __restrict__ st,
         double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond, const int* __restrict__ done) {
-    CFA_GRID_DEP();
-    if (done && *done) return;
     extern __shared__ __align__(128) unsigned char tsmem[];
     __shared__ double sh[kWarps];
     const bool fuse = FUSEP && beta_ptr != nullptr;
-    const double beta = fuse ? *beta_ptr : 0.0;
+    double beta = 0.0;
     double acc = 0.0;
-    tile_loop(tv, tsmem, [&](int, int r0, int nr, const unsigned char* ch) {
+    // the tiles are packed at the start of the solve, ahead of at least one other kernel
+    const bool go = tile_loop_dep(tv, tsmem, [&] {
+        if (done && *done) return false;
+        if (fuse) beta = *beta_ptr;
+        return true;
+    }, [&](int, int r0, int nr, const unsigned char* ch) {
         const int* rr = reinterpret_cast<const int*>(ch);
         const int ne = rr[nr];
         const int* cs = reinterpret_cast<const int*>(ch + tile_ci_off(nr));
@@ -437,7 +443,7 @@ k_opt_k(TileView tv, const int* __restrict__ tag, OutletBc bc, const double* __r
             }
         }
     });
-    if (!DOT) return;
+    if (!go || !DOT) return;
     double v[1] = {acc};
     block_sum<1>(v, sh);
     if (publish_partials<1>(v, part, counter)) {
@@ -676,13 +682,17 @@ __device__ __forceinline__ void b2_begin_iteration(B2State* st, CondArg cond) {
     if (!(st->active[0] || st->active[1])) { st->done = 1; set_cond(cond, 0); }
 }
 
-// v = A x (x = [x_u | x_v] given as two pointers), r = b - v, r0 = p = r, v = 0, ||r|| (:681-697)
+// The solver's vectors hold the two components interleaved per row: r[i] = (u_i, v_i) as one
+// double2 (the reference keeps [u | v] with stride n, linalg.cuh:666-669). Each row's pair is one
+// 16-byte access, and the SpMV gathers both components of a neighbour with one load.
+//
+// v = A x (x given as the caller's two arrays), r = b - v, r0 = p = r, v = 0, ||r|| (:681-697)
 template <int TPR>
 __global__ void __launch_bounds__(kThreads)
 k_b2_init(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
           const double* __restrict__ xu, const double* __restrict__ xv, const double* __restrict__ bu,
-          const double* __restrict__ bv, double* __restrict__ r, double* __restrict__ r0, double* __restrict__ p,
-          double* __restrict__ vv, B2State* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter,
+          const double* __restrict__ bv, double2* __restrict__ r, double2* __restrict__ r0, double2* __restrict__ p,
+          double2* __restrict__ vv, B2State* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter,
           CondArg cond) {
     CFA_GRID_DEP();
     __shared__ double sh[2 * kWarps];
@@ -700,10 +710,11 @@ k_b2_init(int n, const int* __restrict__ rp, const int* __restrict__ ci, const d
     sv = group_reduce<TPR>(sv);
     if (valid && lane == 0) {
         const double ru = bu[row] - 1.0 * su, rv = bv[row] - 1.0 * sv;
-        r[row] = ru; r[n + row] = rv;
-        r0[row] = ru; r0[n + row] = rv;
-        p[row] = ru; p[n + row] = rv;
-        vv[row] = 0.0; vv[n + row] = 0.0;
+        const double2 rr = make_double2(ru, rv);
+        r[row] = rr;
+        r0[row] = rr;
+        p[row] = rr;
+        vv[row] = make_double2(0.0, 0.0);
         acc[0] += ru * ru;
         acc[1] += rv * rv;
     }
@@ -729,14 +740,17 @@ k_b2_init(int n, const int* __restrict__ rp, const int* __restrict__ ci, const d
 }
 
 // p = r + cb (p - co v) (k_bicg2_p)
-__global__ void k_b2_p(int n, const double* __restrict__ r, const double* __restrict__ v, double* __restrict__ p,
+__global__ void k_b2_p(int n, const double2* __restrict__ r, const double2* __restrict__ v, double2* __restrict__ p,
                        const B2State* __restrict__ st) {
     CFA_GRID_DEP();
     if (st->done) return;
     const double cb0 = st->cb[0], cb1 = st->cb[1], co0 = st->co[0], co1 = st->co[1];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * n; i += gridDim.x * blockDim.x) {
-        const int c = i >= n;
-        p[i] = r[i] + (c ? cb1 : cb0) * (p[i] - (c ? co1 : co0) * v[i]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double2 rr = r[i], vv = v[i];
+        double2 pp = p[i];
+        pp.x = rr.x + cb0 * (pp.x - co0 * vv.x);
+        pp.y = rr.y + cb1 * (pp.y - co1 * vv.y);
+        p[i] = pp;
     }
 }
 
@@ -744,7 +758,7 @@ __global__ void k_b2_p(int n, const double* __restrict__ r, const double* __rest
 template <int TPR>
 __global__ void __launch_bounds__(kThreads)
 k_b2_v(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
-       const double* __restrict__ phat, const double* __restrict__ r0, double* __restrict__ vv, B2State* __restrict__ st,
+       const double2* __restrict__ phat, const double2* __restrict__ r0, double2* __restrict__ vv, B2State* __restrict__ st,
        double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
     CFA_GRID_DEP();
     if (st->done) return;
@@ -756,16 +770,17 @@ k_b2_v(int n, const int* __restrict__ rp, const int* __restrict__ ci, const doub
         for (int k = rp[row] + lane; k < rp[row + 1]; k += TPR) {
             const double a = val[k];
             const int j = ci[k];
-            su += a * phat[j];
-            sv += a * phat[n + j];
+            const double2 g = phat[j];
+            su += a * g.x;
+            sv += a * g.y;
         }
     su = group_reduce<TPR>(su);
     sv = group_reduce<TPR>(sv);
     if (valid && lane == 0) {
-        vv[row] = su;
-        vv[n + row] = sv;
-        acc[0] += r0[row] * su;
-        acc[1] += r0[n + row] * sv;
+        vv[row] = make_double2(su, sv);
+        const double2 q = r0[row];
+        acc[0] += q.x * su;
+        acc[1] += q.y * sv;
     }
     ROWS_END
     block_sum<2>(acc, sh);
@@ -784,20 +799,22 @@ k_b2_v(int n, const int* __restrict__ rp, const int* __restrict__ ci, const doub
 }
 
 // s = r - ca v (k_bicg2_s)
-__global__ void k_b2_s(int n, const double* __restrict__ r, const double* __restrict__ v, double* __restrict__ s,
+__global__ void k_b2_s(int n, const double2* __restrict__ r, const double2* __restrict__ v, double2* __restrict__ s,
                        const B2State* __restrict__ st) {
     CFA_GRID_DEP();
     if (st->done) return;
     const double a0 = st->ca[0], a1 = st->ca[1];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * n; i += gridDim.x * blockDim.x)
-        s[i] = r[i] - (i >= n ? a1 : a0) * v[i];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double2 rr = r[i], vv = v[i];
+        s[i] = make_double2(rr.x - a0 * vv.x, rr.y - a1 * vv.y);
+    }
 }
 
 // t = A shat; s.s, t.t, t.s -> omega, s-stop (:723-736)
 template <int TPR>
 __global__ void __launch_bounds__(kThreads)
 k_b2_t(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
-       const double* __restrict__ shat, const double* __restrict__ s, double* __restrict__ t, B2State* __restrict__ st,
+       const double2* __restrict__ shat, const double2* __restrict__ s, double2* __restrict__ t, B2State* __restrict__ st,
        double* __restrict__ part, unsigned int* __restrict__ counter) {
     CFA_GRID_DEP();
     if (st->done) return;
@@ -809,15 +826,16 @@ k_b2_t(int n, const int* __restrict__ rp, const int* __restrict__ ci, const doub
         for (int k = rp[row] + lane; k < rp[row + 1]; k += TPR) {
             const double a = val[k];
             const int j = ci[k];
-            su += a * shat[j];
-            sv += a * shat[n + j];
+            const double2 g = shat[j];
+            su += a * g.x;
+            sv += a * g.y;
         }
     su = group_reduce<TPR>(su);
     sv = group_reduce<TPR>(sv);
     if (valid && lane == 0) {
-        t[row] = su;
-        t[n + row] = sv;
-        const double s0 = s[row], s1 = s[n + row];
+        t[row] = make_double2(su, sv);
+        const double2 sr = s[row];
+        const double s0 = sr.x, s1 = sr.y;
         acc[0] += s0 * s0; acc[1] += s1 * s1;
         acc[2] += su * su; acc[3] += sv * sv;
         acc[4] += su * s0; acc[5] += sv * s1;
@@ -845,9 +863,9 @@ k_b2_t(int n, const int* __restrict__ rp, const int* __restrict__ ci, const doub
 // x += a1 phat + a2 shat, r = s - cw t; r.r, r0.r -> stop tests, rho (:737-750); then the
 // start of the next iteration
 __global__ void __launch_bounds__(kThreads)
-k_b2_xr(int n, double* __restrict__ xu, double* __restrict__ xv, const double* __restrict__ phat,
-        const double* __restrict__ shat, const double* __restrict__ s, const double* __restrict__ t,
-        double* __restrict__ r, const double* __restrict__ r0, B2State* __restrict__ st, double* __restrict__ part,
+k_b2_xr(int n, double* __restrict__ xu, double* __restrict__ xv, const double2* __restrict__ phat,
+        const double2* __restrict__ shat, const double2* __restrict__ s, const double2* __restrict__ t,
+        double2* __restrict__ r, const double2* __restrict__ r0, B2State* __restrict__ st, double* __restrict__ part,
         unsigned int* __restrict__ counter, CondArg cond) {
     CFA_GRID_DEP();
     if (st->done) return;
@@ -855,13 +873,13 @@ k_b2_xr(int n, double* __restrict__ xu, double* __restrict__ xv, const double* _
     const double a10 = st->a1[0], a11 = st->a1[1], a20 = st->a2[0], a21 = st->a2[1], w0 = st->cw[0], w1 = st->cw[1];
     double acc[4] = {0, 0, 0, 0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        xu[i] += a10 * phat[i] + a20 * shat[i];
-        xv[i] += a11 * phat[n + i] + a21 * shat[n + i];
-        const double ru = s[i] - w0 * t[i], rv = s[n + i] - w1 * t[n + i];
-        r[i] = ru;
-        r[n + i] = rv;
+        const double2 ph = phat[i], sh2 = shat[i], ss = s[i], tt = t[i], q = r0[i];
+        xu[i] += a10 * ph.x + a20 * sh2.x;
+        xv[i] += a11 * ph.y + a21 * sh2.y;
+        const double ru = ss.x - w0 * tt.x, rv = ss.y - w1 * tt.y;
+        r[i] = make_double2(ru, rv);
         acc[0] += ru * ru; acc[1] += rv * rv;
-        acc[2] += r0[i] * ru; acc[3] += r0[n + i] * rv;
+        acc[2] += q.x * ru; acc[3] += q.y * rv;
     }
     block_sum<4>(acc, sh);
     if (publish_partials<4>(acc, part, counter)) {
@@ -897,20 +915,19 @@ k_b2_xr(int n, double* __restrict__ xu, double* __restrict__ xv, const double* _
 template <int TPR, int MODE>
 __global__ void __launch_bounds__(kTileThreads)
 k_b2t(TileView tv, int n, const double* __restrict__ xu, const double* __restrict__ xv, const double* __restrict__ bu,
-      const double* __restrict__ bv, const double* __restrict__ in, const double* __restrict__ aux,
-      double* __restrict__ out, double* __restrict__ r, double* __restrict__ r0, double* __restrict__ p,
+      const double* __restrict__ bv, const double2* __restrict__ in, const double2* __restrict__ aux,
+      double2* __restrict__ out, double2* __restrict__ r, double2* __restrict__ r0, double2* __restrict__ p,
       B2State* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
-    CFA_GRID_DEP();
-    if (MODE != 0 && st->done) return;
     extern __shared__ __align__(128) unsigned char tsmem[];
     constexpr int NV = MODE == 2 ? 6 : 2;
     __shared__ double sh[NV * kWarps];
     double acc[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[q] = 0.0;
-    const double* x0 = MODE == 0 ? xu : in;
-    const double* x1 = MODE == 0 ? xv : in + n;
-    tile_loop(tv, tsmem, [&](int, int r0_, int nr, const unsigned char* ch) {
+    // the tiles are packed by the kernel just before MODE 0 (its first copies wait); MODES 1 and 2
+    // read them later in the solve
+    const bool go = tile_loop_dep<MODE != 0>(tv, tsmem, [&] { return MODE == 0 || !st->done; },
+                                             [&](int, int r0_, int nr, const unsigned char* ch) {
         const int* rr = reinterpret_cast<const int*>(ch);
         const int ne = rr[nr];
         const int* cs = reinterpret_cast<const int*>(ch + tile_ci_off(nr));
@@ -929,8 +946,14 @@ k_b2t(TileView tv, int n, const double* __restrict__ xu, const double* __restric
                         if (e < end) {
                             const int j = cs[e];
                             a[u] = av[e];
-                            g0[u] = x0[j];
-                            g1[u] = x1[j];
+                            if (MODE == 0) {
+                                g0[u] = xu[j];
+                                g1[u] = xv[j];
+                            } else {
+                                const double2 g = in[j];
+                                g0[u] = g.x;
+                                g1[u] = g.y;
+                            }
                         }
                     }
 #pragma unroll
@@ -947,21 +970,22 @@ k_b2t(TileView tv, int n, const double* __restrict__ xu, const double* __restric
                 const int row = r0_ + lr;
                 if (MODE == 0) {
                     const double ru = bu[row] - 1.0 * su, rv = bv[row] - 1.0 * sv;
-                    r[row] = ru; r[n + row] = rv;
-                    r0[row] = ru; r0[n + row] = rv;
-                    p[row] = ru; p[n + row] = rv;
-                    out[row] = 0.0; out[n + row] = 0.0;
+                    const double2 rr = make_double2(ru, rv);
+                    r[row] = rr;
+                    r0[row] = rr;
+                    p[row] = rr;
+                    out[row] = make_double2(0.0, 0.0);
                     acc[0] += ru * ru;
                     acc[1] += rv * rv;
                 } else if (MODE == 1) {
-                    out[row] = su;
-                    out[n + row] = sv;
-                    acc[0] += aux[row] * su;
-                    acc[1] += aux[n + row] * sv;
+                    out[row] = make_double2(su, sv);
+                    const double2 q = aux[row];
+                    acc[0] += q.x * su;
+                    acc[1] += q.y * sv;
                 } else {
-                    out[row] = su;
-                    out[n + row] = sv;
-                    const double s0 = aux[row], s1 = aux[n + row];
+                    out[row] = make_double2(su, sv);
+                    const double2 sr = aux[row];
+                    const double s0 = sr.x, s1 = sr.y;
                     acc[0] += s0 * s0; acc[1] += s1 * s1;
                     acc[2 % NV] += su * su; acc[3 % NV] += sv * sv;
                     acc[4 % NV] += su * s0; acc[5 % NV] += sv * s1;
@@ -969,6 +993,7 @@ k_b2t(TileView tv, int n, const double* __restrict__ xu, const double* __restric
             }
         }
     });
+    if (!go) return;
     block_sum<NV>(acc, sh);
     if (!publish_partials<NV>(acc, part, counter)) return;
     reduce_partials<NV>(acc, part, counter, sh);
@@ -1337,6 +1362,7 @@ static cfa_status pack_operator(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a) {
                    kThreads, 0, nnz2, a.n, a.nnz, a.ci, a.val, a.oss->d_oss_val, m->tag, m->bc, a.oss->d_inv_m,
                    (const int*)W.rp2.p, (const int*)W.slot_row.p, (const int*)W.kpos.p, (const int*)W.pair_ptr.p,
                    (const int*)W.pa.p, (const int*)W.pf.p, W.tk.view(W.err.p), W.tk.data.p);
+        tile_fence(ctx);
     } else if (a.oss) {
         const double* o = a.oss->d_oss_val;
         const size_t nz = (size_t)a.nnz;
@@ -1721,6 +1747,10 @@ struct B2Args {
     double tol;
 };
 
+// the interleaved pair view of a work vector (2 n doubles, 16-byte aligned)
+static inline double2* pair(double* p) { return reinterpret_cast<double2*>(p); }
+static inline const double2* pair(const double* p) { return reinterpret_cast<const double2*>(p); }
+
 template <int MODE>
 static void launch_b2t(cfa_ctx* ctx, B2Work& W, const B2Args& a, const double* in, const double* aux, double* out,
                        CondArg cond) {
@@ -1728,8 +1758,8 @@ static void launch_b2t(cfa_ctx* ctx, B2Work& W, const B2Args& a, const double* i
     const TileLaunch L = tile_launch(ctx, W.tA, nullptr);
     TILE_TPR_SWITCH(W.tA.tpr,
         CFA_LAUNCH(ctx, (k_b2t<TPR, MODE>), L.grid, kTileThreads, L.smem, tv, a.n, (const double*)a.xu,
-                   (const double*)a.xv, a.bu, a.bv, in, aux, out, W.r.p, W.r0.p, W.p.p, W.st.p, W.part.p, W.counter.p,
-                   cond));
+                   (const double*)a.xv, a.bu, a.bv, pair(in), pair(aux), pair(out), pair(W.r.p), pair(W.r0.p),
+                   pair(W.p.p), W.st.p, W.part.p, W.counter.p, cond));
 }
 
 template <int TPR>
@@ -1775,8 +1805,8 @@ static cfa_status b2_init(cfa_ctx* ctx, B2Work& W, const B2Args& a, CondArg cond
     const int tpr = op_tpr(a.n, a.nnz);
     const int grid = row_grid(ctx, a.n, tpr);
     OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_init<TPR>), grid, kThreads, 0, a.n, a.rp, a.ci, a.val, (const double*)a.xu,
-                                  (const double*)a.xv, a.bu, a.bv, W.r.p, W.r0.p, W.p.p, W.v.p, W.st.p, W.part.p,
-                                  W.counter.p, cond));
+                                  (const double*)a.xv, a.bu, a.bv, pair(W.r.p), pair(W.r0.p), pair(W.p.p),
+                                  pair(W.v.p), W.st.p, W.part.p, W.counter.p, cond));
     CFA_CHECK_LAUNCH();
     return CFA_OK;
 }
@@ -1785,22 +1815,22 @@ static cfa_status b2_body(cfa_ctx* ctx, B2Work& W, const B2Args& a, CondArg cond
     const int n = a.n;
     const int tpr = op_tpr(a.n, a.nnz);
     const int grid = row_grid(ctx, n, tpr);
-    const int gv = row_grid(ctx, 2LL * n, 1);
+    const int gv = row_grid(ctx, n, 1);
     const int* done = &W.st.p->done;
-    CFA_LAUNCH(ctx, k_b2_p, gv, kThreads, 0, n, W.r.p, W.v.p, W.p.p, W.st.p);
-    CFA_PROPAGATE(ilu_apply(ctx, a.ilu, W.p.p, W.phat.p, 2, done));
+    CFA_LAUNCH(ctx, k_b2_p, gv, kThreads, 0, n, pair(W.r.p), pair(W.v.p), pair(W.p.p), W.st.p);
+    CFA_PROPAGATE(ilu_apply_pair(ctx, a.ilu, W.p.p, W.phat.p, done));
     if (W.tiled) launch_b2t<1>(ctx, W, a, W.phat.p, W.r0.p, W.v.p, cond);
     else
-        OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_v<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, W.phat.p, W.r0.p,
-                                      W.v.p, W.st.p, W.part.p, W.counter.p, cond));
-    CFA_LAUNCH(ctx, k_b2_s, gv, kThreads, 0, n, W.r.p, W.v.p, W.s.p, W.st.p);
-    CFA_PROPAGATE(ilu_apply(ctx, a.ilu, W.s.p, W.shat.p, 2, done));
+        OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_v<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, pair(W.phat.p),
+                                      pair(W.r0.p), pair(W.v.p), W.st.p, W.part.p, W.counter.p, cond));
+    CFA_LAUNCH(ctx, k_b2_s, gv, kThreads, 0, n, pair(W.r.p), pair(W.v.p), pair(W.s.p), W.st.p);
+    CFA_PROPAGATE(ilu_apply_pair(ctx, a.ilu, W.s.p, W.shat.p, done));
     if (W.tiled) launch_b2t<2>(ctx, W, a, W.shat.p, W.s.p, W.t.p, cond);
     else
-        OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_t<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, W.shat.p, W.s.p,
-                                      W.t.p, W.st.p, W.part.p, W.counter.p));
-    CFA_LAUNCH(ctx, k_b2_xr, row_grid(ctx, n, 1), kThreads, 0, n, a.xu, a.xv, W.phat.p, W.shat.p, W.s.p, W.t.p, W.r.p,
-               W.r0.p, W.st.p, W.part.p, W.counter.p, cond);
+        OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_t<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, pair(W.shat.p),
+                                      pair(W.s.p), pair(W.t.p), W.st.p, W.part.p, W.counter.p));
+    CFA_LAUNCH(ctx, k_b2_xr, row_grid(ctx, n, 1), kThreads, 0, n, a.xu, a.xv, pair(W.phat.p), pair(W.shat.p),
+               pair(W.s.p), pair(W.t.p), pair(W.r.p), pair(W.r0.p), W.st.p, W.part.p, W.counter.p, cond);
     CFA_CHECK_LAUNCH();
     return CFA_OK;
 }

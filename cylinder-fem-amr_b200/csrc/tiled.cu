@@ -3,9 +3,20 @@
 #include <mutex>
 #include <unordered_map>
 
+#include <cstdlib>
+
 #include "tiled.cuh"
 
 namespace cfa {
+
+bool tile_early_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("CFA_TILE_EARLY");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 
 __global__ void k_pack_tiles(int ntiles, const long long* __restrict__ off, const int* __restrict__ row0,
                              const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v0,
@@ -94,9 +105,17 @@ cfa_status pack_tiled(cfa_ctx* ctx, const int* d_rp, const int* d_ci, const doub
     const int grid = std::min(T.ntiles, 16 * ctx->num_sms);
     CFA_LAUNCH(ctx, k_pack_tiles, grid, kTileThreads, 0, T.ntiles, (const long long*)T.off.p, (const int*)T.row0.p,
                d_rp, d_ci, v0, v1, v2, T.nvals, T.vbytes, T.data.p);
+    tile_fence(ctx);
     CFA_CHECK_LAUNCH();
     return CFA_OK;
 }
+
+// Waits for the previous kernel and ends: a kernel launched after it can start (and read tiles
+// before its own griddepcontrol.wait) only once every block of this one has passed its wait, so
+// whatever the kernels before this one wrote is complete and visible to it.
+__global__ void k_tile_fence() { CFA_GRID_DEP(); }
+
+void tile_fence(cfa_ctx* ctx) { launch(ctx, k_tile_fence, 1, 32, 0); }
 
 void allow_tile_kernel(const void* kernel) {
     static std::mutex mu;

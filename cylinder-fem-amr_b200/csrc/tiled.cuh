@@ -38,7 +38,13 @@ struct TileView {
     int tile_rows = 0;                // rows of every tile but the last (tile t starts at t * tile_rows)
     int max_chunk = 0;                // bytes
     int* err = nullptr;               // device error word (timeout)
+    int early = 0;                    // signal dependents as soon as the first copies are issued
 };
+
+// Tile kernels signal their dependent launch (griddepcontrol.launch_dependents) right after
+// issuing their first tile copies, so the next kernel's blocks are scheduled and issue their own
+// first copies while this kernel runs (c1 step 15.72 -> 15.11 ms); CFA_TILE_EARLY=0 turns it off.
+bool tile_early_enabled();
 
 // Host-side description + device buffers of a tiled matrix.
 struct TiledCsr {
@@ -53,6 +59,7 @@ struct TiledCsr {
         TileView v;
         v.data = data.p; v.off = off.p; v.row0 = row0.p; v.ntiles = ntiles; v.rows = rows;
         v.nvals = nvals; v.vbytes = vbytes; v.max_chunk = max_chunk; v.err = err; v.tile_rows = tile_rows;
+        v.early = tile_early_enabled() ? 1 : 0;
         return v;
     }
 };
@@ -73,7 +80,9 @@ __host__ __device__ inline long long tile_bytes(int nr, int ne, int nvals, int v
 cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T);
 
 // Packs pattern + values (FP64 sources; converted to float when vbytes == 4) into T.
-// A NULL source leaves its value section to be filled by its producer. Asynchronous.
+// A NULL source leaves its value section to be filled by its producer. Asynchronous; ends with
+// tile_fence, so the next kernel may read the tiles before its griddepcontrol.wait.
+// Kernels that write tile values themselves (a producer) must be followed by tile_fence too.
 cfa_status pack_tiled(cfa_ctx* ctx, const int* d_rp, const int* d_ci, const double* v0, const double* v1,
                       const double* v2, TiledCsr& T);
 
@@ -186,6 +195,84 @@ __device__ __forceinline__ bool tile_loop(const TileView& tv, unsigned char* sme
     }
     return true;
 }
+
+// tile_loop for a kernel launched as a programmatic dependent of the previous kernel, which
+// replaces the kernel's own griddepcontrol.wait at entry. With PRE, the tiles must hold a matrix
+// that no kernel still running or just finished has written (written before the previous
+// kernel started: every kernel of this library waits for its predecessor before it ends), so the
+// first kTileStages - 1 copies are issued BEFORE griddepcontrol.wait and their latency overlaps
+// the end of the previous kernel; without PRE they are issued after it (tiles packed by the
+// kernel just before). After the wait every thread evaluates gate() (it may read what earlier
+// kernels wrote, e.g. a stop flag or a scalar, and must give the same answer in every thread);
+// if it is false the copies already issued are waited for (bounded) and false is returned
+// without running the body. The kernel must not touch memory that earlier kernels write before
+// this call.
+template <bool PRE = true, class Gate, class Body>
+__device__ __forceinline__ bool tile_loop_dep(const TileView& tv, unsigned char* smem, Gate&& gate, Body&& body) {
+    constexpr int S = kTileStages;
+    __shared__ uint64_t bar[S];
+    __shared__ int abort_flag;
+    const long long stride = align16(tv.max_chunk);
+    const int t0 = blockIdx.x;
+    auto issue_first = [&] {
+#pragma unroll
+        for (int k = 0; k < S - 1; ++k) {
+            const int t = t0 + k * (int)gridDim.x;
+            if (t < tv.ntiles) tile_issue(tv, t, smem + k * stride, &bar[k]);
+        }
+    };
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < S; ++k) mbar_init(&bar[k], 1);
+        mbar_fence_init();
+        abort_flag = 0;
+        if (PRE) issue_first();
+    }
+    if (PRE && tv.early) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    CFA_GRID_DEP();
+    __syncthreads();
+    const bool go = gate();
+    if (!PRE && go && threadIdx.x == 0) issue_first();
+    if (!go) {
+        if (threadIdx.x == 0)
+            for (int k = 0; k < S - 1; ++k)
+                if (t0 + k * (int)gridDim.x < tv.ntiles) mbar_wait(&bar[k], 0u);
+        return false;
+    }
+    if (t0 >= tv.ntiles) return true;
+    unsigned phase = 0u;   // bit k: parity of the next completion of stage k
+    int s = 0;             // stage of tile t
+    for (int t = t0; t < tv.ntiles; t += gridDim.x) {
+        const int sn = s == 0 ? S - 1 : s - 1;
+        const int tn = t + (S - 1) * (int)gridDim.x;
+        if (threadIdx.x == 0 && tn < tv.ntiles) {
+            fence_proxy_async();
+            tile_issue(tv, tn, smem + sn * stride, &bar[sn]);
+        }
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar[s], (phase >> s) & 1u));
+        if (!ok) {
+            if ((threadIdx.x & 31) == 0) atomicExch(tv.err, (int)CFA_TIMEOUT);
+            abort_flag = 1;
+        } else {
+            const int r0 = t * tv.tile_rows;
+            body(t, r0, min(tv.tile_rows, tv.rows - r0), smem + s * stride);
+        }
+        __syncthreads();
+        if (abort_flag) {
+            for (int k = 0; k < S; ++k) {
+                const int sk = (s + k) % S;
+                if (t + k * (int)gridDim.x < tv.ntiles) mbar_wait(&bar[sk], (phase >> sk) & 1u);
+            }
+            return true;
+        }
+        phase ^= 1u << s;
+        s = s + 1 == S ? 0 : s + 1;
+    }
+    return true;
+}
+
+// One-block kernel that only waits for the previous kernel (see tile_loop_dep).
+void tile_fence(cfa_ctx* ctx);
 
 // Launch shape of a tile kernel: persistent grid limited by shared memory (kTileStages tiles).
 struct TileLaunch {

@@ -316,6 +316,15 @@ cfa_status cfa_ilu_set_pattern(cfa_ctx* ctx, cfa_ilu* ilu, int n, const int* h_r
 cfa_status cfa_ilu_factor(cfa_ctx* ctx, cfa_ilu* ilu, const double* d_val);
 /* apply (:544-555): z = (LU)^-1 r for nrhs vectors of stride n. */
 cfa_status cfa_ilu_apply(cfa_ctx* ctx, const cfa_ilu* ilu, const double* d_r, double* d_z, int nrhs);
+/* z = (LU)^-1 r for two right-hand sides stored interleaved per row: d_r[2i] and d_r[2i + 1] are
+ * the first and second right-hand side's entries of row i (d_r, d_z: 2n doubles, 16-byte
+ * aligned, distinct). No counterpart in the reference, whose apply takes the two with stride n
+ * (MulticolourIlu0::apply, src/cfa/linalg.cuh:544-555); this is the layout this library's
+ * BiCGSTAB2 keeps its vectors in, and these are the sweeps it runs. FP64 handles sweep in FP64
+ * (the same operations as cfa_ilu_apply with nrhs = 2); mixed-precision handles sweep in FP32
+ * arithmetic on an FP32 work vector held by the handle (d_r rounded to FP32 once, d_z the FP32
+ * result widened). Calls on one handle must not overlap on the GPU (the work vector). */
+cfa_status cfa_ilu_apply_interleaved(cfa_ctx* ctx, const cfa_ilu* ilu, const double* d_r, double* d_z);
 /* Adjoint support (no counterpart in the reference): factors d_val as cfa_ilu_factor does and
  * keeps (LU)^T in the handle, so that cfa_ilu_apply gives z = (LU)^-T r and the handle
  * preconditions A^T (in the same colour order: (LU)^T = (U^T D^-1)(D L^T)). Needs a structurally

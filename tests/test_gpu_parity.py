@@ -207,6 +207,14 @@ def test_ilu_colouring_factor_apply(ctx, precision):
     zo = oi.apply(b, nrhs=2)
     tol = 1e-12 if precision == cfa.FP64 else 1e-5
     assert np.abs(host(z) - zo).max() <= tol * np.abs(zo).max()
+    # the momentum solve's sweeps: both right-hand sides interleaved per row (FP64: the same
+    # operations as the stacked sweeps; mixed: FP32 arithmetic on an FP32 work vector)
+    zi = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
+    ilu.apply_interleaved(dev(np.stack([b[:n], b[n:]], 1).ravel()), zi)
+    got = host(zi).reshape(n, 2).T.ravel()
+    if precision == cfa.FP64:
+        assert np.array_equal(got, host(z))
+    assert np.abs(got - zo).max() <= tol * np.abs(zo).max()
 
 
 @pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
@@ -339,8 +347,12 @@ def check_hierarchy(amg, oa):
     assert np.array_equal(host(amg.coarse_inverse()), inv)
 
 
-@pytest.mark.parametrize("name,which", [("small", "lap"), ("medium", "lap"), ("medium", "ppe")])
+@pytest.mark.parametrize("name,which", [("small", "lap"), ("medium", "lap"), ("medium", "ppe"), ("c0", "ppe"),
+                                        ("c1", "ppe")])
 def test_amg_setup_bit_exact(ctx, name, which):
+    """The device setup (strength, the aggregation rounds, smoothing, transpose, Galerkin SpGEMM,
+    coarse inverse) against the oracle's sequential host setup, bit for bit, up to the ~400k-node
+    adaptive mesh."""
     m = mesh(name)
     rp, ci = O.csr_build(m.n, m.elem_v)
     if which == "lap":
