@@ -4,9 +4,12 @@
 
 with respect to a per-node viscosity field of the momentum equation and the inflow amplitude U,
 for the loop of ``step.TimeStepper`` (the rotational pressure update takes the scalar viscosity,
-as do the OSS weights). With the OSS pressure stabilisation (stab > 0) the pressure operator is
-(1 + s_K) K - B^T M^-1 B with weights s_K of u*, and its right-hand side carries the OSS terms of
-p^n; their derivatives go through cfa_oss_adjoint.
+as do the OSS weights). Either outlet rule: p = 0 on the outlet (the default), or
+``outlet_dirichlet``, the scaled inflow parabola there and the pressure increment pinned at one
+node, whose right-hand side mean removal cfa_ppe_rhs_adjoint transposes. With the OSS pressure
+stabilisation (stab > 0) the pressure operator is (1 + s_K) K - B^T M^-1 B with weights s_K of u*,
+and its right-hand side carries the OSS terms of p^n; their derivatives go through
+cfa_oss_adjoint.
 
 Every solve's backward is the transposed solve: the pressure operator acts symmetrically on the
 rows that are not Dirichlet (the adjoint right-hand side is zeroed on the Dirichlet rows, whose
@@ -31,7 +34,7 @@ import cfa_b200 as cfa
 class DragAdjoint:
     def __init__(self, mesh, u0, v0, p0, nu_node, u_max=1.5, steps=10, dt=5e-3, nu=1e-3, rho=1.0, tau_time=1e-3,
                  H=1.0, u_mean=1.0, diameter=0.2, precision=cfa.MIXED, tol=1e-12, checkpoint=20, ctx=None,
-                 direct=False, stab=0.0):
+                 direct=False, stab=0.0, outlet_dirichlet=False):
         import torch
         self.torch = torch
         self.ctx = ctx or cfa.default_context()
@@ -55,7 +58,16 @@ class DragAdjoint:
         self.oss_val, self.inv_m = z(4 * nnz), z(n)
         self.oss = cfa.oss_operator(self.dm, self.oss_val, self.inv_m) if self.stab > 0.0 else None
         tag = np.ascontiguousarray(mesh.tag)
-        self.non_dirichlet = t((tag != 2).astype(np.float64))   # BC_OUTLET: p = 0 (the default outlet)
+        if outlet_dirichlet:
+            # the application's --outlet dirichlet: the scaled inflow parabola at the outlet and the
+            # pressure increment pinned at one outlet node (its only Dirichlet row)
+            pin, scale = cfa.pinned_outlet(mesh.x, mesh.y, tag, H)
+            self.dm.set_outlet(1, pin, scale)
+            nd = np.ones(n)
+            nd[pin] = 0.0
+        else:
+            nd = (tag != cfa.BC_OUTLET).astype(np.float64)   # p = 0 on the outlet (the default)
+        self.non_dirichlet = t(nd)
         rp, ci = self.dm.host_pattern()
         self.rp_h, self.ci_h = rp, ci
         self.ilu = cfa.MulticolourIlu0(self.ctx, precision)

@@ -166,6 +166,34 @@ def csr_build(ctx: Context, n: int, d_elem_v):
     return rp, ci
 
 
+# node tags (src/cfa/mesh.cuh:62-70)
+BC_INTERIOR, BC_INLET, BC_OUTLET, BC_WALL, BC_CYLINDER = 0, 1, 2, 3, 4
+
+
+def pinned_outlet(x, y, tag, H: float = 1.0):
+    """(pin, scale) of the application's ``--outlet dirichlet`` rule (src/cfa/device.cuh:153-171):
+    the pressure increment is pinned at the outlet node nearest mid-height, and the outlet
+    parabola is scaled by the ratio of the trapezoidal fluxes of the unit parabola through the
+    inlet and the outlet nodes (the corners y = 0, H counted with zero velocity)."""
+    import numpy as np
+    x, y, tag = np.asarray(x), np.asarray(y), np.asarray(tag)
+    out = np.flatnonzero(tag == BC_OUTLET)
+    if out.size == 0:
+        raise ValueError("pinned outlet: the mesh has no outlet node")
+    # first node of least distance in index order, as the application's strict '<' scan
+    pin = int(out[np.argmin(np.abs(y[out] - 0.5 * H))])
+
+    def flux(t):
+        ys = np.sort(np.concatenate([[0.0, H], y[tag == t]]))
+        prof = ys * (H - ys)
+        q = 0.0
+        for k in range(1, ys.size):
+            q += 0.5 * (ys[k] - ys[k - 1]) * (prof[k] + prof[k - 1])
+        return q
+
+    return pin, flux(BC_INLET) / flux(BC_OUTLET)
+
+
 class DeviceMesh:
     """The device mesh of DeviceMeshBuffers (src/cfa/device.cuh:21-59) plus the assembly plan."""
 
@@ -540,6 +568,12 @@ class AmgPreconditioner:
         lib().cfa_amg_coarse_inverse(self.h, C.byref(p))
         cn = self.coarse_n
         return _dev_view(p.value, cn * cn, torch.float64).reshape(cn, cn)
+
+    def composite(self):
+        """(level, rows) of the composite coarse operator, level -1 when there is none."""
+        lv, rows = C.c_int(), C.c_int()
+        lib().cfa_amg_composite(self.h, C.byref(lv), C.byref(rows), None)
+        return lv.value, rows.value
 
     def __del__(self):
         try:

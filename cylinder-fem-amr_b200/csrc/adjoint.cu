@@ -249,11 +249,14 @@ k_momentum_adjoint_scalars(int n, int ne, const int* __restrict__ tag, const dou
 __global__ void k_ppe_rhs_adjoint(int n, const int* __restrict__ ev, const double* __restrict__ x,
                                   const double* __restrict__ y, const int* __restrict__ tag, OutletBc bc,
                                   const int* __restrict__ inc_ptr, const int* __restrict__ inc,
-                                  const double* __restrict__ lam_p, double c, double* __restrict__ g_u,
-                                  double* __restrict__ g_v) {
+                                  const double* __restrict__ lam_p, const double* __restrict__ mean2, double c,
+                                  double* __restrict__ g_u, double* __restrict__ g_v) {
     CFA_GRID_DEP();
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
+    // with the pinned outlet every row's right-hand side enters the mean removal: the adjoint of
+    // the raw right-hand side is l - (m.l / sum m) on every row, l = lambda zeroed at the pin
+    const double shift = mean2 ? mean2[0] / mean2[1] : 0.0;
     double su = 0.0, sv = 0.0;
     for (int k = inc_ptr[j]; k < inc_ptr[j + 1]; ++k) {
         const int e = inc[k] >> 2, b = inc[k] & 3;
@@ -265,14 +268,37 @@ __global__ void k_ppe_rhs_adjoint(int n, const int* __restrict__ ev, const doubl
         const double dNdx[3] = {(y1 - y2) * inv2A, (y2 - y0) * inv2A, (y0 - y1) * inv2A};
         const double dNdy[3] = {(x2 - x1) * inv2A, (x0 - x2) * inv2A, (x1 - x0) * inv2A};
         double l = 0.0;
-        for (int a = 0; a < 3; ++a)
-            if (!pressure_dirichlet(nd[a], tag[nd[a]], bc)) l += lam_p[nd[a]];
+        for (int a = 0; a < 3; ++a) {
+            const bool dir = pressure_dirichlet(nd[a], tag[nd[a]], bc);
+            if (mean2) l += (dir ? 0.0 : lam_p[nd[a]]) - shift;
+            else if (!dir) l += lam_p[nd[a]];
+        }
         const double w = c * (area / 3.0) * l;
         su += w * dNdx[b];
         sv += w * dNdy[b];
     }
     g_u[j] += su;
     g_v[j] += sv;
+}
+
+// The pinned outlet's mean removal (k_sum / k_subtract_mean, src/cfa/fem_kernels.cuh:493-510)
+// transposed: out[0] = sum_i m_i l_i with l = lambda zeroed at the pin, out[1] = sum_i m_i, both in
+// a fixed order.
+__global__ void __launch_bounds__(kThreads)
+k_pin_mean(int n, int pin, const double* __restrict__ lam, const double* __restrict__ mass,
+           double* __restrict__ part, unsigned int* __restrict__ counter, double* __restrict__ out) {
+    CFA_GRID_DEP();
+    __shared__ double sh[2 * kWarps];
+    double v[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        v[0] += i == pin ? 0.0 : mass[i] * lam[i];
+        v[1] += mass[i];
+    }
+    block_sum<2>(v, sh);
+    if (publish_partials<2>(v, part, counter)) {
+        reduce_partials<2>(v, part, counter, sh);
+        if (threadIdx.x == 0) { out[0] = v[0]; out[1] = v[1]; }
+    }
 }
 
 // Projection (k_velocity_pressure_correction with the rotational term from the increment):
@@ -411,6 +437,8 @@ __global__ void k_forces_adjoint_nodes(int n, const int* __restrict__ inc_ptr, c
 // Per element: g_s = -dPhi/ds_K, mapped to u*, v* through ds_K/du*_j (the weight's formula,
 // differentiated by hand; the zero subgradient where |u-bar| = 0); per vertex: -dPhi/dq_j, the
 // p^n gradient. Five values per element: d/du and d/dv (equal for its three vertices), d/dp0..2.
+// With the pinned outlet the right-hand side's mean removal adds c Phi(1, p^n) (c = m.l / sum m),
+// which vanishes: the constant has no gradient, so Phi(1, .) = 0 and l zeroed at the pin suffices.
 __global__ void __launch_bounds__(kThreads)
 k_oss_adjoint_elems(int ne, const int* __restrict__ ev, const double* __restrict__ x, const double* __restrict__ y,
                     const double* __restrict__ us, const double* __restrict__ vs, const double* __restrict__ elem_s,
@@ -530,10 +558,23 @@ cfa_status cfa_ppe_rhs_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const double* la
                                double* g_u, double* g_v) {
     CFA_ENTER(ctx);
     CFA_ARG(m && lam_p && g_u && g_v && dt_proj > 0.0);
-    CFA_ARG(!m->bc.outlet_dirichlet);
+    const bool pinned = m->bc.outlet_dirichlet != 0;
+    CFA_ARG(!pinned || (m->bc.pin >= 0 && m->bc.pin < m->n));
+    DevBuf<double> buf;   // pinned outlet: lumped mass [n], the two sums
+    const double* mean2 = nullptr;
+    if (pinned) {
+        CFA_CUDA(buf.ensure((size_t)m->n + 2));
+        CFA_PROPAGATE(cfa_lumped_mass(ctx, m, buf.p));
+        const int grid = row_grid(ctx, m->n, 1);
+        CFA_PROPAGATE(ensure_partials(ctx, 2 * (size_t)grid + 2));
+        CFA_LAUNCH(ctx, k_pin_mean, grid, kThreads, 0, m->n, m->bc.pin, lam_p, (const double*)buf.p, ctx->d_part,
+                   ctx->d_counters, buf.p + m->n);
+        mean2 = buf.p + m->n;
+    }
     CFA_LAUNCH(ctx, k_ppe_rhs_adjoint, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->ev, m->x, m->y, m->tag, m->bc,
-               m->inc_ptr.p, m->inc.p, lam_p, -(rho / dt_proj), g_u, g_v);
+               m->inc_ptr.p, m->inc.p, lam_p, mean2, -(rho / dt_proj), g_u, g_v);
     CFA_CHECK_LAUNCH();
+    if (pinned) CFA_CUDA(cudaStreamSynchronize(ctx->stream));   // buf is released on return
     return CFA_OK;
 }
 
@@ -543,7 +584,7 @@ cfa_status cfa_oss_adjoint(cfa_ctx* ctx, const cfa_mesh* m, const double* u_star
                            double* g_p) {
     CFA_ENTER(ctx);
     CFA_ARG(m && u_star && v_star && elem_s && mass_lumped && lam_p && p_old && dp && g_u && g_v && g_p);
-    CFA_ARG(dt_proj > 0.0 && stab > 0.0 && !m->bc.outlet_dirichlet);
+    CFA_ARG(dt_proj > 0.0 && stab > 0.0);
     const int n = m->n, ne = m->ne;
     DevBuf<double> buf;   // l, q, G(l) x/y, G(q) x/y, per-element values
     CFA_CUDA(buf.ensure(6 * (size_t)n + 5 * (size_t)ne));

@@ -17,6 +17,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <functional>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
@@ -771,14 +772,78 @@ __global__ void k_vc_dense(int cn, const double* __restrict__ inv, const B* __re
 }
 
 // ---------------------------------------------------------------------------------------------
+// Composite coarse operator. The V-cycle below a small level is linear in that level's
+// right-hand side (damped Jacobi from a zero start, residual, restriction, the coarse solve,
+// prolongation), so it is one dense matrix M with M b = V-cycle(b). Setup forms M by running the
+// V-cycle's row operations on a block of right-hand sides (the identity); the V-cycle then applies
+// it with k_vc_dense, one launch in place of the levels' chain of dependent launches (about
+// seven per level). M equals the chain up to rounding (the products are summed in another order).
+// Blocks are row-major m x nb (row i, column c at [i * nb + c]), one thread per entry.
+// ---------------------------------------------------------------------------------------------
+enum BmOp { BM_PRE = 0, BM_JAC = 1, BM_RES = 2, BM_SPMV = 3, BM_ADD = 4 };
+
+template <int OP>
+__global__ void k_bm(int m, int nb, const int* __restrict__ rp, const int* __restrict__ ci,
+                     const double* __restrict__ val, const double* __restrict__ dinv, double omega, int jac,
+                     const double* __restrict__ B, const double* __restrict__ X, double* __restrict__ Y) {
+    CFA_GRID_DEP();
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)m * nb) return;
+    const int i = (int)(idx / nb), c = (int)(idx % nb);
+    double s = 0.0;
+    if (OP != BM_PRE || jac)
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+            const int j = ci[k];
+            s += val[k] * (OP == BM_PRE ? omega * dinv[j] * B[(size_t)j * nb + c] : X[(size_t)j * nb + c]);
+        }
+    const size_t o = (size_t)i * nb + c;
+    if (OP == BM_PRE) {
+        const double x0 = omega * dinv[i] * B[o];
+        Y[o] = jac ? x0 + omega * dinv[i] * (B[o] - s) : x0;
+    } else if (OP == BM_JAC) {
+        Y[o] = X[o] + omega * dinv[i] * (B[o] - s);
+    } else if (OP == BM_RES) {
+        Y[o] = B[o] - s;
+    } else if (OP == BM_SPMV) {
+        Y[o] = s;
+    } else {
+        Y[o] += s;
+    }
+}
+
+// X = inv B with the dense coarse inverse (cn x cn), blocks cn x nb
+__global__ void k_bm_dense(int cn, int nb, const double* __restrict__ inv, const double* __restrict__ B,
+                           double* __restrict__ X) {
+    CFA_GRID_DEP();
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)cn * nb) return;
+    const int i = (int)(idx / nb), c = (int)(idx % nb);
+    double s = 0.0;
+    for (int j = 0; j < cn; ++j) s += inv[(size_t)i * cn + j] * B[(size_t)j * nb + c];
+    X[(size_t)i * nb + c] = s;
+}
+
+// B = identity (nb x nb)
+__global__ void k_bm_eye(int nb, double* __restrict__ B) {
+    CFA_GRID_DEP();
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)nb * nb) return;
+    B[idx] = (idx / nb == idx % nb) ? 1.0 : 0.0;
+}
+
+// ---------------------------------------------------------------------------------------------
 // tile-streamed V-cycle kernel (tiled.cuh): one kernel for the five row operations
 // ---------------------------------------------------------------------------------------------
-enum VcOp { VC_PRE = 0, VC_JAC = 1, VC_RES = 2, VC_SPMV = 3, VC_ADD = 4 };
+// VC_RESTRICT (fused transfers): y = [R | -R A] [b ; x] over the next level's rows;
+// VC_ADDJAC: with x' = x + P xc, y = x' + omega D^-1 (b - A x'), x' never stored: sums of
+// [A | A P] and [I | P] over [x ; xc]. A column with the top bit set reads the second vector.
+enum VcOp { VC_PRE = 0, VC_JAC = 1, VC_RES = 2, VC_SPMV = 3, VC_ADD = 4, VC_RESTRICT = 5, VC_ADDJAC = 6 };
+constexpr int kSecondVec = (int)0x80000000u;
 
 template <int TPR, int OP, class V, class T, class B, class O, bool RZ = false>
 __global__ void __launch_bounds__(kTileThreads)
 k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b, const T* __restrict__ x,
-      O* __restrict__ y, const int* __restrict__ done, RzFuse rzf) {
+      O* __restrict__ y, const int* __restrict__ done, RzFuse rzf, const T* __restrict__ xc) {
     extern __shared__ __align__(128) unsigned char tsmem[];
     double dots[2] = {0.0, 0.0};   // RZ: this thread's rows of r.z and z.q
     // the level's tiles are packed at setup: their first copies go out before the wait
@@ -788,6 +853,7 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
         const int ne = rr[nr];
         const int* cs = reinterpret_cast<const int*>(ch + tile_ci_off(nr));
         const V* vv = reinterpret_cast<const V*>(ch + tile_val_off(nr, ne, (int)sizeof(V), 0));
+        const V* vv1 = reinterpret_cast<const V*>(ch + tile_val_off(nr, ne, (int)sizeof(V), 1));
         for (int base = 0; base < nr; base += kTileThreads / TPR) {
             const int lr = base + (int)threadIdx.x / TPR, lane = threadIdx.x % TPR;
             const bool valid = lr < nr;
@@ -795,17 +861,17 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
             // the row's own operands, loaded before the gathers so both round trips overlap
             T di = (T)0, bi = (T)0, xi = (T)0;
             if (valid && lane == 0) {
-                if (OP == VC_PRE || OP == VC_JAC) di = dinv[row];
-                if (OP == VC_PRE || OP == VC_JAC || OP == VC_RES) bi = (T)b[row];
+                if (OP == VC_PRE || OP == VC_JAC || OP == VC_ADDJAC) di = dinv[row];
+                if (OP == VC_PRE || OP == VC_JAC || OP == VC_RES || OP == VC_ADDJAC) bi = (T)b[row];
                 if (OP == VC_JAC) xi = x[row];
                 if (OP == VC_ADD) xi = (T)y[row];
             }
-            T s = (T)0;
+            T s = (T)0, s1 = (T)0;
             if (valid) {
                 const int end = rr[lr + 1];
                 for (int e0 = rr[lr] + lane; e0 < end; e0 += kGatherBatch * TPR) {
                     // all loads of the batch first, then the sums in entry order
-                    V a[kGatherBatch];
+                    V a[kGatherBatch], a1[kGatherBatch];
                     T g0[kGatherBatch];
                     B g1[kGatherBatch];
 #pragma unroll
@@ -815,6 +881,8 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
                             const int j = cs[e];
                             a[u] = vv[e];
                             if (OP == VC_PRE) { g0[u] = dinv[j]; g1[u] = b[j]; }
+                            else if (OP == VC_RESTRICT) g0[u] = j < 0 ? x[j & ~kSecondVec] : (T)b[j];
+                            else if (OP == VC_ADDJAC) { g0[u] = j < 0 ? xc[j & ~kSecondVec] : x[j]; a1[u] = vv1[e]; }
                             else g0[u] = x[j];
                         }
                     }
@@ -823,11 +891,16 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
                         if (e0 + u * TPR < end) {
                             if (OP == VC_PRE) s += (T)a[u] * (omega * g0[u] * (T)g1[u]);
                             else s += (T)a[u] * g0[u];
+                            if (OP == VC_ADDJAC) s1 += (T)a1[u] * g0[u];
                         }
                 }
             }
 #pragma unroll
             for (int o = TPR / 2; o > 0; o /= 2) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
+            if (OP == VC_ADDJAC) {
+#pragma unroll
+                for (int o = TPR / 2; o > 0; o /= 2) s1 += __shfl_down_sync(0xffffffffu, s1, o, TPR);
+            }
             if (valid && lane == 0) {
                 if (OP == VC_PRE) {
                     const T x0 = omega * di * bi;
@@ -842,8 +915,10 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
                     }
                 } else if (OP == VC_RES) {
                     y[row] = (O)(bi - s);
-                } else if (OP == VC_SPMV) {
+                } else if (OP == VC_SPMV || OP == VC_RESTRICT) {
                     y[row] = (O)s;
+                } else if (OP == VC_ADDJAC) {
+                    y[row] = (O)(s1 + omega * di * (bi - s));
                 } else {
                     y[row] = (O)(xi + s);
                 }
@@ -869,7 +944,7 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
 // rz: fold the CG's dots into this launch (the level-0 last sweep only).
 template <int OP, class V, class T, class B, class O>
 static void vct(cfa_ctx* ctx, bool dry, const TiledCsr& M, int* err, const T* dinv, T omega, const B* b, const T* x,
-                O* y, const int* done, const RzFuse* rz = nullptr) {
+                O* y, const int* done, const RzFuse* rz = nullptr, const T* xc = nullptr) {
     constexpr bool kRz = OP == VC_JAC && std::is_same<O, double>::value && std::is_same<B, double>::value;
     const int tpr = M.tpr;
     const TileView tv = M.view(err);
@@ -883,10 +958,10 @@ static void vct(cfa_ctx* ctx, bool dry, const TiledCsr& M, int* err, const T* di
             if (kRz) allow_tile_kernel((const void*)k_vct<N, OP, V, T, B, O, kRz>);                     \
         } else if (kRz && rz) {                                                                         \
             CFA_LAUNCH(ctx, (k_vct<N, OP, V, T, B, O, kRz>), L.grid, kTileThreads, L.smem, tv, dinv, omega, b, x, y, \
-                       done, *rz);                                                                      \
+                       done, *rz, xc);                                                                  \
         } else {                                                                                        \
             CFA_LAUNCH(ctx, (k_vct<N, OP, V, T, B, O>), L.grid, kTileThreads, L.smem, tv, dinv, omega, b, x, y, done, \
-                       none);                                                                           \
+                       none, xc);                                                                       \
         }                                                                                               \
         break;
         VCT_CASE(1) VCT_CASE(2) VCT_CASE(4) VCT_CASE(8) VCT_CASE(16)
@@ -960,7 +1035,11 @@ static void vcycle_level(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     CFA_TPR_SWITCH(tR, CFA_LAUNCH(ctx, (k_vc_spmv<TPR, T, T>), row_grid(ctx, nc, tR), kThreads, 0, nc, V.Rrp, V.Rci,
                                   V.Rv, V.r, 0, cb, done));
     const T* cx;
-    if (!last) {
+    if (!last && l + 1 == amg->comp_level) {
+        cx = view<T>(amg->levels[l + 1]).x;
+        CFA_LAUNCH(ctx, (k_vc_dense<T, T>), ceil_div((long long)amg->comp_n * 32, kThreads), kThreads, 0,
+                   amg->comp_n, amg->comp.p, (const T*)cb, view<T>(amg->levels[l + 1]).x, done);
+    } else if (!last) {
         vcycle_level<T, T>(ctx, amg, l + 1, cb, nullptr, done);
         cx = view<T>(amg->levels[l + 1]).x;
     } else {
@@ -1262,12 +1341,22 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
         vct<VC_JAC, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, t, done);
         std::swap(x, t);
     }
-    vct<VC_RES, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, TVec<T>::r(L), done);
     const bool last = l + 1 == (int)amg->levels.size();
     T* cb = last ? TVec<T>::cb(amg) : TVec<T>::b(amg->levels[l + 1]);
-    vct<VC_SPMV, V, T, T, T>(ctx, dry, L.tR, err, dinv, omega, (const T*)nullptr, (const T*)TVec<T>::r(L), cb, done);
+    if (L.fused) {   // cb = R b - (R A) x in one pass
+        vct<VC_RESTRICT, V, T, B, T>(ctx, dry, L.tQ, err, dinv, omega, b, (const T*)x, cb, done);
+    } else {
+        vct<VC_RES, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, TVec<T>::r(L), done);
+        vct<VC_SPMV, V, T, T, T>(ctx, dry, L.tR, err, dinv, omega, (const T*)nullptr, (const T*)TVec<T>::r(L), cb,
+                                 done);
+    }
     const T* cx;
-    if (!last && l + 1 == amg->tail_level && std::is_same<T, double>::value) {
+    if (!last && l + 1 == amg->comp_level) {
+        if (!dry)
+            CFA_LAUNCH(ctx, (k_vc_dense<T, T>), ceil_div((long long)amg->comp_n * 32, kThreads), kThreads, 0,
+                       amg->comp_n, amg->comp.p, (const T*)cb, TVec<T>::x(amg->levels[l + 1]), done);
+        cx = TVec<T>::x(amg->levels[l + 1]);
+    } else if (!last && l + 1 == amg->tail_level && std::is_same<T, double>::value) {
         if (!dry) launch_tail<V>(ctx, amg, l + 1, done);
         cx = TVec<T>::x(amg->levels[l + 1]);
     } else if (!last) {
@@ -1279,8 +1368,15 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
                        amg->coarse_n, amg->coarse_inv.p, (const T*)cb, TVec<T>::cx(amg), done);
         cx = TVec<T>::cx(amg);
     }
-    vct<VC_ADD, V, T, T, T>(ctx, dry, L.tP, err, dinv, omega, (const T*)nullptr, cx, x, done);
-    for (int k = 0; k < s; ++k) {
+    int k0 = 0;
+    if (L.fused) {   // the first post-smoothing sweep from x + P cx
+        vct<VC_ADDJAC, V, T, B, T>(ctx, dry, L.tW, err, dinv, omega, b, (const T*)x, t, done, nullptr, cx);
+        std::swap(x, t);
+        k0 = 1;
+    } else {
+        vct<VC_ADD, V, T, T, T>(ctx, dry, L.tP, err, dinv, omega, (const T*)nullptr, cx, x, done);
+    }
+    for (int k = k0; k < s; ++k) {
         if (l == 0 && k == s - 1) {
             vct<VC_JAC, V, T, B, double>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, z, done, rz);
         } else {
@@ -1436,12 +1532,13 @@ static cfa_status transpose(cfa_ctx* ctx, SetupScratch& S, const DCsr& A, DCsr& 
 // "Aggregated when i is visited" only involves roots k < i: i is aggregated iff some root k < i
 // has i as a strong neighbour (k -> i); j is iff j is a root below i, or some root k < i has
 // k -> j. So root(i) depends only on the root status of lower-numbered nodes within two strong
-// hops -- the lexicographically first independent set of that conflict relation. It is found in
-// rounds: an undecided node becomes a non-root as soon as one lower conflict is a root, and a
-// root once all of its lower conflicts are decided non-roots. Every round decides at least the
-// lowest undecided node, states only move from undecided to final, so the rounds may read each
-// other's states at any time. Aggregate ids follow root order (a prefix sum); a non-root takes
-// the id of the root that has it as a strong neighbour (at most one can).
+// hops -- the lexicographically first independent set of that conflict relation: an undecided
+// node becomes a non-root as soon as one lower conflict is a root, and a root once all of its
+// lower conflicts are decided non-roots. States only move from undecided to final, so a node may
+// read the others' states at any time. The decisions form chains (about 1800 dependent steps on
+// the ~400k-node pressure matrix), which rule out one launch per step: one launch per phase
+// decides all nodes as a dataflow (k_agg_flow). Aggregate ids follow root order (a prefix sum); a
+// non-root takes the id of the root that has it as a strong neighbour (at most one can).
 // Phase 2 (parallel in the reference too) gives an unaggregated node the aggregate of its first
 // aggregated strong neighbour. Phase 3 visits the rest in index order: an unaggregated node
 // starts a new aggregate and claims its unaggregated strong neighbours (all of higher index), so
@@ -1479,43 +1576,6 @@ __device__ __forceinline__ unsigned char agg_state(const unsigned char* st, int 
     return *reinterpret_cast<const volatile unsigned char*>(st + k);
 }
 
-// One round of phase 1. `more` is set when a node is still undecided at the end of its visit.
-__global__ void k_agg_p1_round(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                               const unsigned char* __restrict__ strong, const int* __restrict__ trp,
-                               const int* __restrict__ tci, unsigned char* st, int* __restrict__ more) {
-    CFA_GRID_DEP();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || agg_state(st, i) != AGG_UNDECIDED) return;
-    bool pending = false;
-    // a root k < i with k -> i aggregated i before its visit
-    for (int q = trp[i]; q < trp[i + 1]; ++q) {
-        const int k = tci[q];
-        if (k >= i) continue;
-        const unsigned char sk = agg_state(st, k);
-        if (sk == AGG_ROOT) { st[i] = AGG_MEMBER; return; }
-        pending |= sk == AGG_UNDECIDED;
-    }
-    // a strong neighbour j aggregated before i's visit: a root below i, or k -> j from a root k < i
-    for (int a = rp[i]; a < rp[i + 1]; ++a) {
-        if (!strong[a]) continue;
-        const int j = ci[a];
-        if (j < i) {
-            const unsigned char sj = agg_state(st, j);
-            if (sj == AGG_ROOT) { st[i] = AGG_MEMBER; return; }
-            pending |= sj == AGG_UNDECIDED;
-        }
-        for (int q = trp[j]; q < trp[j + 1]; ++q) {
-            const int k = tci[q];
-            if (k >= i) continue;
-            const unsigned char sk = agg_state(st, k);
-            if (sk == AGG_ROOT) { st[i] = AGG_MEMBER; return; }
-            pending |= sk == AGG_UNDECIDED;
-        }
-    }
-    if (!pending) st[i] = AGG_ROOT;
-    else *more = 1;
-}
-
 // Phase 1 ids: a root's from the prefix sum of roots; a member's from the root that has it as a
 // strong neighbour; -1 for the rest.
 __global__ void k_agg_p1_ids(int n, const int* __restrict__ trp, const int* __restrict__ tci,
@@ -1551,23 +1611,94 @@ __global__ void k_agg_p2(int n, const int* __restrict__ rp, const int* __restric
     st3[i] = a < 0 ? AGG_UNDECIDED : AGG_MEMBER;
 }
 
-// One round of phase 3: a node left unaggregated is claimed by a lower root k -> i, a root
-// once every lower unaggregated in-neighbour is decided and none is a root.
-__global__ void k_agg_p3_round(int n, const int* __restrict__ trp, const int* __restrict__ tci,
-                               const int* __restrict__ agg2, unsigned char* st, int* __restrict__ more) {
-    CFA_GRID_DEP();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || agg_state(st, i) != AGG_UNDECIDED) return;
+// Both sequential phases as one dataflow launch each. Chunks of kAggChunk consecutive nodes go
+// to CTAs in ticket order (a CTA takes the next chunk when it starts), one node per thread; a
+// thread re-evaluates its node until it is decided. A chunk's states live in shared memory as well
+// as in global memory, so the many decisions that wait on a node of the same chunk (the mesh
+// numbering keeps conflicts close in index) take a shared-memory round trip rather than an L2 one.
+// Progress: the lowest undecided node has all its lower conflicts decided, and its chunk has
+// started, because every CTA with an earlier ticket holds only lower nodes, all decided, and
+// retires. Every wait is bounded: a thread that polls kAggPollLimit times, or sees another thread
+// give up, records CFA_TIMEOUT in *err and leaves its node undecided.
+constexpr int kAggChunk = 1024;
+constexpr unsigned kAggPollLimit = 1u << 20;
+
+struct AggView {
+    const unsigned char* g;     // global states
+    volatile unsigned char* s;  // this chunk's states
+    int base;
+    __device__ __forceinline__ unsigned char operator()(int k) const {
+        const unsigned kk = (unsigned)(k - base);
+        return kk < (unsigned)kAggChunk ? s[kk] : agg_state(g, k);
+    }
+};
+
+// The state node i can take from what its lower conflicts have decided so far (UNDECIDED: not
+// yet). Phase 1: a root k < i with k -> i aggregated i before its visit; so did a strong neighbour
+// j of i that is a root below i or has an in-neighbour root k < i. Phase 3 (nodes that phases 1
+// and 2 left unaggregated): i is claimed by a lower such root k -> i, and is a root once every
+// lower such in-neighbour is decided and none is a root.
+template <bool P3>
+__device__ __forceinline__ unsigned char agg_decide(int i, const int* __restrict__ rp, const int* __restrict__ ci,
+                                                    const unsigned char* __restrict__ strong,
+                                                    const int* __restrict__ trp, const int* __restrict__ tci,
+                                                    const int* __restrict__ agg2, const AggView& st) {
     bool pending = false;
     for (int q = trp[i]; q < trp[i + 1]; ++q) {
         const int k = tci[q];
-        if (k >= i || agg2[k] >= 0) continue;
-        const unsigned char sk = agg_state(st, k);
-        if (sk == AGG_ROOT) { st[i] = AGG_MEMBER; return; }
+        if (k >= i || (P3 && agg2[k] >= 0)) continue;
+        const unsigned char sk = st(k);
+        if (sk == AGG_ROOT) return AGG_MEMBER;
         pending |= sk == AGG_UNDECIDED;
     }
-    if (!pending) st[i] = AGG_ROOT;
-    else *more = 1;
+    if (!P3) {
+        for (int a = rp[i]; a < rp[i + 1]; ++a) {
+            if (!strong[a]) continue;
+            const int j = ci[a];
+            if (j < i) {
+                const unsigned char sj = st(j);
+                if (sj == AGG_ROOT) return AGG_MEMBER;
+                pending |= sj == AGG_UNDECIDED;
+            }
+            for (int q = trp[j]; q < trp[j + 1]; ++q) {
+                const int k = tci[q];
+                if (k >= i) continue;
+                const unsigned char sk = st(k);
+                if (sk == AGG_ROOT) return AGG_MEMBER;
+                pending |= sk == AGG_UNDECIDED;
+            }
+        }
+    }
+    return pending ? AGG_UNDECIDED : AGG_ROOT;
+}
+
+template <bool P3>
+__global__ void __launch_bounds__(kAggChunk)
+k_agg_flow(int n, const int* __restrict__ rp, const int* __restrict__ ci, const unsigned char* __restrict__ strong,
+           const int* __restrict__ trp, const int* __restrict__ tci, const int* __restrict__ agg2, unsigned char* st,
+           int* __restrict__ ticket, int* err) {
+    CFA_GRID_DEP();
+    __shared__ int s_chunk;
+    __shared__ unsigned char s_st[kAggChunk];
+    if (threadIdx.x == 0) s_chunk = atomicAdd(ticket, 1);
+    __syncthreads();
+    const int base = s_chunk * kAggChunk;
+    const int i = base + threadIdx.x;
+    unsigned char mine = i < n ? agg_state(st, i) : AGG_MEMBER;
+    s_st[threadIdx.x] = mine;
+    __syncthreads();
+    const AggView view{st, s_st, base};
+    volatile int* verr = err;
+    for (unsigned it = 0; mine == AGG_UNDECIDED; ++it) {
+        mine = agg_decide<P3>(i, rp, ci, strong, trp, tci, agg2, view);
+        if (mine != AGG_UNDECIDED) {
+            s_st[threadIdx.x] = mine;
+            *reinterpret_cast<volatile unsigned char*>(st + i) = mine;
+        } else if (it >= kAggPollLimit || *verr != 0) {
+            atomicCAS(err, 0, (int)CFA_TIMEOUT);
+            break;
+        }
+    }
 }
 
 // Phase 3 ids (after na1 phase-1 aggregates): roots in order; a claimed node takes its lowest
@@ -1622,27 +1753,6 @@ __global__ void k_agg_is_root(int n, const unsigned char* __restrict__ st, int* 
     if (i <= n) flag[i] = (i < n && st[i] == AGG_ROOT) ? 1 : 0;
 }
 
-// Runs the rounds of one phase until no node is undecided: rounds are launched in groups of
-// `kAggRoundsPerCheck`, the last of each group reporting whether undecided nodes remain. Every
-// round decides at least the lowest undecided node, so the loop ends; `rounds` counts them.
-template <class Launch>
-static cfa_status agg_rounds(cfa_ctx* ctx, SetupScratch& S, int n, Launch launch_round, int* rounds) {
-    constexpr int kAggRoundsPerCheck = 8;
-    int r = 0;
-    for (;;) {
-        CFA_CUDA(cudaMemsetAsync(S.ag_flag.p, 0, sizeof(int), ctx->stream));
-        for (int k = 0; k < kAggRoundsPerCheck; ++k) launch_round(k + 1 == kAggRoundsPerCheck ? S.ag_flag.p : S.ag_flag.p + 1);
-        r += kAggRoundsPerCheck;
-        CFA_CUDA(cudaMemcpyAsync(S.h_ag.p, S.ag_flag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-        CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-        if (S.h_ag.p[0] == 0) break;
-        if (r > n + kAggRoundsPerCheck)
-            return set_error(ctx, CFA_CUDA_ERROR, "aggregation rounds did not finish", __FILE__, __LINE__);
-    }
-    if (rounds) *rounds += r;
-    return CFA_OK;
-}
-
 // The aggregates of A's strong graph (S.strong) into agg[m]; na = their count; the tentative
 // prolongator's row offsets and values into S.p0rp / S.p0v.
 static cfa_status aggregate_device(cfa_ctx* ctx, SetupScratch& S, const DCsr& A, int* agg, int* na_out) {
@@ -1653,7 +1763,7 @@ static cfa_status aggregate_device(cfa_ctx* ctx, SetupScratch& S, const DCsr& A,
     CFA_CUDA(S.ag_tci.ensure(std::max(A.nnz, 1)));
     CFA_CUDA(S.ag_state.ensure(n));
     CFA_CUDA(S.ag_flag.ensure(2));
-    CFA_CUDA(S.h_ag.ensure(2));
+    CFA_CUDA(S.h_ag.ensure(3));
     CFA_CUDA(S.p0v.ensure(n));
     CFA_CUDA(S.p0rp.ensure(n + 1));
     // in-neighbour lists of the strong graph
@@ -1663,13 +1773,13 @@ static cfa_status aggregate_device(cfa_ctx* ctx, SetupScratch& S, const DCsr& A,
     CFA_CUDA(cudaMemsetAsync(S.ag_fill.p, 0, (n + 1) * sizeof(int), ctx->stream));
     CFA_LAUNCH(ctx, k_strong_fill, g, kThreads, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p,
                (const int*)S.ag_trp.p, S.ag_fill.p, S.ag_tci.p);
-    // phase 1
+    // phase 1 (ag_flag: [0] chunk tickets, [1] error status)
+    const int chunks = ceil_div(n, kAggChunk);
     CFA_CUDA(cudaMemsetAsync(S.ag_state.p, AGG_UNDECIDED, n, ctx->stream));
-    int rounds = 0;
-    CFA_PROPAGATE(agg_rounds(ctx, S, n, [&](int* more) {
-        CFA_LAUNCH(ctx, k_agg_p1_round, g, kThreads, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p,
-                   (const int*)S.ag_trp.p, (const int*)S.ag_tci.p, S.ag_state.p, more);
-    }, &rounds));
+    CFA_CUDA(cudaMemsetAsync(S.ag_flag.p, 0, 2 * sizeof(int), ctx->stream));
+    CFA_LAUNCH(ctx, k_agg_flow<false>, chunks, kAggChunk, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p,
+               (const int*)S.ag_trp.p, (const int*)S.ag_tci.p, (const int*)nullptr, S.ag_state.p, S.ag_flag.p,
+               S.ag_flag.p + 1);
     CFA_LAUNCH(ctx, k_agg_is_root, g1, kThreads, 0, n, (const unsigned char*)S.ag_state.p, S.ag_fill.p);
     CFA_PROPAGATE(exclusive_sum(ctx, S, S.ag_fill.p, S.ag_rank.p, n));
     CFA_LAUNCH(ctx, k_agg_p1_ids, g, kThreads, 0, n, (const int*)S.ag_trp.p, (const int*)S.ag_tci.p,
@@ -1679,10 +1789,15 @@ static cfa_status aggregate_device(cfa_ctx* ctx, SetupScratch& S, const DCsr& A,
                (const int*)S.ag_agg1.p, S.ag_agg2.p, S.ag_state.p);
     // phase 3 (the number of phase-1 aggregates first: the ids continue from it)
     CFA_CUDA(cudaMemcpyAsync(S.h_ag.p + 1, S.ag_rank.p + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CFA_PROPAGATE(agg_rounds(ctx, S, n, [&](int* more) {
-        CFA_LAUNCH(ctx, k_agg_p3_round, g, kThreads, 0, n, (const int*)S.ag_trp.p, (const int*)S.ag_tci.p,
-                   (const int*)S.ag_agg2.p, S.ag_state.p, more);
-    }, &rounds));
+    CFA_CUDA(cudaMemsetAsync(S.ag_flag.p, 0, sizeof(int), ctx->stream));
+    CFA_LAUNCH(ctx, k_agg_flow<true>, chunks, kAggChunk, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p,
+               (const int*)S.ag_trp.p, (const int*)S.ag_tci.p, (const int*)S.ag_agg2.p, S.ag_state.p, S.ag_flag.p,
+               S.ag_flag.p + 1);
+    CFA_CUDA(cudaMemcpyAsync(S.h_ag.p + 2, S.ag_flag.p + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (S.h_ag.p[2] != 0)
+        return set_error(ctx, CFA_TIMEOUT, "aggregation: a node's decision waited past its poll limit", __FILE__,
+                         __LINE__);
     const int na1 = S.h_ag.p[1];
     CFA_LAUNCH(ctx, k_agg_is_root, g1, kThreads, 0, n, (const unsigned char*)S.ag_state.p, S.ag_fill.p);
     CFA_PROPAGATE(exclusive_sum(ctx, S, S.ag_fill.p, S.ag_rank.p, n));
@@ -1703,11 +1818,8 @@ static cfa_status aggregate_device(cfa_ctx* ctx, SetupScratch& S, const DCsr& A,
 // CFA_AGG_HOST=0: the aggregation runs as the device rounds; otherwise as the reference's
 // sequential host loop.
 static bool agg_on_host() {
-    static const bool on = [] {
-        const char* e = std::getenv("CFA_AGG_HOST");
-        return !(e && e[0] == '0');
-    }();
-    return on;
+    const char* e = std::getenv("CFA_AGG_HOST");
+    return !(e && e[0] == '0');
 }
 
 static int aggregate_host(int n, const int* rp, const int* ci, const unsigned char* strong, int* agg) {
@@ -1825,6 +1937,129 @@ static cfa_status level_vectors64(cfa_ctx* ctx, AmgLevel& L, int n) {
     return CFA_OK;
 }
 
+// ---- fused transfers (AmgLevel::tQ, tW) ----
+// Q = [R | -R A] row by row: R's entries (columns of b), then R A's with the second-vector bit
+// (columns of x) and negated values. Qrp = Rrp + RArp.
+__global__ void k_fuse_q_rp(int nc, const int* __restrict__ a, const int* __restrict__ b, int* __restrict__ out) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= nc) out[i] = a[i] + b[i];
+}
+
+__global__ void k_fuse_q_fill(int nc, const int* __restrict__ Rrp, const int* __restrict__ Rci,
+                              const double* __restrict__ Rv, const int* __restrict__ Crp, const int* __restrict__ Cci,
+                              const double* __restrict__ Cv, const int* __restrict__ Qrp, int* __restrict__ Qci,
+                              double* __restrict__ Qv) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nc) return;
+    int o = Qrp[i];
+    for (int k = Rrp[i]; k < Rrp[i + 1]; ++k, ++o) { Qci[o] = Rci[k]; Qv[o] = Rv[k]; }
+    for (int k = Crp[i]; k < Crp[i + 1]; ++k, ++o) { Qci[o] = Cci[k] | kSecondVec; Qv[o] = -Cv[k]; }
+}
+
+// W row i = A's entries (columns of x; v0 = A, v1 = 1 on the diagonal), then A P's (columns of
+// the coarse correction; v0 = A P, v1 = P where P has the column), then P's columns that A P
+// lacks (v0 = 0). count: entries per row into cnt; fill: the rows at Wrp.
+template <bool FILL>
+__global__ void k_fuse_w(int n, const int* __restrict__ Arp, const int* __restrict__ Aci, const double* __restrict__ Av,
+                         const int* __restrict__ Brp, const int* __restrict__ Bci, const double* __restrict__ Bv,
+                         const int* __restrict__ Prp, const int* __restrict__ Pci, const double* __restrict__ Pv,
+                         int* __restrict__ cnt, const int* __restrict__ Wrp, int* __restrict__ Wci,
+                         double* __restrict__ W0, double* __restrict__ W1) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int o = FILL ? Wrp[i] : 0;
+    for (int k = Arp[i]; k < Arp[i + 1]; ++k, ++o)
+        if (FILL) { Wci[o] = Aci[k]; W0[o] = Av[k]; W1[o] = Aci[k] == i ? 1.0 : 0.0; }
+    for (int k = Brp[i]; k < Brp[i + 1]; ++k, ++o) {
+        if (!FILL) continue;
+        double pv = 0.0;
+        for (int q = Prp[i]; q < Prp[i + 1]; ++q)
+            if (Pci[q] == Bci[k]) pv = Pv[q];
+        Wci[o] = Bci[k] | kSecondVec; W0[o] = Bv[k]; W1[o] = pv;
+    }
+    for (int q = Prp[i]; q < Prp[i + 1]; ++q) {
+        bool in = false;
+        for (int k = Brp[i]; k < Brp[i + 1] && !in; ++k) in = Bci[k] == Pci[q];
+        if (in) continue;
+        if (FILL) { Wci[o] = Pci[q] | kSecondVec; W0[o] = 0.0; W1[o] = Pv[q]; }
+        ++o;
+    }
+    if (!FILL) cnt[i] = o;
+}
+
+// Levels whose transfers run fused (VC_RESTRICT, VC_ADDJAC): CFA_VC_FUSE=0 none, 1 levels >= 1
+// (the default: there the V-cycle is a chain of short launches), 2 every level. Needs at least
+// two smoothing steps (the first post-smoothing sweep carries the prolongation).
+static bool fuse_level(const cfa_amg* amg, const AmgLevel& L) {
+    const char* e = std::getenv("CFA_VC_FUSE");
+    const int mode = e ? std::atoi(e) : 1;
+    if (mode <= 0 || amg->opts.smooth_steps < 2) return false;
+    return mode >= 2 || &L != &amg->levels[0];
+}
+
+static cfa_status pack_from_device(cfa_ctx* ctx, cfa_amg* amg, const DCsr& M, const double* v0, const double* v1,
+                                   int vb, TiledCsr& T) {
+    HostBuf<int>& hr = amg->scratch.h_rp;
+    CFA_CUDA(hr.ensure(M.rows + 1));
+    CFA_CUDA(cudaMemcpyAsync(hr.p, M.rp.p, (M.rows + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    CFA_PROPAGATE(plan_tiled(ctx, hr.p, M.rows, v1 ? 2 : 1, vb, T));
+    return pack_tiled(ctx, M.rp.p, M.ci.p, v0, v1, nullptr, T);
+}
+
+// The fused transfer operators of a level: Q = [R | -R A] and W = ([A | A P], [I | P]), exact
+// products on the device (the setup's SpGEMM), packed as tiles in the hierarchy precision.
+static cfa_status build_fused(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb) {
+    SetupScratch& S = amg->scratch;
+    const int n = L.A.rows, nc = L.R.rows;
+    CFA_PROPAGATE(spgemm(ctx, S, nc, n, L.R.rp.p, L.R.ci.p, L.R.v.p, L.A.rp.p, L.A.ci.p, L.A.v.p, S.fRA));
+    CFA_PROPAGATE(spgemm(ctx, S, n, L.P.cols, L.A.rp.p, L.A.ci.p, L.A.v.p, L.P.rp.p, L.P.ci.p, L.P.v.p, S.fAP));
+    // Q
+    DCsr& Q = S.fQ;
+    Q.rows = nc;
+    Q.cols = n;
+    Q.nnz = L.R.nnz + S.fRA.nnz;
+    CFA_CUDA(Q.rp.ensure(nc + 1));
+    CFA_CUDA(Q.ci.ensure(std::max(Q.nnz, 1)));
+    CFA_CUDA(Q.v.ensure(std::max(Q.nnz, 1)));
+    CFA_LAUNCH(ctx, k_fuse_q_rp, ceil_div(nc + 1, kThreads), kThreads, 0, nc, (const int*)L.R.rp.p,
+               (const int*)S.fRA.rp.p, Q.rp.p);
+    CFA_LAUNCH(ctx, k_fuse_q_fill, ceil_div(nc, kThreads), kThreads, 0, nc, (const int*)L.R.rp.p,
+               (const int*)L.R.ci.p, (const double*)L.R.v.p, (const int*)S.fRA.rp.p, (const int*)S.fRA.ci.p,
+               (const double*)S.fRA.v.p, (const int*)Q.rp.p, Q.ci.p, Q.v.p);
+    CFA_PROPAGATE(pack_from_device(ctx, amg, Q, Q.v.p, nullptr, vb, L.tQ));
+    // W: count, offsets, fill
+    DCsr& W = S.fW;
+    CFA_CUDA(S.fcnt.ensure(n + 1));
+    CFA_CUDA(W.rp.ensure(n + 1));
+    CFA_LAUNCH(ctx, k_fuse_w<false>, ceil_div(n, kThreads), kThreads, 0, n, (const int*)L.A.rp.p, (const int*)L.A.ci.p,
+               (const double*)L.A.v.p, (const int*)S.fAP.rp.p, (const int*)S.fAP.ci.p, (const double*)S.fAP.v.p,
+               (const int*)L.P.rp.p, (const int*)L.P.ci.p, (const double*)L.P.v.p, S.fcnt.p, (const int*)nullptr,
+               (int*)nullptr, (double*)nullptr, (double*)nullptr);
+    CFA_CUDA(cudaMemsetAsync(S.fcnt.p + n, 0, sizeof(int), ctx->stream));
+    CFA_PROPAGATE(exclusive_sum(ctx, S, S.fcnt.p, W.rp.p, n));
+    int total = 0;
+    CFA_CUDA(cudaMemcpyAsync(&total, W.rp.p + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    W.rows = n;
+    W.cols = n;
+    W.nnz = total;
+    CFA_CUDA(W.ci.ensure(std::max(total, 1)));
+    CFA_CUDA(W.v.ensure(std::max(total, 1)));
+    CFA_CUDA(S.fW1.ensure(std::max(total, 1)));
+    CFA_LAUNCH(ctx, k_fuse_w<true>, ceil_div(n, kThreads), kThreads, 0, n, (const int*)L.A.rp.p, (const int*)L.A.ci.p,
+               (const double*)L.A.v.p, (const int*)S.fAP.rp.p, (const int*)S.fAP.ci.p, (const double*)S.fAP.v.p,
+               (const int*)L.P.rp.p, (const int*)L.P.ci.p, (const double*)L.P.v.p, (int*)nullptr,
+               (const int*)W.rp.p, W.ci.p, W.v.p, S.fW1.p);
+    CFA_PROPAGATE(pack_from_device(ctx, amg, W, W.v.p, S.fW1.p, vb, L.tW));
+    CFA_CHECK_LAUNCH();
+    L.fused = true;
+    return CFA_OK;
+}
+
 // Kernel shapes of one level, its FP32 copies (mixed precision) and its tile-streamed A, P, R in
 // the hierarchy precision.
 static cfa_status prepare_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L) {
@@ -1843,6 +2078,8 @@ static cfa_status prepare_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L) {
     CFA_CHECK_LAUNCH();
     if (!amg->tiled) return CFA_OK;
     const int vb = o.precision == CFA_MIXED ? 4 : 8;
+    L.fused = false;
+    if (fuse_level(amg, L)) CFA_PROPAGATE(build_fused(ctx, amg, L, vb));
     for (DCsr* M : {&L.A, &L.P, &L.R}) {
         TiledCsr& T = M == &L.A ? L.tA : M == &L.P ? L.tP : L.tR;
         HostBuf<int>& hr = amg->scratch.h_rp;
@@ -1863,6 +2100,89 @@ static cfa_status prepare_vcycle(cfa_ctx* ctx, cfa_amg* amg) {
     CFA_PROPAGATE(plan_tail(ctx, amg));
     vcycle_tiled_top(ctx, amg, nullptr, nullptr, nullptr, true);
     CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+// Largest level (rows) whose V-cycle below is formed as one dense operator (CFA_COMPOSITE_ROWS
+// overrides; 0: never). At 2048 rows the FP64 matrix is 32 MB, read in about the time of one
+// dependent launch of the chain it replaces.
+static int composite_rows() {
+    const char* e = std::getenv("CFA_COMPOSITE_ROWS");
+    return e ? std::atoi(e) : 2048;
+}
+
+// Forms the composite of the first level l >= 1 with at most composite_rows() rows (the V-cycle's
+// level 0 keeps its kernels: its last sweep carries the CG's dots). Runs the V-cycle's operations
+// of levels l.. on the identity block in FP64, in the order of vcycle_tiled.
+static cfa_status build_composite(cfa_ctx* ctx, cfa_amg* amg) {
+    amg->comp_level = -1;
+    amg->comp_n = 0;
+    const int limit = composite_rows();
+    const int L = (int)amg->levels.size();
+    int lc = -1;
+    for (int l = 1; l < L; ++l)
+        if (amg->levels[l].A.rows <= limit) { lc = l; break; }
+    if (lc < 0) return CFA_OK;
+    const int nb = amg->levels[lc].A.rows;
+    const int s = amg->opts.smooth_steps;
+    // per level k >= lc: right-hand sides, iterate, scratch, residual (rows(k) x nb); coarse pair
+    std::vector<DevBuf<double>> blk(4 * (L - lc) + 2);
+    for (int k = lc; k < L; ++k)
+        for (int q = 0; q < 4; ++q) CFA_CUDA(blk[4 * (k - lc) + q].ensure((size_t)amg->levels[k].A.rows * nb));
+    const int cn = amg->coarse_n;
+    CFA_CUDA(blk[4 * (L - lc)].ensure((size_t)cn * nb));
+    CFA_CUDA(blk[4 * (L - lc) + 1].ensure((size_t)cn * nb));
+    auto grid = [&](long long entries) { return ceil_div(entries, kThreads); };
+    CFA_LAUNCH(ctx, k_bm_eye, grid((long long)nb * nb), kThreads, 0, nb, blk[0].p);
+    // the V-cycle of level k on the block in blk[4(k - lc)]; returns the block holding its result
+    std::function<double*(int)> level = [&](int k) -> double* {
+        AmgLevel& Lk = amg->levels[k];
+        const int m = Lk.A.rows;
+        const long long me = (long long)m * nb;
+        double* B = blk[4 * (k - lc)].p;
+        double* X = blk[4 * (k - lc) + 1].p;
+        double* T = blk[4 * (k - lc) + 2].p;
+        double* Rr = blk[4 * (k - lc) + 3].p;
+        const DCsr& A = Lk.A;
+        CFA_LAUNCH(ctx, k_bm<BM_PRE>, grid(me), kThreads, 0, m, nb, A.rp.p, A.ci.p, A.v.p, Lk.dinv.p, Lk.omega,
+                   s >= 2 ? 1 : 0, (const double*)B, (const double*)nullptr, X);
+        for (int q = 2; q < s; ++q) {
+            CFA_LAUNCH(ctx, k_bm<BM_JAC>, grid(me), kThreads, 0, m, nb, A.rp.p, A.ci.p, A.v.p, Lk.dinv.p, Lk.omega, 0,
+                       (const double*)B, (const double*)X, T);
+            std::swap(X, T);
+        }
+        CFA_LAUNCH(ctx, k_bm<BM_RES>, grid(me), kThreads, 0, m, nb, A.rp.p, A.ci.p, A.v.p, Lk.dinv.p, Lk.omega, 0,
+                   (const double*)B, (const double*)X, Rr);
+        const bool last = k + 1 == L;
+        const int mc = Lk.R.rows;
+        double* Bc = last ? blk[4 * (L - lc)].p : blk[4 * (k + 1 - lc)].p;
+        CFA_LAUNCH(ctx, k_bm<BM_SPMV>, grid((long long)mc * nb), kThreads, 0, mc, nb, Lk.R.rp.p, Lk.R.ci.p,
+                   Lk.R.v.p, (const double*)nullptr, 0.0, 0, (const double*)nullptr, (const double*)Rr, Bc);
+        const double* Xc;
+        if (last) {
+            double* Xd = blk[4 * (L - lc) + 1].p;
+            CFA_LAUNCH(ctx, k_bm_dense, grid((long long)cn * nb), kThreads, 0, cn, nb,
+                       (const double*)amg->coarse_inv.p, (const double*)Bc, Xd);
+            Xc = Xd;
+        } else {
+            Xc = level(k + 1);
+        }
+        CFA_LAUNCH(ctx, k_bm<BM_ADD>, grid(me), kThreads, 0, m, nb, Lk.P.rp.p, Lk.P.ci.p, Lk.P.v.p,
+                   (const double*)nullptr, 0.0, 0, (const double*)nullptr, Xc, X);
+        for (int q = 0; q < s; ++q) {
+            CFA_LAUNCH(ctx, k_bm<BM_JAC>, grid(me), kThreads, 0, m, nb, A.rp.p, A.ci.p, A.v.p, Lk.dinv.p, Lk.omega, 0,
+                       (const double*)B, (const double*)X, T);
+            std::swap(X, T);
+        }
+        return X;
+    };
+    const double* M = level(lc);
+    CFA_CUDA(amg->comp.ensure((size_t)nb * nb));
+    CFA_CUDA(cudaMemcpyAsync(amg->comp.p, M, (size_t)nb * nb * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CFA_CHECK_LAUNCH();
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));   // the blocks are released on return
+    amg->comp_level = lc;
+    amg->comp_n = nb;
     return CFA_OK;
 }
 
@@ -2006,6 +2326,7 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
     CFA_CHECK_LAUNCH();
     int h_err = 0;
     CFA_CUDA(cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_PROPAGATE(build_composite(ctx, amg));
     phase(7);
     CFA_CUDA(amg->cb64.ensure(cn + 1));
     CFA_CUDA(amg->cx64.ensure(cn + 1));
@@ -2228,6 +2549,14 @@ cfa_status cfa_amg_phases(const cfa_amg* amg, double* ms8) {
 cfa_status cfa_amg_coarse_inverse(const cfa_amg* amg, const double** inv) {
     if (!amg || !inv) return CFA_BAD_ARG;
     *inv = amg->coarse_inv.p;
+    return CFA_OK;
+}
+
+cfa_status cfa_amg_composite(const cfa_amg* amg, int* level, int* rows, const double** m) {
+    if (!amg) return CFA_BAD_ARG;
+    if (level) *level = amg->comp_level;
+    if (rows) *rows = amg->comp_n;
+    if (m) *m = amg->comp_level >= 0 ? amg->comp.p : nullptr;
     return CFA_OK;
 }
 

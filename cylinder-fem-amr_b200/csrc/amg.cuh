@@ -19,6 +19,12 @@ struct DCsr {
 struct AmgLevel {
     DCsr A, P, R;
     TiledCsr tA, tP, tR;           // tile-streamed copies in the hierarchy precision
+    // fused transfers (fused = true): tQ, the restricted residual R b - (R A) x in one pass over
+    // the next level's rows; tW, the prolongation-add folded into the first post-smoothing sweep
+    // (values [A | A P] and [I | P] on one pattern); columns with the top bit set read the second
+    // vector (x, resp. the coarse correction)
+    TiledCsr tQ, tW;
+    bool fused = false;
     DevBuf<double> dinv;
     DevBuf<float> dinv32;
     double omega = 0.0;
@@ -71,6 +77,9 @@ struct SetupScratch {
     HostBuf<unsigned char> h_strong;
     HostBuf<double> h_p0v, h_st;
     DCsr AP0, AP;
+    DCsr fRA, fAP, fQ, fW;              // fused transfers: R A, A P, the merged operators
+    DevBuf<double> fW1;                 // second value array of fW
+    DevBuf<int> fcnt;
 };
 
 }  // namespace cfa
@@ -98,6 +107,12 @@ struct cfa_amg {
     int tail_grid = 0;
     cfa::AmgLevel coarse_holder;         // the coarsest operator (its buffers recycled by the next setup)
     cfa::DevBuf<int> err;                // tile pipeline error word
+    // composite: the V-cycle from level comp_level down (its smoothing, transfers and coarse
+    // solve) is one linear map of that level's right-hand side, kept as a dense row-major FP64
+    // matrix (comp_n x comp_n) and applied as one matrix-vector product; -1: none
+    int comp_level = -1;
+    int comp_n = 0;
+    cfa::DevBuf<double> comp;
 };
 
 namespace cfa {

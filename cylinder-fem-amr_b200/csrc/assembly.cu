@@ -238,131 +238,133 @@ __global__ void k_scalar_gradient_rows(int n, const int* __restrict__ ev, const 
     gy_out[i] = sy;
 }
 
-// Pressure rows: k_assemble_pressure_poisson (fem_kernels.cuh:201-282) gathered per row; with
-// oss_val the rows of B and B^T of k_assemble_oss_operator (:807-847) and inv_m (:849-852) in
-// the same pass; with with_bc the Dirichlet rows/columns of k_apply_bc_pressure (:460-490).
-// A row of up to kPressCap entries accumulates K, Bx, By, B^T x, B^T y in shared memory laid out
-// [array][slot][thread], so that threads adding to different slots of their rows hit different
-// banks; longer rows accumulate in place in global memory. Every entry takes its terms in the
-// element order of the incidence either way.
-constexpr int kPressThreads = 128;
-constexpr int kPressCap = 16;
-constexpr size_t kPressSmem = (size_t)5 * kPressCap * kPressThreads * sizeof(double);
+// Pressure system: k_assemble_pressure_poisson (fem_kernels.cuh:201-282); with oss_val the rows
+// of B and B^T of k_assemble_oss_operator (:807-847) and inv_m (:849-852); with with_bc the
+// Dirichlet rows/columns of k_apply_bc_pressure (:460-490). Three passes:
+//   k_press_elems    one thread per element: its geometry and the element terms every entry and
+//                    row needs (computed once instead of once per vertex), a 16-double record;
+//   k_press_entries  one thread per CSR entry: K, Bx, By, B^T x, B^T y summed over the entry's
+//                    contributions (the mesh's entry plan) and written coalesced;
+//   k_press_rowsums  one thread per row: the right-hand side and the divergence numerator.
+// Every sum takes its terms in the element order of the row's incidence, as a row walking its
+// elements would, and each term is the same expression of the same element values.
+constexpr int kPressRec = 16;   // area, dNdx[3], dNdy[3], s, w, rhs term, div term, gx, gy, sx, sy, -
 
-__global__ void __launch_bounds__(kPressThreads)
-k_pressure_rows(int n, int nnz, const int* __restrict__ ev, const double* __restrict__ x,
-                const double* __restrict__ y, const int* __restrict__ tag, const int* __restrict__ inc_ptr,
-                const int* __restrict__ inc, const int* __restrict__ pos, const int* __restrict__ rp,
-                const int* __restrict__ ci, const double* __restrict__ us, const double* __restrict__ vs,
-                const double* __restrict__ p_old, const double* __restrict__ gpx, const double* __restrict__ gpy,
-                const double* __restrict__ mass, const double* __restrict__ elem_s, double dt, double rho,
-                double stab, int with_bc, OutletBc bc, double* __restrict__ Kp_val, double* __restrict__ rhs_p,
-                double* __restrict__ div_num, double* __restrict__ dp, double* __restrict__ oss_val,
-                double* __restrict__ inv_m) {
+__global__ void k_press_elems(int ne, const int* __restrict__ ev, const double* __restrict__ x,
+                              const double* __restrict__ y, const double* __restrict__ us,
+                              const double* __restrict__ vs, const double* __restrict__ p_old,
+                              const double* __restrict__ gpx, const double* __restrict__ gpy,
+                              const double* __restrict__ mass, const double* __restrict__ elem_s, double dt,
+                              double rho, double stab, int want_oss, double* __restrict__ rec) {
     CFA_GRID_DEP();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int r0 = rp[i], len = rp[i + 1] - r0;
-    const bool local = len <= kPressCap;
-    const bool want_oss = oss_val != nullptr;
-    extern __shared__ double press_sm[];   // [5][kPressCap][blockDim.x]
-    const int T = blockDim.x, tt = threadIdx.x;
-    double* sK = press_sm + tt;                          // sK[q * T]: K entry q of this row
-    double* sBx = press_sm + 1 * kPressCap * T + tt;
-    double* sBy = press_sm + 2 * kPressCap * T + tt;
-    double* sTx = press_sm + 3 * kPressCap * T + tt;
-    double* sTy = press_sm + 4 * kPressCap * T + tt;
-    double *Bx = oss_val, *By = oss_val + (size_t)nnz, *BTx = oss_val + 2 * (size_t)nnz, *BTy = oss_val + 3 * (size_t)nnz;
-    if (local) {
-        for (int q = 0; q < len; ++q) {
-            sK[q * T] = 0.0;
-            if (want_oss) { sBx[q * T] = 0.0; sBy[q * T] = 0.0; sTx[q * T] = 0.0; sTy[q * T] = 0.0; }
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    int nd[3];
+    load_elem(ev, e, nd);
+    const Geom g = elem_geom(nd, x, y);
+    double* r = rec + (size_t)kPressRec * e;
+    r[0] = g.area;
+    if (!g.ok) return;
+    const double area = g.area;
+    const double div_u = us[nd[0]] * g.dNdx[0] + us[nd[1]] * g.dNdx[1] + us[nd[2]] * g.dNdx[2]
+                       + vs[nd[0]] * g.dNdy[0] + vs[nd[1]] * g.dNdy[1] + vs[nd[2]] * g.dNdy[2];
+    double s = 0.0, sx = 0.0, sy = 0.0, gx = 0.0, gy = 0.0;
+    if (stab > 0.0) {
+        s = elem_s[e];
+        const double rs = sqrt(s);
+        gx = p_old[nd[0]] * g.dNdx[0] + p_old[nd[1]] * g.dNdx[1] + p_old[nd[2]] * g.dNdx[2];
+        gy = p_old[nd[0]] * g.dNdy[0] + p_old[nd[1]] * g.dNdy[1] + p_old[nd[2]] * g.dNdy[2];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const double im = 1.0 / fmax(mass[nd[q]], 1.0e-14);
+            sx += gpx[nd[q]] * im;
+            sy += gpy[nd[q]] * im;
         }
-    } else {
-        for (int q = 0; q < len; ++q) Kp_val[r0 + q] = 0.0;
-        if (want_oss)
-            for (int q = 0; q < len; ++q) { Bx[r0 + q] = 0.0; By[r0 + q] = 0.0; BTx[r0 + q] = 0.0; BTy[r0 + q] = 0.0; }
+        sx *= rs / 3.0;
+        sy *= rs / 3.0;
     }
-    double rhs_row = 0.0, div_row = 0.0;
-    for (int k = inc_ptr[i]; k < inc_ptr[i + 1]; ++k) {
-        const int e = inc[k] >> 2, a = inc[k] & 3;
-        int nd[3];
-        load_elem(ev, e, nd);
-        const Geom g = elem_geom(nd, x, y);
-        if (!g.ok) continue;
-        const double area = g.area;
-        const double div_u = us[nd[0]] * g.dNdx[0] + us[nd[1]] * g.dNdx[1] + us[nd[2]] * g.dNdx[2]
-                           + vs[nd[0]] * g.dNdy[0] + vs[nd[1]] * g.dNdy[1] + vs[nd[2]] * g.dNdy[2];
-        const double rhs_contrib = -(rho / dt) * (area / 3.0) * div_u;
-        double s = 0.0, sx = 0.0, sy = 0.0, gx = 0.0, gy = 0.0;
-        if (stab > 0.0) {
-            s = elem_s[e];
-            const double rs = sqrt(s);
-            gx = p_old[nd[0]] * g.dNdx[0] + p_old[nd[1]] * g.dNdx[1] + p_old[nd[2]] * g.dNdx[2];
-            gy = p_old[nd[0]] * g.dNdy[0] + p_old[nd[1]] * g.dNdy[1] + p_old[nd[2]] * g.dNdy[2];
 #pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                const double im = 1.0 / fmax(mass[nd[q]], 1.0e-14);
-                sx += gpx[nd[q]] * im;
-                sy += gpy[nd[q]] * im;
-            }
-            sx *= rs / 3.0;
-            sy *= rs / 3.0;
-        }
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const double K_ij = area * (g.dNdx[a] * g.dNdx[j] + g.dNdy[a] * g.dNdy[j]);
-            const int p = pos[3 * k + j];
-            if (local) sK[(p - r0) * T] += (1.0 + s) * K_ij; else Kp_val[p] += (1.0 + s) * K_ij;
-        }
-        const double stab_i = s * area * (g.dNdx[a] * gx + g.dNdy[a] * gy) - area * (g.dNdx[a] * sx + g.dNdy[a] * sy);
-        rhs_row += rhs_contrib - stab_i;
-        div_row += (area / 3.0) * div_u;
+    for (int q = 0; q < 3; ++q) {
+        r[1 + q] = g.dNdx[q];
+        r[4 + q] = g.dNdy[q];
+    }
+    r[7] = s;
+    r[8] = want_oss ? sqrt(elem_s[e]) * area / 3.0 : 0.0;
+    r[9] = -(rho / dt) * (area / 3.0) * div_u;
+    r[10] = (area / 3.0) * div_u;
+    r[11] = gx;
+    r[12] = gy;
+    r[13] = sx;
+    r[14] = sy;
+}
+
+__global__ void k_press_entries(int nnz, const int* __restrict__ ent_ptr, const int* __restrict__ ent,
+                                const int* __restrict__ erow, const int* __restrict__ ci, const int* __restrict__ inc,
+                                const int* __restrict__ tag, const double* __restrict__ rec, int with_bc, OutletBc bc,
+                                double* __restrict__ Kp_val, double* __restrict__ oss_val) {
+    CFA_GRID_DEP();
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nnz) return;
+    const int i = erow[p], j = ci[p];
+    const bool want_oss = oss_val != nullptr;
+    double K = 0.0, bx = 0.0, by = 0.0, tx = 0.0, ty = 0.0;
+    for (int c = ent_ptr[p]; c < ent_ptr[p + 1]; ++c) {
+        const int code = ent[c];
+        const int sl = code >> 2, b = code & 3;
+        const int e = inc[sl] >> 2, a = inc[sl] & 3;
+        const double* r = rec + (size_t)kPressRec * e;
+        const double area = r[0];
+        if (area < 1.0e-14) continue;
+        const double dxa = r[1 + a], dxb = r[1 + b], dya = r[4 + a], dyb = r[4 + b];
+        const double K_ij = area * (dxa * dxb + dya * dyb);
+        K += (1.0 + r[7]) * K_ij;
         if (want_oss) {
-            const double w = sqrt(elem_s[e]) * area / 3.0;
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const int p = pos[3 * k + j];
-                // B_ij = sum_K w_K grad N_j|K (row i, column j); B^T_ij = B_ji = sum_K w_K grad N_i|K
-                if (local) {
-                    const int q = (p - r0) * T;
-                    sBx[q] += w * g.dNdx[j];
-                    sBy[q] += w * g.dNdy[j];
-                    sTx[q] += w * g.dNdx[a];
-                    sTy[q] += w * g.dNdy[a];
-                } else {
-                    Bx[p] += w * g.dNdx[j];
-                    By[p] += w * g.dNdy[j];
-                    BTx[p] += w * g.dNdx[a];
-                    BTy[p] += w * g.dNdy[a];
-                }
-            }
+            const double w = r[8];
+            // B_ij = sum_K w_K grad N_j|K (row i, column j); B^T_ij = B_ji = sum_K w_K grad N_i|K
+            bx += w * dxb;
+            by += w * dyb;
+            tx += w * dxa;
+            ty += w * dya;
         }
     }
     if (want_oss) {
-        inv_m[i] = 1.0 / fmax(mass[i], 1.0e-14);
-        if (local)
-            for (int q = 0; q < len; ++q) {
-                Bx[r0 + q] = sBx[q * T];
-                By[r0 + q] = sBy[q * T];
-                BTx[r0 + q] = sTx[q * T];
-                BTy[r0 + q] = sTy[q * T];
-            }
+        oss_val[p] = bx;
+        oss_val[(size_t)nnz + p] = by;
+        oss_val[2 * (size_t)nnz + p] = tx;
+        oss_val[3 * (size_t)nnz + p] = ty;
     }
+    if (with_bc) {
+        if (pressure_dirichlet(i, tag[i], bc)) K = (j == i) ? 1.0 : 0.0;
+        else if (j != i && pressure_dirichlet(j, tag[j], bc)) K = 0.0;
+    }
+    Kp_val[p] = K;
+}
+
+__global__ void k_press_rowsums(int n, const int* __restrict__ tag, const int* __restrict__ inc_ptr,
+                                const int* __restrict__ inc, const double* __restrict__ rec,
+                                const double* __restrict__ mass, int with_bc, OutletBc bc, int want_oss,
+                                double* __restrict__ rhs_p, double* __restrict__ div_num, double* __restrict__ dp,
+                                double* __restrict__ inv_m) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double rhs_row = 0.0, div_row = 0.0;
+    for (int k = inc_ptr[i]; k < inc_ptr[i + 1]; ++k) {
+        const int e = inc[k] >> 2, a = inc[k] & 3;
+        const double* r = rec + (size_t)kPressRec * e;
+        const double area = r[0];
+        if (area < 1.0e-14) continue;
+        const double dxa = r[1 + a], dya = r[4 + a], s = r[7];
+        const double stab_i = s * area * (dxa * r[11] + dya * r[12]) - area * (dxa * r[13] + dya * r[14]);
+        rhs_row += r[9] - stab_i;
+        div_row += r[10];
+    }
+    if (want_oss) inv_m[i] = 1.0 / fmax(mass[i], 1.0e-14);
     div_num[i] = div_row;
     if (with_bc && pressure_dirichlet(i, tag[i], bc)) {
-        for (int q = 0; q < len; ++q) Kp_val[r0 + q] = (ci[r0 + q] == i) ? 1.0 : 0.0;
         rhs_p[i] = 0.0;
         if (dp) dp[i] = 0.0;
         return;
-    }
-    for (int q = 0; q < len; ++q) {
-        double v = local ? sK[q * T] : Kp_val[r0 + q];
-        if (with_bc) {
-            const int c = ci[r0 + q];
-            if (c != i && pressure_dirichlet(c, tag[c], bc)) v = 0.0;
-        }
-        Kp_val[r0 + q] = v;
     }
     rhs_p[i] = rhs_row;
 }
@@ -501,14 +503,17 @@ static cfa_status assemble_pressure(cfa_ctx* ctx, const cfa_mesh* m, const doubl
     // With the pinned outlet the RHS loses its mean before the BC rows (apply_bc_pressure,
     // fem_kernels.cuh:519-531): assemble without BC, then sums, then the BC kernel.
     const bool split = apply_bc && m->bc.outlet_dirichlet;
-    static std::once_flag press_once;
-    std::call_once(press_once, [] {
-        cudaFuncSetAttribute(k_pressure_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPressSmem);
-    });
-    CFA_LAUNCH(ctx, k_pressure_rows, ceil_div(m->n, kPressThreads), kPressThreads, kPressSmem, m->n, m->nnz, m->ev,
-               m->x, m->y, m->tag,
-               m->inc_ptr.p, m->inc.p, m->pos.p, m->rp, m->ci, us, vs, p_old, gpx, gpy, mass, elem_s, dt, rho,
-               stab, (apply_bc && !split) ? 1 : 0, m->bc, Kp, rhs, div, dp, oss_val, inv_m);
+    const int bc_now = (apply_bc && !split) ? 1 : 0;
+    const int want_oss = oss_val ? 1 : 0;
+    DevBuf<double> rec;
+    CFA_CUDA(rec.ensure((size_t)kPressRec * std::max(m->ne, 1)));
+    CFA_LAUNCH(ctx, k_press_elems, ceil_div(m->ne, kThreads), kThreads, 0, m->ne, m->ev, m->x, m->y, us, vs, p_old,
+               gpx, gpy, mass, elem_s, dt, rho, stab, want_oss, rec.p);
+    CFA_LAUNCH(ctx, k_press_entries, ceil_div(m->nnz, kThreads), kThreads, 0, m->nnz, (const int*)m->ent_ptr.p,
+               (const int*)m->ent.p, (const int*)m->erow.p, m->ci, (const int*)m->inc.p, m->tag,
+               (const double*)rec.p, bc_now, m->bc, Kp, oss_val);
+    CFA_LAUNCH(ctx, k_press_rowsums, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->tag, (const int*)m->inc_ptr.p,
+               (const int*)m->inc.p, (const double*)rec.p, mass, bc_now, m->bc, want_oss, rhs, div, dp, inv_m);
     if (split) {
         double* sums = ctx->d_part;   // after the partials region
         CFA_PROPAGATE(ensure_partials(ctx, 2 * (size_t)row_grid(ctx, m->n, 1) + 4));

@@ -144,14 +144,17 @@ cfa_status cfa_momentum_adjoint(cfa_ctx* ctx, const cfa_mesh* mesh, const double
                                 const double* d_lambda_u, const double* d_lambda_v, double* d_g_u_old,
                                 double* d_g_v_old, double* d_g_u_prev, double* d_g_v_prev, double* d_g_p_old,
                                 double* d_g_nu_node, double* d_scalars2);
-/* Adjoint pieces of the rest of a step (no counterpart in the reference; the pressure step
- * without OSS, stab = 0, and the default p = 0 outlet). cfa_ppe_rhs_adjoint adds R^T lambda_p to
- * d_g_u, d_g_v, where rhs_p = R (u*, v*) is the PPE right-hand side -(rho/dt') (N_i, div u*) on
- * rows that are not Dirichlet. */
+/* Adjoint pieces of the rest of a step (no counterpart in the reference). cfa_ppe_rhs_adjoint adds
+ * R^T lambda_p to d_g_u, d_g_v, where rhs_p = R (u*, v*) is the PPE right-hand side
+ * -(rho/dt') (N_i, div u*) after the pressure boundary conditions of the mesh's outlet rule: with
+ * the default p = 0 outlet the Dirichlet rows' multipliers are ignored; with the pinned outlet
+ * (cfa_mesh_set_outlet) the right-hand side's mean removal is transposed as well (l - (m.l/sum m)
+ * on every row, l = lambda_p zeroed at the pin; synchronises in that case). lambda_p is the
+ * pressure solve's adjoint. */
 cfa_status cfa_ppe_rhs_adjoint(cfa_ctx* ctx, const cfa_mesh* mesh, const double* d_lambda_p, double dt_proj,
                                double rho, double* d_g_u, double* d_g_v);
-/* Adjoint of the OSS terms of the pressure step (stab > 0, the default p = 0 outlet; no
- * counterpart in the reference). Given the pressure adjoint lambda (the solution of A lambda = g
+/* Adjoint of the OSS terms of the pressure step (stab > 0, either outlet rule; no counterpart in
+ * the reference). Given the pressure adjoint lambda (the solution of A lambda = g
  * with g zeroed on Dirichlet rows, A the step's operator (1 + s) K - B^T M^-1 B), the step's u*,
  * its OSS weights d_elem_s (cfa_oss_weights), p^n and the solution dp, adds the derivatives of
  * lambda^T (rhs_p - A dp) through the weights to d_g_u, d_g_v (u*, v*) and through the OSS
@@ -412,6 +415,12 @@ cfa_status cfa_amg_level(const cfa_amg* amg, int l, int* info, const int** d_agg
 cfa_status cfa_amg_phases(const cfa_amg* amg, double* ms8);
 /* dense inverse of the coarsest operator (device, coarse_n^2 FP64, row-major) */
 cfa_status cfa_amg_coarse_inverse(const cfa_amg* amg, const double** d_inv);
+/* The composite coarse operator (no counterpart in the reference): the V-cycle below a small
+ * level (the first level l >= 1 with at most 2048 rows; CFA_COMPOSITE_ROWS overrides, 0 turns it
+ * off) is one linear map of that level's right-hand side, formed at setup as a dense row-major
+ * FP64 matrix (rows x rows) and applied as one matrix-vector product. *level = -1 when none.
+ * d_m may be NULL. */
+cfa_status cfa_amg_composite(const cfa_amg* amg, int* level, int* rows, const double** d_m);
 
 /* The assembled OSS term of the pressure operator (apply_oss_projection,
  * src/cfa/device.cuh:316-323): A x = K x - B^T M^-1 B x on non-Dirichlet rows. */

@@ -220,3 +220,41 @@ def test_drag_adjoint_iterative_mixed_matches_direct_fp64(stab):
     assert abs(J1 - J0) <= 1e-9 * abs(J0)
     assert torch.abs(g1 - g0).max().item() <= 1e-6 * torch.abs(g0).max().item()
     assert abs(gu1 - gu0) <= 1e-6 * abs(gu0)
+
+
+@pytest.mark.parametrize("stab", [0.0, 0.3])
+def test_drag_adjoint_pinned_outlet_matches_finite_differences(stab):
+    """The same gradient with the application's --outlet dirichlet rule: the scaled inflow parabola
+    on the outlet and the pressure increment pinned at the outlet node nearest mid-height, the
+    PPE right-hand side losing its mass-weighted mean first (src/cfa/fem_kernels.cuh:493-531).
+    Central differences (h = 1e-4 of nu, 1e-6 of U) of J with direct solves."""
+    import adjoint as AD
+    m = F.make_mesh("small")
+    u0, v0, p0, nu = _loop_inputs(m)
+    adj = AD.DragAdjoint(m, u0, v0, p0, nu, u_max=U_MAX, steps=4, dt=DT, precision=cfa.FP64, checkpoint=2,
+                         direct=True, stab=stab, outlet_dirichlet=True)
+    J, g_nu, g_u = adj.gradient()
+    assert abs(J - adj.objective()) <= 1e-12 * abs(J)
+    rng = np.random.default_rng(9)
+    base = adj.nu_node.clone()
+    for _ in range(2):
+        delta = dev(rng.standard_normal(m.n)) * 1e-3
+        h = 1e-4
+        adj.nu_node = base + h * delta
+        jp = adj.objective()
+        adj.nu_node = base - h * delta
+        jm = adj.objective()
+        adj.nu_node = base
+        fd = (jp - jm) / (2 * h)
+        ad = float(torch.dot(g_nu, delta))
+        assert abs(ad - fd) <= 1e-6 * abs(fd) + 1e-9 * abs(J), (ad, fd)
+    h = 1e-6 * U_MAX
+    fd = (adj.objective(U_MAX + h) - adj.objective(U_MAX - h)) / (2 * h)
+    assert abs(g_u - fd) <= 1e-6 * abs(fd), (g_u, fd)
+    # the iterative path (FP32 preconditioners, PCG on the pinned operator) agrees with it
+    it = AD.DragAdjoint(m, u0, v0, p0, nu, u_max=U_MAX, steps=4, dt=DT, precision=cfa.MIXED, checkpoint=2,
+                        tol=1e-12, stab=stab, outlet_dirichlet=True)
+    J1, g1, gu1 = it.gradient()
+    assert abs(J1 - J) <= 1e-9 * abs(J)
+    assert torch.abs(g1 - g_nu).max().item() <= 1e-6 * torch.abs(g_nu).max().item()
+    assert abs(gu1 - g_u) <= 1e-6 * abs(g_u)

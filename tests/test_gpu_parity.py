@@ -347,12 +347,14 @@ def check_hierarchy(amg, oa):
     assert np.array_equal(host(amg.coarse_inverse()), inv)
 
 
+@pytest.mark.parametrize("agg", ["device", "host"])
 @pytest.mark.parametrize("name,which", [("small", "lap"), ("medium", "lap"), ("medium", "ppe"), ("c0", "ppe"),
                                         ("c1", "ppe")])
-def test_amg_setup_bit_exact(ctx, name, which):
-    """The device setup (strength, the aggregation rounds, smoothing, transpose, Galerkin SpGEMM,
-    coarse inverse) against the oracle's sequential host setup, bit for bit, up to the ~400k-node
-    adaptive mesh."""
+def test_amg_setup_bit_exact(ctx, name, which, agg, monkeypatch):
+    """The device setup (strength, the aggregation -- the dataflow kernels on the device, or the
+    sequential host loop --, smoothing, transpose, Galerkin SpGEMM, coarse inverse) against the
+    oracle's sequential host setup, bit for bit, up to the ~400k-node adaptive mesh."""
+    monkeypatch.setenv("CFA_AGG_HOST", "0" if agg == "device" else "1")
     m = mesh(name)
     rp, ci = O.csr_build(m.n, m.elem_v)
     if which == "lap":
@@ -377,6 +379,50 @@ def test_amg_setup_bit_exact(ctx, name, which):
     z32 = torch.zeros(m.n, dtype=torch.float64, device="cuda")
     amg32.apply(dev(r), z32)
     assert np.abs(host(z32) - zo).max() <= 1e-4 * np.abs(zo).max()
+
+
+@pytest.mark.parametrize("name", ["medium", "c1"])
+def test_vcycle_composite_and_fused_transfers_match_level_chain(ctx, name, monkeypatch):
+    """The V-cycle's two reformulations against the plain chain of level kernels: the composite
+    coarse operator (the V-cycle below the first level of at most 2048 rows formed once as a dense
+    matrix) and the fused transfers (the restricted residual R b - (R A) x in one pass, the
+    prolongation folded into the first post-smoothing sweep through [A | A P] and [I | P]), on the
+    levels >= 1 (the default) and on every level. Each sums the same terms in another order: the
+    V-cycles agree to 1e-13 relative in FP64 and 1e-5 in mixed precision, and PCG to 1e-10 takes
+    the same number of iterations within 1."""
+    from tests.golden.make_golden import oracle_pressure_matrix
+    m = mesh(name)
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    a = dev(oracle_pressure_matrix(m, rp, ci, *fields(m)))
+    drp, dci = dev(rp, torch.int32), dev(ci, torch.int32)
+    r = dev(np.sin(0.37 * np.arange(m.n)) + 0.2)
+    out = {}
+    configs = {"chain": ("0", "0"), "default": ("2048", "1"), "fused_all": ("0", "2")}
+    for cfg, (comp, fuse) in configs.items():
+        monkeypatch.setenv("CFA_COMPOSITE_ROWS", comp)
+        monkeypatch.setenv("CFA_VC_FUSE", fuse)
+        for prec in (cfa.FP64, cfa.MIXED):
+            amg = cfa.AmgPreconditioner(ctx, prec)
+            amg.setup(m.n, ci.size, drp, dci, a)
+            lv, rows = amg.composite()
+            if comp == "0":
+                assert lv == -1
+            else:
+                assert lv >= 1 and 0 < rows <= 2048
+                assert amg.level(lv)["rows"] == rows
+            z = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+            amg.apply(r, z)
+            s = cfa.GpuLinearSolver(ctx)
+            x = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+            it = s.solve_pcg(m.n, drp, dci, a, r, x, 4000, 1e-10, None, amg)
+            assert s.converged
+            out[cfg, prec] = (host(z), it, host(x))
+    for cfg in ("default", "fused_all"):
+        for prec, tol in ((cfa.FP64, 1e-13), (cfa.MIXED, 1e-5)):
+            (z1, it1, x1), (z0, it0, x0) = out[cfg, prec], out["chain", prec]
+            assert np.abs(z1 - z0).max() <= tol * np.abs(z0).max(), (cfg, prec)
+            assert abs(it1 - it0) <= 1, (cfg, prec, it1, it0)
+            assert np.abs(x1 - x0).max() <= 1e-8 * np.abs(x0).max(), (cfg, prec)
 
 
 def test_amg_matches_reference_golden(ctx):
