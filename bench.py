@@ -617,6 +617,8 @@ def run_batch(args, rank, world):
     # keep=True: every system's solution (u*, v*, dp) is read back to the host inside the timed
     # region, as a caller of the batch would
     solver = BT.BatchSolver(precision=cfa.MIXED, streams=args.streams, keep=True)
+    if args.autotune:
+        cfa.autotune(True)   # tile heights timed in the warm-up's setups, cached per pattern class
     # warm-up: whole batches (module loading, the worker contexts' first allocations)
     for _ in range(max(1, args.warmup)):
         solver.solve(systems)
@@ -657,7 +659,9 @@ def run_batch(args, rank, world):
                    "vertices_total": int(sum(r.n for r in allr)),
                    "p50_ms": round(float(np.percentile(ms, 50)), 3), "p99_ms": round(float(np.percentile(ms, 99)), 3),
                    "converged": int(sum(r.converged for r in allr)),
-                   "iterations_p_median": int(np.median([r.it_p for r in allr]))},
+                   "iterations_p_median": int(np.median([r.it_p for r in allr])),
+                   "autotune": {"on": bool(args.autotune), "classes": len(cfa.autotune_log()),
+                                "row_shifts": [rec["row_shift"] for rec in cfa.autotune_log()]}},
         "e2e": {"value": round(value, 3), "unit": "systems/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(sum(r.n for r in allr) * 24)},
         "gpu_launches": int(launches),
@@ -677,6 +681,8 @@ def main():
     ap.add_argument("--streams", type=int, default=4, help="concurrent streams per GPU (c4)")
     ap.add_argument("--stab", type=float, default=STAB,
                     help="c3: OSS pressure stabilisation of the differentiated loop (0.3, the reference's default)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="c4: time the V-cycle tile heights per pattern class (cfa_autotune_set)")
     ap.add_argument("--profile", action="store_true",
                     help="one step per precision between cudaProfilerStart/Stop (for ncu --profile-from-start off); no JSON line")
     args = ap.parse_args()

@@ -143,6 +143,21 @@ class Context:
 _default_ctx = None
 
 
+def autotune(enabled: bool = True):
+    """Turns the V-cycle tile autotuner on or off for the AMG setups that follow."""
+    lib().cfa_autotune_set(1 if enabled else 0)
+
+
+def autotune_log() -> list:
+    """The autotuner's choices so far, one dict per tuned pattern class."""
+    import json
+    n = C.c_size_t()
+    lib().cfa_autotune_log(None, 0, C.byref(n))
+    buf = C.create_string_buffer(n.value + 1)
+    lib().cfa_autotune_log(buf, n.value + 1, C.byref(n))
+    return [json.loads(line) for line in buf.value.decode().splitlines() if line.strip()]
+
+
 def default_context() -> Context:
     global _default_ctx
     if _default_ctx is None:

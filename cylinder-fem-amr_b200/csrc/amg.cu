@@ -1616,11 +1616,14 @@ __global__ void k_agg_p2(int n, const int* __restrict__ rp, const int* __restric
 // thread re-evaluates its node until it is decided. A chunk's states live in shared memory as well
 // as in global memory, so the many decisions that wait on a node of the same chunk (the mesh
 // numbering keeps conflicts close in index) take a shared-memory round trip rather than an L2 one.
+// Each evaluation reads the states of the node's lower conflicts from a precomputed list
+// (k_agg_conf_*), kAggBatch loads issued together, so one poll costs about one L2 round trip.
 // Progress: the lowest undecided node has all its lower conflicts decided, and its chunk has
 // started, because every CTA with an earlier ticket holds only lower nodes, all decided, and
 // retires. Every wait is bounded: a thread that polls kAggPollLimit times, or sees another thread
 // give up, records CFA_TIMEOUT in *err and leaves its node undecided.
 constexpr int kAggChunk = 1024;
+constexpr int kAggBatch = 16;
 constexpr unsigned kAggPollLimit = 1u << 20;
 
 struct AggView {
@@ -1633,49 +1636,65 @@ struct AggView {
     }
 };
 
-// The state node i can take from what its lower conflicts have decided so far (UNDECIDED: not
-// yet). Phase 1: a root k < i with k -> i aggregated i before its visit; so did a strong neighbour
-// j of i that is a root below i or has an in-neighbour root k < i. Phase 3 (nodes that phases 1
-// and 2 left unaggregated): i is claimed by a lower such root k -> i, and is a root once every
-// lower such in-neighbour is decided and none is a root.
-template <bool P3>
-__device__ __forceinline__ unsigned char agg_decide(int i, const int* __restrict__ rp, const int* __restrict__ ci,
-                                                    const unsigned char* __restrict__ strong,
-                                                    const int* __restrict__ trp, const int* __restrict__ tci,
-                                                    const int* __restrict__ agg2, const AggView& st) {
-    bool pending = false;
+// Phase 1's lower conflicts of node i (repeats allowed): its in-neighbours k < i (k -> i), its
+// strong neighbours j < i, and the in-neighbours k < i of each strong neighbour j (k -> j). FILL:
+// write them at conf[cptr[i]..]; else count them into cnt[i].
+template <bool FILL>
+__global__ void k_agg_conf(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                           const unsigned char* __restrict__ strong, const int* __restrict__ trp,
+                           const int* __restrict__ tci, int* __restrict__ cnt, const int* __restrict__ cptr,
+                           int* __restrict__ conf) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int o = FILL ? cptr[i] : 0;
     for (int q = trp[i]; q < trp[i + 1]; ++q) {
         const int k = tci[q];
-        if (k >= i || (P3 && agg2[k] >= 0)) continue;
-        const unsigned char sk = st(k);
-        if (sk == AGG_ROOT) return AGG_MEMBER;
-        pending |= sk == AGG_UNDECIDED;
+        if (k < i) { if (FILL) conf[o] = k; ++o; }
     }
-    if (!P3) {
-        for (int a = rp[i]; a < rp[i + 1]; ++a) {
-            if (!strong[a]) continue;
-            const int j = ci[a];
-            if (j < i) {
-                const unsigned char sj = st(j);
-                if (sj == AGG_ROOT) return AGG_MEMBER;
-                pending |= sj == AGG_UNDECIDED;
+    for (int a = rp[i]; a < rp[i + 1]; ++a) {
+        if (!strong[a]) continue;
+        const int j = ci[a];
+        if (j < i) { if (FILL) conf[o] = j; ++o; }
+        for (int q = trp[j]; q < trp[j + 1]; ++q) {
+            const int k = tci[q];
+            if (k < i) { if (FILL) conf[o] = k; ++o; }
+        }
+    }
+    if (!FILL) cnt[i] = o;
+}
+
+// The state node i can take from what its lower conflicts have decided so far (UNDECIDED: not
+// yet): a non-root as soon as one is a root, a root once all are decided non-roots. Phase 1: the
+// conflict list of k_agg_conf. Phase 3 (nodes that phases 1 and 2 left unaggregated; the others
+// hold the non-root state): the in-neighbours k < i (k -> i).
+__device__ __forceinline__ unsigned char agg_decide(int i, const int* __restrict__ list, int beg, int end,
+                                                    bool lower_only, const AggView& st) {
+    bool pending = false;
+    for (int q = beg; q < end; q += kAggBatch) {
+        unsigned char sv[kAggBatch];
+#pragma unroll
+        for (int u = 0; u < kAggBatch; ++u) {
+            sv[u] = AGG_MEMBER;
+            if (q + u < end) {
+                const int k = list[q + u];
+                if (!lower_only || k < i) sv[u] = st(k);
             }
-            for (int q = trp[j]; q < trp[j + 1]; ++q) {
-                const int k = tci[q];
-                if (k >= i) continue;
-                const unsigned char sk = st(k);
-                if (sk == AGG_ROOT) return AGG_MEMBER;
-                pending |= sk == AGG_UNDECIDED;
-            }
+        }
+#pragma unroll
+        for (int u = 0; u < kAggBatch; ++u) {
+            if (sv[u] == AGG_ROOT) return AGG_MEMBER;
+            pending |= sv[u] == AGG_UNDECIDED;
         }
     }
     return pending ? AGG_UNDECIDED : AGG_ROOT;
 }
 
+// P3 = false: phase 1 on the conflict lists (lptr, list); P3 = true: phase 3 on the in-neighbour
+// lists (lptr = trp, list = tci).
 template <bool P3>
 __global__ void __launch_bounds__(kAggChunk)
-k_agg_flow(int n, const int* __restrict__ rp, const int* __restrict__ ci, const unsigned char* __restrict__ strong,
-           const int* __restrict__ trp, const int* __restrict__ tci, const int* __restrict__ agg2, unsigned char* st,
+k_agg_flow(int n, const int* __restrict__ lptr, const int* __restrict__ list, unsigned char* st,
            int* __restrict__ ticket, int* err) {
     CFA_GRID_DEP();
     __shared__ int s_chunk;
@@ -1689,8 +1708,9 @@ k_agg_flow(int n, const int* __restrict__ rp, const int* __restrict__ ci, const 
     __syncthreads();
     const AggView view{st, s_st, base};
     volatile int* verr = err;
+    const int beg = i < n ? lptr[i] : 0, end = i < n ? lptr[i + 1] : 0;
     for (unsigned it = 0; mine == AGG_UNDECIDED; ++it) {
-        mine = agg_decide<P3>(i, rp, ci, strong, trp, tci, agg2, view);
+        mine = agg_decide(i, list, beg, end, P3, view);
         if (mine != AGG_UNDECIDED) {
             s_st[threadIdx.x] = mine;
             *reinterpret_cast<volatile unsigned char*>(st + i) = mine;
@@ -1773,13 +1793,24 @@ static cfa_status aggregate_device(cfa_ctx* ctx, SetupScratch& S, const DCsr& A,
     CFA_CUDA(cudaMemsetAsync(S.ag_fill.p, 0, (n + 1) * sizeof(int), ctx->stream));
     CFA_LAUNCH(ctx, k_strong_fill, g, kThreads, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p,
                (const int*)S.ag_trp.p, S.ag_fill.p, S.ag_tci.p);
+    // phase 1's conflict lists
+    CFA_CUDA(S.ag_cptr.ensure(n + 1));
+    CFA_LAUNCH(ctx, k_agg_conf<false>, g, kThreads, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p,
+               (const int*)S.ag_trp.p, (const int*)S.ag_tci.p, S.ag_fill.p, (const int*)nullptr, (int*)nullptr);
+    CFA_CUDA(cudaMemsetAsync(S.ag_fill.p + n, 0, sizeof(int), ctx->stream));
+    CFA_PROPAGATE(exclusive_sum(ctx, S, S.ag_fill.p, S.ag_cptr.p, n));
+    int nconf = 0;
+    CFA_CUDA(cudaMemcpyAsync(&nconf, S.ag_cptr.p + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    CFA_CUDA(S.ag_conf.ensure(std::max(nconf, 1)));
+    CFA_LAUNCH(ctx, k_agg_conf<true>, g, kThreads, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p,
+               (const int*)S.ag_trp.p, (const int*)S.ag_tci.p, (int*)nullptr, (const int*)S.ag_cptr.p, S.ag_conf.p);
     // phase 1 (ag_flag: [0] chunk tickets, [1] error status)
     const int chunks = ceil_div(n, kAggChunk);
     CFA_CUDA(cudaMemsetAsync(S.ag_state.p, AGG_UNDECIDED, n, ctx->stream));
     CFA_CUDA(cudaMemsetAsync(S.ag_flag.p, 0, 2 * sizeof(int), ctx->stream));
-    CFA_LAUNCH(ctx, k_agg_flow<false>, chunks, kAggChunk, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p,
-               (const int*)S.ag_trp.p, (const int*)S.ag_tci.p, (const int*)nullptr, S.ag_state.p, S.ag_flag.p,
-               S.ag_flag.p + 1);
+    CFA_LAUNCH(ctx, k_agg_flow<false>, chunks, kAggChunk, 0, n, (const int*)S.ag_cptr.p, (const int*)S.ag_conf.p,
+               S.ag_state.p, S.ag_flag.p, S.ag_flag.p + 1);
     CFA_LAUNCH(ctx, k_agg_is_root, g1, kThreads, 0, n, (const unsigned char*)S.ag_state.p, S.ag_fill.p);
     CFA_PROPAGATE(exclusive_sum(ctx, S, S.ag_fill.p, S.ag_rank.p, n));
     CFA_LAUNCH(ctx, k_agg_p1_ids, g, kThreads, 0, n, (const int*)S.ag_trp.p, (const int*)S.ag_tci.p,
@@ -1790,9 +1821,8 @@ static cfa_status aggregate_device(cfa_ctx* ctx, SetupScratch& S, const DCsr& A,
     // phase 3 (the number of phase-1 aggregates first: the ids continue from it)
     CFA_CUDA(cudaMemcpyAsync(S.h_ag.p + 1, S.ag_rank.p + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaMemsetAsync(S.ag_flag.p, 0, sizeof(int), ctx->stream));
-    CFA_LAUNCH(ctx, k_agg_flow<true>, chunks, kAggChunk, 0, n, A.rp.p, A.ci.p, (const unsigned char*)S.strong.p,
-               (const int*)S.ag_trp.p, (const int*)S.ag_tci.p, (const int*)S.ag_agg2.p, S.ag_state.p, S.ag_flag.p,
-               S.ag_flag.p + 1);
+    CFA_LAUNCH(ctx, k_agg_flow<true>, chunks, kAggChunk, 0, n, (const int*)S.ag_trp.p, (const int*)S.ag_tci.p,
+               S.ag_state.p, S.ag_flag.p, S.ag_flag.p + 1);
     CFA_CUDA(cudaMemcpyAsync(S.h_ag.p + 2, S.ag_flag.p + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     if (S.h_ag.p[2] != 0)
@@ -2016,7 +2046,11 @@ static cfa_status build_fused(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb) {
     SetupScratch& S = amg->scratch;
     const int n = L.A.rows, nc = L.R.rows;
     CFA_PROPAGATE(spgemm(ctx, S, nc, n, L.R.rp.p, L.R.ci.p, L.R.v.p, L.A.rp.p, L.A.ci.p, L.A.v.p, S.fRA));
-    CFA_PROPAGATE(spgemm(ctx, S, n, L.P.cols, L.A.rp.p, L.A.ci.p, L.A.v.p, L.P.rp.p, L.P.ci.p, L.P.v.p, S.fAP));
+    // A P: the Galerkin product's, unless a remap changed P since
+    const bool keep_ap = L.AP.rows == n && L.AP.cols == L.P.cols && L.AP.nnz > 0;
+    if (!keep_ap)
+        CFA_PROPAGATE(spgemm(ctx, S, n, L.P.cols, L.A.rp.p, L.A.ci.p, L.A.v.p, L.P.rp.p, L.P.ci.p, L.P.v.p, S.fAP));
+    const DCsr& AP = keep_ap ? L.AP : S.fAP;
     // Q
     DCsr& Q = S.fQ;
     Q.rows = nc;
@@ -2036,7 +2070,7 @@ static cfa_status build_fused(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb) {
     CFA_CUDA(S.fcnt.ensure(n + 1));
     CFA_CUDA(W.rp.ensure(n + 1));
     CFA_LAUNCH(ctx, k_fuse_w<false>, ceil_div(n, kThreads), kThreads, 0, n, (const int*)L.A.rp.p, (const int*)L.A.ci.p,
-               (const double*)L.A.v.p, (const int*)S.fAP.rp.p, (const int*)S.fAP.ci.p, (const double*)S.fAP.v.p,
+               (const double*)L.A.v.p, (const int*)AP.rp.p, (const int*)AP.ci.p, (const double*)AP.v.p,
                (const int*)L.P.rp.p, (const int*)L.P.ci.p, (const double*)L.P.v.p, S.fcnt.p, (const int*)nullptr,
                (int*)nullptr, (double*)nullptr, (double*)nullptr);
     CFA_CUDA(cudaMemsetAsync(S.fcnt.p + n, 0, sizeof(int), ctx->stream));
@@ -2051,12 +2085,108 @@ static cfa_status build_fused(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb) {
     CFA_CUDA(W.v.ensure(std::max(total, 1)));
     CFA_CUDA(S.fW1.ensure(std::max(total, 1)));
     CFA_LAUNCH(ctx, k_fuse_w<true>, ceil_div(n, kThreads), kThreads, 0, n, (const int*)L.A.rp.p, (const int*)L.A.ci.p,
-               (const double*)L.A.v.p, (const int*)S.fAP.rp.p, (const int*)S.fAP.ci.p, (const double*)S.fAP.v.p,
+               (const double*)L.A.v.p, (const int*)AP.rp.p, (const int*)AP.ci.p, (const double*)AP.v.p,
                (const int*)L.P.rp.p, (const int*)L.P.ci.p, (const double*)L.P.v.p, (int*)nullptr,
                (const int*)W.rp.p, W.ci.p, W.v.p, S.fW1.p);
     CFA_PROPAGATE(pack_from_device(ctx, amg, W, W.v.p, S.fW1.p, vb, L.tW));
     CFA_CHECK_LAUNCH();
     L.fused = true;
+    return CFA_OK;
+}
+
+// ---- autotuner for the tile heights of the V-cycle's matrices (tiled.cuh) ----
+// Mean time of one launch of operation OP on the tiles M (3 untimed launches first), in us.
+template <int OP, class V, class T>
+static double time_tile_op(cfa_ctx* ctx, const TiledCsr& M, int* err, const T* dinv, const T* b, const T* x, T* y,
+                           const T* xc) {
+    constexpr int kReps = 10;
+    vct<OP, V, T, T, T>(ctx, true, M, err, dinv, (T)0.5, b, x, y, nullptr, nullptr, xc);
+    for (int k = 0; k < 3; ++k) vct<OP, V, T, T, T>(ctx, false, M, err, dinv, (T)0.5, b, x, y, nullptr, nullptr, xc);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, ctx->stream);
+    for (int k = 0; k < kReps; ++k) vct<OP, V, T, T, T>(ctx, false, M, err, dinv, (T)0.5, b, x, y, nullptr, nullptr, xc);
+    cudaEventRecord(e1, ctx->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return 1e3 * ms / kReps;
+}
+
+// One matrix: the cached choice of its pattern class, or the candidates timed and the fastest
+// kept; T is re-planned and re-packed when the choice is not the default height.
+template <class V, class T>
+static cfa_status tune_one(cfa_ctx* ctx, cfa_amg* amg, const char* kind, int op, const DCsr& M, const double* v0,
+                           const double* v1, int vb, TiledCsr& tiles, const T* dinv, T* const* vec) {
+    const int nvals = v1 ? 2 : 1;
+    HostBuf<int>& hr = amg->scratch.h_rp;
+    auto replan = [&](TiledCsr& dst, int shift) -> cfa_status {
+        CFA_CUDA(hr.ensure(M.rows + 1));
+        CFA_CUDA(cudaMemcpyAsync(hr.p, M.rp.p, (M.rows + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+        const cfa_status st = plan_tiled(ctx, hr.p, M.rows, nvals, vb, dst, shift);
+        if (st != CFA_OK) return st;
+        return pack_tiled(ctx, M.rp.p, M.ci.p, v0, v1, nullptr, dst);
+    };
+    int best = 0;
+    if (!autotune_lookup(kind, vb, nvals, M.rows, M.nnz, &best)) {
+        int* err = amg->err.p;
+        const int cand[4] = {-2, -1, 0, 1};
+        double us[4];
+        int shifts[4], nc = 0;
+        double best_us = 0.0;
+        for (int c : cand) {
+            TiledCsr trial;
+            const TiledCsr* use = &tiles;
+            if (c != 0) {
+                if (replan(trial, c) != CFA_OK) continue;
+                use = &trial;
+            }
+            double t = 0.0;
+            switch (op) {
+                case VC_JAC: t = time_tile_op<VC_JAC, V, T>(ctx, *use, err, dinv, vec[0], vec[1], vec[2], nullptr); break;
+                case VC_ADD: t = time_tile_op<VC_ADD, V, T>(ctx, *use, err, dinv, nullptr, vec[3], vec[2], nullptr); break;
+                case VC_SPMV: t = time_tile_op<VC_SPMV, V, T>(ctx, *use, err, dinv, nullptr, vec[1], vec[2], nullptr); break;
+                case VC_RESTRICT: t = time_tile_op<VC_RESTRICT, V, T>(ctx, *use, err, dinv, vec[0], vec[1], vec[2], nullptr); break;
+                default: t = time_tile_op<VC_ADDJAC, V, T>(ctx, *use, err, dinv, vec[0], vec[1], vec[2], vec[3]); break;
+            }
+            CFA_CHECK_LAUNCH();
+            if (nc == 0 || t < best_us) { best_us = t; best = c; }
+            us[nc] = t;
+            shifts[nc++] = c;
+        }
+        autotune_store(kind, vb, nvals, M.rows, M.nnz, best, us, shifts, nc);
+    }
+    if (best != 0) CFA_PROPAGATE(replan(tiles, best));
+    return CFA_OK;
+}
+
+// The tile heights of a level's matrices whose kernels carry no reduction: every matrix of the
+// levels >= 1, and level 0's transfers (level 0's A carries the CG's dots in its last sweep).
+template <class V, class T>
+static cfa_status tune_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb) {
+    const bool lv0 = &L == &amg->levels[0];
+    const int n = L.A.rows, nc = L.R.rows;
+    DevBuf<T> buf;
+    const size_t len = (size_t)std::max(n, nc) + 1;
+    CFA_CUDA(buf.ensure(4 * len));
+    CFA_CUDA(cudaMemsetAsync(buf.p, 0, 4 * len * sizeof(T), ctx->stream));
+    T* vec[4] = {buf.p, buf.p + len, buf.p + 2 * len, buf.p + 3 * len};   // b, x, y, coarse x
+    const T* dinv = std::is_same<T, float>::value ? (const T*)(const void*)L.dinv32.p : (const T*)(const void*)L.dinv.p;
+    auto vals = [&](const DCsr& M) { return (const double*)M.v.p; };
+    if (!lv0) CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "A", VC_JAC, L.A, vals(L.A), nullptr, vb, L.tA, dinv, vec)));
+    if (L.fused) {
+        SetupScratch& S = amg->scratch;
+        CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "Q", VC_RESTRICT, S.fQ, S.fQ.v.p, nullptr, vb, L.tQ, dinv, vec)));
+        CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "W", VC_ADDJAC, S.fW, S.fW.v.p, S.fW1.p, vb, L.tW, dinv, vec)));
+    } else {
+        CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "P", VC_ADD, L.P, vals(L.P), nullptr, vb, L.tP, dinv, vec)));
+        CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "R", VC_SPMV, L.R, vals(L.R), nullptr, vb, L.tR, dinv, vec)));
+    }
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));   // buf is released on return
     return CFA_OK;
 }
 
@@ -2079,6 +2209,12 @@ static cfa_status prepare_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L) {
     if (!amg->tiled) return CFA_OK;
     const int vb = o.precision == CFA_MIXED ? 4 : 8;
     L.fused = false;
+    // levels the composite operator replaces run no tile kernel
+    const int l = (int)(&L - &amg->levels[0]);
+    if (amg->comp_level >= 0 && l >= amg->comp_level) {
+        if (o.precision == CFA_MIXED) CFA_PROPAGATE(level_vectors(ctx, amg, L, L.A.rows));
+        return level_vectors64(ctx, L, L.A.rows);
+    }
     if (fuse_level(amg, L)) CFA_PROPAGATE(build_fused(ctx, amg, L, vb));
     for (DCsr* M : {&L.A, &L.P, &L.R}) {
         TiledCsr& T = M == &L.A ? L.tA : M == &L.P ? L.tP : L.tR;
@@ -2090,7 +2226,13 @@ static cfa_status prepare_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L) {
         CFA_PROPAGATE(pack_tiled(ctx, M->rp.p, M->ci.p, M->v.p, nullptr, nullptr, T));
     }
     if (o.precision == CFA_MIXED) CFA_PROPAGATE(level_vectors(ctx, amg, L, L.A.rows));   // FP32 V-cycle vectors
-    return level_vectors64(ctx, L, L.A.rows);
+    CFA_PROPAGATE(level_vectors64(ctx, L, L.A.rows));
+    if (autotune_enabled()) {
+        if (o.precision != CFA_MIXED) CFA_PROPAGATE((tune_level<double, double>(ctx, amg, L, vb)));
+        else if (vcycle_fp32(amg)) CFA_PROPAGATE((tune_level<float, float>(ctx, amg, L, vb)));
+        else CFA_PROPAGATE((tune_level<float, double>(ctx, amg, L, vb)));
+    }
+    return CFA_OK;
 }
 
 // The V-cycle's coarse tail plan, and the kernels' shared-memory limits raised now, outside any
@@ -2291,6 +2433,7 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
         DCsr& AP = S.AP;
         CFA_PROPAGATE(spgemm(ctx, S, m, na, A.rp.p, A.ci.p, A.v.p, L.P.rp.p, L.P.ci.p, L.P.v.p, AP));
         CFA_PROPAGATE(spgemm(ctx, S, na, na, L.R.rp.p, L.R.ci.p, L.R.v.p, AP.rp.p, AP.ci.p, AP.v.p, next.A));
+        std::swap(L.AP, S.AP);   // kept for the level's fused transfers
         phase(5);
         L.omega = omega;
         CFA_PROPAGATE(level_vectors(ctx, amg, L, m));
@@ -2435,6 +2578,7 @@ static cfa_status amg_remap(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
     }
     // level 0: new operator, inverse diagonal, P (uploaded), R = P^T
     amg->version = next_uid();
+    L.AP.rows = 0;   // A P of the old level 0 no longer holds
     L.P.rows = n;
     L.P.nnz = pnnz;
     CFA_CUDA(L.P.rp.ensure(n + 1));

@@ -25,6 +25,7 @@ struct AmgLevel {
     // vector (x, resp. the coarse correction)
     TiledCsr tQ, tW;
     bool fused = false;
+    DCsr AP;                       // A P of the Galerkin product (rows 0 after a remap changed P)
     DevBuf<double> dinv;
     DevBuf<float> dinv32;
     double omega = 0.0;
@@ -68,7 +69,7 @@ struct SetupScratch {
     DevBuf<long long> sg_off;
     DevBuf<double> sg_sval, pow_x, pow_y, pow_py, pow_px, pow_st, p0v, M, colbuf;
     DevBuf<unsigned char> strong;
-    DevBuf<int> ag_trp, ag_tci, ag_fill, ag_rank, ag_agg1, ag_agg2, ag_size, ag_flag;   // device aggregation
+    DevBuf<int> ag_trp, ag_tci, ag_fill, ag_rank, ag_agg1, ag_agg2, ag_size, ag_flag, ag_cptr, ag_conf;   // device aggregation
     DevBuf<unsigned char> ag_state;
     HostBuf<int> h_ag;                  // flag / totals read back by the aggregation rounds
     DevBuf<char> cub_tmp;

@@ -47,109 +47,142 @@ __device__ __forceinline__ double momentum_bc_u(int tag, double yi, double u_max
     return 0.0;
 }
 
-// Momentum rows: k_assemble_momentum_fem (fem_kernels.cuh:40-181) gathered per row, lumped mass,
-// and (with_bc) the Dirichlet rows of k_apply_bc_momentum (:411-453) on A and the RHS. A row of
-// up to kMomCap entries accumulates in shared memory laid out [slot][thread] (conflict-free for
-// any slot a thread adds to); longer rows in place in global memory. Same addition order.
-constexpr int kMomCap = 16;
-constexpr size_t kMomSmem = (size_t)kMomCap * kThreads * sizeof(double);
+// Momentum system: k_assemble_momentum_fem (fem_kernels.cuh:40-181), the lumped mass and (with_bc)
+// the Dirichlet rows of k_apply_bc_momentum (:411-453) on A and the RHS, in three passes as the
+// pressure system (k_press_*): an element record (geometry, SUPG tau, convective and BDF2 terms,
+// computed once per element), every CSR entry summed over its contributions, every row's mass and
+// right-hand side. Each sum takes its terms in the element order of the row's incidence, each term
+// the same expression of the same element values as a row walking its elements.
+constexpr int kMomRec = 24;   // area, dNdx[3], dNdy[3], ugN[3], tau, div_w, nu, u_h[3], v_h[3], dp/dx, dp/dy
 
-__global__ void __launch_bounds__(kThreads)
-k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x, const double* __restrict__ y,
-                const int* __restrict__ tag, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
-                const int* __restrict__ pos, const int* __restrict__ rp, const int* __restrict__ ci,
-                const double* __restrict__ u_old, const double* __restrict__ v_old,
-                const double* __restrict__ u_prev, const double* __restrict__ v_prev,
-                const double* __restrict__ p_old, const double* __restrict__ nu_node, MomParams P, int with_bc,
-                double u_max, double H, OutletBc bc, double* __restrict__ A_val, double* __restrict__ rhs_u,
-                double* __restrict__ rhs_v, double* __restrict__ mass) {
+// reciprocals of the constant and per-launch divisors (the products differ from the quotients in
+// the last bit at most; the element formula is division-bound in FP64)
+constexpr double kThird = 1.0 / 3.0, kSixth = 1.0 / 6.0, kTwelfth = 1.0 / 12.0;
+
+__global__ void k_mom_elems(int ne, const int* __restrict__ ev, const double* __restrict__ x,
+                            const double* __restrict__ y, const double* __restrict__ u_old,
+                            const double* __restrict__ v_old, const double* __restrict__ u_prev,
+                            const double* __restrict__ v_prev, const double* __restrict__ p_old,
+                            const double* __restrict__ nu_node, MomParams P, double* __restrict__ rec) {
+    CFA_GRID_DEP();
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    int nd[3];
+    load_elem(ev, e, nd);
+    const Geom g = elem_geom(nd, x, y);
+    double* r = rec + (size_t)kMomRec * e;
+    r[0] = g.area;
+    if (!g.ok) return;
+    const double area = g.area;
+    const double inv_rho = 1.0 / P.rho, term_t = 2.0 / P.tau_time;
+    double w_u = 0.0, w_v = 0.0, div_w = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double un = u_old[nd[k]], vn = v_old[nd[k]], um = u_prev[nd[k]], vm = v_prev[nd[k]];
+        r[13 + k] = P.a1 * un + P.a2 * um;
+        r[16 + k] = P.a1 * vn + P.a2 * vm;
+        const double wu = P.c1 * un + P.c2 * um, wv = P.c1 * vn + P.c2 * vm;
+        w_u += wu * kThird;
+        w_v += wv * kThird;
+        div_w += wu * g.dNdx[k] + wv * g.dNdy[k];
+    }
+    const double vel_mag = sqrt(w_u * w_u + w_v * w_v) + 1.0e-12;
+    const double h_K = sqrt(2.0 * area);
+    // element viscosity: the scalar nu, or the mean of a nodal field
+    const double nu = nu_node ? (nu_node[nd[0]] + nu_node[nd[1]] + nu_node[nd[2]]) * kThird : P.nu;
+    const double term_c = 2.0 * vel_mag / h_K;
+    const double term_d = 4.0 * nu / (h_K * h_K);
+    const double tau_supg = 1.0 / sqrt(term_t * term_t + term_c * term_c + 9.0 * term_d * term_d);
+    const double p0 = p_old[nd[0]], p1 = p_old[nd[1]], p2 = p_old[nd[2]];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        r[1 + k] = g.dNdx[k];
+        r[4 + k] = g.dNdy[k];
+        r[7 + k] = w_u * g.dNdx[k] + w_v * g.dNdy[k];
+    }
+    r[10] = tau_supg;
+    r[11] = div_w;
+    r[12] = nu;
+    r[19] = (p0 * g.dNdx[0] + p1 * g.dNdx[1] + p2 * g.dNdx[2]) * inv_rho;
+    r[20] = (p0 * g.dNdy[0] + p1 * g.dNdy[1] + p2 * g.dNdy[2]) * inv_rho;
+}
+
+// M_ij + Ms_ij and A_ij of element record r for local row vertex a and column vertex j
+__device__ __forceinline__ double mom_A(const double* __restrict__ r, int a, int j, const MomParams& P,
+                                        double* MMs) {
+    const double area = r[0], area3 = area * kThird;
+    const double M_ij = (a == j) ? (area * kSixth) : (area * kTwelfth);
+    const double K_ij = area * (r[1 + a] * r[1 + j] + r[4 + a] * r[4 + j]);
+    const double C_ij = area3 * r[7 + j] + P.skew_coef * r[11] * M_ij;
+    const double S_ij = area * r[10] * r[7 + a] * r[7 + j];
+    const double Ms_ij = area3 * r[10] * r[7 + a];
+    *MMs = M_ij + Ms_ij;
+    return P.a0 * (M_ij + Ms_ij) + r[12] * K_ij + C_ij + S_ij;
+}
+
+__global__ void k_mom_entries(int nnz, const int* __restrict__ ent_ptr, const int* __restrict__ ent,
+                              const int* __restrict__ erow, const int* __restrict__ ci, const int* __restrict__ inc,
+                              const int* __restrict__ tag, const double* __restrict__ rec, MomParams P, int with_bc,
+                              OutletBc bc, double* __restrict__ A_val) {
+    CFA_GRID_DEP();
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nnz) return;
+    const int i = erow[p];
+    if (with_bc && momentum_dirichlet(tag[i], bc)) {
+        A_val[p] = (ci[p] == i) ? 1.0 : 0.0;
+        return;
+    }
+    double acc = 0.0;
+    for (int c = ent_ptr[p]; c < ent_ptr[p + 1]; ++c) {
+        const int code = ent[c];
+        const int sl = code >> 2, j = code & 3;
+        const int e = inc[sl] >> 2, a = inc[sl] & 3;
+        const double* r = rec + (size_t)kMomRec * e;
+        if (r[0] < 1.0e-14) continue;
+        double mms;
+        acc += mom_A(r, a, j, P, &mms);
+    }
+    A_val[p] = acc;
+}
+
+__global__ void k_mom_rowsums(int n, const double* __restrict__ y, const int* __restrict__ tag,
+                              const int* __restrict__ inc_ptr, const int* __restrict__ inc,
+                              const double* __restrict__ rec, MomParams P, int with_bc, double u_max, double H,
+                              OutletBc bc, double* __restrict__ rhs_u, double* __restrict__ rhs_v,
+                              double* __restrict__ mass) {
     CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int r0 = rp[i], len = rp[i + 1] - r0;
     const bool dir = with_bc && momentum_dirichlet(tag[i], bc);
-    const bool local = len <= kMomCap;
-    extern __shared__ double mom_sm[];   // [kMomCap][blockDim.x]
-    const int T = blockDim.x;
-    double* acc = mom_sm + threadIdx.x;  // acc[q * T]: entry q of this row
-    if (!dir) {
-        if (local) {
-            for (int q = 0; q < len; ++q) acc[q * T] = 0.0;
-        } else {
-            for (int q = 0; q < len; ++q) A_val[r0 + q] = 0.0;
-        }
-    }
     double f_u_row = 0.0, f_v_row = 0.0, m_row = 0.0;
-    // reciprocals of the constant and per-launch divisors, taken once (the products differ from
-    // the quotients in the last bit at most; the element formula is division-bound in FP64)
-    constexpr double kThird = 1.0 / 3.0, kSixth = 1.0 / 6.0, kTwelfth = 1.0 / 12.0;
-    const double inv_rho = 1.0 / P.rho, term_t_p = 2.0 / P.tau_time;
     for (int s = inc_ptr[i]; s < inc_ptr[i + 1]; ++s) {
         const int e = inc[s] >> 2, a = inc[s] & 3;
-        int nd[3];
-        load_elem(ev, e, nd);
-        const Geom g = elem_geom(nd, x, y);
-        if (!g.ok) continue;
-        const double area = g.area;
+        const double* r = rec + (size_t)kMomRec * e;
+        const double area = r[0];
+        if (area < 1.0e-14) continue;
         const double area3 = area * kThird;
         m_row += area3;
         if (dir) continue;
-        double u_h[3], v_h[3], w_u = 0.0, w_v = 0.0, div_w = 0.0;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const double un = u_old[nd[k]], vn = v_old[nd[k]], um = u_prev[nd[k]], vm = v_prev[nd[k]];
-            u_h[k] = P.a1 * un + P.a2 * um;
-            v_h[k] = P.a1 * vn + P.a2 * vm;
-            const double wu = P.c1 * un + P.c2 * um, wv = P.c1 * vn + P.c2 * vm;
-            w_u += wu * kThird;
-            w_v += wv * kThird;
-            div_w += wu * g.dNdx[k] + wv * g.dNdy[k];
-        }
-        const double vel_mag = sqrt(w_u * w_u + w_v * w_v) + 1.0e-12;
-        const double h_K = sqrt(2.0 * area);
-        // element viscosity: the scalar nu, or the mean of a nodal field
-        const double nu = nu_node ? (nu_node[nd[0]] + nu_node[nd[1]] + nu_node[nd[2]]) * kThird : P.nu;
-        const double term_t = term_t_p;
-        const double term_c = 2.0 * vel_mag / h_K;
-        const double term_d = 4.0 * nu / (h_K * h_K);
-        const double tau_supg = 1.0 / sqrt(term_t * term_t + term_c * term_c + 9.0 * term_d * term_d);
-        const double p0 = p_old[nd[0]], p1 = p_old[nd[1]], p2 = p_old[nd[2]];
-        const double dpdx = (p0 * g.dNdx[0] + p1 * g.dNdx[1] + p2 * g.dNdx[2]) * inv_rho;
-        const double dpdy = (p0 * g.dNdy[0] + p1 * g.dNdy[1] + p2 * g.dNdy[2]) * inv_rho;
-        double ugN[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) ugN[k] = w_u * g.dNdx[k] + w_v * g.dNdy[k];
         double f_u = 0.0, f_v = 0.0;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            const double M_ij = (a == j) ? (area * kSixth) : (area * kTwelfth);
-            const double K_ij = area * (g.dNdx[a] * g.dNdx[j] + g.dNdy[a] * g.dNdy[j]);
-            const double C_ij = area3 * ugN[j] + P.skew_coef * div_w * M_ij;
-            const double S_ij = area * tau_supg * ugN[a] * ugN[j];
-            const double Ms_ij = area3 * tau_supg * ugN[a];
-            const double A_ij = P.a0 * (M_ij + Ms_ij) + nu * K_ij + C_ij + S_ij;
-            const int p = pos[3 * s + j];
-            if (local) acc[(p - r0) * T] += A_ij; else A_val[p] += A_ij;
-            f_u += (M_ij + Ms_ij) * u_h[j];
-            f_v += (M_ij + Ms_ij) * v_h[j];
+            double mms;
+            (void)mom_A(r, a, j, P, &mms);
+            f_u += mms * r[13 + j];
+            f_v += mms * r[16 + j];
         }
-        const double tw = area3 + area * tau_supg * ugN[a];
-        f_u -= tw * dpdx;
-        f_v -= tw * dpdy;
+        const double tw = area3 + area * r[10] * r[7 + a];
+        f_u -= tw * r[19];
+        f_v -= tw * r[20];
         f_u_row += f_u;
         f_v_row += f_v;
     }
     mass[i] = m_row;
     if (dir) {
-        const int t = tag[i];
-        const double ub = momentum_bc_u(t, y[i], u_max, H, bc);
-        for (int q = 0; q < len; ++q) A_val[r0 + q] = (ci[r0 + q] == i) ? 1.0 : 0.0;
-        rhs_u[i] = ub;
+        rhs_u[i] = momentum_bc_u(tag[i], y[i], u_max, H, bc);
         rhs_v[i] = 0.0;
         return;
     }
-    if (local)
-        for (int q = 0; q < len; ++q) A_val[r0 + q] = acc[q * T];
     rhs_u[i] = f_u_row;
     rhs_v[i] = f_v_row;
 }
@@ -446,9 +479,15 @@ cfa_status cfa_assemble_momentum_nu(cfa_ctx* ctx, const cfa_mesh* m, const doubl
     CFA_ARG(!bcp || (u && v));
     MomParams P{prm->dt, prm->nu, prm->rho, prm->a0, prm->a1, prm->a2, prm->c1, prm->c2, prm->tau_time, prm->skew_coef};
     const double u_max = bcp ? bcp->u_max : 0.0, H = bcp ? bcp->H : 1.0;
-    CFA_LAUNCH(ctx, k_momentum_rows, ceil_div(m->n, kThreads), kThreads, kMomSmem, m->n, m->ev, m->x, m->y, m->tag,
-               m->inc_ptr.p, m->inc.p, m->pos.p, m->rp, m->ci, u_old, v_old, u_prev, v_prev, p_old, nu_node, P,
-               bcp ? 1 : 0, u_max, H, m->bc, A_val, rhs_u, rhs_v, mass);
+    DevBuf<double> rec;
+    CFA_CUDA(rec.ensure((size_t)kMomRec * std::max(m->ne, 1)));
+    CFA_LAUNCH(ctx, k_mom_elems, ceil_div(m->ne, kThreads), kThreads, 0, m->ne, m->ev, m->x, m->y, u_old, v_old, u_prev,
+               v_prev, p_old, nu_node, P, rec.p);
+    CFA_LAUNCH(ctx, k_mom_entries, ceil_div(m->nnz, kThreads), kThreads, 0, m->nnz, (const int*)m->ent_ptr.p,
+               (const int*)m->ent.p, (const int*)m->erow.p, m->ci, (const int*)m->inc.p, m->tag, (const double*)rec.p,
+               P, bcp ? 1 : 0, m->bc, A_val);
+    CFA_LAUNCH(ctx, k_mom_rowsums, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->y, m->tag, (const int*)m->inc_ptr.p,
+               (const int*)m->inc.p, (const double*)rec.p, P, bcp ? 1 : 0, u_max, H, m->bc, rhs_u, rhs_v, mass);
     if (bcp)   // solution values on Dirichlet nodes after the rows (u may alias u_old)
         CFA_LAUNCH(ctx, k_momentum_bc, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->tag, m->y, m->rp, m->ci,
                    u_max, H, m->bc, 0, A_val, rhs_u, rhs_v, u, v);

@@ -1,9 +1,12 @@
 // Tile planning and packing for the tile-streamed CSR kernels (tiled.cuh).
 #include <algorithm>
+#include <cstdio>
 #include <mutex>
+#include <string>
 #include <unordered_map>
 
 #include <cstdlib>
+#include <cstring>
 
 #include "tiled.cuh"
 
@@ -47,7 +50,7 @@ __global__ void k_pack_tiles(int ntiles, const long long* __restrict__ off, cons
     }
 }
 
-cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T) {
+cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T, int row_shift) {
     const double per_row = rows > 0 ? (double)h_rp[rows] / rows : 1.0;
     int tpr = 1;
     while (tpr < 32 && per_row > (double)kGatherBatch * tpr) tpr *= 2;
@@ -71,6 +74,16 @@ cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vb
     }
     T.tpr = tpr;
     if (T.max_chunk > kTileBudget) return set_error(ctx, CFA_BAD_ARG, "matrix row too long for the tile budget", __FILE__, __LINE__);
+    if (row_shift != 0) {
+        tr = row_shift > 0 ? tr << row_shift : std::max(1, tr >> -row_shift);
+        long long mx = 0;
+        for (int r0 = 0; r0 < rows; r0 += tr) {
+            const int r1 = std::min(rows, r0 + tr);
+            mx = std::max(mx, tile_bytes(r1 - r0, h_rp[r1] - h_rp[r0], nvals, vbytes));
+        }
+        if (mx > kTileBudget) return CFA_BAD_ARG;   // not a usable candidate (no error recorded)
+        T.max_chunk = (int)mx;
+    }
     T.rows = rows;
     T.nnz = h_rp[rows];
     T.nvals = nvals;
@@ -110,6 +123,62 @@ cfa_status pack_tiled(cfa_ctx* ctx, const int* d_rp, const int* d_ci, const doub
     return CFA_OK;
 }
 
+// ---- autotuner cache and log ----
+namespace {
+struct TuneState {
+    std::mutex mu;
+    int enabled = -1;   // -1: not set, read CFA_AUTOTUNE
+    std::unordered_map<std::string, int> best;
+    std::string log;
+};
+TuneState& tune_state() {
+    static TuneState st;
+    return st;
+}
+std::string tune_key(const char* kind, int vbytes, int nvals, int rows, long long nnz) {
+    int lg = 0;
+    while ((1LL << (lg + 1)) <= rows) ++lg;
+    const long long q = rows > 0 ? (4 * nnz + rows / 2) / rows : 0;   // entries per row to a quarter
+    return std::string(kind) + "/v" + std::to_string(vbytes) + "/n" + std::to_string(nvals) + "/r2^" +
+           std::to_string(lg) + "/e" + std::to_string(q);
+}
+}  // namespace
+
+bool autotune_enabled() {
+    TuneState& st = tune_state();
+    std::lock_guard<std::mutex> lock(st.mu);
+    if (st.enabled < 0) {
+        const char* e = std::getenv("CFA_AUTOTUNE");
+        st.enabled = (e && e[0] == '1') ? 1 : 0;
+    }
+    return st.enabled == 1;
+}
+
+bool autotune_lookup(const char* kind, int vbytes, int nvals, int rows, long long nnz, int* shift) {
+    TuneState& st = tune_state();
+    std::lock_guard<std::mutex> lock(st.mu);
+    auto it = st.best.find(tune_key(kind, vbytes, nvals, rows, nnz));
+    if (it == st.best.end()) return false;
+    *shift = it->second;
+    return true;
+}
+
+void autotune_store(const char* kind, int vbytes, int nvals, int rows, long long nnz, int shift, const double* us,
+                    const int* shifts, int ncand) {
+    TuneState& st = tune_state();
+    std::lock_guard<std::mutex> lock(st.mu);
+    const std::string key = tune_key(kind, vbytes, nvals, rows, nnz);
+    st.best[key] = shift;
+    std::string line = "{\"class\": \"" + key + "\", \"rows\": " + std::to_string(rows) + ", \"nnz\": " +
+                       std::to_string(nnz) + ", \"row_shift\": " + std::to_string(shift) + ", \"us\": {";
+    for (int k = 0; k < ncand; ++k) {
+        char buf[64];
+        snprintf(buf, sizeof buf, "%s\"%d\": %.2f", k ? ", " : "", shifts[k], us[k]);
+        line += buf;
+    }
+    st.log += line + "}}\n";
+}
+
 // Waits for the previous kernel and ends: a kernel launched after it can start (and read tiles
 // before its own griddepcontrol.wait) only once every block of this one has passed its wait, so
 // whatever the kernels before this one wrote is complete and visible to it.
@@ -136,3 +205,26 @@ TileLaunch tile_launch(const cfa_ctx* ctx, const TiledCsr& T, const void*) {
 }
 
 }  // namespace cfa
+
+extern "C" {
+
+cfa_status cfa_autotune_set(int enabled) {
+    cfa::TuneState& st = cfa::tune_state();
+    std::lock_guard<std::mutex> lock(st.mu);
+    st.enabled = enabled ? 1 : 0;
+    return CFA_OK;
+}
+
+cfa_status cfa_autotune_log(char* buf, size_t cap, size_t* len) {
+    cfa::TuneState& st = cfa::tune_state();
+    std::lock_guard<std::mutex> lock(st.mu);
+    if (len) *len = st.log.size();
+    if (buf && cap) {
+        const size_t k = std::min(cap - 1, st.log.size());
+        memcpy(buf, st.log.data(), k);
+        buf[k] = '\0';
+    }
+    return CFA_OK;
+}
+
+}  // extern "C"

@@ -77,7 +77,23 @@ __host__ __device__ inline long long tile_bytes(int nr, int ne, int nvals, int v
 // with at most about kGatherBatch entries per lane on average, raised until a tile of
 // kTileThreads / tpr rows fits kTileBudget (at tpr = 32 the tile rows are halved instead).
 // Allocates the device buffers (the pattern and values are packed by pack_tiled).
-cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T);
+// row_shift != 0 scales the rows of a tile by 2^row_shift (lanes per row unchanged, so every row's
+// sum keeps its order); CFA_BAD_ARG when such a tile would exceed the budget.
+cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vbytes, TiledCsr& T, int row_shift = 0);
+
+// ---------------------------------------------------------------------------------------------
+// Autotuner (off unless cfa_autotune_set(1) or CFA_AUTOTUNE=1). For a tiled matrix whose kernels
+// carry no fused reduction, it times the tile heights 2^k * (kTileThreads / lanes per row),
+// k in {-2, -1, 0, 1}, on the kernel that reads the matrix and keeps the fastest. Lanes per row
+// stay those of the row-length rule, so the results do not depend on the choice. Choices are
+// cached per pattern class (kind, precision, value arrays, log2 rows, entries per row to a
+// quarter) for the life of the process and logged (cfa_autotune_log).
+// ---------------------------------------------------------------------------------------------
+bool autotune_enabled();
+// The cached row shift of a pattern class, if any.
+bool autotune_lookup(const char* kind, int vbytes, int nvals, int rows, long long nnz, int* shift);
+void autotune_store(const char* kind, int vbytes, int nvals, int rows, long long nnz, int shift,
+                    const double* us, const int* shifts, int ncand);
 
 // Packs pattern + values (FP64 sources; converted to float when vbytes == 4) into T.
 // A NULL source leaves its value section to be filled by its producer. Asynchronous; ends with

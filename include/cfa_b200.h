@@ -72,6 +72,19 @@ cfa_status cfa_ctx_sync(cfa_ctx* ctx);
 cfa_status cfa_mem_trim(cfa_ctx* ctx);
 cfa_status cfa_mem_cached(size_t* device_bytes, size_t* pinned_bytes);
 
+/* Autotuner of the V-cycle's tile heights (replaces, where it is on, the fixed shapes of the
+ * reference's csr_threads_per_row rule, src/cfa/linalg.cuh:918-927, for the matrices it tunes).
+ * Off by default; cfa_autotune_set(1) or CFA_AUTOTUNE=1 turns it on for the AMG setups that
+ * follow. For each tile-streamed matrix of the hierarchy whose kernel carries no reduction (every
+ * matrix of the levels >= 1, and level 0's transfers), it times tiles of 1/4, 1/2, 1 and 2 times
+ * the default height on that kernel and keeps the fastest; lanes per row are not changed, so
+ * every result is bit for bit the one of the default shapes. Choices are cached per pattern
+ * class for the life of the process. cfa_autotune_log copies the log (one JSON object per line:
+ * class, rows, nnz, chosen row_shift, the microseconds per candidate) into buf (cap bytes,
+ * NUL-terminated) and its full length into *len. */
+cfa_status cfa_autotune_set(int enabled);
+cfa_status cfa_autotune_log(char* buf, size_t cap, size_t* len);
+
 /* ---------------------------------------------------------------------------------------------
  * CSR pattern of the P1 mesh graph: node i's row holds i and the vertices of its elements,
  * sorted and unique. Replaces build_csr_and_boundary_topology (src/cfa/mesh.cuh:198-249).

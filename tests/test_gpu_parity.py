@@ -425,6 +425,40 @@ def test_vcycle_composite_and_fused_transfers_match_level_chain(ctx, name, monke
             assert np.abs(x1 - x0).max() <= 1e-8 * np.abs(x0).max(), (cfg, prec)
 
 
+@pytest.mark.parametrize("prec", [cfa.FP64, cfa.MIXED])
+def test_autotuned_tiles_give_the_same_vcycle_bits(ctx, prec):
+    """The tile-height autotuner changes which CTA streams which rows, never a row's own sum: the
+    V-cycle through a tuned hierarchy equals the default one bit for bit. Its choices are logged
+    per pattern class, and a second setup of the same matrix takes them from the cache."""
+    from tests.golden.make_golden import oracle_pressure_matrix
+    m = mesh("c0")
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    a = dev(oracle_pressure_matrix(m, rp, ci, *fields(m)))
+    drp, dci = dev(rp, torch.int32), dev(ci, torch.int32)
+    r = dev(np.sin(0.37 * np.arange(m.n)) + 0.2)
+    zs = []
+    try:
+        for tune in (False, True, True):
+            cfa.autotune(tune)
+            n_log = len(cfa.autotune_log())
+            amg = cfa.AmgPreconditioner(ctx, prec)
+            amg.setup(m.n, ci.size, drp, dci, a)
+            z = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+            amg.apply(r, z)
+            zs.append(host(z))
+            if tune:
+                log = cfa.autotune_log()
+                if len(zs) == 2:
+                    assert len(log) > n_log
+                    for rec in log[n_log:]:
+                        assert rec["row_shift"] in (-2, -1, 0, 1) and str(rec["row_shift"]) in rec["us"]
+                else:
+                    assert len(log) == n_log   # every class cached
+    finally:
+        cfa.autotune(False)
+    assert np.array_equal(zs[0], zs[1]) and np.array_equal(zs[0], zs[2])
+
+
 def test_amg_matches_reference_golden(ctx):
     for name in ("tiny", "small"):
         g = golden(f"ref_host_{name}.npz")
