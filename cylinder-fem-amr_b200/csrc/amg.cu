@@ -757,7 +757,10 @@ __global__ void k_vc_spmv(int n, const int* __restrict__ rp, const int* __restri
     ROW_LOOP_END
 }
 
-// x = A_c^-1 b with the stored FP64 inverse, one warp per row (k_dense_matvec, :929-937)
+// x = M b with a dense row-major FP64 matrix (the coarsest inverse, k_dense_matvec, :929-937, or
+// the composite operator), one warp per row. A lane takes the columns lane + 32 k; eight of its
+// loads are issued before they are summed (eight partial sums, combined in a fixed order), so a
+// row costs a few L2 round trips rather than one per 32 columns.
 template <class B, class X>
 __global__ void k_vc_dense(int cn, const double* __restrict__ inv, const B* __restrict__ b, X* __restrict__ x,
                            const int* __restrict__ done) {
@@ -765,8 +768,24 @@ __global__ void k_vc_dense(int cn, const double* __restrict__ inv, const B* __re
     if (done && *done) return;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x & 31;
     if (i >= cn) return;
-    double s = 0.0;
-    for (int j = lane; j < cn; j += 32) s += inv[(size_t)i * cn + j] * (double)b[j];
+    const double* m = inv + (size_t)i * cn;
+    constexpr int U = 8;
+    double acc[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) acc[u] = 0.0;
+    int j = lane;
+    for (; j + 32 * (U - 1) < cn; j += 32 * U) {
+        double a[U], g[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            a[u] = __ldg(m + j + 32 * u);
+            g[u] = (double)b[j + 32 * u];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc[u] += a[u] * g[u];
+    }
+    for (; j < cn; j += 32) acc[0] += m[j] * (double)b[j];
+    double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
     s = warp_sum(s);
     if (lane == 0) x[i] = (X)s;
 }
@@ -1343,7 +1362,7 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     }
     const bool last = l + 1 == (int)amg->levels.size();
     T* cb = last ? TVec<T>::cb(amg) : TVec<T>::b(amg->levels[l + 1]);
-    if (L.fused) {   // cb = R b - (R A) x in one pass
+    if (L.fusedQ) {   // cb = R b - (R A) x in one pass
         vct<VC_RESTRICT, V, T, B, T>(ctx, dry, L.tQ, err, dinv, omega, b, (const T*)x, cb, done);
     } else {
         vct<VC_RES, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, TVec<T>::r(L), done);
@@ -1369,7 +1388,7 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
         cx = TVec<T>::cx(amg);
     }
     int k0 = 0;
-    if (L.fused) {   // the first post-smoothing sweep from x + P cx
+    if (L.fusedW) {   // the first post-smoothing sweep from x + P cx
         vct<VC_ADDJAC, V, T, B, T>(ctx, dry, L.tW, err, dinv, omega, b, (const T*)x, t, done, nullptr, cx);
         std::swap(x, t);
         k0 = 1;
@@ -2020,14 +2039,35 @@ __global__ void k_fuse_w(int n, const int* __restrict__ Arp, const int* __restri
     if (!FILL) cnt[i] = o;
 }
 
-// Levels whose transfers run fused (VC_RESTRICT, VC_ADDJAC): CFA_VC_FUSE=0 none, 1 levels >= 1
-// (the default: there the V-cycle is a chain of short launches), 2 every level. Needs at least
-// two smoothing steps (the first post-smoothing sweep carries the prolongation).
+// Levels whose transfers run fused: CFA_VC_FUSE=0 none, 1 levels >= 1 (the default: there the
+// V-cycle is a chain of short launches), 2 every level. Needs at least two smoothing steps (the
+// first post-smoothing sweep carries the prolongation). The restriction (VC_RESTRICT) is fused on
+// every such level; the prolongation (VC_ADDJAC) only on levels of at most CFA_VC_ADDJAC_ROWS rows
+// (default 16384): [A | A P] holds about twice A's and P's entries together, which costs more than
+// the launch it saves once a level's sweeps are no longer latency-bound.
 static bool fuse_level(const cfa_amg* amg, const AmgLevel& L) {
     const char* e = std::getenv("CFA_VC_FUSE");
     const int mode = e ? std::atoi(e) : 1;
     if (mode <= 0 || amg->opts.smooth_steps < 2) return false;
     return mode >= 2 || &L != &amg->levels[0];
+}
+
+static bool fuse_prolongation(const AmgLevel& L) {
+    const char* e = std::getenv("CFA_VC_ADDJAC_ROWS");
+    const int rows = e ? std::atoi(e) : 16384;
+    return L.A.rows <= rows;
+}
+
+// a_ij == a_ji to within 1e-10 of their magnitude on every entry of A, A^T = T (same pattern)
+__global__ void k_sym_check(int n, const int* __restrict__ arp, const int* __restrict__ aci,
+                            const double* __restrict__ av, const int* __restrict__ trp, const int* __restrict__ tci,
+                            const double* __restrict__ tv, int* __restrict__ asym) {
+    CFA_GRID_DEP();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (arp[i + 1] - arp[i] != trp[i + 1] - trp[i]) { *asym = 1; return; }
+    for (int k = arp[i], q = trp[i]; k < arp[i + 1]; ++k, ++q)
+        if (aci[k] != tci[q] || fabs(av[k] - tv[q]) > 1e-10 * (fabs(av[k]) + fabs(tv[q])) + 1e-300) { *asym = 1; return; }
 }
 
 static cfa_status pack_from_device(cfa_ctx* ctx, cfa_amg* amg, const DCsr& M, const double* v0, const double* v1,
@@ -2040,17 +2080,28 @@ static cfa_status pack_from_device(cfa_ctx* ctx, cfa_amg* amg, const DCsr& M, co
     return pack_tiled(ctx, M.rp.p, M.ci.p, v0, v1, nullptr, T);
 }
 
-// The fused transfer operators of a level: Q = [R | -R A] and W = ([A | A P], [I | P]), exact
-// products on the device (the setup's SpGEMM), packed as tiles in the hierarchy precision.
-static cfa_status build_fused(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb) {
+// The fused transfer operators of a level: Q = [R | -R A] and, with_w, W = ([A | A P], [I | P]),
+// packed as tiles in the hierarchy precision. A P is the Galerkin product's (recomputed after a
+// remap changed P). R A = P^T A is (A P)^T when A is symmetric (checked entry by entry; the
+// Galerkin operators are, to rounding); otherwise the exact-order SpGEMM forms it.
+static cfa_status build_fused(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb, bool with_w) {
     SetupScratch& S = amg->scratch;
     const int n = L.A.rows, nc = L.R.rows;
-    CFA_PROPAGATE(spgemm(ctx, S, nc, n, L.R.rp.p, L.R.ci.p, L.R.v.p, L.A.rp.p, L.A.ci.p, L.A.v.p, S.fRA));
-    // A P: the Galerkin product's, unless a remap changed P since
     const bool keep_ap = L.AP.rows == n && L.AP.cols == L.P.cols && L.AP.nnz > 0;
     if (!keep_ap)
         CFA_PROPAGATE(spgemm(ctx, S, n, L.P.cols, L.A.rp.p, L.A.ci.p, L.A.v.p, L.P.rp.p, L.P.ci.p, L.P.v.p, S.fAP));
     const DCsr& AP = keep_ap ? L.AP : S.fAP;
+    CFA_PROPAGATE(transpose(ctx, S, L.A, S.fAt));
+    CFA_CUDA(S.ierr.ensure(1));
+    CFA_CUDA(cudaMemsetAsync(S.ierr.p, 0, sizeof(int), ctx->stream));
+    CFA_LAUNCH(ctx, k_sym_check, ceil_div(n, kThreads), kThreads, 0, n, (const int*)L.A.rp.p, (const int*)L.A.ci.p,
+               (const double*)L.A.v.p, (const int*)S.fAt.rp.p, (const int*)S.fAt.ci.p, (const double*)S.fAt.v.p,
+               S.ierr.p);
+    int asym = 0;
+    CFA_CUDA(cudaMemcpyAsync(&asym, S.ierr.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (asym) CFA_PROPAGATE(spgemm(ctx, S, nc, n, L.R.rp.p, L.R.ci.p, L.R.v.p, L.A.rp.p, L.A.ci.p, L.A.v.p, S.fRA));
+    else CFA_PROPAGATE(transpose(ctx, S, AP, S.fRA));
     // Q
     DCsr& Q = S.fQ;
     Q.rows = nc;
@@ -2065,6 +2116,11 @@ static cfa_status build_fused(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb) {
                (const int*)L.R.ci.p, (const double*)L.R.v.p, (const int*)S.fRA.rp.p, (const int*)S.fRA.ci.p,
                (const double*)S.fRA.v.p, (const int*)Q.rp.p, Q.ci.p, Q.v.p);
     CFA_PROPAGATE(pack_from_device(ctx, amg, Q, Q.v.p, nullptr, vb, L.tQ));
+    L.fusedQ = true;
+    if (!with_w) {
+        CFA_CHECK_LAUNCH();
+        return CFA_OK;
+    }
     // W: count, offsets, fill
     DCsr& W = S.fW;
     CFA_CUDA(S.fcnt.ensure(n + 1));
@@ -2090,7 +2146,7 @@ static cfa_status build_fused(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb) {
                (const int*)W.rp.p, W.ci.p, W.v.p, S.fW1.p);
     CFA_PROPAGATE(pack_from_device(ctx, amg, W, W.v.p, S.fW1.p, vb, L.tW));
     CFA_CHECK_LAUNCH();
-    L.fused = true;
+    L.fusedW = true;
     return CFA_OK;
 }
 
@@ -2178,14 +2234,11 @@ static cfa_status tune_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb) {
     const T* dinv = std::is_same<T, float>::value ? (const T*)(const void*)L.dinv32.p : (const T*)(const void*)L.dinv.p;
     auto vals = [&](const DCsr& M) { return (const double*)M.v.p; };
     if (!lv0) CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "A", VC_JAC, L.A, vals(L.A), nullptr, vb, L.tA, dinv, vec)));
-    if (L.fused) {
-        SetupScratch& S = amg->scratch;
-        CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "Q", VC_RESTRICT, S.fQ, S.fQ.v.p, nullptr, vb, L.tQ, dinv, vec)));
-        CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "W", VC_ADDJAC, S.fW, S.fW.v.p, S.fW1.p, vb, L.tW, dinv, vec)));
-    } else {
-        CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "P", VC_ADD, L.P, vals(L.P), nullptr, vb, L.tP, dinv, vec)));
-        CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "R", VC_SPMV, L.R, vals(L.R), nullptr, vb, L.tR, dinv, vec)));
-    }
+    SetupScratch& S = amg->scratch;
+    if (L.fusedQ) CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "Q", VC_RESTRICT, S.fQ, S.fQ.v.p, nullptr, vb, L.tQ, dinv, vec)));
+    else CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "R", VC_SPMV, L.R, vals(L.R), nullptr, vb, L.tR, dinv, vec)));
+    if (L.fusedW) CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "W", VC_ADDJAC, S.fW, S.fW.v.p, S.fW1.p, vb, L.tW, dinv, vec)));
+    else CFA_PROPAGATE((tune_one<V, T>(ctx, amg, "P", VC_ADD, L.P, vals(L.P), nullptr, vb, L.tP, dinv, vec)));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));   // buf is released on return
     return CFA_OK;
 }
@@ -2208,14 +2261,14 @@ static cfa_status prepare_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L) {
     CFA_CHECK_LAUNCH();
     if (!amg->tiled) return CFA_OK;
     const int vb = o.precision == CFA_MIXED ? 4 : 8;
-    L.fused = false;
+    L.fusedQ = L.fusedW = false;
     // levels the composite operator replaces run no tile kernel
     const int l = (int)(&L - &amg->levels[0]);
     if (amg->comp_level >= 0 && l >= amg->comp_level) {
         if (o.precision == CFA_MIXED) CFA_PROPAGATE(level_vectors(ctx, amg, L, L.A.rows));
         return level_vectors64(ctx, L, L.A.rows);
     }
-    if (fuse_level(amg, L)) CFA_PROPAGATE(build_fused(ctx, amg, L, vb));
+    if (fuse_level(amg, L)) CFA_PROPAGATE(build_fused(ctx, amg, L, vb, fuse_prolongation(L)));
     for (DCsr* M : {&L.A, &L.P, &L.R}) {
         TiledCsr& T = M == &L.A ? L.tA : M == &L.P ? L.tP : L.tR;
         HostBuf<int>& hr = amg->scratch.h_rp;

@@ -19,12 +19,12 @@ struct DCsr {
 struct AmgLevel {
     DCsr A, P, R;
     TiledCsr tA, tP, tR;           // tile-streamed copies in the hierarchy precision
-    // fused transfers (fused = true): tQ, the restricted residual R b - (R A) x in one pass over
-    // the next level's rows; tW, the prolongation-add folded into the first post-smoothing sweep
-    // (values [A | A P] and [I | P] on one pattern); columns with the top bit set read the second
-    // vector (x, resp. the coarse correction)
+    // fused transfers: tQ (fusedQ), the restricted residual R b - (R A) x in one pass over the
+    // next level's rows; tW (fusedW), the prolongation-add folded into the first post-smoothing
+    // sweep (values [A | A P] and [I | P] on one pattern); columns with the top bit set read the
+    // second vector (x, resp. the coarse correction)
     TiledCsr tQ, tW;
-    bool fused = false;
+    bool fusedQ = false, fusedW = false;
     DCsr AP;                       // A P of the Galerkin product (rows 0 after a remap changed P)
     DevBuf<double> dinv;
     DevBuf<float> dinv32;
@@ -78,7 +78,7 @@ struct SetupScratch {
     HostBuf<unsigned char> h_strong;
     HostBuf<double> h_p0v, h_st;
     DCsr AP0, AP;
-    DCsr fRA, fAP, fQ, fW;              // fused transfers: R A, A P, the merged operators
+    DCsr fRA, fAP, fQ, fW, fAt;         // fused transfers: R A, A P, the merged operators, A^T
     DevBuf<double> fW1;                 // second value array of fW
     DevBuf<int> fcnt;
 };

@@ -47,142 +47,109 @@ __device__ __forceinline__ double momentum_bc_u(int tag, double yi, double u_max
     return 0.0;
 }
 
-// Momentum system: k_assemble_momentum_fem (fem_kernels.cuh:40-181), the lumped mass and (with_bc)
-// the Dirichlet rows of k_apply_bc_momentum (:411-453) on A and the RHS, in three passes as the
-// pressure system (k_press_*): an element record (geometry, SUPG tau, convective and BDF2 terms,
-// computed once per element), every CSR entry summed over its contributions, every row's mass and
-// right-hand side. Each sum takes its terms in the element order of the row's incidence, each term
-// the same expression of the same element values as a row walking its elements.
-constexpr int kMomRec = 24;   // area, dNdx[3], dNdy[3], ugN[3], tau, div_w, nu, u_h[3], v_h[3], dp/dx, dp/dy
+// Momentum rows: k_assemble_momentum_fem (fem_kernels.cuh:40-181) gathered per row, lumped mass,
+// and (with_bc) the Dirichlet rows of k_apply_bc_momentum (:411-453) on A and the RHS. A row of
+// up to kMomCap entries accumulates in shared memory laid out [slot][thread] (conflict-free for
+// any slot a thread adds to); longer rows in place in global memory. Same addition order.
+constexpr int kMomCap = 16;
+constexpr size_t kMomSmem = (size_t)kMomCap * kThreads * sizeof(double);
 
-// reciprocals of the constant and per-launch divisors (the products differ from the quotients in
-// the last bit at most; the element formula is division-bound in FP64)
-constexpr double kThird = 1.0 / 3.0, kSixth = 1.0 / 6.0, kTwelfth = 1.0 / 12.0;
-
-__global__ void k_mom_elems(int ne, const int* __restrict__ ev, const double* __restrict__ x,
-                            const double* __restrict__ y, const double* __restrict__ u_old,
-                            const double* __restrict__ v_old, const double* __restrict__ u_prev,
-                            const double* __restrict__ v_prev, const double* __restrict__ p_old,
-                            const double* __restrict__ nu_node, MomParams P, double* __restrict__ rec) {
-    CFA_GRID_DEP();
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= ne) return;
-    int nd[3];
-    load_elem(ev, e, nd);
-    const Geom g = elem_geom(nd, x, y);
-    double* r = rec + (size_t)kMomRec * e;
-    r[0] = g.area;
-    if (!g.ok) return;
-    const double area = g.area;
-    const double inv_rho = 1.0 / P.rho, term_t = 2.0 / P.tau_time;
-    double w_u = 0.0, w_v = 0.0, div_w = 0.0;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const double un = u_old[nd[k]], vn = v_old[nd[k]], um = u_prev[nd[k]], vm = v_prev[nd[k]];
-        r[13 + k] = P.a1 * un + P.a2 * um;
-        r[16 + k] = P.a1 * vn + P.a2 * vm;
-        const double wu = P.c1 * un + P.c2 * um, wv = P.c1 * vn + P.c2 * vm;
-        w_u += wu * kThird;
-        w_v += wv * kThird;
-        div_w += wu * g.dNdx[k] + wv * g.dNdy[k];
-    }
-    const double vel_mag = sqrt(w_u * w_u + w_v * w_v) + 1.0e-12;
-    const double h_K = sqrt(2.0 * area);
-    // element viscosity: the scalar nu, or the mean of a nodal field
-    const double nu = nu_node ? (nu_node[nd[0]] + nu_node[nd[1]] + nu_node[nd[2]]) * kThird : P.nu;
-    const double term_c = 2.0 * vel_mag / h_K;
-    const double term_d = 4.0 * nu / (h_K * h_K);
-    const double tau_supg = 1.0 / sqrt(term_t * term_t + term_c * term_c + 9.0 * term_d * term_d);
-    const double p0 = p_old[nd[0]], p1 = p_old[nd[1]], p2 = p_old[nd[2]];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        r[1 + k] = g.dNdx[k];
-        r[4 + k] = g.dNdy[k];
-        r[7 + k] = w_u * g.dNdx[k] + w_v * g.dNdy[k];
-    }
-    r[10] = tau_supg;
-    r[11] = div_w;
-    r[12] = nu;
-    r[19] = (p0 * g.dNdx[0] + p1 * g.dNdx[1] + p2 * g.dNdx[2]) * inv_rho;
-    r[20] = (p0 * g.dNdy[0] + p1 * g.dNdy[1] + p2 * g.dNdy[2]) * inv_rho;
-}
-
-// M_ij + Ms_ij and A_ij of element record r for local row vertex a and column vertex j
-__device__ __forceinline__ double mom_A(const double* __restrict__ r, int a, int j, const MomParams& P,
-                                        double* MMs) {
-    const double area = r[0], area3 = area * kThird;
-    const double M_ij = (a == j) ? (area * kSixth) : (area * kTwelfth);
-    const double K_ij = area * (r[1 + a] * r[1 + j] + r[4 + a] * r[4 + j]);
-    const double C_ij = area3 * r[7 + j] + P.skew_coef * r[11] * M_ij;
-    const double S_ij = area * r[10] * r[7 + a] * r[7 + j];
-    const double Ms_ij = area3 * r[10] * r[7 + a];
-    *MMs = M_ij + Ms_ij;
-    return P.a0 * (M_ij + Ms_ij) + r[12] * K_ij + C_ij + S_ij;
-}
-
-__global__ void k_mom_entries(int nnz, const int* __restrict__ ent_ptr, const int* __restrict__ ent,
-                              const int* __restrict__ erow, const int* __restrict__ ci, const int* __restrict__ inc,
-                              const int* __restrict__ tag, const double* __restrict__ rec, MomParams P, int with_bc,
-                              OutletBc bc, double* __restrict__ A_val) {
-    CFA_GRID_DEP();
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= nnz) return;
-    const int i = erow[p];
-    if (with_bc && momentum_dirichlet(tag[i], bc)) {
-        A_val[p] = (ci[p] == i) ? 1.0 : 0.0;
-        return;
-    }
-    double acc = 0.0;
-    for (int c = ent_ptr[p]; c < ent_ptr[p + 1]; ++c) {
-        const int code = ent[c];
-        const int sl = code >> 2, j = code & 3;
-        const int e = inc[sl] >> 2, a = inc[sl] & 3;
-        const double* r = rec + (size_t)kMomRec * e;
-        if (r[0] < 1.0e-14) continue;
-        double mms;
-        acc += mom_A(r, a, j, P, &mms);
-    }
-    A_val[p] = acc;
-}
-
-__global__ void k_mom_rowsums(int n, const double* __restrict__ y, const int* __restrict__ tag,
-                              const int* __restrict__ inc_ptr, const int* __restrict__ inc,
-                              const double* __restrict__ rec, MomParams P, int with_bc, double u_max, double H,
-                              OutletBc bc, double* __restrict__ rhs_u, double* __restrict__ rhs_v,
-                              double* __restrict__ mass) {
+__global__ void __launch_bounds__(kThreads)
+k_momentum_rows(int n, const int* __restrict__ ev, const double* __restrict__ x, const double* __restrict__ y,
+                const int* __restrict__ tag, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
+                const int* __restrict__ pos, const int* __restrict__ rp, const int* __restrict__ ci,
+                const double* __restrict__ u_old, const double* __restrict__ v_old,
+                const double* __restrict__ u_prev, const double* __restrict__ v_prev,
+                const double* __restrict__ p_old, const double* __restrict__ nu_node, MomParams P, int with_bc,
+                double u_max, double H, OutletBc bc, double* __restrict__ A_val, double* __restrict__ rhs_u,
+                double* __restrict__ rhs_v, double* __restrict__ mass) {
     CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const int r0 = rp[i], len = rp[i + 1] - r0;
     const bool dir = with_bc && momentum_dirichlet(tag[i], bc);
+    const bool local = len <= kMomCap;
+    extern __shared__ double mom_sm[];   // [kMomCap][blockDim.x]
+    const int T = blockDim.x;
+    double* acc = mom_sm + threadIdx.x;  // acc[q * T]: entry q of this row
+    if (!dir) {
+        if (local) {
+            for (int q = 0; q < len; ++q) acc[q * T] = 0.0;
+        } else {
+            for (int q = 0; q < len; ++q) A_val[r0 + q] = 0.0;
+        }
+    }
     double f_u_row = 0.0, f_v_row = 0.0, m_row = 0.0;
+    // reciprocals of the constant and per-launch divisors, taken once (the products differ from
+    // the quotients in the last bit at most; the element formula is division-bound in FP64)
+    constexpr double kThird = 1.0 / 3.0, kSixth = 1.0 / 6.0, kTwelfth = 1.0 / 12.0;
+    const double inv_rho = 1.0 / P.rho, term_t_p = 2.0 / P.tau_time;
     for (int s = inc_ptr[i]; s < inc_ptr[i + 1]; ++s) {
         const int e = inc[s] >> 2, a = inc[s] & 3;
-        const double* r = rec + (size_t)kMomRec * e;
-        const double area = r[0];
-        if (area < 1.0e-14) continue;
+        int nd[3];
+        load_elem(ev, e, nd);
+        const Geom g = elem_geom(nd, x, y);
+        if (!g.ok) continue;
+        const double area = g.area;
         const double area3 = area * kThird;
         m_row += area3;
         if (dir) continue;
+        double u_h[3], v_h[3], w_u = 0.0, w_v = 0.0, div_w = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const double un = u_old[nd[k]], vn = v_old[nd[k]], um = u_prev[nd[k]], vm = v_prev[nd[k]];
+            u_h[k] = P.a1 * un + P.a2 * um;
+            v_h[k] = P.a1 * vn + P.a2 * vm;
+            const double wu = P.c1 * un + P.c2 * um, wv = P.c1 * vn + P.c2 * vm;
+            w_u += wu * kThird;
+            w_v += wv * kThird;
+            div_w += wu * g.dNdx[k] + wv * g.dNdy[k];
+        }
+        const double vel_mag = sqrt(w_u * w_u + w_v * w_v) + 1.0e-12;
+        const double h_K = sqrt(2.0 * area);
+        // element viscosity: the scalar nu, or the mean of a nodal field
+        const double nu = nu_node ? (nu_node[nd[0]] + nu_node[nd[1]] + nu_node[nd[2]]) * kThird : P.nu;
+        const double term_t = term_t_p;
+        const double term_c = 2.0 * vel_mag / h_K;
+        const double term_d = 4.0 * nu / (h_K * h_K);
+        const double tau_supg = 1.0 / sqrt(term_t * term_t + term_c * term_c + 9.0 * term_d * term_d);
+        const double p0 = p_old[nd[0]], p1 = p_old[nd[1]], p2 = p_old[nd[2]];
+        const double dpdx = (p0 * g.dNdx[0] + p1 * g.dNdx[1] + p2 * g.dNdx[2]) * inv_rho;
+        const double dpdy = (p0 * g.dNdy[0] + p1 * g.dNdy[1] + p2 * g.dNdy[2]) * inv_rho;
+        double ugN[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) ugN[k] = w_u * g.dNdx[k] + w_v * g.dNdy[k];
         double f_u = 0.0, f_v = 0.0;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            double mms;
-            (void)mom_A(r, a, j, P, &mms);
-            f_u += mms * r[13 + j];
-            f_v += mms * r[16 + j];
+            const double M_ij = (a == j) ? (area * kSixth) : (area * kTwelfth);
+            const double K_ij = area * (g.dNdx[a] * g.dNdx[j] + g.dNdy[a] * g.dNdy[j]);
+            const double C_ij = area3 * ugN[j] + P.skew_coef * div_w * M_ij;
+            const double S_ij = area * tau_supg * ugN[a] * ugN[j];
+            const double Ms_ij = area3 * tau_supg * ugN[a];
+            const double A_ij = P.a0 * (M_ij + Ms_ij) + nu * K_ij + C_ij + S_ij;
+            const int p = pos[3 * s + j];
+            if (local) acc[(p - r0) * T] += A_ij; else A_val[p] += A_ij;
+            f_u += (M_ij + Ms_ij) * u_h[j];
+            f_v += (M_ij + Ms_ij) * v_h[j];
         }
-        const double tw = area3 + area * r[10] * r[7 + a];
-        f_u -= tw * r[19];
-        f_v -= tw * r[20];
+        const double tw = area3 + area * tau_supg * ugN[a];
+        f_u -= tw * dpdx;
+        f_v -= tw * dpdy;
         f_u_row += f_u;
         f_v_row += f_v;
     }
     mass[i] = m_row;
     if (dir) {
-        rhs_u[i] = momentum_bc_u(tag[i], y[i], u_max, H, bc);
+        const int t = tag[i];
+        const double ub = momentum_bc_u(t, y[i], u_max, H, bc);
+        for (int q = 0; q < len; ++q) A_val[r0 + q] = (ci[r0 + q] == i) ? 1.0 : 0.0;
+        rhs_u[i] = ub;
         rhs_v[i] = 0.0;
         return;
     }
+    if (local)
+        for (int q = 0; q < len; ++q) A_val[r0 + q] = acc[q * T];
     rhs_u[i] = f_u_row;
     rhs_v[i] = f_v_row;
 }
@@ -271,133 +238,131 @@ __global__ void k_scalar_gradient_rows(int n, const int* __restrict__ ev, const 
     gy_out[i] = sy;
 }
 
-// Pressure system: k_assemble_pressure_poisson (fem_kernels.cuh:201-282); with oss_val the rows
-// of B and B^T of k_assemble_oss_operator (:807-847) and inv_m (:849-852); with with_bc the
-// Dirichlet rows/columns of k_apply_bc_pressure (:460-490). Three passes:
-//   k_press_elems    one thread per element: its geometry and the element terms every entry and
-//                    row needs (computed once instead of once per vertex), a 16-double record;
-//   k_press_entries  one thread per CSR entry: K, Bx, By, B^T x, B^T y summed over the entry's
-//                    contributions (the mesh's entry plan) and written coalesced;
-//   k_press_rowsums  one thread per row: the right-hand side and the divergence numerator.
-// Every sum takes its terms in the element order of the row's incidence, as a row walking its
-// elements would, and each term is the same expression of the same element values.
-constexpr int kPressRec = 16;   // area, dNdx[3], dNdy[3], s, w, rhs term, div term, gx, gy, sx, sy, -
+// Pressure rows: k_assemble_pressure_poisson (fem_kernels.cuh:201-282) gathered per row; with
+// oss_val the rows of B and B^T of k_assemble_oss_operator (:807-847) and inv_m (:849-852) in
+// the same pass; with with_bc the Dirichlet rows/columns of k_apply_bc_pressure (:460-490).
+// A row of up to kPressCap entries accumulates K, Bx, By, B^T x, B^T y in shared memory laid out
+// [array][slot][thread], so that threads adding to different slots of their rows hit different
+// banks; longer rows accumulate in place in global memory. Every entry takes its terms in the
+// element order of the incidence either way.
+constexpr int kPressThreads = 128;
+constexpr int kPressCap = 16;
+constexpr size_t kPressSmem = (size_t)5 * kPressCap * kPressThreads * sizeof(double);
 
-__global__ void k_press_elems(int ne, const int* __restrict__ ev, const double* __restrict__ x,
-                              const double* __restrict__ y, const double* __restrict__ us,
-                              const double* __restrict__ vs, const double* __restrict__ p_old,
-                              const double* __restrict__ gpx, const double* __restrict__ gpy,
-                              const double* __restrict__ mass, const double* __restrict__ elem_s, double dt,
-                              double rho, double stab, int want_oss, double* __restrict__ rec) {
-    CFA_GRID_DEP();
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= ne) return;
-    int nd[3];
-    load_elem(ev, e, nd);
-    const Geom g = elem_geom(nd, x, y);
-    double* r = rec + (size_t)kPressRec * e;
-    r[0] = g.area;
-    if (!g.ok) return;
-    const double area = g.area;
-    const double div_u = us[nd[0]] * g.dNdx[0] + us[nd[1]] * g.dNdx[1] + us[nd[2]] * g.dNdx[2]
-                       + vs[nd[0]] * g.dNdy[0] + vs[nd[1]] * g.dNdy[1] + vs[nd[2]] * g.dNdy[2];
-    double s = 0.0, sx = 0.0, sy = 0.0, gx = 0.0, gy = 0.0;
-    if (stab > 0.0) {
-        s = elem_s[e];
-        const double rs = sqrt(s);
-        gx = p_old[nd[0]] * g.dNdx[0] + p_old[nd[1]] * g.dNdx[1] + p_old[nd[2]] * g.dNdx[2];
-        gy = p_old[nd[0]] * g.dNdy[0] + p_old[nd[1]] * g.dNdy[1] + p_old[nd[2]] * g.dNdy[2];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            const double im = 1.0 / fmax(mass[nd[q]], 1.0e-14);
-            sx += gpx[nd[q]] * im;
-            sy += gpy[nd[q]] * im;
-        }
-        sx *= rs / 3.0;
-        sy *= rs / 3.0;
-    }
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        r[1 + q] = g.dNdx[q];
-        r[4 + q] = g.dNdy[q];
-    }
-    r[7] = s;
-    r[8] = want_oss ? sqrt(elem_s[e]) * area / 3.0 : 0.0;
-    r[9] = -(rho / dt) * (area / 3.0) * div_u;
-    r[10] = (area / 3.0) * div_u;
-    r[11] = gx;
-    r[12] = gy;
-    r[13] = sx;
-    r[14] = sy;
-}
-
-__global__ void k_press_entries(int nnz, const int* __restrict__ ent_ptr, const int* __restrict__ ent,
-                                const int* __restrict__ erow, const int* __restrict__ ci, const int* __restrict__ inc,
-                                const int* __restrict__ tag, const double* __restrict__ rec, int with_bc, OutletBc bc,
-                                double* __restrict__ Kp_val, double* __restrict__ oss_val) {
-    CFA_GRID_DEP();
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= nnz) return;
-    const int i = erow[p], j = ci[p];
-    const bool want_oss = oss_val != nullptr;
-    double K = 0.0, bx = 0.0, by = 0.0, tx = 0.0, ty = 0.0;
-    for (int c = ent_ptr[p]; c < ent_ptr[p + 1]; ++c) {
-        const int code = ent[c];
-        const int sl = code >> 2, b = code & 3;
-        const int e = inc[sl] >> 2, a = inc[sl] & 3;
-        const double* r = rec + (size_t)kPressRec * e;
-        const double area = r[0];
-        if (area < 1.0e-14) continue;
-        const double dxa = r[1 + a], dxb = r[1 + b], dya = r[4 + a], dyb = r[4 + b];
-        const double K_ij = area * (dxa * dxb + dya * dyb);
-        K += (1.0 + r[7]) * K_ij;
-        if (want_oss) {
-            const double w = r[8];
-            // B_ij = sum_K w_K grad N_j|K (row i, column j); B^T_ij = B_ji = sum_K w_K grad N_i|K
-            bx += w * dxb;
-            by += w * dyb;
-            tx += w * dxa;
-            ty += w * dya;
-        }
-    }
-    if (want_oss) {
-        oss_val[p] = bx;
-        oss_val[(size_t)nnz + p] = by;
-        oss_val[2 * (size_t)nnz + p] = tx;
-        oss_val[3 * (size_t)nnz + p] = ty;
-    }
-    if (with_bc) {
-        if (pressure_dirichlet(i, tag[i], bc)) K = (j == i) ? 1.0 : 0.0;
-        else if (j != i && pressure_dirichlet(j, tag[j], bc)) K = 0.0;
-    }
-    Kp_val[p] = K;
-}
-
-__global__ void k_press_rowsums(int n, const int* __restrict__ tag, const int* __restrict__ inc_ptr,
-                                const int* __restrict__ inc, const double* __restrict__ rec,
-                                const double* __restrict__ mass, int with_bc, OutletBc bc, int want_oss,
-                                double* __restrict__ rhs_p, double* __restrict__ div_num, double* __restrict__ dp,
-                                double* __restrict__ inv_m) {
+__global__ void __launch_bounds__(kPressThreads)
+k_pressure_rows(int n, int nnz, const int* __restrict__ ev, const double* __restrict__ x,
+                const double* __restrict__ y, const int* __restrict__ tag, const int* __restrict__ inc_ptr,
+                const int* __restrict__ inc, const int* __restrict__ pos, const int* __restrict__ rp,
+                const int* __restrict__ ci, const double* __restrict__ us, const double* __restrict__ vs,
+                const double* __restrict__ p_old, const double* __restrict__ gpx, const double* __restrict__ gpy,
+                const double* __restrict__ mass, const double* __restrict__ elem_s, double dt, double rho,
+                double stab, int with_bc, OutletBc bc, double* __restrict__ Kp_val, double* __restrict__ rhs_p,
+                double* __restrict__ div_num, double* __restrict__ dp, double* __restrict__ oss_val,
+                double* __restrict__ inv_m) {
     CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const int r0 = rp[i], len = rp[i + 1] - r0;
+    const bool local = len <= kPressCap;
+    const bool want_oss = oss_val != nullptr;
+    extern __shared__ double press_sm[];   // [5][kPressCap][blockDim.x]
+    const int T = blockDim.x, tt = threadIdx.x;
+    double* sK = press_sm + tt;                          // sK[q * T]: K entry q of this row
+    double* sBx = press_sm + 1 * kPressCap * T + tt;
+    double* sBy = press_sm + 2 * kPressCap * T + tt;
+    double* sTx = press_sm + 3 * kPressCap * T + tt;
+    double* sTy = press_sm + 4 * kPressCap * T + tt;
+    double *Bx = oss_val, *By = oss_val + (size_t)nnz, *BTx = oss_val + 2 * (size_t)nnz, *BTy = oss_val + 3 * (size_t)nnz;
+    if (local) {
+        for (int q = 0; q < len; ++q) {
+            sK[q * T] = 0.0;
+            if (want_oss) { sBx[q * T] = 0.0; sBy[q * T] = 0.0; sTx[q * T] = 0.0; sTy[q * T] = 0.0; }
+        }
+    } else {
+        for (int q = 0; q < len; ++q) Kp_val[r0 + q] = 0.0;
+        if (want_oss)
+            for (int q = 0; q < len; ++q) { Bx[r0 + q] = 0.0; By[r0 + q] = 0.0; BTx[r0 + q] = 0.0; BTy[r0 + q] = 0.0; }
+    }
     double rhs_row = 0.0, div_row = 0.0;
     for (int k = inc_ptr[i]; k < inc_ptr[i + 1]; ++k) {
         const int e = inc[k] >> 2, a = inc[k] & 3;
-        const double* r = rec + (size_t)kPressRec * e;
-        const double area = r[0];
-        if (area < 1.0e-14) continue;
-        const double dxa = r[1 + a], dya = r[4 + a], s = r[7];
-        const double stab_i = s * area * (dxa * r[11] + dya * r[12]) - area * (dxa * r[13] + dya * r[14]);
-        rhs_row += r[9] - stab_i;
-        div_row += r[10];
+        int nd[3];
+        load_elem(ev, e, nd);
+        const Geom g = elem_geom(nd, x, y);
+        if (!g.ok) continue;
+        const double area = g.area;
+        const double div_u = us[nd[0]] * g.dNdx[0] + us[nd[1]] * g.dNdx[1] + us[nd[2]] * g.dNdx[2]
+                           + vs[nd[0]] * g.dNdy[0] + vs[nd[1]] * g.dNdy[1] + vs[nd[2]] * g.dNdy[2];
+        const double rhs_contrib = -(rho / dt) * (area / 3.0) * div_u;
+        double s = 0.0, sx = 0.0, sy = 0.0, gx = 0.0, gy = 0.0;
+        if (stab > 0.0) {
+            s = elem_s[e];
+            const double rs = sqrt(s);
+            gx = p_old[nd[0]] * g.dNdx[0] + p_old[nd[1]] * g.dNdx[1] + p_old[nd[2]] * g.dNdx[2];
+            gy = p_old[nd[0]] * g.dNdy[0] + p_old[nd[1]] * g.dNdy[1] + p_old[nd[2]] * g.dNdy[2];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const double im = 1.0 / fmax(mass[nd[q]], 1.0e-14);
+                sx += gpx[nd[q]] * im;
+                sy += gpy[nd[q]] * im;
+            }
+            sx *= rs / 3.0;
+            sy *= rs / 3.0;
+        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double K_ij = area * (g.dNdx[a] * g.dNdx[j] + g.dNdy[a] * g.dNdy[j]);
+            const int p = pos[3 * k + j];
+            if (local) sK[(p - r0) * T] += (1.0 + s) * K_ij; else Kp_val[p] += (1.0 + s) * K_ij;
+        }
+        const double stab_i = s * area * (g.dNdx[a] * gx + g.dNdy[a] * gy) - area * (g.dNdx[a] * sx + g.dNdy[a] * sy);
+        rhs_row += rhs_contrib - stab_i;
+        div_row += (area / 3.0) * div_u;
+        if (want_oss) {
+            const double w = sqrt(elem_s[e]) * area / 3.0;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const int p = pos[3 * k + j];
+                // B_ij = sum_K w_K grad N_j|K (row i, column j); B^T_ij = B_ji = sum_K w_K grad N_i|K
+                if (local) {
+                    const int q = (p - r0) * T;
+                    sBx[q] += w * g.dNdx[j];
+                    sBy[q] += w * g.dNdy[j];
+                    sTx[q] += w * g.dNdx[a];
+                    sTy[q] += w * g.dNdy[a];
+                } else {
+                    Bx[p] += w * g.dNdx[j];
+                    By[p] += w * g.dNdy[j];
+                    BTx[p] += w * g.dNdx[a];
+                    BTy[p] += w * g.dNdy[a];
+                }
+            }
+        }
     }
-    if (want_oss) inv_m[i] = 1.0 / fmax(mass[i], 1.0e-14);
+    if (want_oss) {
+        inv_m[i] = 1.0 / fmax(mass[i], 1.0e-14);
+        if (local)
+            for (int q = 0; q < len; ++q) {
+                Bx[r0 + q] = sBx[q * T];
+                By[r0 + q] = sBy[q * T];
+                BTx[r0 + q] = sTx[q * T];
+                BTy[r0 + q] = sTy[q * T];
+            }
+    }
     div_num[i] = div_row;
     if (with_bc && pressure_dirichlet(i, tag[i], bc)) {
+        for (int q = 0; q < len; ++q) Kp_val[r0 + q] = (ci[r0 + q] == i) ? 1.0 : 0.0;
         rhs_p[i] = 0.0;
         if (dp) dp[i] = 0.0;
         return;
+    }
+    for (int q = 0; q < len; ++q) {
+        double v = local ? sK[q * T] : Kp_val[r0 + q];
+        if (with_bc) {
+            const int c = ci[r0 + q];
+            if (c != i && pressure_dirichlet(c, tag[c], bc)) v = 0.0;
+        }
+        Kp_val[r0 + q] = v;
     }
     rhs_p[i] = rhs_row;
 }
@@ -479,15 +444,9 @@ cfa_status cfa_assemble_momentum_nu(cfa_ctx* ctx, const cfa_mesh* m, const doubl
     CFA_ARG(!bcp || (u && v));
     MomParams P{prm->dt, prm->nu, prm->rho, prm->a0, prm->a1, prm->a2, prm->c1, prm->c2, prm->tau_time, prm->skew_coef};
     const double u_max = bcp ? bcp->u_max : 0.0, H = bcp ? bcp->H : 1.0;
-    DevBuf<double> rec;
-    CFA_CUDA(rec.ensure((size_t)kMomRec * std::max(m->ne, 1)));
-    CFA_LAUNCH(ctx, k_mom_elems, ceil_div(m->ne, kThreads), kThreads, 0, m->ne, m->ev, m->x, m->y, u_old, v_old, u_prev,
-               v_prev, p_old, nu_node, P, rec.p);
-    CFA_LAUNCH(ctx, k_mom_entries, ceil_div(m->nnz, kThreads), kThreads, 0, m->nnz, (const int*)m->ent_ptr.p,
-               (const int*)m->ent.p, (const int*)m->erow.p, m->ci, (const int*)m->inc.p, m->tag, (const double*)rec.p,
-               P, bcp ? 1 : 0, m->bc, A_val);
-    CFA_LAUNCH(ctx, k_mom_rowsums, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->y, m->tag, (const int*)m->inc_ptr.p,
-               (const int*)m->inc.p, (const double*)rec.p, P, bcp ? 1 : 0, u_max, H, m->bc, rhs_u, rhs_v, mass);
+    CFA_LAUNCH(ctx, k_momentum_rows, ceil_div(m->n, kThreads), kThreads, kMomSmem, m->n, m->ev, m->x, m->y, m->tag,
+               m->inc_ptr.p, m->inc.p, m->pos.p, m->rp, m->ci, u_old, v_old, u_prev, v_prev, p_old, nu_node, P,
+               bcp ? 1 : 0, u_max, H, m->bc, A_val, rhs_u, rhs_v, mass);
     if (bcp)   // solution values on Dirichlet nodes after the rows (u may alias u_old)
         CFA_LAUNCH(ctx, k_momentum_bc, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->tag, m->y, m->rp, m->ci,
                    u_max, H, m->bc, 0, A_val, rhs_u, rhs_v, u, v);
@@ -542,17 +501,14 @@ static cfa_status assemble_pressure(cfa_ctx* ctx, const cfa_mesh* m, const doubl
     // With the pinned outlet the RHS loses its mean before the BC rows (apply_bc_pressure,
     // fem_kernels.cuh:519-531): assemble without BC, then sums, then the BC kernel.
     const bool split = apply_bc && m->bc.outlet_dirichlet;
-    const int bc_now = (apply_bc && !split) ? 1 : 0;
-    const int want_oss = oss_val ? 1 : 0;
-    DevBuf<double> rec;
-    CFA_CUDA(rec.ensure((size_t)kPressRec * std::max(m->ne, 1)));
-    CFA_LAUNCH(ctx, k_press_elems, ceil_div(m->ne, kThreads), kThreads, 0, m->ne, m->ev, m->x, m->y, us, vs, p_old,
-               gpx, gpy, mass, elem_s, dt, rho, stab, want_oss, rec.p);
-    CFA_LAUNCH(ctx, k_press_entries, ceil_div(m->nnz, kThreads), kThreads, 0, m->nnz, (const int*)m->ent_ptr.p,
-               (const int*)m->ent.p, (const int*)m->erow.p, m->ci, (const int*)m->inc.p, m->tag,
-               (const double*)rec.p, bc_now, m->bc, Kp, oss_val);
-    CFA_LAUNCH(ctx, k_press_rowsums, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->tag, (const int*)m->inc_ptr.p,
-               (const int*)m->inc.p, (const double*)rec.p, mass, bc_now, m->bc, want_oss, rhs, div, dp, inv_m);
+    static std::once_flag press_once;
+    std::call_once(press_once, [] {
+        cudaFuncSetAttribute(k_pressure_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPressSmem);
+    });
+    CFA_LAUNCH(ctx, k_pressure_rows, ceil_div(m->n, kPressThreads), kPressThreads, kPressSmem, m->n, m->nnz, m->ev,
+               m->x, m->y, m->tag,
+               m->inc_ptr.p, m->inc.p, m->pos.p, m->rp, m->ci, us, vs, p_old, gpx, gpy, mass, elem_s, dt, rho,
+               stab, (apply_bc && !split) ? 1 : 0, m->bc, Kp, rhs, div, dp, oss_val, inv_m);
     if (split) {
         double* sums = ctx->d_part;   // after the partials region
         CFA_PROPAGATE(ensure_partials(ctx, 2 * (size_t)row_grid(ctx, m->n, 1) + 4));

@@ -164,51 +164,6 @@ static cfa_status build_incidence(cfa_ctx* ctx, int n, int ne, const int* d_ev, 
     return CFA_OK;
 }
 
-// Entry plan: the contributions of every CSR entry, from the scatter map pos.
-__global__ void k_entry_keys(int m, const int* __restrict__ pos, int* __restrict__ keys, int* __restrict__ vals) {
-    CFA_GRID_DEP();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= m) return;
-    keys[t] = pos[t];
-    vals[t] = ((t / 3) << 2) | (t % 3);   // slot << 2 | column vertex
-}
-
-__global__ void k_csr_entry_rows(int n, const int* __restrict__ rp, int* __restrict__ erow) {
-    CFA_GRID_DEP();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    for (int p = rp[i]; p < rp[i + 1]; ++p) erow[p] = i;
-}
-
-static cfa_status build_entry_plan(cfa_ctx* ctx, cfa_mesh* m) {
-    const int cnt = 9 * m->ne;
-    DevBuf<int> keys, vals, keys_out;
-    CFA_CUDA(keys.ensure(cnt));
-    CFA_CUDA(vals.ensure(cnt));
-    CFA_CUDA(keys_out.ensure(cnt));
-    CFA_CUDA(m->ent.ensure(cnt));
-    CFA_CUDA(m->ent_ptr.ensure(m->nnz + 1));
-    CFA_CUDA(m->erow.ensure(std::max(m->nnz, 1)));
-    CFA_LAUNCH(ctx, k_entry_keys, ceil_div(cnt, kThreads), kThreads, 0, cnt, (const int*)m->pos.p, keys.p, vals.p);
-    int bits = 1;
-    while ((1LL << bits) <= m->nnz) ++bits;
-    size_t tmp_bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys.p, keys_out.p, vals.p, m->ent.p, cnt, 0, bits,
-                                    ctx->stream);
-    DevBuf<char> tmp;
-    CFA_CUDA(tmp.ensure(tmp_bytes + 16));
-    // stable: the contributions of an entry keep ascending slot order
-    CFA_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, keys.p, keys_out.p, vals.p, m->ent.p, cnt, 0, bits,
-                                             ctx->stream));
-    ctx->launches += 4;
-    CFA_LAUNCH(ctx, k_incidence_ptr, ceil_div(cnt + 1, kThreads), kThreads, 0, m->nnz, cnt, (const int*)keys_out.p,
-               m->ent_ptr.p);
-    CFA_LAUNCH(ctx, k_csr_entry_rows, ceil_div(m->n, kThreads), kThreads, 0, m->n, m->rp, m->erow.p);
-    CFA_CHECK_LAUNCH();
-    CFA_CUDA(cudaStreamSynchronize(ctx->stream));   // the temporaries are released on return
-    return CFA_OK;
-}
-
 }  // namespace cfa
 
 using namespace cfa;
@@ -376,8 +331,6 @@ cfa_status cfa_mesh_create(cfa_ctx* ctx, int n, int ne, const int* d_ev, const d
     if (e != cudaSuccess) { delete m; return set_error(ctx, CFA_CUDA_ERROR, cudaGetErrorString(e), __FILE__, __LINE__); }
     if (h_err) { delete m; return set_error(ctx, CFA_BAD_ARG, "element edge missing from the CSR pattern", __FILE__, __LINE__); }
     m->nnz = h_nnz;
-    s = build_entry_plan(ctx, m);
-    if (s != CFA_OK) { delete m; return s; }
     *out = m;
     return CFA_OK;
 }

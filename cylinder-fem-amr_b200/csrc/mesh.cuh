@@ -34,11 +34,5 @@ struct cfa_mesh {
     cfa::DevBuf<int> inc_ptr;    // [n + 1]
     cfa::DevBuf<int> inc;        // [3 ne]: element << 2 | local vertex, ascending element per node
     cfa::DevBuf<int> pos;        // [9 ne]: pos[3 s + b] = CSR index of (node of s, vertex b of its element)
-    // the same map inverted: the contributions to CSR entry p are ent[ent_ptr[p] .. ent_ptr[p + 1])
-    // (slot s << 2 | column vertex b, ascending s: the order in which a row walks its elements);
-    // erow[p] = the row of entry p
-    cfa::DevBuf<int> ent_ptr;    // [nnz + 1]
-    cfa::DevBuf<int> ent;        // [9 ne]
-    cfa::DevBuf<int> erow;       // [nnz]
     cfa::OutletBc bc;
 };

@@ -386,8 +386,9 @@ def test_vcycle_composite_and_fused_transfers_match_level_chain(ctx, name, monke
     """The V-cycle's two reformulations against the plain chain of level kernels: the composite
     coarse operator (the V-cycle below the first level of at most 2048 rows formed once as a dense
     matrix) and the fused transfers (the restricted residual R b - (R A) x in one pass, the
-    prolongation folded into the first post-smoothing sweep through [A | A P] and [I | P]), on the
-    levels >= 1 (the default) and on every level. Each sums the same terms in another order: the
+    prolongation folded into the first post-smoothing sweep through [A | A P] and [I | P]): the
+    default (restriction fused on the levels >= 1, prolongation on those of at most 16384 rows)
+    and both fused on every level. Each sums the same terms in another order: the
     V-cycles agree to 1e-13 relative in FP64 and 1e-5 in mixed precision, and PCG to 1e-10 takes
     the same number of iterations within 1."""
     from tests.golden.make_golden import oracle_pressure_matrix
@@ -397,10 +398,12 @@ def test_vcycle_composite_and_fused_transfers_match_level_chain(ctx, name, monke
     drp, dci = dev(rp, torch.int32), dev(ci, torch.int32)
     r = dev(np.sin(0.37 * np.arange(m.n)) + 0.2)
     out = {}
-    configs = {"chain": ("0", "0"), "default": ("2048", "1"), "fused_all": ("0", "2")}
-    for cfg, (comp, fuse) in configs.items():
+    # (composite rows, fused levels, largest level with the prolongation folded)
+    configs = {"chain": ("0", "0", "0"), "default": ("2048", "1", "16384"), "fused_all": ("0", "2", "1000000000")}
+    for cfg, (comp, fuse, addjac) in configs.items():
         monkeypatch.setenv("CFA_COMPOSITE_ROWS", comp)
         monkeypatch.setenv("CFA_VC_FUSE", fuse)
+        monkeypatch.setenv("CFA_VC_ADDJAC_ROWS", addjac)
         for prec in (cfa.FP64, cfa.MIXED):
             amg = cfa.AmgPreconditioner(ctx, prec)
             amg.setup(m.n, ci.size, drp, dci, a)
