@@ -130,7 +130,7 @@ def workload_inputs(name):
 
 def workload_name(name, n, nnz):
     """The workload string both arms print (the same mesh, the same step)."""
-    kind = "uniform" if name == "c0" else "adaptive"
+    kind = "uniform" if name in ("c0", "c2") else "adaptive"
     return f"{name}: {kind} NVB mesh n={n}, nnz={nnz}, BDF2 step, OSS 0.3, tol 1e-10"
 
 
@@ -683,6 +683,8 @@ def main():
                     help="c3: OSS pressure stabilisation of the differentiated loop (0.3, the reference's default)")
     ap.add_argument("--autotune", action="store_true",
                     help="c4: time the V-cycle tile heights per pattern class (cfa_autotune_set)")
+    ap.add_argument("--step", action="store_true",
+                    help="c2: time the whole step path (as c1 does) instead of the repeated solve pairs")
     ap.add_argument("--profile", action="store_true",
                     help="one step per precision between cudaProfilerStart/Stop (for ncu --profile-from-start off); no JSON line")
     args = ap.parse_args()
@@ -702,7 +704,7 @@ def main():
     if args.workload == "c4":
         run_batch(args, rank, world)
         return
-    if args.workload == "c2":
+    if args.workload == "c2" and not args.step:
         if rank == 0:
             run_stress(args, rank, world)
         return

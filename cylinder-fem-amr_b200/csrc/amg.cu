@@ -20,6 +20,7 @@
 #include <functional>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <mutex>
 #include <type_traits>
@@ -2058,16 +2059,23 @@ static bool fuse_prolongation(const AmgLevel& L) {
     return L.A.rows <= rows;
 }
 
-// a_ij == a_ji to within 1e-10 of their magnitude on every entry of A, A^T = T (same pattern)
+// a_ij == a_ji on every entry of A (T = A^T, the same pattern), to 1e-10 of the entries or 1e-12
+// of sqrt(|a_ii a_jj|) (entries left by cancellation in the Galerkin sums differ in their last
+// bits relative to themselves, not to the row's scale)
 __global__ void k_sym_check(int n, const int* __restrict__ arp, const int* __restrict__ aci,
                             const double* __restrict__ av, const int* __restrict__ trp, const int* __restrict__ tci,
-                            const double* __restrict__ tv, int* __restrict__ asym) {
+                            const double* __restrict__ tv, const double* __restrict__ dinv, int* __restrict__ asym) {
     CFA_GRID_DEP();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (arp[i + 1] - arp[i] != trp[i + 1] - trp[i]) { *asym = 1; return; }
-    for (int k = arp[i], q = trp[i]; k < arp[i + 1]; ++k, ++q)
-        if (aci[k] != tci[q] || fabs(av[k] - tv[q]) > 1e-10 * (fabs(av[k]) + fabs(tv[q])) + 1e-300) { *asym = 1; return; }
+    for (int k = arp[i], q = trp[i]; k < arp[i + 1]; ++k, ++q) {
+        const int j = aci[k];
+        if (j != tci[q]) { *asym = 1; return; }
+        const double d = fabs(av[k] - tv[q]);
+        const double scale = sqrt(fabs(1.0 / (dinv[i] * dinv[j])));
+        if (!(d <= 1e-10 * (fabs(av[k]) + fabs(tv[q])) || d <= 1e-12 * scale)) { *asym = 1; return; }
+    }
 }
 
 static cfa_status pack_from_device(cfa_ctx* ctx, cfa_amg* amg, const DCsr& M, const double* v0, const double* v1,
@@ -2096,12 +2104,13 @@ static cfa_status build_fused(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb, b
     CFA_CUDA(cudaMemsetAsync(S.ierr.p, 0, sizeof(int), ctx->stream));
     CFA_LAUNCH(ctx, k_sym_check, ceil_div(n, kThreads), kThreads, 0, n, (const int*)L.A.rp.p, (const int*)L.A.ci.p,
                (const double*)L.A.v.p, (const int*)S.fAt.rp.p, (const int*)S.fAt.ci.p, (const double*)S.fAt.v.p,
-               S.ierr.p);
+               (const double*)L.dinv.p, S.ierr.p);
     int asym = 0;
     CFA_CUDA(cudaMemcpyAsync(&asym, S.ierr.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     if (asym) CFA_PROPAGATE(spgemm(ctx, S, nc, n, L.R.rp.p, L.R.ci.p, L.R.v.p, L.A.rp.p, L.A.ci.p, L.A.v.p, S.fRA));
     else CFA_PROPAGATE(transpose(ctx, S, AP, S.fRA));
+    L.ra_spgemm = asym != 0;
     // Q
     DCsr& Q = S.fQ;
     Q.rows = nc;
@@ -2537,8 +2546,30 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
         CFA_CUDA(amg->err.ensure(1));
         CFA_CUDA(cudaMemsetAsync(amg->err.p, 0, sizeof(int), ctx->stream));
     }
-    for (AmgLevel& L : amg->levels) CFA_PROPAGATE(prepare_level(ctx, amg, L));
-    CFA_PROPAGATE(prepare_vcycle(ctx, amg));
+    static const bool setup_log = [] {
+        const char* e = std::getenv("CFA_SETUP_LOG");
+        return e && e[0] == '1';
+    }();
+    for (AmgLevel& L : amg->levels) {
+        const auto t0l = std::chrono::steady_clock::now();
+        CFA_PROPAGATE(prepare_level(ctx, amg, L));
+        if (setup_log) {
+            cudaStreamSynchronize(ctx->stream);
+            fprintf(stderr, "[cfa setup] level %d: rows %d, tiles/fused %.3f ms (fusedQ %d, fusedW %d, R A by %s)\n",
+                    (int)(&L - &amg->levels[0]), L.A.rows,
+                    std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0l).count(),
+                    (int)L.fusedQ, (int)L.fusedW, L.ra_spgemm ? "SpGEMM" : "transpose");
+        }
+    }
+    {
+        const auto t0v = std::chrono::steady_clock::now();
+        CFA_PROPAGATE(prepare_vcycle(ctx, amg));
+        if (setup_log) {
+            cudaStreamSynchronize(ctx->stream);
+            fprintf(stderr, "[cfa setup] prepare_vcycle %.3f ms\n",
+                    std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0v).count());
+        }
+    }
     phase(6);
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
     amg->setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

@@ -25,6 +25,7 @@ struct AmgLevel {
     // second vector (x, resp. the coarse correction)
     TiledCsr tQ, tW;
     bool fusedQ = false, fusedW = false;
+    bool ra_spgemm = false;        // R A formed by SpGEMM (A not symmetric) rather than as (A P)^T
     DCsr AP;                       // A P of the Galerkin product (rows 0 after a remap changed P)
     DevBuf<double> dinv;
     DevBuf<float> dinv32;

@@ -1411,6 +1411,13 @@ static cfa_status pcg_init(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg c
 // preconditioner (empty otherwise).
 static bool pcg_piece_empty(const PcgArgs& a, int piece) { return piece == 2 && !a.prec; }
 
+// The beta of the PCG with the FP32 V-cycle: Polak-Ribiere (flexible) unless CFA_PCG_FLEXIBLE=0.
+static int pcg_flexible(const cfa_amg* amg) {
+    if (amg->opts.precision != CFA_MIXED) return 0;
+    const char* e = std::getenv("CFA_PCG_FLEXIBLE");
+    return (e && e[0] == '0') ? 0 : 1;
+}
+
 static cfa_status pcg_piece(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, int piece, CondArg cond) {
     const int n = a.n;
     const int gv = row_grid(ctx, n, 1);
@@ -1428,7 +1435,7 @@ static cfa_status pcg_piece(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, int piec
                        (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond);
             if (!a.prec) {
                 // z = M^-1 r with r.z (and z.q) folded into the V-cycle's last sweep where it can be
-                const int flexible = a.amg->opts.precision == CFA_MIXED ? 1 : 0;
+                const int flexible = pcg_flexible(a.amg);
                 const RzFuse f{W.q.p, flexible, &st->rz, &st->beta, &st->alpha, W.part.p, W.counter.p};
                 bool fused = false;
                 CFA_PROPAGATE(amg_vcycle_rz(ctx, a.amg, W.r.p, W.z.p, done, f, &fused));
