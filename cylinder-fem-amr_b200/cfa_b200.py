@@ -584,6 +584,14 @@ class AmgPreconditioner:
         cn = self.coarse_n
         return _dev_view(p.value, cn * cn, torch.float64).reshape(cn, cn)
 
+    def set_vcycle(self, composite_rows: int = -1, fuse_levels: int = -1, fold_rows: int = -1):
+        """The V-cycle's forms for the setups that follow (-1 keeps the default): the composite
+        coarse operator's largest level, the levels with the fused restriction, the largest level
+        with the folded prolongation. (0, 0, 0) runs the plain level chain."""
+        s = lib().cfa_amg_set_vcycle(self.h, composite_rows, fuse_levels, fold_rows)
+        if s != CFA_OK:
+            raise CfaError(s, "cfa_amg_set_vcycle")
+
     def composite(self):
         """(level, rows) of the composite coarse operator, level -1 when there is none."""
         lv, rows = C.c_int(), C.c_int()

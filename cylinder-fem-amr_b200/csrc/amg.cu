@@ -860,12 +860,12 @@ __global__ void k_bm_eye(int nb, double* __restrict__ B) {
 enum VcOp { VC_PRE = 0, VC_JAC = 1, VC_RES = 2, VC_SPMV = 3, VC_ADD = 4, VC_RESTRICT = 5, VC_ADDJAC = 6 };
 constexpr int kSecondVec = (int)0x80000000u;
 
-template <int TPR, int OP, class V, class T, class B, class O, bool RZ = false>
+template <int TPR, int OP, class V, class T, class B, class O, bool RZ = false, bool CGU = false>
 __global__ void __launch_bounds__(kTileThreads)
 k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b, const T* __restrict__ x,
-      O* __restrict__ y, const int* __restrict__ done, RzFuse rzf, const T* __restrict__ xc) {
+      O* __restrict__ y, const int* __restrict__ done, RzFuse rzf, const T* __restrict__ xc, CgFuse cgf) {
     extern __shared__ __align__(128) unsigned char tsmem[];
-    double dots[2] = {0.0, 0.0};   // RZ: this thread's rows of r.z and z.q
+    double dots[2] = {0.0, 0.0};   // RZ: this thread's rows of r.z and z.q; CGU (residual): of |r|^2
     // the level's tiles are packed at setup: their first copies go out before the wait
     const bool go = tile_loop_dep(tv, tsmem, [&] { return !(done && *done); },
                                   [&](int, int r0, int nr, const unsigned char* ch) {
@@ -880,9 +880,18 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
             const int row = r0 + lr;
             // the row's own operands, loaded before the gathers so both round trips overlap
             T di = (T)0, bi = (T)0, xi = (T)0;
+            // CGU: the right-hand side is the CG residual after this iteration's update,
+            // r - alpha q, formed here as the CG's update kernel forms it
+            const double alpha = CGU ? cgf.st->alpha : 0.0;
+            double rn = 0.0;
             if (valid && lane == 0) {
                 if (OP == VC_PRE || OP == VC_JAC || OP == VC_ADDJAC) di = dinv[row];
-                if (OP == VC_PRE || OP == VC_JAC || OP == VC_RES || OP == VC_ADDJAC) bi = (T)b[row];
+                if (CGU) {
+                    rn = (double)b[row] + -alpha * cgf.q[row];
+                    bi = (T)rn;
+                } else if (OP == VC_PRE || OP == VC_JAC || OP == VC_RES || OP == VC_ADDJAC) {
+                    bi = (T)b[row];
+                }
                 if (OP == VC_JAC) xi = x[row];
                 if (OP == VC_ADD) xi = (T)y[row];
             }
@@ -900,7 +909,11 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
                         if (e < end) {
                             const int j = cs[e];
                             a[u] = vv[e];
-                            if (OP == VC_PRE) { g0[u] = dinv[j]; g1[u] = b[j]; }
+                            if (OP == VC_PRE) {
+                                g0[u] = dinv[j];
+                                if (CGU) g1[u] = (B)((double)b[j] + -alpha * cgf.q[j]);
+                                else g1[u] = b[j];
+                            }
                             else if (OP == VC_RESTRICT) g0[u] = j < 0 ? x[j & ~kSecondVec] : (T)b[j];
                             else if (OP == VC_ADDJAC) { g0[u] = j < 0 ? xc[j & ~kSecondVec] : x[j]; a1[u] = vv1[e]; }
                             else g0[u] = x[j];
@@ -935,6 +948,13 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
                     }
                 } else if (OP == VC_RES) {
                     y[row] = (O)(bi - s);
+                    if constexpr (CGU) {   // the CG's update of this row (k_cg_update)
+                        const double pi = cgf.pn[row];
+                        cgf.x[row] += alpha * pi;
+                        cgf.r[row] = rn;
+                        cgf.p[row] = pi;
+                        dots[0] += rn * rn;
+                    }
                 } else if (OP == VC_SPMV || OP == VC_RESTRICT) {
                     y[row] = (O)s;
                 } else if (OP == VC_ADDJAC) {
@@ -946,6 +966,31 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
         }
     });
     if (!go) return;
+    if constexpr (CGU && OP == VC_RES) {
+        // |r| and the stopping test of the CG's update kernel (solve_pcg, src/cfa/linalg.cuh:239-246)
+        __shared__ double sh[2 * kWarps];
+        block_sum<2>(dots, sh);
+        if (publish_partials<2>(dots, cgf.part, cgf.counter)) {
+            reduce_partials<2>(dots, cgf.part, cgf.counter, sh);
+            if (threadIdx.x == 0) {
+                CgState* st = cgf.st;
+                const double rnorm = sqrt(dots[0]);
+                st->rel = rnorm / st->bnorm;
+                const int it = st->iter + 1;
+                st->iter = it;
+                if (rnorm < st->tol * st->bnorm) {
+                    st->done = 1;
+                    st->converged = 1;
+                    set_cond(cgf.cond, 0);
+                } else if (it >= st->max_iter) {
+                    st->done = 1;
+                    st->converged = 0;
+                    st->status = CFA_NOT_CONVERGED;
+                    set_cond(cgf.cond, 0);
+                }
+            }
+        }
+    }
     if constexpr (RZ) {
         __shared__ double sh[2 * kWarps];
         block_sum<2>(dots, sh);
@@ -964,24 +1009,30 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
 // rz: fold the CG's dots into this launch (the level-0 last sweep only).
 template <int OP, class V, class T, class B, class O>
 static void vct(cfa_ctx* ctx, bool dry, const TiledCsr& M, int* err, const T* dinv, T omega, const B* b, const T* x,
-                O* y, const int* done, const RzFuse* rz = nullptr, const T* xc = nullptr) {
+                O* y, const int* done, const RzFuse* rz = nullptr, const T* xc = nullptr, const CgFuse* cg = nullptr) {
     constexpr bool kRz = OP == VC_JAC && std::is_same<O, double>::value && std::is_same<B, double>::value;
+    constexpr bool kCgu = (OP == VC_PRE || OP == VC_RES) && std::is_same<B, double>::value;
     const int tpr = M.tpr;
     const TileView tv = M.view(err);
     const TileLaunch L = tile_launch(ctx, M, nullptr);
     const RzFuse none{};
+    const CgFuse nocg{};
     switch (tpr) {
 #define VCT_CASE(N)                                                                                     \
     case N:                                                                                             \
         if (dry) {                                                                                      \
             allow_tile_kernel((const void*)k_vct<N, OP, V, T, B, O>);                                   \
             if (kRz) allow_tile_kernel((const void*)k_vct<N, OP, V, T, B, O, kRz>);                     \
+            if (kCgu) allow_tile_kernel((const void*)k_vct<N, OP, V, T, B, O, false, kCgu>);            \
         } else if (kRz && rz) {                                                                         \
             CFA_LAUNCH(ctx, (k_vct<N, OP, V, T, B, O, kRz>), L.grid, kTileThreads, L.smem, tv, dinv, omega, b, x, y, \
-                       done, *rz, xc);                                                                  \
+                       done, *rz, xc, nocg);                                                            \
+        } else if (kCgu && cg) {                                                                        \
+            CFA_LAUNCH(ctx, (k_vct<N, OP, V, T, B, O, false, kCgu>), L.grid, kTileThreads, L.smem, tv, dinv, omega, \
+                       b, x, y, done, none, xc, *cg);                                                   \
         } else {                                                                                        \
             CFA_LAUNCH(ctx, (k_vct<N, OP, V, T, B, O>), L.grid, kTileThreads, L.smem, tv, dinv, omega, b, x, y, done, \
-                       none, xc);                                                                       \
+                       none, xc, nocg);                                                                 \
         }                                                                                               \
         break;
         VCT_CASE(1) VCT_CASE(2) VCT_CASE(4) VCT_CASE(8) VCT_CASE(16)
@@ -1340,7 +1391,7 @@ struct TVec<float> {
 // only, no launches)
 template <class V, class T, class B>
 static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* z, const int* done, bool dry,
-                         const RzFuse* rz = nullptr) {
+                         const RzFuse* rz = nullptr, const CgFuse* cg = nullptr) {
     AmgLevel& L = amg->levels[l];
     const int s = amg->opts.smooth_steps;
     int* err = amg->err.p;
@@ -1349,7 +1400,7 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     T* x = TVec<T>::x(L);
     T* t = TVec<T>::t(L);
     if (s >= 2) {
-        vct<VC_PRE, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)nullptr, x, done);
+        vct<VC_PRE, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)nullptr, x, done, nullptr, nullptr, cg);
     } else if (!dry) {
         CFA_TPR_SWITCH(L.A.tpr, CFA_LAUNCH(ctx, (k_vc_pre<TPR, T, B>), row_grid(ctx, L.A.rows, L.A.tpr), kThreads, 0,
                                            L.A.rows, L.A.rp.p, L.A.ci.p,
@@ -1366,7 +1417,8 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     if (L.fusedQ) {   // cb = R b - (R A) x in one pass
         vct<VC_RESTRICT, V, T, B, T>(ctx, dry, L.tQ, err, dinv, omega, b, (const T*)x, cb, done);
     } else {
-        vct<VC_RES, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, TVec<T>::r(L), done);
+        vct<VC_RES, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, TVec<T>::r(L), done, nullptr,
+                                nullptr, cg);
         vct<VC_SPMV, V, T, T, T>(ctx, dry, L.tR, err, dinv, omega, (const T*)nullptr, (const T*)TVec<T>::r(L), cb,
                                  done);
     }
@@ -1416,10 +1468,17 @@ static bool vcycle_fp32(const cfa_amg* amg) {
 }
 
 static void vcycle_tiled_top(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, bool dry,
-                             const RzFuse* rz = nullptr) {
-    if (amg->opts.precision != CFA_MIXED) vcycle_tiled<double, double, double>(ctx, amg, 0, r, z, done, dry, rz);
-    else if (vcycle_fp32(amg)) vcycle_tiled<float, float, double>(ctx, amg, 0, r, z, done, dry, rz);
-    else vcycle_tiled<float, double, double>(ctx, amg, 0, r, z, done, dry, rz);
+                             const RzFuse* rz = nullptr, const CgFuse* cg = nullptr) {
+    if (amg->opts.precision != CFA_MIXED) vcycle_tiled<double, double, double>(ctx, amg, 0, r, z, done, dry, rz, cg);
+    else if (vcycle_fp32(amg)) vcycle_tiled<float, float, double>(ctx, amg, 0, r, z, done, dry, rz, cg);
+    else vcycle_tiled<float, double, double>(ctx, amg, 0, r, z, done, dry, rz, cg);
+}
+
+bool amg_can_fuse_update(const cfa_amg* amg) {
+    const char* e = std::getenv("CFA_CG_FUSE_UPDATE");
+    const bool on = !(e && e[0] == '0');
+    return on && amg && !amg->levels.empty() && amg->tiled && amg->opts.smooth_steps == 2 &&
+           !amg->levels[0].fusedQ;
 }
 
 cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done) {
@@ -1438,10 +1497,12 @@ cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, co
 }
 
 cfa_status amg_vcycle_rz(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, const RzFuse& f,
-                         bool* fused) {
+                         bool* fused, const CgFuse* cg) {
     *fused = false;
+    if (cg && !amg_can_fuse_update(amg))
+        return set_error(ctx, CFA_BAD_ARG, "the CG update cannot be folded into this hierarchy", __FILE__, __LINE__);
     if (amg->levels.empty() || !amg->tiled || amg->opts.smooth_steps < 1) return amg_vcycle(ctx, amg, r, z, done);
-    vcycle_tiled_top(ctx, amg, r, z, done, false, &f);
+    vcycle_tiled_top(ctx, amg, r, z, done, false, &f, cg);
     CFA_CHECK_LAUNCH();
     *fused = true;
     return CFA_OK;
@@ -2048,14 +2109,14 @@ __global__ void k_fuse_w(int n, const int* __restrict__ Arp, const int* __restri
 // the launch it saves once a level's sweeps are no longer latency-bound.
 static bool fuse_level(const cfa_amg* amg, const AmgLevel& L) {
     const char* e = std::getenv("CFA_VC_FUSE");
-    const int mode = e ? std::atoi(e) : 1;
+    const int mode = amg->vc_fuse >= 0 ? amg->vc_fuse : e ? std::atoi(e) : 1;
     if (mode <= 0 || amg->opts.smooth_steps < 2) return false;
     return mode >= 2 || &L != &amg->levels[0];
 }
 
-static bool fuse_prolongation(const AmgLevel& L) {
+static bool fuse_prolongation(const cfa_amg* amg, const AmgLevel& L) {
     const char* e = std::getenv("CFA_VC_ADDJAC_ROWS");
-    const int rows = e ? std::atoi(e) : 16384;
+    const int rows = amg->vc_fold_rows >= 0 ? amg->vc_fold_rows : e ? std::atoi(e) : 16384;
     return L.A.rows <= rows;
 }
 
@@ -2277,7 +2338,7 @@ static cfa_status prepare_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L) {
         if (o.precision == CFA_MIXED) CFA_PROPAGATE(level_vectors(ctx, amg, L, L.A.rows));
         return level_vectors64(ctx, L, L.A.rows);
     }
-    if (fuse_level(amg, L)) CFA_PROPAGATE(build_fused(ctx, amg, L, vb, fuse_prolongation(L)));
+    if (fuse_level(amg, L)) CFA_PROPAGATE(build_fused(ctx, amg, L, vb, fuse_prolongation(amg, L)));
     for (DCsr* M : {&L.A, &L.P, &L.R}) {
         TiledCsr& T = M == &L.A ? L.tA : M == &L.P ? L.tP : L.tR;
         HostBuf<int>& hr = amg->scratch.h_rp;
@@ -2310,7 +2371,8 @@ static cfa_status prepare_vcycle(cfa_ctx* ctx, cfa_amg* amg) {
 // Largest level (rows) whose V-cycle below is formed as one dense operator (CFA_COMPOSITE_ROWS
 // overrides; 0: never). At 2048 rows the FP64 matrix is 32 MB, read in about the time of one
 // dependent launch of the chain it replaces.
-static int composite_rows() {
+static int composite_rows(const cfa_amg* amg) {
+    if (amg->vc_composite_rows >= 0) return amg->vc_composite_rows;
     const char* e = std::getenv("CFA_COMPOSITE_ROWS");
     return e ? std::atoi(e) : 2048;
 }
@@ -2321,7 +2383,7 @@ static int composite_rows() {
 static cfa_status build_composite(cfa_ctx* ctx, cfa_amg* amg) {
     amg->comp_level = -1;
     amg->comp_n = 0;
-    const int limit = composite_rows();
+    const int limit = composite_rows(amg);
     const int L = (int)amg->levels.size();
     int lc = -1;
     for (int l = 1; l < L; ++l)
@@ -2777,6 +2839,14 @@ cfa_status cfa_amg_phases(const cfa_amg* amg, double* ms8) {
 cfa_status cfa_amg_coarse_inverse(const cfa_amg* amg, const double** inv) {
     if (!amg || !inv) return CFA_BAD_ARG;
     *inv = amg->coarse_inv.p;
+    return CFA_OK;
+}
+
+cfa_status cfa_amg_set_vcycle(cfa_amg* amg, int composite_rows, int fuse_levels, int fold_rows) {
+    if (!amg || fuse_levels > 2) return CFA_BAD_ARG;
+    amg->vc_composite_rows = composite_rows < 0 ? -1 : composite_rows;
+    amg->vc_fuse = fuse_levels < 0 ? -1 : fuse_levels;
+    amg->vc_fold_rows = fold_rows < 0 ? -1 : fold_rows;
     return CFA_OK;
 }
 

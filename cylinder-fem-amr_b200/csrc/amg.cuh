@@ -115,9 +115,27 @@ struct cfa_amg {
     int comp_level = -1;
     int comp_n = 0;
     cfa::DevBuf<double> comp;
+    // V-cycle forms chosen for this handle (cfa_amg_set_vcycle); -1: the default / environment
+    int vc_composite_rows = -1, vc_fuse = -1, vc_fold_rows = -1;
 };
 
 namespace cfa {
+// The condition of a solve graph's WHILE node (use = 0 outside a graph)
+struct CondArg {
+    cudaGraphConditionalHandle handle;
+    int use;
+};
+
+__device__ __forceinline__ void set_cond(CondArg c, unsigned v) {
+    if (c.use) cudaGraphSetConditional(c.handle, v);
+}
+
+// Device-resident state of a CG solve
+struct CgState {
+    double bnorm, tol, rz, alpha, beta, rel, zero;
+    int iter, max_iter, done, converged, status, nullb;
+};
+
 // One symmetric V-cycle z = M^-1 r (FP64 in/out). Kernels return at once while *done != 0
 // (done nullable).
 cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done);
@@ -134,8 +152,27 @@ struct RzFuse {
     double* part;
     unsigned int* counter;
 };
+// The CG's update before the preconditioner (x += alpha pn, r -= alpha q, p = pn, |r| and the
+// stopping test) folded into the V-cycle's level-0 kernels: the pre-smoothing sweep gathers
+// r - alpha q for its right-hand side, the residual pass (which reads only its own rows) writes
+// the new r, x and p and finishes |r| as the CG's update kernel would.
+struct CgFuse {
+    double* r;
+    const double* q;
+    const double* pn;
+    double* x;
+    double* p;
+    CgState* st;
+    double* part;
+    unsigned int* counter;
+    CondArg cond;
+};
+// Whether amg_vcycle_rz can take the CG's update (a tile-streamed hierarchy with two or more
+// smoothing steps and level 0's residual pass unfused).
+bool amg_can_fuse_update(const cfa_amg* amg);
 // amg_vcycle with the dots fused when the hierarchy runs tile-streamed (*fused = true); otherwise
-// the plain V-cycle (*fused = false) and the caller computes the dots.
+// the plain V-cycle (*fused = false) and the caller computes the dots. cg (nullable; only where
+// amg_can_fuse_update) folds the CG's update into level 0.
 cfa_status amg_vcycle_rz(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, const RzFuse& f,
-                         bool* fused);
+                         bool* fused, const CgFuse* cg = nullptr);
 }  // namespace cfa

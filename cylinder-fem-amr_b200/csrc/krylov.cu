@@ -26,14 +26,6 @@ namespace cfa {
 // =============================================================================================
 // shared pieces
 // =============================================================================================
-struct CondArg {
-    cudaGraphConditionalHandle handle;
-    int use;
-};
-
-__device__ __forceinline__ void set_cond(CondArg c, unsigned v) {
-    if (c.use) cudaGraphSetConditional(c.handle, v);
-}
 
 #define ROWS_BEGIN(TPR, n)                                                                        \
     {                                                                                             \
@@ -113,10 +105,6 @@ __global__ void k_op_b(int n, int nnz, const int* __restrict__ rp, const int* __
 }
 
 // CG state (all on the device)
-struct CgState {
-    double bnorm, tol, rz, alpha, beta, rel, zero;
-    int iter, max_iter, done, converged, status, nullb;
-};
 
 // Operator pass 2: q = K pn - [not Dirichlet] (B^T_x g_x + B^T_y g_y) (k_spmv_csr + k_oss_apply_BT,
 // src/cfa/fem_kernels.cuh:871-885). FUSEP: pn = z + beta p computed on the fly (no OSS pass 1),
@@ -1431,14 +1419,19 @@ static cfa_status pcg_piece(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, int piec
             CFA_LAUNCH(ctx, k_cg_pq, gv, kThreads, 0, n, (const double*)W.pn.p, (const double*)W.q.p, st, W.part.p,
                        W.counter.p, cond);
         if (a.amg || a.prec) {
-            CFA_LAUNCH(ctx, k_cg_update<false>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p,
-                       (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond);
+            // the update (x, r, p, |r|, the stopping test) folded into the V-cycle's level 0 where
+            // the hierarchy allows it, else its own kernel
+            const bool fuse_update = !a.prec && amg_can_fuse_update(a.amg);
+            if (!fuse_update)
+                CFA_LAUNCH(ctx, k_cg_update<false>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p,
+                           (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond);
             if (!a.prec) {
                 // z = M^-1 r with r.z (and z.q) folded into the V-cycle's last sweep where it can be
                 const int flexible = pcg_flexible(a.amg);
                 const RzFuse f{W.q.p, flexible, &st->rz, &st->beta, &st->alpha, W.part.p, W.counter.p};
+                const CgFuse g{W.r.p, W.q.p, W.pn.p, a.x, W.p.p, st, W.part.p, W.counter.p, cond};
                 bool fused = false;
-                CFA_PROPAGATE(amg_vcycle_rz(ctx, a.amg, W.r.p, W.z.p, done, f, &fused));
+                CFA_PROPAGATE(amg_vcycle_rz(ctx, a.amg, W.r.p, W.z.p, done, f, &fused, fuse_update ? &g : nullptr));
                 if (!fused)
                     CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, flexible, st,
                                W.part.p, W.counter.p, cond);

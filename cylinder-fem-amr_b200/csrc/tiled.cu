@@ -74,21 +74,6 @@ cfa_status plan_tiled(cfa_ctx* ctx, const int* h_rp, int rows, int nvals, int vb
     }
     T.tpr = tpr;
     if (T.max_chunk > kTileBudget) return set_error(ctx, CFA_BAD_ARG, "matrix row too long for the tile budget", __FILE__, __LINE__);
-    // CFA_TILES_PER_SLOT=k: halve the tile height (down to a quarter of the default) while the
-    // matrix has fewer than k tiles per resident CTA (4 per SM), so that a matrix of a few MB is
-    // spread over more, shorter pipelines
-    if (row_shift == 0) {
-        static const int per_slot = [] {
-            const char* e = std::getenv("CFA_TILES_PER_SLOT");
-            return e ? std::atoi(e) : 0;
-        }();
-        const long long slots = 4LL * std::max(ctx->num_sms, 1);
-        int k = 0;
-        while (per_slot > 0 && k < 2 && (long long)((rows + (tr >> k) - 1) / std::max(tr >> k, 1)) < per_slot * slots &&
-               (tr >> k) >= 2)
-            ++k;
-        if (k > 0) row_shift = -k;
-    }
     if (row_shift != 0) {
         tr = row_shift > 0 ? tr << row_shift : std::max(1, tr >> -row_shift);
         long long mx = 0;

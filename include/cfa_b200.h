@@ -434,6 +434,15 @@ cfa_status cfa_amg_coarse_inverse(const cfa_amg* amg, const double** d_inv);
  * FP64 matrix (rows x rows) and applied as one matrix-vector product. *level = -1 when none.
  * d_m may be NULL. */
 cfa_status cfa_amg_composite(const cfa_amg* amg, int* level, int* rows, const double** d_m);
+/* The V-cycle's forms for the setups that follow on this handle (no counterpart in the reference;
+ * -1 keeps the default or the environment's): composite_rows, the largest level replaced by the
+ * composite operator (0: none; default 2048, CFA_COMPOSITE_ROWS); fuse_levels, the levels whose
+ * restriction runs fused, R b - (R A) x in one pass (0 none, 1 levels >= 1, the default, 2 all;
+ * CFA_VC_FUSE); fold_rows, the largest fused level whose prolongation is folded into the first
+ * post-smoothing sweep (default 16384, CFA_VC_ADDJAC_ROWS). Every form is the same preconditioner
+ * up to rounding; each costs setup time that only repeated solves with one hierarchy (a time loop
+ * between rebuilds) earn back, so a caller that solves once per setup turns them off (0, 0, 0). */
+cfa_status cfa_amg_set_vcycle(cfa_amg* amg, int composite_rows, int fuse_levels, int fold_rows);
 
 /* The assembled OSS term of the pressure operator (apply_oss_projection,
  * src/cfa/device.cuh:316-323): A x = K x - B^T M^-1 B x on non-Dirichlet rows. */

@@ -420,6 +420,15 @@ def test_vcycle_composite_and_fused_transfers_match_level_chain(ctx, name, monke
             it = s.solve_pcg(m.n, drp, dci, a, r, x, 4000, 1e-10, None, amg)
             assert s.converged
             out[cfg, prec] = (host(z), it, host(x))
+    # the per-handle setter (0, 0, 0) gives the chain bit for bit, whatever the environment says
+    for prec in (cfa.FP64, cfa.MIXED):
+        amg = cfa.AmgPreconditioner(ctx, prec)
+        amg.set_vcycle(0, 0, 0)
+        amg.setup(m.n, ci.size, drp, dci, a)
+        assert amg.composite()[0] == -1
+        z = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+        amg.apply(r, z)
+        assert np.array_equal(host(z), out["chain", prec][0])
     for cfg in ("default", "fused_all"):
         for prec, tol in ((cfa.FP64, 1e-13), (cfa.MIXED, 1e-5)):
             (z1, it1, x1), (z0, it0, x0) = out[cfg, prec], out["chain", prec]
@@ -619,6 +628,36 @@ def test_pcg_matches_oracle(ctx, use_oss, use_amg):
     Ax = O.spmv(rp, ci, Kp, x)
     if use_oss:
         O.oss_apply(m, rp, ci, oss, inv_m, x, Ax)
+    assert np.linalg.norm(rhs - Ax) <= 1.5e-10 * np.linalg.norm(rhs)
+
+
+@pytest.mark.parametrize("prec", [cfa.FP64, cfa.MIXED])
+def test_pcg_update_folded_into_vcycle_matches_update_kernel(ctx, prec, monkeypatch):
+    """The CG's update (x += alpha pn, r -= alpha q, p = pn, |r| and the stopping test) folded into
+    the V-cycle's level-0 pre-smoothing and residual passes, against the separate update kernel:
+    the same arithmetic per row (up to where the compiler contracts the update into a fused
+    multiply-add), so iteration counts within 1, solutions within 1e-8, and the true residual of
+    the folded solve below 1.5e-10."""
+    m = mesh("c0")
+    dm = cfa.DeviceMesh(ctx, m)
+    rp, ci = dm.host_pattern()
+    Kp, rhs, oss, inv_m = pressure_system(m, rp, ci)
+    dK, db, doss, dinv = dev(Kp), dev(rhs), dev(oss), dev(inv_m)
+    out = {}
+    for fold in ("1", "0"):
+        monkeypatch.setenv("CFA_CG_FUSE_UPDATE", fold)
+        amg = cfa.AmgPreconditioner(ctx, prec)
+        amg.setup(m.n, ci.size, dm.rp, dm.ci, dK)
+        s = cfa.GpuLinearSolver(ctx)
+        x = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+        it = s.solve_pcg(m.n, dm.rp, dm.ci, dK, db, x, 4000, 1e-10, cfa.oss_operator(dm, doss, dinv), amg)
+        assert s.converged
+        out[fold] = (it, host(x))
+    assert abs(out["1"][0] - out["0"][0]) <= 1
+    assert np.abs(out["1"][1] - out["0"][1]).max() <= 1e-8 * np.abs(out["0"][1]).max()
+    x = out["1"][1]
+    Ax = O.spmv(rp, ci, Kp, x)
+    O.oss_apply(m, rp, ci, oss, inv_m, x, Ax)
     assert np.linalg.norm(rhs - Ax) <= 1.5e-10 * np.linalg.norm(rhs)
 
 
