@@ -242,10 +242,7 @@ def run_ours(args, rank, world):
             st.p_n.copy_(hp, non_blocking=True)
             st.u_prev.copy_(st.u_n)
             st.v_prev.copy_(st.v_n)
-            st.run()
-            outs[0].copy_(st.u, non_blocking=True)
-            outs[1].copy_(st.v, non_blocking=True)
-            outs[2].copy_(st.dp, non_blocking=True)
+            st.run(host_out=outs)   # u, v copied out during the pressure solve, dp after it
             ev[1].record()
             ev[1].synchronize()
             e2e_total += ev[0].elapsed_time(ev[1])

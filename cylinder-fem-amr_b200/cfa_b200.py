@@ -588,14 +588,14 @@ class AmgPreconditioner:
         """The V-cycle's forms for the setups that follow (-1 keeps the default): the composite
         coarse operator's largest level, the levels with the fused restriction, the largest level
         with the folded prolongation. (0, 0, 0) runs the plain level chain."""
-        s = lib().cfa_amg_set_vcycle(self.h, composite_rows, fuse_levels, fold_rows)
+        s = lib().cfa_amg_set_vcycle(self._handle(), composite_rows, fuse_levels, fold_rows)
         if s != CFA_OK:
             raise CfaError(s, "cfa_amg_set_vcycle")
 
     def composite(self):
         """(level, rows) of the composite coarse operator, level -1 when there is none."""
         lv, rows = C.c_int(), C.c_int()
-        lib().cfa_amg_composite(self.h, C.byref(lv), C.byref(rows), None)
+        lib().cfa_amg_composite(self._handle(), C.byref(lv), C.byref(rows), None)
         return lv.value, rows.value
 
     def __del__(self):

@@ -167,8 +167,8 @@ struct CgFuse {
     unsigned int* counter;
     CondArg cond;
 };
-// Whether amg_vcycle_rz can take the CG's update (a tile-streamed hierarchy with two or more
-// smoothing steps and level 0's residual pass unfused).
+// Whether amg_vcycle_rz takes the CG's update (CFA_CG_FUSE_UPDATE=1, a tile-streamed hierarchy
+// with two smoothing steps and level 0's residual pass unfused).
 bool amg_can_fuse_update(const cfa_amg* amg);
 // amg_vcycle with the dots fused when the hierarchy runs tile-streamed (*fused = true); otherwise
 // the plain V-cycle (*fused = false) and the caller computes the dots. cg (nullable; only where

@@ -98,12 +98,33 @@ class SolveStep:
         self.amg.setup(self.n, self.nnz, self.dm.rp, self.dm.ci, self.Kp)
         return self.amg.setup_ms
 
-    def run(self):
+    def run(self, host_out=None):
+        """One step's solves. ``host_out`` = (u, v, dp) pinned host tensors: the momentum solution
+        is copied out on a side stream while the pressure system is assembled and solved (both only
+        read it), dp after its solve; the context's stream waits for the side copy, so one
+        synchronisation of it covers all three."""
+        import torch
         self.reset()
         self.assemble_momentum()
         self.solve_momentum()
+        side = None
+        if host_out is not None:
+            if getattr(self, "_copy_stream", None) is None:
+                self._copy_stream = torch.cuda.Stream()
+            side = self._copy_stream
+            ready = torch.cuda.Event()
+            ready.record(self.ctx.stream)
+            side.wait_event(ready)
+            with torch.cuda.stream(side):
+                host_out[0].copy_(self.u, non_blocking=True)
+                host_out[1].copy_(self.v, non_blocking=True)
         self.assemble_pressure()
         self.solve_pressure()
+        if side is not None:
+            host_out[2].copy_(self.dp, non_blocking=True)
+            joined = torch.cuda.Event()
+            joined.record(side)
+            self.ctx.stream.wait_event(joined)
 
     def report(self) -> dict:
         return dict(it_u=self.mom.iters[0], it_v=self.mom.iters[1], it_p=self.it_p,

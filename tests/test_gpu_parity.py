@@ -819,9 +819,15 @@ def test_step_matches_oracle(ctx, precision):
     u, v, p = fields(m)
     st = S.SolveStep(m, u, v, p, precision=precision, ctx=ctx)
     st.amg_setup()
-    st.run()
+    # the solutions copied to pinned host memory by the step itself (u, v during the pressure
+    # solve), one synchronisation of the context's stream
+    outs = [torch.empty(m.n, dtype=torch.float64).pin_memory() for _ in range(3)]
+    st.run(host_out=outs)
+    ctx.stream.synchronize()
     rep = st.report()
     assert all(rep["conv"]), rep
+    for o, d in zip(outs, (st.u, st.v, st.dp)):
+        assert np.array_equal(o.numpy(), host(d))
     rp, ci = st.dm.host_pattern()
     A, ru, rv, mass = O.assemble_momentum(m, rp, ci, u, v, u, v, p, O.bdf2_params())
     uu, vv = u.copy(), v.copy()
