@@ -188,6 +188,8 @@ def run_ours(args, rank, world):
     res = {}
     clk = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
     for prec_name, prec in (("fp64", cfa.FP64), ("mixed", cfa.MIXED)):
+        if args.profile and args.profile_precision not in ("both", prec_name):
+            continue
         st = S.SolveStep(m, u, v, p, precision=prec, ctx=ctx, dt=DT, nu=NU, stab=STAB, u_max=U_MAX, tol=TOL)
         # AMG setup: one untimed setup (first-touch allocations), then the mean of SETUP_REPS
         st.amg_setup()
@@ -682,6 +684,8 @@ def main():
                     help="c4: time the V-cycle tile heights per pattern class (cfa_autotune_set)")
     ap.add_argument("--step", action="store_true",
                     help="c2: time the whole step path (as c1 does) instead of the repeated solve pairs")
+    ap.add_argument("--profile-precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="--profile: the precision(s) whose step is profiled")
     ap.add_argument("--profile", action="store_true",
                     help="one step per precision between cudaProfilerStart/Stop (for ncu --profile-from-start off); no JSON line")
     args = ap.parse_args()
