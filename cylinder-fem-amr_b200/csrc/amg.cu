@@ -759,23 +759,30 @@ __global__ void k_vc_spmv(int n, const int* __restrict__ rp, const int* __restri
 }
 
 // x = M b with a dense row-major FP64 matrix (the coarsest inverse, k_dense_matvec, :929-937, or
-// the composite operator), one warp per row. A lane takes the columns lane + 32 k; eight of its
-// loads are issued before they are summed (eight partial sums, combined in a fixed order), so a
-// row costs a few L2 round trips rather than one per 32 columns.
+// the composite operator): one block of kDenseWarps warps per row, warp w taking the columns
+// [w cn / kDenseWarps, (w + 1) cn / kDenseWarps) with eight loads of each lane issued before they
+// are summed; the warps' partial sums are added in warp order. Four warps per row put four
+// times the loads in flight that one warp per row would (a 1069-row matrix is 1069 rows of
+// 8.5 KB: one warp per row leaves each SM eight warps).
+constexpr int kDenseWarps = 4;
+
 template <class B, class X>
-__global__ void k_vc_dense(int cn, const double* __restrict__ inv, const B* __restrict__ b, X* __restrict__ x,
-                           const int* __restrict__ done) {
+__global__ void __launch_bounds__(32 * kDenseWarps)
+k_vc_dense(int cn, const double* __restrict__ inv, const B* __restrict__ b, X* __restrict__ x,
+           const int* __restrict__ done) {
     CFA_GRID_DEP();
     if (done && *done) return;
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x & 31;
+    __shared__ double part[kDenseWarps];
+    const int i = blockIdx.x, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (i >= cn) return;
     const double* m = inv + (size_t)i * cn;
+    const int c0 = (int)((long long)cn * w / kDenseWarps), c1 = (int)((long long)cn * (w + 1) / kDenseWarps);
     constexpr int U = 8;
     double acc[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) acc[u] = 0.0;
-    int j = lane;
-    for (; j + 32 * (U - 1) < cn; j += 32 * U) {
+    int j = c0 + lane;
+    for (; j + 32 * (U - 1) < c1; j += 32 * U) {
         double a[U], g[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -785,10 +792,16 @@ __global__ void k_vc_dense(int cn, const double* __restrict__ inv, const B* __re
 #pragma unroll
         for (int u = 0; u < U; ++u) acc[u] += a[u] * g[u];
     }
-    for (; j < cn; j += 32) acc[0] += m[j] * (double)b[j];
+    for (; j < c1; j += 32) acc[0] += m[j] * (double)b[j];
     double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
     s = warp_sum(s);
-    if (lane == 0) x[i] = (X)s;
+    if (lane == 0) part[w] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = part[0];
+        for (int k = 1; k < kDenseWarps; ++k) t += part[k];
+        x[i] = (X)t;
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1108,14 +1121,14 @@ static void vcycle_level(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     const T* cx;
     if (!last && l + 1 == amg->comp_level) {
         cx = view<T>(amg->levels[l + 1]).x;
-        CFA_LAUNCH(ctx, (k_vc_dense<T, T>), ceil_div((long long)amg->comp_n * 32, kThreads), kThreads, 0,
+        CFA_LAUNCH(ctx, (k_vc_dense<T, T>), amg->comp_n, 32 * kDenseWarps, 0,
                    amg->comp_n, amg->comp.p, (const T*)cb, view<T>(amg->levels[l + 1]).x, done);
     } else if (!last) {
         vcycle_level<T, T>(ctx, amg, l + 1, cb, nullptr, done);
         cx = view<T>(amg->levels[l + 1]).x;
     } else {
         T* dst = std::is_same<T, double>::value ? (T*)amg->cx64.p : (T*)amg->cx32.p;
-        CFA_LAUNCH(ctx, (k_vc_dense<T, T>), ceil_div((long long)amg->coarse_n * 32, kThreads), kThreads, 0,
+        CFA_LAUNCH(ctx, (k_vc_dense<T, T>), amg->coarse_n, 32 * kDenseWarps, 0,
                    amg->coarse_n, amg->coarse_inv.p, (const T*)cb, dst, done);
         cx = dst;
     }
@@ -1425,7 +1438,7 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     const T* cx;
     if (!last && l + 1 == amg->comp_level) {
         if (!dry)
-            CFA_LAUNCH(ctx, (k_vc_dense<T, T>), ceil_div((long long)amg->comp_n * 32, kThreads), kThreads, 0,
+            CFA_LAUNCH(ctx, (k_vc_dense<T, T>), amg->comp_n, 32 * kDenseWarps, 0,
                        amg->comp_n, amg->comp.p, (const T*)cb, TVec<T>::x(amg->levels[l + 1]), done);
         cx = TVec<T>::x(amg->levels[l + 1]);
     } else if (!last && l + 1 == amg->tail_level && std::is_same<T, double>::value) {
@@ -1436,7 +1449,7 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
         cx = TVec<T>::x(amg->levels[l + 1]);
     } else {
         if (!dry)
-            CFA_LAUNCH(ctx, (k_vc_dense<T, T>), ceil_div((long long)amg->coarse_n * 32, kThreads), kThreads, 0,
+            CFA_LAUNCH(ctx, (k_vc_dense<T, T>), amg->coarse_n, 32 * kDenseWarps, 0,
                        amg->coarse_n, amg->coarse_inv.p, (const T*)cb, TVec<T>::cx(amg), done);
         cx = TVec<T>::cx(amg);
     }
@@ -1486,7 +1499,7 @@ bool amg_can_fuse_update(const cfa_amg* amg) {
 
 cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done) {
     if (amg->levels.empty()) {
-        CFA_LAUNCH(ctx, (k_vc_dense<double, double>), ceil_div((long long)amg->coarse_n * 32, kThreads), kThreads, 0,
+        CFA_LAUNCH(ctx, (k_vc_dense<double, double>), amg->coarse_n, 32 * kDenseWarps, 0,
                    amg->coarse_n, amg->coarse_inv.p, r, z, done);
     } else if (amg->tiled) {
         vcycle_tiled_top(ctx, amg, r, z, done, false);

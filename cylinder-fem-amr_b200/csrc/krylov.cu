@@ -1829,7 +1829,7 @@ static cfa_status b2_body(cfa_ctx* ctx, B2Work& W, const B2Args& a, CondArg cond
     else
         OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_t<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, pair(W.shat.p),
                                       pair(W.s.p), pair(W.t.p), W.st.p, W.part.p, W.counter.p));
-    CFA_LAUNCH(ctx, k_b2_xr, row_grid(ctx, n, 1), kThreads, 0, n, a.xu, a.xv, pair(W.phat.p), pair(W.shat.p),
+    CFA_LAUNCH(ctx, k_b2_xr, gv, kThreads, 0, n, a.xu, a.xv, pair(W.phat.p), pair(W.shat.p),
                pair(W.s.p), pair(W.t.p), pair(W.r.p), pair(W.r0.p), W.st.p, W.part.p, W.counter.p, cond);
     CFA_CHECK_LAUNCH();
     return CFA_OK;
