@@ -870,7 +870,15 @@ __global__ void k_bm_eye(int nb, double* __restrict__ B) {
 // VC_RESTRICT (fused transfers): y = [R | -R A] [b ; x] over the next level's rows;
 // VC_ADDJAC: with x' = x + P xc, y = x' + omega D^-1 (b - A x'), x' never stored: sums of
 // [A | A P] and [I | P] over [x ; xc]. A column with the top bit set reads the second vector.
-enum VcOp { VC_PRE = 0, VC_JAC = 1, VC_RES = 2, VC_SPMV = 3, VC_ADD = 4, VC_RESTRICT = 5, VC_ADDJAC = 6 };
+// Explicitly rounded product and fused multiply-add, so that two kernels which form the same
+// value in different places round it the same way whatever the compiler contracts.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// VC_PREC: VC_PRE with its first iterate c = omega D^-1 b given (x = c, formed by the caller).
+enum VcOp { VC_PRE = 0, VC_JAC = 1, VC_RES = 2, VC_SPMV = 3, VC_ADD = 4, VC_RESTRICT = 5, VC_ADDJAC = 6, VC_PREC = 7 };
 constexpr int kSecondVec = (int)0x80000000u;
 
 template <int TPR, int OP, class V, class T, class B, class O, bool RZ = false, bool CGU = false>
@@ -898,11 +906,12 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
             const double alpha = CGU ? cgf.st->alpha : 0.0;
             double rn = 0.0;
             if (valid && lane == 0) {
-                if (OP == VC_PRE || OP == VC_JAC || OP == VC_ADDJAC) di = dinv[row];
+                if (OP == VC_PRE || OP == VC_PREC || OP == VC_JAC || OP == VC_ADDJAC) di = dinv[row];
+                if (OP == VC_PREC) xi = x[row];
                 if (CGU) {
                     rn = (double)b[row] + -alpha * cgf.q[row];
                     bi = (T)rn;
-                } else if (OP == VC_PRE || OP == VC_JAC || OP == VC_RES || OP == VC_ADDJAC) {
+                } else if (OP == VC_PRE || OP == VC_PREC || OP == VC_JAC || OP == VC_RES || OP == VC_ADDJAC) {
                     bi = (T)b[row];
                 }
                 if (OP == VC_JAC) xi = x[row];
@@ -935,7 +944,7 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
 #pragma unroll
                     for (int u = 0; u < kGatherBatch; ++u)
                         if (e0 + u * TPR < end) {
-                            if (OP == VC_PRE) s += (T)a[u] * (omega * g0[u] * (T)g1[u]);
+                            if (OP == VC_PRE) s += (T)a[u] * mul_rn(omega * g0[u], (T)g1[u]);
                             else s += (T)a[u] * g0[u];
                             if (OP == VC_ADDJAC) s1 += (T)a1[u] * g0[u];
                         }
@@ -949,8 +958,12 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
             }
             if (valid && lane == 0) {
                 if (OP == VC_PRE) {
-                    const T x0 = omega * di * bi;
-                    y[row] = (O)(x0 + omega * di * (bi - s));
+                    // rounded product, then one fused multiply-add: the same operations as the
+                    // pre-scaled form, whose first iterate the caller stored
+                    const T od = omega * di;
+                    y[row] = (O)fma_rn(od, bi - s, mul_rn(od, bi));
+                } else if (OP == VC_PREC) {
+                    y[row] = (O)fma_rn(omega * di, bi - s, xi);
                 } else if (OP == VC_JAC) {
                     const O out = (O)(xi + omega * di * (bi - s));
                     y[row] = out;
@@ -1026,7 +1039,8 @@ static void vct(cfa_ctx* ctx, bool dry, const TiledCsr& M, int* err, const T* di
     constexpr bool kRz = OP == VC_JAC && std::is_same<O, double>::value && std::is_same<B, double>::value;
     constexpr bool kCgu = (OP == VC_PRE || OP == VC_RES) && std::is_same<B, double>::value;
     const int tpr = M.tpr;
-    const TileView tv = M.view(err);
+    TileView tv = M.view(err);
+    tv.l2hint = l2_hint_vcycle();
     const TileLaunch L = tile_launch(ctx, M, nullptr);
     const RzFuse none{};
     const CgFuse nocg{};
@@ -1404,7 +1418,7 @@ struct TVec<float> {
 // only, no launches)
 template <class V, class T, class B>
 static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* z, const int* done, bool dry,
-                         const RzFuse* rz = nullptr, const CgFuse* cg = nullptr) {
+                         const RzFuse* rz = nullptr, const CgFuse* cg = nullptr, const T* c0 = nullptr) {
     AmgLevel& L = amg->levels[l];
     const int s = amg->opts.smooth_steps;
     int* err = amg->err.p;
@@ -1412,7 +1426,10 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     const T* dinv = TVec<T>::dinv(L);
     T* x = TVec<T>::x(L);
     T* t = TVec<T>::t(L);
-    if (s >= 2) {
+    if (s >= 2 && c0 && !cg) {   // the first iterate formed by the caller
+        vct<VC_PREC, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, c0, x, done);
+    } else if (s >= 2) {
+        if (dry) vct<VC_PREC, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)nullptr, x, done);
         vct<VC_PRE, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)nullptr, x, done, nullptr, nullptr, cg);
     } else if (!dry) {
         CFA_TPR_SWITCH(L.A.tpr, CFA_LAUNCH(ctx, (k_vc_pre<TPR, T, B>), row_grid(ctx, L.A.rows, L.A.tpr), kThreads, 0,
@@ -1481,10 +1498,24 @@ static bool vcycle_fp32(const cfa_amg* amg) {
 }
 
 static void vcycle_tiled_top(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, bool dry,
-                             const RzFuse* rz = nullptr, const CgFuse* cg = nullptr) {
-    if (amg->opts.precision != CFA_MIXED) vcycle_tiled<double, double, double>(ctx, amg, 0, r, z, done, dry, rz, cg);
-    else if (vcycle_fp32(amg)) vcycle_tiled<float, float, double>(ctx, amg, 0, r, z, done, dry, rz, cg);
-    else vcycle_tiled<float, double, double>(ctx, amg, 0, r, z, done, dry, rz, cg);
+                             const RzFuse* rz = nullptr, const CgFuse* cg = nullptr, const void* c0 = nullptr) {
+    if (amg->opts.precision != CFA_MIXED)
+        vcycle_tiled<double, double, double>(ctx, amg, 0, r, z, done, dry, rz, cg, (const double*)c0);
+    else if (vcycle_fp32(amg))
+        vcycle_tiled<float, float, double>(ctx, amg, 0, r, z, done, dry, rz, cg, (const float*)c0);
+    else
+        vcycle_tiled<float, double, double>(ctx, amg, 0, r, z, done, dry, rz, cg, (const double*)c0);
+}
+
+bool amg_prescale(const cfa_amg* amg, PreScale* out) {
+    const char* e = std::getenv("CFA_PRESCALE");
+    if ((e && e[0] == '0') || !amg || amg->levels.empty() || !amg->tiled || amg->opts.smooth_steps < 2) return false;
+    const AmgLevel& L = amg->levels[0];
+    const bool f32 = vcycle_fp32(amg);
+    out->dinv = f32 ? (const void*)L.dinv32.p : (const void*)L.dinv.p;
+    out->omega = L.omega;
+    out->fp32 = f32 ? 1 : 0;
+    return true;
 }
 
 // Off unless CFA_CG_FUSE_UPDATE=1: measured at c1 the folded step was not faster (13.78 against
@@ -1513,12 +1544,13 @@ cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, co
 }
 
 cfa_status amg_vcycle_rz(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, const RzFuse& f,
-                         bool* fused, const CgFuse* cg) {
+                         bool* fused, const CgFuse* cg, const void* c) {
     *fused = false;
     if (cg && !amg_can_fuse_update(amg))
         return set_error(ctx, CFA_BAD_ARG, "the CG update cannot be folded into this hierarchy", __FILE__, __LINE__);
     if (amg->levels.empty() || !amg->tiled || amg->opts.smooth_steps < 1) return amg_vcycle(ctx, amg, r, z, done);
-    vcycle_tiled_top(ctx, amg, r, z, done, false, &f, cg);
+    if (c && cg) return set_error(ctx, CFA_BAD_ARG, "prescaled residual with the folded update", __FILE__, __LINE__);
+    vcycle_tiled_top(ctx, amg, r, z, done, false, &f, cg, c);
     CFA_CHECK_LAUNCH();
     *fused = true;
     return CFA_OK;

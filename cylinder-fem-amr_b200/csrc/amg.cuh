@@ -170,9 +170,20 @@ struct CgFuse {
 // Whether amg_vcycle_rz takes the CG's update (CFA_CG_FUSE_UPDATE=1, a tile-streamed hierarchy
 // with two smoothing steps and level 0's residual pass unfused).
 bool amg_can_fuse_update(const cfa_amg* amg);
+// The level-0 pre-smoothing's scaling: its first iterate is c = omega0 D0^-1 r in the V-cycle's
+// level-0 vector type (fp32: float), which a caller that writes r anyway can form (dinv, omega)
+// so that the pre-smoothing gathers c alone. False where the V-cycle does not take c (not
+// tile-streamed, fewer than two smoothing steps, or CFA_PRESCALE=0).
+struct PreScale {
+    const void* dinv;
+    double omega;
+    int fp32;
+};
+bool amg_prescale(const cfa_amg* amg, PreScale* out);
 // amg_vcycle with the dots fused when the hierarchy runs tile-streamed (*fused = true); otherwise
 // the plain V-cycle (*fused = false) and the caller computes the dots. cg (nullable; only where
-// amg_can_fuse_update) folds the CG's update into level 0.
+// amg_can_fuse_update) folds the CG's update into level 0; c (nullable; only where amg_prescale)
+// is omega0 D0^-1 r, formed by the caller.
 cfa_status amg_vcycle_rz(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, const RzFuse& f,
-                         bool* fused, const CgFuse* cg = nullptr);
+                         bool* fused, const CgFuse* cg = nullptr, const void* c = nullptr);
 }  // namespace cfa

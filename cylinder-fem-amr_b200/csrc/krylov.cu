@@ -527,11 +527,15 @@ __global__ void k_inv_diag(int n, const int* __restrict__ rp, const int* __restr
 }
 
 // x += alpha pn, r -= alpha q, p = pn, ||r|| test (:237-247); JAC: z = D^-1 r and r.z -> beta
-template <bool JAC>
+// SC (float or double, with JAC false): also c = omega0 D0^-1 r in the AMG's level-0 vector type,
+// the pre-smoothing's first iterate, which the V-cycle's level-0 pre-smoothing then gathers in
+// place of D0^-1 and r (PreScale); the product is formed as that pass forms it.
+template <bool JAC, class SC = double>
 __global__ void __launch_bounds__(kThreads)
 k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ pn, double* __restrict__ p,
             const double* __restrict__ q, const double* __restrict__ dinv, double* __restrict__ z,
-            CgState* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond) {
+            CgState* __restrict__ st, double* __restrict__ part, unsigned int* __restrict__ counter, CondArg cond,
+            const SC* __restrict__ dinv0 = nullptr, SC omega0 = SC(0), SC* __restrict__ c0 = nullptr) {
     CFA_GRID_DEP();
     if (st->done) return;
     __shared__ double sh[2 * kWarps];
@@ -543,6 +547,7 @@ k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, const double*
         const double ri = r[i] + -alpha * q[i];
         r[i] = ri;
         p[i] = pi;
+        if (c0) c0[i] = SC(omega0 * dinv0[i]) * (SC)ri;   // the level-0 pre-smoothing's (omega D^-1) b, rounded
         v[0] += ri * ri;
         if (JAC) {
             const double zi = dinv[i] * ri;
@@ -1113,6 +1118,7 @@ struct SegGraph {
 struct PcgWork {
     int cap = 0;
     DevBuf<double> r, z, p, pn, q, gx, gy, dinv;
+    DevBuf<double> c0;                 // omega0 D0^-1 r for the V-cycle's level 0 (float or double elements)
     DevBuf<CgState> st;
     // tile-streamed copy of the operator: K - B^T M^-1 B as one matrix on the two-ring pattern
     // (fused), else pass 1: Bx, By; pass 2: K [, BTx, BTy]
@@ -1282,7 +1288,8 @@ static void launch_opt_k(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, const doubl
                          const double* beta_ptr, double* pn, double* q, CondArg cond, const int* done) {
     const cfa_mesh* m = a.oss ? a.oss->mesh : nullptr;
     OutletBc bc = m ? m->bc : OutletBc{};
-    const TileView tv = W.tk.view(W.err.p);
+    TileView tv = W.tk.view(W.err.p);
+    tv.l2hint = l2_hint_operator();
     TileLaunch L;
     TILE_TPR_SWITCH(W.tk.tpr,
         L = tile_launch(ctx, W.tk, (const void*)k_opt_k<TPR, OSS, FUSEP, DOT>);
@@ -1420,25 +1427,40 @@ static cfa_status pcg_piece(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, int piec
                        W.counter.p, cond);
         if (a.amg || a.prec) {
             // the update (x, r, p, |r|, the stopping test) folded into the V-cycle's level 0 where
-            // the hierarchy allows it, else its own kernel
+            // the hierarchy allows it (opt-in), else its own kernel, which also forms the level-0
+            // pre-smoothing's scaled residual where the V-cycle takes it
             const bool fuse_update = !a.prec && amg_can_fuse_update(a.amg);
-            if (!fuse_update)
-                CFA_LAUNCH(ctx, k_cg_update<false>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p,
-                           (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond);
+            PreScale ps{};
+            const bool prescale = !a.prec && !fuse_update && amg_prescale(a.amg, &ps);
+            if (!fuse_update) {
+                if (prescale && ps.fp32)
+                    CFA_LAUNCH(ctx, (k_cg_update<false, float>), gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p,
+                               (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond,
+                               (const float*)ps.dinv, (float)ps.omega, reinterpret_cast<float*>(W.c0.p));
+                else if (prescale)
+                    CFA_LAUNCH(ctx, (k_cg_update<false, double>), gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p,
+                               W.q.p, (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond,
+                               (const double*)ps.dinv, ps.omega, W.c0.p);
+                else
+                    CFA_LAUNCH(ctx, (k_cg_update<false, double>), gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p,
+                               W.q.p, (const double*)nullptr, (double*)nullptr, st, W.part.p, W.counter.p, cond,
+                               (const double*)nullptr, 0.0, (double*)nullptr);
+            }
             if (!a.prec) {
                 // z = M^-1 r with r.z (and z.q) folded into the V-cycle's last sweep where it can be
                 const int flexible = pcg_flexible(a.amg);
                 const RzFuse f{W.q.p, flexible, &st->rz, &st->beta, &st->alpha, W.part.p, W.counter.p};
                 const CgFuse g{W.r.p, W.q.p, W.pn.p, a.x, W.p.p, st, W.part.p, W.counter.p, cond};
                 bool fused = false;
-                CFA_PROPAGATE(amg_vcycle_rz(ctx, a.amg, W.r.p, W.z.p, done, f, &fused, fuse_update ? &g : nullptr));
+                CFA_PROPAGATE(amg_vcycle_rz(ctx, a.amg, W.r.p, W.z.p, done, f, &fused, fuse_update ? &g : nullptr,
+                                            prescale ? (const void*)W.c0.p : nullptr));
                 if (!fused)
                     CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, flexible, st,
                                W.part.p, W.counter.p, cond);
             }
         } else {
-            CFA_LAUNCH(ctx, k_cg_update<true>, gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p, W.dinv.p, W.z.p,
-                       st, W.part.p, W.counter.p, cond);
+            CFA_LAUNCH(ctx, (k_cg_update<true, double>), gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p, W.dinv.p, W.z.p,
+                       st, W.part.p, W.counter.p, cond, (const double*)nullptr, 0.0, (double*)nullptr);
         }
     } else if (a.prec) {
         CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, 0, st, W.part.p,
@@ -1510,7 +1532,7 @@ static cfa_status ensure_pcg_vectors(cfa_ctx* ctx, PcgWork& W, int n) {
     if (n > W.cap) {
         W.graph.reset();
         for (SegGraph& g : W.seg) g.reset();
-        for (DevBuf<double>* b : {&W.r, &W.z, &W.p, &W.pn, &W.q, &W.gx, &W.gy, &W.dinv}) CFA_CUDA(b->ensure(n));
+        for (DevBuf<double>* b : {&W.r, &W.z, &W.p, &W.pn, &W.q, &W.gx, &W.gy, &W.dinv, &W.c0}) CFA_CUDA(b->ensure(n));
         CFA_CUDA(W.st.ensure(1));
         CFA_CUDA(W.counter.ensure(1));
         CFA_CUDA(cudaMemsetAsync(W.counter.p, 0, sizeof(unsigned int), ctx->stream));

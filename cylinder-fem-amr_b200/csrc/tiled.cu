@@ -12,6 +12,16 @@
 
 namespace cfa {
 
+static int l2_hint_env(const char* name, int dflt) {
+    const char* e = std::getenv(name);
+    if (!e || !*e) return dflt;
+    const int v = std::atoi(e);
+    return v >= 0 && v <= 2 ? v : dflt;
+}
+
+int l2_hint_operator() { return l2_hint_env("CFA_L2_OP", 0); }
+int l2_hint_vcycle() { return l2_hint_env("CFA_L2_VC", 0); }
+
 bool tile_early_enabled() {
     static const bool on = [] {
         const char* e = std::getenv("CFA_TILE_EARLY");

@@ -39,7 +39,13 @@ struct TileView {
     int max_chunk = 0;                // bytes
     int* err = nullptr;               // device error word (timeout)
     int early = 0;                    // signal dependents as soon as the first copies are issued
+    int l2hint = 0;                   // L2 policy of the tile copies: 0 normal, 1 evict first, 2 evict last
 };
+
+// L2 policies of the tile streams: the pressure operator's tiles (CFA_L2_OP) and the V-cycle's
+// level tiles (CFA_L2_VC), each 0 (normal), 1 (evict first) or 2 (evict last).
+int l2_hint_operator();
+int l2_hint_vcycle();
 
 // Tile kernels signal their dependent launch (griddepcontrol.launch_dependents) right after
 // issuing their first tile copies, so the next kernel's blocks are scheduled and issue their own
@@ -126,6 +132,25 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                  : "memory");
 }
 
+// The same copy with an L2 cache policy made by createpolicy.
+__device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, unsigned bytes, uint64_t* bar,
+                                              uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+
+__device__ __forceinline__ uint64_t l2_policy(int hint) {
+    uint64_t p;
+    if (hint == 1)
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    else
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
     uint32_t ok;
     asm volatile(
@@ -148,7 +173,10 @@ __device__ __forceinline__ void tile_issue(const TileView& tv, int t, unsigned c
     const long long o0 = tv.off[t], o1 = tv.off[t + 1];
     const unsigned bytes = (unsigned)(o1 - o0);
     mbar_expect_tx(bar, bytes);
-    bulk_g2s(dst, tv.data + o0, bytes, bar);
+    if (tv.l2hint)
+        bulk_g2s_hint(dst, tv.data + o0, bytes, bar, l2_policy(tv.l2hint));
+    else
+        bulk_g2s(dst, tv.data + o0, bytes, bar);
 }
 
 // Runs body(tile, row0, nrows, chunk) for every tile of this CTA (all threads call it; the

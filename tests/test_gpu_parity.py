@@ -218,6 +218,35 @@ def test_ilu_colouring_factor_apply(ctx, precision):
 
 
 @pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
+def test_ilu_sweep_orders_give_the_same_bits(ctx, precision, monkeypatch):
+    """The interleaved-pair ILU apply in its three sweep forms: rows in the reference's natural
+    order (CFA_ILU_PERM=0), the work vector in colour order between a first and a last pass over
+    all rows (1), and the colour kernels reading r and writing z at the rows' natural places
+    themselves (2, the default). The two colour-order forms perform the same operations, so their
+    results are bit for bit the same; the natural-order form agrees to rounding."""
+    from tests.golden.make_golden import momentum_ilu_matrix
+    m = mesh("c0")
+    rp, ci = O.csr_build(m.n, m.elem_v)
+    n = m.n
+    a, b = momentum_ilu_matrix(rp, ci)
+    ilu = cfa.MulticolourIlu0(ctx, precision)
+    ilu.set_pattern(n, rp, ci, dev(rp, torch.int32), dev(ci, torch.int32))
+    assert ilu.n_colours >= 3
+    ilu.factor(dev(a))
+    r = dev(np.stack([b[:n], b[n:]], 1).ravel())
+    out = {}
+    for order in ("0", "1", "2"):
+        monkeypatch.setenv("CFA_ILU_PERM", order)
+        z = torch.full((2 * n,), np.nan, dtype=torch.float64, device="cuda")
+        ilu.apply_interleaved(r, z)
+        out[order] = host(z)
+    assert np.isfinite(out["2"]).all()
+    assert np.array_equal(out["1"], out["2"])
+    tol = 1e-13 if precision == cfa.FP64 else 1e-6
+    assert np.abs(out["0"] - out["2"]).max() <= tol * np.abs(out["0"]).max()
+
+
+@pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
 def test_ilu_set_pattern_reuses_the_handle(ctx, precision):
     """set_pattern on a handle that held another (larger) pattern gives the same colouring, factor
     and sweeps as a fresh handle, and the transposed factor follows the new pattern."""
@@ -659,6 +688,30 @@ def test_pcg_update_folded_into_vcycle_matches_update_kernel(ctx, prec, monkeypa
     Ax = O.spmv(rp, ci, Kp, x)
     O.oss_apply(m, rp, ci, oss, inv_m, x, Ax)
     assert np.linalg.norm(rhs - Ax) <= 1.5e-10 * np.linalg.norm(rhs)
+
+
+@pytest.mark.parametrize("prec", [cfa.FP64, cfa.MIXED])
+def test_pcg_prescaled_residual_gives_the_same_bits(ctx, prec, monkeypatch):
+    """The CG update writing c = omega0 D0^-1 r (in the V-cycle's vector type) for the level-0
+    pre-smoothing, which then gathers c instead of D0^-1 and r: the products are formed in the
+    same order, so the solve is bit-identical to the one that forms them inside the V-cycle."""
+    m = mesh("c0")
+    dm = cfa.DeviceMesh(ctx, m)
+    rp, ci = dm.host_pattern()
+    Kp, rhs, oss, inv_m = pressure_system(m, rp, ci)
+    dK, db, doss, dinv = dev(Kp), dev(rhs), dev(oss), dev(inv_m)
+    out = {}
+    for pre in ("1", "0"):
+        monkeypatch.setenv("CFA_PRESCALE", pre)
+        amg = cfa.AmgPreconditioner(ctx, prec)
+        amg.setup(m.n, ci.size, dm.rp, dm.ci, dK)
+        s = cfa.GpuLinearSolver(ctx)
+        x = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+        it = s.solve_pcg(m.n, dm.rp, dm.ci, dK, db, x, 4000, 1e-10, cfa.oss_operator(dm, doss, dinv), amg)
+        assert s.converged
+        out[pre] = (it, host(x))
+    assert out["1"][0] == out["0"][0]
+    assert np.array_equal(out["1"][1], out["0"][1])
 
 
 @pytest.mark.parametrize("host_prec", [False, True])
