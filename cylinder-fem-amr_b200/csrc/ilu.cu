@@ -577,167 +577,6 @@ static void sweeps_perm(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv
                (const typename Pair<T>::type*)w, z, done);
 }
 
-// ---- the colour-order sweeps reading r and writing z at the rows' natural places ----
-// The same arithmetic as the kernels above, without their first and last passes over all rows:
-// a colour kernel reads its rows' right-hand side r[rows[t]] itself, the forward sweep gathers a
-// colour-0 neighbour's value straight from r (colour 0 has no L entries, so its forward value
-// is r converted to the work precision; lcn holds such columns as ~natural row), every kernel
-// that finishes a row (the last colour's forward step, the backward steps) writes z[rows[t]],
-// and colour 0's backward step, the last kernel, runs over colour 0's positions only.
-template <class T>
-__device__ __forceinline__ typename Pair<T>::type pair_of(double2 v) {
-    typename Pair<T>::type o;
-    o.x = (T)v.x;
-    o.y = (T)v.y;
-    return o;
-}
-
-template <class V, class T>
-__global__ void __launch_bounds__(kThreads)
-k_ilu_lower_io(int m, int cs, const int* __restrict__ rows, const int* __restrict__ lp, const int* __restrict__ lcn,
-               const V* __restrict__ lv, const V* __restrict__ dinv, int last, const double2* __restrict__ r,
-               typename Pair<T>::type* __restrict__ w, double2* __restrict__ z, const int* __restrict__ done,
-               int early) {
-    using T2 = typename Pair<T>::type;
-    const int tl = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = tl < m;
-    const int t = cs + tl;
-    int b = 0, e = 0, nat = 0;
-    int j[kIluBatch];
-    V l[kIluBatch];
-    V d = V(0);
-    if (valid) {
-        nat = __ldg(rows + t);
-        b = __ldg(lp + t);
-        e = __ldg(lp + t + 1);
-#pragma unroll
-        for (int u = 0; u < kIluBatch; ++u)
-            if (b + u < e) {
-                j[u] = __ldg(lcn + b + u);
-                l[u] = __ldg(lv + b + u);
-            }
-        if (last) d = __ldg(dinv + t);
-    }
-    if (early) pdl_launch_dependents();
-    CFA_GRID_DEP();
-    if (done && *done) return;
-    if (!valid) return;
-    const T2 own = pair_of<T>(r[nat]);
-    T a0 = own.x, a1 = own.y;
-    {
-        T2 g[kIluBatch];
-#pragma unroll
-        for (int u = 0; u < kIluBatch; ++u)
-            if (b + u < e) g[u] = j[u] >= 0 ? w[j[u]] : pair_of<T>(r[~j[u]]);
-#pragma unroll
-        for (int u = 0; u < kIluBatch; ++u)
-            if (b + u < e) {
-                a0 -= (T)l[u] * g[u].x;
-                a1 -= (T)l[u] * g[u].y;
-            }
-    }
-    for (int e0 = b + kIluBatch; e0 < e; e0 += kIluBatch) {
-        V lq[kIluBatch];
-        T2 g[kIluBatch];
-#pragma unroll
-        for (int u = 0; u < kIluBatch; ++u)
-            if (e0 + u < e) {
-                lq[u] = __ldg(lv + e0 + u);
-                const int jj = __ldg(lcn + e0 + u);
-                g[u] = jj >= 0 ? w[jj] : pair_of<T>(r[~jj]);
-            }
-#pragma unroll
-        for (int u = 0; u < kIluBatch; ++u)
-            if (e0 + u < e) {
-                a0 -= (T)lq[u] * g[u].x;
-                a1 -= (T)lq[u] * g[u].y;
-            }
-    }
-    if (last) {
-        a0 = a0 * (T)d;
-        a1 = a1 * (T)d;
-    }
-    T2 o;
-    o.x = a0;
-    o.y = a1;
-    w[t] = o;
-    if (last) z[nat] = make_double2((double)a0, (double)a1);
-}
-
-// Backward sweep of colour c >= 1 (positions cs .. cs + m): in place in w, and the row's z.
-template <class V, class T>
-__global__ void __launch_bounds__(kThreads)
-k_ilu_upper_io(int m, int cs, const int* __restrict__ rows, const int* __restrict__ up, const int* __restrict__ ucp,
-               const V* __restrict__ uv, const V* __restrict__ dinv, typename Pair<T>::type* __restrict__ w,
-               double2* __restrict__ z, const int* __restrict__ done, int early) {
-    using T2 = typename Pair<T>::type;
-    const int tl = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = tl < m;
-    const int t = cs + tl;
-    int b = 0, e = 0, nat = 0;
-    int j[kIluBatch];
-    V q[kIluBatch];
-    V d = V(0);
-    if (valid) {
-        nat = __ldg(rows + t);
-        ilu_upper_prefetch(t, up, ucp, uv, dinv, b, e, j, q, d);
-    }
-    if (early) pdl_launch_dependents();
-    CFA_GRID_DEP();
-    if (done && *done) return;
-    if (!valid) return;
-    const T2 o = ilu_upper_row<V, T>(w[t], b, e, j, q, d, ucp, uv, w);
-    w[t] = o;
-    z[nat] = make_double2((double)o.x, (double)o.y);
-}
-
-// Colour 0's backward step (positions 0 .. m), the last kernel: from r, into z.
-template <class V, class T>
-__global__ void __launch_bounds__(kThreads)
-k_ilu_colour0_io(int m, const int* __restrict__ rows, const int* __restrict__ up, const int* __restrict__ ucp,
-                 const V* __restrict__ uv, const V* __restrict__ dinv, const double2* __restrict__ r,
-                 const typename Pair<T>::type* __restrict__ w, double2* __restrict__ z, const int* __restrict__ done) {
-    using T2 = typename Pair<T>::type;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = t < m;
-    int b = 0, e = 0, nat = 0;
-    int j[kIluBatch];
-    V q[kIluBatch];
-    V d = V(0);
-    if (valid) {
-        nat = __ldg(rows + t);
-        ilu_upper_prefetch(t, up, ucp, uv, dinv, b, e, j, q, d);
-    }
-    CFA_GRID_DEP();
-    if (done && *done) return;
-    if (!valid) return;
-    const T2 o = ilu_upper_row<V, T>(pair_of<T>(r[nat]), b, e, j, q, d, ucp, uv, w);
-    z[nat] = make_double2((double)o.x, (double)o.y);
-}
-
-template <class V, class T>
-static void sweeps_io(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv, const V* dinv,
-                      typename Pair<T>::type* w, const double2* r, double2* z, const int* done) {
-    static const int early = env_flag("CFA_ILU_EARLY", 1);
-    const int* rows = h->rows.p;
-    for (int c = 1; c < h->nc; ++c) {
-        const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
-        if (m == 0) continue;
-        CFA_LAUNCH(ctx, (k_ilu_lower_io<V, T>), ceil_div(m, kThreads), kThreads, 0, m, cs, rows, (const int*)h->lp.p,
-                   (const int*)h->lcn.p, lv, dinv, c == h->nc - 1 ? 1 : 0, r, w, z, done, early);
-    }
-    for (int c = h->nc - 2; c >= 1; --c) {
-        const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
-        if (m == 0) continue;
-        CFA_LAUNCH(ctx, (k_ilu_upper_io<V, T>), ceil_div(m, kThreads), kThreads, 0, m, cs, rows, (const int*)h->up.p,
-                   (const int*)h->ucp.p, uv, dinv, w, z, done, early);
-    }
-    const int m0 = h->colour_start[1];
-    if (m0 > 0)
-        CFA_LAUNCH(ctx, (k_ilu_colour0_io<V, T>), ceil_div(m0, kThreads), kThreads, 0, m0, rows, (const int*)h->up.p,
-                   (const int*)h->ucp.p, uv, dinv, r, (const typename Pair<T>::type*)w, z, done);
-}
-
 // pos[rows[t]] = t, and the split pattern's column indices as colour positions
 __global__ void k_ilu_positions(int n, const int* __restrict__ rows, int* __restrict__ pos) {
     CFA_GRID_DEP();
@@ -752,17 +591,6 @@ __global__ void k_ilu_map_cols(int count, const int* __restrict__ cols, const in
     if (e < count) out[e] = pos[cols[e]];
 }
 
-// lcp with the colour-0 columns (positions below c1) as ~natural row, for the sweeps that read r
-__global__ void k_ilu_map_cols_io(int count, const int* __restrict__ cols, const int* __restrict__ pos, int c1,
-                                  int* __restrict__ out) {
-    CFA_GRID_DEP();
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < count) {
-        const int c = cols[e];
-        const int t = pos[c];
-        out[e] = t < c1 ? ~c : t;
-    }
-}
 
 // Position of the mirrored entry (j, i) of every CSR entry (i, j) (binary search in row j);
 // err set when the pattern is not structurally symmetric.
@@ -832,26 +660,20 @@ cfa_status ilu_apply(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z,
 cfa_status ilu_apply_pair(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z, const int* done) {
     const double2* r2 = reinterpret_cast<const double2*>(r);
     double2* z2 = reinterpret_cast<double2*>(z);
-    // 2: colour-order sweeps reading r and writing z in place of the rows (default); 1: colour
-    // order with a first and a last pass over all rows; 0: the reference's natural order
-    const char* pe = std::getenv("CFA_ILU_PERM");
-    const int perm = pe && *pe ? std::atoi(pe) : 2;
-    const bool colour_order = perm && h->nc >= 2;
-    const bool io = perm == 2 && r != z;
+    // colour order (default) or, with CFA_ILU_PERM=0, the reference's natural row order
+    const bool colour_order = env_flag("CFA_ILU_PERM", 1) && h->nc >= 2;
     if (h->precision == CFA_MIXED) {
         // FP32 factors, FP32 sweeps on the handle's FP32 work vector; FP64 in and out
         if (!h->work32.p || h->work32.cap < 2 * (size_t)h->n)
             return set_error(ctx, CFA_BAD_ARG, "ILU handle without its FP32 work vector", __FILE__, __LINE__);
         float2* w = reinterpret_cast<float2*>(h->work32.p);
-        if (colour_order && io) sweeps_io<float, float>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r2, z2, done);
-        else if (colour_order) sweeps_perm<float, float>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r2, z2, done);
+        if (colour_order) sweeps_perm<float, float>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r2, z2, done);
         else sweeps_pair<float, float, true>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r2, z2, done);
     } else if (colour_order) {
         if (!h->work64.p || h->work64.cap < 2 * (size_t)h->n)
             return set_error(ctx, CFA_BAD_ARG, "ILU handle without its FP64 work vector", __FILE__, __LINE__);
-        double2* w = reinterpret_cast<double2*>(h->work64.p);
-        if (io) sweeps_io<double, double>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, w, r2, z2, done);
-        else sweeps_perm<double, double>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, w, r2, z2, done);
+        sweeps_perm<double, double>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p,
+                                    reinterpret_cast<double2*>(h->work64.p), r2, z2, done);
     } else {
         sweeps_pair<double, double, false>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, z2, r2, z2, done);
     }
@@ -1019,13 +841,9 @@ static cfa_status ilu_pattern(cfa_ctx* ctx, cfa_ilu* h, int n, const int* rp, co
     CFA_CUDA(h->lcp.ensure(std::max(h->nl, 1)));
     CFA_CUDA(h->ucp.ensure(std::max(h->nu, 1)));
     CFA_LAUNCH(ctx, k_ilu_positions, ceil_div(n, kThreads), kThreads, 0, n, (const int*)h->rows.p, h->pos.p);
-    CFA_CUDA(h->lcn.ensure(std::max(h->nl, 1)));
-    if (h->nl > 0) {
+    if (h->nl > 0)
         CFA_LAUNCH(ctx, k_ilu_map_cols, ceil_div(h->nl, kThreads), kThreads, 0, h->nl, (const int*)h->lc.p,
                    (const int*)h->pos.p, h->lcp.p);
-        CFA_LAUNCH(ctx, k_ilu_map_cols_io, ceil_div(h->nl, kThreads), kThreads, 0, h->nl, (const int*)h->lc.p,
-                   (const int*)h->pos.p, h->nc >= 2 ? h->colour_start[1] : 0, h->lcn.p);
-    }
     if (h->nu > 0)
         CFA_LAUNCH(ctx, k_ilu_map_cols, ceil_div(h->nu, kThreads), kThreads, 0, h->nu, (const int*)h->uc.p,
                    (const int*)h->pos.p, h->ucp.p);

@@ -20,7 +20,6 @@ struct cfa_ilu {
     cfa::DevBuf<float> work32;        // FP32 sweep work vector of the interleaved pair (mixed), 2 n
     cfa::DevBuf<double> work64;       // FP64 work vector of the colour-order pair sweeps, 2 n
     cfa::DevBuf<int> pos, lcp, ucp;   // colour position of each row; lc / uc as colour positions
-    cfa::DevBuf<int> lcn;             // lcp with colour-0 columns as ~natural row (sweeps reading r)
     // symbolic factorization (elimination program), rows in colour order:
     // elim[ep[t] .. ep[t+1]) = {local index q of l_ik in row i, CSR position of u_kk, first update},
     // upd[elim.ub .. next.ub) = {local index b in row i, CSR position m in row k}: a_ib -= l_ik lu_m

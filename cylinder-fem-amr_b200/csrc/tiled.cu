@@ -19,7 +19,7 @@ static int l2_hint_env(const char* name, int dflt) {
     return v >= 0 && v <= 2 ? v : dflt;
 }
 
-int l2_hint_operator() { return l2_hint_env("CFA_L2_OP", 0); }
+int l2_hint_operator() { return l2_hint_env("CFA_L2_OP", 1); }
 int l2_hint_vcycle() { return l2_hint_env("CFA_L2_VC", 0); }
 
 bool tile_early_enabled() {

@@ -42,8 +42,12 @@ struct TileView {
     int l2hint = 0;                   // L2 policy of the tile copies: 0 normal, 1 evict first, 2 evict last
 };
 
-// L2 policies of the tile streams: the pressure operator's tiles (CFA_L2_OP) and the V-cycle's
-// level tiles (CFA_L2_VC), each 0 (normal), 1 (evict first) or 2 (evict last).
+// L2 policies of the tile streams: the pressure operator's tiles (CFA_L2_OP, default 1) and the
+// V-cycle's level tiles (CFA_L2_VC, default 0), each 0 (normal), 1 (evict first) or 2 (evict
+// last). The operator's stream is read once per CG iteration and is larger than what the rest of
+// the iteration touches; marked evict-first it no longer pushes the V-cycle's levels and the
+// Krylov vectors out of L2 (c1 step 13.56 -> 13.36 ms). Evict-last on the level tiles changed
+// nothing measurable.
 int l2_hint_operator();
 int l2_hint_vcycle();
 

@@ -218,12 +218,10 @@ def test_ilu_colouring_factor_apply(ctx, precision):
 
 
 @pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
-def test_ilu_sweep_orders_give_the_same_bits(ctx, precision, monkeypatch):
-    """The interleaved-pair ILU apply in its three sweep forms: rows in the reference's natural
-    order (CFA_ILU_PERM=0), the work vector in colour order between a first and a last pass over
-    all rows (1), and the colour kernels reading r and writing z at the rows' natural places
-    themselves (2, the default). The two colour-order forms perform the same operations, so their
-    results are bit for bit the same; the natural-order form agrees to rounding."""
+def test_ilu_sweep_orders_agree(ctx, precision, monkeypatch):
+    """The interleaved-pair ILU apply in its two sweep forms: rows in the reference's natural order
+    (CFA_ILU_PERM=0) and the work vector in colour order between a first and a last pass over all
+    rows (the default): the same terms per row, so the results agree to rounding."""
     from tests.golden.make_golden import momentum_ilu_matrix
     m = mesh("c0")
     rp, ci = O.csr_build(m.n, m.elem_v)
@@ -235,15 +233,14 @@ def test_ilu_sweep_orders_give_the_same_bits(ctx, precision, monkeypatch):
     ilu.factor(dev(a))
     r = dev(np.stack([b[:n], b[n:]], 1).ravel())
     out = {}
-    for order in ("0", "1", "2"):
+    for order in ("0", "1"):
         monkeypatch.setenv("CFA_ILU_PERM", order)
         z = torch.full((2 * n,), np.nan, dtype=torch.float64, device="cuda")
         ilu.apply_interleaved(r, z)
         out[order] = host(z)
-    assert np.isfinite(out["2"]).all()
-    assert np.array_equal(out["1"], out["2"])
+    assert np.isfinite(out["1"]).all()
     tol = 1e-13 if precision == cfa.FP64 else 1e-6
-    assert np.abs(out["0"] - out["2"]).max() <= tol * np.abs(out["0"]).max()
+    assert np.abs(out["0"] - out["1"]).max() <= tol * np.abs(out["0"]).max()
 
 
 @pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
