@@ -2187,12 +2187,26 @@ __global__ void k_sym_check(int n, const int* __restrict__ arp, const int* __res
     }
 }
 
+// Pipeline depth of the level tiles (CFA_VC_STAGES, default 2). Two stages leave room for more
+// CTAs per SM (six instead of four on the finest level's 256-row FP32 tiles) and more rows'
+// gathers in flight, while two waves of tiles in flight still cover the DRAM latency: the c2
+// V-cycle 692 -> 620 us, the c1 one unchanged. The pressure operator keeps three.
+static int level_tile_stages() {
+    static const int s = [] {
+        const char* e = std::getenv("CFA_VC_STAGES");
+        const int v = e ? std::atoi(e) : 2;
+        return v >= 2 && v <= kTileStages ? v : 2;
+    }();
+    return s;
+}
+
 static cfa_status pack_from_device(cfa_ctx* ctx, cfa_amg* amg, const DCsr& M, const double* v0, const double* v1,
                                    int vb, TiledCsr& T) {
     HostBuf<int>& hr = amg->scratch.h_rp;
     CFA_CUDA(hr.ensure(M.rows + 1));
     CFA_CUDA(cudaMemcpyAsync(hr.p, M.rp.p, (M.rows + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+    T.stages = level_tile_stages();
     CFA_PROPAGATE(plan_tiled(ctx, hr.p, M.rows, v1 ? 2 : 1, vb, T));
     return pack_tiled(ctx, M.rp.p, M.ci.p, v0, v1, nullptr, T);
 }
@@ -2301,6 +2315,7 @@ static cfa_status tune_one(cfa_ctx* ctx, cfa_amg* amg, const char* kind, int op,
         CFA_CUDA(hr.ensure(M.rows + 1));
         CFA_CUDA(cudaMemcpyAsync(hr.p, M.rp.p, (M.rows + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+        dst.stages = level_tile_stages();
         const cfa_status st = plan_tiled(ctx, hr.p, M.rows, nvals, vb, dst, shift);
         if (st != CFA_OK) return st;
         return pack_tiled(ctx, M.rp.p, M.ci.p, v0, v1, nullptr, dst);
@@ -2393,6 +2408,7 @@ static cfa_status prepare_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L) {
         CFA_CUDA(hr.ensure(M->rows + 1));
         CFA_CUDA(cudaMemcpyAsync(hr.p, M->rp.p, (M->rows + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+        T.stages = level_tile_stages();
         CFA_PROPAGATE(plan_tiled(ctx, hr.p, M->rows, 1, vb, T));
         CFA_PROPAGATE(pack_tiled(ctx, M->rp.p, M->ci.p, M->v.p, nullptr, nullptr, T));
     }

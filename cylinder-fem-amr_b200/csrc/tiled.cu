@@ -207,7 +207,7 @@ void allow_tile_kernel(const void* kernel) {
 
 TileLaunch tile_launch(const cfa_ctx* ctx, const TiledCsr& T, const void*) {
     TileLaunch L;
-    L.smem = (int)(kTileStages * align16(T.max_chunk) + 16);
+    L.smem = (int)(T.stages * align16(T.max_chunk) + 16);
     const int per_sm = std::max(1, std::min(2048 / kTileThreads, (227 * 1024 - 1024) / std::max(L.smem + 64, 1)));
     L.grid = std::max(1, std::min(T.ntiles, per_sm * ctx->num_sms));
     L.tpr = T.tpr;

@@ -40,6 +40,7 @@ struct TileView {
     int* err = nullptr;               // device error word (timeout)
     int early = 0;                    // signal dependents as soon as the first copies are issued
     int l2hint = 0;                   // L2 policy of the tile copies: 0 normal, 1 evict first, 2 evict last
+    int stages = kTileStages;         // pipeline depth, 2 .. kTileStages (the matrix's own)
 };
 
 // L2 policies of the tile streams: the pressure operator's tiles (CFA_L2_OP, default 1) and the
@@ -60,6 +61,7 @@ bool tile_early_enabled();
 struct TiledCsr {
     int rows = 0, nnz = 0, ntiles = 0, nvals = 0, vbytes = 8, tile_rows = 0, max_chunk = 0;
     int tpr = 1;                      // lanes per row of the kernels (tile_rows = kTileThreads / tpr)
+    int stages = kTileStages;         // pipeline depth of the kernels streaming this matrix (2 .. kTileStages)
     long long bytes = 0;
     DevBuf<unsigned char> data;
     DevBuf<long long> off;
@@ -70,6 +72,7 @@ struct TiledCsr {
         v.data = data.p; v.off = off.p; v.row0 = row0.p; v.ntiles = ntiles; v.rows = rows;
         v.nvals = nvals; v.vbytes = vbytes; v.max_chunk = max_chunk; v.err = err; v.tile_rows = tile_rows;
         v.early = tile_early_enabled() ? 1 : 0;
+        v.stages = stages;
         return v;
     }
 };
@@ -188,8 +191,8 @@ __device__ __forceinline__ void tile_issue(const TileView& tv, int t, unsigned c
 // Dynamic shared memory: kTileStages * align16(max_chunk) bytes. Returns false on a timeout.
 template <class Body>
 __device__ __forceinline__ bool tile_loop(const TileView& tv, unsigned char* smem, Body&& body) {
-    constexpr int S = kTileStages;
-    __shared__ uint64_t bar[S];
+    const int S = tv.stages;   // 2 .. kTileStages
+    __shared__ uint64_t bar[kTileStages];
     __shared__ int abort_flag;
     const long long stride = align16(tv.max_chunk);
     if (threadIdx.x == 0) {
@@ -257,8 +260,8 @@ __device__ __forceinline__ bool tile_loop(const TileView& tv, unsigned char* sme
 // this call.
 template <bool PRE = true, class Gate, class Body>
 __device__ __forceinline__ bool tile_loop_dep(const TileView& tv, unsigned char* smem, Gate&& gate, Body&& body) {
-    constexpr int S = kTileStages;
-    __shared__ uint64_t bar[S];
+    const int S = tv.stages;   // 2 .. kTileStages
+    __shared__ uint64_t bar[kTileStages];
     __shared__ int abort_flag;
     const long long stride = align16(tv.max_chunk);
     const int t0 = blockIdx.x;
