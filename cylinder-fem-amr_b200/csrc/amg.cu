@@ -1041,7 +1041,6 @@ static void vct(cfa_ctx* ctx, bool dry, const TiledCsr& M, int* err, const T* di
     const int tpr = M.tpr;
     TileView tv = M.view(err);
     tv.l2hint = l2_hint_vcycle();
-    const TileLaunch L = tile_launch(ctx, M, nullptr);
     const RzFuse none{};
     const CgFuse nocg{};
     switch (tpr) {
@@ -1052,12 +1051,15 @@ static void vct(cfa_ctx* ctx, bool dry, const TiledCsr& M, int* err, const T* di
             if (kRz) allow_tile_kernel((const void*)k_vct<N, OP, V, T, B, O, kRz>);                     \
             if (kCgu) allow_tile_kernel((const void*)k_vct<N, OP, V, T, B, O, false, kCgu>);            \
         } else if (kRz && rz) {                                                                         \
+            const TileLaunch L = tile_launch(ctx, M, (const void*)k_vct<N, OP, V, T, B, O, kRz>);       \
             CFA_LAUNCH(ctx, (k_vct<N, OP, V, T, B, O, kRz>), L.grid, kTileThreads, L.smem, tv, dinv, omega, b, x, y, \
                        done, *rz, xc, nocg);                                                            \
         } else if (kCgu && cg) {                                                                        \
+            const TileLaunch L = tile_launch(ctx, M, (const void*)k_vct<N, OP, V, T, B, O, false, kCgu>); \
             CFA_LAUNCH(ctx, (k_vct<N, OP, V, T, B, O, false, kCgu>), L.grid, kTileThreads, L.smem, tv, dinv, omega, \
                        b, x, y, done, none, xc, *cg);                                                   \
         } else {                                                                                        \
+            const TileLaunch L = tile_launch(ctx, M, (const void*)k_vct<N, OP, V, T, B, O>);            \
             CFA_LAUNCH(ctx, (k_vct<N, OP, V, T, B, O>), L.grid, kTileThreads, L.smem, tv, dinv, omega, b, x, y, done, \
                        none, xc, nocg);                                                                 \
         }                                                                                               \

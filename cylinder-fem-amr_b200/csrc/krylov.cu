@@ -1777,8 +1777,9 @@ template <int MODE>
 static void launch_b2t(cfa_ctx* ctx, B2Work& W, const B2Args& a, const double* in, const double* aux, double* out,
                        CondArg cond) {
     const TileView tv = W.tA.view(W.err.p);
-    const TileLaunch L = tile_launch(ctx, W.tA, nullptr);
+    TileLaunch L;
     TILE_TPR_SWITCH(W.tA.tpr,
+        L = tile_launch(ctx, W.tA, (const void*)k_b2t<TPR, MODE>);
         CFA_LAUNCH(ctx, (k_b2t<TPR, MODE>), L.grid, kTileThreads, L.smem, tv, a.n, (const double*)a.xu,
                    (const double*)a.xv, a.bu, a.bv, pair(in), pair(aux), pair(out), pair(W.r.p), pair(W.r0.p),
                    pair(W.p.p), W.st.p, W.part.p, W.counter.p, cond));

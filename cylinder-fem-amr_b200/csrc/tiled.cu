@@ -205,10 +205,36 @@ void allow_tile_kernel(const void* kernel) {
     done[kernel] = true;
 }
 
-TileLaunch tile_launch(const cfa_ctx* ctx, const TiledCsr& T, const void*) {
+// Resident blocks per SM of a tile kernel with this much dynamic shared memory, as the runtime
+// computes it from the kernel's registers too (cached; 0 when the query fails).
+static int tile_occupancy(const void* kernel, int smem) {
+    static std::mutex mu;
+    static std::unordered_map<std::string, int> cache;
+    char key[64];
+    std::snprintf(key, sizeof(key), "%p/%d", kernel, smem);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kTileThreads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    cache.emplace(key, n);
+    return n;
+}
+
+TileLaunch tile_launch(const cfa_ctx* ctx, const TiledCsr& T, const void* kernel) {
     TileLaunch L;
     L.smem = (int)(T.stages * align16(T.max_chunk) + 16);
-    const int per_sm = std::max(1, std::min(2048 / kTileThreads, (227 * 1024 - 1024) / std::max(L.smem + 64, 1)));
+    int per_sm = std::max(1, std::min(2048 / kTileThreads, (227 * 1024 - 1024) / std::max(L.smem + 64, 1)));
+    // a grid beyond what is resident would leave its last blocks, each with its share of the
+    // tiles, to run after the first ones finish: the kernel's registers may allow fewer blocks
+    // than the shared memory does
+    if (kernel) {
+        const int occ = tile_occupancy(kernel, L.smem);
+        if (occ > 0) per_sm = std::min(per_sm, occ);
+    }
     L.grid = std::max(1, std::min(T.ntiles, per_sm * ctx->num_sms));
     L.tpr = T.tpr;
     return L;
