@@ -381,27 +381,6 @@ k_ilu_first_perm(int n, const int* __restrict__ pos, const double2* __restrict__
     w[t] = o;
 }
 
-// The same first pass in colour order: position t gathers its row's pair from r and the work
-// vector is written contiguously (the scattering form above writes 8 bytes to each of six
-// colour streams per warp instead).
-template <class T>
-__global__ void __launch_bounds__(kThreads)
-k_ilu_first_gather(int n, const int* __restrict__ rows, const double2* __restrict__ r,
-                   typename Pair<T>::type* __restrict__ w, const int* __restrict__ done, int early) {
-    using T2 = typename Pair<T>::type;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = t < n ? __ldg(rows + t) : 0;
-    if (early) pdl_launch_dependents();
-    CFA_GRID_DEP();
-    if (done && *done) return;
-    if (t >= n) return;
-    const double2 v = r[i];
-    T2 o;
-    o.x = (T)v.x;
-    o.y = (T)v.y;
-    w[t] = o;
-}
-
 // Forward sweep of colour c (positions cs .. cs + m): y_t = y_t - sum_L l_te y_e; the last
 // colour also divides by u_tt.
 template <class V, class T>
@@ -574,56 +553,28 @@ k_ilu_last_perm(int n, int c1, const int* __restrict__ pos, const int* __restric
     z[i] = make_double2((double)o.x, (double)o.y);
 }
 
-// Back to natural order after colour 0's backward step ran as a colour kernel: z[i] = w[pos[i]],
-// the work vector gathered, z written contiguously.
-template <class T>
-__global__ void __launch_bounds__(kThreads)
-k_ilu_unpermute(int n, const int* __restrict__ pos, const typename Pair<T>::type* __restrict__ w,
-                double2* __restrict__ z, const int* __restrict__ done) {
-    using T2 = typename Pair<T>::type;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int t = i < n ? __ldg(pos + i) : 0;
-    CFA_GRID_DEP();
-    if (done && *done) return;
-    if (i >= n) return;
-    const T2 o = w[t];
-    z[i] = make_double2((double)o.x, (double)o.y);
-}
-
 template <class V, class T>
 static void sweeps_perm(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv, const V* dinv,
                         typename Pair<T>::type* w, const double2* r, double2* z, const int* done) {
     static const int early = env_flag("CFA_ILU_EARLY", 1);
     const int n = h->n;
-    if (env_flag("CFA_ILU_FIRST_GATHER", 1))
-        CFA_LAUNCH(ctx, (k_ilu_first_gather<T>), ceil_div(n, kThreads), kThreads, 0, n, (const int*)h->rows.p, r, w,
-                   done, early);
-    else
-        CFA_LAUNCH(ctx, (k_ilu_first_perm<T>), ceil_div(n, kThreads), kThreads, 0, n, (const int*)h->pos.p, r, w,
-                   done, early);
+    CFA_LAUNCH(ctx, (k_ilu_first_perm<T>), ceil_div(n, kThreads), kThreads, 0, n, (const int*)h->pos.p, r, w, done,
+               early);
     for (int c = 1; c < h->nc; ++c) {
         const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
         if (m == 0) continue;
         CFA_LAUNCH(ctx, (k_ilu_lower_perm<V, T>), ceil_div(m, kThreads), kThreads, 0, m, cs, (const int*)h->lp.p,
                    (const int*)h->lcp.p, lv, dinv, c == h->nc - 1 ? 1 : 0, w, done, early);
     }
-    // colour 0's backward step either as one more colour kernel (its rows contiguous in w)
-    // followed by a plain gather back to natural order (default), or inside the last kernel
-    // over all rows in natural order (CFA_ILU_LAST_SPLIT=0)
-    const bool split = env_flag("CFA_ILU_LAST_SPLIT", 1);
-    for (int c = h->nc - 2; c >= (split ? 0 : 1); --c) {
+    for (int c = h->nc - 2; c >= 1; --c) {
         const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
         if (m == 0) continue;
         CFA_LAUNCH(ctx, (k_ilu_upper_perm<V, T>), ceil_div(m, kThreads), kThreads, 0, m, cs, (const int*)h->up.p,
                    (const int*)h->ucp.p, uv, dinv, w, done, early);
     }
-    if (split)
-        CFA_LAUNCH(ctx, (k_ilu_unpermute<T>), ceil_div(n, kThreads), kThreads, 0, n, (const int*)h->pos.p,
-                   (const typename Pair<T>::type*)w, z, done);
-    else
-        CFA_LAUNCH(ctx, (k_ilu_last_perm<V, T>), ceil_div(n, kThreads), kThreads, 0, n, h->colour_start[1],
-                   (const int*)h->pos.p, (const int*)h->up.p, (const int*)h->ucp.p, uv, dinv,
-                   (const typename Pair<T>::type*)w, z, done);
+    CFA_LAUNCH(ctx, (k_ilu_last_perm<V, T>), ceil_div(n, kThreads), kThreads, 0, n, h->colour_start[1],
+               (const int*)h->pos.p, (const int*)h->up.p, (const int*)h->ucp.p, uv, dinv,
+               (const typename Pair<T>::type*)w, z, done);
 }
 
 // pos[rows[t]] = t, and the split pattern's column indices as colour positions

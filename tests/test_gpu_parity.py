@@ -219,12 +219,9 @@ def test_ilu_colouring_factor_apply(ctx, precision):
 
 @pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
 def test_ilu_sweep_orders_agree(ctx, precision, monkeypatch):
-    """The interleaved-pair ILU apply in its sweep forms: rows in the reference's natural order
+    """The interleaved-pair ILU apply in its two sweep forms: rows in the reference's natural order
     (CFA_ILU_PERM=0) and the work vector in colour order between a first and a last pass over all
-    rows (the default), the first pass scattering from natural order or gathering in colour order
-    and colour 0's backward step inside the last pass or as a colour kernel of its own. The
-    colour-order forms perform the same operations, so their results are bit for bit the same;
-    the natural-order form agrees to rounding."""
+    rows (the default): the same terms per row, so the results agree to rounding."""
     from tests.golden.make_golden import momentum_ilu_matrix
     m = mesh("c0")
     rp, ci = O.csr_build(m.n, m.elem_v)
@@ -236,19 +233,14 @@ def test_ilu_sweep_orders_agree(ctx, precision, monkeypatch):
     ilu.factor(dev(a))
     r = dev(np.stack([b[:n], b[n:]], 1).ravel())
     out = {}
-    for order, gather, split in (("0", "1", "1"), ("1", "1", "1"), ("1", "0", "1"), ("1", "1", "0"), ("1", "0", "0")):
+    for order in ("0", "1"):
         monkeypatch.setenv("CFA_ILU_PERM", order)
-        monkeypatch.setenv("CFA_ILU_FIRST_GATHER", gather)
-        monkeypatch.setenv("CFA_ILU_LAST_SPLIT", split)
         z = torch.full((2 * n,), np.nan, dtype=torch.float64, device="cuda")
         ilu.apply_interleaved(r, z)
-        out[order + gather + split] = host(z)
-    ref = out["111"]
-    assert np.isfinite(ref).all()
-    for k in ("101", "110", "100"):
-        assert np.array_equal(out[k], ref), k
+        out[order] = host(z)
+    assert np.isfinite(out["1"]).all()
     tol = 1e-13 if precision == cfa.FP64 else 1e-6
-    assert np.abs(out["011"] - ref).max() <= tol * np.abs(out["011"]).max()
+    assert np.abs(out["0"] - out["1"]).max() <= tol * np.abs(out["0"]).max()
 
 
 @pytest.mark.parametrize("precision", [cfa.FP64, cfa.MIXED])
