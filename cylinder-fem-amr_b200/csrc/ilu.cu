@@ -553,95 +553,6 @@ k_ilu_last_perm(int n, int c1, const int* __restrict__ pos, const int* __restric
     z[i] = make_double2((double)o.x, (double)o.y);
 }
 
-// ---- the colour sweeps over bulk-copied tiles of the split factor ----
-// A colour's rows are contiguous in the split layout, so its L (or U) block is a CSR matrix of
-// its own: packed into tiles (row offsets, column positions, values) and streamed through the
-// shared-memory pipeline of the tile kernels, one thread per row, instead of each thread loading
-// its row's offsets, columns and values from global memory. The arithmetic is that of
-// k_ilu_lower_perm / ilu_upper_row, batch for batch and entry for entry.
-template <class V>
-__global__ void k_ilu_tile_values(int ntiles, const long long* __restrict__ off, const int* __restrict__ row0,
-                                  const int* __restrict__ rp, const V* __restrict__ src,
-                                  unsigned char* __restrict__ data) {
-    CFA_GRID_DEP();
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int r0 = row0[t], nr = row0[t + 1] - r0;
-        const int e0 = rp[r0], ne = rp[r0 + nr] - e0;
-        V* d = reinterpret_cast<V*>(data + off[t] + tile_val_off(nr, ne, (int)sizeof(V), 0));
-        for (int e = threadIdx.x; e < ne; e += blockDim.x) d[e] = src[e0 + e];
-    }
-}
-
-// Row of position t: own -= sum over the tile's entries b .. e of value * w[column], in batches
-// of kIluBatch gathers.
-template <class V, class T>
-__device__ __forceinline__ void ilu_tile_row(int b, int e, const int* __restrict__ cj, const V* __restrict__ vv,
-                                             const typename Pair<T>::type* __restrict__ w, T& a0, T& a1) {
-    using T2 = typename Pair<T>::type;
-    for (int e0 = b; e0 < e; e0 += kIluBatch) {
-        V q[kIluBatch];
-        T2 g[kIluBatch];
-#pragma unroll
-        for (int u = 0; u < kIluBatch; ++u)
-            if (e0 + u < e) {
-                q[u] = vv[e0 + u];
-                g[u] = w[cj[e0 + u]];
-            }
-#pragma unroll
-        for (int u = 0; u < kIluBatch; ++u)
-            if (e0 + u < e) {
-                a0 -= (T)q[u] * g[u].x;
-                a1 -= (T)q[u] * g[u].y;
-            }
-    }
-}
-
-// Forward (UPPER false) or backward (UPPER true) sweep of the colour starting at position cs.
-// Forward: y_t -= sum_L l_te y_e, the last colour also times 1/u_tt; backward:
-// z_t = (y_t - sum_U u_te z_e) / u_tt.
-template <class V, class T, bool UPPER>
-__global__ void __launch_bounds__(kTileThreads)
-k_ilu_sweep_tiles(TileView tv, int cs, const V* __restrict__ dinv, int last, typename Pair<T>::type* __restrict__ w,
-                  const int* __restrict__ done) {
-    using T2 = typename Pair<T>::type;
-    extern __shared__ __align__(128) unsigned char tsmem[];
-    tile_loop_dep(tv, tsmem, [&] { return !(done && *done); },
-                  [&](int, int r0, int nr, const unsigned char* ch) {
-        const int* rr = reinterpret_cast<const int*>(ch);
-        const int ne = rr[nr];
-        const int* cj = reinterpret_cast<const int*>(ch + tile_ci_off(nr));
-        const V* vv = reinterpret_cast<const V*>(ch + tile_val_off(nr, ne, (int)sizeof(V), 0));
-        for (int lr = threadIdx.x; lr < nr; lr += kTileThreads) {
-            const int t = cs + r0 + lr;
-            const V d = (UPPER || last) ? __ldg(dinv + t) : V(0);
-            const T2 own = w[t];
-            T a0 = own.x, a1 = own.y;
-            ilu_tile_row<V, T>(rr[lr], rr[lr + 1], cj, vv, w, a0, a1);
-            if (UPPER || last) {
-                a0 = a0 * (T)d;
-                a1 = a1 * (T)d;
-            }
-            T2 o;
-            o.x = a0;
-            o.y = a1;
-            w[t] = o;
-        }
-    });
-}
-
-// Sweep tiles on (default) unless CFA_ILU_TILES=0.
-static bool ilu_tiles_enabled() { return env_flag("CFA_ILU_TILES", 1); }
-
-template <class V, class T, bool UPPER>
-static void launch_sweep_tiles(cfa_ctx* ctx, const cfa_ilu* h, const TiledCsr& M, int cs, const V* dinv, int last,
-                               typename Pair<T>::type* w, const int* done) {
-    const void* k = (const void*)k_ilu_sweep_tiles<V, T, UPPER>;
-    allow_tile_kernel(k);
-    const TileLaunch L = tile_launch(ctx, M, k);
-    CFA_LAUNCH(ctx, (k_ilu_sweep_tiles<V, T, UPPER>), L.grid, kTileThreads, L.smem, M.view(h->err.p), cs, dinv, last,
-               w, done);
-}
-
 template <class V, class T>
 static void sweeps_perm(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv, const V* dinv,
                         typename Pair<T>::type* w, const double2* r, double2* z, const int* done) {
@@ -649,24 +560,17 @@ static void sweeps_perm(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv
     const int n = h->n;
     CFA_LAUNCH(ctx, (k_ilu_first_perm<T>), ceil_div(n, kThreads), kThreads, 0, n, (const int*)h->pos.p, r, w, done,
                early);
-    const bool tiles = !h->ltiles.empty() && ilu_tiles_enabled();
     for (int c = 1; c < h->nc; ++c) {
         const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
         if (m == 0) continue;
-        if (tiles && h->ltiles[c])
-            launch_sweep_tiles<V, T, false>(ctx, h, *h->ltiles[c], cs, dinv, c == h->nc - 1 ? 1 : 0, w, done);
-        else
-            CFA_LAUNCH(ctx, (k_ilu_lower_perm<V, T>), ceil_div(m, kThreads), kThreads, 0, m, cs, (const int*)h->lp.p,
-                       (const int*)h->lcp.p, lv, dinv, c == h->nc - 1 ? 1 : 0, w, done, early);
+        CFA_LAUNCH(ctx, (k_ilu_lower_perm<V, T>), ceil_div(m, kThreads), kThreads, 0, m, cs, (const int*)h->lp.p,
+                   (const int*)h->lcp.p, lv, dinv, c == h->nc - 1 ? 1 : 0, w, done, early);
     }
     for (int c = h->nc - 2; c >= 1; --c) {
         const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
         if (m == 0) continue;
-        if (tiles && h->utiles[c])
-            launch_sweep_tiles<V, T, true>(ctx, h, *h->utiles[c], cs, dinv, 0, w, done);
-        else
-            CFA_LAUNCH(ctx, (k_ilu_upper_perm<V, T>), ceil_div(m, kThreads), kThreads, 0, m, cs, (const int*)h->up.p,
-                       (const int*)h->ucp.p, uv, dinv, w, done, early);
+        CFA_LAUNCH(ctx, (k_ilu_upper_perm<V, T>), ceil_div(m, kThreads), kThreads, 0, m, cs, (const int*)h->up.p,
+                   (const int*)h->ucp.p, uv, dinv, w, done, early);
     }
     CFA_LAUNCH(ctx, (k_ilu_last_perm<V, T>), ceil_div(n, kThreads), kThreads, 0, n, h->colour_start[1],
                (const int*)h->pos.p, (const int*)h->up.p, (const int*)h->ucp.p, uv, dinv,
@@ -835,62 +739,6 @@ __global__ void k_ilu_program(int n, const int* __restrict__ rows, const int* __
     }
 }
 
-// Tiles of the split factor's colour blocks (pattern only; values by pack_sweep_values). One
-// synchronising copy of the split offsets per pattern.
-static cfa_status plan_sweep_tiles(cfa_ctx* ctx, cfa_ilu* h) {
-    h->ltiles.clear();
-    h->utiles.clear();
-    if (h->nc < 2 || !ilu_tiles_enabled()) return CFA_OK;
-    const int n = h->n;
-    std::vector<int> hl(n + 1), hu(n + 1), loc;
-    CFA_CUDA(cudaMemcpyAsync(hl.data(), h->lp.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CFA_CUDA(cudaMemcpyAsync(hu.data(), h->up.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (!h->err.p) {
-        CFA_CUDA(h->err.ensure(1));
-        CFA_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(int), ctx->stream));
-    }
-    const int vb = h->precision == CFA_MIXED ? 4 : 8;
-    h->ltiles.resize(h->nc);
-    h->utiles.resize(h->nc);
-    auto build = [&](const std::vector<int>& H, const int* d_off, const int* d_col, int c,
-                     std::unique_ptr<TiledCsr>& out) -> cfa_status {
-        const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
-        if (m == 0 || H[cs + m] == H[cs]) return CFA_OK;   // no rows or no entries: the plain kernel
-        loc.resize(m + 1);
-        for (int r = 0; r <= m; ++r) loc[r] = H[cs + r] - H[cs];
-        auto T = std::make_unique<TiledCsr>();
-        CFA_PROPAGATE(plan_tiled(ctx, loc.data(), m, 1, vb, *T));
-        CFA_PROPAGATE(pack_tiled(ctx, d_off + cs, d_col, nullptr, nullptr, nullptr, *T));
-        out = std::move(T);
-        return CFA_OK;
-    };
-    for (int c = 1; c < h->nc; ++c) CFA_PROPAGATE(build(hl, h->lp.p, h->lcp.p, c, h->ltiles[c]));
-    for (int c = 1; c + 1 < h->nc; ++c) CFA_PROPAGATE(build(hu, h->up.p, h->ucp.p, c, h->utiles[c]));
-    return CFA_OK;
-}
-
-// Copies the split factor's values (lv, uv of the handle's precision) into the sweep tiles.
-template <class V>
-static void pack_sweep_values(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv) {
-    if (h->ltiles.empty()) return;
-    auto pack = [&](const TiledCsr& T, const int* d_off, int cs, const V* src) {
-        const int grid = std::min(T.ntiles, 16 * ctx->num_sms);
-        CFA_LAUNCH(ctx, k_ilu_tile_values<V>, grid, kTileThreads, 0, T.ntiles, (const long long*)T.off.p,
-                   (const int*)T.row0.p, d_off + cs, src, T.data.p);
-    };
-    for (int c = 1; c < h->nc; ++c)
-        if (h->ltiles[c]) pack(*h->ltiles[c], h->lp.p, h->colour_start[c], lv);
-    for (int c = 1; c + 1 < h->nc; ++c)
-        if (h->utiles[c]) pack(*h->utiles[c], h->up.p, h->colour_start[c], uv);
-    tile_fence(ctx);
-}
-
-static void pack_sweep_values(cfa_ctx* ctx, const cfa_ilu* h) {
-    if (h->precision == CFA_MIXED) pack_sweep_values<float>(ctx, h, h->lv32.p, h->uv32.p);
-    else pack_sweep_values<double>(ctx, h, h->lv64.p, h->uv64.p);
-}
-
 // set_pattern (src/cfa/linalg.cuh:456-528) into handle h, reusing its device buffers (they grow
 // geometrically, as the reference's cap_n / cap_nnz). The greedy colouring (sequential by
 // definition) runs on the host in node order; the split pattern and the elimination program
@@ -1014,7 +862,7 @@ static cfa_status ilu_pattern(cfa_ctx* ctx, cfa_ilu* h, int n, const int* rp, co
     CFA_CHECK_LAUNCH();
     // the scratch buffers (cnt, uo, tmp) are released on return: wait for the kernels using them
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-    return plan_sweep_tiles(ctx, h);
+    return CFA_OK;
 }
 
 }  // namespace cfa
@@ -1070,7 +918,6 @@ cfa_status cfa_ilu_factor(cfa_ctx* ctx, cfa_ilu* h, const double* val) {
     else
         CFA_LAUNCH(ctx, k_ilu_gather<double>, ceil_div(len, kThreads), kThreads, 0, h->nl, h->nu, h->n, h->l_src.p,
                    h->u_src.p, h->d_src.p, h->lu.p, h->lv64.p, h->uv64.p, h->dinv64.p);
-    pack_sweep_values(ctx, h);
     CFA_CHECK_LAUNCH();
     h->transposed = false;
     return CFA_OK;
@@ -1111,7 +958,6 @@ cfa_status cfa_ilu_factor_transposed(cfa_ctx* ctx, cfa_ilu* h, const double* val
         CFA_LAUNCH(ctx, k_ilu_gather_transposed<double>, ceil_div(h->n, kThreads), kThreads, 0, h->n, h->rows.p,
                    h->lp.p, h->up.p, h->lc.p, h->l_src.p, h->u_src.p, h->d_src.p, h->diag.p, h->tpos.p, h->lu.p,
                    h->lv64.p, h->uv64.p, h->dinv64.p);
-    pack_sweep_values(ctx, h);
     CFA_CHECK_LAUNCH();
     h->transposed = true;
     return CFA_OK;

@@ -1,11 +1,9 @@
 // Multicolour ILU(0) handle (MulticolourIlu0, src/cfa/linalg.cuh:435-568).
 #pragma once
 
-#include <memory>
 #include <vector>
 
 #include "internal.cuh"
-#include "tiled.cuh"
 
 struct cfa_ilu {
     int n = 0, nnz = 0, nc = 0, nl = 0, nu = 0;
@@ -22,11 +20,6 @@ struct cfa_ilu {
     cfa::DevBuf<float> work32;        // FP32 sweep work vector of the interleaved pair (mixed), 2 n
     cfa::DevBuf<double> work64;       // FP64 work vector of the colour-order pair sweeps, 2 n
     cfa::DevBuf<int> pos, lcp, ucp;   // colour position of each row; lc / uc as colour positions
-    // the split factor's rows of each colour as bulk-copied tiles for the colour sweeps: L blocks of
-    // colours 1 .. nc-1, U blocks of colours 1 .. nc-2 (columns as colour positions; values
-    // refreshed after every factorization); empty when the sweeps read the split arrays
-    std::vector<std::unique_ptr<cfa::TiledCsr>> ltiles, utiles;
-    cfa::DevBuf<int> err;             // tile pipeline timeouts of the sweeps
     // symbolic factorization (elimination program), rows in colour order:
     // elim[ep[t] .. ep[t+1]) = {local index q of l_ik in row i, CSR position of u_kk, first update},
     // upd[elim.ub .. next.ub) = {local index b in row i, CSR position m in row k}: a_ib -= l_ik lu_m

@@ -1905,15 +1905,12 @@ static cfa_status b2_solve(cfa_ctx* ctx, const B2Args& a, cfa_solve_report* rep)
     }
     CFA_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     B2State h;
-    int h_err = 0, h_ilu_err = 0;
+    int h_err = 0;
     CFA_CUDA(cudaMemcpyAsync(&h, W.st.p, sizeof(B2State), cudaMemcpyDeviceToHost, ctx->stream));
     if (W.err.p) CFA_CUDA(cudaMemcpyAsync(&h_err, W.err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    if (a.ilu && a.ilu->err.p)   // the ILU's tile sweeps
-        CFA_CUDA(cudaMemcpyAsync(&h_ilu_err, a.ilu->err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (h_err || h_ilu_err) {
-        if (h_err) cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream);
-        if (h_ilu_err) cudaMemsetAsync(a.ilu->err.p, 0, sizeof(int), ctx->stream);
+    if (h_err) {
+        cudaMemsetAsync(W.err.p, 0, sizeof(int), ctx->stream);
         return set_error(ctx, CFA_TIMEOUT, "a bounded wait of a tile pipeline timed out", __FILE__, __LINE__);
     }
     float ms = 0.f;
