@@ -592,6 +592,14 @@ class AmgPreconditioner:
         if s != CFA_OK:
             raise CfaError(s, "cfa_amg_set_vcycle")
 
+    def set_fp64_phase(self, switch_rel: float = -1.0):
+        """Mixed precision: the solves' V-cycles in FP64 until the relative residual falls below
+        switch_rel, FP32 after (0: FP32 throughout; negative: the default), for the setups that
+        follow."""
+        s = lib().cfa_amg_set_fp64_phase(self._handle(), C.c_double(switch_rel))
+        if s != CFA_OK:
+            raise CfaError(s, "cfa_amg_set_fp64_phase")
+
     def composite(self):
         """(level, rows) of the composite coarse operator, level -1 when there is none."""
         lv, rows = C.c_int(), C.c_int()

@@ -1424,15 +1424,22 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     AmgLevel& L = amg->levels[l];
     const int s = amg->opts.smooth_steps;
     int* err = amg->err.p;
+    // FP64 values on a mixed hierarchy: its FP64 tile copies
+    const bool t64 = std::is_same<V, double>::value && amg->opts.precision == CFA_MIXED;
+    const TiledCsr& tA = t64 ? L.tA64 : L.tA;
+    const TiledCsr& tP = t64 ? L.tP64 : L.tP;
+    const TiledCsr& tR = t64 ? L.tR64 : L.tR;
+    const TiledCsr& tQ = t64 ? L.tQ64 : L.tQ;
+    const TiledCsr& tW = t64 ? L.tW64 : L.tW;
     const T omega = (T)L.omega;
     const T* dinv = TVec<T>::dinv(L);
     T* x = TVec<T>::x(L);
     T* t = TVec<T>::t(L);
     if (s >= 2 && c0 && !cg) {   // the first iterate formed by the caller
-        vct<VC_PREC, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, c0, x, done);
+        vct<VC_PREC, V, T, B, T>(ctx, dry, tA, err, dinv, omega, b, c0, x, done);
     } else if (s >= 2) {
-        if (dry) vct<VC_PREC, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)nullptr, x, done);
-        vct<VC_PRE, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)nullptr, x, done, nullptr, nullptr, cg);
+        if (dry) vct<VC_PREC, V, T, B, T>(ctx, dry, tA, err, dinv, omega, b, (const T*)nullptr, x, done);
+        vct<VC_PRE, V, T, B, T>(ctx, dry, tA, err, dinv, omega, b, (const T*)nullptr, x, done, nullptr, nullptr, cg);
     } else if (!dry) {
         CFA_TPR_SWITCH(L.A.tpr, CFA_LAUNCH(ctx, (k_vc_pre<TPR, T, B>), row_grid(ctx, L.A.rows, L.A.tpr), kThreads, 0,
                                            L.A.rows, L.A.rp.p, L.A.ci.p,
@@ -1441,17 +1448,17 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
                                            dinv, omega, b, 0, x, done));
     }
     for (int k = 2; k < s; ++k) {
-        vct<VC_JAC, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, t, done);
+        vct<VC_JAC, V, T, B, T>(ctx, dry, tA, err, dinv, omega, b, (const T*)x, t, done);
         std::swap(x, t);
     }
     const bool last = l + 1 == (int)amg->levels.size();
     T* cb = last ? TVec<T>::cb(amg) : TVec<T>::b(amg->levels[l + 1]);
     if (L.fusedQ) {   // cb = R b - (R A) x in one pass
-        vct<VC_RESTRICT, V, T, B, T>(ctx, dry, L.tQ, err, dinv, omega, b, (const T*)x, cb, done);
+        vct<VC_RESTRICT, V, T, B, T>(ctx, dry, tQ, err, dinv, omega, b, (const T*)x, cb, done);
     } else {
-        vct<VC_RES, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, TVec<T>::r(L), done, nullptr,
+        vct<VC_RES, V, T, B, T>(ctx, dry, tA, err, dinv, omega, b, (const T*)x, TVec<T>::r(L), done, nullptr,
                                 nullptr, cg);
-        vct<VC_SPMV, V, T, T, T>(ctx, dry, L.tR, err, dinv, omega, (const T*)nullptr, (const T*)TVec<T>::r(L), cb,
+        vct<VC_SPMV, V, T, T, T>(ctx, dry, tR, err, dinv, omega, (const T*)nullptr, (const T*)TVec<T>::r(L), cb,
                                  done);
     }
     const T* cx;
@@ -1474,17 +1481,17 @@ static void vcycle_tiled(cfa_ctx* ctx, cfa_amg* amg, int l, const B* b, double* 
     }
     int k0 = 0;
     if (L.fusedW) {   // the first post-smoothing sweep from x + P cx
-        vct<VC_ADDJAC, V, T, B, T>(ctx, dry, L.tW, err, dinv, omega, b, (const T*)x, t, done, nullptr, cx);
+        vct<VC_ADDJAC, V, T, B, T>(ctx, dry, tW, err, dinv, omega, b, (const T*)x, t, done, nullptr, cx);
         std::swap(x, t);
         k0 = 1;
     } else {
-        vct<VC_ADD, V, T, T, T>(ctx, dry, L.tP, err, dinv, omega, (const T*)nullptr, cx, x, done);
+        vct<VC_ADD, V, T, T, T>(ctx, dry, tP, err, dinv, omega, (const T*)nullptr, cx, x, done);
     }
     for (int k = k0; k < s; ++k) {
         if (l == 0 && k == s - 1) {
-            vct<VC_JAC, V, T, B, double>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, z, done, rz);
+            vct<VC_JAC, V, T, B, double>(ctx, dry, tA, err, dinv, omega, b, (const T*)x, z, done, rz);
         } else {
-            vct<VC_JAC, V, T, B, T>(ctx, dry, L.tA, err, dinv, omega, b, (const T*)x, t, done);
+            vct<VC_JAC, V, T, B, T>(ctx, dry, tA, err, dinv, omega, b, (const T*)x, t, done);
             std::swap(x, t);
         }
     }
@@ -1500,8 +1507,9 @@ static bool vcycle_fp32(const cfa_amg* amg) {
 }
 
 static void vcycle_tiled_top(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, bool dry,
-                             const RzFuse* rz = nullptr, const CgFuse* cg = nullptr, const void* c0 = nullptr) {
-    if (amg->opts.precision != CFA_MIXED)
+                             const RzFuse* rz = nullptr, const CgFuse* cg = nullptr, const void* c0 = nullptr,
+                             bool fp64 = false) {
+    if (amg->opts.precision != CFA_MIXED || (fp64 && amg->phase_switch > 0.0))
         vcycle_tiled<double, double, double>(ctx, amg, 0, r, z, done, dry, rz, cg, (const double*)c0);
     else if (vcycle_fp32(amg))
         vcycle_tiled<float, float, double>(ctx, amg, 0, r, z, done, dry, rz, cg, (const float*)c0);
@@ -1509,11 +1517,15 @@ static void vcycle_tiled_top(cfa_ctx* ctx, cfa_amg* amg, const double* r, double
         vcycle_tiled<float, double, double>(ctx, amg, 0, r, z, done, dry, rz, cg, (const double*)c0);
 }
 
-bool amg_prescale(const cfa_amg* amg, PreScale* out) {
+double amg_fp64_phase(const cfa_amg* amg) {
+    return amg && amg->tiled && !amg->levels.empty() ? amg->phase_switch : 0.0;
+}
+
+bool amg_prescale(const cfa_amg* amg, PreScale* out, bool fp64) {
     const char* e = std::getenv("CFA_PRESCALE");
     if ((e && e[0] == '0') || !amg || amg->levels.empty() || !amg->tiled || amg->opts.smooth_steps < 2) return false;
     const AmgLevel& L = amg->levels[0];
-    const bool f32 = vcycle_fp32(amg);
+    const bool f32 = vcycle_fp32(amg) && !(fp64 && amg->phase_switch > 0.0);
     out->dinv = f32 ? (const void*)L.dinv32.p : (const void*)L.dinv.p;
     out->omega = L.omega;
     out->fp32 = f32 ? 1 : 0;
@@ -1530,12 +1542,12 @@ bool amg_can_fuse_update(const cfa_amg* amg) {
            !amg->levels[0].fusedQ;
 }
 
-cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done) {
+cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, bool fp64) {
     if (amg->levels.empty()) {
         CFA_LAUNCH(ctx, (k_vc_dense<double, double>), amg->coarse_n, 32 * kDenseWarps, 0,
                    amg->coarse_n, amg->coarse_inv.p, r, z, done);
     } else if (amg->tiled) {
-        vcycle_tiled_top(ctx, amg, r, z, done, false);
+        vcycle_tiled_top(ctx, amg, r, z, done, false, nullptr, nullptr, nullptr, fp64);
     } else if (amg->opts.precision == CFA_MIXED) {
         vcycle_level<float, double>(ctx, amg, 0, r, z, done);
     } else {
@@ -1546,13 +1558,13 @@ cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, co
 }
 
 cfa_status amg_vcycle_rz(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, const RzFuse& f,
-                         bool* fused, const CgFuse* cg, const void* c) {
+                         bool* fused, const CgFuse* cg, const void* c, bool fp64) {
     *fused = false;
     if (cg && !amg_can_fuse_update(amg))
         return set_error(ctx, CFA_BAD_ARG, "the CG update cannot be folded into this hierarchy", __FILE__, __LINE__);
-    if (amg->levels.empty() || !amg->tiled || amg->opts.smooth_steps < 1) return amg_vcycle(ctx, amg, r, z, done);
+    if (amg->levels.empty() || !amg->tiled || amg->opts.smooth_steps < 1) return amg_vcycle(ctx, amg, r, z, done, fp64);
     if (c && cg) return set_error(ctx, CFA_BAD_ARG, "prescaled residual with the folded update", __FILE__, __LINE__);
-    vcycle_tiled_top(ctx, amg, r, z, done, false, &f, cg, c);
+    vcycle_tiled_top(ctx, amg, r, z, done, false, &f, cg, c, fp64);
     CFA_CHECK_LAUNCH();
     *fused = true;
     return CFA_OK;
@@ -2250,6 +2262,7 @@ static cfa_status build_fused(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb, b
                (const int*)L.R.ci.p, (const double*)L.R.v.p, (const int*)S.fRA.rp.p, (const int*)S.fRA.ci.p,
                (const double*)S.fRA.v.p, (const int*)Q.rp.p, Q.ci.p, Q.v.p);
     CFA_PROPAGATE(pack_from_device(ctx, amg, Q, Q.v.p, nullptr, vb, L.tQ));
+    if (amg->phase_switch > 0.0 && vb != 8) CFA_PROPAGATE(pack_from_device(ctx, amg, Q, Q.v.p, nullptr, 8, L.tQ64));
     L.fusedQ = true;
     if (!with_w) {
         CFA_CHECK_LAUNCH();
@@ -2279,6 +2292,7 @@ static cfa_status build_fused(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb, b
                (const int*)L.P.rp.p, (const int*)L.P.ci.p, (const double*)L.P.v.p, (int*)nullptr,
                (const int*)W.rp.p, W.ci.p, W.v.p, S.fW1.p);
     CFA_PROPAGATE(pack_from_device(ctx, amg, W, W.v.p, S.fW1.p, vb, L.tW));
+    if (amg->phase_switch > 0.0 && vb != 8) CFA_PROPAGATE(pack_from_device(ctx, amg, W, W.v.p, S.fW1.p, 8, L.tW64));
     CFA_CHECK_LAUNCH();
     L.fusedW = true;
     return CFA_OK;
@@ -2380,6 +2394,15 @@ static cfa_status tune_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb) {
 
 // Kernel shapes of one level, its FP32 copies (mixed precision) and its tile-streamed A, P, R in
 // the hierarchy precision.
+// Relative residual at which a mixed-precision solve's V-cycles switch from FP64 to FP32
+// (CFA_FP64_PHASE; 0 keeps them FP32 throughout).
+static double fp64_phase_env() {
+    const char* e = std::getenv("CFA_FP64_PHASE");
+    if (!e || !*e) return 1e-2;
+    const double v = std::atof(e);
+    return v > 0.0 && v < 1.0 ? v : 0.0;
+}
+
 static cfa_status prepare_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L) {
     const cfa_amg_opts& o = amg->opts;
     L.A.tpr = threads_per_row(L.A.rows, L.A.nnz);
@@ -2413,6 +2436,12 @@ static cfa_status prepare_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L) {
         T.stages = level_tile_stages();
         CFA_PROPAGATE(plan_tiled(ctx, hr.p, M->rows, 1, vb, T));
         CFA_PROPAGATE(pack_tiled(ctx, M->rp.p, M->ci.p, M->v.p, nullptr, nullptr, T));
+        if (amg->phase_switch > 0.0) {   // the FP64 copy for the solves' FP64 phase
+            TiledCsr& T64 = M == &L.A ? L.tA64 : M == &L.P ? L.tP64 : L.tR64;
+            T64.stages = level_tile_stages();
+            CFA_PROPAGATE(plan_tiled(ctx, hr.p, M->rows, 1, 8, T64));
+            CFA_PROPAGATE(pack_tiled(ctx, M->rp.p, M->ci.p, M->v.p, nullptr, nullptr, T64));
+        }
     }
     if (o.precision == CFA_MIXED) CFA_PROPAGATE(level_vectors(ctx, amg, L, L.A.rows));   // FP32 V-cycle vectors
     CFA_PROPAGATE(level_vectors64(ctx, L, L.A.rows));
@@ -2430,6 +2459,7 @@ static cfa_status prepare_vcycle(cfa_ctx* ctx, cfa_amg* amg) {
     if (!amg->tiled) return CFA_OK;
     CFA_PROPAGATE(plan_tail(ctx, amg));
     vcycle_tiled_top(ctx, amg, nullptr, nullptr, nullptr, true);
+    if (amg->phase_switch > 0.0) vcycle_tiled_top(ctx, amg, nullptr, nullptr, nullptr, true, nullptr, nullptr, nullptr, true);
     CFA_CHECK_LAUNCH();
     return CFA_OK;
 }
@@ -2670,6 +2700,9 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
     // precision, kernel shapes and tile-streamed copies of the V-cycle
     const char* te = std::getenv("CFA_TILES");
     amg->tiled = !(te && te[0] == '0') && !amg->levels.empty();
+    amg->phase_switch = !(amg->tiled && o.precision == CFA_MIXED) ? 0.0
+                        : amg->vc_fp64_phase >= 0.0                  ? amg->vc_fp64_phase
+                                                                     : fp64_phase_env();
     if (amg->tiled) {
         CFA_CUDA(amg->err.ensure(1));
         CFA_CUDA(cudaMemsetAsync(amg->err.p, 0, sizeof(int), ctx->stream));
@@ -2913,6 +2946,12 @@ cfa_status cfa_amg_set_vcycle(cfa_amg* amg, int composite_rows, int fuse_levels,
     amg->vc_composite_rows = composite_rows < 0 ? -1 : composite_rows;
     amg->vc_fuse = fuse_levels < 0 ? -1 : fuse_levels;
     amg->vc_fold_rows = fold_rows < 0 ? -1 : fold_rows;
+    return CFA_OK;
+}
+
+cfa_status cfa_amg_set_fp64_phase(cfa_amg* amg, double switch_rel) {
+    if (!amg || !(switch_rel < 1.0)) return CFA_BAD_ARG;
+    amg->vc_fp64_phase = switch_rel < 0.0 ? -1.0 : switch_rel;
     return CFA_OK;
 }
 

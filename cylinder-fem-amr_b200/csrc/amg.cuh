@@ -24,6 +24,9 @@ struct AmgLevel {
     // sweep (values [A | A P] and [I | P] on one pattern); columns with the top bit set read the
     // second vector (x, resp. the coarse correction)
     TiledCsr tQ, tW;
+    // FP64 copies of tA, tP, tR, tQ, tW in a mixed-precision hierarchy, for the FP64 V-cycles that
+    // a solve runs first (amg_fp64_phase); empty otherwise
+    TiledCsr tA64, tP64, tR64, tQ64, tW64;
     bool fusedQ = false, fusedW = false;
     bool ra_spgemm = false;        // R A formed by SpGEMM (A not symmetric) rather than as (A P)^T
     DCsr AP;                       // A P of the Galerkin product (rows 0 after a remap changed P)
@@ -117,6 +120,11 @@ struct cfa_amg {
     cfa::DevBuf<double> comp;
     // V-cycle forms chosen for this handle (cfa_amg_set_vcycle); -1: the default / environment
     int vc_composite_rows = -1, vc_fuse = -1, vc_fold_rows = -1;
+    // mixed precision: relative residual below which a solve's V-cycles switch from FP64 to FP32
+    // (0: FP32 throughout); the FP64 level tiles exist when it is positive. vc_fp64_phase is the
+    // value asked for by cfa_amg_set_fp64_phase (-1: CFA_FP64_PHASE or the default)
+    double phase_switch = 0.0;
+    double vc_fp64_phase = -1.0;
 };
 
 namespace cfa {
@@ -138,7 +146,15 @@ struct CgState {
 
 // One symmetric V-cycle z = M^-1 r (FP64 in/out). Kernels return at once while *done != 0
 // (done nullable).
-cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done);
+cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, bool fp64 = false);
+
+// Mixed precision by phases: a Krylov solve runs its first V-cycles in FP64 on the hierarchy's
+// FP64 tiles and switches to the FP32 V-cycle once its relative residual falls below the
+// returned threshold (0: no FP64 phase). The FP32 V-cycle's rounding, about 1e-7 of the
+// residual it is applied to, enters the CG's search directions; while the residual is large
+// those errors are large against the final 1e-10 and cost iterations at the end (59 -> 67 on
+// the c1 pressure system), but below about 1e-2 of the initial residual they stay below it.
+double amg_fp64_phase(const cfa_amg* amg);
 
 // The CG's dots after the preconditioner (r.z, and z.q for the flexible beta) folded into the
 // V-cycle's last sweep, which already reads r and writes z; its last block finishes them as the
@@ -179,11 +195,11 @@ struct PreScale {
     double omega;
     int fp32;
 };
-bool amg_prescale(const cfa_amg* amg, PreScale* out);
+bool amg_prescale(const cfa_amg* amg, PreScale* out, bool fp64 = false);
 // amg_vcycle with the dots fused when the hierarchy runs tile-streamed (*fused = true); otherwise
 // the plain V-cycle (*fused = false) and the caller computes the dots. cg (nullable; only where
 // amg_can_fuse_update) folds the CG's update into level 0; c (nullable; only where amg_prescale)
 // is omega0 D0^-1 r, formed by the caller.
 cfa_status amg_vcycle_rz(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, const int* done, const RzFuse& f,
-                         bool* fused, const CgFuse* cg = nullptr, const void* c = nullptr);
+                         bool* fused, const CgFuse* cg = nullptr, const void* c = nullptr, bool fp64 = false);
 }  // namespace cfa

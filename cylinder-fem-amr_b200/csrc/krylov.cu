@@ -1134,6 +1134,7 @@ struct PcgWork {
     DevBuf<double> part;
     DevBuf<unsigned int> counter;
     GraphCache graph;
+    GraphCache graph2;   // the second phase of a mixed-precision solve (FP32 V-cycles)
     SegGraph seg[3];   // the pieces of one iteration between host hooks (cfa_pcg_solve_host_ops)
     DevBuf<unsigned long long> fp;
 };
@@ -1267,6 +1268,7 @@ struct PcgArgs {
     cfa_host_op prec = nullptr;
     void* prec_user = nullptr;
     unsigned long long fp = 0;   // fingerprint of the pattern (rp, ci): plans follow its content
+    int vc64 = 0;                // the V-cycle in FP64 on a mixed hierarchy (the solve's first phase)
     bool host_ops() const { return extra || prec; }
 };
 
@@ -1389,7 +1391,7 @@ static cfa_status pcg_init(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, CondArg c
         CFA_CHECK_LAUNCH();
         a.prec(W.r.p, W.z.p, a.prec_user);
     } else if (a.amg) {
-        CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done));
+        CFA_PROPAGATE(amg_vcycle(ctx, a.amg, W.r.p, W.z.p, done, a.vc64 != 0));
     } else {
         CFA_LAUNCH(ctx, k_vmul, gv, kThreads, 0, n, W.dinv.p, W.r.p, W.z.p);
     }
@@ -1431,7 +1433,7 @@ static cfa_status pcg_piece(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, int piec
             // pre-smoothing's scaled residual where the V-cycle takes it
             const bool fuse_update = !a.prec && amg_can_fuse_update(a.amg);
             PreScale ps{};
-            const bool prescale = !a.prec && !fuse_update && amg_prescale(a.amg, &ps);
+            const bool prescale = !a.prec && !fuse_update && amg_prescale(a.amg, &ps, a.vc64 != 0);
             if (!fuse_update) {
                 if (prescale && ps.fp32)
                     CFA_LAUNCH(ctx, (k_cg_update<false, float>), gv, kThreads, 0, n, a.x, W.r.p, W.pn.p, W.p.p, W.q.p,
@@ -1453,7 +1455,7 @@ static cfa_status pcg_piece(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, int piec
                 const CgFuse g{W.r.p, W.q.p, W.pn.p, a.x, W.p.p, st, W.part.p, W.counter.p, cond};
                 bool fused = false;
                 CFA_PROPAGATE(amg_vcycle_rz(ctx, a.amg, W.r.p, W.z.p, done, f, &fused, fuse_update ? &g : nullptr,
-                                            prescale ? (const void*)W.c0.p : nullptr));
+                                            prescale ? (const void*)W.c0.p : nullptr, a.vc64 != 0));
                 if (!fused)
                     CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, flexible, st,
                                W.part.p, W.counter.p, cond);
@@ -1466,6 +1468,41 @@ static cfa_status pcg_piece(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, int piec
         CFA_LAUNCH(ctx, k_cg_rz, gv, kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, 0, st, W.part.p,
                    W.counter.p, cond);
     }
+    CFA_CHECK_LAUNCH();
+    return CFA_OK;
+}
+
+// Between the two phases of a mixed-precision solve: where the FP64 phase stopped at its switch
+// threshold (converged there, iterations left), the solve continues to the final tolerance: the
+// stop is undone and the WHILE condition of the second phase set. Otherwise (the final
+// tolerance already met, a breakdown, the iteration limit) the second phase does nothing.
+__global__ void k_cg_phase(CgState* st, double tol, CondArg cond) {
+    CFA_GRID_DEP();
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (st->converged && st->status == CFA_OK && st->iter < st->max_iter && !(st->rel < tol)) {
+        st->tol = tol;
+        st->done = 0;
+        st->converged = 0;
+        set_cond(cond, 1);
+    } else if (st->converged) {
+        st->tol = tol;
+    }
+}
+
+// The second phase's start: z = M^-1 r for the residual the first phase stopped at (its V-cycle
+// was skipped there), with the dots and the flexible beta as the iteration's own V-cycle forms them.
+static cfa_status pcg_resume(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, double tol, CondArg cond) {
+    const int n = a.n;
+    CgState* st = W.st.p;
+    const int* done = &st->done;
+    CFA_LAUNCH(ctx, k_cg_phase, 1, 32, 0, st, tol, cond);
+    const int flexible = pcg_flexible(a.amg);
+    const RzFuse f{W.q.p, flexible, &st->rz, &st->beta, &st->alpha, W.part.p, W.counter.p};
+    bool fused = false;
+    CFA_PROPAGATE(amg_vcycle_rz(ctx, a.amg, W.r.p, W.z.p, done, f, &fused, nullptr, nullptr, a.vc64 != 0));
+    if (!fused)
+        CFA_LAUNCH(ctx, k_cg_rz, row_grid(ctx, n, 1), kThreads, 0, n, W.r.p, W.z.p, (const double*)W.q.p, 0, flexible,
+                   st, W.part.p, W.counter.p, cond);
     CFA_CHECK_LAUNCH();
     return CFA_OK;
 }
@@ -1531,6 +1568,7 @@ static std::vector<const void*> operator_key(int n, int nnz, const int* rp, cons
 static cfa_status ensure_pcg_vectors(cfa_ctx* ctx, PcgWork& W, int n) {
     if (n > W.cap) {
         W.graph.reset();
+        W.graph2.reset();
         for (SegGraph& g : W.seg) g.reset();
         for (DevBuf<double>* b : {&W.r, &W.z, &W.p, &W.pn, &W.q, &W.gx, &W.gy, &W.dinv, &W.c0}) CFA_CUDA(b->ensure(n));
         CFA_CUDA(W.st.ensure(1));
@@ -1655,6 +1693,7 @@ static cfa_status plan_operator_tiles(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a
     }
     W.tile_key = key;
     W.graph.reset();
+    W.graph2.reset();
     for (SegGraph& g : W.seg) g.reset();
     return CFA_OK;
 }
@@ -1681,9 +1720,14 @@ static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* re
     CFA_PROPAGATE(ensure_pcg_vectors(ctx, W, n));
     CFA_PROPAGATE(plan_operator_tiles(ctx, W, a));
     W.prepared.clear();
+    // a mixed hierarchy's FP64 first phase, down to the switch threshold, then the FP32 V-cycles
+    const double sw = (a.amg && !a.host_ops()) ? amg_fp64_phase(a.amg) : 0.0;
+    const bool two = sw > a.tol;
+    PcgArgs a1 = a;
+    a1.vc64 = two ? 1 : 0;
     // parameters
     CgState init{};
-    init.tol = a.tol;
+    init.tol = two ? sw : a.tol;
     init.max_iter = a.max_iter;
     CFA_CUDA(cudaMemcpyAsync(W.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
     CFA_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -1698,30 +1742,43 @@ static cfa_status pcg_solve(cfa_ctx* ctx, const PcgArgs& a, cfa_solve_report* re
                                           (const void*)(intptr_t)((a.extra ? 1 : 0) | (a.prec ? 2 : 0)),
                                           (const void*)(uintptr_t)a.fp};
     if (graphs_enabled() && !a.host_ops()) {
-        if (!W.graph.exec || W.graph.key != key) {
-            CFA_PROPAGATE(build_graph(ctx, W.graph, [&](CondArg c) { return pcg_init(ctx, W, a, c); },
-                                      [&](CondArg c) { return pcg_body(ctx, W, a, c); }));
-            W.graph.key = key;
+        std::vector<const void*> key1 = key;
+        key1.push_back((const void*)(intptr_t)(two ? 1 : 0));
+        if (!W.graph.exec || W.graph.key != key1) {
+            CFA_PROPAGATE(build_graph(ctx, W.graph, [&](CondArg c) { return pcg_init(ctx, W, a1, c); },
+                                      [&](CondArg c) { return pcg_body(ctx, W, a1, c); }));
+            W.graph.key = key1;
         }
         CFA_CUDA(cudaGraphLaunch(W.graph.exec, ctx->stream));
         extra_body = W.graph.body_kernels;
         ctx->launches += W.graph.init_kernels;
+        if (two) {
+            if (!W.graph2.exec || W.graph2.key != key) {
+                CFA_PROPAGATE(build_graph(ctx, W.graph2, [&](CondArg c) { return pcg_resume(ctx, W, a, a.tol, c); },
+                                          [&](CondArg c) { return pcg_body(ctx, W, a, c); }));
+                W.graph2.key = key;
+            }
+            CFA_CUDA(cudaGraphLaunch(W.graph2.exec, ctx->stream));
+            ctx->launches += W.graph2.init_kernels;
+        }
     } else {
         CondArg none{0, 0};
-        const long long l0 = ctx->launches;
-        CFA_PROPAGATE(pcg_init(ctx, W, a, none));
-        (void)l0;
-        int polled = 0;
+        CFA_PROPAGATE(pcg_init(ctx, W, a1, none));
         const bool segments = graphs_enabled();   // host hooks: one graph per piece of the iteration
-        for (int it = 0; it < a.max_iter; ++it) {
-            if (segments) CFA_PROPAGATE(pcg_body_segments(ctx, W, a, key));
-            else CFA_PROPAGATE(pcg_body(ctx, W, a, none));
-            if (++polled == 8 || it + 1 == a.max_iter) {
-                polled = 0;
-                int d = 0;
-                CFA_CUDA(cudaMemcpyAsync(&d, &W.st.p->done, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-                CFA_CUDA(cudaStreamSynchronize(ctx->stream));
-                if (d) break;
+        for (int phase = 0; phase < (two ? 2 : 1); ++phase) {
+            const PcgArgs& ap = phase == 0 ? a1 : a;
+            if (phase == 1) CFA_PROPAGATE(pcg_resume(ctx, W, a, a.tol, none));
+            int polled = 0;
+            for (int it = 0; it < a.max_iter; ++it) {
+                if (segments) CFA_PROPAGATE(pcg_body_segments(ctx, W, ap, key));
+                else CFA_PROPAGATE(pcg_body(ctx, W, ap, none));
+                if (++polled == 8 || it + 1 == a.max_iter) {
+                    polled = 0;
+                    int d = 0;
+                    CFA_CUDA(cudaMemcpyAsync(&d, &W.st.p->done, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+                    CFA_CUDA(cudaStreamSynchronize(ctx->stream));
+                    if (d) break;
+                }
             }
         }
     }

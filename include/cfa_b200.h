@@ -443,6 +443,14 @@ cfa_status cfa_amg_composite(const cfa_amg* amg, int* level, int* rows, const do
  * up to rounding; each costs setup time that only repeated solves with one hierarchy (a time loop
  * between rebuilds) earn back, so a caller that solves once per setup turns them off (0, 0, 0). */
 cfa_status cfa_amg_set_vcycle(cfa_amg* amg, int composite_rows, int fuse_levels, int fold_rows);
+/* Mixed-precision handles (no counterpart in the reference): the Krylov solves preconditioned by
+ * this handle run their V-cycles in FP64 until the relative residual falls below switch_rel and
+ * in FP32 after that, for the setups that follow (0: FP32 throughout; negative: the default 1e-2
+ * or CFA_FP64_PHASE). The FP32 V-cycle's rounding, about 1e-7 of the residual it is applied to,
+ * enters the CG's search directions and costs iterations near a tight tolerance only when it is
+ * made while the residual is still large; the FP64 copy of the level tiles costs setup time and
+ * memory. CFA_BAD_ARG for switch_rel >= 1. */
+cfa_status cfa_amg_set_fp64_phase(cfa_amg* amg, double switch_rel);
 
 /* The assembled OSS term of the pressure operator (apply_oss_projection,
  * src/cfa/device.cuh:316-323): A x = K x - B^T M^-1 B x on non-Dirichlet rows. */

@@ -711,6 +711,37 @@ def test_pcg_prescaled_residual_gives_the_same_bits(ctx, prec, monkeypatch):
     assert np.array_equal(out["1"][1], out["0"][1])
 
 
+@pytest.mark.parametrize("graphs", ["1", "0"])
+def test_pcg_fp64_phase_of_a_mixed_hierarchy(ctx, graphs, monkeypatch):
+    """A mixed-precision hierarchy whose solves run their V-cycles in FP64 down to a relative
+    residual of 1e-2 and in FP32 after: the switch keeps the flexible CG's state, so the solve
+    reaches the FP64 hierarchy's iteration count (within 1) where FP32 throughout needs more, and
+    its true residual meets the tolerance; with and without the solve graphs."""
+    monkeypatch.setenv("CFA_GRAPHS", graphs)
+    m = mesh("c0")
+    dm = cfa.DeviceMesh(ctx, m)
+    rp, ci = dm.host_pattern()
+    Kp, rhs, oss, inv_m = pressure_system(m, rp, ci)
+    dK, db, doss, dinv = dev(Kp), dev(rhs), dev(oss), dev(inv_m)
+    its = {}
+    for label, prec, phase in (("fp64", cfa.FP64, -1.0), ("fp32", cfa.MIXED, 0.0), ("phase", cfa.MIXED, 1e-2)):
+        amg = cfa.AmgPreconditioner(ctx, prec)
+        amg.set_fp64_phase(phase)
+        amg.setup(m.n, ci.size, dm.rp, dm.ci, dK)
+        s = cfa.GpuLinearSolver(ctx)
+        x = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+        its[label] = s.solve_pcg(m.n, dm.rp, dm.ci, dK, db, x, 4000, 1e-10, cfa.oss_operator(dm, doss, dinv), amg)
+        assert s.converged, label
+        xh = host(x)
+        Ax = O.spmv(rp, ci, Kp, xh)
+        O.oss_apply(m, rp, ci, oss, inv_m, xh, Ax)
+        assert np.linalg.norm(rhs - Ax) <= 1.5e-10 * np.linalg.norm(rhs), label
+    assert abs(its["phase"] - its["fp64"]) <= 1, its
+    assert its["phase"] <= its["fp32"], its
+    with pytest.raises(cfa.CfaError):
+        cfa.AmgPreconditioner(ctx, cfa.MIXED).set_fp64_phase(1.0)
+
+
 @pytest.mark.parametrize("host_prec", [False, True])
 def test_pcg_host_ops_match_handles(ctx, host_prec):
     """solve_pcg with the OSS term (and optionally the preconditioner) as host callbacks, the way
