@@ -340,3 +340,27 @@ def test_oracle_matches_reference_gpu(name):
     xl, repl = O.pcg(rp, ci, h["lap_val"], np.cos(0.11 * np.arange(n)), np.zeros(n), 400, 1e-10, amg=amgl)
     assert repl.converged and abs(repl.iterations - g["lap_pcg_info"][0]) <= 1
     assert np.abs(xl - g["lap_pcg_x"]).max() < 1e-8 * np.abs(g["lap_pcg_x"]).max()
+
+
+def test_fp64_first_phase_keeps_the_fp64_iteration_count():
+    """The CPU emulation of the V-cycle per precision (oracle/vcycle_precision.py) on the c0
+    pressure system: the V-cycle in FP32 throughout takes more PCG iterations to 1e-10 than in
+    FP64, and FP64 V-cycles down to 1e-2 of the initial residual followed by FP32 ones take the
+    FP64 count: the schedule of the mixed-precision solves."""
+    from oracle import vcycle_precision as VP
+    m = F.make_mesh("c0")
+    rp, ci, Kp, rhs, oss, inv_m = VP.pressure_system(m)
+
+    def op(x):
+        y = O.spmv(rp, ci, Kp, x)
+        O.oss_apply(m, rp, ci, oss, inv_m, x, y)
+        return y
+
+    h = VP.Hierarchy(rp, ci, Kp)
+    nl = len(h.levels)
+    all64, all32 = h.cast([np.float64] * nl), h.cast([np.float32] * nl)
+    it64 = VP.pcg_iterations(h, op, rhs, all64)
+    it32 = VP.pcg_iterations(h, op, rhs, all32)
+    itph = VP.pcg_iterations(h, op, rhs, all64, all32, 1e-2)
+    assert 0 < it64 < it32
+    assert itph == it64
