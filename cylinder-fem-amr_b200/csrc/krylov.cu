@@ -498,6 +498,7 @@ k_cg_resid0(int n, const double* __restrict__ b, const double* __restrict__ q, d
         reduce_partials<1>(v, part, counter, sh);
         if (threadIdx.x == 0) {
             const double rn = sqrt(v[0]);
+            st->rel = rn / st->bnorm;
             if (rn < st->tol * st->bnorm) {
                 st->done = 1;
                 st->converged = 1;
@@ -1475,7 +1476,9 @@ static cfa_status pcg_piece(cfa_ctx* ctx, PcgWork& W, const PcgArgs& a, int piec
 // Between the two phases of a mixed-precision solve: where the FP64 phase stopped at its switch
 // threshold (converged there, iterations left), the solve continues to the final tolerance: the
 // stop is undone and the WHILE condition of the second phase set. Otherwise (the final
-// tolerance already met, a breakdown, the iteration limit) the second phase does nothing.
+// tolerance already met, a breakdown, the iteration limit) the second phase does nothing. A
+// warm start below the threshold stops the first phase at its initial residual (no iteration;
+// p is still zero there, so the resumed V-cycle's beta multiplies nothing).
 __global__ void k_cg_phase(CgState* st, double tol, CondArg cond) {
     CFA_GRID_DEP();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;

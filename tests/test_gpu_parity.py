@@ -738,6 +738,19 @@ def test_pcg_fp64_phase_of_a_mixed_hierarchy(ctx, graphs, monkeypatch):
         assert np.linalg.norm(rhs - Ax) <= 1.5e-10 * np.linalg.norm(rhs), label
     assert abs(its["phase"] - its["fp64"]) <= 1, its
     assert its["phase"] <= its["fp32"], its
+    # a warm start below the switch: the first phase stops at its initial residual, the second
+    # iterates to the tolerance
+    x0 = xh + 1e-5 * np.abs(xh).max() * np.sin(0.37 * np.arange(m.n))
+    r0 = O.spmv(rp, ci, Kp, x0)
+    O.oss_apply(m, rp, ci, oss, inv_m, x0, r0)
+    assert 1e-9 < np.linalg.norm(rhs - r0) / np.linalg.norm(rhs) < 1e-2
+    x = dev(x0)
+    it = s.solve_pcg(m.n, dm.rp, dm.ci, dK, db, x, 4000, 1e-10, cfa.oss_operator(dm, doss, dinv), amg)
+    assert s.converged and it >= 1
+    xh = host(x)
+    Ax = O.spmv(rp, ci, Kp, xh)
+    O.oss_apply(m, rp, ci, oss, inv_m, xh, Ax)
+    assert np.linalg.norm(rhs - Ax) <= 1.5e-10 * np.linalg.norm(rhs)
     with pytest.raises(cfa.CfaError):
         cfa.AmgPreconditioner(ctx, cfa.MIXED).set_fp64_phase(1.0)
 
