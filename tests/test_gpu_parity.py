@@ -740,7 +740,7 @@ def test_pcg_fp64_phase_of_a_mixed_hierarchy(ctx, graphs, monkeypatch):
     assert its["phase"] <= its["fp32"], its
     # a warm start below the switch: the first phase stops at its initial residual, the second
     # iterates to the tolerance
-    x0 = xh + 1e-5 * np.abs(xh).max() * np.sin(0.37 * np.arange(m.n))
+    x0 = xh + 1e-8 * np.abs(xh).max() * np.sin(0.37 * np.arange(m.n))
     r0 = O.spmv(rp, ci, Kp, x0)
     O.oss_apply(m, rp, ci, oss, inv_m, x0, r0)
     assert 1e-9 < np.linalg.norm(rhs - r0) / np.linalg.norm(rhs) < 1e-2
