@@ -75,6 +75,10 @@ class DragAdjoint:
         self.mom = cfa.GpuBicgstab2(self.ctx)
         self.pcg = cfa.GpuLinearSolver(self.ctx)
         self.amg = cfa.AmgPreconditioner(self.ctx, precision)
+        # the loop's solves start from the neighbouring step's solution, mostly below the FP64
+        # phase's switch already, so the phase would add its setup and launches for nothing
+        if precision == cfa.MIXED:
+            self.amg.set_fp64_phase(0.0)
         self.amg_ready = False
         self.drag = []
 
