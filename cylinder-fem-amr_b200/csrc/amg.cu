@@ -2398,7 +2398,7 @@ static cfa_status tune_level(cfa_ctx* ctx, cfa_amg* amg, AmgLevel& L, int vb) {
 // (CFA_FP64_PHASE; 0 keeps them FP32 throughout).
 static double fp64_phase_env() {
     const char* e = std::getenv("CFA_FP64_PHASE");
-    if (!e || !*e) return 1e-2;
+    if (!e || !*e) return 1e-1;
     const double v = std::atof(e);
     return v > 0.0 && v < 1.0 ? v : 0.0;
 }

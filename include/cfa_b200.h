@@ -445,7 +445,7 @@ cfa_status cfa_amg_composite(const cfa_amg* amg, int* level, int* rows, const do
 cfa_status cfa_amg_set_vcycle(cfa_amg* amg, int composite_rows, int fuse_levels, int fold_rows);
 /* Mixed-precision handles (no counterpart in the reference): the Krylov solves preconditioned by
  * this handle run their V-cycles in FP64 until the relative residual falls below switch_rel and
- * in FP32 after that, for the setups that follow (0: FP32 throughout; negative: the default 1e-2
+ * in FP32 after that, for the setups that follow (0: FP32 throughout; negative: the default 1e-1
  * or CFA_FP64_PHASE). The FP32 V-cycle's rounding, about 1e-7 of the residual it is applied to,
  * enters the CG's search directions and costs iterations near a tight tolerance only when it is
  * made while the residual is still large; the FP64 copy of the level tiles costs setup time and
