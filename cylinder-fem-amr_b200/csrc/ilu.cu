@@ -555,11 +555,12 @@ k_ilu_last_perm(int n, int c1, const int* __restrict__ pos, const int* __restric
 
 template <class V, class T>
 static void sweeps_perm(cfa_ctx* ctx, const cfa_ilu* h, const V* lv, const V* uv, const V* dinv,
-                        typename Pair<T>::type* w, const double2* r, double2* z, const int* done) {
+                        typename Pair<T>::type* w, const double2* r, double2* z, const int* done, bool staged) {
     static const int early = env_flag("CFA_ILU_EARLY", 1);
     const int n = h->n;
-    CFA_LAUNCH(ctx, (k_ilu_first_perm<T>), ceil_div(n, kThreads), kThreads, 0, n, (const int*)h->pos.p, r, w, done,
-               early);
+    if (!staged)
+        CFA_LAUNCH(ctx, (k_ilu_first_perm<T>), ceil_div(n, kThreads), kThreads, 0, n, (const int*)h->pos.p, r, w,
+                   done, early);
     for (int c = 1; c < h->nc; ++c) {
         const int cs = h->colour_start[c], m = h->colour_start[c + 1] - cs;
         if (m == 0) continue;
@@ -657,23 +658,36 @@ cfa_status ilu_apply(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z,
     return CFA_OK;
 }
 
-cfa_status ilu_apply_pair(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z, const int* done) {
+bool ilu_pair_staging(const cfa_ilu* h, IluStaging* out) {
+    if (!h || h->nc < 2 || !env_flag("CFA_ILU_PERM", 1) || !env_flag("CFA_ILU_STAGED", 1)) return false;
+    const bool f32 = h->precision == CFA_MIXED;
+    void* w = f32 ? (void*)h->work32.p : (void*)h->work64.p;
+    if (!w || !h->pos.p) return false;
+    out->pos = h->pos.p;
+    out->w = w;
+    out->fp32 = f32 ? 1 : 0;
+    return true;
+}
+
+cfa_status ilu_apply_pair(cfa_ctx* ctx, const cfa_ilu* h, const double* r, double* z, const int* done, bool staged) {
     const double2* r2 = reinterpret_cast<const double2*>(r);
     double2* z2 = reinterpret_cast<double2*>(z);
     // colour order (default) or, with CFA_ILU_PERM=0, the reference's natural row order
     const bool colour_order = env_flag("CFA_ILU_PERM", 1) && h->nc >= 2;
+    if (staged && !colour_order)
+        return set_error(ctx, CFA_BAD_ARG, "staged ILU apply without the colour-order work vector", __FILE__, __LINE__);
     if (h->precision == CFA_MIXED) {
         // FP32 factors, FP32 sweeps on the handle's FP32 work vector; FP64 in and out
         if (!h->work32.p || h->work32.cap < 2 * (size_t)h->n)
             return set_error(ctx, CFA_BAD_ARG, "ILU handle without its FP32 work vector", __FILE__, __LINE__);
         float2* w = reinterpret_cast<float2*>(h->work32.p);
-        if (colour_order) sweeps_perm<float, float>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r2, z2, done);
+        if (colour_order) sweeps_perm<float, float>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r2, z2, done, staged);
         else sweeps_pair<float, float, true>(ctx, h, h->lv32.p, h->uv32.p, h->dinv32.p, w, r2, z2, done);
     } else if (colour_order) {
         if (!h->work64.p || h->work64.cap < 2 * (size_t)h->n)
             return set_error(ctx, CFA_BAD_ARG, "ILU handle without its FP64 work vector", __FILE__, __LINE__);
         sweeps_perm<double, double>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p,
-                                    reinterpret_cast<double2*>(h->work64.p), r2, z2, done);
+                                    reinterpret_cast<double2*>(h->work64.p), r2, z2, done, staged);
     } else {
         sweeps_pair<double, double, false>(ctx, h, h->lv64.p, h->uv64.p, h->dinv64.p, z2, r2, z2, done);
     }

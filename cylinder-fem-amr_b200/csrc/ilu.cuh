@@ -40,5 +40,18 @@ cfa_status ilu_apply(cfa_ctx* ctx, const cfa_ilu* ilu, const double* r, double* 
 // z = (LU)^-1 r for the two components of the momentum solve stored interleaved per row
 // (r[2i], r[2i + 1] = u_i, v_i; 16-byte aligned): FP64 handles sweep in FP64 in place in z, mixed
 // handles sweep in FP32 on the handle's FP32 work vector. FP64 in and out.
-cfa_status ilu_apply_pair(cfa_ctx* ctx, const cfa_ilu* ilu, const double* r, double* z, const int* done);
+// staged: the apply's first pass (the right-hand side into the colour-order work vector) was done
+// by the kernel that produced r, as ilu_pair_staging describes.
+cfa_status ilu_apply_pair(cfa_ctx* ctx, const cfa_ilu* ilu, const double* r, double* z, const int* done,
+                          bool staged = false);
+// The colour-order work vector of the pair apply, for a kernel that produces the apply's
+// right-hand side and can also write it there: w[pos[i]] = row i's pair in the work precision
+// (fp32: float2, else double2). False where the apply has no such pass (natural row order, one
+// colour) or CFA_ILU_STAGED=0.
+struct IluStaging {
+    const int* pos;
+    void* w;
+    int fp32;
+};
+bool ilu_pair_staging(const cfa_ilu* ilu, IluStaging* out);
 }  // namespace cfa

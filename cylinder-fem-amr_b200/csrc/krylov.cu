@@ -734,8 +734,18 @@ k_b2_init(int n, const int* __restrict__ rp, const int* __restrict__ ci, const d
 }
 
 // p = r + cb (p - co v) (k_bicg2_p)
+// The ILU apply's first pass done here (ilu_pair_staging): the new pair also goes to its
+// colour position in the apply's work vector, in the work precision (w32 or w64; both null: not
+// staged).
+__device__ __forceinline__ void b2_stage(int i, double2 v, const int* __restrict__ pos, float2* __restrict__ w32,
+                                         double2* __restrict__ w64) {
+    if (w32) w32[pos[i]] = make_float2((float)v.x, (float)v.y);
+    else if (w64) w64[pos[i]] = v;
+}
+
 __global__ void k_b2_p(int n, const double2* __restrict__ r, const double2* __restrict__ v, double2* __restrict__ p,
-                       const B2State* __restrict__ st) {
+                       const B2State* __restrict__ st, const int* __restrict__ pos, float2* __restrict__ w32,
+                       double2* __restrict__ w64) {
     CFA_GRID_DEP();
     if (st->done) return;
     const double cb0 = st->cb[0], cb1 = st->cb[1], co0 = st->co[0], co1 = st->co[1];
@@ -745,6 +755,7 @@ __global__ void k_b2_p(int n, const double2* __restrict__ r, const double2* __re
         pp.x = rr.x + cb0 * (pp.x - co0 * vv.x);
         pp.y = rr.y + cb1 * (pp.y - co1 * vv.y);
         p[i] = pp;
+        b2_stage(i, pp, pos, w32, w64);
     }
 }
 
@@ -794,13 +805,16 @@ k_b2_v(int n, const int* __restrict__ rp, const int* __restrict__ ci, const doub
 
 // s = r - ca v (k_bicg2_s)
 __global__ void k_b2_s(int n, const double2* __restrict__ r, const double2* __restrict__ v, double2* __restrict__ s,
-                       const B2State* __restrict__ st) {
+                       const B2State* __restrict__ st, const int* __restrict__ pos, float2* __restrict__ w32,
+                       double2* __restrict__ w64) {
     CFA_GRID_DEP();
     if (st->done) return;
     const double a0 = st->ca[0], a1 = st->ca[1];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double2 rr = r[i], vv = v[i];
-        s[i] = make_double2(rr.x - a0 * vv.x, rr.y - a1 * vv.y);
+        const double2 ss = make_double2(rr.x - a0 * vv.x, rr.y - a1 * vv.y);
+        s[i] = ss;
+        b2_stage(i, ss, pos, w32, w64);
     }
 }
 
@@ -1900,14 +1914,20 @@ static cfa_status b2_body(cfa_ctx* ctx, B2Work& W, const B2Args& a, CondArg cond
     const int grid = row_grid(ctx, n, tpr);
     const int gv = row_grid(ctx, n, 1);
     const int* done = &W.st.p->done;
-    CFA_LAUNCH(ctx, k_b2_p, gv, kThreads, 0, n, pair(W.r.p), pair(W.v.p), pair(W.p.p), W.st.p);
-    CFA_PROPAGATE(ilu_apply_pair(ctx, a.ilu, W.p.p, W.phat.p, done));
+    // p and s written into the ILU apply's work vector as they are formed (its first pass)
+    IluStaging stg{};
+    const bool staged = ilu_pair_staging(a.ilu, &stg);
+    const int* spos = staged ? stg.pos : nullptr;
+    float2* w32 = staged && stg.fp32 ? static_cast<float2*>(stg.w) : nullptr;
+    double2* w64 = staged && !stg.fp32 ? static_cast<double2*>(stg.w) : nullptr;
+    CFA_LAUNCH(ctx, k_b2_p, gv, kThreads, 0, n, pair(W.r.p), pair(W.v.p), pair(W.p.p), W.st.p, spos, w32, w64);
+    CFA_PROPAGATE(ilu_apply_pair(ctx, a.ilu, W.p.p, W.phat.p, done, staged));
     if (W.tiled) launch_b2t<1>(ctx, W, a, W.phat.p, W.r0.p, W.v.p, cond);
     else
         OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_v<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, pair(W.phat.p),
                                       pair(W.r0.p), pair(W.v.p), W.st.p, W.part.p, W.counter.p, cond));
-    CFA_LAUNCH(ctx, k_b2_s, gv, kThreads, 0, n, pair(W.r.p), pair(W.v.p), pair(W.s.p), W.st.p);
-    CFA_PROPAGATE(ilu_apply_pair(ctx, a.ilu, W.s.p, W.shat.p, done));
+    CFA_LAUNCH(ctx, k_b2_s, gv, kThreads, 0, n, pair(W.r.p), pair(W.v.p), pair(W.s.p), W.st.p, spos, w32, w64);
+    CFA_PROPAGATE(ilu_apply_pair(ctx, a.ilu, W.s.p, W.shat.p, done, staged));
     if (W.tiled) launch_b2t<2>(ctx, W, a, W.shat.p, W.s.p, W.t.p, cond);
     else
         OP_TPR_SWITCH(tpr, CFA_LAUNCH(ctx, (k_b2_t<TPR>), grid, kThreads, 0, n, a.rp, a.ci, a.val, pair(W.shat.p),
