@@ -579,11 +579,13 @@ def run_adjoint(args):
     torch.cuda.synchronize()
     t_grad = (time.perf_counter() - t0) * 1e3
     clk.stop()
-    # central difference with h = 1e-4 U: its truncation error (h^2 J'''/6, about 1e-9 relative
-    # here) and the solves' 1e-12 noise in J divided by h (a few 1e-9) stay below the check's
-    # tolerance; with h = 1e-6 U the noise alone is about 1e-7
-    h = 1e-4 * U_MAX
-    fd = (adj.objective(U_MAX + h) - adj.objective(U_MAX - h)) / (2 * h)
+    # central differences with h = 1e-6 U (the workload's step) and h = 1e-4 U: at 1e-6 the
+    # solves' 1e-12 noise in J divided by h is about 1e-7 of dJ/dU; at 1e-4 it and the truncation
+    # error (h^2 J'''/6) are both near 1e-8
+    fds = {}
+    for rel in (1e-6, 1e-4):
+        h = rel * U_MAX
+        fds[rel] = (adj.objective(U_MAX + h) - adj.objective(U_MAX - h)) / (2 * h)
     ref = make(cfa.FP64)
     J64, g64, gu64 = ref.gradient()
     line = {
@@ -594,7 +596,9 @@ def run_adjoint(args):
         "config": {"workload": f"c3: c1 mesh n={m.n}, dt 5e-3, U 1.5, nu 1e-3, from the inflow profile, "
                                f"OSS stab {stab:g}, checkpoints every 20 steps, solves to 1e-12",
                    "forward_ms": round(t_fwd, 1), "J_mean_drag": J,
-                   "dJ_dU": g_u, "dJ_dU_central_fd_h1e-4": fd, "fd_rel_diff": abs(g_u - fd) / abs(fd),
+                   "dJ_dU": g_u, "dJ_dU_central_fd_h1e-6": fds[1e-6], "dJ_dU_central_fd_h1e-4": fds[1e-4],
+                   "fd_rel_diff": abs(g_u - fds[1e-6]) / abs(fds[1e-6]),
+                   "fd_rel_diff_h1e-4": abs(g_u - fds[1e-4]) / abs(fds[1e-4]),
                    "dJ_dnu_norm": float(torch.linalg.norm(g_nu)),
                    "fp64_grad_rel_diff": float(torch.abs(g_nu - g64).max() / torch.abs(g64).max()),
                    "fp64_dJ_dU_rel_diff": abs(g_u - gu64) / abs(gu64)},
