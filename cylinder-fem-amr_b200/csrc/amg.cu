@@ -1532,8 +1532,8 @@ bool amg_prescale(const cfa_amg* amg, PreScale* out, bool fp64) {
     return true;
 }
 
-// Off unless CFA_CG_FUSE_UPDATE=1: measured at c1 the folded step was not faster (13.78 against
-// 13.60 ms without setup): the pre-smoothing pass gathers q beside r for every entry and the
+// Off unless CFA_CG_FUSE_UPDATE=1: measured on the 402k-vertex step the folded form was not
+// faster (13.78 against 13.60 ms without setup): the pre-smoothing pass gathers q beside r for every entry and the
 // residual pass takes the grid reduction, which cost what the update kernel's launch saved.
 bool amg_can_fuse_update(const cfa_amg* amg) {
     const char* e = std::getenv("CFA_CG_FUSE_UPDATE");
@@ -2203,8 +2203,8 @@ __global__ void k_sym_check(int n, const int* __restrict__ arp, const int* __res
 
 // Pipeline depth of the level tiles (CFA_VC_STAGES, default 2). Two stages leave room for more
 // CTAs per SM (six instead of four on the finest level's 256-row FP32 tiles) and more rows'
-// gathers in flight, while two waves of tiles in flight still cover the DRAM latency: the c2
-// V-cycle 692 -> 620 us, the c1 one unchanged. The pressure operator keeps three.
+// gathers in flight, while two waves of tiles in flight still cover the DRAM latency: the
+// 4.2M-row V-cycle 692 -> 620 us, the 402k-row one unchanged. The pressure operator keeps three.
 static int level_tile_stages() {
     static const int s = [] {
         const char* e = std::getenv("CFA_VC_STAGES");

@@ -152,8 +152,9 @@ cfa_status amg_vcycle(cfa_ctx* ctx, cfa_amg* amg, const double* r, double* z, co
 // FP64 tiles and switches to the FP32 V-cycle once its relative residual falls below the
 // returned threshold (0: no FP64 phase). The FP32 V-cycle's rounding, about 1e-7 of the
 // residual it is applied to, enters the CG's search directions; while the residual is large
-// those errors are large against the final 1e-10 and cost iterations at the end (59 -> 67 on
-// the c1 pressure system), but below about 1e-1 of the initial residual they stay below it.
+// those errors are large against the final 1e-10 and cost iterations at the end (67 instead of
+// 59 on a 402k-vertex pressure system), but made below about 1e-1 of the initial residual they
+// stay below it.
 double amg_fp64_phase(const cfa_amg* amg);
 
 // The CG's dots after the preconditioner (r.z, and z.q for the flexible beta) folded into the

@@ -327,7 +327,7 @@ k_ilu_upper_pair(int m, const int* __restrict__ rows, const int* __restrict__ up
 
 // Runtime switches of the pair sweeps, read once: CFA_ILU_EARLY=0 drops the early dependent
 // launch, CFA_ILU_HINT=1 turns on the evict-first loads of the streamed factors (measured slower
-// on the c1 and c2 meshes), CFA_ILU_PERM=0 selects the natural-order sweeps below instead of the
+// on the 402k- and 4.2M-vertex meshes), CFA_ILU_PERM=0 selects the natural-order sweeps below instead of the
 // colour-order ones.
 static int env_flag(const char* name, int def) {
     const char* e = std::getenv(name);

@@ -145,7 +145,7 @@ struct DevBuf {
 // griddepcontrol.wait returns once the preceding grid has completed and its writes are visible,
 // before this kernel reads or writes anything. For a kernel launched without the attribute it is
 // a no-op. It removes part of the launch gap between the short dependent kernels of a V-cycle
-// (c1 step 17.4 -> 16.8 ms). For kernels that wait at entry an explicit early launch_dependents
+// (402k-vertex step 17.4 -> 16.8 ms). For kernels that wait at entry an explicit early launch_dependents
 // was slower (17.7 ms): blocks of the next kernel parked on the SMs while the current one still
 // ran. The tile kernels (tiled.cuh: tile_loop_dep) and the ILU sweeps (ilu.cu) load constant data
 // (their first tiles, the factors) before they wait, so there the early signal pays.

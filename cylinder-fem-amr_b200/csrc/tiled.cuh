@@ -47,14 +47,14 @@ struct TileView {
 // V-cycle's level tiles (CFA_L2_VC, default 0), each 0 (normal), 1 (evict first) or 2 (evict
 // last). The operator's stream is read once per CG iteration and is larger than what the rest of
 // the iteration touches; marked evict-first it no longer pushes the V-cycle's levels and the
-// Krylov vectors out of L2 (c1 step 13.56 -> 13.36 ms). Evict-last on the level tiles changed
+// Krylov vectors out of L2 (402k-vertex step 13.56 -> 13.36 ms). Evict-last on the level tiles changed
 // nothing measurable.
 int l2_hint_operator();
 int l2_hint_vcycle();
 
 // Tile kernels signal their dependent launch (griddepcontrol.launch_dependents) right after
 // issuing their first tile copies, so the next kernel's blocks are scheduled and issue their own
-// first copies while this kernel runs (c1 step 15.72 -> 15.11 ms); CFA_TILE_EARLY=0 turns it off.
+// first copies while this kernel runs (402k-vertex step 15.72 -> 15.11 ms); CFA_TILE_EARLY=0 turns it off.
 bool tile_early_enabled();
 
 // Host-side description + device buffers of a tiled matrix.
