@@ -135,6 +135,7 @@ def solve_system(ctx: cfa.Context, sysm: BatchSystem, precision: int, tol: float
     # one solve per hierarchy: the plain level chain, whose setup is cheapest (the composite
     # operator and the fused transfers pay back only over repeated solves)
     st.amg.set_vcycle(0, 0, 0)
+    st.amg.set_aggregation(0)   # the device aggregation's waiting blocks would hold SMs the other streams use
     st.amg_setup()          # assembly, ILU factor, BiCGSTAB2, pressure system, AMG setup
     st.solve_pressure()
     ev1.record()

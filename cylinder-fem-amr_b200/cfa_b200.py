@@ -600,6 +600,13 @@ class AmgPreconditioner:
         if s != CFA_OK:
             raise CfaError(s, "cfa_amg_set_fp64_phase")
 
+    def set_aggregation(self, on_device: int = -1):
+        """The setups' greedy aggregation on the device (1, the default) or the host (0); -1
+        follows CFA_AGG_HOST. Both give the same aggregates."""
+        s = lib().cfa_amg_set_aggregation(self._handle(), on_device)
+        if s != CFA_OK:
+            raise CfaError(s, "cfa_amg_set_aggregation")
+
     def composite(self):
         """(level, rows) of the composite coarse operator, level -1 when there is none."""
         lv, rows = C.c_int(), C.c_int()

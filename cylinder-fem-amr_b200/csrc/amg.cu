@@ -1987,12 +1987,14 @@ static cfa_status aggregate_device(cfa_ctx* ctx, SetupScratch& S, const DCsr& A,
 }
 
 
-// Greedy 3-phase aggregation of smoothed_prolongator (:1321-1348) on the host strength flags.
-// CFA_AGG_HOST=0: the aggregation runs as the device rounds; otherwise as the reference's
-// sequential host loop.
-static bool agg_on_host() {
+// Greedy 3-phase aggregation of smoothed_prolongator (:1321-1348) on the host strength flags
+// (aggregate_host, the reference's sequential loop) or in the device rounds (aggregate_device).
+// The greedy aggregation on the host (the reference's loop) or on the device (the same
+// aggregates): the handle's choice (cfa_amg_set_aggregation), else CFA_AGG_HOST, else the device.
+static bool agg_on_host(const cfa_amg* amg) {
+    if (amg->vc_agg_device >= 0) return amg->vc_agg_device == 0;
     const char* e = std::getenv("CFA_AGG_HOST");
-    return !(e && e[0] == '0');
+    return e && e[0] == '1';
 }
 
 static int aggregate_host(int n, const int* rp, const int* ci, const unsigned char* strong, int* agg) {
@@ -2591,7 +2593,7 @@ static cfa_status amg_setup(cfa_ctx* ctx, cfa_amg* amg, int n, int nnz, const in
                    S.strong.p);
         CFA_CUDA(L.agg.ensure(m));
         int na = 0;
-        if (!agg_on_host()) {
+        if (!agg_on_host(amg)) {
             CFA_PROPAGATE(aggregate_device(ctx, S, A, L.agg.p, &na));
             if (na >= (int)(0.85 * m) || na == 0) break;   // coarsening stalled (:1019)
         } else {
@@ -2946,6 +2948,12 @@ cfa_status cfa_amg_set_vcycle(cfa_amg* amg, int composite_rows, int fuse_levels,
     amg->vc_composite_rows = composite_rows < 0 ? -1 : composite_rows;
     amg->vc_fuse = fuse_levels < 0 ? -1 : fuse_levels;
     amg->vc_fold_rows = fold_rows < 0 ? -1 : fold_rows;
+    return CFA_OK;
+}
+
+cfa_status cfa_amg_set_aggregation(cfa_amg* amg, int on_device) {
+    if (!amg || on_device > 1) return CFA_BAD_ARG;
+    amg->vc_agg_device = on_device < 0 ? -1 : on_device;
     return CFA_OK;
 }
 

@@ -125,6 +125,8 @@ struct cfa_amg {
     // value asked for by cfa_amg_set_fp64_phase (-1: CFA_FP64_PHASE or the default)
     double phase_switch = 0.0;
     double vc_fp64_phase = -1.0;
+    // aggregation on the device (1) or the host (0); -1: CFA_AGG_HOST or the device
+    int vc_agg_device = -1;
 };
 
 namespace cfa {

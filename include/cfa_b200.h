@@ -451,6 +451,14 @@ cfa_status cfa_amg_set_vcycle(cfa_amg* amg, int composite_rows, int fuse_levels,
  * made while the residual is still large; the FP64 copy of the level tiles costs setup time and
  * memory. CFA_BAD_ARG for switch_rel >= 1. */
 cfa_status cfa_amg_set_fp64_phase(cfa_amg* amg, double switch_rel);
+/* Where the setups that follow run the greedy aggregation (the reference's host loop,
+ * src/cfa/linalg.cuh:1321-1348): on the device (1, the default), on the host (0), or as
+ * CFA_AGG_HOST says (-1; CFA_AGG_HOST=1 selects the host). Both give the same aggregates. The
+ * device form decides each phase in one launch whose blocks wait on one another's decisions; it
+ * is the faster one for a single solve stream, while callers that overlap many small setups on
+ * several streams (the batch path) keep the SMs free with the host loop. CFA_BAD_ARG for
+ * on_device > 1. */
+cfa_status cfa_amg_set_aggregation(cfa_amg* amg, int on_device);
 
 /* The assembled OSS term of the pressure operator (apply_oss_projection,
  * src/cfa/device.cuh:316-323): A x = K x - B^T M^-1 B x on non-Dirichlet rows. */
