@@ -887,6 +887,10 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
       O* __restrict__ y, const int* __restrict__ done, RzFuse rzf, const T* __restrict__ xc, CgFuse cgf) {
     extern __shared__ __align__(128) unsigned char tsmem[];
     double dots[2] = {0.0, 0.0};   // RZ: this thread's rows of r.z and z.q; CGU (residual): of |r|^2
+    // gathers issued together per lane: with four or more lanes the Galerkin levels' rows carry
+    // five or six entries per lane, so a batch of eight issues a third of its slots predicated
+    // off; the entries are summed in the same order whatever the batch
+    constexpr int kVcBatch = TPR >= 4 ? 6 : kGatherBatch;
     // the level's tiles are packed at setup: their first copies go out before the wait
     const bool go = tile_loop_dep(tv, tsmem, [&] { return !(done && *done); },
                                   [&](int, int r0, int nr, const unsigned char* ch) {
@@ -920,13 +924,13 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
             T s = (T)0, s1 = (T)0;
             if (valid) {
                 const int end = rr[lr + 1];
-                for (int e0 = rr[lr] + lane; e0 < end; e0 += kGatherBatch * TPR) {
+                for (int e0 = rr[lr] + lane; e0 < end; e0 += kVcBatch * TPR) {
                     // all loads of the batch first, then the sums in entry order
-                    V a[kGatherBatch], a1[kGatherBatch];
-                    T g0[kGatherBatch];
-                    B g1[kGatherBatch];
+                    V a[kVcBatch], a1[kVcBatch];
+                    T g0[kVcBatch];
+                    B g1[kVcBatch];
 #pragma unroll
-                    for (int u = 0; u < kGatherBatch; ++u) {
+                    for (int u = 0; u < kVcBatch; ++u) {
                         const int e = e0 + u * TPR;
                         if (e < end) {
                             const int j = cs[e];
@@ -942,7 +946,7 @@ k_vct(TileView tv, const T* __restrict__ dinv, T omega, const B* __restrict__ b,
                         }
                     }
 #pragma unroll
-                    for (int u = 0; u < kGatherBatch; ++u)
+                    for (int u = 0; u < kVcBatch; ++u)
                         if (e0 + u * TPR < end) {
                             if (OP == VC_PRE) s += (T)a[u] * mul_rn(omega * g0[u], (T)g1[u]);
                             else s += (T)a[u] * g0[u];
